@@ -1,0 +1,318 @@
+"""Benchmark of the explicit RK3 residual-and-update path (one JSON line on rank 0).
+
+Workload (the configuration the headline metric is quoted on): 3-D sine-wave advection
+on the perturbed curvilinear periodic grid of 256^3 intervals (257^3 nodes, 4 ghost
+layers), WENO7 primitive reconstruction + AUSM+, 8th-order collocated viscous terms
+(mu = 1e-4 constant, Pr = 0.72), SSP-RK3 at a fixed dt equal to the CFL-0.5 step of the
+initial state.  One "step" = one full SSP-RK3 step (3 stages) of the whole block; one
+cell-update = one interior node advanced through one step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cb200|reference] [--n 256]
+
+--impl reference times the reference algorithm's CPU form on the host cores: the FP64
+oracle (the reference has no CPU implementation of this path; its kernels are CUDA only),
+on a bounded sample of the same workload.
+Under torchrun each rank runs an independent replica of the workload on its own GPU
+(weak scaling, no data-path collective); rank 0 prints the line.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "corefl-cpc_b200"))
+
+METRIC = "RK3 cell-updates/s, mixed vs FP64 at equal L1 error; p50/p99 solve latency"
+UNIT = "cell-updates/s"
+
+# Compulsory FP64 HBM traffic of each kernel per node it processes (every array it reads or
+# writes counted once), used for the roofline of the dominant kernel.
+KERNEL_BYTES_PER_NODE = {
+    "pv_flux_x": 8 * (5 + 3 + 1 + 10), "pv_flux_y": 8 * (5 + 3 + 1 + 10), "pv_flux_z": 8 * (5 + 3 + 1 + 10),
+    "weno_char_x": 8 * (5 + 2 + 3 + 1 + 10), "weno_char_y": 8 * (5 + 2 + 3 + 1 + 10),
+    "weno_char_z": 8 * (5 + 2 + 3 + 1 + 10),
+    "visc8_node_flux": 8 * (4 + 9 + 1 + 12), "visc8_divergence": 8 * (12 + 1 + 8),
+    "stage_update": 8 * (5 + 5 + 5 + 1 + 5 + 6),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cb200", choices=["cb200", "reference"])
+    ap.add_argument("--n", type=int, default=256, help="intervals per direction of the sine-wave grid")
+    ap.add_argument("--cpu-n", type=int, default=48, help="intervals of the CPU-baseline sample grid")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms while running (read-only query)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.th = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.th = threading.Thread(target=self._read, daemon=True)
+        self.th.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.th:
+            self.th.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(args, seconds=None):
+    """FP64 oracle (all host threads) on the sine-wave workload at --cpu-n intervals."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle_py
+    from cb200 import cases
+    n = args.cpu_n
+    case = cases.sine_wave(n=n)
+    p, b, faces = case.param, case.blocks[0], case.faces[0]
+    threads = os.cpu_count() or 1
+    oracle_py.set_threads(threads)
+    oracle_py.boundary(p, b, faces)
+    oracle_py.properties(p, b)
+    dt = oracle_py.cfl_dt(p, b)
+    oracle_py.rk3_step(p, [b], [faces], dt, True)  # warm-up step
+    budget = seconds if seconds is not None else args.cpu_seconds
+    t0 = time.perf_counter()
+    steps = 0
+    while True:
+        oracle_py.rk3_step(p, [b], [faces], dt, True)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= budget or steps >= 50:
+            break
+    nodes = case.n_nodes
+    return {"value": nodes * steps / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"FP64 oracle, sine-wave WENO7+AUSM+/visc8 on {n}^3 intervals ({nodes} nodes), "
+                      f"{steps} RK3 steps in {el:.1f} s", "steps": steps, "seconds": el}
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return
+    base = cpu_baseline(args)
+    line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": base["steps"], "warmup": 1, "ms_per_step": 1e3 * base["seconds"] / base["steps"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"sine-wave 3-D curvilinear periodic, WENO7+AUSM+, 8th-order viscous, "
+                                   f"sample {args.cpu_n}^3 intervals of the {args.n}^3 workload",
+                       "l2": "n/a (CPU)"},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def load_traffic():
+    """DRAM bytes per node of each kernel from the committed ncu summary, if present."""
+    try:
+        with open(os.path.join(REPO, "profiles", "traffic_per_node.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def gpu_arm(args, rank, world, local_rank):
+    import torch
+    import cb200
+    from cb200 import cases
+    from cb200.field import DeviceBlock
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    case = cases.sine_wave(n=args.n)
+    p, hb, faces = case.param, case.blocks[0], case.faces[0]
+    dev = DeviceBlock(hb, device=f"cuda:{local_rank}")
+    host_state = {n: hb.a[n] for n in ("cv", "bv")}
+    del case, hb
+    ctx = cb200.Context(p)
+    ctx.bind(0, dev.view(), faces)
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    ctx.properties(0, sh)
+    dt = ctx.cfl_dt(sh)
+    nodes = (args.n + 1) ** 3
+
+    for _ in range(args.warmup):
+        ctx.rk3_step(dt, True, sh)
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.5)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    n0 = ctx.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        ctx.rk3_step(dt, True, sh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = ctx.launch_count() - n0
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+        ms = float(t.item())
+    clocks = sampler.stop() if sampler else None
+    status = ctx.read_status(sh)
+
+    # per-kernel durations of one profiled step (same stream, CUDA events)
+    ctx.profile(True)
+    ctx.rk3_step(dt, True, sh)
+    torch.cuda.synchronize()
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    total = sum(v[1] for v in prof.values())
+    top = max(prof.items(), key=lambda kv: kv[1][1])
+    kname, (kcount, kms) = top
+    avg_ms = kms / kcount
+    bpn = KERNEL_BYTES_PER_NODE.get(kname)
+    peak, peak_kind = measured_peaks()
+    roof = None
+    if bpn:
+        achieved = bpn * nodes / (avg_ms * 1e-3) / 1e9
+        traffic = load_traffic().get(kname)
+        roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": (traffic * nodes if traffic else None),
+                "algorithmic_bytes": bpn * nodes, "avg_launch_ms": avg_ms,
+                "share": kms / total}
+
+    e2e = None
+    if not args.no_e2e:
+        pin = {n: torch.from_numpy(a).pin_memory() for n, a in host_state.items()}
+        out_cv = torch.empty_like(pin["cv"]).pin_memory()
+        h2d = sum(t.numel() * 8 for t in pin.values())
+        d2h = out_cv.numel() * 8
+        k_e2e = max(1, min(args.steps, 5))
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        for _ in range(k_e2e):
+            dev.t["cv"].copy_(pin["cv"], non_blocking=True)
+            dev.t["bv"].copy_(pin["bv"], non_blocking=True)
+            ctx.rk3_step(dt, True, sh)
+            out_cv.copy_(dev.t["cv"], non_blocking=True)
+        e3.record(stream)
+        torch.cuda.synchronize()
+        ms_e = e2.elapsed_time(e3)
+        if dist:
+            t = torch.tensor([ms_e], device=f"cuda:{local_rank}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_e = float(t.item())
+        e2e = {"value": world * nodes * k_e2e / (ms_e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "steps": k_e2e, "ms_per_step": ms_e / k_e2e}
+
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    base = None if args.no_cpu_baseline else cpu_baseline(args)
+    value = world * nodes * args.steps / (ms * 1e-3)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"sine-wave advection, 3-D curvilinear periodic grid {args.n}^3 intervals "
+                                   f"({args.n + 1}^3 nodes, 4 ghost layers), WENO7 reconstruction + AUSM+, "
+                                   f"8th-order collocated viscous (mu=1e-4, Pr=0.72), SSP-RK3 fixed dt",
+                       "dt": dt, "precision": "plain FP64", "per_gpu_nodes": nodes,
+                       "l2": "inputs larger than L2 (about 7 GB of field arrays per GPU)",
+                       "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
+            "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clocks, "status_flags": status,
+            "kernel_ms_per_step": {k: v[1] for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+    gpu_arm(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,56 @@
+"""ctypes mirror of include/cb200.h (structs and constants)."""
+import ctypes as C
+
+ABI_VERSION = 1
+
+OK = 0
+ERR_CUDA, ERR_INVALID, ERR_NONPHYSICAL, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_NOMEM = -1, -2, -3, -4, -5, -6
+
+INV_ROE, INV_AUSMP, INV_HLLC = 2, 3, 4
+INV_WENO5_CP, INV_WENO5_CH, INV_WENO7_CP, INV_WENO7_CH = 51, 52, 71, 72
+REC_FIRST, REC_MUSCL, REC_NND2, REC_WENO5, REC_WENO7 = 1, 2, 3, 5, 7
+BC_WALL, BC_SYMMETRY, BC_INFLOW, BC_OUTFLOW, BC_PERIODIC = 2, 3, 5, 6, 8
+PREC_FP64, PREC_MIXED = 0, 1
+RHS_VISCOUS, RHS_CHEMISTRY, RHS_INVISCID, RHS_ALL = 1, 2, 4, 7
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+ZONE_ARRAYS = ("cv", "bv", "sv", "qn", "dq", "metric", "jac", "mul", "thermal_conductivity", "rho_D",
+               "acoustic_speed", "gamma", "mach", "fFlux", "gFlux", "hFlux", "vis_flux", "shock_sensor",
+               "dt_local", "reaction_timeScale", "entropy_fix_delta")
+
+
+class ZoneView(C.Structure):
+    _fields_ = [("mx", C.c_int), ("my", C.c_int), ("mz", C.c_int), ("ngg", C.c_int)] + \
+               [(n, C.c_void_p) for n in ZONE_ARRAYS]
+
+
+class FaceBC(C.Structure):
+    _fields_ = [("type", C.c_int), ("face", C.c_int), ("direction", C.c_int),
+                ("range_start", C.c_int * 3), ("range_end", C.c_int * 3),
+                ("rho", C.c_double), ("u", C.c_double), ("v", C.c_double), ("w", C.c_double),
+                ("p", C.c_double), ("T", C.c_double), ("wall_temperature", C.c_double)]
+
+
+MECH_DOUBLE = ("mw", "low_temp_coeff", "high_temp_coeff", "t_low", "t_mid", "t_high", "geometry",
+               "LJ_potent_inv", "vis_coeff", "WjDivWi_to_One4th", "sqrt_WiDivWjPl1Mul8",
+               "binary_diffusivity_coeff", "kb_over_eps_jk", "ZRotF298")
+MECH_INT = ("reac_type", "rev_type", "stoi_f", "stoi_b", "reac_order")
+MECH_REAC = ("A", "b", "Ea", "A2", "b2", "Ea2", "third_body_coeff", "troe_alpha", "troe_t3", "troe_t1", "troe_t2")
+
+
+class Mechanism(C.Structure):
+    _fields_ = [("n_spec", C.c_int), ("n_reac", C.c_int)] + \
+               [(n, _dp) for n in MECH_DOUBLE] + [(n, _ip) for n in MECH_INT] + [(n, _dp) for n in MECH_REAC]
+
+
+class ParamView(C.Structure):
+    _fields_ = [("abi_version", C.c_int), ("dim", C.c_int), ("n_var", C.c_int), ("n_spec", C.c_int),
+                ("n_scalar", C.c_int), ("n_scalar_transported", C.c_int), ("inviscid_scheme", C.c_int),
+                ("reconstruction", C.c_int), ("limiter", C.c_int), ("viscous_order", C.c_int),
+                ("positive_preserving", C.c_int), ("gradP_in_diffusion_flux", C.c_int), ("reaction", C.c_int),
+                ("shock_sensor", C.c_int), ("sensor_eps", C.c_double), ("sensor_threshold", C.c_double),
+                ("entropy_fix_factor", C.c_double), ("Pr", C.c_double), ("cfl", C.c_double),
+                ("rho_ref", C.c_double), ("v_ref", C.c_double), ("mu_constant", C.c_double),
+                ("precision", C.c_int), ("mech", C.POINTER(Mechanism))]

@@ -1,0 +1,148 @@
+"""ctypes binding of libcb200.so.
+
+The shared library is the product: if it is missing this module raises instead of falling
+back to anything else.
+"""
+import ctypes as C
+import os
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "libcb200.so")
+_lib = None
+
+
+class CB2Error(RuntimeError):
+    def __init__(self, code, what):
+        self.code = code
+        lib = load()
+        msg = lib.cb2_strerror(code).decode()
+        if code == abi.ERR_CUDA:
+            msg += ": " + lib.cb2_last_cuda_error().decode()
+        super().__init__(f"{what} failed ({code}): {msg}")
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(f"{LIB_PATH} is not built; run corefl-cpc_b200/build.py")
+    lib = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    P = C.POINTER
+    sig = {
+        "cb2_init": (C.c_int, [P(abi.ParamView), P(vp)]),
+        "cb2_bind_block": (C.c_int, [vp, C.c_int, P(abi.ZoneView), P(abi.FaceBC), C.c_int]),
+        "cb2_destroy": (None, [vp]),
+        "cb2_store_qn": (C.c_int, [vp, C.c_int, vp]),
+        "cb2_rhs": (C.c_int, [vp, C.c_int, C.c_uint, vp]),
+        "cb2_stage_update": (C.c_int, [vp, C.c_int, C.c_double, C.c_int, vp]),
+        "cb2_boundary": (C.c_int, [vp, C.c_int, vp]),
+        "cb2_properties": (C.c_int, [vp, C.c_int, vp]),
+        "cb2_cv_from_bv": (C.c_int, [vp, C.c_int, vp]),
+        "cb2_cfl_dt": (C.c_int, [vp, P(C.c_double), vp]),
+        "cb2_rk3_step": (C.c_int, [vp, P(C.c_double), C.c_int, vp]),
+        "cb2_read_status": (C.c_int, [vp, P(C.c_uint), vp]),
+        "cb2_strerror": (C.c_char_p, [C.c_int]),
+        "cb2_last_cuda_error": (C.c_char_p, []),
+        "cb2_launch_count": (C.c_ulonglong, [vp]),
+        "cb2_profile_enable": (C.c_int, [vp, C.c_int]),
+        "cb2_profile_reset": (C.c_int, [vp]),
+        "cb2_profile_count": (C.c_int, [vp]),
+        "cb2_profile_entry": (C.c_int, [vp, C.c_int, C.c_char_p, C.c_int, P(C.c_ulonglong), P(C.c_double)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc, what):
+    if rc != abi.OK:
+        raise CB2Error(rc, what)
+
+
+class Context:
+    """Owns one cb2_ctx; blocks are bound by index."""
+
+    def __init__(self, param: abi.ParamView):
+        self.lib = load()
+        self._param = param  # keep the mechanism arrays alive
+        h = C.c_void_p()
+        check(self.lib.cb2_init(C.byref(param), C.byref(h)), "cb2_init")
+        self.h = h
+        self._keep = {}
+
+    def bind(self, blk, zone_view, faces):
+        from .field import faces_array
+        arr = faces_array(faces)
+        self._keep[blk] = (zone_view, arr)
+        check(self.lib.cb2_bind_block(self.h, blk, C.byref(zone_view), arr, len(faces)), "cb2_bind_block")
+
+    def rhs(self, blk, mask=abi.RHS_ALL, stream=None):
+        check(self.lib.cb2_rhs(self.h, blk, mask, stream), "cb2_rhs")
+
+    def stage_update(self, blk, dt, rk, stream=None):
+        check(self.lib.cb2_stage_update(self.h, blk, dt, rk, stream), "cb2_stage_update")
+
+    def boundary(self, blk, stream=None):
+        check(self.lib.cb2_boundary(self.h, blk, stream), "cb2_boundary")
+
+    def properties(self, blk, stream=None):
+        check(self.lib.cb2_properties(self.h, blk, stream), "cb2_properties")
+
+    def cv_from_bv(self, blk, stream=None):
+        check(self.lib.cb2_cv_from_bv(self.h, blk, stream), "cb2_cv_from_bv")
+
+    def store_qn(self, blk, stream=None):
+        check(self.lib.cb2_store_qn(self.h, blk, stream), "cb2_store_qn")
+
+    def cfl_dt(self, stream=None):
+        dt = C.c_double()
+        check(self.lib.cb2_cfl_dt(self.h, C.byref(dt), stream), "cb2_cfl_dt")
+        return dt.value
+
+    def rk3_step(self, dt, fixed_dt=True, stream=None):
+        d = C.c_double(dt)
+        check(self.lib.cb2_rk3_step(self.h, C.byref(d), 1 if fixed_dt else 0, stream), "cb2_rk3_step")
+        return d.value
+
+    def read_status(self, stream=None):
+        f = C.c_uint()
+        check(self.lib.cb2_read_status(self.h, C.byref(f), stream), "cb2_read_status")
+        return f.value
+
+    def launch_count(self):
+        return int(self.lib.cb2_launch_count(self.h))
+
+    def profile(self, on=True):
+        check(self.lib.cb2_profile_enable(self.h, 1 if on else 0), "cb2_profile_enable")
+
+    def profile_reset(self):
+        check(self.lib.cb2_profile_reset(self.h), "cb2_profile_reset")
+
+    def profile_read(self):
+        """{kernel name: (launches, total ms)} of the launches recorded while profiling."""
+        out = {}
+        n = self.lib.cb2_profile_count(self.h)
+        buf = C.create_string_buffer(128)
+        cnt, ms = C.c_ulonglong(), C.c_double()
+        for i in range(n):
+            check(self.lib.cb2_profile_entry(self.h, i, buf, 128, C.byref(cnt), C.byref(ms)), "cb2_profile_entry")
+            out[buf.value.decode()] = (int(cnt.value), float(ms.value))
+        return out
+
+    def close(self):
+        if self.h:
+            self.lib.cb2_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

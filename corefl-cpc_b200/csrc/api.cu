@@ -1,0 +1,584 @@
+// extern "C" entry points of libcb200 (declared in include/cb200.h) and the RK3 step
+// orchestration (the stage body of RK3<mix>, src/RK.cuh:107-237).
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "common.cuh"
+#include "launch.h"
+
+namespace cb2 {
+
+static thread_local std::string g_cuda_error;
+
+void set_cuda_error(cudaError_t e) { g_cuda_error = cudaGetErrorString(e); }
+
+// ---- per-launch profiler ------------------------------------------------------------------
+struct Profiler {
+  struct Rec {
+    std::string name;
+    cudaEvent_t a, b;
+  };
+  std::vector<Rec> open;                      // recorded, not yet resolved
+  std::vector<cudaEvent_t> pool;              // reusable events
+  std::vector<std::string> names;             // aggregated results
+  std::vector<unsigned long long> counts;
+  std::vector<double> total_ms;
+  cudaEvent_t take() {
+    if (!pool.empty()) {
+      cudaEvent_t e = pool.back();
+      pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+  void resolve() {
+    for (auto &r : open) {
+      cudaEventSynchronize(r.b);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, r.a, r.b);
+      size_t k = 0;
+      while (k < names.size() && names[k] != r.name) ++k;
+      if (k == names.size()) {
+        names.push_back(r.name);
+        counts.push_back(0);
+        total_ms.push_back(0);
+      }
+      counts[k] += 1;
+      total_ms[k] += ms;
+      pool.push_back(r.a);
+      pool.push_back(r.b);
+    }
+    open.clear();
+  }
+  ~Profiler() {
+    for (auto &r : open) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    for (auto e : pool) cudaEventDestroy(e);
+  }
+};
+
+thread_local Profiler *g_prof = nullptr;
+
+void prof_begin(Profiler *p, const char *name, cudaStream_t s) {
+  Profiler::Rec r{name, p->take(), p->take()};
+  cudaEventRecord(r.a, s);
+  p->open.push_back(r);
+}
+
+void prof_end(Profiler *p, cudaStream_t s) {
+  if (!p->open.empty()) cudaEventRecord(p->open.back().b, s);
+}
+
+struct Block {
+  bool bound = false;
+  cb2_zone_view v{};
+  Zone z{};
+  std::vector<FaceBC> faces;
+  int *d_btype = nullptr;  // six face flag arrays, one allocation
+};
+
+}  // namespace cb2
+
+using namespace cb2;
+
+struct cb2_ctx {
+  Param p{};
+  cb2_param_view view{};
+  void *d_tables = nullptr;  // mechanism tables (one allocation)
+  unsigned *d_status = nullptr;
+  double *d_dtmin = nullptr;     // running min of the CFL dt
+  double *d_partial = nullptr;   // per-CTA partial minima of the reduction
+  int n_partial = 0;
+  std::vector<Block> blocks;
+  unsigned long long n_launch = 0;
+  Profiler *prof = nullptr;  // non-null while profiling is enabled
+};
+
+namespace {
+// Makes the context's profiler current for this thread while an entry point runs.
+struct ProfGuard {
+  Profiler *prev;
+  explicit ProfGuard(cb2_ctx *ctx) : prev(g_prof) { g_prof = ctx ? ctx->prof : nullptr; }
+  ~ProfGuard() { g_prof = prev; }
+};
+}  // namespace
+
+namespace {
+
+int fail_cuda(cudaError_t e) {
+  set_cuda_error(e);
+  return CB2_ERR_CUDA;
+}
+
+// Copies the mechanism into one device allocation and fills the device pointers of Mech.
+int upload_mechanism(const cb2_mechanism &m, cb2_ctx *ctx) {
+  const int ns = m.n_spec, nr = m.n_reac;
+  std::vector<double> buf;
+  std::vector<int> ibuf;
+  struct DSlot { const double **dst; size_t off; };
+  struct ISlot { const int **dst; size_t off; };
+  std::vector<DSlot> ds;
+  std::vector<ISlot> is;
+  Mech &d = ctx->p.mech;
+  auto addd = [&](const double **dst, const double *src, size_t n) {
+    ds.push_back({dst, buf.size()});
+    for (size_t a = 0; a < n; ++a) buf.push_back(src ? src[a] : 0.0);
+  };
+  auto addi = [&](const int **dst, const int *src, size_t n) {
+    is.push_back({dst, ibuf.size()});
+    for (size_t a = 0; a < n; ++a) ibuf.push_back(src ? src[a] : 0);
+  };
+  // 1/mw, R_u/mw and 1/(1/mw) exactly as DParameter and the transport kernel derive them
+  std::vector<double> imw(ns), rg(ns), mw2(ns);
+  for (int s = 0; s < ns; ++s) {
+    imw[s] = 1.0 / m.mw[s];
+    rg[s] = kRu / m.mw[s];
+    mw2[s] = 1.0 / imw[s];
+  }
+  addd(&d.imw, imw.data(), ns);
+  addd(&d.gas_const, rg.data(), ns);
+  addd(&d.mw, mw2.data(), ns);
+  addd(&d.lo, m.low_temp_coeff, (size_t)ns * 7);
+  addd(&d.hi, m.high_temp_coeff, (size_t)ns * 7);
+  addd(&d.t_low, m.t_low, ns);
+  addd(&d.t_mid, m.t_mid, ns);
+  addd(&d.t_high, m.t_high, ns);
+  addd(&d.geometry, m.geometry, ns);
+  addd(&d.lj_inv, m.LJ_potent_inv, ns);
+  addd(&d.vis_coeff, m.vis_coeff, ns);
+  addd(&d.wjwi14, m.WjDivWi_to_One4th, (size_t)ns * ns);
+  addd(&d.sqwiwj8, m.sqrt_WiDivWjPl1Mul8, (size_t)ns * ns);
+  addd(&d.bdc, m.binary_diffusivity_coeff, (size_t)ns * ns);
+  addd(&d.kbe, m.kb_over_eps_jk, (size_t)ns * ns);
+  addd(&d.zrot, m.ZRotF298, ns);
+  addd(&d.A, m.A, nr);
+  addd(&d.b, m.b, nr);
+  addd(&d.Ea, m.Ea, nr);
+  addd(&d.A2, m.A2, nr);
+  addd(&d.b2, m.b2, nr);
+  addd(&d.Ea2, m.Ea2, nr);
+  addd(&d.tbc, m.third_body_coeff, (size_t)nr * ns);
+  addd(&d.troe_alpha, m.troe_alpha, nr);
+  addd(&d.troe_t3, m.troe_t3, nr);
+  addd(&d.troe_t1, m.troe_t1, nr);
+  addd(&d.troe_t2, m.troe_t2, nr);
+  addi(&d.reac_type, m.reac_type, nr);
+  addi(&d.rev_type, m.rev_type, nr);
+  addi(&d.stoi_f, m.stoi_f, (size_t)nr * ns);
+  addi(&d.stoi_b, m.stoi_b, (size_t)nr * ns);
+  addi(&d.reac_order, m.reac_order, nr);
+  const size_t bd = buf.size() * sizeof(double), bi = ibuf.size() * sizeof(int);
+  char *dev = nullptr;
+  cudaError_t e = cudaMalloc(&dev, bd + bi + 16);
+  if (e != cudaSuccess) return fail_cuda(e);
+  ctx->d_tables = dev;
+  if (bd) { e = cudaMemcpy(dev, buf.data(), bd, cudaMemcpyHostToDevice); if (e) return fail_cuda(e); }
+  if (bi) { e = cudaMemcpy(dev + bd, ibuf.data(), bi, cudaMemcpyHostToDevice); if (e) return fail_cuda(e); }
+  for (auto &s : ds) *s.dst = reinterpret_cast<const double *>(dev) + s.off;
+  for (auto &s : is) *s.dst = reinterpret_cast<const int *>(dev + bd) + s.off;
+  d.n_spec = ns;
+  d.n_reac = nr;
+  return CB2_OK;
+}
+
+// register_boundary (src/Mesh.cpp:14-32): the face is the first dimension whose start and
+// end coincide, the low face points to -1; with `extend` the tangential ranges grow by ngg,
+// and for 2-D blocks the k range becomes [-ngg, ngg] (or [0, 0] without extension).
+FaceBC register_face(const cb2_face_bc &f, int dim, int ngg, bool extend) {
+  FaceBC b{};
+  b.type = f.type;
+  for (int a = 0; a < 3; ++a) { b.start[a] = f.range_start[a]; b.end[a] = f.range_end[a]; }
+  b.face = f.face;
+  b.direction = f.direction;
+  const int gx = extend ? ngg : 0;
+  for (int a = 0; a < dim; ++a) {
+    if (a == b.face) continue;
+    if (b.end[a] < b.start[a]) { int t = b.end[a]; b.end[a] = b.start[a]; b.start[a] = t; }
+    b.start[a] -= gx;
+    b.end[a] += gx;
+  }
+  if (dim == 2) { b.start[2] = -gx; b.end[2] = gx; }
+  b.rho = f.rho; b.u = f.u; b.v = f.v; b.w = f.w; b.p = f.p; b.T = f.T; b.wall_T = f.wall_temperature;
+  return b;
+}
+
+Zone make_zone(const cb2_zone_view &v) {
+  Zone z{};
+  z.mx = v.mx; z.my = v.my; z.mz = v.mz; z.ngg = v.ngg;
+  z.L = make_layout(v.mx, v.my, v.mz, v.ngg);
+  z.L0 = make_layout(v.mx, v.my, v.mz, 0);
+  z.L1 = make_layout(v.mx, v.my, v.mz, 1);
+  z.cv = v.cv; z.bv = v.bv; z.sv = v.sv; z.qn = v.qn; z.dq = v.dq; z.metric = v.metric; z.jac = v.jac;
+  z.mul = v.mul; z.kappa = v.thermal_conductivity; z.rhoD = v.rho_D; z.acoustic = v.acoustic_speed;
+  z.gamma = v.gamma; z.mach = v.mach; z.fF = v.fFlux; z.gF = v.gFlux; z.hF = v.hFlux; z.visf = v.vis_flux;
+  z.shock = v.shock_sensor; z.dtl = v.dt_local; z.rts = v.reaction_timeScale; z.efd = v.entropy_fix_delta;
+  return z;
+}
+
+Block *get_block(cb2_ctx *ctx, int blk) {
+  if (!ctx || blk < 0 || blk >= (int)ctx->blocks.size() || !ctx->blocks[blk].bound) return nullptr;
+  return &ctx->blocks[blk];
+}
+
+int count(cb2_ctx *ctx, int n) {
+  ctx->n_launch += (unsigned long long)n;
+  return CB2_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *cb2_strerror(int code) {
+  switch (code) {
+    case CB2_OK: return "ok";
+    case CB2_ERR_CUDA: return "CUDA runtime error";
+    case CB2_ERR_INVALID: return "invalid argument";
+    case CB2_ERR_NONPHYSICAL: return "non-physical state";
+    case CB2_ERR_TIMEOUT: return "device wait timed out";
+    case CB2_ERR_UNSUPPORTED: return "unsupported scheme/model combination";
+    case CB2_ERR_NOMEM: return "out of device memory";
+    default: return "unknown error";
+  }
+}
+
+const char *cb2_last_cuda_error(void) { return g_cuda_error.c_str(); }
+
+unsigned long long cb2_launch_count(const cb2_ctx *ctx) { return ctx ? ctx->n_launch : 0ull; }
+
+int cb2_init(const cb2_param_view *pv, cb2_ctx **out) {
+  if (!pv || !out) return CB2_ERR_INVALID;
+  *out = nullptr;
+  if (pv->abi_version != CB2_ABI_VERSION) return CB2_ERR_INVALID;
+  const int ns = pv->mech ? pv->mech->n_spec : 0;
+  if (pv->n_spec != ns) return CB2_ERR_INVALID;
+  if (ns != 0 && ns != 5 && ns != 9) return CB2_ERR_UNSUPPORTED;
+  if (pv->n_var != 5 + ns || pv->n_scalar != ns) return CB2_ERR_UNSUPPORTED;
+  const int sch = pv->inviscid_scheme;
+  const bool weno_ch = sch == CB2_INV_WENO5_CH || sch == CB2_INV_WENO7_CH;
+  const bool pvpath = sch == CB2_INV_AUSMP || sch == CB2_INV_HLLC || sch == CB2_INV_ROE || (sch == 1 && ns == 0);
+  if (!weno_ch && !pvpath) return CB2_ERR_UNSUPPORTED;
+  if (pvpath) {
+    const int r = pv->reconstruction;
+    if (!(r == 1 || r == 2 || r == 3 || r == 5 || r == 7)) return CB2_ERR_INVALID;
+  }
+  if (pv->viscous_order != 0 && pv->viscous_order != 2 && pv->viscous_order != 8) return CB2_ERR_INVALID;
+  if (pv->viscous_order == 8 && ns != 0) return CB2_ERR_UNSUPPORTED;
+  if (pv->positive_preserving) return CB2_ERR_UNSUPPORTED;
+  if (pv->reaction) return CB2_ERR_UNSUPPORTED;
+  if (pv->precision != CB2_PREC_FP64) return CB2_ERR_UNSUPPORTED;
+  if (pv->sensor_threshold > 1e-10) return CB2_ERR_UNSUPPORTED;  // shock sensor kernel not built
+  cb2_ctx *ctx = new cb2_ctx;
+  ctx->view = *pv;
+  Param &p = ctx->p;
+  p.dim = pv->dim;
+  p.n_var = pv->n_var;
+  p.n_spec = ns;
+  p.n_scalar = pv->n_scalar;
+  p.n_scalar_transported = pv->n_scalar_transported;
+  p.n_reac = pv->mech ? pv->mech->n_reac : 0;
+  p.inviscid_scheme = sch;
+  p.reconstruction = pv->reconstruction;
+  p.limiter = pv->limiter;
+  p.viscous_order = pv->viscous_order;
+  p.positive_preserving = pv->positive_preserving;
+  p.gradP = pv->gradP_in_diffusion_flux;
+  p.reaction = pv->reaction;
+  p.shock_sensor = pv->shock_sensor;
+  p.sensor_eps = pv->sensor_eps;
+  p.sensor_threshold = pv->sensor_threshold;
+  p.entropy_fix_factor = pv->entropy_fix_factor;
+  p.Pr = pv->Pr;
+  p.cfl = pv->cfl;
+  p.rho_ref = pv->rho_ref;
+  p.v_ref = pv->v_ref;
+  // weno_eps_scale = (rho_inf v_inf)^2 (src/DParameter.cu:29-32)
+  p.weno_eps_scale = pv->rho_ref * pv->v_ref * pv->rho_ref * pv->v_ref;
+  p.mu_constant = pv->mu_constant;
+  p.precision = pv->precision;
+  int rc = CB2_OK;
+  if (pv->mech) rc = upload_mechanism(*pv->mech, ctx);
+  if (rc == CB2_OK) {
+    cudaError_t e = cudaMalloc(&ctx->d_status, sizeof(unsigned) + 2 * sizeof(double));
+    if (e != cudaSuccess) rc = fail_cuda(e);
+    else {
+      e = cudaMemset(ctx->d_status, 0, sizeof(unsigned));
+      if (e != cudaSuccess) rc = fail_cuda(e);
+      ctx->d_dtmin = reinterpret_cast<double *>(reinterpret_cast<char *>(ctx->d_status) + sizeof(double));
+      p.status = ctx->d_status;
+    }
+  }
+  if (rc != CB2_OK) {
+    cb2_destroy(ctx);
+    return rc;
+  }
+  *out = ctx;
+  return CB2_OK;
+}
+
+void cb2_destroy(cb2_ctx *ctx) {
+  if (!ctx) return;
+  for (auto &b : ctx->blocks) cudaFree(b.d_btype);
+  cudaFree(ctx->d_tables);
+  cudaFree(ctx->d_status);
+  cudaFree(ctx->d_partial);
+  delete ctx->prof;
+  delete ctx;
+}
+
+int cb2_profile_enable(cb2_ctx *ctx, int on) {
+  if (!ctx) return CB2_ERR_INVALID;
+  if (on && !ctx->prof) ctx->prof = new Profiler;
+  if (!on && ctx->prof) {
+    ctx->prof->resolve();
+    delete ctx->prof;
+    ctx->prof = nullptr;
+  }
+  return CB2_OK;
+}
+
+int cb2_profile_count(cb2_ctx *ctx) {
+  if (!ctx || !ctx->prof) return 0;
+  ctx->prof->resolve();
+  return (int)ctx->prof->names.size();
+}
+
+int cb2_profile_entry(cb2_ctx *ctx, int idx, char *name, int name_len, unsigned long long *count,
+                      double *total_ms) {
+  if (!ctx || !ctx->prof || !name || name_len < 1 || !count || !total_ms) return CB2_ERR_INVALID;
+  Profiler &p = *ctx->prof;
+  p.resolve();
+  if (idx < 0 || idx >= (int)p.names.size()) return CB2_ERR_INVALID;
+  std::snprintf(name, (size_t)name_len, "%s", p.names[idx].c_str());
+  *count = p.counts[idx];
+  *total_ms = p.total_ms[idx];
+  return CB2_OK;
+}
+
+int cb2_profile_reset(cb2_ctx *ctx) {
+  if (!ctx || !ctx->prof) return CB2_ERR_INVALID;
+  ctx->prof->resolve();
+  ctx->prof->names.clear();
+  ctx->prof->counts.clear();
+  ctx->prof->total_ms.clear();
+  return CB2_OK;
+}
+
+int cb2_bind_block(cb2_ctx *ctx, int blk, const cb2_zone_view *v, const cb2_face_bc *faces, int n_faces) {
+  if (!ctx || !v || blk < 0 || n_faces < 0 || (n_faces > 0 && !faces)) return CB2_ERR_INVALID;
+  if (v->mx < 1 || v->my < 1 || v->mz < 1 || v->ngg < 1) return CB2_ERR_INVALID;
+  const Param &p = ctx->p;
+  const int need_g = (p.inviscid_scheme == CB2_INV_WENO7_CH || p.reconstruction == CB2_REC_WENO7 ||
+                      p.viscous_order == 8) ? 4
+                     : (p.inviscid_scheme == CB2_INV_WENO5_CH || p.reconstruction == CB2_REC_WENO5) ? 3 : 2;
+  if (v->ngg < need_g) return CB2_ERR_INVALID;
+  if (!v->cv || !v->bv || !v->dq || !v->metric || !v->jac || !v->qn) return CB2_ERR_INVALID;
+  if (p.n_spec > 0 && (!v->sv || !v->acoustic_speed || !v->gamma || !v->mul || !v->thermal_conductivity ||
+                       !v->rho_D))
+    return CB2_ERR_INVALID;
+  if (p.viscous_order > 0 && !v->mul) return CB2_ERR_INVALID;
+  if (p.viscous_order == 8 && (!v->fFlux || !v->gFlux || !v->hFlux)) return CB2_ERR_INVALID;
+  if (p.inviscid_scheme == CB2_INV_ROE && !v->entropy_fix_delta) return CB2_ERR_INVALID;
+  for (int f = 0; f < n_faces; ++f) {
+    const auto &b = faces[f];
+    if (b.face < 0 || b.face > 2 || (b.direction != 1 && b.direction != -1)) return CB2_ERR_INVALID;
+    if (b.type != CB2_BC_OUTFLOW && b.type != CB2_BC_PERIODIC && b.type != CB2_BC_WALL &&
+        b.type != CB2_BC_SYMMETRY && b.type != CB2_BC_INFLOW)
+      return CB2_ERR_INVALID;
+  }
+  if ((int)ctx->blocks.size() <= blk) ctx->blocks.resize(blk + 1);
+  Block &B = ctx->blocks[blk];
+  cudaFree(B.d_btype);
+  B.d_btype = nullptr;
+  B.v = *v;
+  B.z = make_zone(*v);
+  B.faces.clear();
+  const bool extend = p.viscous_order == 2;
+  for (int f = 0; f < n_faces; ++f) B.faces.push_back(register_face(faces[f], p.dim, v->ngg, extend));
+  // physical-boundary flags per face node, from the raw (unextended) ranges (src/Mesh.cpp:855-900)
+  const int mx = v->mx, my = v->my, mz = v->mz;
+  std::vector<int> il(my * mz, 0), ir(my * mz, 0), jl(mx * mz, 0), jr(mx * mz, 0), kl(mx * my, 0), kr(mx * my, 0);
+  for (int f = 0; f < n_faces; ++f) {
+    const auto &b = faces[f];
+    if (b.type == CB2_BC_PERIODIC) continue;
+    int lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = b.range_start[a] < b.range_end[a] ? b.range_start[a] : b.range_end[a];
+      hi[a] = b.range_start[a] < b.range_end[a] ? b.range_end[a] : b.range_start[a];
+    }
+    for (int a = 0; a < 3; ++a) { if (lo[a] < 0) lo[a] = 0; }
+    if (hi[0] >= mx) hi[0] = mx - 1;
+    if (hi[1] >= my) hi[1] = my - 1;
+    if (hi[2] >= mz) hi[2] = mz - 1;
+    for (int k = lo[2]; k <= hi[2]; ++k)
+      for (int j = lo[1]; j <= hi[1]; ++j)
+        for (int i = lo[0]; i <= hi[0]; ++i) {
+          if (b.face == 0) (b.direction < 0 ? il : ir)[j + k * my] = b.type;
+          else if (b.face == 1) (b.direction < 0 ? jl : jr)[i + k * mx] = b.type;
+          else (b.direction < 0 ? kl : kr)[i + j * mx] = b.type;
+        }
+  }
+  const size_t n_all = il.size() + ir.size() + jl.size() + jr.size() + kl.size() + kr.size();
+  cudaError_t e = cudaMalloc(&B.d_btype, n_all * sizeof(int));
+  if (e != cudaSuccess) return fail_cuda(e);
+  std::vector<int> all;
+  all.reserve(n_all);
+  for (auto *vv : {&il, &ir, &jl, &jr, &kl, &kr}) all.insert(all.end(), vv->begin(), vv->end());
+  e = cudaMemcpy(B.d_btype, all.data(), n_all * sizeof(int), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return fail_cuda(e);
+  size_t off = 0;
+  const int *base = B.d_btype;
+  B.z.bt.il = base + off; off += il.size();
+  B.z.bt.ir = base + off; off += ir.size();
+  B.z.bt.jl = base + off; off += jl.size();
+  B.z.bt.jr = base + off; off += jr.size();
+  B.z.bt.kl = base + off; off += kl.size();
+  B.z.bt.kr = base + off;
+  // reduction scratch sized for the largest bound block
+  const int np = min_reduce_partials((long long)mx * my * mz);
+  if (np > ctx->n_partial) {
+    cudaFree(ctx->d_partial);
+    ctx->d_partial = nullptr;
+    e = cudaMalloc(&ctx->d_partial, np * sizeof(double));
+    if (e != cudaSuccess) { ctx->n_partial = 0; return fail_cuda(e); }
+    ctx->n_partial = np;
+  }
+  B.bound = true;
+  return CB2_OK;
+}
+
+int cb2_store_qn(cb2_ctx *ctx, int blk, void *stream) {
+  Block *B = get_block(ctx, blk);
+  if (!B) return CB2_ERR_INVALID;
+  ProfGuard pg(ctx);
+  cudaStream_t s = (cudaStream_t)stream;
+  ProfScope prof("store_qn", s);
+  const size_t bytes = (size_t)B->z.L.sz * ctx->p.n_var * sizeof(double);
+  return check_cuda(cudaMemcpyAsync(B->z.qn, B->z.cv, bytes, cudaMemcpyDeviceToDevice, s));
+}
+
+int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream) {
+  Block *B = get_block(ctx, blk);
+  if (!B) return CB2_ERR_INVALID;
+  ProfGuard pg(ctx);
+  cudaStream_t s = (cudaStream_t)stream;
+  const Param &p = ctx->p;
+  if ((mask & CB2_RHS_CHEMISTRY) && p.reaction) return CB2_ERR_UNSUPPORTED;
+  int nl = 0;
+  {
+    ProfScope prof("zero_dq", s);
+    CB2_TRY(check_cuda(cudaMemsetAsync(B->z.dq, 0, (size_t)B->z.L0.sz * p.n_var * sizeof(double), s)));
+  }
+  if ((mask & CB2_RHS_VISCOUS) && p.viscous_order > 0)
+    CB2_TRY(launch_viscous(B->z, p, B->faces.data(), (int)B->faces.size(), s, nl));
+  if (mask & CB2_RHS_INVISCID) {
+    if (p.inviscid_scheme == CB2_INV_WENO5_CH || p.inviscid_scheme == CB2_INV_WENO7_CH)
+      CB2_TRY(launch_inviscid_char(B->z, p, s, nl));
+    else
+      CB2_TRY(launch_inviscid_pv(B->z, p, s, nl));
+  }
+  return count(ctx, nl);
+}
+
+int cb2_stage_update(cb2_ctx *ctx, int blk, double dt, int rk, void *stream) {
+  Block *B = get_block(ctx, blk);
+  if (!B || rk < 0 || rk > 2) return CB2_ERR_INVALID;
+  ProfGuard pg(ctx);
+  int nl = 0;
+  CB2_TRY(launch_stage_update(B->z, ctx->p, dt, rk, (cudaStream_t)stream, nl));
+  return count(ctx, nl);
+}
+
+int cb2_boundary(cb2_ctx *ctx, int blk, void *stream) {
+  Block *B = get_block(ctx, blk);
+  if (!B) return CB2_ERR_INVALID;
+  ProfGuard pg(ctx);
+  int nl = 0;
+  cudaStream_t s = (cudaStream_t)stream;
+  CB2_TRY(launch_boundary(B->z, ctx->p, B->faces.data(), (int)B->faces.size(), s, nl));
+  if (ctx->p.dim == 2 && B->z.mz == 1) CB2_TRY(launch_eliminate_k_gradient(B->z, ctx->p, s, nl));
+  return count(ctx, nl);
+}
+
+int cb2_properties(cb2_ctx *ctx, int blk, void *stream) {
+  Block *B = get_block(ctx, blk);
+  if (!B) return CB2_ERR_INVALID;
+  ProfGuard pg(ctx);
+  int nl = 0;
+  CB2_TRY(launch_properties(B->z, ctx->p, (cudaStream_t)stream, nl));
+  return count(ctx, nl);
+}
+
+int cb2_cv_from_bv(cb2_ctx *ctx, int blk, void *stream) {
+  Block *B = get_block(ctx, blk);
+  if (!B) return CB2_ERR_INVALID;
+  ProfGuard pg(ctx);
+  int nl = 0;
+  CB2_TRY(launch_cv_from_bv(B->z, ctx->p, (cudaStream_t)stream, nl));
+  return count(ctx, nl);
+}
+
+// Enqueues the CFL dt of every bound block and their minimum into ctx->d_dtmin.
+static int enqueue_cfl_dt(cb2_ctx *ctx, cudaStream_t s) {
+  int nl = 0;
+  CB2_TRY(launch_set_value(ctx->d_dtmin, 1e+6, s, nl));
+  for (auto &B : ctx->blocks) {
+    if (!B.bound) continue;
+    if (!B.z.dtl) return CB2_ERR_INVALID;
+    CB2_TRY(launch_local_dt(B.z, ctx->p, s, nl));
+    const long long n = (long long)B.z.mx * B.z.my * B.z.mz;
+    CB2_TRY(launch_min_reduce(B.z.dtl, n, ctx->d_partial, min_reduce_partials(n), ctx->d_dtmin, s, nl));
+  }
+  return count(ctx, nl);
+}
+
+int cb2_cfl_dt(cb2_ctx *ctx, double *dt_out, void *stream) {
+  if (!ctx || !dt_out) return CB2_ERR_INVALID;
+  ProfGuard pg(ctx);
+  cudaStream_t s = (cudaStream_t)stream;
+  CB2_TRY(enqueue_cfl_dt(ctx, s));
+  double dt = 0;
+  CB2_TRY(check_cuda(cudaMemcpyAsync(&dt, ctx->d_dtmin, sizeof(double), cudaMemcpyDeviceToHost, s)));
+  CB2_TRY(check_cuda(cudaStreamSynchronize(s)));
+  *dt_out = dt;
+  return CB2_OK;
+}
+
+int cb2_rk3_step(cb2_ctx *ctx, double *dt_inout, int fixed_dt, void *stream) {
+  if (!ctx || !dt_inout) return CB2_ERR_INVALID;
+  ProfGuard pg(ctx);
+  const int nb = (int)ctx->blocks.size();
+  for (int b = 0; b < nb; ++b)
+    if (ctx->blocks[b].bound) CB2_TRY(cb2_store_qn(ctx, b, stream));
+  double dt = *dt_inout;
+  if (!fixed_dt) {
+    CB2_TRY(cb2_cfl_dt(ctx, &dt, stream));
+    *dt_inout = dt;
+  }
+  for (int rk = 0; rk < 3; ++rk) {
+    for (int b = 0; b < nb; ++b) {
+      if (!ctx->blocks[b].bound) continue;
+      CB2_TRY(cb2_rhs(ctx, b, CB2_RHS_ALL, stream));
+      CB2_TRY(cb2_stage_update(ctx, b, dt, rk, stream));
+      CB2_TRY(cb2_boundary(ctx, b, stream));
+    }
+    for (int b = 0; b < nb; ++b)
+      if (ctx->blocks[b].bound) CB2_TRY(cb2_properties(ctx, b, stream));
+  }
+  return CB2_OK;
+}
+
+int cb2_read_status(cb2_ctx *ctx, unsigned *flags_out, void *stream) {
+  if (!ctx || !flags_out) return CB2_ERR_INVALID;
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned f = 0;
+  CB2_TRY(check_cuda(cudaMemcpyAsync(&f, ctx->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, s)));
+  CB2_TRY(check_cuda(cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned), s)));
+  CB2_TRY(check_cuda(cudaStreamSynchronize(s)));
+  *flags_out = f;
+  return CB2_OK;
+}
+
+}  // extern "C"

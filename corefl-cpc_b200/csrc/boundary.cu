@@ -1,0 +1,315 @@
+// Ghost-layer fill of bv/sv/cv from the face boundary conditions of a block.
+//
+// Faces are applied one launch per face in the reference's priority order
+// (farfield < outflow < inflow < symmetry < wall < periodic, src/BoundCond.cu:3846-3998), so
+// the edges and corners shared by two faces end with the same values the reference gets.
+//   outflow  : zeroth-order extrapolation (apply_outflow without back pressure,
+//              src/BoundCond.cu:2204-2350)
+//   periodic : average of the coincident end nodes, then ghost copy from the far side
+//              (apply_periodic, src/BoundCond.cu:3390-3440)
+//   symmetry : mirror with the normal velocity reflected (apply_symmetry, src/BoundCond.cu:2130)
+//   inflow   : fixed state in all ghost layers (apply_inflow constant-state branch,
+//              src/BoundCond.cu:2484)
+//   wall     : no-slip, adiabatic or isothermal (apply_wall, src/BoundCond.cu:3055-3389)
+// Every filled node gets its cv recomputed (compute_cv_from_bv_1_point, FieldOperation.cuh:163).
+#include "common.cuh"
+#include "thermo.cuh"
+#include "launch.h"
+
+namespace cb2 {
+
+template <int NS>
+__device__ __forceinline__ void cv_point(const Zone &z, const Param &p, idx_t g) {
+  const idx_t sz = z.L.sz;
+  const double rho = z.bv[g], u = z.bv[g + sz], v = z.bv[g + 2 * sz], w = z.bv[g + 3 * sz];
+  z.cv[g] = rho;
+  z.cv[g + sz] = rho * u;
+  z.cv[g + 2 * sz] = rho * v;
+  z.cv[g + 3 * sz] = rho * w;
+  double E = 0.5 * (u * u + v * v + w * w);
+  if constexpr (NS == 0) {
+    E *= rho;
+    E += z.bv[g + 4 * sz] / (kGammaAir - 1);
+  } else {
+    double h[NS];
+    nasa7_h<NS>(z.bv[g + 5 * sz], p.mech, h);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const double y = z.sv[g + s * sz];
+      z.cv[g + (5 + s) * sz] = rho * y;
+      E += h[s] * y;
+    }
+    E *= rho;
+    E -= z.bv[g + 4 * sz];
+  }
+  z.cv[g + 4 * sz] = E;
+}
+
+__device__ __forceinline__ bool face_point(const FaceBC &f, int &i, int &j, int &k) {
+  const int n0 = f.end[0] - f.start[0] + 1, n1 = f.end[1] - f.start[1] + 1, n2 = f.end[2] - f.start[2] + 1;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n0 * n1 * n2) return false;
+  i = f.start[0] + (int)(t % n0);
+  j = f.start[1] + (int)((t / n0) % n1);
+  k = f.start[2] + (int)(t / ((long long)n0 * n1));
+  return true;
+}
+
+template <int NS>
+__global__ void k_bc_outflow(Zone z, Param p, FaceBC f) {
+  int i, j, k;
+  if (!face_point(f, i, j, k)) return;
+  int d[3] = {0, 0, 0};
+  d[f.face] = f.direction;
+  const idx_t sz = z.L.sz;
+  const idx_t gb = z.L.at(i, j, k);
+  for (int gl = 1; gl <= z.ngg; ++gl) {
+    const idx_t gg = z.L.at(i + gl * d[0], j + gl * d[1], k + gl * d[2]);
+    for (int l = 0; l < 6; ++l) z.bv[gg + l * sz] = z.bv[gb + l * sz];
+    for (int l = 0; l < p.n_scalar; ++l) z.sv[gg + l * sz] = z.sv[gb + l * sz];
+    cv_point<NS>(z, p, gg);
+  }
+}
+
+template <int NS>
+__global__ void k_bc_periodic(Zone z, Param p, FaceBC f) {
+  int i, j, k;
+  if (!face_point(f, i, j, k)) return;
+  int d[3] = {0, 0, 0};
+  d[f.face] = f.direction;
+  int o[3] = {i, j, k};
+  const int ext[3] = {z.mx, z.my, z.mz};
+  o[f.face] = f.direction < 0 ? ext[f.face] - 1 : 0;
+  const idx_t sz = z.L.sz;
+  const idx_t gb = z.L.at(i, j, k), go = z.L.at(o[0], o[1], o[2]);
+  for (int l = 0; l < 6; ++l) {
+    const double ave = 0.5 * (z.bv[gb + l * sz] + z.bv[go + l * sz]);
+    z.bv[gb + l * sz] = ave;
+    z.bv[go + l * sz] = ave;
+  }
+  for (int l = 0; l < p.n_scalar; ++l) {
+    const double ave = 0.5 * (z.sv[gb + l * sz] + z.sv[go + l * sz]);
+    z.sv[gb + l * sz] = ave;
+    z.sv[go + l * sz] = ave;
+  }
+  cv_point<NS>(z, p, gb);
+  for (int gl = 1; gl <= z.ngg; ++gl) {
+    const idx_t gg = z.L.at(i + gl * d[0], j + gl * d[1], k + gl * d[2]);
+    const idx_t gs = z.L.at(o[0] + gl * d[0], o[1] + gl * d[1], o[2] + gl * d[2]);
+    for (int l = 0; l < 6; ++l) z.bv[gg + l * sz] = z.bv[gs + l * sz];
+    for (int l = 0; l < p.n_scalar; ++l) z.sv[gg + l * sz] = z.sv[gs + l * sz];
+    cv_point<NS>(z, p, gg);
+  }
+}
+
+template <int NS>
+__global__ void k_bc_symmetry(Zone z, Param p, FaceBC f) {
+  int i, j, k;
+  if (!face_point(f, i, j, k)) return;
+  int d[3] = {0, 0, 0};
+  d[f.face] = f.direction;
+  const idx_t sz = z.L.sz;
+  const idx_t gb = z.L.at(i, j, k);
+  const double *M = z.metric + (idx_t)(3 * f.face) * sz;
+  double nx = M[gb], ny = M[gb + sz], nz = M[gb + 2 * sz];
+  const double gni = 1.0 / norm3d(nx, ny, nz);
+  nx *= gni; ny *= gni; nz *= gni;
+  // the boundary node itself loses its normal velocity
+  {
+    const double u = z.bv[gb + sz], v = z.bv[gb + 2 * sz], w = z.bv[gb + 3 * sz];
+    const double vn = nx * u + ny * v + nz * w;
+    z.bv[gb + sz] = u - vn * nx;
+    z.bv[gb + 2 * sz] = v - vn * ny;
+    z.bv[gb + 3 * sz] = w - vn * nz;
+    cv_point<NS>(z, p, gb);
+  }
+  for (int gl = 1; gl <= z.ngg; ++gl) {
+    const idx_t gg = z.L.at(i + gl * d[0], j + gl * d[1], k + gl * d[2]);
+    const idx_t gi = z.L.at(i - gl * d[0], j - gl * d[1], k - gl * d[2]);
+    const double u = z.bv[gi + sz], v = z.bv[gi + 2 * sz], w = z.bv[gi + 3 * sz];
+    const double vn = nx * u + ny * v + nz * w;
+    z.bv[gg] = z.bv[gi];
+    z.bv[gg + sz] = u - 2 * vn * nx;
+    z.bv[gg + 2 * sz] = v - 2 * vn * ny;
+    z.bv[gg + 3 * sz] = w - 2 * vn * nz;
+    z.bv[gg + 4 * sz] = z.bv[gi + 4 * sz];
+    z.bv[gg + 5 * sz] = z.bv[gi + 5 * sz];
+    for (int l = 0; l < p.n_scalar; ++l) z.sv[gg + l * sz] = z.sv[gi + l * sz];
+    cv_point<NS>(z, p, gg);
+  }
+}
+
+template <int NS>
+__global__ void k_bc_inflow(Zone z, Param p, FaceBC f, const double *y_in) {
+  int i, j, k;
+  if (!face_point(f, i, j, k)) return;
+  int d[3] = {0, 0, 0};
+  d[f.face] = f.direction;
+  const idx_t sz = z.L.sz;
+  for (int gl = 0; gl <= z.ngg; ++gl) {
+    const idx_t gg = z.L.at(i + gl * d[0], j + gl * d[1], k + gl * d[2]);
+    z.bv[gg] = f.rho;
+    z.bv[gg + sz] = f.u;
+    z.bv[gg + 2 * sz] = f.v;
+    z.bv[gg + 3 * sz] = f.w;
+    z.bv[gg + 4 * sz] = f.p;
+    z.bv[gg + 5 * sz] = f.T;
+    for (int l = 0; l < p.n_scalar; ++l) z.sv[gg + l * sz] = y_in ? y_in[l] : 0.0;
+    cv_point<NS>(z, p, gg);
+  }
+}
+
+// No-slip wall: the wall node gets zero velocity and T_wall (isothermal) or the first-cell
+// temperature (adiabatic), p from the first interior node; ghosts mirror the interior with
+// reflected velocity and the wall-centred temperature.
+template <int NS>
+__global__ void k_bc_wall(Zone z, Param p, FaceBC f) {
+  int i, j, k;
+  if (!face_point(f, i, j, k)) return;
+  int d[3] = {0, 0, 0};
+  d[f.face] = f.direction;
+  const idx_t sz = z.L.sz;
+  const idx_t gb = z.L.at(i, j, k);
+  const idx_t g1 = z.L.at(i - d[0], j - d[1], k - d[2]);
+  const double t_wall = f.wall_T > 0 ? f.wall_T : z.bv[g1 + 5 * sz];
+  const double p_wall = z.bv[g1 + 4 * sz];
+  double r_mix = kRAir;
+  if constexpr (NS > 0) {
+    r_mix = 0;
+    for (int s = 0; s < NS; ++s) r_mix += z.sv[gb + s * sz] * __ldg(p.mech.gas_const + s);
+  }
+  z.bv[gb + sz] = 0;
+  z.bv[gb + 2 * sz] = 0;
+  z.bv[gb + 3 * sz] = 0;
+  z.bv[gb + 4 * sz] = p_wall;
+  z.bv[gb + 5 * sz] = t_wall;
+  z.bv[gb] = p_wall / (r_mix * t_wall);
+  cv_point<NS>(z, p, gb);
+  for (int gl = 1; gl <= z.ngg; ++gl) {
+    const idx_t gg = z.L.at(i + gl * d[0], j + gl * d[1], k + gl * d[2]);
+    const idx_t gi = z.L.at(i - gl * d[0], j - gl * d[1], k - gl * d[2]);
+    const double t_g = fmax(2 * t_wall - z.bv[gi + 5 * sz], 0.1 * t_wall);
+    z.bv[gg + sz] = -z.bv[gi + sz];
+    z.bv[gg + 2 * sz] = -z.bv[gi + 2 * sz];
+    z.bv[gg + 3 * sz] = -z.bv[gi + 3 * sz];
+    z.bv[gg + 4 * sz] = z.bv[gi + 4 * sz];
+    z.bv[gg + 5 * sz] = t_g;
+    for (int l = 0; l < p.n_scalar; ++l) z.sv[gg + l * sz] = z.sv[gi + l * sz];
+    double rg = kRAir;
+    if constexpr (NS > 0) {
+      rg = 0;
+      for (int s = 0; s < NS; ++s) rg += z.sv[gg + s * sz] * __ldg(p.mech.gas_const + s);
+    }
+    z.bv[gg] = z.bv[gg + 4 * sz] / (rg * t_g);
+    cv_point<NS>(z, p, gg);
+  }
+}
+
+// 2-D blocks: copy the k = 0 plane into every k ghost plane (eliminate_k_gradient,
+// src/FieldOperation.cu:96-121).
+__global__ void k_eliminate_k_gradient(Zone z, Param p) {
+  const int g_ = z.ngg;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x - g_;
+  const int j = blockIdx.y - g_;
+  if (i >= z.mx + g_) return;
+  const idx_t sz = z.L.sz;
+  const idx_t g0 = z.L.at(i, j, 0);
+  for (int kk = 1; kk <= g_; ++kk) {
+    const idx_t gp = z.L.at(i, j, kk), gm = z.L.at(i, j, -kk);
+    for (int l = 0; l < 6; ++l) { z.bv[gp + l * sz] = z.bv[g0 + l * sz]; z.bv[gm + l * sz] = z.bv[g0 + l * sz]; }
+    for (int l = 0; l < p.n_scalar; ++l) { z.sv[gp + l * sz] = z.sv[g0 + l * sz]; z.sv[gm + l * sz] = z.sv[g0 + l * sz]; }
+    for (int l = 0; l < p.n_var; ++l) { z.cv[gp + l * sz] = z.cv[g0 + l * sz]; z.cv[gm + l * sz] = z.cv[g0 + l * sz]; }
+  }
+}
+
+// Periodic exchange of the 8th-order viscous node fluxes (periodic_exchange task 1,
+// src/DataCommunication.cu:665-712).
+__global__ void k_periodic_flux(Zone z, Param p, FaceBC f) {
+  int i, j, k;
+  if (!face_point(f, i, j, k)) return;
+  int d[3] = {0, 0, 0};
+  d[f.face] = f.direction;
+  int o[3] = {i, j, k};
+  const int ext[3] = {z.mx, z.my, z.mz};
+  o[f.face] = f.direction < 0 ? ext[f.face] - 1 : 0;
+  const idx_t sz = z.L.sz;
+  const idx_t gb = z.L.at(i, j, k), go = z.L.at(o[0], o[1], o[2]);
+  double *arr[3] = {z.fF, z.gF, z.hF};
+  for (int l = 0; l < p.n_var; ++l)
+    for (int a = 0; a < 3; ++a) {
+      const double ave = 0.5 * (arr[a][gb + l * sz] + arr[a][go + l * sz]);
+      arr[a][gb + l * sz] = ave;
+      arr[a][go + l * sz] = ave;
+    }
+  for (int gl = 1; gl <= z.ngg; ++gl) {
+    const idx_t gg = z.L.at(i + gl * d[0], j + gl * d[1], k + gl * d[2]);
+    const idx_t gs = z.L.at(o[0] + gl * d[0], o[1] + gl * d[1], o[2] + gl * d[2]);
+    for (int l = 0; l < p.n_var; ++l)
+      for (int a = 0; a < 3; ++a) arr[a][gg + l * sz] = arr[a][gs + l * sz];
+  }
+}
+
+static inline long long face_points(const FaceBC &f) {
+  return (long long)(f.end[0] - f.start[0] + 1) * (f.end[1] - f.start[1] + 1) * (f.end[2] - f.start[2] + 1);
+}
+
+template <int NS>
+static int launch_bc_ns(const Zone &z, const Param &p, const FaceBC *faces, int n, cudaStream_t s, int &nl) {
+  // priority order of the reference
+  const int order[5] = {CB2_BC_OUTFLOW, CB2_BC_INFLOW, CB2_BC_SYMMETRY, CB2_BC_WALL, CB2_BC_PERIODIC};
+  for (int t : order) {
+    for (int f = 0; f < n; ++f) {
+      if (faces[f].type != t) continue;
+      const long long np = face_points(faces[f]);
+      const unsigned blocks = (unsigned)((np + 127) / 128);
+      if (blocks == 0) continue;
+      ProfScope prof("boundary_face", s);
+      switch (t) {
+        case CB2_BC_OUTFLOW: k_bc_outflow<NS><<<blocks, 128, 0, s>>>(z, p, faces[f]); break;
+        case CB2_BC_INFLOW: k_bc_inflow<NS><<<blocks, 128, 0, s>>>(z, p, faces[f], nullptr); break;
+        case CB2_BC_SYMMETRY: k_bc_symmetry<NS><<<blocks, 128, 0, s>>>(z, p, faces[f]); break;
+        case CB2_BC_WALL: k_bc_wall<NS><<<blocks, 128, 0, s>>>(z, p, faces[f]); break;
+        case CB2_BC_PERIODIC: k_bc_periodic<NS><<<blocks, 128, 0, s>>>(z, p, faces[f]); break;
+      }
+      ++nl;
+      CB2_TRY(check_launch());
+    }
+  }
+  return CB2_OK;
+}
+
+int launch_eliminate_k_gradient(const Zone &z, const Param &p, cudaStream_t s, int &nl) {
+  const int g = z.ngg;
+  dim3 grid((z.mx + 2 * g + 127) / 128, z.my + 2 * g, 1);
+  ProfScope prof("eliminate_k_gradient", s);
+  k_eliminate_k_gradient<<<grid, 128, 0, s>>>(z, p);
+  ++nl;
+  return check_launch();
+}
+
+int launch_boundary(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, cudaStream_t s,
+                    int &n_launch) {
+  switch (p.n_spec) {
+    case 0: return launch_bc_ns<0>(z, p, faces, n_faces, s, n_launch);
+    case 5: return launch_bc_ns<5>(z, p, faces, n_faces, s, n_launch);
+    case 9: return launch_bc_ns<9>(z, p, faces, n_faces, s, n_launch);
+    default: return CB2_ERR_UNSUPPORTED;
+  }
+}
+
+int launch_periodic_flux_exchange(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, cudaStream_t s,
+                                  int &n_launch) {
+  for (int f = 0; f < n_faces; ++f) {
+    if (faces[f].type != CB2_BC_PERIODIC) continue;
+    const long long np = face_points(faces[f]);
+    const unsigned blocks = (unsigned)((np + 127) / 128);
+    if (!blocks) continue;
+    ProfScope prof("periodic_flux_exchange", s);
+    k_periodic_flux<<<blocks, 128, 0, s>>>(z, p, faces[f]);
+    ++n_launch;
+    CB2_TRY(check_launch());
+  }
+  return CB2_OK;
+}
+
+}  // namespace cb2

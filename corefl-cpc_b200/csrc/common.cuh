@@ -1,0 +1,103 @@
+// Device-side data model shared by all kernels of the library.
+//
+// The field arrays are the caller's: padded SoA FP64 arrays in the layout of
+// ggxl::VectorField3D<real> (src/gxl_lib/Array.cuh:307-328).  A `Layout` holds the
+// displacements of one ghost width; `Zone` is passed to every kernel by value.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "cb200.h"
+
+namespace cb2 {
+
+// Physical constants (src/Constants.h:11-36).
+constexpr double kRu = 8314.462618;       // J/(kmol K)
+constexpr double kRc = 1.98720425864083;  // cal/(mol K)
+constexpr double kGammaAir = 1.4;
+constexpr double kMwAir = 28.9647;
+constexpr double kRAir = kRu / kMwAir;
+constexpr double kPatm = 101325.0;
+constexpr double kWenoEps = 1e-40;         // src/WENO.cu:8
+
+constexpr int kMaxSpec = 9;   // MAX_SPEC_NUMBER of the reference build (CMakeLists.txt:17)
+constexpr int kMaxReac = 20;
+constexpr int kMaxVar = 5 + kMaxSpec + 1;
+
+typedef long long idx_t;
+
+struct Layout {
+  int mx, my, mz, g;
+  idx_t disp2, disp1, dispt, sz;
+  __host__ __device__ __forceinline__ idx_t at(int i, int j, int k) const {
+    return (idx_t)k * disp1 + (idx_t)j * disp2 + i + dispt;
+  }
+};
+
+inline Layout make_layout(int mx, int my, int mz, int g) {
+  Layout L;
+  L.mx = mx; L.my = my; L.mz = mz; L.g = g;
+  L.disp2 = mx + 2 * g;
+  L.disp1 = (idx_t)(my + 2 * g) * L.disp2;
+  L.dispt = (L.disp1 + L.disp2 + 1) * g;
+  L.sz = (idx_t)(mx + 2 * g) * (my + 2 * g) * (mz + 2 * g);
+  return L;
+}
+
+// Per-face physical-boundary flags, one int per face node (bType_il..kr of DZone,
+// src/Field.h:20, filled as src/Mesh.cpp:855-900 does): 0 = inner or periodic.
+struct BTypes {
+  const int *il, *ir, *jl, *jr, *kl, *kr;  // (my,mz), (my,mz), (mx,mz), (mx,mz), (mx,my), (mx,my)
+};
+
+struct Zone {
+  int mx, my, mz, ngg;
+  Layout L;   // ghost ngg
+  Layout L0;  // ghost 0 (dq, dt_local)
+  Layout L1;  // ghost 1 (vis_flux, entropy_fix_delta)
+  double *cv, *bv, *sv, *qn, *dq, *metric, *jac, *mul, *kappa, *rhoD, *acoustic, *gamma, *mach;
+  double *fF, *gF, *hF, *visf, *shock, *dtl, *rts, *efd;
+  BTypes bt;
+};
+
+// Mechanism tables in device memory (copied from cb2_mechanism by cb2_init).
+struct Mech {
+  int n_spec, n_reac;
+  const double *imw, *gas_const, *mw;
+  const double *lo, *hi;         // [n_spec*7]
+  const double *t_low, *t_mid, *t_high;
+  const double *geometry, *lj_inv, *vis_coeff;
+  const double *wjwi14, *sqwiwj8, *bdc, *kbe;  // [n_spec*n_spec]
+  const double *zrot;
+  const int *reac_type, *rev_type, *stoi_f, *stoi_b, *reac_order;
+  const double *A, *b, *Ea, *A2, *b2, *Ea2, *tbc, *troe_alpha, *troe_t3, *troe_t1, *troe_t2;
+};
+
+// Scalar settings passed by value to kernels.
+struct Param {
+  int dim, n_var, n_spec, n_scalar, n_scalar_transported, n_reac;
+  int inviscid_scheme, reconstruction, limiter, viscous_order, positive_preserving;
+  int gradP, reaction, shock_sensor;
+  double sensor_eps, sensor_threshold, entropy_fix_factor, Pr, cfl;
+  double rho_ref, v_ref, weno_eps_scale, mu_constant;
+  int precision;
+  unsigned *status;  // device status word
+  Mech mech;
+};
+
+__device__ __forceinline__ void flag_status(const Param &p, unsigned bits) {
+  if (p.status) atomicOr(p.status, bits);
+}
+
+// SSP-RK3 Shu-Osher coefficients (src/RK.cuh:12-16).
+__device__ __forceinline__ void ssprk3_coeff(int rk, double &a, double &b, double &c) {
+  if (rk == 0) { a = 1.0; b = 0.0; c = 1.0; }
+  else if (rk == 1) { a = 0.75; b = 0.25; c = 0.25; }
+  else { a = 1.0 / 3.0; b = 2.0 / 3.0; c = 2.0 / 3.0; }
+}
+
+__host__ __device__ __forceinline__ double sutherland(double t) {
+  // src/Transport.cu:7-9
+  return 1.7894e-5 * pow(t / 288.16, 1.5) * (288.16 + 110) / (t + 110);
+}
+
+}  // namespace cb2

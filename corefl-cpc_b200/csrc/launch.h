@@ -1,0 +1,85 @@
+// Host-side launch helpers and the declarations of every kernel launcher in the library.
+#pragma once
+#include <cuda_runtime.h>
+#include "common.cuh"
+
+namespace cb2 {
+
+void set_cuda_error(cudaError_t e);
+
+#define CB2_TRY(expr)                 \
+  do {                                \
+    int _rc = (expr);                 \
+    if (_rc != CB2_OK) return _rc;    \
+  } while (0)
+
+inline int check_launch() {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_cuda_error(e);
+    return CB2_ERR_CUDA;
+  }
+  return CB2_OK;
+}
+
+inline int check_cuda(cudaError_t e) {
+  if (e != cudaSuccess) {
+    set_cuda_error(e);
+    return CB2_ERR_CUDA;
+  }
+  return CB2_OK;
+}
+
+// Per-launch timing (enabled per context by cb2_profile_enable): the API entry points make
+// the context's profiler current for the calling thread; every launcher brackets its
+// kernels with a ProfScope, which records a CUDA event pair on the launch stream.
+struct Profiler;
+extern thread_local Profiler *g_prof;
+void prof_begin(Profiler *p, const char *name, cudaStream_t s);
+void prof_end(Profiler *p, cudaStream_t s);
+
+struct ProfScope {
+  cudaStream_t s;
+  ProfScope(const char *name, cudaStream_t st) : s(st) {
+    if (g_prof) prof_begin(g_prof, name, s);
+  }
+  ~ProfScope() {
+    if (g_prof) prof_end(g_prof, s);
+  }
+};
+
+template <typename K>
+inline int prepare_smem(K kern, size_t bytes) {
+  if (bytes > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) { set_cuda_error(e); return CB2_ERR_CUDA; }
+  }
+  return CB2_OK;
+}
+
+// Face boundary condition in device-usable form (after the reference's register_boundary).
+struct FaceBC {
+  int type, face, direction;
+  int start[3], end[3];
+  double rho, u, v, w, p, T, wall_T;
+};
+
+// ---- launchers (each returns CB2_OK or an error code; n_launch counts kernels) ----------
+int launch_inviscid_char(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
+int launch_inviscid_pv(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
+int launch_stage_update(const Zone &z, const Param &p, double dt, int rk, cudaStream_t s, int &n_launch);
+int launch_cv_from_bv(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
+int launch_properties(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
+int launch_boundary(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, cudaStream_t s,
+                    int &n_launch);
+int launch_eliminate_k_gradient(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
+int launch_periodic_flux_exchange(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, cudaStream_t s,
+                                  int &n_launch);
+int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, cudaStream_t s, int &n_launch);
+int launch_local_dt(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
+int launch_min_reduce(const double *src, long long n, double *partial, int n_partial, double *out,
+                      cudaStream_t s, int &n_launch);
+int min_reduce_partials(long long n);
+int launch_set_value(double *dst, double v, cudaStream_t s, int &n_launch);
+
+}  // namespace cb2

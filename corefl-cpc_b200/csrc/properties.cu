@@ -1,0 +1,200 @@
+// Physical properties over interior and ghost nodes (update_physical_properties<mix>,
+// src/FieldOperation.cuh:183-247), the local CFL time step (local_time_step<mix>,
+// src/TimeAdvanceFunc.cuh:28-127) and its global minimum (min_of_arr + global_time_step,
+// src/TimeAdvanceFunc.cu:114-164).
+#include "common.cuh"
+#include "thermo.cuh"
+#include "transport.cuh"
+#include "launch.h"
+
+namespace cb2 {
+
+constexpr int kPropThreads = 128;
+
+template <int NS>
+__global__ void __launch_bounds__(kPropThreads) k_properties(Zone z, Param p) {
+  const int g_ = z.ngg;
+  const int i = blockIdx.x * kPropThreads + threadIdx.x - g_;
+  const int j = blockIdx.y - g_, k = blockIdx.z - g_;
+  if (i >= z.mx + g_) return;
+  const idx_t g = z.L.at(i, j, k), sz = z.L.sz;
+  const double t = z.bv[g + 5 * sz];
+  const double V = norm3d(z.bv[g + sz], z.bv[g + 2 * sz], z.bv[g + 3 * sz]);
+  if constexpr (NS == 0) {
+    z.mul[g] = p.mu_constant > 0 ? p.mu_constant : sutherland(t);
+    if (z.mach) z.mach[g] = V / sqrt(kGammaAir * kRu / kMwAir * t);
+  } else {
+    double cp[NS], y[NS];
+    nasa7_cp<NS>(t, p.mech, cp);
+    double imw = 0, cpt = 0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      y[s] = z.sv[g + s * sz];
+      imw = fma(y[s], __ldg(p.mech.imw + s), imw);
+      cpt = fma(y[s], cp[s], cpt);
+    }
+    const double mw = 1 / fmax(imw, 1e-12);
+    const double R = kRu * imw;
+    const double gam = cpt / (cpt - R);
+    z.gamma[g] = gam;
+    const double c = sqrt(gam * R * t);
+    z.acoustic[g] = c;
+    if (z.mach) z.mach[g] = V / c;
+    double mu, kappa, rhoD[NS];
+    transport_properties<NS>(t, z.bv[g + 4 * sz], mw, y, cp, p.mech, mu, kappa, rhoD);
+    z.mul[g] = mu;
+    z.kappa[g] = kappa;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) z.rhoD[g + s * sz] = rhoD[s];
+  }
+}
+
+int launch_properties(const Zone &z, const Param &p, cudaStream_t s, int &n_launch) {
+  const int g = z.ngg;
+  dim3 grid((z.mx + 2 * g + kPropThreads - 1) / kPropThreads, z.my + 2 * g, z.mz + 2 * g);
+  ++n_launch;
+  ProfScope prof("properties", s);
+  switch (p.n_spec) {
+    case 0:
+      if (p.mu_constant > 0 && !z.mach) { --n_launch; return CB2_OK; }  // nothing changes
+      k_properties<0><<<grid, kPropThreads, 0, s>>>(z, p);
+      break;
+    case 5: k_properties<5><<<grid, kPropThreads, 0, s>>>(z, p); break;
+    case 9: k_properties<9><<<grid, kPropThreads, 0, s>>>(z, p); break;
+    default: return CB2_ERR_UNSUPPORTED;
+  }
+  return check_launch();
+}
+
+// ---- local time step --------------------------------------------------------------------
+template <int NS>
+__global__ void __launch_bounds__(kPropThreads) k_local_dt(Zone z, Param p) {
+  const int i = blockIdx.x * kPropThreads + threadIdx.x;
+  const int j = blockIdx.y, k = blockIdx.z;
+  if (i >= z.mx) return;
+  const idx_t g = z.L.at(i, j, k), sz = z.L.sz;
+  const double *M = z.metric;
+  const double gxi = norm3d(M[g], M[g + sz], M[g + 2 * sz]);
+  const double geta = norm3d(M[g + 3 * sz], M[g + 4 * sz], M[g + 5 * sz]);
+  const double gzeta = norm3d(M[g + 6 * sz], M[g + 7 * sz], M[g + 8 * sz]);
+  const double u = z.bv[g + sz], v = z.bv[g + 2 * sz], w = z.bv[g + 3 * sz];
+  const double U = u * M[g] + v * M[g + sz] + w * M[g + 2 * sz];
+  const double Vc = u * M[g + 3 * sz] + v * M[g + 4 * sz] + w * M[g + 5 * sz];
+  const double W = u * M[g + 6 * sz] + v * M[g + 7 * sz] + w * M[g + 8 * sz];
+  double a;
+  if constexpr (NS == 0) a = sqrt(kGammaAir * kRAir * z.bv[g + 5 * sz]);
+  else a = z.acoustic[g];
+  const bool d3 = z.mz != 1;
+  double lam = fmax(fabs(U) + a * gxi, fabs(Vc) + a * geta);
+  if (d3) lam = fmax(lam, fabs(W) + a * gzeta);
+  if (p.viscous_order > 0) {
+    double len = fmax(gxi, geta);
+    if (d3) len = fmax(len, gzeta);
+    const double irho = 1.0 / z.bv[g];
+    double dv;
+    if constexpr (NS == 0) {
+      dv = fmax(kGammaAir, 4.0 / 3.0) * irho;
+      dv *= z.mul[g] / p.Pr;
+    } else {
+      double cp[NS];
+      nasa7_cp<NS>(z.bv[g + 5 * sz], p.mech, cp);
+      double cpt = 0, mrd = 0;
+      for (int s = 0; s < NS; ++s) {
+        cpt += cp[s] * z.sv[g + s * sz];
+        mrd = fmax(mrd, z.rhoD[g + s * sz]);
+      }
+      dv = z.mul[g] * irho;
+      dv = fmax(dv, z.kappa[g] * irho * z.gamma[g] / cpt);
+      dv = fmax(dv, mrd * irho);
+    }
+    lam = fmax(lam, len * len * dv);
+  }
+  double dt = p.cfl / lam;
+  if constexpr (NS > 0) {
+    if (p.n_reac > 0 && z.rts) {
+      const double rdt = p.cfl * z.rts[g];
+      if (rdt > 1e-20 && rdt < 1e-5) dt = fmin(dt, rdt);
+    }
+  }
+  z.dtl[z.L0.at(i, j, k)] = dt;
+}
+
+int launch_local_dt(const Zone &z, const Param &p, cudaStream_t s, int &n_launch) {
+  dim3 grid((z.mx + kPropThreads - 1) / kPropThreads, z.my, z.mz);
+  ++n_launch;
+  ProfScope prof("local_dt", s);
+  switch (p.n_spec) {
+    case 0: k_local_dt<0><<<grid, kPropThreads, 0, s>>>(z, p); break;
+    case 5: k_local_dt<5><<<grid, kPropThreads, 0, s>>>(z, p); break;
+    case 9: k_local_dt<9><<<grid, kPropThreads, 0, s>>>(z, p); break;
+    default: return CB2_ERR_UNSUPPORTED;
+  }
+  return check_launch();
+}
+
+// ---- min reduction: grid-stride partial minima, then one CTA over the partials ----------
+constexpr int kRedThreads = 256;
+
+__device__ __forceinline__ double warp_min(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ double block_min(double v) {
+  __shared__ double sw[kRedThreads / 32];
+  v = warp_min(v);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sw[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    v = lane < kRedThreads / 32 ? sw[lane] : 1e+6;
+    v = warp_min(v);
+  }
+  return v;
+}
+
+// The reference seeds every thread with 1e+6 (src/TimeAdvanceFunc.cu:152), so a block
+// whose every dt exceeds 1e6 reports 1e6; the same seed is kept here.
+__global__ void __launch_bounds__(kRedThreads) k_min_partial(const double *src, long long n, double *partial) {
+  double v = 1e+6;
+  for (long long t = (long long)blockIdx.x * kRedThreads + threadIdx.x; t < n; t += (long long)gridDim.x * kRedThreads)
+    v = fmin(v, src[t]);
+  v = block_min(v);
+  if (threadIdx.x == 0) partial[blockIdx.x] = v;
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_min_final(const double *partial, int n, double *out) {
+  double v = 1e+6;
+  for (int t = threadIdx.x; t < n; t += kRedThreads) v = fmin(v, partial[t]);
+  v = block_min(v);
+  if (threadIdx.x == 0) *out = fmin(*out, v);
+}
+
+__global__ void k_set_value(double *dst, double v) { *dst = v; }
+
+int launch_set_value(double *dst, double v, cudaStream_t s, int &n_launch) {
+  k_set_value<<<1, 1, 0, s>>>(dst, v);
+  ++n_launch;
+  return check_launch();
+}
+
+int min_reduce_partials(long long n) {
+  long long b = (n + kRedThreads - 1) / kRedThreads;
+  if (b > 148 * 8) b = 148 * 8;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+// out must hold the running minimum on entry (the caller seeds it, e.g. with 1e6).
+int launch_min_reduce(const double *src, long long n, double *partial, int n_partial, double *out, cudaStream_t s,
+                      int &n_launch) {
+  ProfScope prof("min_reduce", s);
+  k_min_partial<<<n_partial, kRedThreads, 0, s>>>(src, n, partial);
+  CB2_TRY(check_launch());
+  k_min_final<<<1, kRedThreads, 0, s>>>(partial, n_partial, out);
+  n_launch += 2;
+  return check_launch();
+}
+
+}  // namespace cb2

@@ -1,0 +1,121 @@
+// NASA7 two-range thermodynamics of a thermally perfect mixture (the Combustion2Part
+// branch of src/Thermo.cu:386-632) and the Roe-state "characteristic thermo" helper
+// (src/Thermo.cuh:49-110, one-temperature form).  Coefficients are read from the device
+// copy of the mechanism; outside [t_low, t_high] the enthalpy is extended linearly with
+// the edge cp and cp is held constant, as the reference does.
+#pragma once
+#include "common.cuh"
+
+namespace cb2 {
+
+// h_k [J/kg] and cp_k [J/(kg K)] of every species at temperature t
+// (compute_enthalpy_and_cp, src/Thermo.cu:453-523).
+template <int NS>
+__device__ __forceinline__ void nasa7_h_cp(double t, const Mech &m, double *h, double *cp) {
+  const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, t5 = t4 * t;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const double tl = __ldg(m.t_low + s), th = __ldg(m.t_high + s);
+    if (t < tl || t > th) {
+      const double tt = t < tl ? tl : th;
+      const double *c = (t < tl ? m.lo : m.hi) + s * 7;
+      const double tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt, tt5 = tt4 * tt;
+      double hs = __ldg(c + 0) * tt + 0.5 * __ldg(c + 1) * tt2 + __ldg(c + 2) * tt3 / 3 + 0.25 * __ldg(c + 3) * tt4 +
+                  0.2 * __ldg(c + 4) * tt5 + __ldg(c + 5);
+      const double cps = __ldg(c + 0) + __ldg(c + 1) * tt + __ldg(c + 2) * tt2 + __ldg(c + 3) * tt3 + __ldg(c + 4) * tt4;
+      hs += cps * (t - tt);
+      h[s] = hs * __ldg(m.gas_const + s);
+      cp[s] = cps * __ldg(m.gas_const + s);
+    } else {
+      const double *c = (t < __ldg(m.t_mid + s) ? m.lo : m.hi) + s * 7;
+      const double hs = __ldg(c + 0) * t + 0.5 * __ldg(c + 1) * t2 + __ldg(c + 2) * t3 / 3 + 0.25 * __ldg(c + 3) * t4 +
+                        0.2 * __ldg(c + 4) * t5 + __ldg(c + 5);
+      const double cps = __ldg(c + 0) + __ldg(c + 1) * t + __ldg(c + 2) * t2 + __ldg(c + 3) * t3 + __ldg(c + 4) * t4;
+      h[s] = hs * __ldg(m.gas_const + s);
+      cp[s] = cps * __ldg(m.gas_const + s);
+    }
+  }
+}
+
+// h_k only (compute_enthalpy, src/Thermo.cu:386-451).
+template <int NS>
+__device__ __forceinline__ void nasa7_h(double t, const Mech &m, double *h) {
+  const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, t5 = t4 * t;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const double tl = __ldg(m.t_low + s), th = __ldg(m.t_high + s);
+    double hs;
+    if (t < tl || t > th) {
+      const double tt = t < tl ? tl : th;
+      const double *c = (t < tl ? m.lo : m.hi) + s * 7;
+      const double tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt, tt5 = tt4 * tt;
+      hs = __ldg(c + 0) * tt + 0.5 * __ldg(c + 1) * tt2 + __ldg(c + 2) * tt3 / 3 + 0.25 * __ldg(c + 3) * tt4 +
+           0.2 * __ldg(c + 4) * tt5 + __ldg(c + 5);
+      const double cps = __ldg(c + 0) + __ldg(c + 1) * tt + __ldg(c + 2) * tt2 + __ldg(c + 3) * tt3 + __ldg(c + 4) * tt4;
+      hs += cps * (t - tt);
+    } else {
+      const double *c = (t < __ldg(m.t_mid + s) ? m.lo : m.hi) + s * 7;
+      hs = __ldg(c + 0) * t + 0.5 * __ldg(c + 1) * t2 + __ldg(c + 2) * t3 / 3 + 0.25 * __ldg(c + 3) * t4 +
+           0.2 * __ldg(c + 4) * t5 + __ldg(c + 5);
+    }
+    h[s] = hs * __ldg(m.gas_const + s);
+  }
+}
+
+// cp_k only (compute_cp, src/Thermo.cu:525-574).
+template <int NS>
+__device__ __forceinline__ void nasa7_cp(double t, const Mech &m, double *cp) {
+  const double t2 = t * t, t3 = t2 * t, t4 = t3 * t;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const double tl = __ldg(m.t_low + s), th = __ldg(m.t_high + s);
+    double tt = t;
+    const double *c;
+    if (t < tl) { tt = tl; c = m.lo + s * 7; }
+    else if (t > th) { tt = th; c = m.hi + s * 7; }
+    else c = (t < __ldg(m.t_mid + s) ? m.lo : m.hi) + s * 7;
+    double cps;
+    if (tt == t) cps = __ldg(c + 0) + __ldg(c + 1) * t + __ldg(c + 2) * t2 + __ldg(c + 3) * t3 + __ldg(c + 4) * t4;
+    else {
+      const double tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt;
+      cps = __ldg(c + 0) + __ldg(c + 1) * tt + __ldg(c + 2) * tt2 + __ldg(c + 3) * tt3 + __ldg(c + 4) * tt4;
+    }
+    cp[s] = cps * __ldg(m.gas_const + s);
+  }
+}
+
+// Mixture gamma and sound speed at the Roe state, plus the scalar rows of the left
+// eigenvectors (alpha_s) and the energy coefficients of the right eigenvectors
+// (src/Thermo.cuh:49-110 with two_temperature off: e_ve = 0).
+template <int NS>
+__device__ __forceinline__ void characteristic_thermo(double t, const double *y, const Mech &m, double &gamma,
+                                                      double &c, double *alpha, double *ecoef, double *e_tr_out) {
+  const double te = fmax(t, 1.0);
+  double h[NS], cp[NS];
+  nasa7_h_cp<NS>(te, m, h, cp);
+  double e_tr = 0, r = 0, cpm = 0, cvm = 0;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const double rs = __ldg(m.gas_const + s);
+    e_tr += y[s] * (h[s] - rs * te);
+    r += y[s] * rs;
+    cpm += y[s] * cp[s];
+    cvm += y[s] * (cp[s] - rs);
+  }
+  gamma = cpm / fmax(cvm, 1e-8);
+  c = sqrt(fmax(gamma * r * te, 1e-12));
+  if (e_tr_out) *e_tr_out = e_tr;
+  if (alpha) {
+    const double gm1 = gamma - 1.0;
+    const double c2 = fmax(c * c, 1e-30);
+    const double inv_gm1 = 1.0 / fmax(gm1, 1e-12);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const double a = (gamma * __ldg(m.gas_const + s) * te - gm1 * h[s]) / c2;
+      alpha[s] = a;
+      ecoef[s] = -a * c2 * inv_gm1;
+    }
+  }
+}
+
+}  // namespace cb2

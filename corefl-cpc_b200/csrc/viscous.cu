@@ -1,0 +1,328 @@
+// Viscous fluxes.
+//
+// Order 8 (compute_viscous_flux_collocated<mix,8>, src/ViscousScheme.cu:470-585;
+// compute_viscous_flux_derivative<8>, :790-834; stencils d_dXi/d_dEta/d_dZeta, :140-468):
+//   node gradients of u,v,w,T with 8th-order central differences (one-sided closures on the
+//   four nodes next to a physical boundary), collocated node fluxes into fFlux/gFlux/hFlux,
+//   periodic exchange of the node fluxes, then dq += J (dF/dxi + dG/deta + dH/dzeta).
+// Order 2 (compute_{fv,gv,hv}_2nd_order, src/ViscousScheme.cu:836-1512; compute_dFv_dx etc.,
+//   :86-138): face fluxes from face-averaged metrics/coefficients and compact differences,
+//   mixture species diffusion with the correction velocity and the h_k J_k energy term;
+//   the face difference is taken in the same kernel as the face flux through shared memory.
+#include "common.cuh"
+#include "thermo.cuh"
+#include "launch.h"
+
+namespace cb2 {
+
+// ---- 8th-order derivative along one index direction ---------------------------------
+// f(m) returns the field at offset m along the direction; n = node index, nx = extent.
+template <typename F>
+__device__ __forceinline__ double d8(F f, int n, int nx, bool bl, bool br) {
+  if (bl) {
+    if (n == 0) return -25.0 / 12 * f(0) + 4.0 * f(1) - 3 * f(2) + 4.0 / 3 * f(3) - 0.25 * f(4);
+    if (n == 1) return -0.25 * f(-1) - 5.0 / 6 * f(0) + 1.5 * f(1) - 0.5 * f(2) + 1.0 / 12 * f(3);
+    if (n == 2) return -1.0 / 12 * (f(2) - f(-2)) + 2.0 / 3 * (f(1) - f(-1));
+    if (n == 3) return 0.75 * (f(1) - f(-1)) - 0.15 * (f(2) - f(-2)) + 1.0 / 60 * (f(3) - f(-3));
+  }
+  if (br) {
+    if (n == nx - 1) return 25.0 / 12 * f(0) - 4.0 * f(-1) + 3 * f(-2) - 4.0 / 3 * f(-3) + 0.25 * f(-4);
+    if (n == nx - 2) return 0.25 * f(1) + 5.0 / 6 * f(0) - 1.5 * f(-1) + 0.5 * f(-2) - 1.0 / 12 * f(-3);
+    if (n == nx - 3) return -1.0 / 12 * (f(2) - f(-2)) + 2.0 / 3 * (f(1) - f(-1));
+    if (n == nx - 4) return 0.75 * (f(1) - f(-1)) - 0.15 * (f(2) - f(-2)) + 1.0 / 60 * (f(3) - f(-3));
+  }
+  return 0.8 * (f(1) - f(-1)) + -0.2 * (f(2) - f(-2)) + 4.0 / 105 * (f(3) - f(-3)) + -1.0 / 280 * (f(4) - f(-4));
+}
+
+struct BFlags {
+  bool il, ir, jl, jr, kl, kr;
+};
+
+__device__ __forceinline__ BFlags bflags(const Zone &z, int i, int j, int k) {
+  BFlags b;
+  b.il = z.bt.il[j + k * z.my] != 0;
+  b.ir = z.bt.ir[j + k * z.my] != 0;
+  b.jl = z.bt.jl[i + k * z.mx] != 0;
+  b.jr = z.bt.jr[i + k * z.mx] != 0;
+  b.kl = z.bt.kl[i + j * z.mx] != 0;
+  b.kr = z.bt.kr[i + j * z.mx] != 0;
+  return b;
+}
+
+constexpr int kVisThreads = 128;
+
+// Node fluxes of the momentum and energy equations (air); comps 1..4 of fFlux/gFlux/hFlux.
+__global__ void __launch_bounds__(kVisThreads) k_visc8_node_flux_air(Zone z, Param p) {
+  const int i = blockIdx.x * kVisThreads + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  if (i >= z.mx) return;
+  const Layout &L = z.L;
+  const idx_t sz = L.sz, g = L.at(i, j, k);
+  const BFlags b = bflags(z, i, j, k);
+  const idx_t si = 1, sj = L.disp2, sk = L.disp1;
+  auto der = [&](int comp, double &dxi, double &deta, double &dzeta) {
+    const double *f = z.bv + comp * sz + g;
+    dxi = d8([&](int m) { return f[m * si]; }, i, z.mx, b.il, b.ir);
+    deta = d8([&](int m) { return f[m * sj]; }, j, z.my, b.jl, b.jr);
+    dzeta = d8([&](int m) { return f[m * sk]; }, k, z.mz, b.kl, b.kr);
+  };
+  double u_xi, u_eta, u_zeta, v_xi, v_eta, v_zeta, w_xi, w_eta, w_zeta, t_xi, t_eta, t_zeta;
+  der(1, u_xi, u_eta, u_zeta);
+  der(2, v_xi, v_eta, v_zeta);
+  der(3, w_xi, w_eta, w_zeta);
+  der(5, t_xi, t_eta, t_zeta);
+  const double *M = z.metric + g;
+  const double xi_x = M[0], xi_y = M[sz], xi_z = M[2 * sz];
+  const double eta_x = M[3 * sz], eta_y = M[4 * sz], eta_z = M[5 * sz];
+  const double zeta_x = M[6 * sz], zeta_y = M[7 * sz], zeta_z = M[8 * sz];
+  const double u_x = u_xi * xi_x + u_eta * eta_x + u_zeta * zeta_x;
+  const double u_y = u_xi * xi_y + u_eta * eta_y + u_zeta * zeta_y;
+  const double u_z = u_xi * xi_z + u_eta * eta_z + u_zeta * zeta_z;
+  const double v_x = v_xi * xi_x + v_eta * eta_x + v_zeta * zeta_x;
+  const double v_y = v_xi * xi_y + v_eta * eta_y + v_zeta * zeta_y;
+  const double v_z = v_xi * xi_z + v_eta * eta_z + v_zeta * zeta_z;
+  const double w_x = w_xi * xi_x + w_eta * eta_x + w_zeta * zeta_x;
+  const double w_y = w_xi * xi_y + w_eta * eta_y + w_zeta * zeta_y;
+  const double w_z = w_xi * xi_z + w_eta * eta_z + w_zeta * zeta_z;
+  const double mu = z.mul[g];
+  const double txx = mu * (4 * u_x - 2 * v_y - 2 * w_z) / 3.0;
+  const double tyy = mu * (4 * v_y - 2 * u_x - 2 * w_z) / 3.0;
+  const double tzz = mu * (4 * w_z - 2 * u_x - 2 * v_y) / 3.0;
+  const double txy = mu * (u_y + v_x), txz = mu * (u_z + w_x), tyz = mu * (v_z + w_y);
+  const double t_x = t_xi * xi_x + t_eta * eta_x + t_zeta * zeta_x;
+  const double t_y = t_xi * xi_y + t_eta * eta_y + t_zeta * zeta_y;
+  const double t_z = t_xi * xi_z + t_eta * eta_z + t_zeta * zeta_z;
+  const double cp = kGammaAir * kRAir / (kGammaAir - 1);
+  const double kap = mu / p.Pr * cp;
+  const double u = z.bv[g + sz], v = z.bv[g + 2 * sz], w = z.bv[g + 3 * sz];
+  const double Ex = u * txx + v * txy + w * txz + kap * t_x;
+  const double Ey = u * txy + v * tyy + w * tyz + kap * t_y;
+  const double Ez = u * txz + v * tyz + w * tzz + kap * t_z;
+  z.fF[g + sz] = xi_x * txx + xi_y * txy + xi_z * txz;
+  z.fF[g + 2 * sz] = xi_x * txy + xi_y * tyy + xi_z * tyz;
+  z.fF[g + 3 * sz] = xi_x * txz + xi_y * tyz + xi_z * tzz;
+  z.gF[g + sz] = eta_x * txx + eta_y * txy + eta_z * txz;
+  z.gF[g + 2 * sz] = eta_x * txy + eta_y * tyy + eta_z * tyz;
+  z.gF[g + 3 * sz] = eta_x * txz + eta_y * tyz + eta_z * tzz;
+  z.hF[g + sz] = zeta_x * txx + zeta_y * txy + zeta_z * txz;
+  z.hF[g + 2 * sz] = zeta_x * txy + zeta_y * tyy + zeta_z * tyz;
+  z.hF[g + 3 * sz] = zeta_x * txz + zeta_y * tyz + zeta_z * tzz;
+  z.fF[g + 4 * sz] = xi_x * Ex + xi_y * Ey + xi_z * Ez;
+  z.gF[g + 4 * sz] = eta_x * Ex + eta_y * Ey + eta_z * Ez;
+  z.hF[g + 4 * sz] = zeta_x * Ex + zeta_y * Ey + zeta_z * Ez;
+}
+
+__global__ void __launch_bounds__(kVisThreads) k_visc8_divergence(Zone z, Param p) {
+  const int i = blockIdx.x * kVisThreads + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  if (i >= z.mx) return;
+  const Layout &L = z.L;
+  const idx_t sz = L.sz, g = L.at(i, j, k);
+  const BFlags b = bflags(z, i, j, k);
+  const idx_t sj = L.disp2, sk = L.disp1;
+  const double jac = z.jac[g];
+  const idx_t g0 = z.L0.at(i, j, k), sz0 = z.L0.sz;
+  for (int l = 1; l < p.n_var; ++l) {
+    const double *f = z.fF + l * sz + g, *gg = z.gF + l * sz + g, *h = z.hF + l * sz + g;
+    const double d = d8([&](int m) { return f[m]; }, i, z.mx, b.il, b.ir) +
+                     d8([&](int m) { return gg[m * sj]; }, j, z.my, b.jl, b.jr) +
+                     d8([&](int m) { return h[m * sk]; }, k, z.mz, b.kl, b.kr);
+    z.dq[g0 + l * sz0] += d * jac;
+  }
+}
+
+// ---- 2nd-order face fluxes ----------------------------------------------------------------
+// Face between node (i,j,k) and its +1 neighbour along DIR.  The compact difference is taken
+// along DIR and the two transverse derivatives are averaged over the two nodes (4-point).
+template <int NS, int DIR>
+__device__ __forceinline__ void visc2_face(const Zone &z, const Param &p, int i, int j, int k, double *fv) {
+  const Layout &L = z.L;
+  const idx_t sz = L.sz;
+  const idx_t st[3] = {1, L.disp2, L.disp1};
+  const idx_t g = L.at(i, j, k), gn = g + st[DIR];
+  const double *M = z.metric;
+  double mtr[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) mtr[c] = 0.5 * (M[g + c * sz] + M[gn + c * sz]);
+  // derivatives of a field along xi, eta, zeta at the face
+  auto grad = [&](const double *f, double &dxi, double &deta, double &dzeta) {
+    double d[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (a == DIR) d[a] = f[gn] - f[g];
+      else d[a] = 0.25 * (f[g + st[a]] - f[g - st[a]] + f[gn + st[a]] - f[gn - st[a]]);
+    }
+    dxi = d[0]; deta = d[1]; dzeta = d[2];
+  };
+  double u_xi, u_eta, u_zeta, v_xi, v_eta, v_zeta, w_xi, w_eta, w_zeta, t_xi, t_eta, t_zeta;
+  grad(z.bv + sz, u_xi, u_eta, u_zeta);
+  grad(z.bv + 2 * sz, v_xi, v_eta, v_zeta);
+  grad(z.bv + 3 * sz, w_xi, w_eta, w_zeta);
+  grad(z.bv + 5 * sz, t_xi, t_eta, t_zeta);
+  const double xi_x = mtr[0], xi_y = mtr[1], xi_z = mtr[2], eta_x = mtr[3], eta_y = mtr[4], eta_z = mtr[5];
+  const double zeta_x = mtr[6], zeta_y = mtr[7], zeta_z = mtr[8];
+  const double u_x = u_xi * xi_x + u_eta * eta_x + u_zeta * zeta_x;
+  const double u_y = u_xi * xi_y + u_eta * eta_y + u_zeta * zeta_y;
+  const double u_z = u_xi * xi_z + u_eta * eta_z + u_zeta * zeta_z;
+  const double v_x = v_xi * xi_x + v_eta * eta_x + v_zeta * zeta_x;
+  const double v_y = v_xi * xi_y + v_eta * eta_y + v_zeta * zeta_y;
+  const double v_z = v_xi * xi_z + v_eta * eta_z + v_zeta * zeta_z;
+  const double w_x = w_xi * xi_x + w_eta * eta_x + w_zeta * zeta_x;
+  const double w_y = w_xi * xi_y + w_eta * eta_y + w_zeta * zeta_y;
+  const double w_z = w_xi * xi_z + w_eta * eta_z + w_zeta * zeta_z;
+  const double mu = 0.5 * (z.mul[g] + z.mul[gn]);
+  const double txx = mu * (4 * u_x - 2 * v_y - 2 * w_z) / 3.0;
+  const double tyy = mu * (4 * v_y - 2 * u_x - 2 * w_z) / 3.0;
+  const double tzz = mu * (4 * w_z - 2 * u_x - 2 * v_y) / 3.0;
+  const double txy = mu * (u_y + v_x), txz = mu * (u_z + w_x), tyz = mu * (v_z + w_y);
+  const double *Md = M + (idx_t)(3 * DIR) * sz;
+  const double jl = z.jac[g], jr = z.jac[gn];
+  const double kxj = 0.5 * (Md[g] * jl + Md[gn] * jr);
+  const double kyj = 0.5 * (Md[g + sz] * jl + Md[gn + sz] * jr);
+  const double kzj = 0.5 * (Md[g + 2 * sz] * jl + Md[gn + 2 * sz] * jr);
+  fv[0] = kxj * txx + kyj * txy + kzj * txz;
+  fv[1] = kxj * txy + kyj * tyy + kzj * tyz;
+  fv[2] = kxj * txz + kyj * tyz + kzj * tzz;
+  const double um = 0.5 * (z.bv[g + sz] + z.bv[gn + sz]);
+  const double vm = 0.5 * (z.bv[g + 2 * sz] + z.bv[gn + 2 * sz]);
+  const double wm = 0.5 * (z.bv[g + 3 * sz] + z.bv[gn + 3 * sz]);
+  const double t_x = t_xi * xi_x + t_eta * eta_x + t_zeta * zeta_x;
+  const double t_y = t_xi * xi_y + t_eta * eta_y + t_zeta * zeta_y;
+  const double t_z = t_xi * xi_z + t_eta * eta_z + t_zeta * zeta_z;
+  double kap;
+  if constexpr (NS == 0) {
+    const double cp = kGammaAir * kRAir / (kGammaAir - 1);
+    kap = mu / p.Pr * cp;
+  } else {
+    kap = 0.5 * (z.kappa[g] + z.kappa[gn]);
+  }
+  fv[3] = um * fv[0] + vm * fv[1] + wm * fv[2] + kap * (kxj * t_x + kyj * t_y + kzj * t_z);
+  if constexpr (NS > 0) {
+    const Mech &m = p.mech;
+    double dif[NS], yk[NS], force[NS];
+    double sum_gy_w = 0, sum_rdy = 0, corr = 0, mwt = 0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const double *ys = z.sv + s * sz;
+      yk[s] = 0.5 * (ys[g] + ys[gn]);
+      dif[s] = 0.5 * (z.rhoD[g + s * sz] + z.rhoD[gn + s * sz]);
+      double y_xi, y_eta, y_zeta;
+      grad(ys, y_xi, y_eta, y_zeta);
+      const double y_x = y_xi * xi_x + y_eta * eta_x + y_zeta * zeta_x;
+      const double y_y = y_xi * xi_y + y_eta * eta_y + y_zeta * zeta_y;
+      const double y_z = y_xi * xi_z + y_eta * eta_z + y_zeta * zeta_z;
+      const double gdy = kxj * y_x + kyj * y_y + kzj * y_z;
+      force[s] = gdy;
+      corr += dif[s] * gdy;
+      sum_gy_w += gdy * __ldg(m.imw + s);
+      mwt += yk[s] * __ldg(m.imw + s);
+      sum_rdy += dif[s] * yk[s];
+    }
+    mwt = 1.0 / mwt;
+    corr -= mwt * sum_rdy * sum_gy_w;
+    if (p.gradP) {
+      double p_xi, p_eta, p_zeta;
+      grad(z.bv + 4 * sz, p_xi, p_eta, p_zeta);
+      const double p_x = p_xi * xi_x + p_eta * eta_x + p_zeta * zeta_x;
+      const double p_y = p_xi * xi_y + p_eta * eta_y + p_zeta * zeta_y;
+      const double p_z = p_xi * xi_z + p_eta * eta_z + p_zeta * zeta_z;
+      const double gp = (kxj * p_x + kyj * p_y + kzj * p_z) / (0.5 * (z.bv[gn + 4 * sz] + z.bv[g + 4 * sz]));
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        force[s] += (mwt * __ldg(m.imw + s) - 1) * yk[s] * gp;
+        corr += (mwt * __ldg(m.imw + s) - 1) * yk[s] * gp * dif[s];
+      }
+    }
+    double h[NS];
+    nasa7_h<NS>(0.5 * (z.bv[g + 5 * sz] + z.bv[gn + 5 * sz]), m, h);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const double jd = dif[s] * (force[s] - mwt * yk[s] * sum_gy_w) - yk[s] * corr;
+      fv[4 + s] = jd;
+      fv[3] += h[s] * jd;
+    }
+  }
+}
+
+constexpr int kV2TI = 16, kV2TS = 16;  // tile of 16 transverse x 16 faces along the direction
+
+// Face fluxes of a tile and their difference: a CTA owns kV2TS faces along DIR (the first
+// one is the left face of the first node) for kV2TI positions of the transverse index.
+template <int NS, int DIR>
+__global__ void __launch_bounds__(kV2TI *kV2TS) k_visc2(Zone z, Param p) {
+  constexpr int NF = 4 + NS;
+  __shared__ double sfv[NF][kV2TI * kV2TS];
+  const int tid = threadIdx.x;
+  const int tt = tid % kV2TI, ts = tid / kV2TI;
+  int i, j, k, n;
+  const int s0 = blockIdx.y * (kV2TS - 1);
+  n = s0 - 1 + ts;  // face n + 1/2 along DIR
+  if (DIR == 0) { i = n; j = blockIdx.x * kV2TI + tt; k = blockIdx.z; }
+  else if (DIR == 1) { i = blockIdx.x * kV2TI + tt; j = n; k = blockIdx.z; }
+  else { i = blockIdx.x * kV2TI + tt; j = blockIdx.z; k = n; }
+  const int ext[3] = {z.mx, z.my, z.mz};
+  const int tr = DIR == 0 ? j : i;
+  const int trmax = DIR == 0 ? z.my : z.mx;
+  const bool valid = tr < trmax && n <= ext[DIR] - 1;
+  if (valid) {
+    double fv[NF];
+    visc2_face<NS, DIR>(z, p, i, j, k, fv);
+#pragma unroll
+    for (int c = 0; c < NF; ++c) sfv[c][tid] = fv[c];
+  }
+  __syncthreads();
+  if (valid && ts >= 1 && n >= 0) {
+    const idx_t g0 = z.L0.at(i, j, k), sz0 = z.L0.sz;
+#pragma unroll
+    for (int c = 0; c < NF; ++c) z.dq[g0 + (c + 1) * sz0] += sfv[c][tid] - sfv[c][tid - kV2TI];
+  }
+}
+
+template <int NS>
+static int launch_visc2_ns(const Zone &z, const Param &p, cudaStream_t s, int &nl) {
+  const int ndir = z.mz > 1 ? 3 : 2;
+  for (int d = 0; d < ndir; ++d) {
+    const int ext[3] = {z.mx, z.my, z.mz};
+    const int tr = d == 0 ? z.my : z.mx;
+    const int other = d == 2 ? z.my : z.mz;
+    dim3 grid((tr + kV2TI - 1) / kV2TI, (ext[d] + kV2TS - 2) / (kV2TS - 1), other);
+    static const char *names[3] = {"visc2_x", "visc2_y", "visc2_z"};
+    ProfScope prof(names[d], s);
+    if (d == 0) k_visc2<NS, 0><<<grid, kV2TI * kV2TS, 0, s>>>(z, p);
+    else if (d == 1) k_visc2<NS, 1><<<grid, kV2TI * kV2TS, 0, s>>>(z, p);
+    else k_visc2<NS, 2><<<grid, kV2TI * kV2TS, 0, s>>>(z, p);
+    ++nl;
+    CB2_TRY(check_launch());
+  }
+  return CB2_OK;
+}
+
+int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, cudaStream_t s, int &nl) {
+  if (p.viscous_order == 0) return CB2_OK;
+  if (p.viscous_order == 8) {
+    if (p.n_spec != 0) return CB2_ERR_UNSUPPORTED;
+    dim3 grid((z.mx + kVisThreads - 1) / kVisThreads, z.my, z.mz);
+    {
+      ProfScope prof("visc8_node_flux", s);
+      k_visc8_node_flux_air<<<grid, kVisThreads, 0, s>>>(z, p);
+    }
+    ++nl;
+    CB2_TRY(check_launch());
+    CB2_TRY(launch_periodic_flux_exchange(z, p, faces, n_faces, s, nl));
+    {
+      ProfScope prof("visc8_divergence", s);
+      k_visc8_divergence<<<grid, kVisThreads, 0, s>>>(z, p);
+    }
+    ++nl;
+    return check_launch();
+  }
+  if (p.viscous_order == 2) {
+    switch (p.n_spec) {
+      case 0: return launch_visc2_ns<0>(z, p, s, nl);
+      case 5: return launch_visc2_ns<5>(z, p, s, nl);
+      case 9: return launch_visc2_ns<9>(z, p, s, nl);
+      default: return CB2_ERR_UNSUPPORTED;
+    }
+  }
+  return CB2_ERR_UNSUPPORTED;
+}
+
+}  // namespace cb2

@@ -1,0 +1,246 @@
+/*
+ * cb200.h -- C ABI of the B200-native explicit residual-and-update path of COREFL.
+ *
+ * The reference calls this path from `RK3<mix>()` (src/RK.cuh:107-272) as a sequence of
+ * C++ launches on `DZone*` / `DParameter*`.  Every entry point below replaces one of those
+ * calls (cited per function).  The library never allocates or frees the caller's field
+ * arrays: it borrows the device pointers of the caller's padded per-block arrays, exactly
+ * as `Field::setup_device_memory` (src/Field.cu:440-672) lays them out.
+ *
+ * Array layout (ggxl::VectorField3D<real>, ColMajor, src/gxl_lib/Array.cuh:307-328):
+ *   a padded array with `g` ghost layers on (mx,my,mz) nodes holds element (i,j,k,l) at
+ *     val[k*disp1 + j*disp2 + i + dispt + l*sz]
+ *   with disp2 = mx+2g, disp1 = (my+2g)*disp2, dispt = (disp1+disp2+1)*g,
+ *        sz = (mx+2g)*(my+2g)*(mz+2g);  -g <= i < mx+g etc.
+ *   The ghost width of each array is the one the reference allocates: `ngg` for the flow
+ *   fields, 0 for dq and dt_local, 1 for vis_flux.
+ *
+ * All pointers in cb2_zone_view are DEVICE pointers of the current CUDA device.  All
+ * pointers in cb2_param_view / cb2_mechanism are HOST pointers; cb2_init copies them.
+ * Streams are passed as `void*` (a cudaStream_t; NULL = legacy default stream).
+ *
+ * Every function returns 0 on success or a negative CB2_ERR_* code; none aborts.
+ */
+#ifndef CB200_H
+#define CB200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CB2_ABI_VERSION 1
+
+/* ---- status codes ---------------------------------------------------------------- */
+#define CB2_OK 0
+#define CB2_ERR_CUDA (-1)        /* a CUDA runtime call failed (see cb2_last_cuda_error) */
+#define CB2_ERR_INVALID (-2)     /* bad argument, view or parameter combination          */
+#define CB2_ERR_NONPHYSICAL (-3) /* a kernel met rho<=0, T<=0 or a non-finite state      */
+#define CB2_ERR_TIMEOUT (-4)     /* a bounded device-side wait gave up                    */
+#define CB2_ERR_UNSUPPORTED (-5) /* scheme/model combination not built                    */
+#define CB2_ERR_NOMEM (-6)       /* private scratch could not be allocated                */
+
+/* ---- scheme codes (the reference's setup.txt keys, src/Parameter.cpp:234-312) -------- */
+#define CB2_INV_ROE 2     /* inviscid_scheme = 2  : Roe + Harten fix, MUSCL/NND/1st       */
+#define CB2_INV_AUSMP 3   /* inviscid_scheme = 3  : AUSM+ with primitive reconstruction   */
+#define CB2_INV_HLLC 4    /* inviscid_scheme = 4  : HLLC with primitive reconstruction    */
+#define CB2_INV_WENO5_CP 51
+#define CB2_INV_WENO5_CH 52
+#define CB2_INV_WENO7_CP 71
+#define CB2_INV_WENO7_CH 72
+
+#define CB2_REC_FIRST 1 /* reconstruction = 1 */
+#define CB2_REC_MUSCL 2 /* reconstruction = 2 (kappa = 1/3, minmod) */
+#define CB2_REC_NND2 3  /* reconstruction = 3 */
+#define CB2_REC_WENO5 5 /* added: WENO5-JS weights on primitive variables (no reference kernel) */
+#define CB2_REC_WENO7 7 /* added: WENO7-Z weights on primitive variables (no reference kernel)  */
+
+/* boundary types: the reference's BC kinds (src/BoundCond.cu:3846-3998 comments) */
+#define CB2_BC_WALL 2
+#define CB2_BC_SYMMETRY 3
+#define CB2_BC_INFLOW 5
+#define CB2_BC_OUTFLOW 6
+#define CB2_BC_PERIODIC 8
+
+/* precision forms */
+#define CB2_PREC_FP64 0  /* plain form: FP64 throughout                                    */
+#define CB2_PREC_MIXED 1 /* FP32 reconstruction/fluxes/viscous stencils, FP64 elsewhere      */
+
+/* stage masks for cb2_rhs */
+#define CB2_RHS_VISCOUS 1u
+#define CB2_RHS_CHEMISTRY 2u
+#define CB2_RHS_INVISCID 4u
+#define CB2_RHS_ALL 7u
+
+/* ---- views ------------------------------------------------------------------------- */
+
+/* Device arrays of one block (the fields of `DZone`, src/Field.h:12-112).  Arrays the
+ * configured path does not read may be NULL. */
+typedef struct cb2_zone_view {
+  int mx, my, mz, ngg;
+  double *cv;       /* n_var comps, ghost ngg  (DZone::cv)                 */
+  double *bv;       /* 6 comps (rho,u,v,w,p,T), ghost ngg  (DZone::bv)      */
+  double *sv;       /* n_scalar comps, ghost ngg (DZone::sv)                */
+  double *qn;       /* n_var comps, ghost ngg (DZone::qn)                   */
+  double *dq;       /* n_var comps, ghost 0   (DZone::dq)                   */
+  double *metric;   /* 9 comps (xi_xyz, eta_xyz, zeta_xyz), ghost ngg        */
+  double *jac;      /* ghost ngg (DZone::jac)                               */
+  double *mul;      /* ghost ngg (DZone::mul)                               */
+  double *thermal_conductivity; /* ghost ngg, mixtures                       */
+  double *rho_D;    /* n_spec comps, ghost ngg, mixtures                    */
+  double *acoustic_speed; /* ghost ngg, mixtures                             */
+  double *gamma;    /* ghost ngg, mixtures                                  */
+  double *mach;     /* ghost ngg, optional                                  */
+  double *fFlux, *gFlux, *hFlux; /* n_var comps, ghost ngg (8th-order viscous node fluxes) */
+  double *vis_flux; /* n_var-1 comps, ghost 1 (2nd-order viscous face fluxes)  */
+  double *shock_sensor;         /* ghost ngg, hybrid schemes only           */
+  double *dt_local;             /* ghost 0                                  */
+  double *reaction_timeScale;   /* ghost ngg, reacting cases                */
+  double *entropy_fix_delta;    /* ghost 1, Roe                             */
+} cb2_zone_view;
+
+/* One face boundary condition of a block (cfd::Boundary, src/Mesh.h:8-30, after
+ * register_boundary, src/Mesh.cpp:14-32): node ranges are inclusive, `face` is the normal
+ * direction (0 i, 1 j, 2 k) and `direction` is -1 on the low face, +1 on the high face. */
+typedef struct cb2_face_bc {
+  int type;          /* CB2_BC_* */
+  int face, direction;
+  int range_start[3], range_end[3];
+  /* inflow / wall data (unused for outflow and periodic) */
+  double rho, u, v, w, p, T;
+  double wall_temperature; /* <=0 : adiabatic wall */
+} cb2_face_bc;
+
+/* Species / reaction data (the fields of `DParameter` that come from cfd::Species and
+ * cfd::Reaction, src/DParameter.cuh:82-130).  All arrays are host arrays, row-major. */
+typedef struct cb2_mechanism {
+  int n_spec, n_reac;
+  const double *mw;            /* [n_spec] kg/kmol                                         */
+  /* NASA7 two-range polynomials (Combustion2Part): coefficients a0..a6 */
+  const double *low_temp_coeff;  /* [n_spec*7] */
+  const double *high_temp_coeff; /* [n_spec*7] */
+  const double *t_low, *t_mid, *t_high; /* [n_spec] */
+  /* transport (Species::geometry etc., src/ChemData.cpp) */
+  const double *geometry;       /* [n_spec] 0 atom, 1 linear, 2 nonlinear                 */
+  const double *LJ_potent_inv;  /* [n_spec] 1/(eps/kB)                                    */
+  const double *vis_coeff;      /* [n_spec] viscosity prefactor                           */
+  const double *WjDivWi_to_One4th;      /* [n_spec*n_spec] */
+  const double *sqrt_WiDivWjPl1Mul8;    /* [n_spec*n_spec] */
+  const double *binary_diffusivity_coeff; /* [n_spec*n_spec] */
+  const double *kb_over_eps_jk;         /* [n_spec*n_spec] */
+  const double *ZRotF298;               /* [n_spec] */
+  /* reactions (Reaction, src/ChemData.h:60-115) */
+  const int *reac_type;   /* [n_reac] */
+  const int *rev_type;    /* [n_reac] */
+  const int *stoi_f;      /* [n_reac*n_spec] */
+  const int *stoi_b;      /* [n_reac*n_spec] */
+  const int *reac_order;  /* [n_reac] */
+  const double *A, *b, *Ea;          /* [n_reac], Ea already divided by R_c */
+  const double *A2, *b2, *Ea2;       /* [n_reac] low-pressure / reverse Arrhenius        */
+  const double *third_body_coeff;    /* [n_reac*n_spec] */
+  const double *troe_alpha, *troe_t3, *troe_t1, *troe_t2; /* [n_reac] */
+} cb2_mechanism;
+
+/* Scalar settings (the scalar fields of `DParameter`, src/DParameter.cuh:13-160, with the
+ * setup.txt meaning given in src/Parameter.cpp:358-546). */
+typedef struct cb2_param_view {
+  int abi_version;         /* must be CB2_ABI_VERSION */
+  int dim;                 /* 1, 2 or 3 (only decides the 2D/3D branches the reference has) */
+  int n_var, n_spec, n_scalar, n_scalar_transported;
+  int inviscid_scheme;     /* CB2_INV_* */
+  int reconstruction;      /* CB2_REC_* (primitive-reconstruction schemes only) */
+  int limiter;             /* 0 minmod */
+  int viscous_order;       /* 0, 2 or 8 */
+  int positive_preserving; /* 0/1 */
+  int gradP_in_diffusion_flux;
+  int reaction;            /* 0 or 1 (finite-rate chemistry) */
+  int shock_sensor;        /* 0 Ducros, 1 Jameson, 2 jump */
+  double sensor_eps, sensor_threshold; /* threshold <= 1e-10: WENO weights everywhere */
+  double entropy_fix_factor;
+  double Pr, cfl;
+  double rho_ref, v_ref;   /* rho_inf, v_inf: WENO eps = 1e-40*(rho_ref*v_ref)^2 */
+  /* air viscosity: <= 0 -> Sutherland (the reference's only air model,
+   * src/FieldOperation.cuh:244); > 0 -> this constant value (added for constant-mu cases) */
+  double mu_constant;
+  int precision;           /* CB2_PREC_* */
+  const cb2_mechanism *mech; /* NULL for the calorically perfect air model */
+} cb2_param_view;
+
+typedef struct cb2_ctx cb2_ctx;
+
+/* ---- life cycle ---------------------------------------------------------------------- */
+
+/* Replaces the construction of `DParameter` (src/DParameter.cu:6-436) as the hot path
+ * sees it: validates the scheme combination and copies the scalar settings and the
+ * mechanism tables to the device.  Allocates only the library's private tables. */
+int cb2_init(const cb2_param_view *param, cb2_ctx **ctx_out);
+
+/* Borrows the device arrays of block `blk` (Field::d_ptr / h_ptr, src/Field.h:164-167)
+ * and its face boundary conditions.  Calling it again for the same `blk` rebinds. */
+int cb2_bind_block(cb2_ctx *ctx, int blk, const cb2_zone_view *zone, const cb2_face_bc *faces,
+                   int n_faces);
+
+void cb2_destroy(cb2_ctx *ctx);
+
+/* ---- the stage pieces (each one replaces one call of RK3, src/RK.cuh) --------------- */
+
+/* qn <- cv: replaces the per-step cudaMemcpy D2D at src/RK.cuh:126-129. */
+int cb2_store_qn(cb2_ctx *ctx, int blk, void *stream);
+
+/* dq <- 0, then the viscous (compute_viscous_flux, src/RK.cuh:173), chemistry
+ * (finite_rate_chemistry, src/RK.cuh:180) and inviscid (compute_inviscid_flux,
+ * src/RK.cuh:186) residual contributions selected by `mask` (CB2_RHS_*). */
+int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream);
+
+/* Shu-Osher stage `rk` (0,1,2) with time step dt, species clipping and primitive recovery:
+ * replaces update_cv_and_bv_rk<mix> (src/RK.cuh:277-367). */
+int cb2_stage_update(cb2_ctx *ctx, int blk, double dt, int rk, void *stream);
+
+/* Ghost fill of bv/sv/cv from the face conditions bound with the block (periodic,
+ * outflow, ...): replaces DBoundCond::apply_boundary_conditions (src/BoundCond.cu:3846). */
+int cb2_boundary(cb2_ctx *ctx, int blk, void *stream);
+
+/* gamma, c, Mach, mu, kappa, rho*D over interior and ghosts: replaces
+ * update_physical_properties<mix> (src/FieldOperation.cuh:183-247). */
+int cb2_properties(cb2_ctx *ctx, int blk, void *stream);
+
+/* cv from bv/sv over interior and ghosts: replaces compute_cv_from_bv<mix>
+ * (src/FieldOperation.cuh:136-161). */
+int cb2_cv_from_bv(cb2_ctx *ctx, int blk, void *stream);
+
+/* Local CFL time step of every node and the min over all bound blocks, returned to the
+ * host: replaces local_time_step<mix> + global_time_step (src/TimeAdvanceFunc.cuh:28-127,
+ * src/TimeAdvanceFunc.cu:114-139).  Synchronises `stream`. */
+int cb2_cfl_dt(cb2_ctx *ctx, double *dt_out, void *stream);
+
+/* One whole SSP-RK3 step over all bound blocks (src/RK.cuh:107-237): qn<-cv, [CFL dt],
+ * 3 x (rhs, stage update, boundary, properties).  With fixed_dt != 0 the step uses
+ * *dt_inout and performs no host synchronisation; otherwise the CFL dt is computed first
+ * and written to *dt_inout. */
+int cb2_rk3_step(cb2_ctx *ctx, double *dt_inout, int fixed_dt, void *stream);
+
+/* ---- diagnostics --------------------------------------------------------------------- */
+
+/* Reads and clears the device status word that kernels set on non-physical states
+ * (bit 0: rho<=0 or non-finite after a stage update; bit 1: T<=0 or Newton failure). */
+int cb2_read_status(cb2_ctx *ctx, unsigned *flags_out, void *stream);
+
+const char *cb2_strerror(int code);
+const char *cb2_last_cuda_error(void);
+
+/* Number of kernels this context launched since creation (a counter the bench reports). */
+unsigned long long cb2_launch_count(const cb2_ctx *ctx);
+
+/* Per-kernel timing, the counterpart of the reference's `profile_rk_breakdown` switch
+ * (src/RK.cuh:90-101, 248-255), without its device-wide synchronisations: while enabled,
+ * every launch is bracketed by a CUDA event pair on its stream and the durations are
+ * aggregated by kernel name.  cb2_profile_count/entry synchronise on the recorded events. */
+int cb2_profile_enable(cb2_ctx *ctx, int on);
+int cb2_profile_reset(cb2_ctx *ctx);
+int cb2_profile_count(cb2_ctx *ctx);
+int cb2_profile_entry(cb2_ctx *ctx, int idx, char *name, int name_len, unsigned long long *count,
+                      double *total_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CB200_H */

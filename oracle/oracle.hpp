@@ -1,0 +1,93 @@
+// FP64 host oracle of COREFL's explicit residual-and-update path.
+//
+// TEST INFRASTRUCTURE ONLY: this restatement of the reference algorithm is the checker the
+// parity tests, smoke() and the bench's CPU-baseline leg compare the CUDA library against.
+// The product (libcb200) never links, loads or calls it.
+//
+// Every routine restates one reference kernel as a plain loop over nodes, in the same
+// arithmetic order as the reference source (cited per function, paths relative to the
+// COREFL-CPC source tree).  Arrays use the reference's padded SoA layout
+// (ggxl::VectorField3D, src/gxl_lib/Array.cuh:307-328), so the same buffers can be handed
+// to the oracle and (after a host->device copy) to the library.
+#pragma once
+#include <cmath>
+#include <cstdint>
+#include <vector>
+#include <algorithm>
+#include "cb200.h"
+
+namespace oracle {
+
+constexpr double R_u = 8314.462618;   // src/Constants.h:15
+constexpr double R_c = 1.98720425864083;
+constexpr double gamma_air = 1.4;     // src/Constants.h:19
+constexpr double mw_air = 28.9647;    // src/Constants.h:25
+constexpr double R_air = R_u / mw_air;
+constexpr double p_atm = 101325;
+constexpr double eps_weno = 1e-40;    // src/WENO.cu:8
+constexpr double pi = 3.141592653589793;
+
+// A padded array view with g ghost layers: element (i,j,k,l) at
+// k*d1 + j*d2 + i + dt + l*sz (src/gxl_lib/Array.cuh:315-324).
+struct Arr {
+  double *p = nullptr;
+  long long d2 = 0, d1 = 0, dt = 0, sz = 0;
+  Arr() = default;
+  Arr(double *ptr, int mx, int my, int mz, int g) : p(ptr) {
+    d2 = mx + 2 * g;
+    d1 = (long long)(my + 2 * g) * d2;
+    dt = (d1 + d2 + 1) * g;
+    sz = (long long)(mx + 2 * g) * (my + 2 * g) * (mz + 2 * g);
+  }
+  double &operator()(int i, int j, int k, int l = 0) const { return p[k * d1 + j * d2 + i + dt + l * sz]; }
+  explicit operator bool() const { return p != nullptr; }
+};
+
+struct Mechanism {
+  int n_spec = 0, n_reac = 0;
+  std::vector<double> imw, gas_const, mw;
+  std::vector<double> lo, hi, t_low, t_mid, t_high;
+  std::vector<double> geometry, lj_inv, vis_coeff, wjwi14, sqwiwj8, bdc, kbe, zrot;
+  std::vector<int> reac_type, rev_type, stoi_f, stoi_b, reac_order;
+  std::vector<double> A, b, Ea, A2, b2, Ea2, tbc, troe_alpha, troe_t3, troe_t1, troe_t2;
+};
+
+struct Param {
+  int dim = 3, n_var = 5, n_spec = 0, n_scalar = 0, n_scalar_transported = 0, n_reac = 0;
+  int inviscid_scheme = 52, reconstruction = 2, limiter = 0, viscous_order = 0;
+  int positive_preserving = 0, gradP = 0, reaction = 0, shock_sensor = 0;
+  double sensor_eps = 0, sensor_threshold = 0, entropy_fix_factor = 0.125, Pr = 0.72, cfl = 0.5;
+  double rho_ref = 1, v_ref = 1, weno_eps_scale = 1, mu_constant = 0;
+  Mechanism mech;
+};
+
+struct FaceBC {
+  int type = 0, face = 0, direction = 1;
+  int start[3] = {0, 0, 0}, end[3] = {0, 0, 0};
+  double rho = 0, u = 0, v = 0, w = 0, p = 0, T = 0, wall_T = 0;
+};
+
+struct Zone {
+  int mx = 0, my = 0, mz = 0, ngg = 0;
+  Arr cv, bv, sv, qn, dq, metric, jac, mul, kappa, rhoD, acoustic, gamma, mach, fF, gF, hF, visf, shock, dtl, rts,
+      efd;
+  std::vector<int> il, ir, jl, jr, kl, kr;  // physical-boundary flags per face node
+  std::vector<FaceBC> faces;
+};
+
+Param make_param(const cb2_param_view &pv);
+Zone make_zone(const cb2_zone_view &v, const cb2_face_bc *faces, int n_faces, const Param &p);
+
+void update_cv_and_bv_rk(Zone &z, const Param &p, double dt, int rk);
+void compute_cv_from_bv(Zone &z, const Param &p);
+void compute_inviscid_flux(Zone &z, const Param &p);
+void compute_viscous_flux(Zone &z, const Param &p);
+void update_physical_properties(Zone &z, const Param &p);
+void apply_boundary_conditions(Zone &z, const Param &p);
+double local_time_step_min(Zone &z, const Param &p);
+void rk3_step(std::vector<Zone> &zones, const Param &p, double &dt, bool fixed_dt);
+
+// thermodynamics used by the tests directly
+void nasa7_h_cp(double t, const Mechanism &m, double *h, double *cp);
+
+}  // namespace oracle

@@ -1,0 +1,99 @@
+// C ABI of the FP64 host oracle (loaded by the tests through ctypes).
+// TEST INFRASTRUCTURE ONLY: never linked into or called by libcb200.
+//
+// The oracle takes the same cb2_param_view / cb2_zone_view / cb2_face_bc structs as the
+// library, with HOST pointers in the zone view.
+#include "oracle.hpp"
+#include <cstring>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+using namespace oracle;
+
+extern "C" {
+
+void oracle_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
+int oracle_max_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+int oracle_stage_update(const cb2_param_view *pv, const cb2_zone_view *zv, double dt, int rk) {
+  Param p = make_param(*pv);
+  Zone z = make_zone(*zv, nullptr, 0, p);
+  update_cv_and_bv_rk(z, p, dt, rk);
+  return 0;
+}
+
+int oracle_cv_from_bv(const cb2_param_view *pv, const cb2_zone_view *zv) {
+  Param p = make_param(*pv);
+  Zone z = make_zone(*zv, nullptr, 0, p);
+  compute_cv_from_bv(z, p);
+  return 0;
+}
+
+int oracle_rhs(const cb2_param_view *pv, const cb2_zone_view *zv, const cb2_face_bc *faces, int n_faces,
+               unsigned mask) {
+  Param p = make_param(*pv);
+  Zone z = make_zone(*zv, faces, n_faces, p);
+  std::memset(z.dq.p, 0, (size_t)z.dq.sz * p.n_var * sizeof(double));
+  if (mask & CB2_RHS_VISCOUS) compute_viscous_flux(z, p);
+  if (mask & CB2_RHS_INVISCID) compute_inviscid_flux(z, p);
+  return 0;
+}
+
+int oracle_boundary(const cb2_param_view *pv, const cb2_zone_view *zv, const cb2_face_bc *faces, int n_faces) {
+  Param p = make_param(*pv);
+  Zone z = make_zone(*zv, faces, n_faces, p);
+  apply_boundary_conditions(z, p);
+  return 0;
+}
+
+int oracle_properties(const cb2_param_view *pv, const cb2_zone_view *zv) {
+  Param p = make_param(*pv);
+  Zone z = make_zone(*zv, nullptr, 0, p);
+  update_physical_properties(z, p);
+  return 0;
+}
+
+int oracle_cfl_dt(const cb2_param_view *pv, const cb2_zone_view *zv, double *dt) {
+  Param p = make_param(*pv);
+  Zone z = make_zone(*zv, nullptr, 0, p);
+  *dt = local_time_step_min(z, p);
+  return 0;
+}
+
+// One RK3 step over n_zones blocks; faces of zone b are faces[off_b .. off_b + n_faces[b]).
+int oracle_rk3_step(const cb2_param_view *pv, const cb2_zone_view *zvs, const cb2_face_bc *faces,
+                    const int *n_faces, int n_zones, double *dt, int fixed_dt) {
+  Param p = make_param(*pv);
+  std::vector<Zone> zones;
+  int off = 0;
+  for (int b = 0; b < n_zones; ++b) {
+    zones.push_back(make_zone(zvs[b], faces + off, n_faces[b], p));
+    off += n_faces[b];
+  }
+  rk3_step(zones, p, *dt, fixed_dt != 0);
+  return 0;
+}
+
+void oracle_nasa7_h_cp(const cb2_mechanism *m, double t, double *h, double *cp) {
+  cb2_param_view pv{};
+  pv.mech = m;
+  pv.n_spec = m->n_spec;
+  Param p = make_param(pv);
+  nasa7_h_cp(t, p.mech, h, cp);
+}
+
+}  // extern "C"

@@ -1,0 +1,103 @@
+"""ctypes binding of the FP64 host oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline leg to check or time the CUDA library; never by the library itself.
+"""
+import ctypes as C
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(os.path.dirname(HERE), "corefl-cpc_b200"))
+from cb200 import abi  # noqa: E402
+
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            import importlib.util
+            spec = importlib.util.spec_from_file_location("oracle_build", os.path.join(HERE, "build.py"))
+            mod = importlib.util.module_from_spec(spec)
+            spec.loader.exec_module(mod)
+            mod.build()
+        lib = C.CDLL(LIB_PATH)
+        P = C.POINTER
+        sig = {
+            "oracle_set_threads": (None, [C.c_int]),
+            "oracle_max_threads": (C.c_int, []),
+            "oracle_stage_update": (C.c_int, [P(abi.ParamView), P(abi.ZoneView), C.c_double, C.c_int]),
+            "oracle_cv_from_bv": (C.c_int, [P(abi.ParamView), P(abi.ZoneView)]),
+            "oracle_rhs": (C.c_int, [P(abi.ParamView), P(abi.ZoneView), P(abi.FaceBC), C.c_int, C.c_uint]),
+            "oracle_boundary": (C.c_int, [P(abi.ParamView), P(abi.ZoneView), P(abi.FaceBC), C.c_int]),
+            "oracle_properties": (C.c_int, [P(abi.ParamView), P(abi.ZoneView)]),
+            "oracle_cfl_dt": (C.c_int, [P(abi.ParamView), P(abi.ZoneView), P(C.c_double)]),
+            "oracle_rk3_step": (C.c_int, [P(abi.ParamView), P(abi.ZoneView), P(abi.FaceBC), P(C.c_int), C.c_int,
+                                          P(C.c_double), C.c_int]),
+            "oracle_nasa7_h_cp": (None, [P(abi.Mechanism), C.c_double, P(C.c_double), P(C.c_double)]),
+        }
+        for n, (r, a) in sig.items():
+            f = getattr(lib, n)
+            f.restype = r
+            f.argtypes = a
+        _lib = lib
+    return _lib
+
+
+def _faces(faces):
+    arr = (abi.FaceBC * max(1, len(faces)))()
+    for a, f in enumerate(faces):
+        arr[a] = f
+    return arr
+
+
+def set_threads(n):
+    load().oracle_set_threads(n)
+
+
+def max_threads():
+    return load().oracle_max_threads()
+
+
+def rhs(param, block, faces, mask=abi.RHS_ALL):
+    v = block.view()
+    load().oracle_rhs(C.byref(param), C.byref(v), _faces(faces), len(faces), mask)
+
+
+def stage_update(param, block, dt, rk):
+    v = block.view()
+    load().oracle_stage_update(C.byref(param), C.byref(v), dt, rk)
+
+
+def boundary(param, block, faces):
+    v = block.view()
+    load().oracle_boundary(C.byref(param), C.byref(v), _faces(faces), len(faces))
+
+
+def properties(param, block):
+    v = block.view()
+    load().oracle_properties(C.byref(param), C.byref(v))
+
+
+def cv_from_bv(param, block):
+    v = block.view()
+    load().oracle_cv_from_bv(C.byref(param), C.byref(v))
+
+
+def cfl_dt(param, block):
+    v = block.view()
+    d = C.c_double()
+    load().oracle_cfl_dt(C.byref(param), C.byref(v), C.byref(d))
+    return d.value
+
+
+def rk3_step(param, blocks, faces_per_block, dt, fixed_dt=True):
+    views = (abi.ZoneView * len(blocks))(*[b.view() for b in blocks])
+    flat = [f for fl in faces_per_block for f in fl]
+    nf = (C.c_int * len(blocks))(*[len(fl) for fl in faces_per_block])
+    d = C.c_double(dt)
+    load().oracle_rk3_step(C.byref(param), views, _faces(flat), nf, len(blocks), C.byref(d), 1 if fixed_dt else 0)
+    return d.value

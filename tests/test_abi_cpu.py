@@ -1,0 +1,62 @@
+"""The C-ABI library loads and exports every symbol include/cb200.h declares, and argument
+validation fails cleanly without touching a GPU."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+import cb200
+from cb200 import abi, cases
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    hdr = open(os.path.join(REPO, "include", "cb200.h")).read()
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    return sorted(set(re.findall(r"\b(cb2_\w+)\s*\(", hdr)))
+
+
+def test_library_exports_every_declared_symbol(cb200_lib):
+    names = declared_symbols()
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(cb200_lib, n)]
+    assert not missing, missing
+
+
+def test_struct_sizes_match_header():
+    # 4 ints + 21 pointers; 3 ints + 6 ints + 7 doubles; versioned param view
+    assert C.sizeof(abi.ZoneView) == 4 * 4 + 21 * 8
+    assert C.sizeof(abi.FaceBC) == 4 * 9 + 4 + 7 * 8  # 36 bytes of ints, padded to 8
+    assert abi.ParamView.abi_version.offset == 0
+
+
+def test_init_rejects_bad_arguments(cb200_lib):
+    h = C.c_void_p()
+    assert cb200_lib.cb2_init(None, C.byref(h)) == abi.ERR_INVALID
+    p = cases.make_param()
+    p.abi_version = 999
+    assert cb200_lib.cb2_init(C.byref(p), C.byref(h)) == abi.ERR_INVALID
+    p = cases.make_param(n_var=7)  # n_var must be 5 + n_spec
+    assert cb200_lib.cb2_init(C.byref(p), C.byref(h)) == abi.ERR_UNSUPPORTED
+    p = cases.make_param(inviscid_scheme=abi.INV_AUSMP, reconstruction=4)
+    assert cb200_lib.cb2_init(C.byref(p), C.byref(h)) == abi.ERR_INVALID
+    p = cases.make_param(viscous_order=3)
+    assert cb200_lib.cb2_init(C.byref(p), C.byref(h)) == abi.ERR_INVALID
+    assert not h.value
+
+
+def test_strerror_covers_codes(cb200_lib):
+    for code in (abi.OK, abi.ERR_CUDA, abi.ERR_INVALID, abi.ERR_NONPHYSICAL, abi.ERR_TIMEOUT,
+                 abi.ERR_UNSUPPORTED, abi.ERR_NOMEM):
+        assert cb200_lib.cb2_strerror(code).decode() != "unknown error"
+
+
+def test_null_context_calls_are_invalid(cb200_lib):
+    assert cb200_lib.cb2_rhs(None, 0, abi.RHS_ALL, None) == abi.ERR_INVALID
+    assert cb200_lib.cb2_stage_update(None, 0, 1e-3, 0, None) == abi.ERR_INVALID
+    assert cb200_lib.cb2_boundary(None, 0, None) == abi.ERR_INVALID
+    d = C.c_double(0.0)
+    assert cb200_lib.cb2_rk3_step(None, C.byref(d), 1, None) == abi.ERR_INVALID
+    assert cb200_lib.cb2_launch_count(None) == 0
