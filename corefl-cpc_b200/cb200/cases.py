@@ -13,6 +13,7 @@ import numpy as np
 
 from . import abi
 from .field import HostBlock, array_specs, box_faces
+from .mech import stoich_h2_air
 
 R_U = 8314.462618
 MW_AIR = 28.9647
@@ -167,3 +168,143 @@ def sine_wave(n=256, ngg=4, amp=0.05, mu=1e-4, scheme=abi.INV_AUSMP, reconstruct
     p = make_param(dim=3, inviscid_scheme=scheme, reconstruction=reconstruction, viscous_order=viscous_order,
                    cfl=0.5, rho_ref=1.0, v_ref=math.sqrt(3.0), mu_constant=mu)
     return Case("sine_wave", p, [b], [faces], {"n": n, "amp": amp})
+
+
+# ---- thermally perfect mixtures ------------------------------------------------------------
+def nasa7_h(mech, t):
+    """h_k(T) [J/kg] on an array of temperatures (NASA7 two-range, linear extension outside)."""
+    d = mech.d
+    ns = mech.ns
+    lo = np.asarray(d["low_temp_coeff"]).reshape(ns, 7)
+    hi = np.asarray(d["high_temp_coeff"]).reshape(ns, 7)
+    tl, tm, th = (np.asarray(d[k]) for k in ("t_low", "t_mid", "t_high"))
+    out = np.empty((ns,) + np.shape(t))
+    for s in range(ns):
+        tt = np.clip(t, tl[s], th[s])
+        c = np.where((tt < tm[s])[None], lo[s][:, None].reshape((7,) + (1,) * np.ndim(t)),
+                     hi[s][:, None].reshape((7,) + (1,) * np.ndim(t)))
+        h = c[0] * tt + 0.5 * c[1] * tt ** 2 + c[2] * tt ** 3 / 3 + 0.25 * c[3] * tt ** 4 + 0.2 * c[4] * tt ** 5 + c[5]
+        cp = c[0] + c[1] * tt + c[2] * tt ** 2 + c[3] * tt ** 3 + c[4] * tt ** 4
+        h = h + cp * (t - tt)
+        out[s] = h * R_U / mech.mw[s]
+    return out
+
+
+def fill_mixture_state(b: HostBlock, mech, rho, u, v, w, p, t, y):
+    """bv, sv and cv of a thermally perfect mixture on the whole padded block."""
+    bv, sv, cv = b.a["bv"], b.a["sv"], b.a["cv"]
+    bv[0], bv[1], bv[2], bv[3], bv[4], bv[5] = rho, u, v, w, p, t
+    for s in range(mech.ns):
+        sv[s] = y[s]
+    h = nasa7_h(mech, bv[5])
+    E = 0.5 * (bv[1] ** 2 + bv[2] ** 2 + bv[3] ** 2)
+    for s in range(mech.ns):
+        E = E + h[s] * sv[s]
+    cv[0] = bv[0]
+    cv[1], cv[2], cv[3] = bv[0] * bv[1], bv[0] * bv[2], bv[0] * bv[3]
+    cv[4] = E * bv[0] - bv[4]
+    for s in range(mech.ns):
+        cv[5 + s] = bv[0] * sv[s]
+
+
+def _mix_r(mech, y):
+    return sum(y[s] * R_U / mech.mw[s] for s in range(mech.ns))
+
+
+def turbulence_field(n, u_rms, k_max=8, k0=4.0, seed=1234):
+    """Divergence-free random-phase velocity on an n^3 periodic lattice with the spectrum
+    E(k) ~ k^4 exp(-2 k^2/k0^2) for |k| <= k_max, scaled to the given u_rms."""
+    rng = np.random.default_rng(seed)
+    kk = np.fft.fftfreq(n, 1.0 / n)
+    KZ, KY, KX = np.meshgrid(kk, kk, kk, indexing="ij")
+    K = np.sqrt(KX ** 2 + KY ** 2 + KZ ** 2)
+    mask = (K > 0) & (K <= k_max)
+    amp = np.zeros_like(K)
+    Ek = K[mask] ** 4 * np.exp(-2 * K[mask] ** 2 / k0 ** 2)
+    amp[mask] = np.sqrt(Ek / (4 * math.pi * K[mask] ** 2))
+    comps = []
+    for _ in range(3):
+        ph = rng.uniform(0, 2 * math.pi, K.shape)
+        comps.append(amp * np.exp(1j * ph))
+    # project onto the plane normal to k
+    kd = [KX, KY, KZ]
+    K2 = np.where(K > 0, K ** 2, 1.0)
+    dot = (kd[0] * comps[0] + kd[1] * comps[1] + kd[2] * comps[2]) / K2
+    vel = [np.real(np.fft.ifftn(comps[a] - kd[a] * dot)) for a in range(3)]
+    rms = math.sqrt(sum(np.mean(v_ ** 2) for v_ in vel) / 3)
+    return [v_ * (u_rms / rms) for v_ in vel]
+
+
+def h2_air_box(mech, n_nodes=192, ngg=3, length=1e-3, seed=2024, scheme=abi.INV_HLLC,
+               reconstruction=abi.REC_WENO5, viscous_order=2, reaction=True):
+    """Reacting H2/air box: n_nodes^3 uniform periodic grid (node 0 == node n-1) with sides L,
+    divergence-free random-phase velocity (|k| <= 8, k^4 exp(-2k^2/k0^2), k0 = 4,
+    u_rms = 10 m/s), T = 1200 K + five 300 K Gaussian hot spots of radius 0.05 mm at seeded
+    positions, p = 1 atm, stoichiometric premixed H2/air."""
+    m = n_nodes
+    nper = m - 1  # periodic intervals
+    dx = length / nper
+    specs = array_specs(m, m, m, ngg, 5 + mech.ns, mech.ns, viscous_order=viscous_order,
+                        roe=(scheme == abi.INV_ROE), reaction=reaction)
+    b = HostBlock(m, m, m, ngg, specs)
+    idx = (np.arange(-ngg, m + ngg)) % nper  # periodic image of every padded node
+    u, v, w = turbulence_field(nper, 10.0, seed=seed)
+    U = [f[np.ix_(idx, idx, idx)] for f in (u, v, w)]  # arrays indexed [k, j, i]
+    rng = np.random.default_rng(seed + 1)
+    centres = rng.uniform(0, length, (5, 3))
+    q = idx * dx
+    Z, Y, X = np.meshgrid(q, q, q, indexing="ij")
+    T = np.full(X.shape, 1200.0)
+    r0 = 0.05e-3
+    for c in centres:
+        d2 = 0
+        for coord, cc in zip((X, Y, Z), c):
+            dd = np.abs(coord - cc)
+            dd = np.minimum(dd, length - dd)
+            d2 = d2 + dd ** 2
+        T += 300.0 * np.exp(-d2 / r0 ** 2)
+    y = stoich_h2_air(mech)
+    p = np.full(X.shape, 101325.0)
+    rho = p / (_mix_r(mech, y) * T)
+    fill_mixture_state(b, mech, rho, U[0], U[1], U[2], p, T, [np.full(X.shape, ys) for ys in y])
+    mt = b.a["metric"]
+    mt[0] = mt[4] = mt[8] = 1.0 / dx
+    b.a["jac"][0] = dx ** 3
+    faces = box_faces(m, m, m, {(d, s): abi.BC_PERIODIC for d in range(3) for s in (-1, 1)})
+    c0 = math.sqrt(1.4 * 101325.0 / float(rho.mean()))
+    par = make_param(n_var=5 + mech.ns, n_spec=mech.ns, dim=3, inviscid_scheme=scheme,
+                     reconstruction=reconstruction, viscous_order=viscous_order, cfl=0.5,
+                     rho_ref=float(rho.mean()), v_ref=c0, mech=mech.ptr())
+    par.reaction = 1 if reaction else 0
+    return Case("h2_air_box", par, [b], [faces], {"dt": 2e-9, "mech": mech, "dx": dx})
+
+
+def reactive_shock_tube(mech, n_nodes=400, ngg=3, length=0.1, scheme=abi.INV_HLLC,
+                        reconstruction=abi.REC_WENO5, reaction=True):
+    """1-D reactive shock tube, stoichiometric H2/air: (T, p) = (1500 K, 5 atm) left of
+    x = L/2 and (300 K, 1 atm) right of it, outflow faces."""
+    mx, my, mz = n_nodes, 1, 1
+    specs = array_specs(mx, my, mz, ngg, 5 + mech.ns, mech.ns, roe=(scheme == abi.INV_ROE), reaction=reaction)
+    b = HostBlock(mx, my, mz, ngg, specs)
+    dx = length / (mx - 1)
+    x = np.arange(-ngg, mx + ngg) * dx
+    left = x <= 0.5 * length
+    shape = b.a["bv"][0].shape
+    T = np.broadcast_to(np.where(left, 1500.0, 300.0)[None, None, :], shape).copy()
+    p = np.broadcast_to(np.where(left, 5 * 101325.0, 101325.0)[None, None, :], shape).copy()
+    y = stoich_h2_air(mech)
+    rho = p / (_mix_r(mech, y) * T)
+    z0 = np.zeros(shape)
+    fill_mixture_state(b, mech, rho, z0, z0, z0, p, T, [np.full(shape, ys) for ys in y])
+    mt = b.a["metric"]
+    mt[0] = 1.0 / dx
+    mt[4] = mt[8] = 1.0
+    b.a["jac"][0] = dx
+    faces = box_faces(mx, my, mz, {(0, -1): abi.BC_OUTFLOW, (0, 1): abi.BC_OUTFLOW,
+                                   (1, -1): abi.BC_OUTFLOW, (1, 1): abi.BC_OUTFLOW})
+    rho_l = float(rho[0, 0, 0])
+    c_l = math.sqrt(1.4 * 5 * 101325.0 / rho_l)
+    par = make_param(n_var=5 + mech.ns, n_spec=mech.ns, dim=2, inviscid_scheme=scheme,
+                     reconstruction=reconstruction, cfl=0.5, rho_ref=rho_l, v_ref=c_l, mech=mech.ptr())
+    par.reaction = 1 if reaction else 0
+    return Case("reactive_shock_tube", par, [b], [faces], {"t_end": 50e-6, "mech": mech, "dx": dx})

@@ -1,0 +1,64 @@
+"""Mechanism tables for cb2_mechanism.
+
+A mechanism is a dict with the fields of cb2_mechanism (the JSON the reference's own parser
+writes; see tests/golden/make_mech.py).  `to_struct` keeps the numpy arrays alive on the
+returned object so the pointers stay valid while the struct is in use.
+"""
+import ctypes as C
+import json
+
+import numpy as np
+
+from . import abi
+
+
+class MechStruct:
+    def __init__(self, d):
+        self.d = d
+        self.ns = int(d["n_spec"])
+        self.nr = int(d.get("n_reac", 0))
+        self.arrays = {}
+        s = abi.Mechanism()
+        s.n_spec = self.ns
+        s.n_reac = self.nr
+        for name in abi.MECH_DOUBLE + abi.MECH_REAC:
+            if name in d:
+                a = np.ascontiguousarray(np.asarray(d[name], dtype=np.float64))
+                self.arrays[name] = a
+                setattr(s, name, a.ctypes.data_as(C.POINTER(C.c_double)))
+        for name in abi.MECH_INT:
+            if name in d:
+                a = np.ascontiguousarray(np.asarray(d[name], dtype=np.int32))
+                self.arrays[name] = a
+                setattr(s, name, a.ctypes.data_as(C.POINTER(C.c_int)))
+        self.struct = s
+
+    @property
+    def species(self):
+        return list(self.d.get("species", []))
+
+    @property
+    def mw(self):
+        return np.asarray(self.d["mw"], dtype=np.float64)
+
+    def index(self, name):
+        return self.species.index(name)
+
+    def ptr(self):
+        return C.pointer(self.struct)
+
+
+def load_json(path):
+    with open(path) as f:
+        return MechStruct(json.load(f))
+
+
+def stoich_h2_air(mech):
+    """Mass fractions of stoichiometric H2/air (X_H2 : X_O2 : X_N2 = 2 : 1 : 3.76)."""
+    y = np.zeros(mech.ns)
+    x = {"H2": 2.0, "O2": 1.0, "N2": 3.76}
+    w = mech.mw
+    tot = sum(x[n] * w[mech.index(n)] for n in x)
+    for n, v in x.items():
+        y[mech.index(n)] = v * w[mech.index(n)] / tot
+    return y

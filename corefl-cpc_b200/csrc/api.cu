@@ -267,7 +267,7 @@ int cb2_init(const cb2_param_view *pv, cb2_ctx **out) {
   if (pv->viscous_order != 0 && pv->viscous_order != 2 && pv->viscous_order != 8) return CB2_ERR_INVALID;
   if (pv->viscous_order == 8 && ns != 0) return CB2_ERR_UNSUPPORTED;
   if (pv->positive_preserving) return CB2_ERR_UNSUPPORTED;
-  if (pv->reaction) return CB2_ERR_UNSUPPORTED;
+  if (pv->reaction && ns == 0) return CB2_ERR_INVALID;
   if (pv->precision != CB2_PREC_FP64) return CB2_ERR_UNSUPPORTED;
   if (pv->sensor_threshold > 1e-10) return CB2_ERR_UNSUPPORTED;  // shock sensor kernel not built
   cb2_ctx *ctx = new cb2_ctx;
@@ -465,7 +465,6 @@ int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream) {
   ProfGuard pg(ctx);
   cudaStream_t s = (cudaStream_t)stream;
   const Param &p = ctx->p;
-  if ((mask & CB2_RHS_CHEMISTRY) && p.reaction) return CB2_ERR_UNSUPPORTED;
   int nl = 0;
   {
     ProfScope prof("zero_dq", s);
@@ -473,6 +472,7 @@ int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream) {
   }
   if ((mask & CB2_RHS_VISCOUS) && p.viscous_order > 0)
     CB2_TRY(launch_viscous(B->z, p, B->faces.data(), (int)B->faces.size(), s, nl));
+  if ((mask & CB2_RHS_CHEMISTRY) && p.reaction) CB2_TRY(launch_chemistry(B->z, p, s, nl));
   if (mask & CB2_RHS_INVISCID) {
     if (p.inviscid_scheme == CB2_INV_WENO5_CH || p.inviscid_scheme == CB2_INV_WENO7_CH)
       CB2_TRY(launch_inviscid_char(B->z, p, s, nl));

@@ -76,6 +76,7 @@ int launch_eliminate_k_gradient(const Zone &z, const Param &p, cudaStream_t s, i
 int launch_periodic_flux_exchange(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, cudaStream_t s,
                                   int &n_launch);
 int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, cudaStream_t s, int &n_launch);
+int launch_chemistry(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
 int launch_local_dt(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
 int launch_min_reduce(const double *src, long long n, double *partial, int n_partial, double *out,
                       cudaStream_t s, int &n_launch);

@@ -84,6 +84,28 @@ __device__ __forceinline__ void nasa7_cp(double t, const Mech &m, double *cp) {
   }
 }
 
+// g_k/(R_k T) of every species (compute_gibbs_div_rt, src/Thermo.cu:576-632, NASA7 branch);
+// outside [t_low, t_high] the polynomial is evaluated at the range edge.
+template <int NS>
+__device__ __forceinline__ void nasa7_gibbs_rt(double t, const Mech &m, double *g) {
+  const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, t_inv = 1 / t, log_t = log(t);
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const double tl = __ldg(m.t_low + s), th = __ldg(m.t_high + s);
+    if (t < tl || t > th) {
+      const double tt = t < tl ? tl : th;
+      const double *c = (t < tl ? m.lo : m.hi) + s * 7;
+      const double tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt, tt_inv = 1 / tt, log_tt = log(tt);
+      g[s] = __ldg(c + 0) * (1.0 - log_tt) - 0.5 * __ldg(c + 1) * tt - __ldg(c + 2) * tt2 / 6.0 -
+             __ldg(c + 3) * tt3 / 12.0 - __ldg(c + 4) * tt4 * 0.05 + __ldg(c + 5) * tt_inv - __ldg(c + 6);
+    } else {
+      const double *c = (t < __ldg(m.t_mid + s) ? m.lo : m.hi) + s * 7;
+      g[s] = __ldg(c + 0) * (1.0 - log_t) - 0.5 * __ldg(c + 1) * t - __ldg(c + 2) * t2 / 6.0 -
+             __ldg(c + 3) * t3 / 12.0 - __ldg(c + 4) * t4 * 0.05 + __ldg(c + 5) * t_inv - __ldg(c + 6);
+    }
+  }
+}
+
 // Mixture gamma and sound speed at the Roe state, plus the scalar rows of the left
 // eigenvectors (alpha_s) and the energy coefficients of the right eigenvectors
 // (src/Thermo.cuh:49-110 with two_temperature off: e_ve = 0).

@@ -1013,6 +1013,142 @@ void transport(double t, double mw_total, const double *y, const double *cp, con
   for (int l = 0; l < ns; ++l) rhoD[l] = num[l] * ti / dsum[l];
 }
 
+// ---------------------------------------------------------------------------------------
+// Finite-rate chemistry (src/FiniteRateChem.cu:1406-1681, generic mechanisms, 1T)
+// ---------------------------------------------------------------------------------------
+void gibbs_div_rt(double t, const Mechanism &m, double *g) {
+  // compute_gibbs_div_rt (src/Thermo.cu:576-605)
+  const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, t_inv = 1 / t, log_t = std::log(t);
+  for (int i = 0; i < m.n_spec; ++i) {
+    if (t < m.t_low[i] || t > m.t_high[i]) {
+      const double tt = t < m.t_low[i] ? m.t_low[i] : m.t_high[i];
+      const double *c = (t < m.t_low[i] ? m.lo.data() : m.hi.data()) + 7 * i;
+      const double tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt, tt_inv = 1 / tt, log_tt = std::log(tt);
+      g[i] = c[0] * (1.0 - log_tt) - 0.5 * c[1] * tt - c[2] * tt2 / 6.0 - c[3] * tt3 / 12.0 - c[4] * tt4 * 0.05 +
+             c[5] * tt_inv - c[6];
+    } else {
+      const double *c = (t < m.t_mid[i] ? m.lo.data() : m.hi.data()) + 7 * i;
+      g[i] = c[0] * (1.0 - log_t) - 0.5 * c[1] * t - c[2] * t2 / 6.0 - c[3] * t3 / 12.0 - c[4] * t4 * 0.05 +
+             c[5] * t_inv - c[6];
+    }
+  }
+}
+
+double arrhenius(double t, double A, double b, double Ea) { return A * std::pow(t, b) * std::exp(-Ea / t); }
+
+void chemistry_point(const Mechanism &m, double rho, double t, const double *y, double *omega, double *omega_d) {
+  const int ns = m.n_spec, nr = m.n_reac;
+  double c[16], kf[32], kb[32], q1[32], q2[32];
+  for (int l = 0; l < ns; ++l) c[l] = rho * y[l] * m.imw[l] * 1e-3;
+  // forward_reaction_rate (:1505-1554), 1T reaction temperature
+  for (int i = 0; i < nr; ++i) {
+    kf[i] = arrhenius(t, m.A[i], m.b[i], m.Ea[i]);
+    const int ty = m.reac_type[i];
+    if (ty == 3) {
+      kf[i] += arrhenius(t, m.A2[i], m.b2[i], m.Ea2[i]);
+    } else if (ty > 3) {
+      double cc = 0;
+      for (int l = 0; l < ns; ++l) cc += c[l] * m.tbc[i * ns + l];
+      if (ty == 4) {
+        kf[i] *= cc;
+      } else {
+        const double kf_low = arrhenius(t, m.A2[i], m.b2[i], m.Ea2[i]);
+        const double kf_high = kf[i];
+        if (kf_high < 1e-25 && kf_low < 1e-25) {
+          kf[i] = 0;
+          continue;
+        }
+        const double pr = kf_low * cc / kf_high;
+        double F = 1.0;
+        if (ty > 5) {
+          double fc = (1 - m.troe_alpha[i]) * std::exp(-t / m.troe_t3[i]) + m.troe_alpha[i] * std::exp(-t / m.troe_t1[i]);
+          if (ty == 7) fc += std::exp(-m.troe_t2[i] / t);
+          const double lfc = std::log10(fc);
+          const double cq = -0.4 - 0.67 * lfc;
+          const double nq = 0.75 - 1.27 * lfc;
+          const double lpr = std::log10(pr);
+          const double tempo = (lpr + cq) / (nq - 0.14 * (lpr + cq));
+          const double pp = lfc / (1.0 + tempo * tempo);
+          F = std::pow(10, pp);
+        }
+        kf[i] = kf_high * pr / (1.0 + pr) * F;
+      }
+    }
+  }
+  // backward_reaction_rate (:1593-1636)
+  int n_gibbs = nr;
+  for (int i = 0; i < nr; ++i) {
+    if (m.reac_type[i] == 0) {
+      kb[i] = 0;
+      --n_gibbs;
+    } else if (m.rev_type[i] == 1) {
+      kb[i] = arrhenius(t, m.A2[i], m.b2[i], m.Ea2[i]);
+      if (m.reac_type[i] == 4) {
+        double cc = 0;
+        for (int l = 0; l < ns; ++l) cc += c[l] * m.tbc[i * ns + l];
+        kb[i] *= cc;
+      }
+      --n_gibbs;
+    }
+  }
+  if (n_gibbs >= 1) {
+    double g[16];
+    gibbs_div_rt(t, m, g);
+    const double temp_p = p_atm / R_u * 1e-3;
+    const double temp_t = temp_p / t;
+    for (int i = 0; i < nr; ++i) {
+      if (m.reac_type[i] != 2 && m.reac_type[i] != 0) {
+        double dg = 0;
+        for (int l = 0; l < ns; ++l) dg += g[l] * (m.stoi_b[i * ns + l] - m.stoi_f[i * ns + l]);
+        const double kc = std::pow(temp_t, m.reac_order[i]) * std::exp(-dg);
+        kb[i] = kf[i] / kc;
+      }
+    }
+  }
+  // rate_of_progress (:1638-1663)
+  for (int i = 0; i < nr; ++i) {
+    q1[i] = 1.0;
+    q2[i] = m.reac_type[i] != 0 ? 1.0 : 0.0;
+    for (int j = 0; j < ns; ++j) {
+      q1[i] *= std::pow(c[j], m.stoi_f[i * ns + j]);
+      if (m.reac_type[i] != 0) q2[i] *= std::pow(c[j], m.stoi_b[i * ns + j]);
+    }
+    q1[i] *= kf[i];
+    if (m.reac_type[i] != 0) q2[i] *= kb[i];
+  }
+  // chemical_source (:1665-1681)
+  for (int i = 0; i < ns; ++i) {
+    double creation = 0;
+    omega_d[i] = 0;
+    for (int j = 0; j < nr; ++j) {
+      creation += q2[j] * m.stoi_f[j * ns + i] + q1[j] * m.stoi_b[j * ns + i];
+      omega_d[i] += q1[j] * m.stoi_f[j * ns + i] + q2[j] * m.stoi_b[j * ns + i];
+    }
+    creation *= 1e+3 / m.imw[i];
+    omega_d[i] *= 1e+3 / m.imw[i];
+    omega[i] = creation - omega_d[i];
+  }
+}
+
+void finite_rate_chemistry(Zone &z, const Param &p) {
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int k = 0; k < z.mz; ++k)
+    for (int j = 0; j < z.my; ++j)
+      for (int i = 0; i < z.mx; ++i) {
+        const int ns = p.n_spec;
+        double y[16], om[16], od[16];
+        for (int l = 0; l < ns; ++l) y[l] = z.sv(i, j, k, l);
+        const double rho = z.bv(i, j, k, 0);
+        chemistry_point(p.mech, rho, z.bv(i, j, k, 5), y, om, od);
+        double ts = 1e+6;
+        for (int l = 0; l < ns; ++l) {
+          z.dq(i, j, k, l + 5) += z.jac(i, j, k) * om[l];
+          if (y[l] > 1e-25 && std::fabs(od[l]) > 1e-25) ts = std::min(ts, std::fabs(rho * y[l] / od[l]));
+        }
+        if (z.rts) z.rts(i, j, k) = ts;
+      }
+}
+
 double sutherland(double t) { return 1.7894e-5 * std::pow(t / 288.16, 1.5) * (288.16 + 110) / (t + 110); }
 
 void cv_point(Zone &z, const Param &p, int i, int j, int k) {
@@ -1263,6 +1399,12 @@ void compute_inviscid_flux(Zone &z, const Param &p) {
   }
 }
 
+void compute_chemistry(Zone &z, const Param &p) { finite_rate_chemistry(z, p); }
+
+void chemistry_source(const Mechanism &m, double rho, double t, const double *y, double *omega, double *omega_d) {
+  chemistry_point(m, rho, t, y, omega, omega_d);
+}
+
 void compute_viscous_flux(Zone &z, const Param &p) {
   if (p.viscous_order == 8) viscous_8th(z, p);
   else if (p.viscous_order == 2) viscous_2nd(z, p);
@@ -1428,6 +1570,7 @@ void rk3_step(std::vector<Zone> &zones, const Param &p, double &dt, bool fixed_d
       compute_viscous_flux(z, p);
     }
     for (auto &z : zones) {
+      if (p.reaction) finite_rate_chemistry(z, p);
       compute_inviscid_flux(z, p);
       update_cv_and_bv_rk(z, p, dt, rk);
       apply_boundary_conditions(z, p);

@@ -82,6 +82,8 @@ void update_cv_and_bv_rk(Zone &z, const Param &p, double dt, int rk);
 void compute_cv_from_bv(Zone &z, const Param &p);
 void compute_inviscid_flux(Zone &z, const Param &p);
 void compute_viscous_flux(Zone &z, const Param &p);
+void compute_chemistry(Zone &z, const Param &p);
+void chemistry_source(const Mechanism &m, double rho, double t, const double *y, double *omega, double *omega_d);
 void update_physical_properties(Zone &z, const Param &p);
 void apply_boundary_conditions(Zone &z, const Param &p);
 double local_time_step_min(Zone &z, const Param &p);

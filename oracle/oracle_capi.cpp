@@ -49,6 +49,7 @@ int oracle_rhs(const cb2_param_view *pv, const cb2_zone_view *zv, const cb2_face
   Zone z = make_zone(*zv, faces, n_faces, p);
   std::memset(z.dq.p, 0, (size_t)z.dq.sz * p.n_var * sizeof(double));
   if (mask & CB2_RHS_VISCOUS) compute_viscous_flux(z, p);
+  if ((mask & CB2_RHS_CHEMISTRY) && p.reaction) compute_chemistry(z, p);
   if (mask & CB2_RHS_INVISCID) compute_inviscid_flux(z, p);
   return 0;
 }
@@ -94,6 +95,16 @@ void oracle_nasa7_h_cp(const cb2_mechanism *m, double t, double *h, double *cp) 
   pv.n_spec = m->n_spec;
   Param p = make_param(pv);
   nasa7_h_cp(t, p.mech, h, cp);
+}
+
+// omega_k and the destruction part omega_d,k [kg/(m^3 s)] of one state (rho, T, Y).
+void oracle_chemistry_source(const cb2_mechanism *m, double rho, double t, const double *y, double *omega,
+                             double *omega_d) {
+  cb2_param_view pv{};
+  pv.mech = m;
+  pv.n_spec = m->n_spec;
+  Param p = make_param(pv);
+  chemistry_source(p.mech, rho, t, y, omega, omega_d);
 }
 
 }  // extern "C"

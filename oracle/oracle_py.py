@@ -101,3 +101,26 @@ def rk3_step(param, blocks, faces_per_block, dt, fixed_dt=True):
     d = C.c_double(dt)
     load().oracle_rk3_step(C.byref(param), views, _faces(flat), nf, len(blocks), C.byref(d), 1 if fixed_dt else 0)
     return d.value
+
+
+def chemistry_source(mech, rho, t, y):
+    """(omega, omega_d) [kg/(m^3 s)] of one state from the oracle's finite-rate chemistry."""
+    import numpy as np
+    lib = load()
+    lib.oracle_chemistry_source.restype = None
+    P = C.POINTER(C.c_double)
+    lib.oracle_chemistry_source.argtypes = [C.POINTER(abi.Mechanism), C.c_double, C.c_double, P, P, P]
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    om = np.zeros(mech.ns)
+    od = np.zeros(mech.ns)
+    lib.oracle_chemistry_source(mech.ptr(), rho, t, y.ctypes.data_as(P), om.ctypes.data_as(P), od.ctypes.data_as(P))
+    return om, od
+
+
+def nasa7_h_cp(mech, t):
+    import numpy as np
+    h = np.zeros(mech.ns)
+    cp = np.zeros(mech.ns)
+    P = C.POINTER(C.c_double)
+    load().oracle_nasa7_h_cp(mech.ptr(), t, h.ctypes.data_as(P), cp.ctypes.data_as(P))
+    return h, cp

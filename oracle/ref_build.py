@@ -1,0 +1,49 @@
+"""Build the reference's own host code into oracle/_ref/ (TEST INFRASTRUCTURE ONLY).
+
+Compiles, straight from the reference source tree (never copied into this repository):
+  dump_mech : cfd::Species / cfd::Reaction (src/ChemData.cpp) + cfd::Parameter
+              (src/Parameter.cpp) + src/Element.cpp + src/gxl_lib/MyString.cpp, with the
+              single-process oracle/ref/mpi.h, oracle/ref/stubs.cpp and
+              oracle/ref/dump_mech.cpp; it writes the mechanism tables as JSON.
+The reference's CMake build needs MPI and is not used.
+Usage: python oracle/ref_build.py [/path/to/reference]
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "_ref")
+
+
+def build(ref="/root/reference", force=False):
+    src = os.path.join(ref, "src")
+    if not os.path.isdir(src):
+        return None
+    os.makedirs(OUT, exist_ok=True)
+    exe = os.path.join(OUT, "dump_mech")
+    mine = [os.path.join(HERE, "ref", f) for f in ("stubs.cpp", "dump_mech.cpp", "mpi.h")]
+    theirs = [os.path.join(src, f) for f in ("ChemData.cpp", "Parameter.cpp", "Element.cpp",
+                                             os.path.join("gxl_lib", "MyString.cpp"))]
+    if not force and os.path.exists(exe) and os.path.getmtime(exe) >= max(os.path.getmtime(f) for f in mine):
+        return exe
+    cmd = ["g++", "-std=c++20", "-O1", "-DMAX_SPEC_NUMBER=9", "-DMAX_REAC_NUMBER=20", "-DCombustion2Part",
+           "-I", os.path.join(HERE, "ref"), "-I", src,
+           *[f for f in theirs], *[f for f in mine if f.endswith(".cpp")], "-o", exe]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("reference host build failed:\n" + r.stderr[-4000:])
+    # dump_chem: the same parser plus the host chemistry of src/ConstVolumeReactor.cpp
+    exe2 = os.path.join(OUT, "dump_chem")
+    cmd2 = [c for c in cmd if not c.endswith("dump_mech.cpp")]
+    cmd2[-1] = exe2
+    cmd2[-2:-2] = [os.path.join(src, "ConstVolumeReactor.cpp"), os.path.join(HERE, "ref", "dump_chem.cpp"),
+                   os.path.join(HERE, "ref", "chem_stubs.cpp")]
+    r = subprocess.run(cmd2, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("reference host chemistry build failed:\n" + r.stderr[-4000:])
+    return exe
+
+
+if __name__ == "__main__":
+    print(build(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", force=True))

@@ -1,0 +1,59 @@
+"""Write the mechanism fixtures of tests/golden/ with the reference's own parser.
+
+Runs oracle/_ref/dump_mech (cfd::Species + cfd::Reaction of the reference, built by
+oracle/ref_build.py) on the reference's example data files and keeps its JSON output:
+  h2_li2004.json : 9 species / 19 reactions, Li et al. 2004 H2/O2 mechanism
+                   (example/constantVolumeReactor/input/chemistry/2004-Li-IntJ.Chem.Kinet.inp)
+                   with NASA7 thermo and transport from example/reactiveShockTube/input/chemistry/
+                   (therm_nasa_7_9 = 7)
+  h2_chem_states.json : 48 seeded (rho, T, Y) states with the reference's host chemistry
+                   source cfd::compute_src, h_k/cp_k from Species::compute_enthalpy_and_cp and
+                   the Newton temperature of cfd::update_t (src/ConstVolumeReactor.cpp)
+Usage: python tests/golden/make_mech.py [/path/to/reference]
+"""
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+
+
+def run(ref, name, files, nasa, prog="dump_mech", extra=()):
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("ref_build", os.path.join(REPO, "oracle", "ref_build.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    exe = mod.build(ref)
+    with tempfile.TemporaryDirectory() as d:
+        os.makedirs(os.path.join(d, "input", "chemistry"))
+        for key, rel in files.items():
+            shutil.copy(os.path.join(ref, rel), os.path.join(d, "input", "chemistry", os.path.basename(rel)))
+        setup = os.path.join(d, "setup.txt")
+        with open(setup, "w") as f:
+            f.write("int species = 1\nint reaction = 1\nint myid = 0\nint chemSrcMethod = 0\n"
+                    "int n_var = 5\nint n_scalar = 0\n")
+            f.write(f"int therm_nasa_7_9 = {nasa}\n")
+            for key, rel in files.items():
+                f.write(f"string {key} = chemistry/{os.path.basename(rel)}\n")
+        out = os.path.join(HERE, name)
+        exe_p = os.path.join(os.path.dirname(exe), prog)
+        r = subprocess.run([exe_p, setup, out, *extra], cwd=d, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(r.stdout + r.stderr)
+    return out
+
+
+def main(ref):
+    chem = "example/reactiveShockTube/input/chemistry/"
+    files = {"mechanism_file": "example/constantVolumeReactor/input/chemistry/2004-Li-IntJ.Chem.Kinet.inp",
+             "therm_file": chem + "therm.dat", "transport_file": chem + "tran.dat"}
+    print(run(ref, "h2_li2004.json", files, 7))
+    print(run(ref, "h2_chem_states.json", files, 7, prog="dump_chem", extra=("48",)))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
