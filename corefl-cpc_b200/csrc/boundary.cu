@@ -7,10 +7,12 @@
 //              src/BoundCond.cu:2204-2350)
 //   periodic : average of the coincident end nodes, then ghost copy from the far side
 //              (apply_periodic, src/BoundCond.cu:3390-3440)
-//   symmetry : mirror with the normal velocity reflected (apply_symmetry, src/BoundCond.cu:2130)
-//   inflow   : fixed state in all ghost layers (apply_inflow constant-state branch,
-//              src/BoundCond.cu:2484)
-//   wall     : no-slip, adiabatic or isothermal (apply_wall, src/BoundCond.cu:3055-3389)
+//   symmetry : mirror with the normal velocity reflected (apply_symmetry, src/BoundCond.cu:2130-2202)
+//   inflow   : fixed supersonic state on the face node and all ghost layers (the constant
+//              state of apply_inflow, src/BoundCond.cu:2484; its profile, subsonic and
+//              turbulent-fluctuation branches are not built)
+//   wall     : no-slip, non-catalytic, adiabatic or isothermal (apply_wall,
+//              src/BoundCond.cu:3055-3389)
 // Every filled node gets its cv recomputed (compute_cv_from_bv_1_point, FieldOperation.cuh:163).
 #include "common.cuh"
 #include "thermo.cuh"
@@ -102,6 +104,9 @@ __global__ void k_bc_periodic(Zone z, Param p, FaceBC f) {
   }
 }
 
+// Symmetry (apply_symmetry, src/BoundCond.cu:2130-2202): the face node takes the tangential
+// velocity and the rho, p, T, Y of its inner neighbour; ghosts mirror the interior with the
+// normal velocity reflected.
 template <int NS>
 __global__ void k_bc_symmetry(Zone z, Param p, FaceBC f) {
   int i, j, k;
@@ -110,28 +115,32 @@ __global__ void k_bc_symmetry(Zone z, Param p, FaceBC f) {
   d[f.face] = f.direction;
   const idx_t sz = z.L.sz;
   const idx_t gb = z.L.at(i, j, k);
+  const idx_t g1 = z.L.at(i - d[0], j - d[1], k - d[2]);
   const double *M = z.metric + (idx_t)(3 * f.face) * sz;
-  double nx = M[gb], ny = M[gb + sz], nz = M[gb + 2 * sz];
-  const double gni = 1.0 / norm3d(nx, ny, nz);
-  nx *= gni; ny *= gni; nz *= gni;
-  // the boundary node itself loses its normal velocity
+  double kx = M[gb], ky = M[gb + sz], kz = M[gb + 2 * sz];
+  const double km = sqrt(kx * kx + ky * ky + kz * kz);
+  kx /= km; ky /= km; kz /= km;
   {
-    const double u = z.bv[gb + sz], v = z.bv[gb + 2 * sz], w = z.bv[gb + 3 * sz];
-    const double vn = nx * u + ny * v + nz * w;
-    z.bv[gb + sz] = u - vn * nx;
-    z.bv[gb + 2 * sz] = v - vn * ny;
-    z.bv[gb + 3 * sz] = w - vn * nz;
+    const double u1 = z.bv[g1 + sz], v1 = z.bv[g1 + 2 * sz], w1 = z.bv[g1 + 3 * sz];
+    const double uk = kx * u1 + ky * v1 + kz * w1;
+    z.bv[gb + sz] = u1 - kx * uk;
+    z.bv[gb + 2 * sz] = v1 - ky * uk;
+    z.bv[gb + 3 * sz] = w1 - kz * uk;
+    z.bv[gb] = z.bv[g1];
+    z.bv[gb + 4 * sz] = z.bv[g1 + 4 * sz];
+    z.bv[gb + 5 * sz] = z.bv[g1 + 5 * sz];
+    for (int l = 0; l < p.n_scalar; ++l) z.sv[gb + l * sz] = z.sv[g1 + l * sz];
     cv_point<NS>(z, p, gb);
   }
   for (int gl = 1; gl <= z.ngg; ++gl) {
     const idx_t gg = z.L.at(i + gl * d[0], j + gl * d[1], k + gl * d[2]);
     const idx_t gi = z.L.at(i - gl * d[0], j - gl * d[1], k - gl * d[2]);
-    const double u = z.bv[gi + sz], v = z.bv[gi + 2 * sz], w = z.bv[gi + 3 * sz];
-    const double vn = nx * u + ny * v + nz * w;
     z.bv[gg] = z.bv[gi];
-    z.bv[gg + sz] = u - 2 * vn * nx;
-    z.bv[gg + 2 * sz] = v - 2 * vn * ny;
-    z.bv[gg + 3 * sz] = w - 2 * vn * nz;
+    const double u = z.bv[gi + sz], v = z.bv[gi + 2 * sz], w = z.bv[gi + 3 * sz];
+    const double uk = kx * u + ky * v + kz * w;
+    z.bv[gg + sz] = u - 2 * uk * kx;
+    z.bv[gg + 2 * sz] = v - 2 * uk * ky;
+    z.bv[gg + 3 * sz] = w - 2 * uk * kz;
     z.bv[gg + 4 * sz] = z.bv[gi + 4 * sz];
     z.bv[gg + 5 * sz] = z.bv[gi + 5 * sz];
     for (int l = 0; l < p.n_scalar; ++l) z.sv[gg + l * sz] = z.sv[gi + l * sz];
@@ -159,9 +168,30 @@ __global__ void k_bc_inflow(Zone z, Param p, FaceBC f, const double *y_in) {
   }
 }
 
-// No-slip wall: the wall node gets zero velocity and T_wall (isothermal) or the first-cell
-// temperature (adiabatic), p from the first interior node; ghosts mirror the interior with
-// reflected velocity and the wall-centred temperature.
+// Index of the interior node a wall reads, moved off any physical boundary of the block
+// (project_to_interior in apply_wall, src/BoundCond.cu:3070-3088).  The face flags exist for
+// face nodes only; a tangential index in the ghost range (extended face ranges) reads no
+// flag here, where the reference's flag lookup would leave the array.
+__device__ __forceinline__ bool flag_at(const int *f, int a, int na, int b, int nb) {
+  return a >= 0 && a < na && b >= 0 && b < nb && f[a + b * na] != 0;
+}
+
+__device__ __forceinline__ void project_to_interior(const Zone &z, int &i, int &j, int &k) {
+  if (i <= 0 && flag_at(z.bt.il, j, z.my, k, z.mz)) i = 1;
+  else if (i >= z.mx - 1 && flag_at(z.bt.ir, j, z.my, k, z.mz)) i = z.mx - 2;
+  if (j <= 0 && flag_at(z.bt.jl, i, z.mx, k, z.mz)) j = 1;
+  else if (j >= z.my - 1 && flag_at(z.bt.jr, i, z.mx, k, z.mz)) j = z.my - 2;
+  if (z.mz > 1) {
+    if (k <= 0 && flag_at(z.bt.kl, i, z.mx, j, z.my)) k = 1;
+    else if (k >= z.mz - 1 && flag_at(z.bt.kr, i, z.mx, j, z.my)) k = z.mz - 2;
+  }
+}
+
+// No-slip, non-catalytic wall, isothermal (wall_T > 0) or adiabatic (apply_wall,
+// src/BoundCond.cu:3055-3389, without jets, blowing or wall fluctuations): the wall node takes
+// p and Y of the first interior node and T_wall; ghosts mirror the interior velocity and, for
+// an isothermal wall, T_ghost = 2 T_wall - T_inner (floored at T_wall when it drops below
+// 0.1 T_wall).
 template <int NS>
 __global__ void k_bc_wall(Zone z, Param p, FaceBC f) {
   int i, j, k;
@@ -170,37 +200,51 @@ __global__ void k_bc_wall(Zone z, Param p, FaceBC f) {
   d[f.face] = f.direction;
   const idx_t sz = z.L.sz;
   const idx_t gb = z.L.at(i, j, k);
-  const idx_t g1 = z.L.at(i - d[0], j - d[1], k - d[2]);
-  const double t_wall = f.wall_T > 0 ? f.wall_T : z.bv[g1 + 5 * sz];
-  const double p_wall = z.bv[g1 + 4 * sz];
-  double r_mix = kRAir;
+  int ii = i - d[0], ij = j - d[1], ik = k - d[2];
+  project_to_interior(z, ii, ij, ik);
+  const idx_t g1 = z.L.at(ii, ij, ik);
+  const bool iso = f.wall_T > 0;
+  const double t_wall = iso ? f.wall_T : z.bv[g1 + 5 * sz];
+  const double pw = z.bv[g1 + 4 * sz];
+  double R = kRAir;
   if constexpr (NS > 0) {
-    r_mix = 0;
-    for (int s = 0; s < NS; ++s) r_mix += z.sv[gb + s * sz] * __ldg(p.mech.gas_const + s);
+    R = 0;
+    for (int s = 0; s < NS; ++s) {
+      z.sv[gb + s * sz] = z.sv[g1 + s * sz];
+      R += z.sv[gb + s * sz] * __ldg(p.mech.gas_const + s);
+    }
   }
+  z.bv[gb] = pw / (t_wall * R);
   z.bv[gb + sz] = 0;
   z.bv[gb + 2 * sz] = 0;
   z.bv[gb + 3 * sz] = 0;
-  z.bv[gb + 4 * sz] = p_wall;
+  z.bv[gb + 4 * sz] = pw;
   z.bv[gb + 5 * sz] = t_wall;
-  z.bv[gb] = p_wall / (r_mix * t_wall);
   cv_point<NS>(z, p, gb);
   for (int gl = 1; gl <= z.ngg; ++gl) {
+    int ai = i - gl * d[0], aj = j - gl * d[1], ak = k - gl * d[2];
+    project_to_interior(z, ai, aj, ak);
+    const idx_t gi = z.L.at(ai, aj, ak);
     const idx_t gg = z.L.at(i + gl * d[0], j + gl * d[1], k + gl * d[2]);
-    const idx_t gi = z.L.at(i - gl * d[0], j - gl * d[1], k - gl * d[2]);
-    const double t_g = fmax(2 * t_wall - z.bv[gi + 5 * sz], 0.1 * t_wall);
+    const double p_i = z.bv[gi + 4 * sz], t_i = z.bv[gi + 5 * sz];
+    double t_g = t_i;
+    if (iso) {
+      t_g = 2 * t_wall - t_i;
+      if (t_g <= 0.1 * t_wall) t_g = t_wall;
+    }
+    if constexpr (NS > 0) {
+      R = 0;
+      for (int s = 0; s < NS; ++s) {
+        z.sv[gg + s * sz] = z.sv[gi + s * sz];
+        R += z.sv[gi + s * sz] * __ldg(p.mech.gas_const + s);
+      }
+    }
+    z.bv[gg] = p_i / (t_g * R);
     z.bv[gg + sz] = -z.bv[gi + sz];
     z.bv[gg + 2 * sz] = -z.bv[gi + 2 * sz];
     z.bv[gg + 3 * sz] = -z.bv[gi + 3 * sz];
-    z.bv[gg + 4 * sz] = z.bv[gi + 4 * sz];
+    z.bv[gg + 4 * sz] = p_i;
     z.bv[gg + 5 * sz] = t_g;
-    for (int l = 0; l < p.n_scalar; ++l) z.sv[gg + l * sz] = z.sv[gi + l * sz];
-    double rg = kRAir;
-    if constexpr (NS > 0) {
-      rg = 0;
-      for (int s = 0; s < NS; ++s) rg += z.sv[gg + s * sz] * __ldg(p.mech.gas_const + s);
-    }
-    z.bv[gg] = z.bv[gg + 4 * sz] / (rg * t_g);
     cv_point<NS>(z, p, gg);
   }
 }

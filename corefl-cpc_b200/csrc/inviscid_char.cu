@@ -97,7 +97,8 @@ __device__ __forceinline__ void char_flux(const double *__restrict__ sQ, const d
   }
 
   double fch[NV];
-#pragma unroll
+  // one characteristic field at a time: keeps the stencil projections of a single field live
+#pragma unroll 1
   for (int l = 0; l < 5; ++l) {
     double L0, L1, L2, L3, L4, tc;
     if (l == 0 || l == 4) {
@@ -134,7 +135,7 @@ __device__ __forceinline__ void char_flux(const double *__restrict__ sQ, const d
     fch[l] = weno_pm<ORDER>(vp, vmn, eps, shock);
   }
   if constexpr (NS > 0) {
-#pragma unroll
+#pragma unroll 1
     for (int s = 0; s < NS; ++s) {
       double vp[NW], vmn[NW];
 #pragma unroll

@@ -1447,9 +1447,32 @@ void update_physical_properties(Zone &z, const Param &p) {
       }
 }
 
-// apply_boundary_conditions (src/BoundCond.cu:3846-3998): outflow and periodic faces
+bool flag_at(const std::vector<int> &f, int a, int na, int b, int nb) {
+  return a >= 0 && a < na && b >= 0 && b < nb && f[a + b * na] != 0;
+}
+
+// project_to_interior of apply_wall (src/BoundCond.cu:3070-3088)
+void project_to_interior(const Zone &z, int &i, int &j, int &k) {
+  if (i <= 0 && flag_at(z.il, j, z.my, k, z.mz)) i = 1;
+  else if (i >= z.mx - 1 && flag_at(z.ir, j, z.my, k, z.mz)) i = z.mx - 2;
+  if (j <= 0 && flag_at(z.jl, i, z.mx, k, z.mz)) j = 1;
+  else if (j >= z.my - 1 && flag_at(z.jr, i, z.mx, k, z.mz)) j = z.my - 2;
+  if (z.mz > 1) {
+    if (k <= 0 && flag_at(z.kl, i, z.mx, j, z.my)) k = 1;
+    else if (k >= z.mz - 1 && flag_at(z.kr, i, z.mx, j, z.my)) k = z.mz - 2;
+  }
+}
+
+double mix_r(const Zone &z, const Param &p, int i, int j, int k) {
+  if (p.n_spec == 0) return R_air;
+  double R = 0;
+  for (int l = 0; l < p.n_spec; ++l) R += z.sv(i, j, k, l) * p.mech.gas_const[l];
+  return R;
+}
+
+// apply_boundary_conditions (src/BoundCond.cu:3846-3998) in its priority order
 void apply_boundary_conditions(Zone &z, const Param &p) {
-  for (int type : {CB2_BC_OUTFLOW, CB2_BC_PERIODIC}) {
+  for (int type : {CB2_BC_OUTFLOW, CB2_BC_INFLOW, CB2_BC_SYMMETRY, CB2_BC_WALL, CB2_BC_PERIODIC}) {
     for (const auto &f : z.faces) {
       if (f.type != type) continue;
       int dir[3] = {0, 0, 0};
@@ -1464,7 +1487,77 @@ void apply_boundary_conditions(Zone &z, const Param &p) {
                 for (int l = 0; l < p.n_scalar; ++l) z.sv(gi, gj, gk, l) = z.sv(i, j, k, l);
                 cv_point(z, p, gi, gj, gk);
               }
-            } else {  // src/BoundCond.cu:3390-3440
+            } else if (type == CB2_BC_INFLOW) {  // constant supersonic state
+              for (int g = 0; g <= z.ngg; ++g) {
+                const int gi = i + g * dir[0], gj = j + g * dir[1], gk = k + g * dir[2];
+                const double st[6] = {f.rho, f.u, f.v, f.w, f.p, f.T};
+                for (int l = 0; l < 6; ++l) z.bv(gi, gj, gk, l) = st[l];
+                for (int l = 0; l < p.n_scalar; ++l) z.sv(gi, gj, gk, l) = 0.0;
+                cv_point(z, p, gi, gj, gk);
+              }
+            } else if (type == CB2_BC_SYMMETRY) {  // src/BoundCond.cu:2130-2202
+              const int in[3] = {i - dir[0], j - dir[1], k - dir[2]};
+              double kx = z.metric(i, j, k, f.face * 3), ky = z.metric(i, j, k, f.face * 3 + 1),
+                     kz = z.metric(i, j, k, f.face * 3 + 2);
+              const double km = std::sqrt(kx * kx + ky * ky + kz * kz);
+              kx /= km; ky /= km; kz /= km;
+              const double u1 = z.bv(in[0], in[1], in[2], 1), v1 = z.bv(in[0], in[1], in[2], 2),
+                           w1 = z.bv(in[0], in[1], in[2], 3);
+              double uk = kx * u1 + ky * v1 + kz * w1;
+              z.bv(i, j, k, 1) = u1 - kx * uk;
+              z.bv(i, j, k, 2) = v1 - ky * uk;
+              z.bv(i, j, k, 3) = w1 - kz * uk;
+              z.bv(i, j, k, 0) = z.bv(in[0], in[1], in[2], 0);
+              z.bv(i, j, k, 4) = z.bv(in[0], in[1], in[2], 4);
+              z.bv(i, j, k, 5) = z.bv(in[0], in[1], in[2], 5);
+              for (int l = 0; l < p.n_scalar; ++l) z.sv(i, j, k, l) = z.sv(in[0], in[1], in[2], l);
+              cv_point(z, p, i, j, k);
+              for (int g = 1; g <= z.ngg; ++g) {
+                const int gi = i + g * dir[0], gj = j + g * dir[1], gk = k + g * dir[2];
+                const int ii = i - g * dir[0], ij = j - g * dir[1], ik = k - g * dir[2];
+                z.bv(gi, gj, gk, 0) = z.bv(ii, ij, ik, 0);
+                const double u = z.bv(ii, ij, ik, 1), v = z.bv(ii, ij, ik, 2), w = z.bv(ii, ij, ik, 3);
+                uk = kx * u + ky * v + kz * w;
+                z.bv(gi, gj, gk, 1) = u - 2 * uk * kx;
+                z.bv(gi, gj, gk, 2) = v - 2 * uk * ky;
+                z.bv(gi, gj, gk, 3) = w - 2 * uk * kz;
+                z.bv(gi, gj, gk, 4) = z.bv(ii, ij, ik, 4);
+                z.bv(gi, gj, gk, 5) = z.bv(ii, ij, ik, 5);
+                for (int l = 0; l < p.n_scalar; ++l) z.sv(gi, gj, gk, l) = z.sv(ii, ij, ik, l);
+                cv_point(z, p, gi, gj, gk);
+              }
+            } else if (type == CB2_BC_WALL) {  // src/BoundCond.cu:3055-3389, non-catalytic
+              int idx[3] = {i - dir[0], j - dir[1], k - dir[2]};
+              project_to_interior(z, idx[0], idx[1], idx[2]);
+              const bool iso = f.wall_T > 0;
+              const double t_wall = iso ? f.wall_T : z.bv(idx[0], idx[1], idx[2], 5);
+              const double pw = z.bv(idx[0], idx[1], idx[2], 4);
+              for (int l = 0; l < p.n_spec; ++l) z.sv(i, j, k, l) = z.sv(idx[0], idx[1], idx[2], l);
+              double R = mix_r(z, p, i, j, k);
+              z.bv(i, j, k, 0) = pw / (t_wall * R);
+              z.bv(i, j, k, 1) = z.bv(i, j, k, 2) = z.bv(i, j, k, 3) = 0;
+              z.bv(i, j, k, 4) = pw;
+              z.bv(i, j, k, 5) = t_wall;
+              cv_point(z, p, i, j, k);
+              for (int g = 1; g <= z.ngg; ++g) {
+                int in[3] = {i - g * dir[0], j - g * dir[1], k - g * dir[2]};
+                project_to_interior(z, in[0], in[1], in[2]);
+                const int gh[3] = {i + g * dir[0], j + g * dir[1], k + g * dir[2]};
+                const double p_i = z.bv(in[0], in[1], in[2], 4), t_i = z.bv(in[0], in[1], in[2], 5);
+                double t_g = t_i;
+                if (iso) {
+                  t_g = 2 * t_wall - t_i;
+                  if (t_g <= 0.1 * t_wall) t_g = t_wall;
+                }
+                for (int l = 0; l < p.n_spec; ++l) z.sv(gh[0], gh[1], gh[2], l) = z.sv(in[0], in[1], in[2], l);
+                R = mix_r(z, p, in[0], in[1], in[2]);
+                z.bv(gh[0], gh[1], gh[2], 0) = p_i / (t_g * R);
+                for (int c = 1; c <= 3; ++c) z.bv(gh[0], gh[1], gh[2], c) = -z.bv(in[0], in[1], in[2], c);
+                z.bv(gh[0], gh[1], gh[2], 4) = p_i;
+                z.bv(gh[0], gh[1], gh[2], 5) = t_g;
+                cv_point(z, p, gh[0], gh[1], gh[2]);
+              }
+            } else {  // periodic, src/BoundCond.cu:3390-3440
               int o[3] = {i, j, k};
               const int ext[3] = {z.mx, z.my, z.mz};
               o[f.face] = f.direction < 0 ? ext[f.face] - 1 : 0;

@@ -142,3 +142,49 @@ def test_sod_to_t02_matches_oracle_and_exact(oracle_lib):
     ex = np.loadtxt(os.path.join(os.path.dirname(__file__), "golden", "sod_exact.txt"))
     x = np.arange(1000) / 999.0
     assert np.mean(np.abs(rho_g - np.interp(x, ex[:, 0], ex[:, 2]))) < 1.5e-3
+
+
+def _channel(oracle, visc=2, dims=(24, 16, 1), seed=9):
+    """2-D channel: supersonic inflow (i-), outflow (i+), isothermal wall (j-), symmetry (j+)."""
+    from cb200.field import HostBlock, array_specs, face
+    mx, my, mz = dims
+    p, hb, _ = helpers.curvilinear_air_case(mx, my, 1, scheme=abi.INV_HLLC, reconstruction=abi.REC_MUSCL,
+                                           viscous_order=visc, bc="outflow", seed=seed, jump=False)
+    p.dim = 2
+    faces = [face(abi.BC_INFLOW, 0, -1, (0, 0, 0), (0, my - 1, 0), rho=1.1, u=2.5, v=0.1, w=0.0, p=1.0,
+                  T=1.0 / (1.1 * cases.R_AIR)),
+             face(abi.BC_OUTFLOW, 0, 1, (mx - 1, 0, 0), (mx - 1, my - 1, 0)),
+             face(abi.BC_WALL, 1, -1, (0, 0, 0), (mx - 1, 0, 0), wall_temperature=0.004),
+             face(abi.BC_SYMMETRY, 1, 1, (0, my - 1, 0), (mx - 1, my - 1, 0))]
+    oracle.boundary(p, hb, faces)
+    dev = DeviceBlock(hb)
+    ctx = cb200.Context(p)
+    ctx.bind(0, dev.view(), faces)
+    return p, hb, faces, dev, ctx
+
+
+@pytest.mark.parametrize("visc", [0, 2])
+def test_wall_symmetry_inflow_boundary_parity(oracle_lib, visc):
+    p, hb, faces, dev, ctx = _channel(oracle_lib, visc)
+    rng = np.random.default_rng(2)
+    hb.a["bv"][...] *= 1 + 0.01 * rng.standard_normal(hb.a["bv"].shape)
+    dev.load(hb, ["bv"])
+    ctx.boundary(0)
+    _sync()
+    oracle_lib.boundary(p, hb, faces)
+    out = dev.to_host(["bv", "cv"])
+    assert helpers.rel_err(out["bv"], hb.a["bv"]) < 1e-15
+    assert helpers.rel_err(out["cv"], hb.a["cv"]) < 1e-15
+
+
+def test_channel_rk3_parity(oracle_lib):
+    p, hb, faces, dev, ctx = _channel(oracle_lib, 2)
+    dt = 0.2 * oracle_lib.cfl_dt(p, hb)
+    for _ in range(3):
+        ctx.rk3_step(dt, fixed_dt=True)
+        oracle_lib.rk3_step(p, [hb], [faces], dt, fixed_dt=True)
+    _sync()
+    out = dev.to_host(["cv"])
+    g = hb.ngg
+    sl = (slice(None), slice(g, -g), slice(g, -g), slice(g, -g))
+    assert helpers.rel_err(out["cv"][sl], hb.a["cv"][sl]) < 3 * TOL
