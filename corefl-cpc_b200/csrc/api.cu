@@ -257,7 +257,8 @@ int cb2_init(const cb2_param_view *pv, cb2_ctx **out) {
   if (ns != 0 && ns != 5 && ns != 9) return CB2_ERR_UNSUPPORTED;
   if (pv->n_var != 5 + ns || pv->n_scalar != ns) return CB2_ERR_UNSUPPORTED;
   const int sch = pv->inviscid_scheme;
-  const bool weno_ch = sch == CB2_INV_WENO5_CH || sch == CB2_INV_WENO7_CH;
+  const bool weno_ch = sch == CB2_INV_WENO5_CH || sch == CB2_INV_WENO7_CH || sch == CB2_INV_WENO5_CP ||
+                       sch == CB2_INV_WENO7_CP;
   const bool pvpath = sch == CB2_INV_AUSMP || sch == CB2_INV_HLLC || sch == CB2_INV_ROE || (sch == 1 && ns == 0);
   if (!weno_ch && !pvpath) return CB2_ERR_UNSUPPORTED;
   if (pvpath) {
@@ -269,7 +270,6 @@ int cb2_init(const cb2_param_view *pv, cb2_ctx **out) {
   if (pv->positive_preserving) return CB2_ERR_UNSUPPORTED;
   if (pv->reaction && ns == 0) return CB2_ERR_INVALID;
   if (pv->precision != CB2_PREC_FP64) return CB2_ERR_UNSUPPORTED;
-  if (pv->sensor_threshold > 1e-10) return CB2_ERR_UNSUPPORTED;  // shock sensor kernel not built
   cb2_ctx *ctx = new cb2_ctx;
   ctx->view = *pv;
   Param &p = ctx->p;
@@ -370,9 +370,13 @@ int cb2_bind_block(cb2_ctx *ctx, int blk, const cb2_zone_view *v, const cb2_face
   if (!ctx || !v || blk < 0 || n_faces < 0 || (n_faces > 0 && !faces)) return CB2_ERR_INVALID;
   if (v->mx < 1 || v->my < 1 || v->mz < 1 || v->ngg < 1) return CB2_ERR_INVALID;
   const Param &p = ctx->p;
-  const int need_g = (p.inviscid_scheme == CB2_INV_WENO7_CH || p.reconstruction == CB2_REC_WENO7 ||
-                      p.viscous_order == 8) ? 4
-                     : (p.inviscid_scheme == CB2_INV_WENO5_CH || p.reconstruction == CB2_REC_WENO5) ? 3 : 2;
+  const int sch = p.inviscid_scheme;
+  const bool pvpath = !(sch == CB2_INV_WENO5_CH || sch == CB2_INV_WENO7_CH || sch == CB2_INV_WENO5_CP ||
+                        sch == CB2_INV_WENO7_CP);
+  const int need_g = (sch == CB2_INV_WENO7_CH || sch == CB2_INV_WENO7_CP ||
+                      (pvpath && p.reconstruction == CB2_REC_WENO7) || p.viscous_order == 8) ? 4
+                     : (sch == CB2_INV_WENO5_CH || sch == CB2_INV_WENO5_CP ||
+                        (pvpath && p.reconstruction == CB2_REC_WENO5)) ? 3 : 2;
   if (v->ngg < need_g) return CB2_ERR_INVALID;
   if (!v->cv || !v->bv || !v->dq || !v->metric || !v->jac || !v->qn) return CB2_ERR_INVALID;
   if (p.n_spec > 0 && (!v->sv || !v->acoustic_speed || !v->gamma || !v->mul || !v->thermal_conductivity ||
@@ -381,6 +385,7 @@ int cb2_bind_block(cb2_ctx *ctx, int blk, const cb2_zone_view *v, const cb2_face
   if (p.viscous_order > 0 && !v->mul) return CB2_ERR_INVALID;
   if (p.viscous_order == 8 && (!v->fFlux || !v->gFlux || !v->hFlux)) return CB2_ERR_INVALID;
   if (p.inviscid_scheme == CB2_INV_ROE && !v->entropy_fix_delta) return CB2_ERR_INVALID;
+  if (p.sensor_threshold > 1e-10 && !v->shock_sensor) return CB2_ERR_INVALID;
   for (int f = 0; f < n_faces; ++f) {
     const auto &b = faces[f];
     if (b.face < 0 || b.face > 2 || (b.direction != 1 && b.direction != -1)) return CB2_ERR_INVALID;
@@ -476,9 +481,20 @@ int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream) {
   if (mask & CB2_RHS_INVISCID) {
     if (p.inviscid_scheme == CB2_INV_WENO5_CH || p.inviscid_scheme == CB2_INV_WENO7_CH)
       CB2_TRY(launch_inviscid_char(B->z, p, s, nl));
+    else if (p.inviscid_scheme == CB2_INV_WENO5_CP || p.inviscid_scheme == CB2_INV_WENO7_CP)
+      CB2_TRY(launch_inviscid_comp(B->z, p, s, nl));
     else
       CB2_TRY(launch_inviscid_pv(B->z, p, s, nl));
   }
+  return count(ctx, nl);
+}
+
+int cb2_shock_sensor(cb2_ctx *ctx, int blk, void *stream) {
+  Block *B = get_block(ctx, blk);
+  if (!B || !B->z.shock) return CB2_ERR_INVALID;
+  ProfGuard pg(ctx);
+  int nl = 0;
+  CB2_TRY(launch_shock_sensor(B->z, ctx->p, (cudaStream_t)stream, nl));
   return count(ctx, nl);
 }
 
@@ -552,6 +568,9 @@ int cb2_rk3_step(cb2_ctx *ctx, double *dt_inout, int fixed_dt, void *stream) {
   const int nb = (int)ctx->blocks.size();
   for (int b = 0; b < nb; ++b)
     if (ctx->blocks[b].bound) CB2_TRY(cb2_store_qn(ctx, b, stream));
+  if (ctx->p.sensor_threshold > 1e-10)  // hybrid linear/WENO weights (src/RK.cuh:139-143)
+    for (int b = 0; b < nb; ++b)
+      if (ctx->blocks[b].bound) CB2_TRY(cb2_shock_sensor(ctx, b, stream));
   double dt = *dt_inout;
   if (!fixed_dt) {
     CB2_TRY(cb2_cfl_dt(ctx, &dt, stream));

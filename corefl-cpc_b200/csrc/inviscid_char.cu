@@ -300,6 +300,181 @@ __global__ void __launch_bounds__(kSweepThreads) k_weno_char(Zone z, Param p, id
   }
 }
 
+// ---- component-wise WENO (inviscid_scheme 51/71, src/WENO.cu:890-1089) ---------------------
+// Each node is split with its own LLF speed lambda0 = |U_k| + c|grad k|:
+//   F+- = 0.5 J ((U_k +- lambda0) Q + p (0, k_x, k_y, k_z, U_k)),
+// and every conservative component is reconstructed on its own, with eps scaled by v_ref^2
+// for momentum and v_ref^4 for energy.
+template <int NS, int DIR>
+__device__ __forceinline__ void load_node_split(const Zone &z, idx_t g, double *sP, double *sM, int NN, int slot) {
+  constexpr int NV = 5 + NS;
+  const idx_t sz = z.L.sz;
+  const double q0 = z.cv[g], q1 = z.cv[g + sz], q2 = z.cv[g + 2 * sz], q3 = z.cv[g + 3 * sz], q4 = z.cv[g + 4 * sz];
+  const double m0 = z.metric[g + (3 * DIR) * sz], m1 = z.metric[g + (3 * DIR + 1) * sz],
+               m2 = z.metric[g + (3 * DIR + 2) * sz];
+  double pk = z.bv[g + 4 * sz];
+  const double Uk = (q1 * m0 + q2 * m1 + q3 * m2) / q0;
+  double cg = norm3d(m0, m1, m2);
+  if constexpr (NS == 0) cg *= sqrt(kGammaAir * kRAir * z.bv[g + 5 * sz]);
+  else cg *= z.acoustic[g];
+  const double lambda0 = fabs(Uk) + cg;
+  const double hj = 0.5 * z.jac[g];
+  const double sp = hj * (Uk + lambda0), sm = hj * (Uk - lambda0);
+  pk *= hj;
+  sP[0 * NN + slot] = sp * q0;
+  sP[1 * NN + slot] = fma(sp, q1, pk * m0);
+  sP[2 * NN + slot] = fma(sp, q2, pk * m1);
+  sP[3 * NN + slot] = fma(sp, q3, pk * m2);
+  sP[4 * NN + slot] = fma(sp, q4, pk * Uk);
+  sM[0 * NN + slot] = sm * q0;
+  sM[1 * NN + slot] = fma(sm, q1, pk * m0);
+  sM[2 * NN + slot] = fma(sm, q2, pk * m1);
+  sM[3 * NN + slot] = fma(sm, q3, pk * m2);
+  sM[4 * NN + slot] = fma(sm, q4, pk * Uk);
+#pragma unroll
+  for (int v = 5; v < NV; ++v) {
+    const double ql = z.cv[g + v * sz];
+    sP[v * NN + slot] = sp * ql;
+    sM[v * NN + slot] = sm * ql;
+  }
+}
+
+template <int NS, int DIR, int ORDER>
+__global__ void __launch_bounds__(kSweepThreads) k_weno_comp(Zone z, Param p, idx_t run) {
+  constexpr int NV = 5 + NS;
+  constexpr int R = ORDER / 2 + 1;
+  constexpr int NW = 2 * R - 1;
+  constexpr int NN = DIR == 0 ? (kSweepThreads + 2 * R - 1) : kTI * (kTS + 2 * R - 1);
+  extern __shared__ double smem[];
+  double *sP = smem;
+  double *sM = sP + NV * NN;
+  double *sFl = sM + NV * NN;
+  const int tid = threadIdx.x;
+  const int g = z.ngg;
+  const Layout &L = z.L;
+  int i, j, k;
+  bool valid_if;
+  int c, st;
+  if constexpr (DIR == 0) {
+    k = blockIdx.z;
+    const idx_t q0 = (idx_t)blockIdx.x * (kSweepThreads - 1) - 1;
+    const idx_t base = (idx_t)k * L.disp1 + L.dispt - g;
+    const idx_t qlo = q0 - R + 1;
+    const idx_t qmin = -(idx_t)g * L.disp2, qmax = (idx_t)(L.my + g) * L.disp2;
+    for (int s = tid; s < NN; s += kSweepThreads) {
+      const idx_t q = qlo + s;
+      if (q >= qmin && q < qmax) load_node_split<NS, 0>(z, base + q, sP, sM, NN, s);
+    }
+    const idx_t q = q0 + tid;
+    const idx_t jj = q >= 0 ? q / L.disp2 : -1;
+    i = (int)(q - jj * L.disp2) - g;
+    j = (int)jj;
+    valid_if = q >= 0 && q < run && i >= -1 && i <= L.mx - 1;
+    c = tid + R - 1;
+    st = 1;
+  } else {
+    const int ti = tid % kTI, ts = tid / kTI;
+    i = blockIdx.x * kTI + ti;
+    const int s0 = blockIdx.y * (kTS - 1);
+    const int ms = DIR == 1 ? L.my : L.mz;
+    if (DIR == 1) k = blockIdx.z; else j = blockIdx.z;
+    for (int s = ts; s < kTS + 2 * R - 1; s += kTS) {
+      const int n = s0 - R + s;
+      if (i < L.mx && n < ms + g) {
+        const idx_t gi = DIR == 1 ? L.at(i, n, k) : L.at(i, j, n);
+        load_node_split<NS, DIR>(z, gi, sP, sM, NN, s * kTI + ti);
+      }
+    }
+    const int n_if = s0 - 1 + ts;
+    if (DIR == 1) j = n_if; else k = n_if;
+    valid_if = i < L.mx && n_if <= ms - 1;
+    c = (ts + R - 1) * kTI + ti;
+    st = kTI;
+  }
+  __syncthreads();
+  if (valid_if) {
+    bool shock = true;
+    if (p.sensor_threshold > 1e-10) {
+      shock = false;
+      for (int d = -g + 1; d <= g; ++d) {
+        const idx_t gs = DIR == 0 ? L.at(i + d, j, k) : (DIR == 1 ? L.at(i, j + d, k) : L.at(i, j, k + d));
+        if (z.shock[gs] > p.sensor_threshold) { shock = true; break; }
+      }
+    }
+    const double e0 = kWenoEps * p.weno_eps_scale;
+    const double e1 = e0 * p.v_ref * p.v_ref, e2 = e1 * p.v_ref * p.v_ref;
+#pragma unroll 1
+    for (int l = 0; l < NV; ++l) {
+      const double eps = (l >= 1 && l <= 3) ? e1 : (l == 4 ? e2 : e0);
+      double vp[NW], vm[NW];
+#pragma unroll
+      for (int m = 0; m < NW; ++m) {
+        vp[m] = sP[l * NN + c + (m - R + 1) * st];
+        vm[m] = sM[l * NN + c + (m - R + 2) * st];
+      }
+      sFl[l * kSweepThreads + tid] = weno_pm<ORDER>(vp, vm, eps, shock);
+    }
+  }
+  __syncthreads();
+  bool valid_node;
+  if constexpr (DIR == 0) valid_node = tid >= 1 && valid_if && i >= 0;
+  else valid_node = (tid / kTI) >= 1 && valid_if && (DIR == 1 ? j >= 0 : k >= 0);
+  if (valid_node) {
+    const int tprev = DIR == 0 ? tid - 1 : tid - kTI;
+    const idx_t gd = z.L0.at(i, j, k);
+    const idx_t sz0 = z.L0.sz;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) z.dq[gd + v * sz0] -= sFl[v * kSweepThreads + tid] - sFl[v * kSweepThreads + tprev];
+  }
+}
+
+template <int NS, int ORDER>
+static int launch_comp_dir(int dir, const Zone &z, const Param &p, cudaStream_t s) {
+  constexpr int NV = 5 + NS;
+  constexpr int R = ORDER / 2 + 1;
+  SweepGeom geo;
+  const dim3 grid = sweep_grid(dir, z.L, geo);
+  const size_t smem = sizeof(double) * ((size_t)2 * NV * sweep_nodes(dir, R) + (size_t)NV * kSweepThreads);
+  if (grid.x == 0 || grid.y == 0 || grid.z == 0) return CB2_OK;
+  static const char *names[3] = {"weno_comp_x", "weno_comp_y", "weno_comp_z"};
+  ProfScope prof(names[dir], s);
+  if (dir == 0) {
+    auto kern = k_weno_comp<NS, 0, ORDER>;
+    CB2_TRY(prepare_smem(kern, smem));
+    kern<<<grid, kSweepThreads, smem, s>>>(z, p, geo.run);
+  } else if (dir == 1) {
+    auto kern = k_weno_comp<NS, 1, ORDER>;
+    CB2_TRY(prepare_smem(kern, smem));
+    kern<<<grid, kSweepThreads, smem, s>>>(z, p, 0);
+  } else {
+    auto kern = k_weno_comp<NS, 2, ORDER>;
+    CB2_TRY(prepare_smem(kern, smem));
+    kern<<<grid, kSweepThreads, smem, s>>>(z, p, 0);
+  }
+  return check_launch();
+}
+
+template <int NS>
+static int launch_comp_ns(const Zone &z, const Param &p, int order, cudaStream_t s, int &n_launch) {
+  const int ndir = z.mz > 1 ? 3 : 2;
+  for (int d = 0; d < ndir; ++d) {
+    int rc = order == 5 ? launch_comp_dir<NS, 5>(d, z, p, s) : launch_comp_dir<NS, 7>(d, z, p, s);
+    if (rc) return rc;
+    ++n_launch;
+  }
+  return CB2_OK;
+}
+
+int launch_inviscid_comp(const Zone &z, const Param &p, cudaStream_t s, int &n_launch) {
+  const int order = (p.inviscid_scheme == CB2_INV_WENO5_CP) ? 5 : 7;
+  switch (p.n_spec) {
+    case 0: return launch_comp_ns<0>(z, p, order, s, n_launch);
+    case 5: return launch_comp_ns<5>(z, p, order, s, n_launch);
+    case 9: return launch_comp_ns<9>(z, p, order, s, n_launch);
+    default: return CB2_ERR_UNSUPPORTED;
+  }
+}
+
 template <int NS, int ORDER>
 static int launch_dir(int dir, const Zone &z, const Param &p, cudaStream_t s) {
   constexpr int NV = 5 + NS;

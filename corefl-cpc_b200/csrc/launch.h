@@ -66,6 +66,7 @@ struct FaceBC {
 
 // ---- launchers (each returns CB2_OK or an error code; n_launch counts kernels) ----------
 int launch_inviscid_char(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
+int launch_inviscid_comp(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
 int launch_inviscid_pv(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
 int launch_stage_update(const Zone &z, const Param &p, double dt, int rk, cudaStream_t s, int &n_launch);
 int launch_cv_from_bv(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
@@ -77,6 +78,7 @@ int launch_periodic_flux_exchange(const Zone &z, const Param &p, const FaceBC *f
                                   int &n_launch);
 int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, cudaStream_t s, int &n_launch);
 int launch_chemistry(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
+int launch_shock_sensor(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
 int launch_local_dt(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
 int launch_min_reduce(const double *src, long long n, double *partial, int n_partial, double *out,
                       cudaStream_t s, int &n_launch);

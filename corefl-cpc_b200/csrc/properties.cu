@@ -198,3 +198,64 @@ int launch_min_reduce(const double *src, long long n, double *partial, int n_par
 }
 
 }  // namespace cb2
+
+namespace cb2 {
+
+// ---- shock sensor (compute_shock_sensor, src/FieldOperation.cu:123-228) -------------------
+// Computed on interior nodes once per step; the ghost values are never written (the
+// reference's RK3 loop never exchanges them either), so the caller's zero fill stands there.
+__global__ void __launch_bounds__(kPropThreads) k_shock_sensor(Zone z, Param p) {
+  const int i = blockIdx.x * kPropThreads + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  if (i >= z.mx) return;
+  const Layout &L = z.L;
+  const idx_t sz = L.sz, g = L.at(i, j, k);
+  const idx_t st[3] = {1, L.disp2, L.disp1};
+  const double *bv = z.bv;
+  double sensor = 1;
+  if (p.shock_sensor == 1) {  // modified Jameson (src/FieldOperation.cu:172-185)
+    const double *pp = bv + 4 * sz + g;
+    const double twoP = pp[0] * 2;
+    double s = 0;
+    for (int a = 0; a < 3; ++a) {
+      const double pn = pp[st[a]] + pp[-st[a]];
+      s += fabs(pn - twoP) / (pn + twoP);
+    }
+    sensor = s;
+  } else if (p.shock_sensor == 2) {  // density / pressure jump (src/FieldOperation.cu:187-205)
+    const double rho = bv[g], rhoI = 1.0 / rho, pr = bv[g + 4 * sz], pI = 1.0 / pr;
+    double s = 0;
+    for (int a = 0; a < 3; ++a) s = fmax(s, fabs(bv[g + st[a]] - rho) * rhoI);
+    for (int a = 0; a < 3; ++a) s = fmax(s, fabs(bv[g + 4 * sz + st[a]] - pr) * pI);
+    sensor = s;
+  } else {  // modified Ducros (src/FieldOperation.cu:123-170)
+    constexpr double c12 = 1.0 / 12.0, c23 = 2.0 / 3.0;
+    double d[3][3];  // d[var u,v,w][dir]
+    for (int c = 0; c < 3; ++c) {
+      const double *f = bv + (1 + c) * sz + g;
+      for (int a = 0; a < 3; ++a)
+        d[c][a] = c12 * f[-2 * st[a]] - c23 * f[-st[a]] + c23 * f[st[a]] - c12 * f[2 * st[a]];
+    }
+    const double *M = z.metric + g;
+    auto cart = [&](int c, int x) { return d[c][0] * M[x * sz] + d[c][1] * M[(3 + x) * sz] + d[c][2] * M[(6 + x) * sz]; };
+    double div = cart(0, 0) + cart(1, 1) + cart(2, 2);
+    if (div > 0) sensor = 0;
+    else {
+      const double duDy = cart(0, 1), duDz = cart(0, 2), dvDx = cart(1, 0), dvDz = cart(1, 2);
+      const double dwDx = cart(2, 0), dwDy = cart(2, 1);
+      div *= div;
+      const double curl2 = (dwDy - dvDz) * (dwDy - dvDz) + (duDz - dwDx) * (duDz - dwDx) + (dvDx - duDy) * (dvDx - duDy);
+      sensor = div / (div + curl2 + p.sensor_eps);
+    }
+  }
+  z.shock[g] = sensor;
+}
+
+int launch_shock_sensor(const Zone &z, const Param &p, cudaStream_t s, int &n_launch) {
+  dim3 grid((z.mx + kPropThreads - 1) / kPropThreads, z.my, z.mz);
+  ProfScope prof("shock_sensor", s);
+  k_shock_sensor<<<grid, kPropThreads, 0, s>>>(z, p);
+  ++n_launch;
+  return check_launch();
+}
+
+}  // namespace cb2

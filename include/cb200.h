@@ -191,6 +191,12 @@ int cb2_store_qn(cb2_ctx *ctx, int blk, void *stream);
  * src/RK.cuh:186) residual contributions selected by `mask` (CB2_RHS_*). */
 int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream);
 
+/* Shock sensor (Ducros / Jameson / density-pressure jump by `shock_sensor`) on the interior
+ * nodes: replaces compute_shock_sensor (src/FieldOperation.cu:207-228, src/RK.cuh:139-143).
+ * With sensor_threshold > 1e-10 the WENO kernels use nonlinear weights only where the
+ * sensor exceeds the threshold within the stencil window, and linear weights elsewhere. */
+int cb2_shock_sensor(cb2_ctx *ctx, int blk, void *stream);
+
 /* Shu-Osher stage `rk` (0,1,2) with time step dt, species clipping and primitive recovery:
  * replaces update_cv_and_bv_rk<mix> (src/RK.cuh:277-367). */
 int cb2_stage_update(cb2_ctx *ctx, int blk, double dt, int rk, void *stream);

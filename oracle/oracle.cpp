@@ -351,6 +351,81 @@ void convective_term_weno_char(Zone &z, const Param &p, int dir) {
       }
 }
 
+// Component-wise WENO with node-wise LLF splitting (inviscid_scheme 51/71,
+// src/WENO.cu:890-1089 and the y/z twins)
+void convective_term_weno_comp(Zone &z, const Param &p, int dir) {
+  const int order = (p.inviscid_scheme == 51) ? 5 : 7;
+  const int r = order == 5 ? 3 : 4;
+  const int ext[3] = {z.mx, z.my, z.mz};
+  const double eps_ref = eps_weno * p.weno_eps_scale;
+  const double eps_scaled[3] = {eps_ref, eps_ref * p.v_ref * p.v_ref, eps_ref * p.v_ref * p.v_ref * p.v_ref * p.v_ref};
+  std::vector<double> own((size_t)z.cv.sz * p.n_var, 0.0);
+  Arr F_out(own.data(), z.mx, z.my, z.mz, z.ngg);
+  int lo[3] = {0, 0, 0}, hi[3] = {z.mx, z.my, z.mz};
+  lo[dir] = -1;
+  hi[dir] = ext[dir];
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int k = lo[2]; k < hi[2]; ++k)
+    for (int j = lo[1]; j < hi[1]; ++j)
+      for (int i = lo[0]; i < hi[0]; ++i) {
+        double fp[16][8], fm[16][8];
+        for (int m = 0; m < 2 * r; ++m) {
+          int a = i, b = j, c = k;
+          shift(dir, m - r + 1, a, b, c);
+          const double q0 = z.cv(a, b, c, 0), q1 = z.cv(a, b, c, 1), q2 = z.cv(a, b, c, 2), q3 = z.cv(a, b, c, 3),
+                       q4 = z.cv(a, b, c, 4);
+          double pk = z.bv(a, b, c, 4);
+          const double m0 = z.metric(a, b, c, 3 * dir), m1 = z.metric(a, b, c, 3 * dir + 1),
+                       m2 = z.metric(a, b, c, 3 * dir + 2);
+          const double Uk = (q1 * m0 + q2 * m1 + q3 * m2) / q0;
+          double cg = std::sqrt(m0 * m0 + m1 * m1 + m2 * m2);
+          if (p.n_spec == 0) cg *= std::sqrt(gamma_air * R_air * z.bv(a, b, c, 5));
+          else cg *= z.acoustic(a, b, c);
+          const double lambda0 = std::fabs(Uk) + cg;
+          const double jac = z.jac(a, b, c);
+          const double sPlus = 0.5 * jac * (Uk + lambda0), sMinus = 0.5 * jac * (Uk - lambda0);
+          pk *= 0.5 * jac;
+          fp[0][m] = sPlus * q0;
+          fp[1][m] = sPlus * q1 + pk * m0;
+          fp[2][m] = sPlus * q2 + pk * m1;
+          fp[3][m] = sPlus * q3 + pk * m2;
+          fp[4][m] = sPlus * q4 + pk * Uk;
+          fm[0][m] = sMinus * q0;
+          fm[1][m] = sMinus * q1 + pk * m0;
+          fm[2][m] = sMinus * q2 + pk * m1;
+          fm[3][m] = sMinus * q3 + pk * m2;
+          fm[4][m] = sMinus * q4 + pk * Uk;
+          for (int l = 5; l < p.n_var; ++l) {
+            const double ql = z.cv(a, b, c, l);
+            fp[l][m] = sPlus * ql;
+            fm[l][m] = sMinus * ql;
+          }
+        }
+        bool shock = true;
+        if (p.sensor_threshold > 1e-10) {
+          shock = false;
+          for (int d = -z.ngg + 1; d <= z.ngg; ++d) {
+            int a = i, b = j, c = k;
+            shift(dir, d, a, b, c);
+            if (z.shock(a, b, c) > p.sensor_threshold) { shock = true; break; }
+          }
+        }
+        for (int l = 0; l < p.n_var; ++l) {
+          const double eps = (l >= 1 && l <= 3) ? eps_scaled[1] : (l == 4 ? eps_scaled[2] : eps_scaled[0]);
+          F_out(i, j, k, l) =
+              order == 5 ? WENO5(&fp[l][0], &fm[l][1], eps, shock) : WENO7(&fp[l][0], &fm[l][1], eps, shock);
+        }
+      }
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int k = 0; k < z.mz; ++k)
+    for (int j = 0; j < z.my; ++j)
+      for (int i = 0; i < z.mx; ++i) {
+        int a = i, b = j, c = k;
+        shift(dir, -1, a, b, c);
+        for (int l = 0; l < p.n_var; ++l) z.dq(i, j, k, l) -= F_out(i, j, k, l) - F_out(a, b, c, l);
+      }
+}
+
 // ---------------------------------------------------------------------------------------
 // Primitive reconstruction + Riemann solvers (src/InviscidScheme.cu:28-786,
 // src/Reconstruction.cu, src/Limiter.cuh)
@@ -1392,9 +1467,11 @@ void compute_cv_from_bv(Zone &z, const Param &p) {
 void compute_inviscid_flux(Zone &z, const Param &p) {
   const int ndir = z.mz > 1 ? 3 : 2;
   const bool ch = p.inviscid_scheme == 52 || p.inviscid_scheme == 72;
-  if (!ch && p.inviscid_scheme == 2) entropy_fix_delta(z, p);
+  const bool cp = p.inviscid_scheme == 51 || p.inviscid_scheme == 71;
+  if (!ch && !cp && p.inviscid_scheme == 2) entropy_fix_delta(z, p);
   for (int d = 0; d < ndir; ++d) {
     if (ch) convective_term_weno_char(z, p, d);
+    else if (cp) convective_term_weno_comp(z, p, d);
     else convective_term_pv(z, p, d);
   }
 }
@@ -1646,12 +1723,69 @@ double local_time_step_min(Zone &z, const Param &p) {
   return dt_min;
 }
 
+// compute_shock_sensor (src/FieldOperation.cu:123-228) on interior nodes
+void compute_shock_sensor(Zone &z, const Param &p) {
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int k = 0; k < z.mz; ++k)
+    for (int j = 0; j < z.my; ++j)
+      for (int i = 0; i < z.mx; ++i) {
+        const Arr &bv = z.bv;
+        double sensor = 1;
+        if (p.shock_sensor == 1) {
+          const double twoP = bv(i, j, k, 4) * 2;
+          const double pI = bv(i + 1, j, k, 4) + bv(i - 1, j, k, 4);
+          const double pJ = bv(i, j + 1, k, 4) + bv(i, j - 1, k, 4);
+          const double pK = bv(i, j, k + 1, 4) + bv(i, j, k - 1, 4);
+          sensor = std::fabs(pI - twoP) / (pI + twoP) + std::fabs(pJ - twoP) / (pJ + twoP) +
+                   std::fabs(pK - twoP) / (pK + twoP);
+        } else if (p.shock_sensor == 2) {
+          const double rho = bv(i, j, k, 0), rhoI = 1.0 / rho, pr = bv(i, j, k, 4), pI = 1.0 / pr;
+          double s = 0;
+          s = std::max(s, std::fabs(bv(i + 1, j, k, 0) - rho) * rhoI);
+          s = std::max(s, std::fabs(bv(i, j + 1, k, 0) - rho) * rhoI);
+          s = std::max(s, std::fabs(bv(i, j, k + 1, 0) - rho) * rhoI);
+          s = std::max(s, std::fabs(bv(i + 1, j, k, 4) - pr) * pI);
+          s = std::max(s, std::fabs(bv(i, j + 1, k, 4) - pr) * pI);
+          s = std::max(s, std::fabs(bv(i, j, k + 1, 4) - pr) * pI);
+          sensor = s;
+        } else {
+          const double c12 = 1.0 / 12.0, c23 = 2.0 / 3.0;
+          double d[3][3];
+          for (int c = 0; c < 3; ++c) {
+            d[c][0] = c12 * bv(i - 2, j, k, 1 + c) - c23 * bv(i - 1, j, k, 1 + c) + c23 * bv(i + 1, j, k, 1 + c) -
+                      c12 * bv(i + 2, j, k, 1 + c);
+            d[c][1] = c12 * bv(i, j - 2, k, 1 + c) - c23 * bv(i, j - 1, k, 1 + c) + c23 * bv(i, j + 1, k, 1 + c) -
+                      c12 * bv(i, j + 2, k, 1 + c);
+            d[c][2] = c12 * bv(i, j, k - 2, 1 + c) - c23 * bv(i, j, k - 1, 1 + c) + c23 * bv(i, j, k + 1, 1 + c) -
+                      c12 * bv(i, j, k + 2, 1 + c);
+          }
+          auto cart = [&](int c, int x) {
+            return d[c][0] * z.metric(i, j, k, x) + d[c][1] * z.metric(i, j, k, 3 + x) +
+                   d[c][2] * z.metric(i, j, k, 6 + x);
+          };
+          double div = cart(0, 0) + cart(1, 1) + cart(2, 2);
+          if (div > 0) sensor = 0;
+          else {
+            const double duDy = cart(0, 1), duDz = cart(0, 2), dvDx = cart(1, 0), dvDz = cart(1, 2);
+            const double dwDx = cart(2, 0), dwDy = cart(2, 1);
+            div *= div;
+            const double curl2 =
+                (dwDy - dvDz) * (dwDy - dvDz) + (duDz - dwDx) * (duDz - dwDx) + (dvDx - duDy) * (dvDx - duDy);
+            sensor = div / (div + curl2 + p.sensor_eps);
+          }
+        }
+        z.shock(i, j, k) = sensor;
+      }
+}
+
 // One SSP-RK3 step over all zones (src/RK.cuh:107-237, single process, no MPI)
 void rk3_step(std::vector<Zone> &zones, const Param &p, double &dt, bool fixed_dt) {
   for (auto &z : zones) {
     const size_t n = (size_t)z.cv.sz * p.n_var;
     std::memcpy(z.qn.p, z.cv.p, n * sizeof(double));
   }
+  if (p.sensor_threshold > 1e-10)
+    for (auto &z : zones) compute_shock_sensor(z, p);
   if (!fixed_dt) {
     double m = 1e+6;
     for (auto &z : zones) m = std::min(m, local_time_step_min(z, p));

@@ -85,6 +85,7 @@ void compute_viscous_flux(Zone &z, const Param &p);
 void compute_chemistry(Zone &z, const Param &p);
 void chemistry_source(const Mechanism &m, double rho, double t, const double *y, double *omega, double *omega_d);
 void update_physical_properties(Zone &z, const Param &p);
+void compute_shock_sensor(Zone &z, const Param &p);
 void apply_boundary_conditions(Zone &z, const Param &p);
 double local_time_step_min(Zone &z, const Param &p);
 void rk3_step(std::vector<Zone> &zones, const Param &p, double &dt, bool fixed_dt);

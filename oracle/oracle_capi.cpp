@@ -61,6 +61,13 @@ int oracle_boundary(const cb2_param_view *pv, const cb2_zone_view *zv, const cb2
   return 0;
 }
 
+int oracle_shock_sensor(const cb2_param_view *pv, const cb2_zone_view *zv) {
+  Param p = make_param(*pv);
+  Zone z = make_zone(*zv, nullptr, 0, p);
+  compute_shock_sensor(z, p);
+  return 0;
+}
+
 int oracle_properties(const cb2_param_view *pv, const cb2_zone_view *zv) {
   Param p = make_param(*pv);
   Zone z = make_zone(*zv, nullptr, 0, p);

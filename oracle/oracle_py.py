@@ -34,6 +34,7 @@ def load():
             "oracle_rhs": (C.c_int, [P(abi.ParamView), P(abi.ZoneView), P(abi.FaceBC), C.c_int, C.c_uint]),
             "oracle_boundary": (C.c_int, [P(abi.ParamView), P(abi.ZoneView), P(abi.FaceBC), C.c_int]),
             "oracle_properties": (C.c_int, [P(abi.ParamView), P(abi.ZoneView)]),
+            "oracle_shock_sensor": (C.c_int, [P(abi.ParamView), P(abi.ZoneView)]),
             "oracle_cfl_dt": (C.c_int, [P(abi.ParamView), P(abi.ZoneView), P(C.c_double)]),
             "oracle_rk3_step": (C.c_int, [P(abi.ParamView), P(abi.ZoneView), P(abi.FaceBC), P(C.c_int), C.c_int,
                                           P(C.c_double), C.c_int]),
@@ -75,6 +76,11 @@ def stage_update(param, block, dt, rk):
 def boundary(param, block, faces):
     v = block.view()
     load().oracle_boundary(C.byref(param), C.byref(v), _faces(faces), len(faces))
+
+
+def shock_sensor(param, block):
+    v = block.view()
+    load().oracle_shock_sensor(C.byref(param), C.byref(v))
 
 
 def properties(param, block):

@@ -21,12 +21,14 @@ def rel_err(a, b, axis_comp=True):
 
 
 def curvilinear_air_case(mx=20, my=18, mz=16, ngg=4, scheme=abi.INV_WENO5_CH, reconstruction=abi.REC_MUSCL,
-                         viscous_order=0, bc="periodic", seed=0, jump=True, mu=None):
+                         viscous_order=0, bc="periodic", seed=0, jump=True, mu=None, sensor=None):
     """A small 3-D air block on the perturbed sine-wave map (non-uniform metrics), with a
-    smooth random state, an optional density/pressure jump and periodic or outflow faces."""
+    smooth random state, an optional density/pressure jump and periodic or outflow faces.
+    sensor = (kind, threshold, eps) switches on the hybrid linear/WENO weights."""
     rng = np.random.default_rng(seed)
     n = max(mx, my, mz) - 1
-    specs = array_specs(mx, my, mz, ngg, 5, 0, viscous_order=viscous_order, roe=(scheme == abi.INV_ROE))
+    specs = array_specs(mx, my, mz, ngg, 5, 0, viscous_order=viscous_order, roe=(scheme == abi.INV_ROE),
+                        hybrid=sensor is not None)
     b = HostBlock(mx, my, mz, ngg, specs)
     (x, y, z), metric, det = cases.sine_wave_metrics(n, ngg, 0.05)
     sl = (slice(0, mz + 2 * ngg), slice(0, my + 2 * ngg), slice(0, mx + 2 * ngg))
@@ -55,4 +57,6 @@ def curvilinear_air_case(mx=20, my=18, mz=16, ngg=4, scheme=abi.INV_WENO5_CH, re
     param = cases.make_param(dim=3, inviscid_scheme=scheme, reconstruction=reconstruction,
                              viscous_order=viscous_order, cfl=0.5, rho_ref=1.0, v_ref=1.0,
                              mu_constant=(mu if mu is not None else 1e-3) if viscous_order else 0.0)
+    if sensor is not None:
+        param.shock_sensor, param.sensor_threshold, param.sensor_eps = sensor
     return param, b, faces

@@ -51,7 +51,8 @@ def test_sod_against_reference_exact_solution(oracle_lib):
 
 
 @pytest.mark.parametrize("scheme,rec", [(abi.INV_WENO7_CH, abi.REC_MUSCL), (abi.INV_AUSMP, abi.REC_MUSCL),
-                                        (abi.INV_HLLC, abi.REC_WENO5), (abi.INV_ROE, abi.REC_MUSCL)])
+                                        (abi.INV_HLLC, abi.REC_WENO5), (abi.INV_ROE, abi.REC_MUSCL),
+                                        (abi.INV_WENO5_CP, abi.REC_MUSCL), (abi.INV_WENO7_CP, abi.REC_MUSCL)])
 def test_sod_other_schemes_converge(oracle_lib, scheme, rec):
     ex = np.loadtxt(os.path.join(GOLDEN, "sod_exact.txt"))
     case = cases.sod(mx=400, scheme=scheme, reconstruction=rec)
