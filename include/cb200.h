@@ -218,6 +218,21 @@ int cb2_cv_from_bv(cb2_ctx *ctx, int blk, void *stream);
  * src/TimeAdvanceFunc.cu:114-139).  Synchronises `stream`. */
 int cb2_cfl_dt(cb2_ctx *ctx, double *dt_out, void *stream);
 
+/* Allocation-free minimum of a per-node time-step array (no counterpart in the reference).
+ * For callers that may not allocate device memory, e.g. codes that give all device memory
+ * to their own pool before the solve, or that cannot afford the device-wide synchronisation
+ * of cudaFree while other streams run.  `dt_local` (device, n doubles, e.g. the dt_local
+ * array local_time_step fills) is reduced to its minimum, seeded with 1e6 as the reference
+ * does, and the result is written to the device double *dt_min.  Nothing is allocated: the
+ * partial minima use a fixed device array of CB2_NOALLOC_MAX_PARTIALS doubles (128 KiB) that
+ * every GPU loading the library holds until the process exits, so n may not exceed
+ * CB2_NOALLOC_MAX_NODES (CB2_ERR_INVALID beyond).  The first call on a device resolves that
+ * array's device address, so make it before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU race. */
+#define CB2_NOALLOC_MAX_PARTIALS 16384
+#define CB2_NOALLOC_MAX_NODES (16384LL * 2048LL)
+int cb2_min_dt_noalloc(const double *dt_local, long long n, double *dt_min, void *stream);
+
 /* One whole SSP-RK3 step over all bound blocks (src/RK.cuh:107-237): qn<-cv, [CFL dt],
  * 3 x (rhs, stage update, boundary, properties).  With fixed_dt != 0 the step uses
  * *dt_inout and performs no host synchronisation; otherwise the CFL dt is computed first
