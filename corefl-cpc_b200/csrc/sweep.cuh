@@ -32,6 +32,32 @@ __host__ __device__ __forceinline__ int sweep_nodes(int dir, int r) {
   return dir == 0 ? (kSweepThreads + 2 * r - 1) : kTI * (kTS + 2 * r - 1);
 }
 
+// Node-centred tiling: a CTA of kSweepThreads threads owns kSweepThreads consecutive nodes
+// along the sweep; each thread reconstructs both faces of its node, the interfaces between
+// neighbouring threads are formed from shared memory, and the kSweepThreads-2 inner nodes are
+// updated (CTAs overlap by two nodes).  x sweep: one contiguous padded run as above.  y/z
+// sweep: kNI consecutive i x kNS nodes along the sweep.
+constexpr int kNI = 8;
+constexpr int kNS = kSweepThreads / kNI;
+
+__host__ __device__ __forceinline__ int node_sweep_nodes(int dir, int r) {
+  return dir == 0 ? (kSweepThreads + 2 * r) : kNI * (kNS + 2 * r);
+}
+
+inline dim3 node_sweep_grid(int dir, const Layout &L, SweepGeom &g) {
+  g.dir = dir;
+  if (dir == 0) {
+    g.run = (idx_t)L.my * L.disp2;
+    const idx_t per = kSweepThreads - 2;
+    return dim3((unsigned)((g.run + per - 1) / per), 1, (unsigned)L.mz);
+  }
+  g.n_itile = (L.mx + kNI - 1) / kNI;
+  const int ms = dir == 1 ? L.my : L.mz;
+  g.n_stile = (ms + kNS - 3) / (kNS - 2);
+  const int other = dir == 1 ? L.mz : L.my;
+  return dim3((unsigned)g.n_itile, (unsigned)g.n_stile, (unsigned)other);
+}
+
 inline dim3 sweep_grid(int dir, const Layout &L, SweepGeom &g) {
   g.dir = dir;
   if (dir == 0) {

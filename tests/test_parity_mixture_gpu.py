@@ -109,7 +109,7 @@ def test_rhs_parity_mixture(oracle_lib, h2, name, scheme, rec, visc, chem):
 
 
 def test_reacting_box_rk3_parity(oracle_lib, h2):
-    """Config 3 in miniature: WENO5 + HLLC, 2nd-order viscous, chemistry, 3 RK3 steps at 2e-9 s."""
+    """Reacting H2-air box in miniature: WENO5 + HLLC, 2nd-order viscous, chemistry, 3 RK3 steps at 2e-9 s."""
     p, hb, faces, dev, ctx = _box(oracle_lib, h2, scheme=abi.INV_HLLC, rec=abi.REC_WENO5, visc=2, reaction=True)
     for _ in range(3):
         ctx.rk3_step(2e-9, fixed_dt=True)
