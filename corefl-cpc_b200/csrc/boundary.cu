@@ -297,6 +297,125 @@ static inline long long face_points(const FaceBC &f) {
   return (long long)(f.end[0] - f.start[0] + 1) * (f.end[1] - f.start[1] + 1) * (f.end[2] - f.start[2] + 1);
 }
 
+// ---- both periodic faces of one direction in one launch -----------------------------------
+// Work item p of a face line: p = 0 averages the two coincident end nodes, p in [1, g] fills
+// left ghost -p from node m-1-p, p in [g+1, 2g] fills right ghost m-1+(p-g) from node p-g.
+// Applying the two faces one after the other gives exactly this when no copy source is an end
+// node (m >= g + 2) and both faces span the same tangential range; the launcher checks both.
+// Items are ordered so that consecutive threads touch consecutive addresses: along x the item
+// index runs fastest, along y/z the i index does.
+struct PairItem {
+  int p, i, j, k;  // i, j, k of the left face node
+};
+
+__device__ __forceinline__ bool pair_item(const FaceBC &f, int g, PairItem &it) {
+  const int P = 2 * g + 1;
+  const int n0 = f.end[0] - f.start[0] + 1, n1 = f.end[1] - f.start[1] + 1, n2 = f.end[2] - f.start[2] + 1;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)P * n0 * n1 * n2) return false;
+  if (f.face == 0) {
+    it.p = (int)(t % P); t /= P;
+    it.i = f.start[0];
+    it.j = f.start[1] + (int)(t % n1);
+    it.k = f.start[2] + (int)(t / n1);
+  } else {
+    it.i = f.start[0] + (int)(t % n0); t /= n0;
+    it.p = (int)(t % P); t /= P;
+    if (f.face == 1) { it.j = f.start[1]; it.k = f.start[2] + (int)t; }
+    else { it.j = f.start[1] + (int)t; it.k = f.start[2]; }
+  }
+  return true;
+}
+
+// Node at offset `off` along the face direction from node (i,j,k) with the direction index
+// replaced by `e`.
+__device__ __forceinline__ idx_t along(const Layout &L, int face, int i, int j, int k, int e) {
+  if (face == 0) return L.at(e, j, k);
+  if (face == 1) return L.at(i, e, k);
+  return L.at(i, j, e);
+}
+
+template <int NS>
+__global__ void k_bc_periodic_pair(Zone z, Param p, FaceBC f) {
+  PairItem it;
+  const int g = z.ngg;
+  if (!pair_item(f, g, it)) return;
+  const int m = f.face == 0 ? z.mx : (f.face == 1 ? z.my : z.mz);
+  const idx_t sz = z.L.sz;
+  if (it.p == 0) {
+    const idx_t ga = along(z.L, f.face, it.i, it.j, it.k, 0), gb = along(z.L, f.face, it.i, it.j, it.k, m - 1);
+    for (int l = 0; l < 6; ++l) {
+      const double ave = 0.5 * (z.bv[ga + l * sz] + z.bv[gb + l * sz]);
+      z.bv[ga + l * sz] = ave;
+      z.bv[gb + l * sz] = ave;
+    }
+    for (int l = 0; l < p.n_scalar; ++l) {
+      const double ave = 0.5 * (z.sv[ga + l * sz] + z.sv[gb + l * sz]);
+      z.sv[ga + l * sz] = ave;
+      z.sv[gb + l * sz] = ave;
+    }
+    cv_point<NS>(z, p, ga);
+    cv_point<NS>(z, p, gb);
+    return;
+  }
+  const bool left = it.p <= g;
+  const int dst = left ? -it.p : m - 1 + (it.p - g);
+  const int src = left ? m - 1 - it.p : it.p - g;
+  const idx_t gg = along(z.L, f.face, it.i, it.j, it.k, dst), gs = along(z.L, f.face, it.i, it.j, it.k, src);
+  for (int l = 0; l < 6; ++l) z.bv[gg + l * sz] = z.bv[gs + l * sz];
+  for (int l = 0; l < p.n_scalar; ++l) z.sv[gg + l * sz] = z.sv[gs + l * sz];
+  cv_point<NS>(z, p, gg);
+}
+
+// The same pairing for the 8th-order viscous node fluxes (components 1..n_var-1 of the three
+// flux arrays; component 0 carries no viscous flux and is never read).
+__global__ void k_periodic_flux_pair(Zone z, Param p, FaceBC f) {
+  PairItem it;
+  const int g = z.ngg;
+  if (!pair_item(f, g, it)) return;
+  const int m = f.face == 0 ? z.mx : (f.face == 1 ? z.my : z.mz);
+  const idx_t sz = z.L.sz;
+  double *arr[3] = {z.fF, z.gF, z.hF};
+  if (it.p == 0) {
+    const idx_t ga = along(z.L, f.face, it.i, it.j, it.k, 0), gb = along(z.L, f.face, it.i, it.j, it.k, m - 1);
+    for (int l = 1; l < p.n_var; ++l)
+      for (int a = 0; a < 3; ++a) {
+        const double ave = 0.5 * (arr[a][ga + l * sz] + arr[a][gb + l * sz]);
+        arr[a][ga + l * sz] = ave;
+        arr[a][gb + l * sz] = ave;
+      }
+    return;
+  }
+  const bool left = it.p <= g;
+  const int dst = left ? -it.p : m - 1 + (it.p - g);
+  const int src = left ? m - 1 - it.p : it.p - g;
+  const idx_t gg = along(z.L, f.face, it.i, it.j, it.k, dst), gs = along(z.L, f.face, it.i, it.j, it.k, src);
+  for (int l = 1; l < p.n_var; ++l)
+    for (int a = 0; a < 3; ++a) arr[a][gg + l * sz] = arr[a][gs + l * sz];
+}
+
+// If periodic face f and the next periodic face in list order are the two faces of one
+// direction that can be applied together, return the index of the left one (direction -1),
+// else -1.  *next receives the index of the partner.
+static int periodic_pair(const Zone &z, const FaceBC *faces, int n, int f, int *next) {
+  int q = f + 1;
+  while (q < n && faces[q].type != CB2_BC_PERIODIC) ++q;
+  if (q >= n) return -1;
+  const FaceBC &a = faces[f], &b = faces[q];
+  if (a.face != b.face || a.direction == b.direction) return -1;
+  const int d = a.face;
+  for (int c = 0; c < 3; ++c)
+    if (c != d && (a.start[c] != b.start[c] || a.end[c] != b.end[c])) return -1;
+  const int m = d == 0 ? z.mx : (d == 1 ? z.my : z.mz);
+  if (m < z.ngg + 2) return -1;
+  const FaceBC &l = a.direction < 0 ? a : b;
+  if (l.start[d] != 0 || l.end[d] != 0) return -1;
+  const FaceBC &r = a.direction < 0 ? b : a;
+  if (r.start[d] != m - 1 || r.end[d] != m - 1) return -1;
+  *next = q;
+  return a.direction < 0 ? f : q;
+}
+
 template <int NS>
 static int launch_bc_ns(const Zone &z, const Param &p, const FaceBC *faces, int n, cudaStream_t s, int &nl) {
   // priority order of the reference
@@ -304,6 +423,19 @@ static int launch_bc_ns(const Zone &z, const Param &p, const FaceBC *faces, int 
   for (int t : order) {
     for (int f = 0; f < n; ++f) {
       if (faces[f].type != t) continue;
+      if (t == CB2_BC_PERIODIC) {
+        int q = -1;
+        const int lf = periodic_pair(z, faces, n, f, &q);
+        if (lf >= 0) {
+          const long long np = face_points(faces[lf]) * (2 * z.ngg + 1);
+          ProfScope prof("boundary_face", s);
+          k_bc_periodic_pair<NS><<<(unsigned)((np + 127) / 128), 128, 0, s>>>(z, p, faces[lf]);
+          ++nl;
+          CB2_TRY(check_launch());
+          f = q;  // the partner is done
+          continue;
+        }
+      }
       const long long np = face_points(faces[f]);
       const unsigned blocks = (unsigned)((np + 127) / 128);
       if (blocks == 0) continue;
@@ -345,6 +477,17 @@ int launch_periodic_flux_exchange(const Zone &z, const Param &p, const FaceBC *f
                                   int &n_launch) {
   for (int f = 0; f < n_faces; ++f) {
     if (faces[f].type != CB2_BC_PERIODIC) continue;
+    int q = -1;
+    const int lf = periodic_pair(z, faces, n_faces, f, &q);
+    if (lf >= 0) {
+      const long long np = face_points(faces[lf]) * (2 * z.ngg + 1);
+      ProfScope prof("periodic_flux_exchange", s);
+      k_periodic_flux_pair<<<(unsigned)((np + 127) / 128), 128, 0, s>>>(z, p, faces[lf]);
+      ++n_launch;
+      CB2_TRY(check_launch());
+      f = q;
+      continue;
+    }
     const long long np = face_points(faces[f]);
     const unsigned blocks = (unsigned)((np + 127) / 128);
     if (!blocks) continue;

@@ -36,46 +36,41 @@ __device__ __forceinline__ double pv_eps(const Param &p, int l) {
 }
 
 // Node slots: PV[v] (v < NV), then 3 metric comps, J, and (Roe) the entropy-fix delta.
+// Reconstructs, from the stencil around node n (slot c, stride st along the sweep), the left
+// state at n+1/2 (pl) and the right state at n-1/2 (pr).  Node n+1 supplies the right state of
+// the interface n+1/2, so each interface is formed by the thread of its left node.
 template <int NS, int REC>
-__device__ __forceinline__ void reconstruct(const double *sN, int NN, int c, int st, const Param &p, double *pl,
-                                            double *pr) {
+__device__ __forceinline__ void reconstruct_node(const double *sN, int NN, int c, int st, const Param &p,
+                                                 double *pl, double *pr) {
   constexpr int NV = 5 + NS;
 #define PV(v, m) sN[(v) * NN + c + (m) * st]
 #pragma unroll
   for (int l = 0; l < NV; ++l) {
     if constexpr (REC == 1) {
-      pl[l] = PV(l, 0);
-      pr[l] = PV(l, 1);
+      pl[l] = pr[l] = PV(l, 0);
     } else if constexpr (REC == 2 || REC == 3) {
-      const double di = PV(l, 0) - PV(l, -1);
-      const double di1 = PV(l, 1) - PV(l, 0);
-      const double di2 = PV(l, 2) - PV(l, 1);
+      const double v0 = PV(l, 0);
+      const double a = v0 - PV(l, -1), b = PV(l, 1) - v0;
       if constexpr (REC == 2) {
+        // MUSCL kappa = 1/3 with minmod; minmod is symmetric, so both faces use one slope pair
         constexpr double kappa = 1.0 / 3.0;
-        const double dnl = minmod(di, di1), dpl = minmod(di1, di);
-        const double dnr = minmod(di1, di2), dpr = minmod(di2, di1);
-        pl[l] = PV(l, 0) + 0.25 * ((1 - kappa) * dnl + (1 + kappa) * dpl);
-        pr[l] = PV(l, 1) - 0.25 * ((1 - kappa) * dpr + (1 + kappa) * dnr);
+        const double m = minmod(a, b);
+        const double d = 0.25 * ((1 - kappa) * m + (1 + kappa) * m);
+        pl[l] = v0 + d;
+        pr[l] = v0 - d;
       } else {
-        pl[l] = PV(l, 0) + 0.5 * minmod(di, di1);
-        pr[l] = PV(l, 1) - 0.5 * minmod(di1, di2);
+        const double d = 0.5 * minmod(a, b);
+        pl[l] = v0 + d;
+        pr[l] = v0 - d;
       }
     } else {
-      constexpr int R = REC / 2 + 1;
-      double v[2 * R - 1], w[2 * R - 1];
+      constexpr int W = REC;  // stencil width, node n in the middle
+      double v[W];
 #pragma unroll
-      for (int m = 0; m < 2 * R - 1; ++m) {
-        v[m] = PV(l, m - R + 1);
-        w[m] = PV(l, m - R + 2);
-      }
+      for (int m = 0; m < W; ++m) v[m] = PV(l, m - W / 2);
       const double eps = pv_eps(p, l);
-      if constexpr (REC == 5) {
-        pl[l] = weno5_plus(v, eps, true);
-        pr[l] = weno5_minus(w, eps, true);
-      } else {
-        pl[l] = weno7_plus(v, eps, true);
-        pr[l] = weno7_minus(w, eps, true);
-      }
+      if constexpr (REC == 5) weno5_node(v, eps, pl[l], pr[l]);
+      else weno7_node(v, eps, pl[l], pr[l]);
     }
   }
 #undef PV
@@ -345,15 +340,20 @@ __device__ __forceinline__ void lax_friedrichs_air(const double *pl, const doubl
   fc[4] = ((pl[NV] + pl[4]) * Ukl + (pr[NV] + pr[4]) * Ukr - sr * (pr[NV] - pl[NV])) * hj;
 }
 
+// Half-width of the node-centred reconstruction stencil.
+template <int REC>
+__host__ __device__ constexpr int pv_half_width() { return REC == 1 ? 0 : (REC <= 3 ? 1 : REC / 2); }
+
 template <int NS, int DIR, int REC, int SOLVER>
 __global__ void __launch_bounds__(kSweepThreads) k_inviscid_pv(Zone z, Param p, idx_t run) {
   constexpr int NV = 5 + NS;
-  constexpr int R = (REC <= 3) ? 2 : REC / 2 + 1;  // half-width of the reconstruction stencil
-  constexpr int NN = DIR == 0 ? (kSweepThreads + 2 * R - 1) : kTI * (kTS + 2 * R - 1);
+  constexpr int RH = pv_half_width<REC>();
+  constexpr int NN = DIR == 0 ? (kSweepThreads + 2 * RH) : kNI * (kNS + 2 * RH);
   constexpr int NSLOT = NV + 4 + (SOLVER == CB2_INV_ROE ? 1 : 0);
   extern __shared__ double smem[];
-  double *sN = smem;
-  double *sFl = sN + NSLOT * NN;
+  double *sN = smem;                          // node data [NSLOT][NN]
+  double *sR = sN + NSLOT * NN;               // right state at n-1/2 of each thread's node [NV+2][T]
+  double *sF = sR + (NV + 2) * kSweepThreads; // interface flux between a node and the next [NV][T]
   const int tid = threadIdx.x;
   const int g = z.ngg;
   const Layout &L = z.L;
@@ -374,14 +374,17 @@ __global__ void __launch_bounds__(kSweepThreads) k_inviscid_pv(Zone z, Param p, 
     }
   };
 
-  int i, j, k;
-  bool valid_if;
+  // Thread tid owns node n.  rec: n lies in [-1, m] along the sweep (both of its faces are
+  // needed); face: the interface n+1/2 is an interior face, i.e. n in [-1, m-1], and node n+1
+  // belongs to this CTA; upd: n in [0, m-1] is updated from the faces n-1/2 and n+1/2.
+  int i, j, k, n, ms, tpos;
+  bool inside;
   int c, st;
   if constexpr (DIR == 0) {
     k = blockIdx.z;
-    const idx_t q0 = (idx_t)blockIdx.x * (kSweepThreads - 1) - 1;
+    const idx_t q0 = (idx_t)blockIdx.x * (kSweepThreads - 2) - 1;
     const idx_t base = (idx_t)k * L.disp1 + L.dispt - g;
-    const idx_t qlo = q0 - R + 1;
+    const idx_t qlo = q0 - RH;
     const idx_t qmin = -(idx_t)g * L.disp2, qmax = (idx_t)(L.my + g) * L.disp2;
     for (int s = tid; s < NN; s += kSweepThreads) {
       const idx_t q = qlo + s;
@@ -394,35 +397,53 @@ __global__ void __launch_bounds__(kSweepThreads) k_inviscid_pv(Zone z, Param p, 
     const idx_t jj = q >= 0 ? q / L.disp2 : -1;
     i = (int)(q - jj * L.disp2) - g;
     j = (int)jj;
-    valid_if = q >= 0 && q < run && i >= -1 && i <= L.mx - 1;
-    c = tid + R - 1;
+    n = i;
+    ms = L.mx;
+    inside = q >= 0 && q < run;
+    tpos = tid;
+    c = tid + RH;
     st = 1;
   } else {
-    const int ti = tid % kTI, ts = tid / kTI;
-    i = blockIdx.x * kTI + ti;
-    const int s0 = blockIdx.y * (kTS - 1);
-    const int ms = DIR == 1 ? L.my : L.mz;
+    const int ti = tid % kNI, ts = tid / kNI;
+    i = blockIdx.x * kNI + ti;
+    const int s0 = blockIdx.y * (kNS - 2) - 1;
+    ms = DIR == 1 ? L.my : L.mz;
     if (DIR == 1) k = blockIdx.z; else j = blockIdx.z;
-    for (int s = ts; s < kTS + 2 * R - 1; s += kTS) {
-      const int n = s0 - R + s;
-      if (i < L.mx && n < ms + g) {
-        if (DIR == 1) load(L.at(i, n, k), s * kTI + ti, i, n, k);
-        else load(L.at(i, j, n), s * kTI + ti, i, j, n);
+    for (int s = ts; s < kNS + 2 * RH; s += kNS) {
+      const int nn = s0 - RH + s;
+      if (i < L.mx && nn < ms + g) {
+        if (DIR == 1) load(L.at(i, nn, k), s * kNI + ti, i, nn, k);
+        else load(L.at(i, j, nn), s * kNI + ti, i, j, nn);
       }
     }
-    const int n_if = s0 - 1 + ts;
-    if (DIR == 1) j = n_if; else k = n_if;
-    valid_if = i < L.mx && n_if <= ms - 1;
-    c = (ts + R - 1) * kTI + ti;
-    st = kTI;
+    n = s0 + ts;
+    if (DIR == 1) j = n; else k = n;
+    inside = i < L.mx;
+    tpos = ts;
+    c = (ts + RH) * kNI + ti;
+    st = kNI;
+  }
+  const bool rec = inside && n >= -1 && n <= ms;
+  const bool face = rec && n <= ms - 1 && tpos < (DIR == 0 ? kSweepThreads : kNS) - 1;
+  const bool upd = face && n >= 0 && tpos >= 1;
+  __syncthreads();
+
+  double pl[NV + 2];
+  if (rec) {
+    double pr[NV + 2];
+    reconstruct_node<NS, REC>(sN, NN, c, st, p, pl, pr);
+    state_energy<NS>(pl, p.mech);
+    state_energy<NS>(pr, p.mech);
+#pragma unroll
+    for (int v = 0; v < NV + 2; ++v) sR[v * kSweepThreads + tid] = pr[v];
   }
   __syncthreads();
 
-  if (valid_if) {
-    double pl[NV + 2], pr[NV + 2];
-    reconstruct<NS, REC>(sN, NN, c, st, p, pl, pr);
-    state_energy<NS>(pl, p.mech);
-    state_energy<NS>(pr, p.mech);
+  if (face) {
+    const int tn = tid + st;  // the thread of node n+1 (st is 1 or kNI, as the thread layout)
+    double pr[NV + 2];
+#pragma unroll
+    for (int v = 0; v < NV + 2; ++v) pr[v] = sR[v * kSweepThreads + tn];
     const double ml[3] = {sN[NV * NN + c], sN[(NV + 1) * NN + c], sN[(NV + 2) * NN + c]};
     const double mr[3] = {sN[NV * NN + c + st], sN[(NV + 1) * NN + c + st], sN[(NV + 2) * NN + c + st]};
     const double jl = sN[(NV + 3) * NN + c], jr = sN[(NV + 3) * NN + c + st];
@@ -433,19 +454,16 @@ __global__ void __launch_bounds__(kSweepThreads) k_inviscid_pv(Zone z, Param p, 
       roe_flux<NS>(pl, pr, ml, mr, jl, jr, sN[(NV + 4) * NN + c], sN[(NV + 4) * NN + c + st], p, fc);
     else lax_friedrichs_air(pl, pr, ml, mr, jl, jr, fc);
 #pragma unroll
-    for (int v = 0; v < NV; ++v) sFl[v * kSweepThreads + tid] = fc[v];
+    for (int v = 0; v < NV; ++v) sF[v * kSweepThreads + tid] = fc[v];
   }
   __syncthreads();
 
-  bool valid_node;
-  if constexpr (DIR == 0) valid_node = tid >= 1 && valid_if && i >= 0;
-  else valid_node = (tid / kTI) >= 1 && valid_if && (DIR == 1 ? j >= 0 : k >= 0);
-  if (valid_node) {
-    const int tprev = DIR == 0 ? tid - 1 : tid - kTI;
+  if (upd) {
+    const int tprev = tid - st;
     const idx_t gd = z.L0.at(i, j, k);
     const idx_t sz0 = z.L0.sz;
 #pragma unroll
-    for (int v = 0; v < NV; ++v) z.dq[gd + v * sz0] -= sFl[v * kSweepThreads + tid] - sFl[v * kSweepThreads + tprev];
+    for (int v = 0; v < NV; ++v) z.dq[gd + v * sz0] -= sF[v * kSweepThreads + tid] - sF[v * kSweepThreads + tprev];
   }
 }
 
@@ -475,7 +493,7 @@ __global__ void k_entropy_fix_delta(Zone z, Param p) {
 template <int NS, int REC, int SOLVER>
 static int launch_pv_dirs(const Zone &z, const Param &p, cudaStream_t s, int &nl) {
   constexpr int NV = 5 + NS;
-  constexpr int R = (REC <= 3) ? 2 : REC / 2 + 1;
+  constexpr int RH = pv_half_width<REC>();
   constexpr int NSLOT = NV + 4 + (SOLVER == CB2_INV_ROE ? 1 : 0);
   if (SOLVER == CB2_INV_ROE) {
     dim3 grid((z.mx + 2 + 127) / 128, z.my + 2, z.mz + 2);
@@ -487,8 +505,9 @@ static int launch_pv_dirs(const Zone &z, const Param &p, cudaStream_t s, int &nl
   const int ndir = z.mz > 1 ? 3 : 2;
   for (int d = 0; d < ndir; ++d) {
     SweepGeom geo;
-    const dim3 grid = sweep_grid(d, z.L, geo);
-    const size_t smem = sizeof(double) * ((size_t)NSLOT * sweep_nodes(d, R) + (size_t)NV * kSweepThreads);
+    const dim3 grid = node_sweep_grid(d, z.L, geo);
+    const size_t smem =
+        sizeof(double) * ((size_t)NSLOT * node_sweep_nodes(d, RH) + (size_t)(2 * NV + 2) * kSweepThreads);
     static const char *names[3] = {"pv_flux_x", "pv_flux_y", "pv_flux_z"};
     ProfScope prof(names[d], s);
     if (d == 0) {
