@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
+    ap.add_argument("--accuracy-steps", type=int, default=100,
+                    help="RK3 steps of the mixed-vs-FP64 accuracy run (the workload's 100 steps)")
     return ap.parse_args()
 
 
@@ -194,6 +197,8 @@ def gpu_arm(args, rank, world, local_rank):
     p, hb, faces = case.param, case.blocks[0], case.faces[0]
     dev = DeviceBlock(hb, device=f"cuda:{local_rank}")
     host_state = {n: hb.a[n] for n in ("cv", "bv")}
+    gh = hb.ngg
+    xyz = torch.from_numpy(case.meta["xyz_sum"][gh:-gh, gh:-gh, gh:-gh].copy())
     del case, hb
     ctx = cb200.Context(p)
     ctx.bind(0, dev.view(), faces)
@@ -280,6 +285,10 @@ def gpu_arm(args, rank, world, local_rank):
         e2e = {"value": world * nodes * k_e2e / (ms_e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "steps": k_e2e, "ms_per_step": ms_e / k_e2e}
 
+    mixed = None
+    if not args.no_mixed:
+        mixed = mixed_form(args, p, dev, faces, host_state, xyz, dt, ctx, stream, nodes, world, dist, local_rank)
+
     ctx.close()
     if dist:
         dist.barrier()
@@ -298,9 +307,86 @@ def gpu_arm(args, rank, world, local_rank):
                        "l2": "inputs larger than L2 (about 7 GB of field arrays per GPU)",
                        "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
             "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clocks, "status_flags": status,
+            "clocks": clocks, "status_flags": status, "mixed": mixed,
             "kernel_ms_per_step": {k: v[1] for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}}
     print(json.dumps(line), flush=True)
+
+
+def mixed_form(args, p, dev, faces, host_state, xyz, dt, ctx64, stream, nodes, world, dist, local_rank):
+    """The mixed-precision form on the same workload: FP32 reconstruction, fluxes and viscous
+    stencils, FP64 state and stage update.  Both forms run `accuracy_steps` RK3 steps from the
+    same initial state; the mixed run is timed with CUDA events and its density is compared with
+    the FP64 run (which the parity tests tie to the FP64 oracle) and with the exact advected
+    profile."""
+    import torch
+    import cb200
+    from cb200 import abi
+    sh = stream.cuda_stream
+    pm = abi.ParamView.from_buffer_copy(p)
+    pm.precision = abi.PREC_MIXED
+    ctx32 = cb200.Context(pm)
+    ctx32.bind(0, dev.view(), faces)
+    dev_init = {n: torch.from_numpy(a).to(dev.t[n].device) for n, a in host_state.items()}
+    g = (dev.t["bv"].shape[-1] - int(round(xyz.shape[-1]))) // 2
+
+    def reset():
+        for n, t in dev_init.items():
+            dev.t[n].copy_(t)
+        ctx64.properties(0, sh)
+
+    def rho():
+        return dev.t["bv"][0, g:-g, g:-g, g:-g].clone()
+
+    def run(ctx, steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e0.record(stream)
+        for _ in range(steps):
+            ctx.rk3_step(dt, True, sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([ms], device=f"cuda:{local_rank}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    S = args.accuracy_steps
+    for _ in range(args.warmup):
+        ctx32.rk3_step(dt, True, sh)
+    reset()
+    ms32 = run(ctx32, S)
+    r32 = rho()
+    status32 = ctx32.read_status(sh)
+    ctx32.profile(True)
+    ctx32.rk3_step(dt, True, sh)
+    torch.cuda.synchronize()
+    prof32 = ctx32.profile_read()
+    ctx32.profile(False)
+    reset()
+    ms64 = run(ctx64, S)
+    r64 = rho()
+    ctx32.close()
+    t_end = S * dt
+    ex = 1.0 + 0.2 * torch.sin(2 * math.pi * (xyz.to(r64.device) - 3.0 * t_end))
+    mean64 = r64.abs().mean()
+    d = (r32 - r64).abs()
+    out = {"precision": "mixed: FP32 reconstruction/AUSM+/8th-order viscous stencils, FP64 state, "
+                        "temperature and stage update",
+           "steps": S, "value": world * nodes * S / (ms32 * 1e-3), "ms_per_step": ms32 / S,
+           "fp64_value_same_run": world * nodes * S / (ms64 * 1e-3), "fp64_ms_per_step": ms64 / S,
+           "speedup_vs_fp64": ms64 / ms32,
+           "l1_rho_vs_fp64": float(d.mean() / mean64), "linf_rho_vs_fp64": float(d.max() / mean64),
+           "l1_rho_vs_exact_mixed": float((r32 - ex).abs().mean() / ex.abs().mean()),
+           "l1_rho_vs_exact_fp64": float((r64 - ex).abs().mean() / ex.abs().mean()),
+           "t_end": t_end, "status_flags": status32,
+           "accuracy_bound_l1": 1e-6,
+           "kernel_ms_per_step": {k: v[1] for k, v in sorted(prof32.items(), key=lambda kv: -kv[1][1])}}
+    out["meets_accuracy_bound"] = out["l1_rho_vs_fp64"] <= 1e-6
+    return out
 
 
 def main():

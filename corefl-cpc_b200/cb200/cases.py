@@ -167,7 +167,8 @@ def sine_wave(n=256, ngg=4, amp=0.05, mu=1e-4, scheme=abi.INV_AUSMP, reconstruct
     faces = box_faces(m, m, m, {(d, s): abi.BC_PERIODIC for d in range(3) for s in (-1, 1)})
     p = make_param(dim=3, inviscid_scheme=scheme, reconstruction=reconstruction, viscous_order=viscous_order,
                    cfl=0.5, rho_ref=1.0, v_ref=math.sqrt(3.0), mu_constant=mu)
-    return Case("sine_wave", p, [b], [faces], {"n": n, "amp": amp})
+    # x + y + z of every node: the exact solution is rho = 1 + 0.2 sin(2 pi (x + y + z - 3 t))
+    return Case("sine_wave", p, [b], [faces], {"n": n, "amp": amp, "xyz_sum": x + y + z})
 
 
 # ---- thermally perfect mixtures ------------------------------------------------------------

@@ -269,7 +269,11 @@ int cb2_init(const cb2_param_view *pv, cb2_ctx **out) {
   if (pv->viscous_order == 8 && ns != 0) return CB2_ERR_UNSUPPORTED;
   if (pv->positive_preserving) return CB2_ERR_UNSUPPORTED;
   if (pv->reaction && ns == 0) return CB2_ERR_INVALID;
-  if (pv->precision != CB2_PREC_FP64) return CB2_ERR_UNSUPPORTED;
+  if (pv->precision != CB2_PREC_FP64 && pv->precision != CB2_PREC_MIXED) return CB2_ERR_INVALID;
+  // mixed form: FP32 sweeps for WENO5/7 primitive reconstruction with AUSM+/HLLC/Roe
+  if (pv->precision == CB2_PREC_MIXED &&
+      (!pvpath || sch == 1 || (pv->reconstruction != CB2_REC_WENO5 && pv->reconstruction != CB2_REC_WENO7)))
+    return CB2_ERR_UNSUPPORTED;
   cb2_ctx *ctx = new cb2_ctx;
   ctx->view = *pv;
   Param &p = ctx->p;
@@ -587,6 +591,26 @@ int cb2_rk3_step(cb2_ctx *ctx, double *dt_inout, int fixed_dt, void *stream) {
       if (ctx->blocks[b].bound) CB2_TRY(cb2_properties(ctx, b, stream));
   }
   return CB2_OK;
+}
+
+int cb2_reactor_setup(cb2_ctx *ctx, cb2_reactor *reactors, int n, const double *T0, const double *p0,
+                      const double *Y, const double *t_end, double h0, void *stream) {
+  if (!ctx || !reactors || n < 0 || !T0 || !p0 || !Y || !t_end || !(h0 > 0)) return CB2_ERR_INVALID;
+  if (ctx->p.n_spec == 0) return CB2_ERR_UNSUPPORTED;
+  if (n == 0) return CB2_OK;
+  ProfGuard pg(ctx);
+  ++ctx->n_launch;
+  return launch_reactor_setup(ctx->p, reactors, n, T0, p0, Y, t_end, h0, (cudaStream_t)stream);
+}
+
+int cb2_reactor_advance(cb2_ctx *ctx, cb2_reactor *reactors, int n, int max_attempts, double rtol, double atol,
+                        void *stream) {
+  if (!ctx || !reactors || n < 0 || max_attempts < 1 || !(rtol > 0) || !(atol > 0)) return CB2_ERR_INVALID;
+  if (ctx->p.n_spec == 0) return CB2_ERR_UNSUPPORTED;
+  if (n == 0) return CB2_OK;
+  ProfGuard pg(ctx);
+  ++ctx->n_launch;
+  return launch_reactor_advance(ctx->p, reactors, n, max_attempts, rtol, atol, (cudaStream_t)stream);
 }
 
 int cb2_read_status(cb2_ctx *ctx, unsigned *flags_out, void *stream) {

@@ -14,38 +14,10 @@
 //   wall     : no-slip, non-catalytic, adiabatic or isothermal (apply_wall,
 //              src/BoundCond.cu:3055-3389)
 // Every filled node gets its cv recomputed (compute_cv_from_bv_1_point, FieldOperation.cuh:163).
-#include "common.cuh"
-#include "thermo.cuh"
+#include "point.cuh"
 #include "launch.h"
 
 namespace cb2 {
-
-template <int NS>
-__device__ __forceinline__ void cv_point(const Zone &z, const Param &p, idx_t g) {
-  const idx_t sz = z.L.sz;
-  const double rho = z.bv[g], u = z.bv[g + sz], v = z.bv[g + 2 * sz], w = z.bv[g + 3 * sz];
-  z.cv[g] = rho;
-  z.cv[g + sz] = rho * u;
-  z.cv[g + 2 * sz] = rho * v;
-  z.cv[g + 3 * sz] = rho * w;
-  double E = 0.5 * (u * u + v * v + w * w);
-  if constexpr (NS == 0) {
-    E *= rho;
-    E += z.bv[g + 4 * sz] / (kGammaAir - 1);
-  } else {
-    double h[NS];
-    nasa7_h<NS>(z.bv[g + 5 * sz], p.mech, h);
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      const double y = z.sv[g + s * sz];
-      z.cv[g + (5 + s) * sz] = rho * y;
-      E += h[s] * y;
-    }
-    E *= rho;
-    E -= z.bv[g + 4 * sz];
-  }
-  z.cv[g + 4 * sz] = E;
-}
 
 __device__ __forceinline__ bool face_point(const FaceBC &f, int &i, int &j, int &k) {
   const int n0 = f.end[0] - f.start[0] + 1, n1 = f.end[1] - f.start[1] + 1, n2 = f.end[2] - f.start[2] + 1;

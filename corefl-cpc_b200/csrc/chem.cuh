@@ -1,0 +1,146 @@
+// Finite-rate chemistry of one state: concentrations -> forward/backward rates -> rates of
+// progress -> species creation and destruction (finite_rate_chemistry, generic-mechanism branch,
+// src/FiniteRateChem.cu:1406-1488; forward_reaction_rate :1505-1554 with Troe :1536-1549;
+// backward_reaction_rate :1560-1636; rate_of_progress :1638-1663; chemical_source :1665-1681).
+//
+// The reaction loop is fused: each reaction's rate of progress is added to the per-species
+// creation/destruction accumulators as soon as it is known, so no per-reaction arrays are
+// needed; the additions happen in the reference's reaction order.  Callers that need the rates
+// of progress themselves (the point-implicit Jacobian) pass arrays for them.  Arrhenius and
+// Gibbs exponentials are FP64 in every precision form.
+#pragma once
+#include "common.cuh"
+#include "thermo.cuh"
+
+namespace cb2 {
+
+__device__ __forceinline__ double arrhenius(double t, double A, double b, double Ea) {
+  return A * pow(t, b) * exp(-Ea / t);
+}
+
+// c^n for the small non-negative integer stoichiometric coefficients of a mechanism.
+__device__ __forceinline__ double ipow(double c, int n) {
+  double r = 1.0;
+  for (int a = 0; a < n; ++a) r *= c;
+  return r;
+}
+
+// t [K], c [mol/cm^3]; creation/destruction accumulate sum_r of q2 nu_f + q1 nu_b and
+// q1 nu_f + q2 nu_b [mol/(cm^3 s)]; q1r/q2r (may be null) receive the forward and backward
+// rates of progress of every reaction.
+template <int NS>
+__device__ __forceinline__ void chem_rates(double t, const double *c, const Mech &m, double *creation,
+                                           double *destruction, double *q1r, double *q2r) {
+  bool need_gibbs = false;
+  for (int r = 0; r < m.n_reac; ++r) {
+    const int ty = __ldg(m.reac_type + r);
+    if (ty != 0 && __ldg(m.rev_type + r) != 1 && ty != 2) need_gibbs = true;
+  }
+  double gibbs[NS];
+  if (need_gibbs) nasa7_gibbs_rt<NS>(t, m, gibbs);
+  constexpr double temp_p = kPatm / kRu * 1e-3;
+  const double temp_t = temp_p / t;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) creation[s] = destruction[s] = 0;
+
+  for (int r = 0; r < m.n_reac; ++r) {
+    const int ty = __ldg(m.reac_type + r);
+    const int *sf = m.stoi_f + r * NS, *sb = m.stoi_b + r * NS;
+    // forward rate
+    double kf = arrhenius(t, __ldg(m.A + r), __ldg(m.b + r), __ldg(m.Ea + r));
+    double cc = 0;
+    if (ty > 3 || (ty != 0 && __ldg(m.rev_type + r) == 1 && ty == 4)) {
+#pragma unroll
+      for (int s = 0; s < NS; ++s) cc += c[s] * __ldg(m.tbc + r * NS + s);
+    }
+    if (ty == 3) {
+      kf += arrhenius(t, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
+    } else if (ty == 4) {
+      kf *= cc;
+    } else if (ty > 4) {
+      const double kf_low = arrhenius(t, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
+      const double kf_high = kf;
+      if (kf_high < 1e-25 && kf_low < 1e-25) {
+        kf = 0;
+      } else {
+        const double pr = kf_low * cc / kf_high;
+        double F = 1.0;
+        if (ty > 5) {
+          const double al = __ldg(m.troe_alpha + r);
+          double fc = (1 - al) * exp(-t / __ldg(m.troe_t3 + r)) + al * exp(-t / __ldg(m.troe_t1 + r));
+          if (ty == 7) fc += exp(-__ldg(m.troe_t2 + r) / t);
+          const double lfc = log10(fc);
+          const double cq = -0.4 - 0.67 * lfc;
+          const double nq = 0.75 - 1.27 * lfc;
+          const double lpr = log10(pr);
+          const double tmp = (lpr + cq) / (nq - 0.14 * (lpr + cq));
+          F = pow(10.0, lfc / (1.0 + tmp * tmp));
+        }
+        kf = kf_high * pr / (1.0 + pr) * F;
+      }
+    }
+    // backward rate
+    double kb = 0;
+    if (ty != 0) {
+      if (__ldg(m.rev_type + r) == 1) {
+        kb = arrhenius(t, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
+        if (ty == 4) kb *= cc;
+      } else if (ty != 2) {
+        double dg = 0;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) dg += gibbs[s] * (__ldg(sb + s) - __ldg(sf + s));
+        const double kc = pow(temp_t, __ldg(m.reac_order + r)) * exp(-dg);
+        kb = kf / kc;
+      }
+    }
+    // rates of progress
+    double q1 = 1.0, q2 = ty != 0 ? 1.0 : 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      q1 *= ipow(c[s], __ldg(sf + s));
+      if (ty != 0) q2 *= ipow(c[s], __ldg(sb + s));
+    }
+    q1 *= kf;
+    if (ty != 0) q2 *= kb;
+    if (q1r) {
+      q1r[r] = q1;
+      q2r[r] = q2;
+    }
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const double f = __ldg(sf + s), b = __ldg(sb + s);
+      creation[s] += q2 * f + q1 * b;
+      destruction[s] += q1 * f + q2 * b;
+    }
+  }
+}
+
+// One node of the explicit source: dq[5+k] += J omega_k and the reaction time scale.
+template <int NS>
+__device__ __forceinline__ void chemistry_point(const Zone &z, const Param &p, int i, int j, int k) {
+  const Mech &m = p.mech;
+  const idx_t g = z.L.at(i, j, k), sz = z.L.sz;
+  const double rho = z.bv[g], t = z.bv[g + 5 * sz];
+  double c[NS], y[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    y[s] = z.sv[g + s * sz];
+    c[s] = rho * y[s] * __ldg(m.imw + s) * 1e-3;
+  }
+  double creation[NS], destruction[NS];
+  chem_rates<NS>(t, c, m, creation, destruction, nullptr, nullptr);
+  const double jac = z.jac[g];
+  const idx_t g0 = z.L0.at(i, j, k), sz0 = z.L0.sz;
+  double ts = 1e+6;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const double w = 1e+3 / __ldg(m.imw + s);
+    const double od = destruction[s] * w;
+    const double om = creation[s] * w - od;
+    z.dq[g0 + (5 + s) * sz0] += jac * om;
+    if (y[s] > 1e-25 && fabs(od) > 1e-25) ts = fmin(ts, fabs(rho * y[s] / od));
+  }
+  if (z.rts) z.rts[g] = ts;
+}
+
+}  // namespace cb2

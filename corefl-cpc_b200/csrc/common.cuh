@@ -27,6 +27,7 @@ typedef long long idx_t;
 
 struct Layout {
   int mx, my, mz, g;
+  int gj;  // ghost layers stored along j (g for a block layout, 0 for a compact 1-D case)
   idx_t disp2, disp1, dispt, sz;
   __host__ __device__ __forceinline__ idx_t at(int i, int j, int k) const {
     return (idx_t)k * disp1 + (idx_t)j * disp2 + i + dispt;
@@ -35,11 +36,23 @@ struct Layout {
 
 inline Layout make_layout(int mx, int my, int mz, int g) {
   Layout L;
-  L.mx = mx; L.my = my; L.mz = mz; L.g = g;
+  L.mx = mx; L.my = my; L.mz = mz; L.g = g; L.gj = g;
   L.disp2 = mx + 2 * g;
   L.disp1 = (idx_t)(my + 2 * g) * L.disp2;
   L.dispt = (L.disp1 + L.disp2 + 1) * g;
   L.sz = (idx_t)(mx + 2 * g) * (my + 2 * g) * (mz + 2 * g);
+  return L;
+}
+
+// A 1-D case stored without ghost rows or planes: only the g ghost nodes at each end of the
+// single i-line (the batched cases use it; at(i, 0, 0) = i + g).
+inline Layout make_layout_1d(int mx, int g) {
+  Layout L;
+  L.mx = mx; L.my = 1; L.mz = 1; L.g = g; L.gj = 0;
+  L.disp2 = mx + 2 * g;
+  L.disp1 = L.disp2;
+  L.dispt = g;
+  L.sz = L.disp2;
   return L;
 }
 

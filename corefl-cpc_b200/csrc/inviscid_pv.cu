@@ -1,542 +1,18 @@
-// Inviscid flux from reconstructed primitive variables and an approximate Riemann solver,
-// fused with the flux difference (compute_convective_term_pv_1D, src/InviscidScheme.cu:61-169;
-// Roe_compute_inviscid_flux_1D, :306-395).
-//
-// Reconstruction of (rho,u,v,w,p,Y) at i+1/2 (reconstruction<mix>, src/InviscidScheme.cu:171-219):
-//   1 first order, 2 MUSCL kappa=1/3 with minmod (src/Reconstruction.cu:14-32),
-//   3 NND2 (src/Reconstruction.cu:34-45), and, added here, 5/7 = WENO5-JS / WENO7-Z weights
-//   applied to the primitive point values (left state from the left-biased stencil, right
-//   state from the right-biased one).
-// Riemann solvers: AUSM+ (riemannSolver_ausmPlus, :397-469), HLLC with Roe-averaged wave
-//   speeds (riemannSolver_hllc, :471-590), Roe with the Harten entropy fix
-//   (riemannSolver_Roe + compute_half_sum_left_right_flux, :592-746; the fix delta comes from
-//   compute_entropy_fix_delta, :269-304), Lax-Friedrichs for air (:748-786).
-#include "common.cuh"
-#include "thermo.cuh"
-#include "weno.cuh"
-#include "sweep.cuh"
-#include "launch.h"
+// Plain-form (FP64) instantiations of the primitive-variable sweep and the precision dispatch.
+// The kernels and Riemann solvers live in inviscid_pv.cuh; the FP32 (mixed-form) instantiations
+// are compiled in inviscid_pv_f32.cu.
+#include "inviscid_pv.cuh"
 
 namespace cb2 {
-
-__device__ __forceinline__ double sgn1(double a) { return a < 0 ? -1.0 : 1.0; }
-__device__ __forceinline__ double minmod(double a, double b) {
-  return 0.5 * (sgn1(a) + sgn1(b)) * fmin(fabs(a), fabs(b));
-}
-
-// Per-variable WENO eps for primitive reconstruction: 1e-40 times the square of the
-// variable's reference scale (rho_ref, v_ref, rho_ref v_ref^2, 1 for mass fractions).
-__device__ __forceinline__ double pv_eps(const Param &p, int l) {
-  double s;
-  if (l == 0) s = p.rho_ref;
-  else if (l <= 3) s = p.v_ref;
-  else if (l == 4) s = p.rho_ref * p.v_ref * p.v_ref;
-  else s = 1.0;
-  return kWenoEps * s * s;
-}
-
-// Node slots: PV[v] (v < NV), then 3 metric comps, J, and (Roe) the entropy-fix delta.
-// Reconstructs, from the stencil around node n (slot c, stride st along the sweep), the left
-// state at n+1/2 (pl) and the right state at n-1/2 (pr).  Node n+1 supplies the right state of
-// the interface n+1/2, so each interface is formed by the thread of its left node.
-template <int NS, int REC>
-__device__ __forceinline__ void reconstruct_node(const double *sN, int NN, int c, int st, const Param &p,
-                                                 double *pl, double *pr) {
-  constexpr int NV = 5 + NS;
-#define PV(v, m) sN[(v) * NN + c + (m) * st]
-#pragma unroll
-  for (int l = 0; l < NV; ++l) {
-    if constexpr (REC == 1) {
-      pl[l] = pr[l] = PV(l, 0);
-    } else if constexpr (REC == 2 || REC == 3) {
-      const double v0 = PV(l, 0);
-      const double a = v0 - PV(l, -1), b = PV(l, 1) - v0;
-      if constexpr (REC == 2) {
-        // MUSCL kappa = 1/3 with minmod; minmod is symmetric, so both faces use one slope pair
-        constexpr double kappa = 1.0 / 3.0;
-        const double m = minmod(a, b);
-        const double d = 0.25 * ((1 - kappa) * m + (1 + kappa) * m);
-        pl[l] = v0 + d;
-        pr[l] = v0 - d;
-      } else {
-        const double d = 0.5 * minmod(a, b);
-        pl[l] = v0 + d;
-        pr[l] = v0 - d;
-      }
-    } else {
-      constexpr int W = REC;  // stencil width, node n in the middle
-      double v[W];
-#pragma unroll
-      for (int m = 0; m < W; ++m) v[m] = PV(l, m - W / 2);
-      const double eps = pv_eps(p, l);
-      if constexpr (REC == 5) weno5_node(v, eps, pl[l], pr[l]);
-      else weno7_node(v, eps, pl[l], pr[l]);
-    }
-  }
-#undef PV
-}
-
-// Total energy (index NV) and gamma (index NV+1) of a reconstructed state.
-template <int NS>
-__device__ __forceinline__ void state_energy(double *pv, const Mech &m) {
-  constexpr int NV = 5 + NS;
-  const double ek = 0.5 * (pv[1] * pv[1] + pv[2] * pv[2] + pv[3] * pv[3]);
-  if constexpr (NS == 0) {
-    pv[NV] = ek * pv[0] + pv[4] / (kGammaAir - 1);
-    pv[NV + 1] = kGammaAir;
-  } else {
-    double r = 0;
-#pragma unroll
-    for (int s = 0; s < NS; ++s) r += pv[5 + s] * __ldg(m.gas_const + s);
-    const double t = pv[4] / fmax(pv[0] * r, 1e-12);
-    double gam, c, etr;
-    characteristic_thermo<NS>(t, pv + 5, m, gam, c, nullptr, nullptr, &etr);
-    pv[NV] = pv[0] * (ek + etr);
-    pv[NV + 1] = gam;
-  }
-}
-
-template <int NS>
-__device__ __forceinline__ void ausm_plus(const double *pl, const double *pr, const double *ml, const double *mr,
-                                          double jl, double jr, double *fc) {
-  constexpr int NV = 5 + NS;
-  const double k1 = 0.5 * (jl * ml[0] + jr * mr[0]);
-  const double k2 = 0.5 * (jl * ml[1] + jr * mr[1]);
-  const double k3 = 0.5 * (jl * ml[2] + jr * mr[2]);
-  const double gk = sqrt(k1 * k1 + k2 * k2 + k3 * k3);
-  const double ul = (k1 * pl[1] + k2 * pl[2] + k3 * pl[3]) / gk;
-  const double ur = (k1 * pr[1] + k2 * pr[2] + k3 * pr[3]) / gk;
-  const double c = 0.5 * (sqrt(pl[NV + 1] * pl[4] / pl[0]) + sqrt(pr[NV + 1] * pr[4] / pr[0]));
-  const double Ml = ul / c, Mr = ur / c;
-  constexpr double alpha = 3 / 16.0;
-  double mlp, plp, mrn, prn;
-  if (fabs(Ml) > 1) {
-    mlp = 0.5 * (Ml + fabs(Ml));
-    plp = mlp / Ml;
-  } else {
-    const double a = (Ml + 1) * (Ml + 1) * 0.25, b = (Ml * Ml - 1) * (Ml * Ml - 1);
-    mlp = a + 0.125 * b;
-    plp = a * (2 - Ml) + alpha * Ml * b;
-  }
-  if (fabs(Mr) > 1) {
-    mrn = 0.5 * (Mr - fabs(Mr));
-    prn = mrn / Mr;
-  } else {
-    const double a = (Mr - 1) * (Mr - 1) * 0.25, b = (Mr * Mr - 1) * (Mr * Mr - 1);
-    mrn = -a - 0.125 * b;
-    prn = a * (2 + Mr) - alpha * Mr * b;
-  }
-  const double pc = plp * pl[4] + prn * pr[4];
-  const double mh = mlp + mrn;
-  const double mflux = c * (pl[0] * 0.5 * (mh + fabs(mh)) + pr[0] * 0.5 * (mh - fabs(mh)));
-  const double coeff = mflux * gk;
-  const double *pu = mflux >= 0 ? pl : pr;
-  fc[0] = coeff;
-  fc[1] = coeff * pu[1] + pc * k1;
-  fc[2] = coeff * pu[2] + pc * k2;
-  fc[3] = coeff * pu[3] + pc * k3;
-  fc[4] = coeff * (pu[NV] + pu[4]) / pu[0];
-#pragma unroll
-  for (int l = 5; l < NV; ++l) fc[l] = coeff * pu[l];
-}
-
-template <int NS>
-__device__ __forceinline__ void hllc(const double *pl, const double *pr, const double *ml, const double *mr,
-                                     double jl, double jr, const Mech &mech, double *fc) {
-  constexpr int NV = 5 + NS;
-  const double sl0 = sqrt(pl[0]), sr0 = sqrt(pr[0]);
-  const double rlc = sl0 / (sl0 + sr0), rrc = sr0 / (sl0 + sr0);
-  const double ut = pl[1] * rlc + pr[1] * rrc, vt = pl[2] * rlc + pr[2] * rrc, wt = pl[3] * rlc + pr[3] * rrc;
-  double ct;
-  if constexpr (NS == 0) {
-    const double hl = (pl[NV] + pl[4]) / pl[0], hr = (pr[NV] + pr[4]) / pr[0];
-    const double ht = hl * rlc + hr * rrc;
-    const double ekt = 0.5 * (ut * ut + vt * vt + wt * wt);
-    ct = sqrt((kGammaAir - 1) * (ht - ekt));
-  } else {
-    double svm[NS], r = 0;
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      svm[s] = rlc * pl[5 + s] + rrc * pr[5 + s];
-      r += svm[s] * __ldg(mech.gas_const + s);
-    }
-    const double t = (rlc * (pl[4] / pl[0]) + rrc * (pr[4] / pr[0])) / fmax(r, 1e-12);
-    double gam;
-    characteristic_thermo<NS>(t, svm, mech, gam, ct, nullptr, nullptr, nullptr);
-  }
-  const double kx = 0.5 * (ml[0] + mr[0]), ky = 0.5 * (ml[1] + mr[1]), kz = 0.5 * (ml[2] + mr[2]);
-  const double gk = sqrt(kx * kx + ky * ky + kz * kz);
-  const double Ut = (kx * ut + ky * vt + kz * wt) / gk;
-  const double ja = 0.5 * (jl + jr);
-  const double Ul = kx * pl[1] + ky * pl[2] + kz * pl[3];
-  const double cl = sqrt(pl[NV + 1] * pl[4] / pl[0]);
-  const double sl = fmin(Ul / gk - cl, Ut - ct);
-  if (sl >= 0) {
-    const double rU = pl[0] * Ul;
-    fc[0] = ja * rU;
-    fc[1] = ja * (rU * pl[1] + pl[4] * kx);
-    fc[2] = ja * (rU * pl[2] + pl[4] * ky);
-    fc[3] = ja * (rU * pl[3] + pl[4] * kz);
-    fc[4] = ja * ((pl[NV] + pl[4]) * Ul);
-#pragma unroll
-    for (int l = 5; l < NV; ++l) fc[l] = ja * rU * pl[l];
-    return;
-  }
-  const double Ur = kx * pr[1] + ky * pr[2] + kz * pr[3];
-  const double cr = sqrt(pr[NV + 1] * pr[4] / pr[0]);
-  const double sr = fmax(Ur / gk + cr, Ut + ct);
-  if (sr < 0) {
-    const double rU = pr[0] * Ur;
-    fc[0] = ja * rU;
-    fc[1] = ja * (rU * pr[1] + pr[4] * kx);
-    fc[2] = ja * (rU * pr[2] + pr[4] * ky);
-    fc[3] = ja * (rU * pr[3] + pr[4] * kz);
-    fc[4] = ja * ((pr[NV] + pr[4]) * Ur);
-#pragma unroll
-    for (int l = 5; l < NV; ++l) fc[l] = ja * rU * pr[l];
-    return;
-  }
-  const double sm = ((pr[0] * Ur * (sr - Ur / gk) - pl[0] * Ul * (sl - Ul / gk)) / gk + pl[4] - pr[4]) /
-                    (pr[0] * (sr - Ur / gk) - pl[0] * (sl - Ul / gk));
-  const double pm = pl[0] * (sl - Ul / gk) * (sm - Ul / gk) + pl[4];
-  const bool left = sm >= 0;
-  const double *ps = left ? pl : pr;
-  const double ss = left ? sl : sr, Us = left ? Ul : Ur;
-  const double pco = 1.0 / (ss - sm);
-  const double qco = ja * pco * sm * (ss * gk - Us) * ps[0];
-  fc[0] = qco;
-  const double dP = (ss * pm - sm * ps[4]) * pco * ja;
-  fc[1] = qco * ps[1] + dP * kx;
-  fc[2] = qco * ps[2] + dP * ky;
-  fc[3] = qco * ps[3] + dP * kz;
-  fc[4] = qco * ps[NV] / ps[0] + pco * ja * (ss * pm * sm * gk - sm * ps[4] * Us);
-#pragma unroll
-  for (int l = 5; l < NV; ++l) fc[l] = qco * ps[l];
-}
-
-template <int NS>
-__device__ __forceinline__ void roe_flux(const double *pl, const double *pr, const double *ml, const double *mr,
-                                         double jl, double jr, double efl, double efr, const Param &p,
-                                         double *fc) {
-  constexpr int NV = 5 + NS;
-  // half sum of the left and right physical fluxes
-  {
-    double JKx = jl * ml[0], JKy = jl * ml[1], JKz = jl * ml[2];
-    double Uk = pl[1] * JKx + pl[2] * JKy + pl[3] * JKz;
-    double co = Uk * pl[0];
-    fc[0] = 0.5 * co;
-    fc[1] = 0.5 * (co * pl[1] + pl[4] * JKx);
-    fc[2] = 0.5 * (co * pl[2] + pl[4] * JKy);
-    fc[3] = 0.5 * (co * pl[3] + pl[4] * JKz);
-    fc[4] = 0.5 * Uk * (pl[4] + pl[NV]);
-#pragma unroll
-    for (int l = 5; l < NV; ++l) fc[l] = 0.5 * co * pl[l];
-    JKx = jr * mr[0]; JKy = jr * mr[1]; JKz = jr * mr[2];
-    Uk = pr[1] * JKx + pr[2] * JKy + pr[3] * JKz;
-    co = Uk * pr[0];
-    fc[0] += 0.5 * co;
-    fc[1] += 0.5 * (co * pr[1] + pr[4] * JKx);
-    fc[2] += 0.5 * (co * pr[2] + pr[4] * JKy);
-    fc[3] += 0.5 * (co * pr[3] + pr[4] * JKz);
-    fc[4] += 0.5 * Uk * (pr[4] + pr[NV]);
-#pragma unroll
-    for (int l = 5; l < NV; ++l) fc[l] += 0.5 * co * pr[l];
-  }
-  const double dl = sqrt(pl[0]), dr = sqrt(pr[0]);
-  const double idn = 1.0 / (dl + dr);
-  const double u = (dl * pl[1] + dr * pr[1]) * idn, v = (dl * pl[2] + dr * pr[2]) * idn,
-               w = (dl * pl[3] + dr * pr[3]) * idn;
-  const double ek = 0.5 * (u * u + v * v + w * w);
-  const double hl = (pl[NV] + pl[4]) / pl[0], hr = (pr[NV] + pr[4]) / pr[0];
-  const double h = (dl * hl + dr * hr) * idn;
-  double gamma = kGammaAir;
-  double c = sqrt((gamma - 1) * (h - ek));
-  double svm[NS > 0 ? NS : 1], alpha[NS > 0 ? NS : 1], ecoef[NS > 0 ? NS : 1];
-  if constexpr (NS > 0) {
-    double r = 0;
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      svm[s] = (dl * pl[5 + s] + dr * pr[5 + s]) * idn;
-      r += svm[s] * __ldg(p.mech.gas_const + s);
-    }
-    const double t = (dl * (pl[4] / pl[0]) + dr * (pr[4] / pr[0])) * idn / fmax(r, 1e-12);
-    characteristic_thermo<NS>(t, svm, p.mech, gamma, c, alpha, ecoef, nullptr);
-  }
-  double kx = 0.5 * (ml[0] + mr[0]), ky = 0.5 * (ml[1] + mr[1]), kz = 0.5 * (ml[2] + mr[2]);
-  const double gk = sqrt(kx * kx + ky * ky + kz * kz);
-  double Uk = kx * u + ky * v + kz * w;
-  double ch[3] = {Uk - gk * c, Uk, Uk + gk * c};
-  const double efd = 0.5 * (efl + efr);
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    ch[a] = fabs(ch[a]);
-    if (ch[a] < efd) ch[a] = 0.5 * (ch[a] * ch[a] / efd + efd);
-  }
-  kx /= gk; ky /= gk; kz /= gk; Uk /= gk;
-  const double ja = 0.5 * (jl + jr);
-  double dq[NV];
-  dq[0] = ja * (pr[0] - pl[0]);
-#pragma unroll
-  for (int l = 1; l < NV; ++l) dq[l] = ja * (pr[0] * pr[l] - pl[0] * pl[l]);
-  dq[4] = ja * (pr[NV] - pl[NV]);
-  double c1 = (gamma - 1) * (ek * dq[0] - u * dq[1] - v * dq[2] - w * dq[3] + dq[4]) / (c * c);
-  double c2 = (kx * dq[1] + ky * dq[2] + kz * dq[3] - Uk * dq[0]) / c;
-  if constexpr (NS > 0) {
-#pragma unroll
-    for (int s = 0; s < NS; ++s) c1 += alpha[s] * dq[s + 5];
-  }
-  double c3 = dq[0] - c1;
-  double b[NV];
-  {
-    double L[NV];
-    L[0] = 0.5 * (c1 - c2);
-    L[1] = kx * c3 - ((kz * v - ky * w) * dq[0] - kz * dq[2] + ky * dq[3]) / c;
-    L[2] = ky * c3 - ((kx * w - kz * u) * dq[0] - kx * dq[3] + kz * dq[1]) / c;
-    L[3] = kz * c3 - ((ky * u - kx * v) * dq[0] - ky * dq[1] + kx * dq[2]) / c;
-    L[4] = 0.5 * (c1 + c2);
-    if constexpr (NS > 0) {
-#pragma unroll
-      for (int s = 0; s < NS; ++s) L[s + 5] = dq[s + 5] - svm[s] * dq[0];
-    }
-    b[0] = -ch[0] * L[0];
-#pragma unroll
-    for (int l = 1; l < NV; ++l) b[l] = -ch[1] * L[l];
-    b[4] = -ch[2] * L[4];
-  }
-  const double c0 = kx * b[1] + ky * b[2] + kz * b[3];
-  c1 = c0 + b[0] + b[4];
-  c2 = c * (b[4] - b[0]);
-  c3 = 0;
-  if constexpr (NS > 0) {
-#pragma unroll
-    for (int s = 0; s < NS; ++s) c3 += ecoef[s] * b[s + 5];
-  }
-  fc[0] += 0.5 * c1;
-  fc[1] += 0.5 * (u * c1 + kx * c2 - c * (kz * b[2] - ky * b[3]));
-  fc[2] += 0.5 * (v * c1 + ky * c2 - c * (kx * b[3] - kz * b[1]));
-  fc[3] += 0.5 * (w * c1 + kz * c2 - c * (ky * b[1] - kx * b[2]));
-  fc[4] += 0.5 * (h * c1 + Uk * c2 - c * c * c0 / (gamma - 1) +
-                  c * ((kz * v - ky * w) * b[1] + (kx * w - kz * u) * b[2] + (ky * u - kx * v) * b[3]) + c3);
-  if constexpr (NS > 0) {
-#pragma unroll
-    for (int s = 0; s < NS; ++s) fc[5 + s] += 0.5 * (b[s + 5] + svm[s] * c1);
-  }
-}
-
-__device__ __forceinline__ void lax_friedrichs_air(const double *pl, const double *pr, const double *ml,
-                                                   const double *mr, double jl, double jr, double *fc) {
-  constexpr int NV = 5;
-  const double kx = 0.5 * (ml[0] + mr[0]), ky = 0.5 * (ml[1] + mr[1]), kz = 0.5 * (ml[2] + mr[2]);
-  const double gk = sqrt(kx * kx + ky * ky + kz * kz);
-  const double Ukl = pl[1] * kx + pl[2] * ky + pl[3] * kz, Ukr = pr[1] * kx + pr[2] * ky + pr[3] * kz;
-  const double cl = sqrt(kGammaAir * pl[4] / pl[0]), cr = sqrt(kGammaAir * pr[4] / pr[0]);
-  const double sr = fmax(fabs(Ukl) + cl * gk, fabs(Ukr) + cr * gk);
-  const double hj = 0.5 * 0.5 * (jl + jr);
-  const double rUl = pl[0] * Ukl, rUr = pr[0] * Ukr;
-  fc[0] = (rUl + rUr - sr * (pr[0] - pl[0])) * hj;
-  fc[1] = (rUl * pl[1] + rUr * pr[1] + kx * (pl[4] + pr[4]) - sr * (pr[1] * pr[0] - pl[1] * pl[0])) * hj;
-  fc[2] = (rUl * pl[2] + rUr * pr[2] + ky * (pl[4] + pr[4]) - sr * (pr[2] * pr[0] - pl[2] * pl[0])) * hj;
-  fc[3] = (rUl * pl[3] + rUr * pr[3] + kz * (pl[4] + pr[4]) - sr * (pr[3] * pr[0] - pl[3] * pl[0])) * hj;
-  fc[4] = ((pl[NV] + pl[4]) * Ukl + (pr[NV] + pr[4]) * Ukr - sr * (pr[NV] - pl[NV])) * hj;
-}
-
-// Half-width of the node-centred reconstruction stencil.
-template <int REC>
-__host__ __device__ constexpr int pv_half_width() { return REC == 1 ? 0 : (REC <= 3 ? 1 : REC / 2); }
-
-template <int NS, int DIR, int REC, int SOLVER>
-__global__ void __launch_bounds__(kSweepThreads) k_inviscid_pv(Zone z, Param p, idx_t run) {
-  constexpr int NV = 5 + NS;
-  constexpr int RH = pv_half_width<REC>();
-  constexpr int NN = DIR == 0 ? (kSweepThreads + 2 * RH) : kNI * (kNS + 2 * RH);
-  constexpr int NSLOT = NV + 4 + (SOLVER == CB2_INV_ROE ? 1 : 0);
-  extern __shared__ double smem[];
-  double *sN = smem;                          // node data [NSLOT][NN]
-  double *sR = sN + NSLOT * NN;               // right state at n-1/2 of each thread's node [NV+2][T]
-  double *sF = sR + (NV + 2) * kSweepThreads; // interface flux between a node and the next [NV][T]
-  const int tid = threadIdx.x;
-  const int g = z.ngg;
-  const Layout &L = z.L;
-  const idx_t sz = L.sz;
-
-  auto load = [&](idx_t gi, int slot, int i, int j, int k) {
-#pragma unroll
-    for (int l = 0; l < 5; ++l) sN[l * NN + slot] = z.bv[gi + l * sz];
-#pragma unroll
-    for (int s = 0; s < NS; ++s) sN[(5 + s) * NN + slot] = z.sv[gi + s * sz];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) sN[(NV + c) * NN + slot] = z.metric[gi + (3 * DIR + c) * sz];
-    sN[(NV + 3) * NN + slot] = z.jac[gi];
-    if constexpr (SOLVER == CB2_INV_ROE) {
-      // entropy-fix delta exists on [-1, m] only (ghost width 1)
-      const bool in1 = i >= -1 && i <= z.mx && j >= -1 && j <= z.my && k >= -1 && k <= z.mz;
-      sN[(NV + 4) * NN + slot] = in1 ? z.efd[z.L1.at(i, j, k)] : 0.0;
-    }
-  };
-
-  // Thread tid owns node n.  rec: n lies in [-1, m] along the sweep (both of its faces are
-  // needed); face: the interface n+1/2 is an interior face, i.e. n in [-1, m-1], and node n+1
-  // belongs to this CTA; upd: n in [0, m-1] is updated from the faces n-1/2 and n+1/2.
-  int i, j, k, n, ms, tpos;
-  bool inside;
-  int c, st;
-  if constexpr (DIR == 0) {
-    k = blockIdx.z;
-    const idx_t q0 = (idx_t)blockIdx.x * (kSweepThreads - 2) - 1;
-    const idx_t base = (idx_t)k * L.disp1 + L.dispt - g;
-    const idx_t qlo = q0 - RH;
-    const idx_t qmin = -(idx_t)g * L.disp2, qmax = (idx_t)(L.my + g) * L.disp2;
-    for (int s = tid; s < NN; s += kSweepThreads) {
-      const idx_t q = qlo + s;
-      if (q >= qmin && q < qmax) {
-        const idx_t jj = q >= 0 ? q / L.disp2 : -((-q + L.disp2 - 1) / L.disp2);
-        load(base + q, s, (int)(q - jj * L.disp2) - g, (int)jj, k);
-      }
-    }
-    const idx_t q = q0 + tid;
-    const idx_t jj = q >= 0 ? q / L.disp2 : -1;
-    i = (int)(q - jj * L.disp2) - g;
-    j = (int)jj;
-    n = i;
-    ms = L.mx;
-    inside = q >= 0 && q < run;
-    tpos = tid;
-    c = tid + RH;
-    st = 1;
-  } else {
-    const int ti = tid % kNI, ts = tid / kNI;
-    i = blockIdx.x * kNI + ti;
-    const int s0 = blockIdx.y * (kNS - 2) - 1;
-    ms = DIR == 1 ? L.my : L.mz;
-    if (DIR == 1) k = blockIdx.z; else j = blockIdx.z;
-    for (int s = ts; s < kNS + 2 * RH; s += kNS) {
-      const int nn = s0 - RH + s;
-      if (i < L.mx && nn < ms + g) {
-        if (DIR == 1) load(L.at(i, nn, k), s * kNI + ti, i, nn, k);
-        else load(L.at(i, j, nn), s * kNI + ti, i, j, nn);
-      }
-    }
-    n = s0 + ts;
-    if (DIR == 1) j = n; else k = n;
-    inside = i < L.mx;
-    tpos = ts;
-    c = (ts + RH) * kNI + ti;
-    st = kNI;
-  }
-  const bool rec = inside && n >= -1 && n <= ms;
-  const bool face = rec && n <= ms - 1 && tpos < (DIR == 0 ? kSweepThreads : kNS) - 1;
-  const bool upd = face && n >= 0 && tpos >= 1;
-  __syncthreads();
-
-  double pl[NV + 2];
-  if (rec) {
-    double pr[NV + 2];
-    reconstruct_node<NS, REC>(sN, NN, c, st, p, pl, pr);
-    state_energy<NS>(pl, p.mech);
-    state_energy<NS>(pr, p.mech);
-#pragma unroll
-    for (int v = 0; v < NV + 2; ++v) sR[v * kSweepThreads + tid] = pr[v];
-  }
-  __syncthreads();
-
-  if (face) {
-    const int tn = tid + st;  // the thread of node n+1 (st is 1 or kNI, as the thread layout)
-    double pr[NV + 2];
-#pragma unroll
-    for (int v = 0; v < NV + 2; ++v) pr[v] = sR[v * kSweepThreads + tn];
-    const double ml[3] = {sN[NV * NN + c], sN[(NV + 1) * NN + c], sN[(NV + 2) * NN + c]};
-    const double mr[3] = {sN[NV * NN + c + st], sN[(NV + 1) * NN + c + st], sN[(NV + 2) * NN + c + st]};
-    const double jl = sN[(NV + 3) * NN + c], jr = sN[(NV + 3) * NN + c + st];
-    double fc[NV];
-    if constexpr (SOLVER == CB2_INV_AUSMP) ausm_plus<NS>(pl, pr, ml, mr, jl, jr, fc);
-    else if constexpr (SOLVER == CB2_INV_HLLC) hllc<NS>(pl, pr, ml, mr, jl, jr, p.mech, fc);
-    else if constexpr (SOLVER == CB2_INV_ROE)
-      roe_flux<NS>(pl, pr, ml, mr, jl, jr, sN[(NV + 4) * NN + c], sN[(NV + 4) * NN + c + st], p, fc);
-    else lax_friedrichs_air(pl, pr, ml, mr, jl, jr, fc);
-#pragma unroll
-    for (int v = 0; v < NV; ++v) sF[v * kSweepThreads + tid] = fc[v];
-  }
-  __syncthreads();
-
-  if (upd) {
-    const int tprev = tid - st;
-    const idx_t gd = z.L0.at(i, j, k);
-    const idx_t sz0 = z.L0.sz;
-#pragma unroll
-    for (int v = 0; v < NV; ++v) z.dq[gd + v * sz0] -= sF[v * kSweepThreads + tid] - sF[v * kSweepThreads + tprev];
-  }
-}
-
-// Entropy-fix delta of the Roe scheme on [-1, m] in every direction (ghost width 1).
-template <int NS>
-__global__ void k_entropy_fix_delta(Zone z, Param p) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x - 1, j = blockIdx.y - 1, k = blockIdx.z - 1;
-  if (i > z.mx) return;
-  const idx_t g = z.L.at(i, j, k), sz = z.L.sz;
-  const double *M = z.metric + g;
-  const double u = z.bv[g + sz], v = z.bv[g + 2 * sz], w = z.bv[g + 3 * sz];
-  const double U = fabs(u * M[0] + v * M[sz] + w * M[2 * sz]);
-  const double V = fabs(u * M[3 * sz] + v * M[4 * sz] + w * M[5 * sz]);
-  const double W = fabs(u * M[6 * sz] + v * M[7 * sz] + w * M[8 * sz]);
-  const double kx = norm3d(M[0], M[sz], M[2 * sz]);
-  const double ky = norm3d(M[3 * sz], M[4 * sz], M[5 * sz]);
-  const double kz = norm3d(M[6 * sz], M[7 * sz], M[8 * sz]);
-  double a;
-  if constexpr (NS == 0) a = sqrt(kGammaAir * z.bv[g + 4 * sz] / z.bv[g]);
-  else a = z.acoustic[g];
-  double d;
-  if (p.dim == 2) d = p.entropy_fix_factor * (U + V + a * 0.5 * (kx + ky));
-  else d = p.entropy_fix_factor * (U + V + W + a * (kx + ky + kz) / 3.0);
-  z.efd[z.L1.at(i, j, k)] = d;
-}
-
-template <int NS, int REC, int SOLVER>
-static int launch_pv_dirs(const Zone &z, const Param &p, cudaStream_t s, int &nl) {
-  constexpr int NV = 5 + NS;
-  constexpr int RH = pv_half_width<REC>();
-  constexpr int NSLOT = NV + 4 + (SOLVER == CB2_INV_ROE ? 1 : 0);
-  if (SOLVER == CB2_INV_ROE) {
-    dim3 grid((z.mx + 2 + 127) / 128, z.my + 2, z.mz + 2);
-    ProfScope prof("entropy_fix_delta", s);
-    k_entropy_fix_delta<NS><<<grid, 128, 0, s>>>(z, p);
-    ++nl;
-    CB2_TRY(check_launch());
-  }
-  const int ndir = z.mz > 1 ? 3 : 2;
-  for (int d = 0; d < ndir; ++d) {
-    SweepGeom geo;
-    const dim3 grid = node_sweep_grid(d, z.L, geo);
-    const size_t smem =
-        sizeof(double) * ((size_t)NSLOT * node_sweep_nodes(d, RH) + (size_t)(2 * NV + 2) * kSweepThreads);
-    static const char *names[3] = {"pv_flux_x", "pv_flux_y", "pv_flux_z"};
-    ProfScope prof(names[d], s);
-    if (d == 0) {
-      auto kern = k_inviscid_pv<NS, 0, REC, SOLVER>;
-      CB2_TRY(prepare_smem(kern, smem));
-      kern<<<grid, kSweepThreads, smem, s>>>(z, p, geo.run);
-    } else if (d == 1) {
-      auto kern = k_inviscid_pv<NS, 1, REC, SOLVER>;
-      CB2_TRY(prepare_smem(kern, smem));
-      kern<<<grid, kSweepThreads, smem, s>>>(z, p, 0);
-    } else {
-      auto kern = k_inviscid_pv<NS, 2, REC, SOLVER>;
-      CB2_TRY(prepare_smem(kern, smem));
-      kern<<<grid, kSweepThreads, smem, s>>>(z, p, 0);
-    }
-    ++nl;
-    CB2_TRY(check_launch());
-  }
-  return CB2_OK;
-}
 
 template <int NS, int SOLVER>
 static int launch_pv_rec(const Zone &z, const Param &p, cudaStream_t s, int &nl) {
   switch (p.reconstruction) {
-    case CB2_REC_MUSCL: return launch_pv_dirs<NS, 2, SOLVER>(z, p, s, nl);
-    case CB2_REC_NND2: return launch_pv_dirs<NS, 3, SOLVER>(z, p, s, nl);
-    case CB2_REC_WENO5: return launch_pv_dirs<NS, 5, SOLVER>(z, p, s, nl);
-    case CB2_REC_WENO7: return launch_pv_dirs<NS, 7, SOLVER>(z, p, s, nl);
-    default: return launch_pv_dirs<NS, 1, SOLVER>(z, p, s, nl);
+    case CB2_REC_MUSCL: return launch_pv_dirs<double, NS, 2, SOLVER>(z, p, s, nl);
+    case CB2_REC_NND2: return launch_pv_dirs<double, NS, 3, SOLVER>(z, p, s, nl);
+    case CB2_REC_WENO5: return launch_pv_dirs<double, NS, 5, SOLVER>(z, p, s, nl);
+    case CB2_REC_WENO7: return launch_pv_dirs<double, NS, 7, SOLVER>(z, p, s, nl);
+    default: return launch_pv_dirs<double, NS, 1, SOLVER>(z, p, s, nl);
   }
 }
 
@@ -554,6 +30,7 @@ static int launch_pv_ns(const Zone &z, const Param &p, cudaStream_t s, int &nl) 
 }
 
 int launch_inviscid_pv(const Zone &z, const Param &p, cudaStream_t s, int &n_launch) {
+  if (p.precision == CB2_PREC_MIXED) return launch_inviscid_pv_f32(z, p, s, n_launch);
   switch (p.n_spec) {
     case 0: return launch_pv_ns<0>(z, p, s, n_launch);
     case 5: return launch_pv_ns<5>(z, p, s, n_launch);

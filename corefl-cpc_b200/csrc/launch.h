@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "common.cuh"
+#include "cb200_serve.h"
 
 namespace cb2 {
 
@@ -68,6 +69,7 @@ struct FaceBC {
 int launch_inviscid_char(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
 int launch_inviscid_comp(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
 int launch_inviscid_pv(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
+int launch_inviscid_pv_f32(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
 int launch_stage_update(const Zone &z, const Param &p, double dt, int rk, cudaStream_t s, int &n_launch);
 int launch_cv_from_bv(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
 int launch_properties(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
@@ -84,5 +86,11 @@ int launch_min_reduce(const double *src, long long n, double *partial, int n_par
                       cudaStream_t s, int &n_launch);
 int min_reduce_partials(long long n);
 int launch_set_value(double *dst, double v, cudaStream_t s, int &n_launch);
+
+// batched 0-D reactors (reactor.cu); the state type is cb2_reactor of cb200_serve.h
+int launch_reactor_setup(const Param &p, cb2_reactor *r, int n, const double *T0, const double *p0,
+                         const double *Y, const double *t_end, double h0, cudaStream_t s);
+int launch_reactor_advance(const Param &p, cb2_reactor *r, int n, int max_attempts, double rtol, double atol,
+                           cudaStream_t s);
 
 }  // namespace cb2

@@ -2,9 +2,7 @@
 // src/FieldOperation.cuh:183-247), the local CFL time step (local_time_step<mix>,
 // src/TimeAdvanceFunc.cuh:28-127) and its global minimum (min_of_arr + global_time_step,
 // src/TimeAdvanceFunc.cu:114-164).
-#include "common.cuh"
-#include "thermo.cuh"
-#include "transport.cuh"
+#include "point.cuh"
 #include "launch.h"
 
 namespace cb2 {
@@ -17,36 +15,7 @@ __global__ void __launch_bounds__(kPropThreads) k_properties(Zone z, Param p) {
   const int i = blockIdx.x * kPropThreads + threadIdx.x - g_;
   const int j = blockIdx.y - g_, k = blockIdx.z - g_;
   if (i >= z.mx + g_) return;
-  const idx_t g = z.L.at(i, j, k), sz = z.L.sz;
-  const double t = z.bv[g + 5 * sz];
-  const double V = norm3d(z.bv[g + sz], z.bv[g + 2 * sz], z.bv[g + 3 * sz]);
-  if constexpr (NS == 0) {
-    z.mul[g] = p.mu_constant > 0 ? p.mu_constant : sutherland(t);
-    if (z.mach) z.mach[g] = V / sqrt(kGammaAir * kRu / kMwAir * t);
-  } else {
-    double cp[NS], y[NS];
-    nasa7_cp<NS>(t, p.mech, cp);
-    double imw = 0, cpt = 0;
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      y[s] = z.sv[g + s * sz];
-      imw = fma(y[s], __ldg(p.mech.imw + s), imw);
-      cpt = fma(y[s], cp[s], cpt);
-    }
-    const double mw = 1 / fmax(imw, 1e-12);
-    const double R = kRu * imw;
-    const double gam = cpt / (cpt - R);
-    z.gamma[g] = gam;
-    const double c = sqrt(gam * R * t);
-    z.acoustic[g] = c;
-    if (z.mach) z.mach[g] = V / c;
-    double mu, kappa, rhoD[NS];
-    transport_properties<NS>(t, z.bv[g + 4 * sz], mw, y, cp, p.mech, mu, kappa, rhoD);
-    z.mul[g] = mu;
-    z.kappa[g] = kappa;
-#pragma unroll
-    for (int s = 0; s < NS; ++s) z.rhoD[g + s * sz] = rhoD[s];
-  }
+  properties_point<NS>(z, p, i, j, k);
 }
 
 int launch_properties(const Zone &z, const Param &p, cudaStream_t s, int &n_launch) {
@@ -72,51 +41,7 @@ __global__ void __launch_bounds__(kPropThreads) k_local_dt(Zone z, Param p) {
   const int i = blockIdx.x * kPropThreads + threadIdx.x;
   const int j = blockIdx.y, k = blockIdx.z;
   if (i >= z.mx) return;
-  const idx_t g = z.L.at(i, j, k), sz = z.L.sz;
-  const double *M = z.metric;
-  const double gxi = norm3d(M[g], M[g + sz], M[g + 2 * sz]);
-  const double geta = norm3d(M[g + 3 * sz], M[g + 4 * sz], M[g + 5 * sz]);
-  const double gzeta = norm3d(M[g + 6 * sz], M[g + 7 * sz], M[g + 8 * sz]);
-  const double u = z.bv[g + sz], v = z.bv[g + 2 * sz], w = z.bv[g + 3 * sz];
-  const double U = u * M[g] + v * M[g + sz] + w * M[g + 2 * sz];
-  const double Vc = u * M[g + 3 * sz] + v * M[g + 4 * sz] + w * M[g + 5 * sz];
-  const double W = u * M[g + 6 * sz] + v * M[g + 7 * sz] + w * M[g + 8 * sz];
-  double a;
-  if constexpr (NS == 0) a = sqrt(kGammaAir * kRAir * z.bv[g + 5 * sz]);
-  else a = z.acoustic[g];
-  const bool d3 = z.mz != 1;
-  double lam = fmax(fabs(U) + a * gxi, fabs(Vc) + a * geta);
-  if (d3) lam = fmax(lam, fabs(W) + a * gzeta);
-  if (p.viscous_order > 0) {
-    double len = fmax(gxi, geta);
-    if (d3) len = fmax(len, gzeta);
-    const double irho = 1.0 / z.bv[g];
-    double dv;
-    if constexpr (NS == 0) {
-      dv = fmax(kGammaAir, 4.0 / 3.0) * irho;
-      dv *= z.mul[g] / p.Pr;
-    } else {
-      double cp[NS];
-      nasa7_cp<NS>(z.bv[g + 5 * sz], p.mech, cp);
-      double cpt = 0, mrd = 0;
-      for (int s = 0; s < NS; ++s) {
-        cpt += cp[s] * z.sv[g + s * sz];
-        mrd = fmax(mrd, z.rhoD[g + s * sz]);
-      }
-      dv = z.mul[g] * irho;
-      dv = fmax(dv, z.kappa[g] * irho * z.gamma[g] / cpt);
-      dv = fmax(dv, mrd * irho);
-    }
-    lam = fmax(lam, len * len * dv);
-  }
-  double dt = p.cfl / lam;
-  if constexpr (NS > 0) {
-    if (p.n_reac > 0 && z.rts) {
-      const double rdt = p.cfl * z.rts[g];
-      if (rdt > 1e-20 && rdt < 1e-5) dt = fmin(dt, rdt);
-    }
-  }
-  z.dtl[z.L0.at(i, j, k)] = dt;
+  z.dtl[z.L0.at(i, j, k)] = local_dt_point<NS>(z, p, i, j, k);
 }
 
 int launch_local_dt(const Zone &z, const Param &p, cudaStream_t s, int &n_launch) {

@@ -17,21 +17,22 @@ namespace cb2 {
 
 // ---- 8th-order derivative along one index direction ---------------------------------
 // f(m) returns the field at offset m along the direction; n = node index, nx = extent.
-template <typename F>
-__device__ __forceinline__ double d8(F f, int n, int nx, bool bl, bool br) {
+template <typename T, typename F>
+__device__ __forceinline__ T d8(F f, int n, int nx, bool bl, bool br) {
   if (bl) {
-    if (n == 0) return -25.0 / 12 * f(0) + 4.0 * f(1) - 3 * f(2) + 4.0 / 3 * f(3) - 0.25 * f(4);
-    if (n == 1) return -0.25 * f(-1) - 5.0 / 6 * f(0) + 1.5 * f(1) - 0.5 * f(2) + 1.0 / 12 * f(3);
-    if (n == 2) return -1.0 / 12 * (f(2) - f(-2)) + 2.0 / 3 * (f(1) - f(-1));
-    if (n == 3) return 0.75 * (f(1) - f(-1)) - 0.15 * (f(2) - f(-2)) + 1.0 / 60 * (f(3) - f(-3));
+    if (n == 0) return T(-25.0 / 12) * f(0) + T(4.0) * f(1) - 3 * f(2) + T(4.0 / 3) * f(3) - T(0.25) * f(4);
+    if (n == 1) return T(-0.25) * f(-1) - T(5.0 / 6) * f(0) + T(1.5) * f(1) - T(0.5) * f(2) + T(1.0 / 12) * f(3);
+    if (n == 2) return T(-1.0 / 12) * (f(2) - f(-2)) + T(2.0 / 3) * (f(1) - f(-1));
+    if (n == 3) return T(0.75) * (f(1) - f(-1)) - T(0.15) * (f(2) - f(-2)) + T(1.0 / 60) * (f(3) - f(-3));
   }
   if (br) {
-    if (n == nx - 1) return 25.0 / 12 * f(0) - 4.0 * f(-1) + 3 * f(-2) - 4.0 / 3 * f(-3) + 0.25 * f(-4);
-    if (n == nx - 2) return 0.25 * f(1) + 5.0 / 6 * f(0) - 1.5 * f(-1) + 0.5 * f(-2) - 1.0 / 12 * f(-3);
-    if (n == nx - 3) return -1.0 / 12 * (f(2) - f(-2)) + 2.0 / 3 * (f(1) - f(-1));
-    if (n == nx - 4) return 0.75 * (f(1) - f(-1)) - 0.15 * (f(2) - f(-2)) + 1.0 / 60 * (f(3) - f(-3));
+    if (n == nx - 1) return T(25.0 / 12) * f(0) - T(4.0) * f(-1) + 3 * f(-2) - T(4.0 / 3) * f(-3) + T(0.25) * f(-4);
+    if (n == nx - 2) return T(0.25) * f(1) + T(5.0 / 6) * f(0) - T(1.5) * f(-1) + T(0.5) * f(-2) - T(1.0 / 12) * f(-3);
+    if (n == nx - 3) return T(-1.0 / 12) * (f(2) - f(-2)) + T(2.0 / 3) * (f(1) - f(-1));
+    if (n == nx - 4) return T(0.75) * (f(1) - f(-1)) - T(0.15) * (f(2) - f(-2)) + T(1.0 / 60) * (f(3) - f(-3));
   }
-  return 0.8 * (f(1) - f(-1)) + -0.2 * (f(2) - f(-2)) + 4.0 / 105 * (f(3) - f(-3)) + -1.0 / 280 * (f(4) - f(-4));
+  return T(0.8) * (f(1) - f(-1)) + T(-0.2) * (f(2) - f(-2)) + T(4.0 / 105) * (f(3) - f(-3)) +
+         T(-1.0 / 280) * (f(4) - f(-4));
 }
 
 struct BFlags {
@@ -52,6 +53,9 @@ __device__ __forceinline__ BFlags bflags(const Zone &z, int i, int j, int k) {
 constexpr int kVisThreads = 128;
 
 // Node fluxes of the momentum and energy equations (air); comps 1..4 of fFlux/gFlux/hFlux.
+// T is the arithmetic type (double: plain form; float: mixed form, FP64 arrays read and
+// written, the stencils, stresses and fluxes evaluated in FP32).
+template <typename T>
 __global__ void __launch_bounds__(kVisThreads) k_visc8_node_flux_air(Zone z, Param p) {
   const int i = blockIdx.x * kVisThreads + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
   if (i >= z.mx) return;
@@ -59,44 +63,44 @@ __global__ void __launch_bounds__(kVisThreads) k_visc8_node_flux_air(Zone z, Par
   const idx_t sz = L.sz, g = L.at(i, j, k);
   const BFlags b = bflags(z, i, j, k);
   const idx_t si = 1, sj = L.disp2, sk = L.disp1;
-  auto der = [&](int comp, double &dxi, double &deta, double &dzeta) {
+  auto der = [&](int comp, T &dxi, T &deta, T &dzeta) {
     const double *f = z.bv + comp * sz + g;
-    dxi = d8([&](int m) { return f[m * si]; }, i, z.mx, b.il, b.ir);
-    deta = d8([&](int m) { return f[m * sj]; }, j, z.my, b.jl, b.jr);
-    dzeta = d8([&](int m) { return f[m * sk]; }, k, z.mz, b.kl, b.kr);
+    dxi = d8<T>([&](int m) { return T(f[m * si]); }, i, z.mx, b.il, b.ir);
+    deta = d8<T>([&](int m) { return T(f[m * sj]); }, j, z.my, b.jl, b.jr);
+    dzeta = d8<T>([&](int m) { return T(f[m * sk]); }, k, z.mz, b.kl, b.kr);
   };
-  double u_xi, u_eta, u_zeta, v_xi, v_eta, v_zeta, w_xi, w_eta, w_zeta, t_xi, t_eta, t_zeta;
+  T u_xi, u_eta, u_zeta, v_xi, v_eta, v_zeta, w_xi, w_eta, w_zeta, t_xi, t_eta, t_zeta;
   der(1, u_xi, u_eta, u_zeta);
   der(2, v_xi, v_eta, v_zeta);
   der(3, w_xi, w_eta, w_zeta);
   der(5, t_xi, t_eta, t_zeta);
   const double *M = z.metric + g;
-  const double xi_x = M[0], xi_y = M[sz], xi_z = M[2 * sz];
-  const double eta_x = M[3 * sz], eta_y = M[4 * sz], eta_z = M[5 * sz];
-  const double zeta_x = M[6 * sz], zeta_y = M[7 * sz], zeta_z = M[8 * sz];
-  const double u_x = u_xi * xi_x + u_eta * eta_x + u_zeta * zeta_x;
-  const double u_y = u_xi * xi_y + u_eta * eta_y + u_zeta * zeta_y;
-  const double u_z = u_xi * xi_z + u_eta * eta_z + u_zeta * zeta_z;
-  const double v_x = v_xi * xi_x + v_eta * eta_x + v_zeta * zeta_x;
-  const double v_y = v_xi * xi_y + v_eta * eta_y + v_zeta * zeta_y;
-  const double v_z = v_xi * xi_z + v_eta * eta_z + v_zeta * zeta_z;
-  const double w_x = w_xi * xi_x + w_eta * eta_x + w_zeta * zeta_x;
-  const double w_y = w_xi * xi_y + w_eta * eta_y + w_zeta * zeta_y;
-  const double w_z = w_xi * xi_z + w_eta * eta_z + w_zeta * zeta_z;
-  const double mu = z.mul[g];
-  const double txx = mu * (4 * u_x - 2 * v_y - 2 * w_z) / 3.0;
-  const double tyy = mu * (4 * v_y - 2 * u_x - 2 * w_z) / 3.0;
-  const double tzz = mu * (4 * w_z - 2 * u_x - 2 * v_y) / 3.0;
-  const double txy = mu * (u_y + v_x), txz = mu * (u_z + w_x), tyz = mu * (v_z + w_y);
-  const double t_x = t_xi * xi_x + t_eta * eta_x + t_zeta * zeta_x;
-  const double t_y = t_xi * xi_y + t_eta * eta_y + t_zeta * zeta_y;
-  const double t_z = t_xi * xi_z + t_eta * eta_z + t_zeta * zeta_z;
-  const double cp = kGammaAir * kRAir / (kGammaAir - 1);
-  const double kap = mu / p.Pr * cp;
-  const double u = z.bv[g + sz], v = z.bv[g + 2 * sz], w = z.bv[g + 3 * sz];
-  const double Ex = u * txx + v * txy + w * txz + kap * t_x;
-  const double Ey = u * txy + v * tyy + w * tyz + kap * t_y;
-  const double Ez = u * txz + v * tyz + w * tzz + kap * t_z;
+  const T xi_x = T(M[0]), xi_y = T(M[sz]), xi_z = T(M[2 * sz]);
+  const T eta_x = T(M[3 * sz]), eta_y = T(M[4 * sz]), eta_z = T(M[5 * sz]);
+  const T zeta_x = T(M[6 * sz]), zeta_y = T(M[7 * sz]), zeta_z = T(M[8 * sz]);
+  const T u_x = u_xi * xi_x + u_eta * eta_x + u_zeta * zeta_x;
+  const T u_y = u_xi * xi_y + u_eta * eta_y + u_zeta * zeta_y;
+  const T u_z = u_xi * xi_z + u_eta * eta_z + u_zeta * zeta_z;
+  const T v_x = v_xi * xi_x + v_eta * eta_x + v_zeta * zeta_x;
+  const T v_y = v_xi * xi_y + v_eta * eta_y + v_zeta * zeta_y;
+  const T v_z = v_xi * xi_z + v_eta * eta_z + v_zeta * zeta_z;
+  const T w_x = w_xi * xi_x + w_eta * eta_x + w_zeta * zeta_x;
+  const T w_y = w_xi * xi_y + w_eta * eta_y + w_zeta * zeta_y;
+  const T w_z = w_xi * xi_z + w_eta * eta_z + w_zeta * zeta_z;
+  const T mu = T(z.mul[g]);
+  const T txx = mu * (4 * u_x - 2 * v_y - 2 * w_z) / 3;
+  const T tyy = mu * (4 * v_y - 2 * u_x - 2 * w_z) / 3;
+  const T tzz = mu * (4 * w_z - 2 * u_x - 2 * v_y) / 3;
+  const T txy = mu * (u_y + v_x), txz = mu * (u_z + w_x), tyz = mu * (v_z + w_y);
+  const T t_x = t_xi * xi_x + t_eta * eta_x + t_zeta * zeta_x;
+  const T t_y = t_xi * xi_y + t_eta * eta_y + t_zeta * zeta_y;
+  const T t_z = t_xi * xi_z + t_eta * eta_z + t_zeta * zeta_z;
+  const T cp = T(kGammaAir * kRAir / (kGammaAir - 1));
+  const T kap = mu / T(p.Pr) * cp;
+  const T u = T(z.bv[g + sz]), v = T(z.bv[g + 2 * sz]), w = T(z.bv[g + 3 * sz]);
+  const T Ex = u * txx + v * txy + w * txz + kap * t_x;
+  const T Ey = u * txy + v * tyy + w * tyz + kap * t_y;
+  const T Ez = u * txz + v * tyz + w * tzz + kap * t_z;
   z.fF[g + sz] = xi_x * txx + xi_y * txy + xi_z * txz;
   z.fF[g + 2 * sz] = xi_x * txy + xi_y * tyy + xi_z * tyz;
   z.fF[g + 3 * sz] = xi_x * txz + xi_y * tyz + xi_z * tzz;
@@ -111,6 +115,7 @@ __global__ void __launch_bounds__(kVisThreads) k_visc8_node_flux_air(Zone z, Par
   z.hF[g + 4 * sz] = zeta_x * Ex + zeta_y * Ey + zeta_z * Ez;
 }
 
+template <typename T>
 __global__ void __launch_bounds__(kVisThreads) k_visc8_divergence(Zone z, Param p) {
   const int i = blockIdx.x * kVisThreads + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
   if (i >= z.mx) return;
@@ -118,14 +123,14 @@ __global__ void __launch_bounds__(kVisThreads) k_visc8_divergence(Zone z, Param 
   const idx_t sz = L.sz, g = L.at(i, j, k);
   const BFlags b = bflags(z, i, j, k);
   const idx_t sj = L.disp2, sk = L.disp1;
-  const double jac = z.jac[g];
+  const T jac = T(z.jac[g]);
   const idx_t g0 = z.L0.at(i, j, k), sz0 = z.L0.sz;
   for (int l = 1; l < p.n_var; ++l) {
     const double *f = z.fF + l * sz + g, *gg = z.gF + l * sz + g, *h = z.hF + l * sz + g;
-    const double d = d8([&](int m) { return f[m]; }, i, z.mx, b.il, b.ir) +
-                     d8([&](int m) { return gg[m * sj]; }, j, z.my, b.jl, b.jr) +
-                     d8([&](int m) { return h[m * sk]; }, k, z.mz, b.kl, b.kr);
-    z.dq[g0 + l * sz0] += d * jac;
+    const T d = d8<T>([&](int m) { return T(f[m]); }, i, z.mx, b.il, b.ir) +
+                d8<T>([&](int m) { return T(gg[m * sj]); }, j, z.my, b.jl, b.jr) +
+                d8<T>([&](int m) { return T(h[m * sk]); }, k, z.mz, b.kl, b.kr);
+    z.dq[g0 + l * sz0] += double(d * jac);
   }
 }
 
@@ -302,14 +307,16 @@ int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_fac
     dim3 grid((z.mx + kVisThreads - 1) / kVisThreads, z.my, z.mz);
     {
       ProfScope prof("visc8_node_flux", s);
-      k_visc8_node_flux_air<<<grid, kVisThreads, 0, s>>>(z, p);
+      if (p.precision == CB2_PREC_MIXED) k_visc8_node_flux_air<float><<<grid, kVisThreads, 0, s>>>(z, p);
+      else k_visc8_node_flux_air<double><<<grid, kVisThreads, 0, s>>>(z, p);
     }
     ++nl;
     CB2_TRY(check_launch());
     CB2_TRY(launch_periodic_flux_exchange(z, p, faces, n_faces, s, nl));
     {
       ProfScope prof("visc8_divergence", s);
-      k_visc8_divergence<<<grid, kVisThreads, 0, s>>>(z, p);
+      // the divergence is a load-bound sum of four 9-point stencils: FP64 in both forms
+      k_visc8_divergence<double><<<grid, kVisThreads, 0, s>>>(z, p);
     }
     ++nl;
     return check_launch();

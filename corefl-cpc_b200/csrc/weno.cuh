@@ -120,6 +120,13 @@ __device__ __forceinline__ T weno7_minus(const T *v, T eps, bool shock) {
   return weno7_side(v[6], v[5], v[4], v[3], v[2], v[1], v[0], eps, shock);
 }
 
+// FP32 weights.  The single-division product form needs the product of three or four
+// (eps + beta)^2 terms, which FP32 cannot hold across the dynamic range of a discontinuity.  The
+// FP32 path normalises by the smallest term instead: with r_s = D_min / D_s in (0, 1],
+//   WENO-JS  alpha_s ~ c_s r_s,   WENO-Z  alpha_s ~ c_s (D_min + tau r_s),
+// the same weights up to a common factor, every term bounded by c_s (D_min + tau).
+__device__ __forceinline__ float rcp32(float x) { return __frcp_rn(x); }
+
 // ---- node-centred pair ---------------------------------------------------------------
 // Both one-sided values that the stencil centred on node n produces: the left-biased value at
 // n+1/2 (`lp`, the plus side) and the right-biased value at n-1/2 (`rm`, the minus side).
@@ -141,9 +148,15 @@ __device__ __forceinline__ void weno5_node(const T *v, T eps, T &lp, T &rm) {
   const T b1 = k13 * sq(v[1] + v[3] - 2 * v[2]) + T(0.25) * sq(v[1] - v[3]);
   const T b0 = k13 * sq(v[0] + v[2] - 2 * v[1]) + T(0.25) * sq(v[0] - 4 * v[1] + 3 * v[2]);
   T D0 = sq(eps + b0), D1 = sq(eps + b1), D2 = sq(eps + b2);
-  const T sc = binade_inv(fmax(fmax(D0, D1), D2));
-  D0 *= sc; D1 *= sc; D2 *= sc;
-  const T E2 = D0 * D1, E1 = D0 * D2, E0 = D1 * D2;  // E_r = prod of D over the other sub-stencils
+  T E0, E1, E2;  // weights of the sub-stencils up to a common factor
+  if constexpr (sizeof(T) == 4) {
+    const T Dm = fmin(fmin(D0, D1), D2);
+    E0 = Dm * rcp32(D0); E1 = Dm * rcp32(D1); E2 = Dm * rcp32(D2);
+  } else {
+    const T sc = binade_inv(fmax(fmax(D0, D1), D2));
+    D0 *= sc; D1 *= sc; D2 *= sc;
+    E2 = D0 * D1; E1 = D0 * D2; E0 = D1 * D2;  // prod of D over the other sub-stencils
+  }
   const T w2 = T(0.3) * E2, w1 = T(0.6) * E1, w0 = T(0.1) * E0;
   lp = (w2 * q2 + w1 * q1 + w0 * q0) / (w2 + w1 + w0);
   const T u0 = T(0.1) * E2, u1 = T(0.6) * E1, u2 = T(0.3) * E0;
@@ -172,11 +185,18 @@ __device__ __forceinline__ void weno7_node(const T *u, T eps, T &lp, T &rm) {
                      -u[3] + 3 * u[4] - 3 * u[5] + u[6]);
   T tau = sq(b0 + 3 * b1 - 3 * b2 - b3);  // unchanged by the mirroring
   T D0 = sq(eps + b0), D1 = sq(eps + b1), D2 = sq(eps + b2), D3 = sq(eps + b3);
-  const T sc = binade_inv(fmax(fmax(D0, D1), fmax(D2, D3)));
-  D0 *= sc; D1 *= sc; D2 *= sc; D3 *= sc; tau *= sc;
-  const T D01 = D0 * D1, D23 = D2 * D3;
-  const T E0 = (D0 + tau) * (D1 * D23), E1 = (D1 + tau) * (D0 * D23);
-  const T E2 = (D2 + tau) * (D01 * D3), E3 = (D3 + tau) * (D01 * D2);
+  T E0, E1, E2, E3;  // Z weights of the sub-stencils up to a common factor
+  if constexpr (sizeof(T) == 4) {
+    const T Dm = fmin(fmin(D0, D1), fmin(D2, D3));
+    E0 = Dm + tau * (Dm * rcp32(D0)); E1 = Dm + tau * (Dm * rcp32(D1));
+    E2 = Dm + tau * (Dm * rcp32(D2)); E3 = Dm + tau * (Dm * rcp32(D3));
+  } else {
+    const T sc = binade_inv(fmax(fmax(D0, D1), fmax(D2, D3)));
+    D0 *= sc; D1 *= sc; D2 *= sc; D3 *= sc; tau *= sc;
+    const T D01 = D0 * D1, D23 = D2 * D3;
+    E0 = (D0 + tau) * (D1 * D23); E1 = (D1 + tau) * (D0 * D23);
+    E2 = (D2 + tau) * (D01 * D3); E3 = (D3 + tau) * (D01 * D2);
+  }
   const T w0 = c0 * E0, w1 = c1 * E1, w2 = c2 * E2, w3 = c3 * E3;
   lp = T(1.0 / 12) * (w0 * q0 + w1 * q1 + w2 * q2 + w3 * q3) / (w0 + w1 + w2 + w3);
   const T v0 = c0 * E3, v1 = c1 * E2, v2 = c2 * E1, v3 = c3 * E0;

@@ -44,6 +44,13 @@ def test_init_rejects_bad_arguments(cb200_lib):
     assert cb200_lib.cb2_init(C.byref(p), C.byref(h)) == abi.ERR_INVALID
     p = cases.make_param(viscous_order=3)
     assert cb200_lib.cb2_init(C.byref(p), C.byref(h)) == abi.ERR_INVALID
+    p = cases.make_param(precision=7)
+    assert cb200_lib.cb2_init(C.byref(p), C.byref(h)) == abi.ERR_INVALID
+    # the mixed form covers the WENO5/7 primitive sweeps; the characteristic path stays FP64 only
+    p = cases.make_param(inviscid_scheme=abi.INV_WENO5_CH, precision=abi.PREC_MIXED)
+    assert cb200_lib.cb2_init(C.byref(p), C.byref(h)) == abi.ERR_UNSUPPORTED
+    p = cases.make_param(inviscid_scheme=abi.INV_AUSMP, reconstruction=abi.REC_MUSCL, precision=abi.PREC_MIXED)
+    assert cb200_lib.cb2_init(C.byref(p), C.byref(h)) == abi.ERR_UNSUPPORTED
     assert not h.value
 
 

@@ -1,0 +1,103 @@
+"""Mixed-precision form: FP32 reconstruction, Riemann fluxes and 8th-order viscous stencils on
+the FP64 field arrays, with the FP64 stage update and temperature.
+
+The mixed form is not meant to match the FP64 oracle to 1e-12; its bar is the accuracy of the
+whole solve.  These tests state the bounds it meets:
+- one right-hand side against the FP64 oracle, relative to each variable's largest |dq|;
+- 100 RK3 steps of the sine wave: the L1 density difference from the FP64 GPU path (which the
+  parity tests tie to the oracle at 1e-12 per stage) stays below 1e-6 of the mean density;
+- a mixed step keeps every node physical (no status bits).
+"""
+import math
+
+import numpy as np
+import pytest
+
+import cb200
+from cb200 import abi, cases
+from cb200.field import DeviceBlock
+
+import helpers
+
+pytestmark = pytest.mark.gpu
+
+# FP32 carries about 7 significant digits; the flux difference of a smooth field loses about
+# one more to cancellation on these coarse grids (the case has a jump at the non-periodic z
+# faces, where the nonlinear weights work hardest).
+RHS_TOL = 5e-5
+
+MIXED_SCHEMES = [
+    ("ausm_weno7", abi.INV_AUSMP, abi.REC_WENO7, 0),
+    ("ausm_weno7_visc8", abi.INV_AUSMP, abi.REC_WENO7, 8),
+    ("ausm_weno5", abi.INV_AUSMP, abi.REC_WENO5, 0),
+    ("hllc_weno5", abi.INV_HLLC, abi.REC_WENO5, 0),
+    ("hllc_weno7", abi.INV_HLLC, abi.REC_WENO7, 0),
+    ("roe_weno5", abi.INV_ROE, abi.REC_WENO5, 0),
+]
+
+
+def _sync():
+    import torch
+    torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("name,scheme,rec,visc", MIXED_SCHEMES, ids=[s[0] for s in MIXED_SCHEMES])
+def test_mixed_rhs_close_to_fp64_oracle(oracle_lib, name, scheme, rec, visc):
+    p, hb, faces = helpers.curvilinear_air_case(20, 18, 16, scheme=scheme, reconstruction=rec, viscous_order=visc,
+                                                bc="periodic", seed=3, jump=False)
+    oracle_lib.boundary(p, hb, faces)
+    dev = DeviceBlock(hb)
+    pm = abi.ParamView.from_buffer_copy(p)
+    pm.precision = abi.PREC_MIXED
+    ctx = cb200.Context(pm)
+    ctx.bind(0, dev.view(), faces)
+    ctx.rhs(0)
+    _sync()
+    oracle_lib.rhs(p, hb, faces)
+    dq = dev.to_host(["dq"])["dq"]
+    ref = hb.a["dq"]
+    per_var = [float(np.abs(dq[v] - ref[v]).max() / np.abs(ref[v]).max()) for v in range(dq.shape[0])]
+    worst = int(np.argmax(per_var))
+    loc = np.unravel_index(int(np.argmax(np.abs(dq[worst] - ref[worst]))), ref[worst].shape)
+    err = max(per_var)
+    print(name, "per-variable error", per_var, "worst at", worst, loc)
+    assert 0 < err < RHS_TOL, (per_var, worst, loc)  # not bit-equal (FP32 arithmetic ran), but close
+    ctx.close()
+
+
+def test_mixed_sine_wave_l1_density_within_1e6():
+    import torch
+    n, steps = 48, 100
+    case = cases.sine_wave(n=n)
+    p, hb, faces = case.param, case.blocks[0], case.faces[0]
+    g = hb.ngg
+    dev = DeviceBlock(hb)
+    init = {k: dev.t[k].clone() for k in ("cv", "bv")}
+    pm = abi.ParamView.from_buffer_copy(p)
+    pm.precision = abi.PREC_MIXED
+    c64, c32 = cb200.Context(p), cb200.Context(pm)
+    c64.bind(0, dev.view(), faces)
+    c32.bind(0, dev.view(), faces)
+    c64.properties(0)
+    dt = c64.cfl_dt()
+    rho = {}
+    for name, ctx in (("fp64", c64), ("mixed", c32)):
+        for k, t in init.items():
+            dev.t[k].copy_(t)
+        c64.properties(0)
+        for _ in range(steps):
+            ctx.rk3_step(dt, True)
+        _sync()
+        assert ctx.read_status() == 0
+        rho[name] = dev.t["bv"][0, g:-g, g:-g, g:-g].clone()
+    d = (rho["mixed"] - rho["fp64"]).abs()
+    l1 = float(d.mean() / rho["fp64"].abs().mean())
+    assert 0 < l1 <= 1e-6, l1
+    # both forms are equally far from the exact advected profile (the scheme's own error)
+    xyz = torch.from_numpy(case.meta["xyz_sum"][g:-g, g:-g, g:-g].copy()).to(d.device)
+    ex = 1.0 + 0.2 * torch.sin(2 * math.pi * (xyz - 3.0 * steps * dt))
+    e64 = float((rho["fp64"] - ex).abs().mean())
+    e32 = float((rho["mixed"] - ex).abs().mean())
+    assert abs(e32 - e64) <= 1e-3 * e64, (e32, e64)
+    c64.close()
+    c32.close()
