@@ -54,3 +54,15 @@ class ParamView(C.Structure):
                 ("entropy_fix_factor", C.c_double), ("Pr", C.c_double), ("cfl", C.c_double),
                 ("rho_ref", C.c_double), ("v_ref", C.c_double), ("mu_constant", C.c_double),
                 ("precision", C.c_int), ("mech", C.POINTER(Mechanism))]
+
+
+# ---- batched solves (include/cb200_serve.h) ---------------------------------------------------
+REACTOR_MAX_SPEC = 9
+REACTOR_DONE, REACTOR_NONPHYSICAL = 1, 2
+
+
+class Reactor(C.Structure):
+    _fields_ = [("rhoY", C.c_double * REACTOR_MAX_SPEC), ("rho", C.c_double), ("E", C.c_double),
+                ("T", C.c_double), ("p", C.c_double), ("time", C.c_double), ("t_end", C.c_double),
+                ("h", C.c_double), ("err_last", C.c_double), ("step", C.c_int), ("n_reject", C.c_int),
+                ("status", C.c_int), ("pad", C.c_int)]

@@ -53,6 +53,8 @@ def load():
         "cb2_profile_reset": (C.c_int, [vp]),
         "cb2_profile_count": (C.c_int, [vp]),
         "cb2_profile_entry": (C.c_int, [vp, C.c_int, C.c_char_p, C.c_int, P(C.c_ulonglong), P(C.c_double)]),
+        "cb2_reactor_setup": (C.c_int, [vp, vp, C.c_int, vp, vp, vp, vp, C.c_double, vp]),
+        "cb2_reactor_advance": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_double, C.c_double, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -114,6 +116,15 @@ class Context:
         d = C.c_double(dt)
         check(self.lib.cb2_rk3_step(self.h, C.byref(d), 1 if fixed_dt else 0, stream), "cb2_rk3_step")
         return d.value
+
+    def reactor_setup(self, reactors, n, T0, p0, Y, t_end, h0=1e-8, stream=None):
+        """Set n reactors (device pointer to abi.Reactor[n]) from device pointers T0, p0, Y
+        (n x n_spec mass fractions) and t_end."""
+        check(self.lib.cb2_reactor_setup(self.h, reactors, n, T0, p0, Y, t_end, h0, stream), "cb2_reactor_setup")
+
+    def reactor_advance(self, reactors, n, max_attempts, rtol=1e-6, atol=1e-12, stream=None):
+        check(self.lib.cb2_reactor_advance(self.h, reactors, n, max_attempts, rtol, atol, stream),
+              "cb2_reactor_advance")
 
     def read_status(self, stream=None):
         f = C.c_uint()

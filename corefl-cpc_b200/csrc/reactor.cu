@@ -180,6 +180,10 @@ __global__ void __launch_bounds__(kReactorThreads) k_reactor_advance(cb2_reactor
   for (int a = 0; a < max_attempts && st.time < st.t_end; ++a) {
     reactor_source<NS>(st.T, rhoY, m, omega, q1, q2);
     const double h = fmin(st.h, st.t_end - st.time);
+    if (!(h > 0) || !isfinite(h)) {
+      st.status |= CB2_REACTOR_NONPHYSICAL;
+      break;
+    }
     // lhs = I - h gamma J, J from the rates of progress of this state
     for (int r = 0; r < NS; ++r) {
       const double mwr = __ldg(m.mw + r);

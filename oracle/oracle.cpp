@@ -1111,10 +1111,11 @@ void gibbs_div_rt(double t, const Mechanism &m, double *g) {
 
 double arrhenius(double t, double A, double b, double Ea) { return A * std::pow(t, b) * std::exp(-Ea / t); }
 
-void chemistry_point(const Mechanism &m, double rho, double t, const double *y, double *omega, double *omega_d) {
+// Forward and backward rates of progress q1, q2 [mol/(cm^3 s)] of every reaction at t [K] and
+// concentrations c [mol/cm^3].
+void rates_of_progress(const Mechanism &m, double t, const double *c, double *q1, double *q2) {
   const int ns = m.n_spec, nr = m.n_reac;
-  double c[16], kf[32], kb[32], q1[32], q2[32];
-  for (int l = 0; l < ns; ++l) c[l] = rho * y[l] * m.imw[l] * 1e-3;
+  double kf[32], kb[32];
   // forward_reaction_rate (:1505-1554), 1T reaction temperature
   for (int i = 0; i < nr; ++i) {
     kf[i] = arrhenius(t, m.A[i], m.b[i], m.Ea[i]);
@@ -1191,6 +1192,13 @@ void chemistry_point(const Mechanism &m, double rho, double t, const double *y, 
     q1[i] *= kf[i];
     if (m.reac_type[i] != 0) q2[i] *= kb[i];
   }
+}
+
+void chemistry_point(const Mechanism &m, double rho, double t, const double *y, double *omega, double *omega_d) {
+  const int ns = m.n_spec, nr = m.n_reac;
+  double c[16], q1[32], q2[32];
+  for (int l = 0; l < ns; ++l) c[l] = rho * y[l] * m.imw[l] * 1e-3;
+  rates_of_progress(m, t, c, q1, q2);
   // chemical_source (:1665-1681)
   for (int i = 0; i < ns; ++i) {
     double creation = 0;
@@ -1251,6 +1259,10 @@ void cv_point(Zone &z, const Param &p, int i, int j, int k) {
 }
 
 }  // namespace
+
+void reaction_rates(const Mechanism &m, double t, const double *c, double *q1, double *q2) {
+  rates_of_progress(m, t, c, q1, q2);
+}
 
 void nasa7_h_cp(double t, const Mechanism &m, double *h, double *cp) {
   // compute_enthalpy_and_cp (src/Thermo.cu:453-523)

@@ -93,4 +93,17 @@ void rk3_step(std::vector<Zone> &zones, const Param &p, double &dt, bool fixed_d
 // thermodynamics used by the tests directly
 void nasa7_h_cp(double t, const Mechanism &m, double *h, double *cp);
 
+// forward/backward rates of progress [mol/(cm^3 s)] of every reaction at t and c [mol/cm^3]
+void reaction_rates(const Mechanism &m, double t, const double *c, double *q1, double *q2);
+
+// 0-D constant-volume reactor (reactor.cpp)
+struct ReactorState {
+  std::vector<double> rhoY;
+  double rho = 0, E = 0, T = 0, p = 0, time = 0, t_end = 0, h = 0, err_last = 0;
+  int step = 0, n_reject = 0, status = 0;
+};
+void reactor_setup(const Mechanism &m, double T0, double p0, const double *Y, double t_end, double h0,
+                   ReactorState &st);
+void reactor_advance(const Mechanism &m, ReactorState &st, int max_attempts, double rtol, double atol);
+
 }  // namespace oracle

@@ -4,6 +4,7 @@
 // The oracle takes the same cb2_param_view / cb2_zone_view / cb2_face_bc structs as the
 // library, with HOST pointers in the zone view.
 #include "oracle.hpp"
+#include "cb200_serve.h"
 #include <cstring>
 #ifdef _OPENMP
 #include <omp.h>
@@ -112,6 +113,24 @@ void oracle_chemistry_source(const cb2_mechanism *m, double rho, double t, const
   pv.n_spec = m->n_spec;
   Param p = make_param(pv);
   chemistry_source(p.mech, rho, t, y, omega, omega_d);
+}
+
+// A 0-D reactor from (T0, p0, Y) advanced by at most max_attempts ROK4E attempts (or to t_end);
+// the state is returned in the cb2_reactor layout of include/cb200_serve.h.
+void oracle_reactor_run(const cb2_mechanism *m, double T0, double p0, const double *Y, double t_end, double h0,
+                        double rtol, double atol, int max_attempts, cb2_reactor *out) {
+  cb2_param_view pv{};
+  pv.mech = m;
+  pv.n_spec = m->n_spec;
+  Param p = make_param(pv);
+  ReactorState st;
+  reactor_setup(p.mech, T0, p0, Y, t_end, h0, st);
+  reactor_advance(p.mech, st, max_attempts, rtol, atol);
+  std::memset(out, 0, sizeof(*out));
+  for (int l = 0; l < m->n_spec; ++l) out->rhoY[l] = st.rhoY[l];
+  out->rho = st.rho; out->E = st.E; out->T = st.T; out->p = st.p;
+  out->time = st.time; out->t_end = st.t_end; out->h = st.h; out->err_last = st.err_last;
+  out->step = st.step; out->n_reject = st.n_reject; out->status = st.status;
 }
 
 }  // extern "C"

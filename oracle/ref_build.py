@@ -23,9 +23,10 @@ def build(ref="/root/reference", force=False):
     os.makedirs(OUT, exist_ok=True)
     exe = os.path.join(OUT, "dump_mech")
     mine = [os.path.join(HERE, "ref", f) for f in ("stubs.cpp", "dump_mech.cpp", "mpi.h")]
+    drivers = [os.path.join(HERE, "ref", f) for f in ("dump_chem.cpp", "dump_reactor.cpp", "chem_stubs.cpp")]
     theirs = [os.path.join(src, f) for f in ("ChemData.cpp", "Parameter.cpp", "Element.cpp",
                                              os.path.join("gxl_lib", "MyString.cpp"))]
-    if not force and os.path.exists(exe) and os.path.getmtime(exe) >= max(os.path.getmtime(f) for f in mine):
+    if not force and os.path.exists(exe) and os.path.getmtime(exe) >= max(os.path.getmtime(f) for f in mine + drivers):
         return exe
     cmd = ["g++", "-std=c++20", "-O1", "-DMAX_SPEC_NUMBER=9", "-DMAX_REAC_NUMBER=20", "-DCombustion2Part",
            "-I", os.path.join(HERE, "ref"), "-I", src,
@@ -42,6 +43,13 @@ def build(ref="/root/reference", force=False):
     r = subprocess.run(cmd2, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("reference host chemistry build failed:\n" + r.stderr[-4000:])
+    # dump_reactor: the same host chemistry driven through the ROK4E reactor sequence
+    exe3 = os.path.join(OUT, "dump_reactor")
+    cmd3 = [c if not c.endswith("dump_chem.cpp") else os.path.join(HERE, "ref", "dump_reactor.cpp") for c in cmd2]
+    cmd3[-1] = exe3
+    r = subprocess.run(cmd3, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("reference reactor driver build failed:\n" + r.stderr[-4000:])
     return exe
 
 

@@ -9,6 +9,10 @@ oracle/ref_build.py) on the reference's example data files and keeps its JSON ou
   h2_chem_states.json : 48 seeded (rho, T, Y) states with the reference's host chemistry
                    source cfd::compute_src, h_k/cp_k from Species::compute_enthalpy_and_cp and
                    the Newton temperature of cfd::update_t (src/ConstVolumeReactor.cpp)
+  h2_reactor_runs.json : 0-D reactors run with the reference's host chemistry, Jacobian, LU
+                   and Newton through the adaptive ROK4E sequence (RTol 1e-6, ATol 1e-12,
+                   first step 1e-8): the reference's example case to 1.2 ms and 8 seeded
+                   (T0, p0, phi) requests to 1 ms, each after 8 step attempts and at the end
 Usage: python tests/golden/make_mech.py [/path/to/reference]
 """
 import os
@@ -53,6 +57,7 @@ def main(ref):
              "therm_file": chem + "therm.dat", "transport_file": chem + "tran.dat"}
     print(run(ref, "h2_li2004.json", files, 7))
     print(run(ref, "h2_chem_states.json", files, 7, prog="dump_chem", extra=("48",)))
+    print(run(ref, "h2_reactor_runs.json", files, 7, prog="dump_reactor", extra=("9",)))
 
 
 if __name__ == "__main__":

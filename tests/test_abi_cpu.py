@@ -1,4 +1,4 @@
-"""The C-ABI library loads and exports every symbol include/cb200.h declares, and argument
+"""The C-ABI library loads and exports every symbol include/*.h declares, and argument
 validation fails cleanly without touching a GPU."""
 import ctypes as C
 import os
@@ -13,9 +13,13 @@ REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared_symbols():
-    hdr = open(os.path.join(REPO, "include", "cb200.h")).read()
-    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
-    return sorted(set(re.findall(r"\b(cb2_\w+)\s*\(", hdr)))
+    names = set()
+    inc = os.path.join(REPO, "include")
+    for f in sorted(os.listdir(inc)):
+        if f.endswith(".h"):
+            hdr = re.sub(r"/\*.*?\*/", "", open(os.path.join(inc, f)).read(), flags=re.S)
+            names.update(re.findall(r"\b(cb2_\w+)\s*\(", hdr))
+    return sorted(names)
 
 
 def test_library_exports_every_declared_symbol(cb200_lib):

@@ -1,0 +1,67 @@
+"""0-D constant-volume reactor (ROK4E, full Jacobian): the oracle restatement against runs of
+the reference's own host functions (tests/golden/h2_reactor_runs.json, written by
+tests/golden/make_mech.py through oracle/_ref/dump_reactor), and against the reference's
+published example result."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from cb200 import mech as mechmod
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = os.path.join(HERE, "golden")
+
+
+@pytest.fixture(scope="module")
+def runs():
+    with open(os.path.join(GOLD, "h2_reactor_runs.json")) as f:
+        return json.load(f)
+
+
+@pytest.fixture(scope="module")
+def h2():
+    return mechmod.load_json(os.path.join(GOLD, "h2_li2004.json"))
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def test_oracle_reactor_first_steps_match_reference(oracle_lib, runs, h2):
+    # the first 8 attempts accept and reject alike; the adaptive step sizes agree to rounding
+    # (the step controller's pow() of the error norm amplifies ulp differences a little)
+    for r in runs["runs"]:
+        st = oracle_lib.reactor_run(h2, r["T0"], r["p0"], r["Y"], r["t_end"], runs["h0"], runs["rtol"], runs["atol"],
+                                    max_attempts=8)
+        g = r["after_8_attempts"]
+        assert st.step == g["step"] and st.n_reject == g["n_reject"]
+        assert abs(st.time - g["time"]) <= 1e-10 * g["time"]
+        assert abs(st.T - g["T"]) <= 1e-10 * g["T"]
+        assert _rel(list(st.rhoY)[:h2.ns], g["rhoY"]) < 1e-8
+
+
+def test_oracle_reactor_final_state_matches_reference(oracle_lib, runs, h2):
+    # ~1e5 adaptive steps: rounding moves the step sequence, the integration tolerance bounds
+    # the end state (RTol 1e-6)
+    for r in runs["runs"][:4]:
+        st = oracle_lib.reactor_run(h2, r["T0"], r["p0"], r["Y"], r["t_end"], runs["h0"], runs["rtol"], runs["atol"])
+        g = r["final"]
+        assert st.status & 1
+        assert abs(st.T - g["T"]) <= 1e-5 * g["T"], (st.T, g["T"])
+        assert abs(st.p - g["p"]) <= 1e-5 * g["p"]
+        rho_y = np.array(list(st.rhoY)[:h2.ns])
+        major = np.array(g["rhoY"]) > 1e-6 * max(g["rhoY"])
+        assert _rel(rho_y[major], np.array(g["rhoY"])[major]) < 1e-4
+
+
+def test_reference_example_reactor_temperature(runs):
+    # the reference publishes T = 2973.956 K, p = 5.3484e5 Pa at 1.2 ms for this case
+    # (example/constantVolumeReactor/const_volume_reactor_output.dat); its run used another
+    # NASA7 thermo file than the one these fixtures take, which moves T by about 0.1 %
+    g = runs["runs"][0]
+    assert g["T0"] == 1000 and g["p0"] == 202650
+    assert abs(g["final"]["T"] - 2973.956) < 0.002 * 2973.956
+    assert abs(g["final"]["p"] - 5.3484e5) < 0.002 * 5.3484e5
