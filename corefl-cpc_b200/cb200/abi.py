@@ -66,3 +66,31 @@ class Reactor(C.Structure):
                 ("T", C.c_double), ("p", C.c_double), ("time", C.c_double), ("t_end", C.c_double),
                 ("h", C.c_double), ("err_last", C.c_double), ("step", C.c_int), ("n_reject", C.c_int),
                 ("status", C.c_int), ("pad", C.c_int)]
+
+REQ_REACTOR, REQ_TUBE = 0, 1
+TUBE_DONE, TUBE_FAILED = 1, 2
+
+
+class Request(C.Structure):
+    _fields_ = [("kind", C.c_int), ("n_nodes", C.c_int), ("arrival", C.c_double), ("T0", C.c_double),
+                ("p0", C.c_double), ("t_end", C.c_double), ("Y", C.c_double * REACTOR_MAX_SPEC),
+                ("out_state", C.c_void_p)]
+
+
+class Result(C.Structure):
+    _fields_ = [("t_arrival", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double),
+                ("latency", C.c_double), ("T", C.c_double), ("p", C.c_double), ("time", C.c_double),
+                ("steps", C.c_int), ("status", C.c_int)]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [("iterations", C.c_longlong), ("peak_pool_bytes", C.c_longlong), ("wall_s", C.c_double)]
+
+
+class ServeOptions(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_size_t), ("max_tubes", C.c_int), ("max_reactors", C.c_int),
+                ("tube_steps_per_launch", C.c_int), ("reactor_attempts_per_launch", C.c_int),
+                ("rtol", C.c_double), ("atol", C.c_double), ("h0", C.c_double), ("tube_length", C.c_double),
+                ("tube_TL", C.c_double), ("tube_pL", C.c_double), ("tube_TR", C.c_double),
+                ("tube_pR", C.c_double), ("tube_Y", C.POINTER(C.c_double)), ("time_limit_s", C.c_double),
+                ("stats", C.POINTER(ServeStats))]

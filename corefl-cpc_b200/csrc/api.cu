@@ -96,6 +96,10 @@ struct cb2_ctx {
   Profiler *prof = nullptr;  // non-null while profiling is enabled
 };
 
+namespace cb2 {
+const Param *ctx_param(const cb2_ctx *ctx) { return ctx ? &ctx->p : nullptr; }
+}  // namespace cb2
+
 namespace {
 // Makes the context's profiler current for this thread while an entry point runs.
 struct ProfGuard {

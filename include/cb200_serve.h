@@ -48,6 +48,60 @@ int cb2_reactor_setup(cb2_ctx *ctx, cb2_reactor *reactors, int n, const double *
 int cb2_reactor_advance(cb2_ctx *ctx, cb2_reactor *reactors, int n, int max_attempts, double rtol, double atol,
                         void *stream);
 
+/* ---- serving: continuous batching of reactors and shock tubes --------------------------- */
+
+#define CB2_REQ_REACTOR 0 /* 0-D constant-volume reactor from (T0, p0, Y) to t_end            */
+#define CB2_REQ_TUBE 1    /* 1-D two-state shock tube of n_nodes nodes to t_end               */
+
+typedef struct {
+  int kind;             /* CB2_REQ_* */
+  int n_nodes;          /* tube: nodes (8 .. 2^22) */
+  double arrival;       /* seconds after the start of cb2_serve_run */
+  double T0, p0;        /* reactor: initial temperature [K] and pressure [Pa] */
+  double t_end;         /* physical end time [s] */
+  double Y[CB2_REACTOR_MAX_SPEC]; /* reactor: mass fractions */
+  void *out_state;      /* optional host buffer for the final state: a cb2_reactor, or for a tube
+                         * the interior primitives bv[6][n_nodes] followed by sv[n_spec][n_nodes] */
+} cb2_request;
+
+typedef struct {
+  double t_arrival, t_admit, t_done; /* seconds after the start, host clock */
+  double latency;                    /* t_done - t_arrival */
+  double T, p;                       /* reactor: final T and p; tube: peak T (p unused) */
+  double time;                       /* physical time reached */
+  int steps, status;                 /* accepted steps; CB2_REACTOR_* bits, or for a tube
+                                      * 1 = done, 2 = failed (non-finite dt or state) */
+} cb2_result;
+
+typedef struct {
+  long long iterations;      /* batched launches per kind */
+  long long peak_pool_bytes; /* peak device memory held by admitted tubes */
+  double wall_s;             /* duration of the run */
+} cb2_serve_stats;
+
+typedef struct {
+  size_t hbm_budget_bytes;            /* device pool for the admitted tubes' state */
+  int max_tubes, max_reactors;        /* concurrent slots of each kind */
+  int tube_steps_per_launch;          /* RK3 steps per batched tube launch */
+  int reactor_attempts_per_launch;    /* ROK4E attempts per batched reactor launch */
+  double rtol, atol, h0;              /* reactor error control and first step */
+  double tube_length;                 /* [m]; the two states meet at the middle */
+  double tube_TL, tube_pL, tube_TR, tube_pR;
+  const double *tube_Y;               /* host, n_spec mass fractions of the tube gas */
+  double time_limit_s;                /* > 0: give up with CB2_ERR_TIMEOUT after this wall time */
+  cb2_serve_stats *stats;             /* optional */
+} cb2_serve_options;
+
+/* Serves n requests that arrive on the timeline reqs[].arrival: admits each one as soon as it
+ * has arrived, a slot of its kind is free and its state fits in the pool, keeps it resident
+ * until it finishes, and advances all admitted cases with one batched launch per kind per
+ * iteration (reactors on ctx_reactor's mechanism; tubes with ctx_tube's scheme: 1-D, inviscid,
+ * 9-species mixture, WENO5 with HLLC or AUSM+).  Fills out[i] for reqs[i].  A case's result does
+ * not depend on which other cases share its launches.  Blocks until every request is done.
+ * No counterpart in the reference, which runs one case per process. */
+int cb2_serve_run(cb2_ctx *ctx_reactor, cb2_ctx *ctx_tube, const cb2_request *reqs, int n,
+                  const cb2_serve_options *opt, cb2_result *out);
+
 #ifdef __cplusplus
 }
 #endif

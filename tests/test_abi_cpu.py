@@ -36,6 +36,30 @@ def test_struct_sizes_match_header():
     assert abi.ParamView.abi_version.offset == 0
 
 
+def test_serve_struct_sizes_match_header():
+    # sizes of include/cb200_serve.h's structs as a C compiler lays them out (x86-64)
+    assert C.sizeof(abi.Reactor) == 152
+    assert C.sizeof(abi.Request) == 120
+    assert C.sizeof(abi.Result) == 64
+    assert C.sizeof(abi.ServeOptions) == 112
+
+
+def test_serve_rejects_bad_arguments(cb200_lib):
+    f = cb200_lib.cb2_serve_run
+    f.restype = C.c_int
+    f.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(abi.Request), C.c_int, C.POINTER(abi.ServeOptions),
+                  C.POINTER(abi.Result)]
+    reqs = (abi.Request * 1)()
+    out = (abi.Result * 1)()
+    opt = abi.ServeOptions()
+    assert f(None, None, reqs, 1, C.byref(opt), out) == abi.ERR_INVALID  # a reactor without a context
+    reqs[0].kind = 7
+    assert f(None, None, reqs, 1, C.byref(opt), out) == abi.ERR_INVALID
+    reqs[0].kind, reqs[0].n_nodes = abi.REQ_TUBE, 3  # too few nodes
+    assert f(None, None, reqs, 1, C.byref(opt), out) == abi.ERR_INVALID
+    assert f(None, None, reqs, 0, C.byref(opt), out) == abi.OK
+
+
 def test_init_rejects_bad_arguments(cb200_lib):
     h = C.c_void_p()
     assert cb200_lib.cb2_init(None, C.byref(h)) == abi.ERR_INVALID
