@@ -54,6 +54,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served reactor/shock-tube workload")
+    ap.add_argument("--serve-seconds", type=float, default=0.25,
+                    help="length of the seeded Poisson arrival window of the served workload")
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="mean arrivals per second")
     ap.add_argument("--accuracy-steps", type=int, default=100,
                     help="RK3 steps of the mixed-vs-FP64 accuracy run (the workload's 100 steps)")
     return ap.parse_args()
@@ -290,6 +294,9 @@ def gpu_arm(args, rank, world, local_rank):
         mixed = mixed_form(args, p, dev, faces, host_state, xyz, dt, ctx, stream, nodes, world, dist, local_rank)
 
     ctx.close()
+    del dev, xyz
+    torch.cuda.empty_cache()
+    served = None if args.no_serve else serve_workload(args)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -307,7 +314,7 @@ def gpu_arm(args, rank, world, local_rank):
                        "l2": "inputs larger than L2 (about 7 GB of field arrays per GPU)",
                        "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
             "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clocks, "status_flags": status, "mixed": mixed,
+            "clocks": clocks, "status_flags": status, "mixed": mixed, "serve": served,
             "kernel_ms_per_step": {k: v[1] for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}}
     print(json.dumps(line), flush=True)
 
@@ -386,6 +393,44 @@ def mixed_form(args, p, dev, faces, host_state, xyz, dt, ctx64, stream, nodes, w
            "accuracy_bound_l1": 1e-6,
            "kernel_ms_per_step": {k: v[1] for k, v in sorted(prof32.items(), key=lambda kv: -kv[1][1])}}
     out["meets_accuracy_bound"] = out["l1_rho_vs_fp64"] <= 1e-6
+    return out
+
+
+def serve_workload(args):
+    """The served workload: seeded Poisson arrivals (mean --serve-rate per second over
+    --serve-seconds) of 0-D H2/air reactors (T0 ~ U[1000, 1500] K, p0 ~ U[1, 10] atm,
+    phi ~ U[0.5, 2], to 1 ms, ROK4E with RTol 1e-6, ATol 1e-12) and 1-D reactive shock tubes
+    (N ~ U{200..4000} nodes over 0.1 m, (1500 K, 5 atm) | (300 K, 1 atm) stoichiometric H2/air,
+    WENO5 + HLLC with chemistry, CFL 0.5, to 50 us), half each, served by cb2_serve_run on this
+    GPU.  Latency = completion - arrival on the host clock."""
+    import cb200
+    from cb200 import abi, cases, serve
+    from cb200 import mech as mechmod
+    h2 = mechmod.load_json(os.path.join(REPO, "tests", "golden", "h2_li2004.json"))
+    p = cases.make_param(n_var=5 + h2.ns, n_spec=h2.ns, dim=2, inviscid_scheme=abi.INV_HLLC,
+                         reconstruction=abi.REC_WENO5, cfl=0.5, mech=h2.ptr())
+    p.reaction = 1
+    ctx = cb200.Context(p)
+    reqs = serve.request_stream(h2, rate=args.serve_rate, duration=args.serve_seconds, seed=2026)
+    opt = serve.options(h2, hbm_budget=16 << 30, max_tubes=296, max_reactors=4096, tube_steps=20,
+                        reactor_attempts=500, time_limit=900.0)
+    res, st = serve.serve(ctx, ctx, reqs, opt)
+    ctx.close()
+    kinds = {"reactor": [r for q, r in zip(reqs, res) if q.kind == abi.REQ_REACTOR],
+             "shock_tube": [r for q, r in zip(reqs, res) if q.kind == abi.REQ_TUBE]}
+    tube_cu = sum(q.n_nodes * r.steps for q, r in zip(reqs, res) if q.kind == abi.REQ_TUBE)
+    out = {"workload": "seeded Poisson arrivals of 0-D H2/air reactors (to 1 ms) and 1-D reactive shock tubes "
+                       "(200..4000 nodes, to 50 us), half each",
+           "arrival_rate_per_s": args.serve_rate, "arrival_window_s": args.serve_seconds, "requests": len(reqs),
+           "wall_s": st.wall_s, "throughput_requests_per_s": len(reqs) / st.wall_s,
+           "tube_cell_updates_per_s": tube_cu / st.wall_s, "batched_iterations": st.iterations,
+           "peak_pool_bytes": st.peak_pool_bytes,
+           "failed": int(sum(1 for q, r in zip(reqs, res) if (q.kind == abi.REQ_TUBE and r.status & 2)
+                             or (q.kind == abi.REQ_REACTOR and r.status & abi.REACTOR_NONPHYSICAL)))}
+    for k, v in kinds.items():
+        if v:
+            out[f"latency_{k}"] = serve.latency_summary(v)
+    out["latency_all"] = serve.latency_summary(res)
     return out
 
 
