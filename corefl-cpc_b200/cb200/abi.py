@@ -1,7 +1,7 @@
 """ctypes mirror of include/cb200.h (structs and constants)."""
 import ctypes as C
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 OK = 0
 ERR_CUDA, ERR_INVALID, ERR_NONPHYSICAL, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_NOMEM = -1, -2, -3, -4, -5, -6
@@ -53,7 +53,8 @@ class ParamView(C.Structure):
                 ("shock_sensor", C.c_int), ("sensor_eps", C.c_double), ("sensor_threshold", C.c_double),
                 ("entropy_fix_factor", C.c_double), ("Pr", C.c_double), ("cfl", C.c_double),
                 ("rho_ref", C.c_double), ("v_ref", C.c_double), ("mu_constant", C.c_double),
-                ("precision", C.c_int), ("mech", C.POINTER(Mechanism))]
+                ("precision", C.c_int), ("mech", C.POINTER(Mechanism)), ("limit_flow", C.c_int), ("p_ref", C.c_double),
+                ("c_ref", C.c_double)]
 
 
 # ---- batched solves (include/cb200_serve.h) ---------------------------------------------------

@@ -273,6 +273,7 @@ int cb2_init(const cb2_param_view *pv, cb2_ctx **out) {
   if (pv->viscous_order == 8 && ns != 0) return CB2_ERR_UNSUPPORTED;
   if (pv->positive_preserving) return CB2_ERR_UNSUPPORTED;
   if (pv->reaction && ns == 0) return CB2_ERR_INVALID;
+  if (pv->limit_flow && !(pv->rho_ref > 0 && pv->p_ref > 0)) return CB2_ERR_INVALID;
   if (pv->precision != CB2_PREC_FP64 && pv->precision != CB2_PREC_MIXED) return CB2_ERR_INVALID;
   // mixed form: FP32 sweeps for WENO5/7 primitive reconstruction with AUSM+/HLLC/Roe
   if (pv->precision == CB2_PREC_MIXED &&
@@ -306,6 +307,19 @@ int cb2_init(const cb2_param_view *pv, cb2_ctx **out) {
   p.weno_eps_scale = pv->rho_ref * pv->v_ref * pv->rho_ref * pv->v_ref;
   p.mu_constant = pv->mu_constant;
   p.precision = pv->precision;
+  p.limit_flow = pv->limit_flow;
+  if (p.limit_flow) {
+    // bounds of src/DParameter.cu:371-387
+    p.lf_ll[0] = 1e-6 * pv->rho_ref;
+    p.lf_ul[0] = 1e+3 * pv->rho_ref;
+    const double vref = fabs(pv->v_ref) < 1 ? pv->c_ref : pv->v_ref;
+    for (int l = 1; l < 4; ++l) {
+      p.lf_ll[l] = -1000 * vref;
+      p.lf_ul[l] = 1000 * vref;
+    }
+    p.lf_ll[4] = 1e-6 * pv->p_ref;
+    p.lf_ul[4] = 1e+3 * pv->p_ref;
+  }
   int rc = CB2_OK;
   if (pv->mech) rc = upload_mechanism(*pv->mech, ctx);
   if (rc == CB2_OK) {

@@ -93,6 +93,8 @@ struct Param {
   double sensor_eps, sensor_threshold, entropy_fix_factor, Pr, cfl;
   double rho_ref, v_ref, weno_eps_scale, mu_constant;
   int precision;
+  int limit_flow;
+  double lf_ll[5], lf_ul[5];  // limit_flow bounds of rho, u, v, w, p
   unsigned *status;  // device status word
   Mech mech;
 };

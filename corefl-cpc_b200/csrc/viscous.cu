@@ -50,15 +50,17 @@ __device__ __forceinline__ BFlags bflags(const Zone &z, int i, int j, int k) {
   return b;
 }
 
-constexpr int kVisThreads = 128;
+// 8th-order kernels: one thread per node, CTAs of kVisTI (i) x kVisTJ (j) nodes of one k-plane,
+// so the j-neighbours of a stencil are mostly lines the same CTA already brought into L1.
+constexpr int kVisTI = 32, kVisTJ = 8, kVisThreads = kVisTI * kVisTJ;
 
 // Node fluxes of the momentum and energy equations (air); comps 1..4 of fFlux/gFlux/hFlux.
 // T is the arithmetic type (double: plain form; float: mixed form, FP64 arrays read and
 // written, the stencils, stresses and fluxes evaluated in FP32).
 template <typename T>
 __global__ void __launch_bounds__(kVisThreads) k_visc8_node_flux_air(Zone z, Param p) {
-  const int i = blockIdx.x * kVisThreads + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
-  if (i >= z.mx) return;
+  const int i = blockIdx.x * kVisTI + threadIdx.x, j = blockIdx.y * kVisTJ + threadIdx.y, k = blockIdx.z;
+  if (i >= z.mx || j >= z.my) return;
   const Layout &L = z.L;
   const idx_t sz = L.sz, g = L.at(i, j, k);
   const BFlags b = bflags(z, i, j, k);
@@ -117,8 +119,8 @@ __global__ void __launch_bounds__(kVisThreads) k_visc8_node_flux_air(Zone z, Par
 
 template <typename T>
 __global__ void __launch_bounds__(kVisThreads) k_visc8_divergence(Zone z, Param p) {
-  const int i = blockIdx.x * kVisThreads + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
-  if (i >= z.mx) return;
+  const int i = blockIdx.x * kVisTI + threadIdx.x, j = blockIdx.y * kVisTJ + threadIdx.y, k = blockIdx.z;
+  if (i >= z.mx || j >= z.my) return;
   const Layout &L = z.L;
   const idx_t sz = L.sz, g = L.at(i, j, k);
   const BFlags b = bflags(z, i, j, k);
@@ -304,11 +306,11 @@ int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_fac
   if (p.viscous_order == 0) return CB2_OK;
   if (p.viscous_order == 8) {
     if (p.n_spec != 0) return CB2_ERR_UNSUPPORTED;
-    dim3 grid((z.mx + kVisThreads - 1) / kVisThreads, z.my, z.mz);
+    const dim3 grid((z.mx + kVisTI - 1) / kVisTI, (z.my + kVisTJ - 1) / kVisTJ, z.mz), block(kVisTI, kVisTJ);
     {
       ProfScope prof("visc8_node_flux", s);
-      if (p.precision == CB2_PREC_MIXED) k_visc8_node_flux_air<float><<<grid, kVisThreads, 0, s>>>(z, p);
-      else k_visc8_node_flux_air<double><<<grid, kVisThreads, 0, s>>>(z, p);
+      if (p.precision == CB2_PREC_MIXED) k_visc8_node_flux_air<float><<<grid, block, 0, s>>>(z, p);
+      else k_visc8_node_flux_air<double><<<grid, block, 0, s>>>(z, p);
     }
     ++nl;
     CB2_TRY(check_launch());
@@ -316,7 +318,7 @@ int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_fac
     {
       ProfScope prof("visc8_divergence", s);
       // the divergence is a load-bound sum of four 9-point stencils: FP64 in both forms
-      k_visc8_divergence<double><<<grid, kVisThreads, 0, s>>>(z, p);
+      k_visc8_divergence<double><<<grid, block, 0, s>>>(z, p);
     }
     ++nl;
     return check_launch();

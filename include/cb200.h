@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define CB2_ABI_VERSION 1
+#define CB2_ABI_VERSION 2
 
 /* ---- status codes ---------------------------------------------------------------- */
 #define CB2_OK 0
@@ -163,6 +163,12 @@ typedef struct cb2_param_view {
   double mu_constant;
   int precision;           /* CB2_PREC_* */
   const cb2_mechanism *mech; /* NULL for the calorically perfect air model */
+  /* limit_flow (src/TimeAdvanceFunc.cuh:129-232, bounds src/DParameter.cu:371-387): after each
+   * stage update, nodes with NaN or rho, u, v, w, p outside [1e-6, 1e3] x rho_ref / p_ref and
+   * +-1000 x velocity scale (v_ref, or c_ref when |v_ref| < 1) take the mean of their good
+   * neighbours */
+  int limit_flow;
+  double p_ref, c_ref;     /* p_inf, speed_of_sound */
 } cb2_param_view;
 
 typedef struct cb2_ctx cb2_ctx;

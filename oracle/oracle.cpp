@@ -1,5 +1,7 @@
 // FP64 host oracle (see oracle.hpp).  TEST INFRASTRUCTURE ONLY.
 #include "oracle.hpp"
+#include <array>
+#include <cmath>
 #include <cstring>
 #include <cstdio>
 
@@ -1309,6 +1311,19 @@ Param make_param(const cb2_param_view &pv) {
   p.v_ref = pv.v_ref;
   p.weno_eps_scale = pv.rho_ref * pv.v_ref * pv.rho_ref * pv.v_ref;
   p.mu_constant = pv.mu_constant;
+  p.limit_flow = pv.limit_flow;
+  if (p.limit_flow) {
+    // src/DParameter.cu:371-387
+    p.lf_ll[0] = 1e-6 * pv.rho_ref;
+    p.lf_ul[0] = 1e+3 * pv.rho_ref;
+    const double vref = std::fabs(pv.v_ref) < 1 ? pv.c_ref : pv.v_ref;
+    for (int l = 1; l < 4; ++l) {
+      p.lf_ll[l] = -1000 * vref;
+      p.lf_ul[l] = 1000 * vref;
+    }
+    p.lf_ll[4] = 1e-6 * pv.p_ref;
+    p.lf_ul[4] = 1e+3 * pv.p_ref;
+  }
   if (pv.mech) {
     const cb2_mechanism &m = *pv.mech;
     Mechanism &o = p.mech;
@@ -1410,6 +1425,66 @@ Zone make_zone(const cb2_zone_view &v, const cb2_face_bc *faces, int n_faces, co
 
 // update_cv_and_bv_rk (src/RK.cuh:277-367) with compute_temperature_and_pressure
 // (src/FieldOperation.cu:4-94)
+// limit_flow (src/TimeAdvanceFunc.cuh:129-232), read from the state the stage update left: a
+// bad node (NaN or rho, u, v, w, p outside the bounds) takes the mean of the good nodes of its
+// 3x3x3 neighbourhood, or its own clamped values if none is good; then T and cv.  The
+// reference updates in place from parallel threads; reading only the pre-limit state is the
+// race-free reading of the same rule.
+static bool lf_bad(const Zone &z, const Param &p, int i, int j, int k) {
+  for (int l = 0; l < 5; ++l) {
+    const double v = z.bv(i, j, k, l);
+    if (std::isnan(v) || v < p.lf_ll[l] || v > p.lf_ul[l]) return true;
+  }
+  return false;
+}
+
+void limit_flow(Zone &z, const Param &p) {
+  std::vector<std::array<double, 6>> fix;
+  for (int k = 0; k < z.mz; ++k)
+    for (int j = 0; j < z.my; ++j)
+      for (int i = 0; i < z.mx; ++i) {
+        if (!lf_bad(z, p, i, j, k)) continue;
+        double v[5] = {0, 0, 0, 0, 0};
+        int kn = 0;
+        for (int ka = -1; ka < 2; ++ka) {
+          const int k1 = k + ka;
+          if (k1 < 0 || k1 >= z.mz) continue;
+          for (int ja = -1; ja < 2; ++ja) {
+            const int j1 = j + ja;
+            if (j1 < 0 || j1 >= z.my) continue;
+            for (int ia = -1; ia < 2; ++ia) {
+              const int i1 = i + ia;
+              if (i1 < 0 || i1 >= z.mx) continue;
+              if (lf_bad(z, p, i1, j1, k1)) continue;
+              for (int l = 0; l < 5; ++l) v[l] += z.bv(i1, j1, k1, l);
+              ++kn;
+            }
+          }
+        }
+        if (kn > 0) {
+          const double inv = 1.0 / kn;
+          for (double &x : v) x *= inv;
+        } else {
+          for (int l = 0; l < 5; ++l) v[l] = std::min(std::max(z.bv(i, j, k, l), p.lf_ll[l]), p.lf_ul[l]);
+        }
+        const double idx = (double)((k * z.my + j) * z.mx + i);
+        fix.push_back({idx, v[0], v[1], v[2], v[3], v[4]});
+      }
+  for (const auto &f : fix) {
+    const long n = (long)f[0];
+    const int i = (int)(n % z.mx), j = (int)((n / z.mx) % z.my), k = (int)(n / ((long)z.mx * z.my));
+    for (int l = 0; l < 5; ++l) z.bv(i, j, k, l) = f[1 + l];
+    if (p.n_spec == 0) {
+      z.bv(i, j, k, 5) = f[5] * mw_air / (f[1] * R_u);
+    } else {
+      double r = 0;
+      for (int s = 0; s < p.n_spec; ++s) r += z.sv(i, j, k, s) * p.mech.gas_const[s];
+      z.bv(i, j, k, 5) = f[5] / (f[1] * r);
+    }
+    cv_point(z, p, i, j, k);
+  }
+}
+
 void update_cv_and_bv_rk(Zone &z, const Param &p, double dt, int rk) {
   const double A[3] = {1.0, 0.75, 1.0 / 3.0}, B[3] = {0.0, 0.25, 2.0 / 3.0}, C[3] = {1.0, 0.25, 2.0 / 3.0};
 #pragma omp parallel for collapse(2) schedule(static)
@@ -1466,6 +1541,7 @@ void update_cv_and_bv_rk(Zone &z, const Param &p, double dt, int rk) {
         z.bv(i, j, k, 5) = t;
         z.bv(i, j, k, 4) = rho * t * gc;
       }
+  if (p.limit_flow) limit_flow(z, p);
 }
 
 void compute_cv_from_bv(Zone &z, const Param &p) {

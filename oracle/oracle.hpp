@@ -58,6 +58,8 @@ struct Param {
   int positive_preserving = 0, gradP = 0, reaction = 0, shock_sensor = 0;
   double sensor_eps = 0, sensor_threshold = 0, entropy_fix_factor = 0.125, Pr = 0.72, cfl = 0.5;
   double rho_ref = 1, v_ref = 1, weno_eps_scale = 1, mu_constant = 0;
+  int limit_flow = 0;
+  double lf_ll[5] = {0, 0, 0, 0, 0}, lf_ul[5] = {0, 0, 0, 0, 0};
   Mechanism mech;
 };
 
@@ -79,6 +81,7 @@ Param make_param(const cb2_param_view &pv);
 Zone make_zone(const cb2_zone_view &v, const cb2_face_bc *faces, int n_faces, const Param &p);
 
 void update_cv_and_bv_rk(Zone &z, const Param &p, double dt, int rk);
+void limit_flow(Zone &z, const Param &p);
 void compute_cv_from_bv(Zone &z, const Param &p);
 void compute_inviscid_flux(Zone &z, const Param &p);
 void compute_viscous_flux(Zone &z, const Param &p);

@@ -193,3 +193,36 @@ def test_channel_rk3_parity(oracle_lib):
     g = hb.ngg
     sl = (slice(None), slice(g, -g), slice(g, -g), slice(g, -g))
     assert helpers.rel_err(out["cv"][sl], hb.a["cv"][sl]) < 3 * TOL
+
+
+def test_limit_flow_parity(oracle_lib):
+    """limit_flow after a stage update: planted bad nodes (negative density, NaN velocity, a
+    pair of adjacent over-pressure nodes, a corner whose whole neighbourhood is bad) are
+    replaced as the oracle replaces them; good nodes are untouched."""
+    p, hb, faces = helpers.curvilinear_air_case(20, 18, 16, scheme=abi.INV_AUSMP, reconstruction=abi.REC_WENO5,
+                                                bc="periodic", seed=5, jump=False)
+    p.limit_flow, p.p_ref, p.c_ref = 1, 1.0, 1.2
+    g = hb.ngg
+    a = hb.a
+    a["qn"][...] = a["cv"]
+    a["dq"][...] = 0.0
+    q = a["qn"]
+    q[0, g + 5, g + 6, g + 7] = -0.5                      # negative density
+    q[1, g + 9, g + 2, g + 3] = np.nan                    # NaN momentum
+    q[4, g + 3, g + 10, g + 10:g + 12] = 1e9              # two adjacent nodes far above p_max
+    q[4, g:g + 2, g:g + 2, g:g + 2] = 1e9                 # a corner with no good neighbour
+    dev = DeviceBlock(hb)
+    ctx = cb200.Context(p)
+    ctx.bind(0, dev.view(), faces)
+    ctx.stage_update(0, 1e-3, 0)
+    _sync()
+    oracle_lib.stage_update(p, hb, 1e-3, 0)
+    out = dev.to_host(["bv", "cv"])
+    inner = (slice(None), slice(g, -g), slice(g, -g), slice(g, -g))
+    assert np.isfinite(out["bv"][inner]).all() and np.isfinite(a["bv"][inner]).all()
+    assert out["bv"][inner][0].min() > 0
+    assert helpers.rel_err(out["bv"][inner], a["bv"][inner]) < 1e-13
+    assert helpers.rel_err(out["cv"][inner], a["cv"][inner]) < 1e-13
+    # the corner took its own values clamped into the bounds: p = 1e3 * p_ref
+    assert out["bv"][4, g, g, g] == 1e3
+    ctx.close()
