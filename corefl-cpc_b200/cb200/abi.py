@@ -54,7 +54,7 @@ class ParamView(C.Structure):
                 ("entropy_fix_factor", C.c_double), ("Pr", C.c_double), ("cfl", C.c_double),
                 ("rho_ref", C.c_double), ("v_ref", C.c_double), ("mu_constant", C.c_double),
                 ("precision", C.c_int), ("mech", C.POINTER(Mechanism)), ("limit_flow", C.c_int), ("p_ref", C.c_double),
-                ("c_ref", C.c_double)]
+                ("c_ref", C.c_double), ("dt", C.c_double)]
 
 
 # ---- batched solves (include/cb200_serve.h) ---------------------------------------------------

@@ -65,6 +65,7 @@ def make_param(n_var=5, n_spec=0, dim=3, inviscid_scheme=abi.INV_WENO5_CH, recon
     p.limit_flow = 0
     p.p_ref = 0.0
     p.c_ref = 0.0
+    p.dt = 0.0
     return p
 
 

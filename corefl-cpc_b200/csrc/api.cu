@@ -271,7 +271,9 @@ int cb2_init(const cb2_param_view *pv, cb2_ctx **out) {
   }
   if (pv->viscous_order != 0 && pv->viscous_order != 2 && pv->viscous_order != 8) return CB2_ERR_INVALID;
   if (pv->viscous_order == 8 && ns != 0) return CB2_ERR_UNSUPPORTED;
-  if (pv->positive_preserving) return CB2_ERR_UNSUPPORTED;
+  // the positivity limiter acts on the species rows of the characteristic-WENO fluxes
+  if (pv->positive_preserving && (ns == 0 || !(sch == CB2_INV_WENO5_CH || sch == CB2_INV_WENO7_CH)))
+    return CB2_ERR_UNSUPPORTED;
   if (pv->reaction && ns == 0) return CB2_ERR_INVALID;
   if (pv->limit_flow && !(pv->rho_ref > 0 && pv->p_ref > 0)) return CB2_ERR_INVALID;
   if (pv->precision != CB2_PREC_FP64 && pv->precision != CB2_PREC_MIXED) return CB2_ERR_INVALID;
@@ -307,6 +309,7 @@ int cb2_init(const cb2_param_view *pv, cb2_ctx **out) {
   p.weno_eps_scale = pv->rho_ref * pv->v_ref * pv->rho_ref * pv->v_ref;
   p.mu_constant = pv->mu_constant;
   p.precision = pv->precision;
+  p.dt = pv->dt;
   p.limit_flow = pv->limit_flow;
   if (p.limit_flow) {
     // bounds of src/DParameter.cu:371-387
@@ -581,6 +584,7 @@ int cb2_cfl_dt(cb2_ctx *ctx, double *dt_out, void *stream) {
   CB2_TRY(check_cuda(cudaMemcpyAsync(&dt, ctx->d_dtmin, sizeof(double), cudaMemcpyDeviceToHost, s)));
   CB2_TRY(check_cuda(cudaStreamSynchronize(s)));
   *dt_out = dt;
+  ctx->p.dt = dt;  // the global step, as update_dt_global leaves it (src/RK.cuh:151)
   return CB2_OK;
 }
 
@@ -598,6 +602,7 @@ int cb2_rk3_step(cb2_ctx *ctx, double *dt_inout, int fixed_dt, void *stream) {
     CB2_TRY(cb2_cfl_dt(ctx, &dt, stream));
     *dt_inout = dt;
   }
+  ctx->p.dt = dt;
   for (int rk = 0; rk < 3; ++rk) {
     for (int b = 0; b < nb; ++b) {
       if (!ctx->blocks[b].bound) continue;

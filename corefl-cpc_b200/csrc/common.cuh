@@ -95,6 +95,7 @@ struct Param {
   int precision;
   int limit_flow;
   double lf_ll[5], lf_ul[5];  // limit_flow bounds of rho, u, v, w, p
+  double dt;                  // the current step's time step (positivity limiter)
   unsigned *status;  // device status word
   Mech mech;
 };

@@ -201,6 +201,60 @@ __device__ __forceinline__ void load_node(const Zone &z, idx_t g, double *sQ, do
   sF[6 * NN + slot] = z.jac[g];
 }
 
+// Positivity limiter of the species rows of an interface flux (src/WENO.cu:1459-1528): with
+// alpha = 1/3 (3-D) or 1/2, every species flux is blended with a first-order flux f1 by
+// theta = min(theta_p, theta_m) so that the one-sided updates alpha J rhoY -+ dt f of the left
+// and right nodes stay non-negative.  Slots cl / cr of the left / right node.
+template <int NS>
+__device__ __forceinline__ void positive_limit(const double *sQ, const double *sF, int NN, int cl, int cr,
+                                               const Param &p, double *fc) {
+  const double dt = p.dt;
+  const double alpha = p.dim == 3 ? 1.0 / 3.0 : 0.5;
+  const double jl = sF[6 * NN + cl], jr = sF[6 * NN + cr];
+  const double alphaL = 0.5 * alpha * jl, alphaR = 0.5 * alpha * jr;
+  int start = -1;
+  for (int s = 0; s < NS; ++s) {
+    const double up = alphaL * sQ[(s + 5) * NN + cl] - dt * fc[s + 5];
+    const double um = alphaR * sQ[(s + 5) * NN + cr] + dt * fc[s + 5];
+    if (up < 0 || um < 0) {
+      start = s;
+      break;
+    }
+  }
+  if (start < 0) return;
+  const double Ul = sF[cl], Ur = sF[cr];
+  const double U1 = Ul * jl, U2 = Ur * jr;
+  for (int s = start; s < NS; ++s) {
+    double f1 = 0, theta_p = 1, theta_m = 1;
+    bool have_f1 = false;
+    const double yl = sQ[(s + 5) * NN + cl], yr = sQ[(s + 5) * NN + cr];
+    const double fp = 0.5 * jl * (Ul + sF[5 * NN + cl]) * yl;
+    const double fm = 0.5 * jr * (Ur - sF[5 * NN + cr]) * yr;
+    const double up = alphaL * yl - dt * fc[s + 5];
+    if (up < 0) {
+      f1 = 0.5 * (fp + U1 * yl) + 0.5 * (fm - U2 * yr);
+      have_f1 = true;
+      const double up_lf = alphaL * yl - dt * f1;
+      if (fabs(up - up_lf) > 1e-20 * p.rho_ref) {
+        theta_p = (0 - up_lf) / (up - up_lf);
+        if (theta_p > 1) theta_p = 1.0;
+        else if (theta_p < 0) theta_p = 0;
+      }
+    }
+    const double um = alphaR * yr + dt * fc[s + 5];
+    if (um < 0) {
+      if (!have_f1) f1 = 0.5 * (fp + U1 * yl) + 0.5 * (fm - U2 * yr);
+      const double um_lf = alphaR * yr + dt * f1;
+      if (fabs(um - um_lf) > 1e-20 * p.rho_ref) {
+        theta_m = (0 - um_lf) / (um - um_lf);
+        if (theta_m > 1) theta_m = 1.0;
+        else if (theta_m < 0) theta_m = 0;
+      }
+    }
+    fc[s + 5] = fmin(theta_p, theta_m) * (fc[s + 5] - f1) + f1;
+  }
+}
+
 template <int NS, int DIR, int ORDER>
 __global__ void __launch_bounds__(kSweepThreads) k_weno_char(Zone z, Param p, idx_t run) {
   constexpr int NV = 5 + NS;
@@ -275,6 +329,9 @@ __global__ void __launch_bounds__(kSweepThreads) k_weno_char(Zone z, Param p, id
     }
     double fc[NV];
     char_flux<NS, ORDER>(sQ, sF, NN, c, st, kx, ky, kz, kWenoEps * p.weno_eps_scale, shock, p.mech, fc);
+    if constexpr (NS > 0) {
+      if (p.positive_preserving) positive_limit<NS>(sQ, sF, NN, c, c + st, p, fc);
+    }
 #pragma unroll
     for (int v = 0; v < NV; ++v) sFl[v * kSweepThreads + tid] = fc[v];
   }

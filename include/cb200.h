@@ -150,7 +150,7 @@ typedef struct cb2_param_view {
   int reconstruction;      /* CB2_REC_* (primitive-reconstruction schemes only) */
   int limiter;             /* 0 minmod */
   int viscous_order;       /* 0, 2 or 8 */
-  int positive_preserving; /* 0/1 */
+  int positive_preserving; /* 0/1: species positivity limiter (characteristic WENO, mixtures) */
   int gradP_in_diffusion_flux;
   int reaction;            /* 0 or 1 (finite-rate chemistry) */
   int shock_sensor;        /* 0 Ducros, 1 Jameson, 2 jump */
@@ -169,6 +169,9 @@ typedef struct cb2_param_view {
    * neighbours */
   int limit_flow;
   double p_ref, c_ref;     /* p_inf, speed_of_sound */
+  /* time step the positivity limiter starts with (DParameter::dt, the setup's fixed step);
+   * cb2_cfl_dt and cb2_rk3_step replace it with the step they take */
+  double dt;
 } cb2_param_view;
 
 typedef struct cb2_ctx cb2_ctx;

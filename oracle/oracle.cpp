@@ -285,6 +285,58 @@ inline void shift(int dir, int m, int &i, int &j, int &k) {
   else k += m;
 }
 
+// Positivity limiter of the species rows of a characteristic-WENO interface flux
+// (src/WENO.cu:1459-1528): with alpha = 1/3 (3-D) or 1/2, each species flux is blended with a
+// first-order flux f1 by theta = min(theta_p, theta_m) so that the two one-sided updates
+// alpha J rho_Y -+ dt f stay non-negative.  Q/F are the node slots of the interface's stencil,
+// l = left node, l + 1 = right node.
+void positive_limit(const Param &p, const double Q[][8], const double F[][8], int l, double *fc) {
+  const double dt = p.dt;
+  const double alpha = p.dim == 3 ? 1.0 / 3.0 : 0.5;
+  const double jl = F[6][l], jr = F[6][l + 1];
+  const double alphaL = 0.5 * alpha * jl, alphaR = 0.5 * alpha * jr;
+  int start = -1;
+  for (int s = 0; s < p.n_spec; ++s) {
+    const double up = alphaL * Q[s + 5][l] - dt * fc[s + 5];
+    const double um = alphaR * Q[s + 5][l + 1] + dt * fc[s + 5];
+    if (up < 0 || um < 0) {
+      start = s;
+      break;
+    }
+  }
+  if (start < 0) return;
+  const double U1 = F[0][l] * jl, U2 = F[0][l + 1] * jr;
+  for (int s = start; s < p.n_spec; ++s) {
+    double f1 = 0, theta_p = 1, theta_m = 1;
+    bool have_f1 = false;
+    const double yl = Q[s + 5][l], yr = Q[s + 5][l + 1];
+    const double fp = 0.5 * F[6][l] * (F[0][l] + F[5][l]) * yl;
+    const double fm = 0.5 * F[6][l + 1] * (F[0][l + 1] - F[5][l + 1]) * yr;
+    const double up = alphaL * yl - dt * fc[s + 5];
+    if (up < 0) {
+      f1 = 0.5 * (fp + U1 * yl) + 0.5 * (fm - U2 * yr);
+      have_f1 = true;
+      const double up_lf = alphaL * yl - dt * f1;
+      if (std::abs(up - up_lf) > 1e-20 * p.rho_ref) {
+        theta_p = (0 - up_lf) / (up - up_lf);
+        if (theta_p > 1) theta_p = 1.0;
+        else if (theta_p < 0) theta_p = 0;
+      }
+    }
+    const double um = alphaR * yr + dt * fc[s + 5];
+    if (um < 0) {
+      if (!have_f1) f1 = 0.5 * (fp + U1 * yl) + 0.5 * (fm - U2 * yr);
+      const double um_lf = alphaR * yr + dt * f1;
+      if (std::abs(um - um_lf) > 1e-20 * p.rho_ref) {
+        theta_m = (0 - um_lf) / (um - um_lf);
+        if (theta_m > 1) theta_m = 1.0;
+        else if (theta_m < 0) theta_m = 0;
+      }
+    }
+    fc[s + 5] = std::min(theta_p, theta_m) * (fc[s + 5] - f1) + f1;
+  }
+}
+
 void convective_term_weno_char(Zone &z, const Param &p, int dir) {
   const int order = (p.inviscid_scheme == 52) ? 5 : 7;
   const int r = order == 5 ? 3 : 4;
@@ -340,6 +392,7 @@ void convective_term_weno_char(Zone &z, const Param &p, int dir) {
         }
         double f[16];
         weno_char_interface(p, order, Q, F, kx, ky, kz, eps_ref, shock, f);
+        if (p.positive_preserving && p.n_spec > 0) positive_limit(p, Q, F, r - 1, f);
         for (int l = 0; l < p.n_var; ++l) F_out(i, j, k, l) = f[l];
       }
   // compute_derivative_{x,y,z} (src/WENO.cu:1532-1559)
@@ -1311,6 +1364,7 @@ Param make_param(const cb2_param_view &pv) {
   p.v_ref = pv.v_ref;
   p.weno_eps_scale = pv.rho_ref * pv.v_ref * pv.rho_ref * pv.v_ref;
   p.mu_constant = pv.mu_constant;
+  p.dt = pv.dt;
   p.limit_flow = pv.limit_flow;
   if (p.limit_flow) {
     // src/DParameter.cu:371-387
@@ -1867,7 +1921,8 @@ void compute_shock_sensor(Zone &z, const Param &p) {
 }
 
 // One SSP-RK3 step over all zones (src/RK.cuh:107-237, single process, no MPI)
-void rk3_step(std::vector<Zone> &zones, const Param &p, double &dt, bool fixed_dt) {
+void rk3_step(std::vector<Zone> &zones, const Param &p_in, double &dt, bool fixed_dt) {
+  Param p = p_in;
   for (auto &z : zones) {
     const size_t n = (size_t)z.cv.sz * p.n_var;
     std::memcpy(z.qn.p, z.cv.p, n * sizeof(double));
@@ -1879,6 +1934,7 @@ void rk3_step(std::vector<Zone> &zones, const Param &p, double &dt, bool fixed_d
     for (auto &z : zones) m = std::min(m, local_time_step_min(z, p));
     dt = m;
   }
+  p.dt = dt;
   for (int rk = 0; rk < 3; ++rk) {
     for (auto &z : zones) {
       std::memset(z.dq.p, 0, (size_t)z.dq.sz * p.n_var * sizeof(double));

@@ -59,6 +59,7 @@ struct Param {
   double sensor_eps = 0, sensor_threshold = 0, entropy_fix_factor = 0.125, Pr = 0.72, cfl = 0.5;
   double rho_ref = 1, v_ref = 1, weno_eps_scale = 1, mu_constant = 0;
   int limit_flow = 0;
+  double dt = 0;  // the step's time step (positivity limiter)
   double lf_ll[5] = {0, 0, 0, 0, 0}, lf_ul[5] = {0, 0, 0, 0, 0};
   Mechanism mech;
 };
