@@ -55,8 +55,12 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
     ap.add_argument("--no-serve", action="store_true", help="skip the served reactor/shock-tube workload")
-    ap.add_argument("--serve-seconds", type=float, default=0.25,
+    ap.add_argument("--serve-seconds", type=float, default=0.05,
                     help="length of the seeded Poisson arrival window of the served workload")
+    ap.add_argument("--serve-tube-t-end", type=float, default=1e-6,
+                    help="physical end time of the served shock tubes (the workload's is 50e-6)")
+    ap.add_argument("--serve-reactor-t-end", type=float, default=1e-3,
+                    help="physical end time of the served 0-D reactors")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="mean arrivals per second")
     ap.add_argument("--accuracy-steps", type=int, default=100,
                     help="RK3 steps of the mixed-vs-FP64 accuracy run (the workload's 100 steps)")
@@ -411,7 +415,8 @@ def serve_workload(args):
                          reconstruction=abi.REC_WENO5, cfl=0.5, mech=h2.ptr())
     p.reaction = 1
     ctx = cb200.Context(p)
-    reqs = serve.request_stream(h2, rate=args.serve_rate, duration=args.serve_seconds, seed=2026)
+    reqs = serve.request_stream(h2, rate=args.serve_rate, duration=args.serve_seconds, seed=2026,
+                                t_reactor=args.serve_reactor_t_end, t_tube=args.serve_tube_t_end)
     opt = serve.options(h2, hbm_budget=16 << 30, max_tubes=296, max_reactors=4096, tube_steps=20,
                         reactor_attempts=500, time_limit=900.0)
     res, st = serve.serve(ctx, ctx, reqs, opt)
@@ -419,8 +424,10 @@ def serve_workload(args):
     kinds = {"reactor": [r for q, r in zip(reqs, res) if q.kind == abi.REQ_REACTOR],
              "shock_tube": [r for q, r in zip(reqs, res) if q.kind == abi.REQ_TUBE]}
     tube_cu = sum(q.n_nodes * r.steps for q, r in zip(reqs, res) if q.kind == abi.REQ_TUBE)
-    out = {"workload": "seeded Poisson arrivals of 0-D H2/air reactors (to 1 ms) and 1-D reactive shock tubes "
-                       "(200..4000 nodes, to 50 us), half each",
+    out = {"workload": f"seeded Poisson arrivals of 0-D H2/air reactors (to {args.serve_reactor_t_end:g} s) and "
+                       f"1-D reactive shock tubes (200..4000 nodes, to {args.serve_tube_t_end:g} s; the served "
+                       f"workload's tubes run to 5e-05 s), half each",
+           "tube_time_step": "CFL 0.5 with the reference's reaction-time-scale limit (local_time_step)",
            "arrival_rate_per_s": args.serve_rate, "arrival_window_s": args.serve_seconds, "requests": len(reqs),
            "wall_s": st.wall_s, "throughput_requests_per_s": len(reqs) / st.wall_s,
            "tube_cell_updates_per_s": tube_cu / st.wall_s, "batched_iterations": st.iterations,

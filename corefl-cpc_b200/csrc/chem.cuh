@@ -25,87 +25,104 @@ __device__ __forceinline__ double ipow(double c, int n) {
   return r;
 }
 
+// Forward and backward rates of progress of reaction r at t, concentrations c and
+// g/(RT) of every species (used only for reactions whose backward rate follows from the
+// equilibrium constant); temp_t = p_atm / (R_u T) * 1e-3.
+template <int NS>
+__device__ __forceinline__ void reaction_progress(int r, double t, const double *c, const double *gibbs,
+                                                  double temp_t, const Mech &m, double &q1_out, double &q2_out) {
+  const int ty = __ldg(m.reac_type + r);
+  const int *sf = m.stoi_f + r * NS, *sb = m.stoi_b + r * NS;
+  // forward rate
+  double kf = arrhenius(t, __ldg(m.A + r), __ldg(m.b + r), __ldg(m.Ea + r));
+  double cc = 0;
+  if (ty > 3 || (ty != 0 && __ldg(m.rev_type + r) == 1 && ty == 4)) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) cc += c[s] * __ldg(m.tbc + r * NS + s);
+  }
+  if (ty == 3) {
+    kf += arrhenius(t, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
+  } else if (ty == 4) {
+    kf *= cc;
+  } else if (ty > 4) {
+    const double kf_low = arrhenius(t, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
+    const double kf_high = kf;
+    if (kf_high < 1e-25 && kf_low < 1e-25) {
+      kf = 0;
+    } else {
+      const double pr = kf_low * cc / kf_high;
+      double F = 1.0;
+      if (ty > 5) {
+        const double al = __ldg(m.troe_alpha + r);
+        double fc = (1 - al) * exp(-t / __ldg(m.troe_t3 + r)) + al * exp(-t / __ldg(m.troe_t1 + r));
+        if (ty == 7) fc += exp(-__ldg(m.troe_t2 + r) / t);
+        const double lfc = log10(fc);
+        const double cq = -0.4 - 0.67 * lfc;
+        const double nq = 0.75 - 1.27 * lfc;
+        const double lpr = log10(pr);
+        const double tmp = (lpr + cq) / (nq - 0.14 * (lpr + cq));
+        F = pow(10.0, lfc / (1.0 + tmp * tmp));
+      }
+      kf = kf_high * pr / (1.0 + pr) * F;
+    }
+  }
+  // backward rate
+  double kb = 0;
+  if (ty != 0) {
+    if (__ldg(m.rev_type + r) == 1) {
+      kb = arrhenius(t, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
+      if (ty == 4) kb *= cc;
+    } else if (ty != 2) {
+      double dg = 0;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) dg += gibbs[s] * (__ldg(sb + s) - __ldg(sf + s));
+      const double kc = pow(temp_t, __ldg(m.reac_order + r)) * exp(-dg);
+      kb = kf / kc;
+    }
+  }
+  // rates of progress
+  double q1 = 1.0, q2 = ty != 0 ? 1.0 : 0.0;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    q1 *= ipow(c[s], __ldg(sf + s));
+    if (ty != 0) q2 *= ipow(c[s], __ldg(sb + s));
+  }
+  q1 *= kf;
+  if (ty != 0) q2 *= kb;
+  q1_out = q1;
+  q2_out = q2;
+}
+
+// Whether any reaction takes its backward rate from the equilibrium constant.
+__device__ __forceinline__ bool mech_needs_gibbs(const Mech &m) {
+  for (int r = 0; r < m.n_reac; ++r) {
+    const int ty = __ldg(m.reac_type + r);
+    if (ty != 0 && __ldg(m.rev_type + r) != 1 && ty != 2) return true;
+  }
+  return false;
+}
+
 // t [K], c [mol/cm^3]; creation/destruction accumulate sum_r of q2 nu_f + q1 nu_b and
 // q1 nu_f + q2 nu_b [mol/(cm^3 s)]; q1r/q2r (may be null) receive the forward and backward
 // rates of progress of every reaction.
 template <int NS>
 __device__ __forceinline__ void chem_rates(double t, const double *c, const Mech &m, double *creation,
                                            double *destruction, double *q1r, double *q2r) {
-  bool need_gibbs = false;
-  for (int r = 0; r < m.n_reac; ++r) {
-    const int ty = __ldg(m.reac_type + r);
-    if (ty != 0 && __ldg(m.rev_type + r) != 1 && ty != 2) need_gibbs = true;
-  }
   double gibbs[NS];
-  if (need_gibbs) nasa7_gibbs_rt<NS>(t, m, gibbs);
+  if (mech_needs_gibbs(m)) nasa7_gibbs_rt<NS>(t, m, gibbs);
   constexpr double temp_p = kPatm / kRu * 1e-3;
   const double temp_t = temp_p / t;
 #pragma unroll
   for (int s = 0; s < NS; ++s) creation[s] = destruction[s] = 0;
 
   for (int r = 0; r < m.n_reac; ++r) {
-    const int ty = __ldg(m.reac_type + r);
-    const int *sf = m.stoi_f + r * NS, *sb = m.stoi_b + r * NS;
-    // forward rate
-    double kf = arrhenius(t, __ldg(m.A + r), __ldg(m.b + r), __ldg(m.Ea + r));
-    double cc = 0;
-    if (ty > 3 || (ty != 0 && __ldg(m.rev_type + r) == 1 && ty == 4)) {
-#pragma unroll
-      for (int s = 0; s < NS; ++s) cc += c[s] * __ldg(m.tbc + r * NS + s);
-    }
-    if (ty == 3) {
-      kf += arrhenius(t, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
-    } else if (ty == 4) {
-      kf *= cc;
-    } else if (ty > 4) {
-      const double kf_low = arrhenius(t, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
-      const double kf_high = kf;
-      if (kf_high < 1e-25 && kf_low < 1e-25) {
-        kf = 0;
-      } else {
-        const double pr = kf_low * cc / kf_high;
-        double F = 1.0;
-        if (ty > 5) {
-          const double al = __ldg(m.troe_alpha + r);
-          double fc = (1 - al) * exp(-t / __ldg(m.troe_t3 + r)) + al * exp(-t / __ldg(m.troe_t1 + r));
-          if (ty == 7) fc += exp(-__ldg(m.troe_t2 + r) / t);
-          const double lfc = log10(fc);
-          const double cq = -0.4 - 0.67 * lfc;
-          const double nq = 0.75 - 1.27 * lfc;
-          const double lpr = log10(pr);
-          const double tmp = (lpr + cq) / (nq - 0.14 * (lpr + cq));
-          F = pow(10.0, lfc / (1.0 + tmp * tmp));
-        }
-        kf = kf_high * pr / (1.0 + pr) * F;
-      }
-    }
-    // backward rate
-    double kb = 0;
-    if (ty != 0) {
-      if (__ldg(m.rev_type + r) == 1) {
-        kb = arrhenius(t, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
-        if (ty == 4) kb *= cc;
-      } else if (ty != 2) {
-        double dg = 0;
-#pragma unroll
-        for (int s = 0; s < NS; ++s) dg += gibbs[s] * (__ldg(sb + s) - __ldg(sf + s));
-        const double kc = pow(temp_t, __ldg(m.reac_order + r)) * exp(-dg);
-        kb = kf / kc;
-      }
-    }
-    // rates of progress
-    double q1 = 1.0, q2 = ty != 0 ? 1.0 : 0.0;
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      q1 *= ipow(c[s], __ldg(sf + s));
-      if (ty != 0) q2 *= ipow(c[s], __ldg(sb + s));
-    }
-    q1 *= kf;
-    if (ty != 0) q2 *= kb;
+    double q1, q2;
+    reaction_progress<NS>(r, t, c, gibbs, temp_t, m, q1, q2);
     if (q1r) {
       q1r[r] = q1;
       q2r[r] = q2;
     }
+    const int *sf = m.stoi_f + r * NS, *sb = m.stoi_b + r * NS;
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
       const double f = __ldg(sf + s), b = __ldg(sb + s);

@@ -1,4 +1,4 @@
-// Batched 0-D constant-volume reactors: one thread per reactor, FP64 throughout.
+// Batched 0-D constant-volume reactors: one warp per reactor, FP64 throughout.
 //
 // The integrator is the adaptive ROK4E Rosenbrock-Krylov scheme in its full-Jacobian form, as
 // const_volume_reactor runs it with advance_scheme = 1, build_arnoldi = 0,
@@ -38,77 +38,8 @@ constexpr double e1 = -0.217819895945721 - b1, e2 = 1.03130847478467 - b2, e3 = 
 
 constexpr int kReactorThreads = 64;
 
-// omega [kg/(m^3 s)] of a state and the rates of progress q1/q2 of every reaction.
-template <int NS>
-__device__ __forceinline__ void reactor_source(double t, const double *rhoY, const Mech &m, double *omega,
-                                               double *q1, double *q2) {
-  double c[NS], cre[NS], des[NS];
-#pragma unroll
-  for (int s = 0; s < NS; ++s) c[s] = rhoY[s] / __ldg(m.mw + s) * 1e-3;
-  chem_rates<NS>(t, c, m, cre, des, q1, q2);
-#pragma unroll
-  for (int s = 0; s < NS; ++s) {
-    const double w = 1e+3 * __ldg(m.mw + s);
-    omega[s] = cre[s] * w - des[s] * w;
-  }
-}
-
-// T from the internal energy E at fixed composition (Newton from t0).
-template <int NS>
-__device__ __forceinline__ double reactor_temperature(double t0, double imw, const double *y, double E,
-                                                      const Mech &m) {
-  double t = t0;
-  const double R = kRu * imw;
-  double err = 1e+6;
-  int iter = 0;
-  double h[NS], cp[NS];
-  while (err > 1e-8 && iter++ < 100) {
-    nasa7_h_cp<NS>(t, m, h, cp);
-    double cpt = 0, ht = 0;
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      cpt += cp[s] * y[s];
-      ht += h[s] * y[s];
-    }
-    const double et = ht - R * t;
-    const double cv = cpt - R;
-    const double t1 = t - (et - E) / cv;
-    err = fabs(1 - t1 / t);
-    t = t1;
-  }
-  return t;
-}
-
-// In-place LU of the N x N row-major matrix a with row pivoting (Crout ordering: column n of L
-// and then row n of U), piv[n] = the row swapped into n.
-template <int N>
-__device__ __forceinline__ void lu_factor(double *a, int *piv) {
-  for (int n = 0; n < N; ++n) {
-    int ik = n;
-    for (int r = n; r < N; ++r) {
-      double v = a[r * N + n];
-      for (int t = 0; t < n; ++t) v -= a[r * N + t] * a[t * N + n];
-      a[r * N + n] = v;
-      if (fabs(v) > fabs(a[ik * N + n])) ik = r;
-    }
-    piv[n] = ik;
-    if (ik != n) {
-      for (int t = 0; t < N; ++t) {
-        const double x = a[ik * N + t];
-        a[ik * N + t] = a[n * N + t];
-        a[n * N + t] = x;
-      }
-    }
-    for (int c = n + 1; c < N; ++c) {
-      double v = a[n * N + c];
-      for (int t = 0; t < n; ++t) v -= a[n * N + t] * a[t * N + c];
-      a[n * N + c] = v;
-    }
-    const double d = a[n * N + n];
-    for (int r = n + 1; r < N; ++r) a[r * N + n] /= d;
-  }
-}
-
+// Forward and back substitution with the LU factors of warp_lu (row pivots in piv), as
+// lu_to_solution does (src/ConstVolumeReactor.cpp:1835-1857).
 template <int N>
 __device__ __forceinline__ void lu_solve(const double *a, const int *piv, double *b) {
   for (int r = 0; r < N; ++r) {
@@ -163,125 +94,265 @@ __global__ void __launch_bounds__(kReactorThreads) k_reactor_setup(cb2_reactor *
   R[id] = st;
 }
 
+// ---- one warp per reactor ----------------------------------------------------------------
+// The lanes of a warp share one reactor: species-wise work on lanes 0..NS-1, one reaction per
+// lane for the rates of progress, three Jacobian entries per lane, the rows of a column in the
+// LU.  Every sum keeps the serial order: its terms are parked in shared memory and summed in
+// index order by each lane, so every lane holds the same value.
+constexpr int kReactorWarps = 4;  // reactors per CTA
+
 template <int NS>
-__global__ void __launch_bounds__(kReactorThreads) k_reactor_advance(cb2_reactor *R, int n, Mech m, int max_attempts,
-                                                                     double rtol, double atol) {
-  using namespace rok4e;
-  const int id = blockIdx.x * kReactorThreads + threadIdx.x;
-  if (id >= n) return;
-  cb2_reactor st = R[id];
-  if (st.status || st.time >= st.t_end) return;
-  double rhoY[NS], omega[NS], k1[NS], k2[NS], k3[NS], k4[NS], ys[NS], yk[NS];
-  double q1[kMaxReac], q2[kMaxReac], lhs[NS * NS];
+struct ReactorShared {
+  double rhoY[NS], omega[NS], k1[NS], k2[NS], k3[NS], k4[NS], ys[NS], yk[NS], c[NS], gibbs[NS];
+  double ta[NS], tb[NS];
+  double q1[kMaxReac], q2[kMaxReac];
+  double lhs[NS * NS];
   int piv[NS];
+};
+
+// Species s as a one-species mechanism (for the per-species thermo of one lane).
+__device__ __forceinline__ Mech mech_species(const Mech &m, int s) {
+  Mech o = m;
+  o.t_low += s; o.t_mid += s; o.t_high += s;
+  o.lo += 7 * s; o.hi += 7 * s;
+  o.gas_const += s; o.imw += s; o.mw += s;
+  return o;
+}
+
+// omega of the state y (partial densities) at temperature t; q1/q2 of every reaction.
+template <int NS>
+__device__ __forceinline__ void warp_source(double t, const double *y, const Mech &m, bool gibbs_needed,
+                                            ReactorShared<NS> &S, int lane) {
+  if (lane < NS) {
+    S.c[lane] = y[lane] / __ldg(m.mw + lane) * 1e-3;
+    if (gibbs_needed) nasa7_gibbs_rt<1>(t, mech_species(m, lane), &S.gibbs[lane]);
+  }
+  __syncwarp();
+  constexpr double temp_p = kPatm / kRu * 1e-3;
+  const double temp_t = temp_p / t;
+  for (int r = lane; r < m.n_reac; r += 32) reaction_progress<NS>(r, t, S.c, S.gibbs, temp_t, m, S.q1[r], S.q2[r]);
+  __syncwarp();
+  if (lane < NS) {
+    double cre = 0, des = 0;
+    for (int r = 0; r < m.n_reac; ++r) {
+      const double f = __ldg(m.stoi_f + r * NS + lane), b = __ldg(m.stoi_b + r * NS + lane);
+      cre += S.q2[r] * f + S.q1[r] * b;
+      des += S.q1[r] * f + S.q2[r] * b;
+    }
+    const double w = 1e+3 * __ldg(m.mw + lane);
+    S.omega[lane] = cre * w - des * w;
+  }
+  __syncwarp();
+}
+
+// Newton T from E at the composition S.yk (mass fractions), mean 1/W imw, from t0.
+template <int NS>
+__device__ __forceinline__ double warp_temperature(double t0, double imw, double E, const Mech &m,
+                                                   ReactorShared<NS> &S, int lane) {
+  double t = t0;
+  const double R = kRu * imw;
+  double err = 1e+6;
+  int iter = 0;
+  while (err > 1e-8 && iter++ < 100) {
+    if (lane < NS) {
+      double h, cp;
+      nasa7_h_cp<1>(t, mech_species(m, lane), &h, &cp);
+      S.ta[lane] = cp * S.yk[lane];
+      S.tb[lane] = h * S.yk[lane];
+    }
+    __syncwarp();
+    double cpt = 0, ht = 0;
 #pragma unroll
-  for (int s = 0; s < NS; ++s) rhoY[s] = st.rhoY[s];
-  const double rho = st.rho, E = st.E;
-  for (int a = 0; a < max_attempts && st.time < st.t_end; ++a) {
-    reactor_source<NS>(st.T, rhoY, m, omega, q1, q2);
-    const double h = fmin(st.h, st.t_end - st.time);
+    for (int s = 0; s < NS; ++s) {
+      cpt += S.ta[s];
+      ht += S.tb[s];
+    }
+    __syncwarp();
+    const double et = ht - R * t;
+    const double cv = cpt - R;
+    const double t1 = t - (et - E) / cv;
+    err = fabs(1 - t1 / t);
+    t = t1;
+  }
+  return t;
+}
+
+// sum over s of S.ta[s] in index order, after lanes 0..NS-1 wrote their terms
+template <int NS>
+__device__ __forceinline__ double warp_sum_ta(ReactorShared<NS> &S) {
+  __syncwarp();
+  double v = 0;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) v += S.ta[s];
+  __syncwarp();
+  return v;
+}
+
+// LU of S.lhs with row pivoting in the Crout ordering of lu_decomp (src/ConstVolumeReactor.cpp:
+// 1802-1833: column n of L, pivot, row n of U, scale), the rows or columns of each step on
+// separate lanes; the pivot search keeps the serial rule (the first largest |.|).
+template <int N, typename SH>
+__device__ __forceinline__ void warp_lu(SH &S, int lane) {
+  double *a = S.lhs;
+  for (int n = 0; n < N; ++n) {
+    if (lane >= n && lane < N) {
+      double v = a[lane * N + n];
+      for (int t = 0; t < n; ++t) v -= a[lane * N + t] * a[t * N + n];
+      a[lane * N + n] = v;
+    }
+    __syncwarp();
+    int ik = n;
+    for (int r = n + 1; r < N; ++r)
+      if (fabs(a[r * N + n]) > fabs(a[ik * N + n])) ik = r;
+    if (lane == 0) S.piv[n] = ik;
+    if (ik != n && lane < N) {
+      const double x = a[ik * N + lane];
+      a[ik * N + lane] = a[n * N + lane];
+      a[n * N + lane] = x;
+    }
+    __syncwarp();
+    if (lane > n && lane < N) {
+      double v = a[n * N + lane];
+      for (int t = 0; t < n; ++t) v -= a[n * N + t] * a[t * N + lane];
+      a[n * N + lane] = v;
+    }
+    __syncwarp();
+    const double d = a[n * N + n];
+    if (lane > n && lane < N) a[lane * N + n] /= d;
+    __syncwarp();
+  }
+}
+
+// Solves LU b = rhs in place on lane 0 (the substitutions are serial), then shares it.
+template <int N, typename SH>
+__device__ __forceinline__ void warp_solve(SH &S, double *b, int lane) {
+  __syncwarp();
+  if (lane == 0) lu_solve<N>(S.lhs, S.piv, b);
+  __syncwarp();
+}
+
+template <int NS>
+__global__ void __launch_bounds__(32 * kReactorWarps) k_reactor_advance(cb2_reactor *R, int n, Mech m,
+                                                                        int max_attempts, double rtol, double atol) {
+  using namespace rok4e;
+  __shared__ ReactorShared<NS> smem[kReactorWarps];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int id = blockIdx.x * kReactorWarps + wid;
+  if (id >= n) return;  // warp-uniform
+  ReactorShared<NS> &S = smem[wid];
+  double time = R[id].time, t_end = R[id].t_end, hh = R[id].h, err_last = R[id].err_last, T = R[id].T;
+  double pr = R[id].p;
+  int step = R[id].step, n_reject = R[id].n_reject, status = R[id].status;
+  if (status || time >= t_end) return;
+  const double rho = R[id].rho, E = R[id].E;
+  if (lane < NS) S.rhoY[lane] = R[id].rhoY[lane];
+  __syncwarp();
+  const bool gibbs_needed = mech_needs_gibbs(m);
+  for (int a = 0; a < max_attempts && time < t_end; ++a) {
+    warp_source<NS>(T, S.rhoY, m, gibbs_needed, S, lane);
+    const double h = fmin(hh, t_end - time);
     if (!(h > 0) || !isfinite(h)) {
-      st.status |= CB2_REACTOR_NONPHYSICAL;
+      status |= CB2_REACTOR_NONPHYSICAL;
       break;
     }
-    // lhs = I - h gamma J, J from the rates of progress of this state
-    for (int r = 0; r < NS; ++r) {
-      const double mwr = __ldg(m.mw + r);
-      for (int c = 0; c < NS; ++c) {
-        double zz = 0;
-        if (rhoY[c] > 1e-30) {
-          for (int q = 0; q < m.n_reac; ++q) {
-            const int fr = __ldg(m.stoi_f + q * NS + r), br = __ldg(m.stoi_b + q * NS + r);
-            const int fc = __ldg(m.stoi_f + q * NS + c), bc = __ldg(m.stoi_b + q * NS + c);
-            zz += (br - fr) * (fc * q1[q] - bc * q2[q]);
-          }
-          zz /= rhoY[c];
+    // lhs = I - h gamma J
+    for (int e = lane; e < NS * NS; e += 32) {
+      const int r = e / NS, c = e % NS;
+      double zz = 0;
+      if (S.rhoY[c] > 1e-30) {
+        for (int q = 0; q < m.n_reac; ++q) {
+          const int fr = __ldg(m.stoi_f + q * NS + r), br = __ldg(m.stoi_b + q * NS + r);
+          const int fc = __ldg(m.stoi_f + q * NS + c), bc = __ldg(m.stoi_b + q * NS + c);
+          zz += (br - fr) * (fc * S.q1[q] - bc * S.q2[q]);
         }
-        const double j = zz * 1e+3 * mwr;
-        lhs[r * NS + c] = r == c ? 1.0 - h * gamma * j : -h * gamma * j;
+        zz /= S.rhoY[c];
       }
+      const double j = zz * 1e+3 * __ldg(m.mw + r);
+      S.lhs[e] = r == c ? 1.0 - h * gamma * j : -h * gamma * j;
     }
-    lu_factor<NS>(lhs, piv);
+    __syncwarp();
+    warp_lu<NS>(S, lane);
     // stage 1
-#pragma unroll
-    for (int s = 0; s < NS; ++s) k1[s] = omega[s];
-    lu_solve<NS>(lhs, piv, k1);
+    if (lane < NS) S.k1[lane] = S.omega[lane];
+    warp_solve<NS>(S, S.k1, lane);
     // stage 2
-    double imw = 0;
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      ys[s] = rhoY[s] + h * a21 * k1[s];
-      yk[s] = ys[s] / rho;
-      imw += yk[s] / __ldg(m.mw + s);
+    if (lane < NS) {
+      S.ys[lane] = S.rhoY[lane] + h * a21 * S.k1[lane];
+      S.yk[lane] = S.ys[lane] / rho;
+      S.ta[lane] = S.yk[lane] / __ldg(m.mw + lane);
     }
-    double ts = reactor_temperature<NS>(st.T, imw, yk, E, m);
-    reactor_source<NS>(ts, ys, m, omega, q1, q2);
-#pragma unroll
-    for (int s = 0; s < NS; ++s) k2[s] = omega[s] + g21 * k1[s];
-    lu_solve<NS>(lhs, piv, k2);
-#pragma unroll
-    for (int s = 0; s < NS; ++s) k2[s] -= g21 * k1[s];
+    double imw = warp_sum_ta<NS>(S);
+    double ts = warp_temperature<NS>(T, imw, E, m, S, lane);
+    warp_source<NS>(ts, S.ys, m, gibbs_needed, S, lane);
+    if (lane < NS) S.k2[lane] = S.omega[lane] + g21 * S.k1[lane];
+    warp_solve<NS>(S, S.k2, lane);
+    if (lane < NS) S.k2[lane] -= g21 * S.k1[lane];
+    __syncwarp();
     // stage 3
-    imw = 0;
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      ys[s] = rhoY[s] + h * (a31 * k1[s] + a32 * k2[s]);
-      yk[s] = ys[s] / rho;
-      imw += yk[s] / __ldg(m.mw + s);
+    if (lane < NS) {
+      S.ys[lane] = S.rhoY[lane] + h * (a31 * S.k1[lane] + a32 * S.k2[lane]);
+      S.yk[lane] = S.ys[lane] / rho;
+      S.ta[lane] = S.yk[lane] / __ldg(m.mw + lane);
     }
-    ts = reactor_temperature<NS>(ts, imw, yk, E, m);
-    reactor_source<NS>(ts, ys, m, omega, q1, q2);
-#pragma unroll
-    for (int s = 0; s < NS; ++s) k3[s] = omega[s] + g31 * k1[s] + g32 * k2[s];
-    lu_solve<NS>(lhs, piv, k3);
-#pragma unroll
-    for (int s = 0; s < NS; ++s) k3[s] -= g31 * k1[s] + g32 * k2[s];
+    imw = warp_sum_ta<NS>(S);
+    ts = warp_temperature<NS>(ts, imw, E, m, S, lane);
+    warp_source<NS>(ts, S.ys, m, gibbs_needed, S, lane);
+    if (lane < NS) S.k3[lane] = S.omega[lane] + g31 * S.k1[lane] + g32 * S.k2[lane];
+    warp_solve<NS>(S, S.k3, lane);
+    if (lane < NS) S.k3[lane] -= g31 * S.k1[lane] + g32 * S.k2[lane];
+    __syncwarp();
     // stage 4 (the source of stage 3 again)
-#pragma unroll
-    for (int s = 0; s < NS; ++s) k4[s] = omega[s] + g41 * k1[s] + g42 * k2[s] + g43 * k3[s];
-    lu_solve<NS>(lhs, piv, k4);
-#pragma unroll
-    for (int s = 0; s < NS; ++s) k4[s] -= g41 * k1[s] + g42 * k2[s] + g43 * k3[s];
+    if (lane < NS) S.k4[lane] = S.omega[lane] + g41 * S.k1[lane] + g42 * S.k2[lane] + g43 * S.k3[lane];
+    warp_solve<NS>(S, S.k4, lane);
+    if (lane < NS) S.k4[lane] -= g41 * S.k1[lane] + g42 * S.k2[lane] + g43 * S.k3[lane];
+    __syncwarp();
     // embedded error estimate and step control
-    double err = 0;
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      ys[s] = rhoY[s] + h * (b1 * k1[s] + b2 * k2[s] + b4 * k4[s]);
-      double dy = h * (e1 * k1[s] + e2 * k2[s] + e3 * k3[s] + e4 * k4[s]);
-      dy /= rtol * ys[s] + atol;
-      err += dy * dy;
+    if (lane < NS) {
+      S.ys[lane] = S.rhoY[lane] + h * (b1 * S.k1[lane] + b2 * S.k2[lane] + b4 * S.k4[lane]);
+      double dy = h * (e1 * S.k1[lane] + e2 * S.k2[lane] + e3 * S.k3[lane] + e4 * S.k4[lane]);
+      dy /= rtol * S.ys[lane] + atol;
+      S.ta[lane] = dy * dy;
     }
+    double err = warp_sum_ta<NS>(S);
     err = sqrt(err / NS);
     double h_next = h;
-    if (st.step > 0) h_next *= fmin(5.0, fmax(0.2, 0.8 * pow(st.err_last, 0.1) * pow(err + 1e-20, -0.175)));
+    if (step > 0) h_next *= fmin(5.0, fmax(0.2, 0.8 * pow(err_last, 0.1) * pow(err + 1e-20, -0.175)));
     else if (err > 1) h_next *= 0.2;
     if (err <= 1) {
-      imw = 0;
-#pragma unroll
-      for (int s = 0; s < NS; ++s) {
-        rhoY[s] = ys[s];
-        yk[s] = ys[s] / rho;
-        imw += yk[s] / __ldg(m.mw + s);
+      if (lane < NS) {
+        S.rhoY[lane] = S.ys[lane];
+        S.yk[lane] = S.ys[lane] / rho;
+        S.ta[lane] = S.yk[lane] / __ldg(m.mw + lane);
       }
-      st.time += h;
-      st.err_last = err;
-      st.h = h_next;
-      st.T = reactor_temperature<NS>(st.T, imw, yk, E, m);
-      st.p = rho * kRu * imw * st.T;
-      ++st.step;
-      if (!(st.T > 0) || !isfinite(st.T)) {
-        st.status |= CB2_REACTOR_NONPHYSICAL;
+      imw = warp_sum_ta<NS>(S);
+      time += h;
+      err_last = err;
+      hh = h_next;
+      T = warp_temperature<NS>(T, imw, E, m, S, lane);
+      pr = rho * kRu * imw * T;
+      ++step;
+      if (!(T > 0) || !isfinite(T)) {
+        status |= CB2_REACTOR_NONPHYSICAL;
         break;
       }
     } else {
-      st.h = h_next;
-      ++st.n_reject;
+      hh = h_next;
+      ++n_reject;
     }
   }
-#pragma unroll
-  for (int s = 0; s < NS; ++s) st.rhoY[s] = rhoY[s];
-  if (st.time >= st.t_end) st.status |= CB2_REACTOR_DONE;
-  R[id] = st;
+  __syncwarp();
+  if (lane < NS) R[id].rhoY[lane] = S.rhoY[lane];
+  if (lane == 0) {
+    if (time >= t_end) status |= CB2_REACTOR_DONE;
+    R[id].time = time;
+    R[id].h = hh;
+    R[id].err_last = err_last;
+    R[id].T = T;
+    R[id].p = pr;
+    R[id].step = step;
+    R[id].n_reject = n_reject;
+    R[id].status = status;
+  }
 }
 
 int launch_reactor_setup(const Param &p, cb2_reactor *r, int n, const double *T0, const double *p0,
@@ -298,11 +369,11 @@ int launch_reactor_setup(const Param &p, cb2_reactor *r, int n, const double *T0
 
 int launch_reactor_advance(const Param &p, cb2_reactor *r, int n, int max_attempts, double rtol, double atol,
                            cudaStream_t s) {
-  const unsigned blocks = (unsigned)((n + kReactorThreads - 1) / kReactorThreads);
+  const unsigned blocks = (unsigned)((n + kReactorWarps - 1) / kReactorWarps);
   ProfScope prof("reactor_advance", s);
   switch (p.n_spec) {
-    case 5: k_reactor_advance<5><<<blocks, kReactorThreads, 0, s>>>(r, n, p.mech, max_attempts, rtol, atol); break;
-    case 9: k_reactor_advance<9><<<blocks, kReactorThreads, 0, s>>>(r, n, p.mech, max_attempts, rtol, atol); break;
+    case 5: k_reactor_advance<5><<<blocks, 32 * kReactorWarps, 0, s>>>(r, n, p.mech, max_attempts, rtol, atol); break;
+    case 9: k_reactor_advance<9><<<blocks, 32 * kReactorWarps, 0, s>>>(r, n, p.mech, max_attempts, rtol, atol); break;
     default: return CB2_ERR_UNSUPPORTED;
   }
   return check_launch();

@@ -87,13 +87,14 @@ def test_served_results_same_alone_and_in_the_mix(h2):
     opt = serve.options(h2, hbm_budget=1 << 28, tube_steps=5, reactor_attempts=40)
     out_t1 = np.zeros((6 + h2.ns) * n_t)
     out_r1 = abi.Reactor()
-    res1, _ = serve.serve(ctx_r, ctx_t, [_tube_req(n_t, 2e-6, out=out_t1)], opt)
-    res2, _ = serve.serve(ctx_r, ctx_t, [_reactor_req(h2, 1200.0, 3e5, 1.0, 2e-5, out=out_r1)], opt)
+    # short end times: behind the hot side the reaction time scale limits the tube steps to ~1e-10 s
+    res1, _ = serve.serve(ctx_r, ctx_t, [_tube_req(n_t, 2e-7, out=out_t1)], opt)
+    res2, _ = serve.serve(ctx_r, ctx_t, [_reactor_req(h2, 1200.0, 3e5, 1.0, 5e-6, out=out_r1)], opt)
     out_t2 = np.zeros_like(out_t1)
     out_r2 = abi.Reactor()
-    mix = [_tube_req(400, 3e-6, 0.0), _tube_req(n_t, 2e-6, 0.001, out=out_t2), _tube_req(1000, 1e-6, 0.0),
-           _reactor_req(h2, 1400.0, 8e5, 0.7, 2e-5, 0.0), _reactor_req(h2, 1200.0, 3e5, 1.0, 2e-5, 0.002, out=out_r2),
-           _tube_req(50, 5e-6, 0.0)]
+    mix = [_tube_req(400, 3e-7, 0.0), _tube_req(n_t, 2e-7, 0.001, out=out_t2), _tube_req(1000, 1e-7, 0.0),
+           _reactor_req(h2, 1400.0, 8e5, 0.7, 5e-6, 0.0), _reactor_req(h2, 1200.0, 3e5, 1.0, 5e-6, 0.002, out=out_r2),
+           _tube_req(50, 5e-7, 0.0)]
     resm, stats = serve.serve(ctx_r, ctx_t, mix, opt)
     assert all(r.status == 1 for r in resm)
     assert res1[0].status == 1 and res2[0].status == 1
