@@ -50,8 +50,8 @@ __device__ __forceinline__ BFlags bflags(const Zone &z, int i, int j, int k) {
   return b;
 }
 
-// 8th-order kernels: one thread per node, CTAs of kVisTI (i) x kVisTJ (j) nodes of one k-plane,
-// so the j-neighbours of a stencil are mostly lines the same CTA already brought into L1.
+// 8th-order node fluxes: one thread per node, CTAs of kVisTI (i) x kVisTJ (j) nodes of one
+// k-plane, so the j-neighbours of a stencil are mostly lines the same CTA brought into L1.
 constexpr int kVisTI = 32, kVisTJ = 8, kVisThreads = kVisTI * kVisTJ;
 
 // Node fluxes of the momentum and energy equations (air); comps 1..4 of fFlux/gFlux/hFlux.
@@ -117,10 +117,14 @@ __global__ void __launch_bounds__(kVisThreads) k_visc8_node_flux_air(Zone z, Par
   z.hF[g + 4 * sz] = zeta_x * Ex + zeta_y * Ey + zeta_z * Ez;
 }
 
+// The divergence reads each flux array along one direction only; rows of kVisRow i-nodes
+// measured faster than 2-D tiles for it.
+constexpr int kVisRow = 128;
+
 template <typename T>
-__global__ void __launch_bounds__(kVisThreads) k_visc8_divergence(Zone z, Param p) {
-  const int i = blockIdx.x * kVisTI + threadIdx.x, j = blockIdx.y * kVisTJ + threadIdx.y, k = blockIdx.z;
-  if (i >= z.mx || j >= z.my) return;
+__global__ void __launch_bounds__(kVisRow) k_visc8_divergence(Zone z, Param p) {
+  const int i = blockIdx.x * kVisRow + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  if (i >= z.mx) return;
   const Layout &L = z.L;
   const idx_t sz = L.sz, g = L.at(i, j, k);
   const BFlags b = bflags(z, i, j, k);
@@ -318,7 +322,8 @@ int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_fac
     {
       ProfScope prof("visc8_divergence", s);
       // the divergence is a load-bound sum of four 9-point stencils: FP64 in both forms
-      k_visc8_divergence<double><<<grid, block, 0, s>>>(z, p);
+      const dim3 grow((z.mx + kVisRow - 1) / kVisRow, z.my, z.mz);
+      k_visc8_divergence<double><<<grow, kVisRow, 0, s>>>(z, p);
     }
     ++nl;
     return check_launch();
