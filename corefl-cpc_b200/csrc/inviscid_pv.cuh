@@ -380,41 +380,23 @@ __host__ __device__ constexpr size_t pv_tile_smem(int dir) {
                       (size_t)(2 * (5 + NS) + 2) * kSweepThreads);
 }
 
-// Asynchronous 8-byte global->shared copies (completed by cp_async_wait_all).
-__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
-// Phases of a sweep tile: kTileAll loads the node data and computes; kTileLoadAsync only issues
-// the node-data copies as cp.async (T = double) and returns; kTileCompute assumes the node data
-// is in sN already.
-constexpr int kTileAll = 0, kTileLoadAsync = 1, kTileCompute = 2;
-
 // One tile of the sweep: tile (bx, by, bz) of the grid that node_sweep_grid describes, run by a
 // CTA of kSweepThreads threads; sN holds the node data [NSLOT][NN], sR the right states
-// [NV+2][kSweepThreads], sF the interface fluxes [NV][kSweepThreads].  The compute phase begins
-// and ends with the whole CTA in step, so a CTA may run several tiles back to back.
-template <typename T, int NS, int DIR, int REC, int SOLVER, int PHASE>
-__device__ __forceinline__ void pv_tile_phase(const Zone &z, const Param &p, idx_t run, int bx, int by, int bz,
-                                              T *sN, T *sR, T *sF) {
+// [NV+2][kSweepThreads], sF the interface fluxes [NV][kSweepThreads].  The tile ends with the
+// whole CTA in step, so a CTA may run several tiles back to back.
+template <typename T, int NS, int DIR, int REC, int SOLVER>
+__device__ __forceinline__ void pv_tile_body(const Zone &z, const Param &p, idx_t run, int bx, int by, int bz,
+                                             T *sN, T *sR, T *sF) {
   constexpr int NV = 5 + NS;
   constexpr int RH = pv_half_width<REC>();
   constexpr int NN = DIR == 0 ? (kSweepThreads + 2 * RH) : kNI * (kNS + 2 * RH);
-  static_assert(PHASE != kTileLoadAsync || sizeof(T) == 8, "asynchronous node loads copy FP64 values");
   const int tid = threadIdx.x;
   const int g = z.ngg;
   const Layout &L = z.L;
   const idx_t sz = L.sz;
 
-  auto put = [&](int idx, const double *src) {
-    if constexpr (PHASE == kTileLoadAsync) cp_async8(&sN[idx], src);
-    else sN[idx] = T(*src);
-  };
+  auto put = [&](int idx, const double *src) { sN[idx] = T(*src); };
   auto load = [&](idx_t gi, int slot, int i, int j, int k) {
-    if constexpr (PHASE == kTileCompute) return;
 #pragma unroll
     for (int l = 0; l < 5; ++l) put(l * NN + slot, z.bv + gi + l * sz);
 #pragma unroll
@@ -479,7 +461,6 @@ __device__ __forceinline__ void pv_tile_phase(const Zone &z, const Param &p, idx
     c = (ts + RH) * kNI + ti;
     st = kNI;
   }
-  if constexpr (PHASE == kTileLoadAsync) return;
   const bool rec = inside && n >= -1 && n <= ms;
   const bool face = rec && n <= ms - 1 && tpos < (DIR == 0 ? kSweepThreads : kNS) - 1;
   const bool upd = face && n >= 0 && tpos >= 1;
@@ -537,59 +518,13 @@ __device__ __forceinline__ void pv_tile(const Zone &z, const Param &p, idx_t run
   T *sN = reinterpret_cast<T *>(pv_smem);
   T *sR = sN + NSLOT * NN;
   T *sF = sR + (NV + 2) * kSweepThreads;
-  pv_tile_phase<T, NS, DIR, REC, SOLVER, kTileAll>(z, p, run, bx, by, bz, sN, sR, sF);
+  pv_tile_body<T, NS, DIR, REC, SOLVER>(z, p, run, bx, by, bz, sN, sR, sF);
 }
 
 template <typename T, int NS, int DIR, int REC, int SOLVER>
 __global__ void __launch_bounds__(kSweepThreads) k_inviscid_pv(Zone z, Param p, idx_t run) {
   extern __shared__ __align__(16) unsigned char pv_smem[];
   pv_tile<T, NS, DIR, REC, SOLVER>(z, p, run, blockIdx.x, blockIdx.y, blockIdx.z, pv_smem);
-}
-
-// Persistent, double-buffered FP64 sweep: each CTA walks the tiles blockIdx.x, +gridDim.x, ...
-// and issues the cp.async copies of its next tile's node data before computing the current
-// one, so the loads of one tile overlap the arithmetic of the previous.  The arithmetic is the
-// same as k_inviscid_pv's.
-template <int NS, int DIR, int REC, int SOLVER>
-__global__ void __launch_bounds__(kSweepThreads) k_inviscid_pv_pipe(Zone z, Param p, idx_t run, int nbx, int nby,
-                                                                     int ntiles) {
-  constexpr int NV = 5 + NS;
-  constexpr int RH = pv_half_width<REC>();
-  constexpr int NN = DIR == 0 ? (kSweepThreads + 2 * RH) : kNI * (kNS + 2 * RH);
-  constexpr int NSLOT = NV + 4 + (SOLVER == CB2_INV_ROE ? 1 : 0);
-  extern __shared__ __align__(16) unsigned char pv_smem[];
-  double *buf[2];
-  buf[0] = reinterpret_cast<double *>(pv_smem);
-  buf[1] = buf[0] + NSLOT * NN;
-  double *sR = buf[1] + NSLOT * NN;
-  double *sF = sR + (NV + 2) * kSweepThreads;
-  auto decode = [&](int t, int &bx, int &by, int &bz) {
-    bx = t % nbx;
-    const int r = t / nbx;
-    by = r % nby;
-    bz = r / nby;
-  };
-  int t = blockIdx.x;
-  if (t >= ntiles) return;
-  int bx, by, bz;
-  decode(t, bx, by, bz);
-  pv_tile_phase<double, NS, DIR, REC, SOLVER, kTileLoadAsync>(z, p, run, bx, by, bz, buf[0], sR, sF);
-  cp_async_commit();
-  int cur = 0;
-  for (; t < ntiles; t += gridDim.x) {
-    cp_async_wait_all();
-    __syncthreads();
-    const int tn = t + gridDim.x;
-    if (tn < ntiles) {
-      int nx, ny, nz;
-      decode(tn, nx, ny, nz);
-      pv_tile_phase<double, NS, DIR, REC, SOLVER, kTileLoadAsync>(z, p, run, nx, ny, nz, buf[cur ^ 1], sR, sF);
-      cp_async_commit();
-    }
-    decode(t, bx, by, bz);
-    pv_tile_phase<double, NS, DIR, REC, SOLVER, kTileCompute>(z, p, run, bx, by, bz, buf[cur], sR, sF);
-    cur ^= 1;
-  }
 }
 
 // Entropy-fix delta of the Roe scheme on [-1, m] in every direction (ghost width 1), FP64.
@@ -615,28 +550,6 @@ __global__ void k_entropy_fix_delta(Zone z, Param p) {
   z.efd[z.L1.at(i, j, k)] = d;
 }
 
-// Persistent launch of the pipelined FP64 sweep: as many CTAs as fit on the GPU at once.
-template <int NS, int DIR, int REC, int SOLVER>
-static int launch_pv_pipe(const Zone &z, const Param &p, idx_t run, dim3 tiles, cudaStream_t s) {
-  constexpr int NV = 5 + NS;
-  constexpr int RH = pv_half_width<REC>();
-  constexpr int NN = DIR == 0 ? (kSweepThreads + 2 * RH) : kNI * (kNS + 2 * RH);
-  constexpr int NSLOT = NV + 4 + (SOLVER == CB2_INV_ROE ? 1 : 0);
-  constexpr size_t smem = sizeof(double) * (2 * (size_t)NSLOT * NN + (size_t)(2 * NV + 2) * kSweepThreads);
-  auto kern = k_inviscid_pv_pipe<NS, DIR, REC, SOLVER>;
-  CB2_TRY(prepare_smem(kern, smem));
-  int dev = 0, n_sm = 0, per_sm = 0;
-  CB2_TRY(check_cuda(cudaGetDevice(&dev)));
-  CB2_TRY(check_cuda(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev)));
-  CB2_TRY(check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kSweepThreads, smem)));
-  const long long ntiles = (long long)tiles.x * tiles.y * tiles.z;
-  if (ntiles <= 0) return CB2_OK;
-  if (ntiles > 0x7fffffffLL) return CB2_ERR_UNSUPPORTED;
-  const int nb = (int)std::min<long long>(ntiles, (long long)std::max(1, per_sm) * n_sm);
-  kern<<<nb, kSweepThreads, smem, s>>>(z, p, run, (int)tiles.x, (int)tiles.y, (int)ntiles);
-  return check_launch();
-}
-
 template <typename T, int NS, int REC, int SOLVER>
 static int launch_pv_dirs(const Zone &z, const Param &p, cudaStream_t s, int &nl) {
   if (SOLVER == CB2_INV_ROE) {
@@ -653,14 +566,6 @@ static int launch_pv_dirs(const Zone &z, const Param &p, cudaStream_t s, int &nl
     const size_t smem = pv_tile_smem<T, NS, REC, SOLVER>(d);
     static const char *names[3] = {"pv_flux_x", "pv_flux_y", "pv_flux_z"};
     ProfScope prof(names[d], s);
-    if constexpr (sizeof(T) == 8 && NS == 0) {
-      // air, FP64: the pipelined persistent sweep (its double buffer fits 3 CTAs per SM)
-      if (d == 0) CB2_TRY((launch_pv_pipe<NS, 0, REC, SOLVER>(z, p, geo.run, grid, s)));
-      else if (d == 1) CB2_TRY((launch_pv_pipe<NS, 1, REC, SOLVER>(z, p, 0, grid, s)));
-      else CB2_TRY((launch_pv_pipe<NS, 2, REC, SOLVER>(z, p, 0, grid, s)));
-      ++nl;
-      continue;
-    }
     if (d == 0) {
       auto kern = k_inviscid_pv<T, NS, 0, REC, SOLVER>;
       CB2_TRY(prepare_smem(kern, smem));
