@@ -45,6 +45,8 @@ def load():
         "cb2_cv_from_bv": (C.c_int, [vp, C.c_int, vp]),
         "cb2_cfl_dt": (C.c_int, [vp, P(C.c_double), vp]),
         "cb2_rk3_step": (C.c_int, [vp, P(C.c_double), C.c_int, vp]),
+        "cb2_rk3_run": (C.c_int, [vp, C.c_double, C.c_int, C.c_longlong, C.c_double, P(C.c_double),
+                                  P(C.c_longlong), P(C.c_double), vp]),
         "cb2_read_status": (C.c_int, [vp, P(C.c_uint), vp]),
         "cb2_strerror": (C.c_char_p, [C.c_int]),
         "cb2_last_cuda_error": (C.c_char_p, []),
@@ -116,6 +118,16 @@ class Context:
         d = C.c_double(dt)
         check(self.lib.cb2_rk3_step(self.h, C.byref(d), 1 if fixed_dt else 0, stream), "cb2_rk3_step")
         return d.value
+
+    def rk3_run(self, max_steps, t_end=float("inf"), time=0.0, dt=0.0, fixed_dt=False, stream=None):
+        """Device-driven loop of up to max_steps steps until time >= t_end (one graph launch).
+        Returns (time reached, steps taken, last dt)."""
+        t = C.c_double(time)
+        n = C.c_longlong(0)
+        d = C.c_double(0.0)
+        check(self.lib.cb2_rk3_run(self.h, dt, 1 if fixed_dt else 0, max_steps, t_end, C.byref(t), C.byref(n),
+                                   C.byref(d), stream), "cb2_rk3_run")
+        return t.value, n.value, d.value
 
     def reactor_setup(self, reactors, n, T0, p0, Y, t_end, h0=1e-8, stream=None):
         """Set n reactors (device pointer to abi.Reactor[n]) from device pointers T0, p0, Y

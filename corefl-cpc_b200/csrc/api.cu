@@ -1,5 +1,6 @@
 // extern "C" entry points of libcb200 (declared in include/cb200.h) and the RK3 step
 // orchestration (the stage body of RK3<mix>, src/RK.cuh:107-237).
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -94,6 +95,17 @@ struct cb2_ctx {
   std::vector<Block> blocks;
   unsigned long long n_launch = 0;
   Profiler *prof = nullptr;  // non-null while profiling is enabled
+  unsigned long long bind_gen = 0;  // bumped by every cb2_bind_block (invalidates the step graph)
+  // device-driven step loop of cb2_rk3_run: one CUDA graph whose WHILE node replays one step
+  struct StepGraph {
+    cudaStream_t capture = nullptr;  // capture stream (non-blocking, created on first use)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long gen = ~0ull;  // bind_gen the graph was captured at
+    int fixed_dt = -1;               // the dt mode it was captured in
+    unsigned long long launches = 0; // kernels per step inside the graph
+  } sg;
+  RunState *d_run = nullptr;  // time, t_end, dt, step counter of the graph loop
 };
 
 namespace cb2 {
@@ -345,6 +357,10 @@ int cb2_init(const cb2_param_view *pv, cb2_ctx **out) {
 
 void cb2_destroy(cb2_ctx *ctx) {
   if (!ctx) return;
+  if (ctx->sg.exec) cudaGraphExecDestroy(ctx->sg.exec);
+  if (ctx->sg.graph) cudaGraphDestroy(ctx->sg.graph);
+  if (ctx->sg.capture) cudaStreamDestroy(ctx->sg.capture);
+  cudaFree(ctx->d_run);
   for (auto &b : ctx->blocks) cudaFree(b.d_btype);
   cudaFree(ctx->d_tables);
   cudaFree(ctx->d_status);
@@ -476,6 +492,7 @@ int cb2_bind_block(cb2_ctx *ctx, int blk, const cb2_zone_view *v, const cb2_face
     ctx->n_partial = np;
   }
   B.bound = true;
+  ++ctx->bind_gen;
   return CB2_OK;
 }
 
@@ -588,21 +605,22 @@ int cb2_cfl_dt(cb2_ctx *ctx, double *dt_out, void *stream) {
   return CB2_OK;
 }
 
-int cb2_rk3_step(cb2_ctx *ctx, double *dt_inout, int fixed_dt, void *stream) {
-  if (!ctx || !dt_inout) return CB2_ERR_INVALID;
-  ProfGuard pg(ctx);
+}  // extern "C"
+
+// qn <- cv and the shock sensor of every bound block: the part of a step before its dt.
+static int enqueue_step_head(cb2_ctx *ctx, void *stream) {
   const int nb = (int)ctx->blocks.size();
   for (int b = 0; b < nb; ++b)
     if (ctx->blocks[b].bound) CB2_TRY(cb2_store_qn(ctx, b, stream));
   if (ctx->p.sensor_threshold > 1e-10)  // hybrid linear/WENO weights (src/RK.cuh:139-143)
     for (int b = 0; b < nb; ++b)
       if (ctx->blocks[b].bound) CB2_TRY(cb2_shock_sensor(ctx, b, stream));
-  double dt = *dt_inout;
-  if (!fixed_dt) {
-    CB2_TRY(cb2_cfl_dt(ctx, &dt, stream));
-    *dt_inout = dt;
-  }
-  ctx->p.dt = dt;
+  return CB2_OK;
+}
+
+// The three stages of a step (src/RK.cuh:164-237).
+static int enqueue_stages(cb2_ctx *ctx, double dt, void *stream) {
+  const int nb = (int)ctx->blocks.size();
   for (int rk = 0; rk < 3; ++rk) {
     for (int b = 0; b < nb; ++b) {
       if (!ctx->blocks[b].bound) continue;
@@ -613,6 +631,120 @@ int cb2_rk3_step(cb2_ctx *ctx, double *dt_inout, int fixed_dt, void *stream) {
     for (int b = 0; b < nb; ++b)
       if (ctx->blocks[b].bound) CB2_TRY(cb2_properties(ctx, b, stream));
   }
+  return CB2_OK;
+}
+
+static void drop_step_graph(cb2_ctx *ctx) {
+  auto &g = ctx->sg;
+  if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (g.graph) cudaGraphDestroy(g.graph);
+  g.exec = nullptr;
+  g.graph = nullptr;
+  g.gen = ~0ull;
+  g.fixed_dt = -1;
+}
+
+// Builds the graph of cb2_rk3_run: a WHILE node whose body, captured from the same enqueue
+// functions cb2_rk3_step uses, is one step followed by k_run_advance.  Inside the body every
+// kernel reads the step's dt from the device (Param::dt_dev): RunState::dt in fixed mode, the
+// CFL minimum otherwise.  Per-launch profiling is off inside the graph.
+static int capture_step_graph(cb2_ctx *ctx, int fixed_dt) {
+  auto &g = ctx->sg;
+  drop_step_graph(ctx);
+  if (!g.capture) CB2_TRY(check_cuda(cudaStreamCreateWithFlags(&g.capture, cudaStreamNonBlocking)));
+  if (!ctx->d_run) CB2_TRY(check_cuda(cudaMalloc(&ctx->d_run, sizeof(RunState))));
+  CB2_TRY(check_cuda(cudaGraphCreate(&g.graph, 0)));
+  cudaGraphConditionalHandle h;
+  int rc = check_cuda(cudaGraphConditionalHandleCreate(&h, g.graph, 1u, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams np{};
+  cudaGraphNode_t node;
+  if (rc == CB2_OK) {
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    rc = check_cuda(cudaGraphAddNode(&node, g.graph, nullptr, 0, &np));
+  }
+  if (rc != CB2_OK) {
+    drop_step_graph(ctx);
+    return rc;
+  }
+  const Param saved = ctx->p;
+  Profiler *saved_prof = ctx->prof;
+  const unsigned long long n0 = ctx->n_launch;
+  ctx->prof = nullptr;
+  ctx->p.dt_dev = fixed_dt ? &ctx->d_run->dt : ctx->d_dtmin;
+  cudaStream_t s = g.capture;
+  rc = check_cuda(cudaStreamBeginCaptureToGraph(s, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                cudaStreamCaptureModeRelaxed));
+  if (rc == CB2_OK) {
+    rc = enqueue_step_head(ctx, s);
+    if (rc == CB2_OK && !fixed_dt) rc = enqueue_cfl_dt(ctx, s);
+    if (rc == CB2_OK) rc = enqueue_stages(ctx, 0.0, s);
+    int nl = 0;
+    if (rc == CB2_OK) rc = launch_run_advance(ctx->d_run, ctx->p.dt_dev, ctx->d_status, h, s, nl);
+    cudaGraph_t body = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s, &body);
+    if (rc == CB2_OK && e != cudaSuccess) rc = fail_cuda(e);
+  }
+  g.launches = ctx->n_launch - n0 + 1;  // the step's kernels and k_run_advance
+  ctx->n_launch = n0;
+  ctx->p = saved;
+  ctx->prof = saved_prof;
+  if (rc == CB2_OK) rc = check_cuda(cudaGraphInstantiate(&g.exec, g.graph, 0));
+  if (rc != CB2_OK) {
+    drop_step_graph(ctx);
+    return rc;
+  }
+  g.gen = ctx->bind_gen;
+  g.fixed_dt = fixed_dt;
+  return CB2_OK;
+}
+
+extern "C" {
+
+int cb2_rk3_step(cb2_ctx *ctx, double *dt_inout, int fixed_dt, void *stream) {
+  if (!ctx || !dt_inout) return CB2_ERR_INVALID;
+  ProfGuard pg(ctx);
+  CB2_TRY(enqueue_step_head(ctx, stream));
+  double dt = *dt_inout;
+  if (!fixed_dt) {
+    CB2_TRY(cb2_cfl_dt(ctx, &dt, stream));
+    *dt_inout = dt;
+  }
+  ctx->p.dt = dt;
+  return enqueue_stages(ctx, dt, stream);
+}
+
+int cb2_rk3_run(cb2_ctx *ctx, double dt, int fixed_dt, long long max_steps, double t_end, double *time_inout,
+                long long *steps_out, double *dt_last_out, void *stream) {
+  if (!ctx || !time_inout || !steps_out || max_steps < 0 || std::isnan(t_end)) return CB2_ERR_INVALID;
+  if (fixed_dt && !(dt > 0.0 && dt < 1e300)) return CB2_ERR_INVALID;
+  *steps_out = 0;
+  if (max_steps == 0 || !(*time_inout < t_end)) return CB2_OK;
+  bool any = false;
+  for (auto &B : ctx->blocks) {
+    any = any || B.bound;
+    if (B.bound && !fixed_dt && !B.z.dtl) return CB2_ERR_INVALID;
+  }
+  if (!any) return CB2_ERR_INVALID;
+  fixed_dt = fixed_dt ? 1 : 0;
+  if (!ctx->sg.exec || ctx->sg.gen != ctx->bind_gen || ctx->sg.fixed_dt != fixed_dt)
+    CB2_TRY(capture_step_graph(ctx, fixed_dt));
+  cudaStream_t s = (cudaStream_t)stream;
+  RunState h{*time_inout, t_end, fixed_dt ? dt : 0.0, 0, max_steps};
+  CB2_TRY(check_cuda(cudaMemcpyAsync(ctx->d_run, &h, sizeof(h), cudaMemcpyHostToDevice, s)));
+  CB2_TRY(check_cuda(cudaGraphLaunch(ctx->sg.exec, s)));
+  unsigned status = 0;
+  CB2_TRY(check_cuda(cudaMemcpyAsync(&h, ctx->d_run, sizeof(h), cudaMemcpyDeviceToHost, s)));
+  CB2_TRY(check_cuda(cudaMemcpyAsync(&status, ctx->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, s)));
+  CB2_TRY(check_cuda(cudaStreamSynchronize(s)));
+  ctx->n_launch += (unsigned long long)h.step * ctx->sg.launches;
+  *time_inout = h.time;
+  *steps_out = h.step;
+  if (dt_last_out) *dt_last_out = h.dt;
+  ctx->p.dt = h.dt;
+  if (status != 0u || !(h.dt > 0.0 && h.dt < 1e300)) return CB2_ERR_NONPHYSICAL;
   return CB2_OK;
 }
 

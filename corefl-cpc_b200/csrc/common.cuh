@@ -96,6 +96,7 @@ struct Param {
   int limit_flow;
   double lf_ll[5], lf_ul[5];  // limit_flow bounds of rho, u, v, w, p
   double dt;                  // the current step's time step (positivity limiter)
+  const double *dt_dev;       // non-null: the step's time step lives on the device (graph runs)
   unsigned *status;  // device status word
   Mech mech;
 };
@@ -103,6 +104,10 @@ struct Param {
 __device__ __forceinline__ void flag_status(const Param &p, unsigned bits) {
   if (p.status) atomicOr(p.status, bits);
 }
+
+// The step's time step: the device copy when the step runs inside a device-driven graph,
+// otherwise the value the launch carries.
+__device__ __forceinline__ double step_dt(const Param &p, double dt) { return p.dt_dev ? *p.dt_dev : dt; }
 
 // SSP-RK3 Shu-Osher coefficients (src/RK.cuh:12-16).
 __device__ __forceinline__ void ssprk3_coeff(int rk, double &a, double &b, double &c) {

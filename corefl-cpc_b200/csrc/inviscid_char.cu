@@ -208,7 +208,7 @@ __device__ __forceinline__ void load_node(const Zone &z, idx_t g, double *sQ, do
 template <int NS>
 __device__ __forceinline__ void positive_limit(const double *sQ, const double *sF, int NN, int cl, int cr,
                                                const Param &p, double *fc) {
-  const double dt = p.dt;
+  const double dt = step_dt(p, p.dt);
   const double alpha = p.dim == 3 ? 1.0 / 3.0 : 0.5;
   const double jl = sF[6 * NN + cl], jr = sF[6 * NN + cr];
   const double alphaL = 0.5 * alpha * jl, alphaR = 0.5 * alpha * jr;

@@ -87,6 +87,16 @@ int launch_min_reduce(const double *src, long long n, double *partial, int n_par
 int min_reduce_partials(long long n);
 int launch_set_value(double *dst, double v, cudaStream_t s, int &n_launch);
 
+// State of the device-driven step loop (cb2_rk3_run, graph.cu): the loop repeats while
+// step < max_steps, time < t_end, dt is positive and finite and the status word is clear.
+struct RunState {
+  double time, t_end;
+  double dt;  // fixed mode: the step every iteration takes; CFL mode: the last step taken
+  long long step, max_steps;
+};
+int launch_run_advance(RunState *r, const double *dt, const unsigned *status, cudaGraphConditionalHandle h,
+                       cudaStream_t s, int &n_launch);
+
 // batched 0-D reactors (reactor.cu); the state type is cb2_reactor of cb200_serve.h
 int launch_reactor_setup(const Param &p, cb2_reactor *r, int n, const double *T0, const double *p0,
                          const double *Y, const double *t_end, double h0, cudaStream_t s);

@@ -15,7 +15,7 @@ __global__ void __launch_bounds__(kPtThreads) k_stage_update(Zone z, Param p, do
   const int i = blockIdx.x * kPtThreads + threadIdx.x;
   const int j = blockIdx.y, k = blockIdx.z;
   if (i >= z.mx) return;
-  stage_update_point<NS>(z, p, dt, rk, i, j, k);
+  stage_update_point<NS>(z, p, step_dt(p, dt), rk, i, j, k);
 }
 
 template <int NS>

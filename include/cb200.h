@@ -248,6 +248,23 @@ int cb2_min_dt_noalloc(const double *dt_local, long long n, double *dt_min, void
  * and written to *dt_inout. */
 int cb2_rk3_step(cb2_ctx *ctx, double *dt_inout, int fixed_dt, void *stream);
 
+/* Device-driven time loop (the while loop of RK3<mix>, src/RK.cuh:107-261): up to max_steps
+ * SSP-RK3 steps over all bound blocks, stopping once the accumulated time *time_inout
+ * reaches t_end (physical_time >= total_simulation_time, src/RK.cuh:257), all in ONE launch of
+ * a CUDA graph whose conditional WHILE node repeats a captured step; the loop test runs on
+ * the device, so there is no host round trip per step.  With fixed_dt != 0 every step takes
+ * dt; otherwise each step computes the CFL dt on the device first (cb2_cfl_dt's kernels) and
+ * every bound block needs dt_local.  The loop also ends after a step that sets the status
+ * word (clear it first with cb2_read_status) or takes a non-positive or non-finite dt; the
+ * call then returns CB2_ERR_NONPHYSICAL and the status word stays set.  On return
+ * *time_inout holds the time reached, *steps_out the steps taken and *dt_last_out (may be
+ * NULL) the last dt.  Synchronises `stream` once, at the end.  The graph is captured on the
+ * first call and again after cb2_bind_block or a change of fixed_dt; the steps give results
+ * identical to as many cb2_rk3_step calls.  Per-launch profiling does not see the graph's
+ * kernels. */
+int cb2_rk3_run(cb2_ctx *ctx, double dt, int fixed_dt, long long max_steps, double t_end, double *time_inout,
+                long long *steps_out, double *dt_last_out, void *stream);
+
 /* ---- diagnostics --------------------------------------------------------------------- */
 
 /* Reads and clears the device status word that kernels set on non-physical states

@@ -94,4 +94,6 @@ def test_null_context_calls_are_invalid(cb200_lib):
     assert cb200_lib.cb2_boundary(None, 0, None) == abi.ERR_INVALID
     d = C.c_double(0.0)
     assert cb200_lib.cb2_rk3_step(None, C.byref(d), 1, None) == abi.ERR_INVALID
+    t, n = C.c_double(0.0), C.c_longlong(0)
+    assert cb200_lib.cb2_rk3_run(None, 1e-3, 1, 10, 1.0, C.byref(t), C.byref(n), None, None) == abi.ERR_INVALID
     assert cb200_lib.cb2_launch_count(None) == 0
