@@ -419,6 +419,8 @@ int cb2_bind_block(cb2_ctx *ctx, int blk, const cb2_zone_view *v, const cb2_face
                      : (sch == CB2_INV_WENO5_CH || sch == CB2_INV_WENO5_CP ||
                         (pvpath && p.reconstruction == CB2_REC_WENO5)) ? 3 : 2;
   if (v->ngg < need_g) return CB2_ERR_INVALID;
+  // the sweeps index one padded k plane with 32-bit positions
+  if ((long long)(v->mx + 2 * v->ngg) * (v->my + 2 * v->ngg) >= (1LL << 31)) return CB2_ERR_UNSUPPORTED;
   if (!v->cv || !v->bv || !v->dq || !v->metric || !v->jac || !v->qn) return CB2_ERR_INVALID;
   if (p.n_spec > 0 && (!v->sv || !v->acoustic_speed || !v->gamma || !v->mul || !v->thermal_conductivity ||
                        !v->rho_D))
@@ -513,12 +515,13 @@ int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream) {
   cudaStream_t s = (cudaStream_t)stream;
   const Param &p = ctx->p;
   int nl = 0;
-  {
+  const bool visc = (mask & CB2_RHS_VISCOUS) && p.viscous_order > 0;
+  const bool assign = visc && viscous_assigns_dq(p);  // the viscous term writes dq: no zeroing
+  if (!assign) {
     ProfScope prof("zero_dq", s);
     CB2_TRY(check_cuda(cudaMemsetAsync(B->z.dq, 0, (size_t)B->z.L0.sz * p.n_var * sizeof(double), s)));
   }
-  if ((mask & CB2_RHS_VISCOUS) && p.viscous_order > 0)
-    CB2_TRY(launch_viscous(B->z, p, B->faces.data(), (int)B->faces.size(), s, nl));
+  if (visc) CB2_TRY(launch_viscous(B->z, p, B->faces.data(), (int)B->faces.size(), assign, s, nl));
   if ((mask & CB2_RHS_CHEMISTRY) && p.reaction) CB2_TRY(launch_chemistry(B->z, p, s, nl));
   if (mask & CB2_RHS_INVISCID) {
     if (p.inviscid_scheme == CB2_INV_WENO5_CH || p.inviscid_scheme == CB2_INV_WENO7_CH)

@@ -80,8 +80,14 @@ __device__ __forceinline__ void reconstruct_node(const T *sN, int NN, int c, int
       // data is a normal FP32 number; like the FP64 eps it only matters where beta ~ 0, where
       // both give the linear weights
       const T eps = sizeof(T) == 4 ? T(pv_eps(p, l) * 1e22) : T(pv_eps(p, l));
-      if constexpr (REC == 5) weno5_node(v, eps, pl[l], pr[l]);
-      else weno7_node(v, eps, pl[l], pr[l]);
+      if constexpr (sizeof(T) == 4) {
+        if constexpr (REC == 5) weno5_node_x2(v, eps, pl[l], pr[l]);
+        else weno7_node_x2(v, eps, pl[l], pr[l]);
+      } else if constexpr (REC == 5) {
+        weno5_node(v, eps, pl[l], pr[l]);
+      } else {
+        weno7_node(v, eps, pl[l], pr[l]);
+      }
     }
   }
 #undef PV
@@ -419,22 +425,25 @@ __device__ __forceinline__ void pv_tile_body(const Zone &z, const Param &p, idx_
   bool inside;
   int c, st;
   if constexpr (DIR == 0) {
+    // positions along the run of one k plane (q = j disp2 + i + g) fit in 32 bits: a plane
+    // holds far fewer than 2^31 nodes, and 32-bit division is several times cheaper
     k = bz;
-    const idx_t q0 = (idx_t)bx * (kSweepThreads - 2) - 1;
+    const int d2 = (int)L.disp2;
+    const int q0 = bx * (kSweepThreads - 2) - 1;
     const idx_t base = (idx_t)k * L.disp1 + L.dispt - g;
-    const idx_t qlo = q0 - RH;
-    const idx_t qmin = -(idx_t)L.gj * L.disp2, qmax = (idx_t)(L.my + L.gj) * L.disp2;
+    const int qlo = q0 - RH;
+    const int qmin = -L.gj * d2, qmax = (L.my + L.gj) * d2;
     for (int s = tid; s < NN; s += kSweepThreads) {
-      const idx_t q = qlo + s;
+      const int q = qlo + s;
       if (q >= qmin && q < qmax) {
-        const idx_t jj = q >= 0 ? q / L.disp2 : -((-q + L.disp2 - 1) / L.disp2);
-        load(base + q, s, (int)(q - jj * L.disp2) - g, (int)jj, k);
+        const int jj = q >= 0 ? q / d2 : -((-q + d2 - 1) / d2);
+        load(base + q, s, q - jj * d2 - g, jj, k);
       }
     }
-    const idx_t q = q0 + tid;
-    const idx_t jj = q >= 0 ? q / L.disp2 : -1;
-    i = (int)(q - jj * L.disp2) - g;
-    j = (int)jj;
+    const int q = q0 + tid;
+    const int jj = q >= 0 ? q / d2 : -1;
+    i = q - jj * d2 - g;
+    j = jj;
     n = i;
     ms = L.mx;
     inside = q >= 0 && q < run;

@@ -78,7 +78,11 @@ int launch_boundary(const Zone &z, const Param &p, const FaceBC *faces, int n_fa
 int launch_eliminate_k_gradient(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
 int launch_periodic_flux_exchange(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, cudaStream_t s,
                                   int &n_launch);
-int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, cudaStream_t s, int &n_launch);
+// The 8th-order air viscous term writes dq instead of adding to it (assign = true) when it runs
+// first in a residual; viscous_assigns_dq tells whether the settings take that path.
+bool viscous_assigns_dq(const Param &p);
+int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, bool assign, cudaStream_t s,
+                   int &n_launch);
 int launch_chemistry(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
 int launch_shock_sensor(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
 int launch_local_dt(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);

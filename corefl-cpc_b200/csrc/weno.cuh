@@ -203,6 +203,88 @@ __device__ __forceinline__ void weno7_node(const T *u, T eps, T &lp, T &rm) {
   rm = T(1.0 / 12) * (v0 * m0 + v1 * m1 + v2 * m2 + v3 * m3) / (v0 + v1 + v2 + v3);
 }
 
+// ---- packed FP32 node-centred pair ------------------------------------------------------
+// The minus side is the plus formula applied to the mirrored stencil, so both sides run as one
+// stream of float2 values through the sm_100 paired FP32 instructions (FFMA2, FADD2, FMUL2):
+// lane x is the plus side on u[k], lane y the minus side on u[last - k].  Mirroring maps the
+// plus sub-stencil r onto sub-stencil last - r, so the packed indicators of the first half of
+// the sub-stencils carry the others in lane y.  Per lane the arithmetic is the FP32 node form
+// above (D_min normalisation), with the final division done as a reciprocal and a product.
+__device__ __forceinline__ float2 p2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 swap2(float2 a) { return make_float2(a.y, a.x); }
+__device__ __forceinline__ float2 rcp2(float2 a) { return make_float2(rcp32(a.x), rcp32(a.y)); }
+// c0 a + c1 b + c2 c (+ c3 d) with scalar coefficients
+__device__ __forceinline__ float2 lin3(float c0, float2 a, float c1, float2 b, float c2, float2 c) {
+  return fma2(p2(c2), c, fma2(p2(c1), b, mul2(p2(c0), a)));
+}
+__device__ __forceinline__ float2 lin4(float c0, float2 a, float c1, float2 b, float c2, float2 c, float c3,
+                                       float2 d) {
+  return fma2(p2(c3), d, lin3(c0, a, c1, b, c2, c));
+}
+__device__ __forceinline__ float2 beta7_x2(float2 d1, float2 d2, float2 d3) {
+  // d1^2 + 13/12 d2^2 + 1043/960 d3^2 + d1 d3/12; invariant under (d1, d3) -> (-d1, -d3), the
+  // sign change that mirroring gives the first and third differences
+  const float2 t = fma2(p2(1.0f / 12), d3, d1);
+  return fma2(p2(1043.0f / 960), mul2(d3, d3), fma2(p2(13.0f / 12), mul2(d2, d2), mul2(d1, t)));
+}
+
+__device__ __forceinline__ void weno5_node_x2(const float *v, float eps, float &lp, float &rm) {
+  const float2 U0 = make_float2(v[0], v[4]), U1 = make_float2(v[1], v[3]), U2 = p2(v[2]);
+  const float2 U3 = make_float2(v[3], v[1]), U4 = make_float2(v[4], v[0]);
+  const float k6 = 1.0f / 6;
+  const float2 Q0 = lin3(2 * k6, U0, -7 * k6, U1, 11 * k6, U2);  // (q0, m0)
+  const float2 Q1 = lin3(-k6, U1, 5 * k6, U2, 2 * k6, U3);       // (q1, m1)
+  const float2 Q2 = lin3(2 * k6, U2, 5 * k6, U3, -k6, U4);       // (q2, m2)
+  const float2 e0 = lin3(1, U0, -2, U1, 1, U2), f0 = lin3(1, U0, -4, U1, 3, U2);
+  const float2 B0 = fma2(p2(13.0f / 12), mul2(e0, e0), mul2(p2(0.25f), mul2(f0, f0)));  // (b0, b2)
+  const float e1 = v[1] + v[3] - 2 * v[2], f1 = v[1] - v[3];
+  const float b1 = 13.0f / 12 * (e1 * e1) + 0.25f * (f1 * f1);
+  const float2 DA = mul2(add2(p2(eps), B0), add2(p2(eps), B0));  // (D0, D2)
+  const float D1 = (eps + b1) * (eps + b1);
+  const float Dm = fminf(fminf(DA.x, DA.y), D1);
+  const float2 EA = mul2(p2(Dm), rcp2(DA));  // (E0, E2)
+  const float E1 = Dm * rcp32(D1);
+  const float2 W0 = mul2(p2(0.1f), EA), W1 = p2(0.6f * E1), W2 = mul2(p2(0.3f), swap2(EA));
+  const float2 num = fma2(W2, Q2, fma2(W1, Q1, mul2(W0, Q0)));
+  const float2 den = add2(add2(W0, W1), W2);
+  const float2 r = mul2(num, rcp2(den));
+  lp = r.x;
+  rm = r.y;
+}
+
+__device__ __forceinline__ void weno7_node_x2(const float *u, float eps, float &lp, float &rm) {
+  float2 U[7];
+#pragma unroll
+  for (int k = 0; k < 7; ++k) U[k] = make_float2(u[k], u[6 - k]);
+  const float2 Q0 = lin4(-3, U[0], 13, U[1], -23, U[2], 25, U[3]);  // (q0, m0)
+  const float2 Q1 = lin4(1, U[1], -5, U[2], 13, U[3], 3, U[4]);
+  const float2 Q2 = lin4(-1, U[2], 7, U[3], 7, U[4], -1, U[5]);
+  const float2 Q3 = lin4(3, U[3], 13, U[4], -5, U[5], 1, U[6]);
+  const float k6 = 1.0f / 6;
+  const float2 B0 = beta7_x2(lin4(-2 * k6, U[0], 9 * k6, U[1], -18 * k6, U[2], 11 * k6, U[3]),
+                             lin4(-1, U[0], 4, U[1], -5, U[2], 2, U[3]), lin4(-1, U[0], 3, U[1], -3, U[2], 1, U[3]));
+  const float2 B1 = beta7_x2(lin4(k6, U[1], -6 * k6, U[2], 3 * k6, U[3], 2 * k6, U[4]), lin3(1, U[2], -2, U[3], 1, U[4]),
+                             lin4(-1, U[1], 3, U[2], -3, U[3], 1, U[4]));
+  // plus side: b0 = B0.x, b1 = B1.x, b2 = B1.y, b3 = B0.y
+  const float t = (B0.x - B0.y) + 3 * (B1.x - B1.y);
+  const float tau = t * t;  // unchanged by the mirroring
+  const float2 A0 = add2(p2(eps), B0), A1 = add2(p2(eps), B1);
+  const float2 DA = mul2(A0, A0), DB = mul2(A1, A1);  // (D0, D3), (D1, D2)
+  const float Dm = fminf(fminf(DA.x, DA.y), fminf(DB.x, DB.y));
+  const float2 EA = fma2(p2(tau), mul2(p2(Dm), rcp2(DA)), p2(Dm));  // (E0, E3)
+  const float2 EB = fma2(p2(tau), mul2(p2(Dm), rcp2(DB)), p2(Dm));  // (E1, E2)
+  const float2 W0 = mul2(p2(1.0f / 35), EA), W1 = mul2(p2(12.0f / 35), EB);
+  const float2 W2 = mul2(p2(18.0f / 35), swap2(EB)), W3 = mul2(p2(4.0f / 35), swap2(EA));
+  const float2 num = fma2(W3, Q3, fma2(W2, Q2, fma2(W1, Q1, mul2(W0, Q0))));
+  const float2 den = add2(add2(W0, W1), add2(W2, W3));
+  const float2 r = mul2(mul2(num, p2(1.0f / 12)), rcp2(den));
+  lp = r.x;
+  rm = r.y;
+}
+
 template <int ORDER, typename T>
 __device__ __forceinline__ T weno_pm(const T *vp, const T *vm, T eps, bool shock) {
   if constexpr (ORDER == 5) return weno5_plus(vp, eps, shock) + weno5_minus(vm, eps, shock);
