@@ -50,101 +50,71 @@ __device__ __forceinline__ BFlags bflags(const Zone &z, int i, int j, int k) {
   return b;
 }
 
-// 8th-order node fluxes.  A CTA owns a kVmTI x kVmTJ column tile of (i, j) and marches up
-// kVmKC planes in k.  Each thread keeps its own column of u, v, w, T at k-4 .. k+4 in registers
-// (the zeta stencil), and the CTA stages plane k with an i/j halo of 4 in shared memory (the
-// xi and eta stencils), so every field value is read from memory about 2.5 times instead of the
-// 25 times that independent 9-point stencils in three directions would read it.
-constexpr int kVmTI = 32, kVmTJ = 8, kVmKC = 32, kVmH = 4;
-constexpr int kVmThreads = kVmTI * kVmTJ;
-constexpr int kVmPI = kVmTI + 2 * kVmH, kVmPJ = kVmTJ + 2 * kVmH;  // staged plane extents
+// 8th-order node fluxes: one thread per node, CTAs of kVisTI (i) x kVisTJ (j) nodes of one
+// k-plane, so the j-neighbours of a stencil are mostly lines the same CTA brought into L1.
+constexpr int kVisTI = 32, kVisTJ = 8, kVisThreads = kVisTI * kVisTJ;
 
 // Node fluxes of the momentum and energy equations (air); comps 1..4 of fFlux/gFlux/hFlux.
 // T is the arithmetic type (double: plain form; float: mixed form, FP64 arrays read and
 // written, the stencils, stresses and fluxes evaluated in FP32).
 template <typename T>
-__global__ void __launch_bounds__(kVmThreads, 2) k_visc8_node_flux_air(Zone z, Param p) {
-  __shared__ T sP[4][kVmPJ][kVmPI];  // u, v, w, T of plane k
-  const int ti = threadIdx.x, tj = threadIdx.y, tid = tj * kVmTI + ti;
-  const int i0 = blockIdx.x * kVmTI, j0 = blockIdx.y * kVmTJ;
-  const int i = i0 + ti, j = j0 + tj;
-  const int k0 = blockIdx.z * kVmKC, k1 = min(k0 + kVmKC, z.mz);
-  const bool act = i < z.mx && j < z.my;
+__global__ void __launch_bounds__(kVisThreads) k_visc8_node_flux_air(Zone z, Param p) {
+  const int i = blockIdx.x * kVisTI + threadIdx.x, j = blockIdx.y * kVisTJ + threadIdx.y, k = blockIdx.z;
+  if (i >= z.mx || j >= z.my) return;
   const Layout &L = z.L;
-  const idx_t sz = L.sz;
-  const int comp[4] = {1, 2, 3, 5};  // u, v, w, T in bv
-  // this thread's column (clamped onto the block for threads past its edge, which only help
-  // to stage the planes)
-  const int ic = min(i, z.mx - 1), jc = min(j, z.my - 1);
-  const double *col = z.bv + L.at(ic, jc, 0);
-  T q[4][9];  // q[f][m]: field f at (i, j, k - 4 + m)
-#pragma unroll
-  for (int m = 1; m < 9; ++m)
-#pragma unroll
-    for (int f = 0; f < 4; ++f) q[f][m] = T(col[comp[f] * sz + (idx_t)(k0 - 5 + m) * L.disp1]);
-  const bool kl = z.bt.kl[ic + jc * z.mx] != 0, kr = z.bt.kr[ic + jc * z.mx] != 0;
+  const idx_t sz = L.sz, g = L.at(i, j, k);
+  const BFlags b = bflags(z, i, j, k);
+  const idx_t si = 1, sj = L.disp2, sk = L.disp1;
+  auto der = [&](int comp, T &dxi, T &deta, T &dzeta) {
+    const double *f = z.bv + comp * sz + g;
+    dxi = d8<T>([&](int m) { return T(f[m * si]); }, i, z.mx, b.il, b.ir);
+    deta = d8<T>([&](int m) { return T(f[m * sj]); }, j, z.my, b.jl, b.jr);
+    dzeta = d8<T>([&](int m) { return T(f[m * sk]); }, k, z.mz, b.kl, b.kr);
+  };
+  T u_xi, u_eta, u_zeta, v_xi, v_eta, v_zeta, w_xi, w_eta, w_zeta, t_xi, t_eta, t_zeta;
+  der(1, u_xi, u_eta, u_zeta);
+  der(2, v_xi, v_eta, v_zeta);
+  der(3, w_xi, w_eta, w_zeta);
+  der(5, t_xi, t_eta, t_zeta);
+  const double *M = z.metric + g;
+  const T xi_x = T(M[0]), xi_y = T(M[sz]), xi_z = T(M[2 * sz]);
+  const T eta_x = T(M[3 * sz]), eta_y = T(M[4 * sz]), eta_z = T(M[5 * sz]);
+  const T zeta_x = T(M[6 * sz]), zeta_y = T(M[7 * sz]), zeta_z = T(M[8 * sz]);
+  const T u_x = u_xi * xi_x + u_eta * eta_x + u_zeta * zeta_x;
+  const T u_y = u_xi * xi_y + u_eta * eta_y + u_zeta * zeta_y;
+  const T u_z = u_xi * xi_z + u_eta * eta_z + u_zeta * zeta_z;
+  const T v_x = v_xi * xi_x + v_eta * eta_x + v_zeta * zeta_x;
+  const T v_y = v_xi * xi_y + v_eta * eta_y + v_zeta * zeta_y;
+  const T v_z = v_xi * xi_z + v_eta * eta_z + v_zeta * zeta_z;
+  const T w_x = w_xi * xi_x + w_eta * eta_x + w_zeta * zeta_x;
+  const T w_y = w_xi * xi_y + w_eta * eta_y + w_zeta * zeta_y;
+  const T w_z = w_xi * xi_z + w_eta * eta_z + w_zeta * zeta_z;
+  const T mu = T(z.mul[g]);
+  const T txx = mu * (4 * u_x - 2 * v_y - 2 * w_z) / 3;
+  const T tyy = mu * (4 * v_y - 2 * u_x - 2 * w_z) / 3;
+  const T tzz = mu * (4 * w_z - 2 * u_x - 2 * v_y) / 3;
+  const T txy = mu * (u_y + v_x), txz = mu * (u_z + w_x), tyz = mu * (v_z + w_y);
+  const T t_x = t_xi * xi_x + t_eta * eta_x + t_zeta * zeta_x;
+  const T t_y = t_xi * xi_y + t_eta * eta_y + t_zeta * zeta_y;
+  const T t_z = t_xi * xi_z + t_eta * eta_z + t_zeta * zeta_z;
   const T cp = T(kGammaAir * kRAir / (kGammaAir - 1));
-  for (int k = k0; k < k1; ++k) {
-#pragma unroll
-    for (int f = 0; f < 4; ++f) {
-#pragma unroll
-      for (int m = 0; m < 8; ++m) q[f][m] = q[f][m + 1];
-      q[f][8] = T(col[comp[f] * sz + (idx_t)(k + 4) * L.disp1]);
-    }
-    __syncthreads();  // the previous plane's shared values are no longer read
-    for (int s = tid; s < kVmPI * kVmPJ; s += kVmThreads) {
-      const int a = s % kVmPI, b = s / kVmPI;
-      const int ii = i0 - kVmH + a, jj = j0 - kVmH + b;
-      if (ii >= -z.ngg && ii < z.mx + z.ngg && jj >= -L.gj && jj < z.my + L.gj) {
-        const double *src = z.bv + L.at(ii, jj, k);
-#pragma unroll
-        for (int f = 0; f < 4; ++f) sP[f][b][a] = T(src[comp[f] * sz]);
-      }
-    }
-    __syncthreads();
-    if (!act) continue;
-    const bool il = z.bt.il[j + k * z.my] != 0, ir = z.bt.ir[j + k * z.my] != 0;
-    const bool jl = z.bt.jl[i + k * z.mx] != 0, jr = z.bt.jr[i + k * z.mx] != 0;
-    const idx_t g = L.at(i, j, k);
-    const double *M = z.metric + g;
-    const T xi_x = T(M[0]), xi_y = T(M[sz]), xi_z = T(M[2 * sz]);
-    const T eta_x = T(M[3 * sz]), eta_y = T(M[4 * sz]), eta_z = T(M[5 * sz]);
-    const T zeta_x = T(M[6 * sz]), zeta_y = T(M[7 * sz]), zeta_z = T(M[8 * sz]);
-    T gx[4], gy[4], gz[4];  // Cartesian gradients of u, v, w, T
-#pragma unroll
-    for (int f = 0; f < 4; ++f) {
-      const T dxi = d8<T>([&](int m) { return sP[f][tj + kVmH][ti + kVmH + m]; }, i, z.mx, il, ir);
-      const T deta = d8<T>([&](int m) { return sP[f][tj + kVmH + m][ti + kVmH]; }, j, z.my, jl, jr);
-      const T dzeta = d8<T>([&](int m) { return q[f][4 + m]; }, k, z.mz, kl, kr);
-      gx[f] = dxi * xi_x + deta * eta_x + dzeta * zeta_x;
-      gy[f] = dxi * xi_y + deta * eta_y + dzeta * zeta_y;
-      gz[f] = dxi * xi_z + deta * eta_z + dzeta * zeta_z;
-    }
-    const T u_x = gx[0], u_y = gy[0], u_z = gz[0], v_x = gx[1], v_y = gy[1], v_z = gz[1];
-    const T w_x = gx[2], w_y = gy[2], w_z = gz[2];
-    const T mu = T(z.mul[g]);
-    const T txx = mu * (4 * u_x - 2 * v_y - 2 * w_z) / 3;
-    const T tyy = mu * (4 * v_y - 2 * u_x - 2 * w_z) / 3;
-    const T tzz = mu * (4 * w_z - 2 * u_x - 2 * v_y) / 3;
-    const T txy = mu * (u_y + v_x), txz = mu * (u_z + w_x), tyz = mu * (v_z + w_y);
-    const T kap = mu / T(p.Pr) * cp;
-    const T u = q[0][4], v = q[1][4], w = q[2][4];
-    const T Ex = u * txx + v * txy + w * txz + kap * gx[3];
-    const T Ey = u * txy + v * tyy + w * tyz + kap * gy[3];
-    const T Ez = u * txz + v * tyz + w * tzz + kap * gz[3];
-    z.fF[g + sz] = xi_x * txx + xi_y * txy + xi_z * txz;
-    z.fF[g + 2 * sz] = xi_x * txy + xi_y * tyy + xi_z * tyz;
-    z.fF[g + 3 * sz] = xi_x * txz + xi_y * tyz + xi_z * tzz;
-    z.gF[g + sz] = eta_x * txx + eta_y * txy + eta_z * txz;
-    z.gF[g + 2 * sz] = eta_x * txy + eta_y * tyy + eta_z * tyz;
-    z.gF[g + 3 * sz] = eta_x * txz + eta_y * tyz + eta_z * tzz;
-    z.hF[g + sz] = zeta_x * txx + zeta_y * txy + zeta_z * txz;
-    z.hF[g + 2 * sz] = zeta_x * txy + zeta_y * tyy + zeta_z * tyz;
-    z.hF[g + 3 * sz] = zeta_x * txz + zeta_y * tyz + zeta_z * tzz;
-    z.fF[g + 4 * sz] = xi_x * Ex + xi_y * Ey + xi_z * Ez;
-    z.gF[g + 4 * sz] = eta_x * Ex + eta_y * Ey + eta_z * Ez;
-    z.hF[g + 4 * sz] = zeta_x * Ex + zeta_y * Ey + zeta_z * Ez;
-  }
+  const T kap = mu / T(p.Pr) * cp;
+  const T u = T(z.bv[g + sz]), v = T(z.bv[g + 2 * sz]), w = T(z.bv[g + 3 * sz]);
+  const T Ex = u * txx + v * txy + w * txz + kap * t_x;
+  const T Ey = u * txy + v * tyy + w * tyz + kap * t_y;
+  const T Ez = u * txz + v * tyz + w * tzz + kap * t_z;
+  z.fF[g + sz] = xi_x * txx + xi_y * txy + xi_z * txz;
+  z.fF[g + 2 * sz] = xi_x * txy + xi_y * tyy + xi_z * tyz;
+  z.fF[g + 3 * sz] = xi_x * txz + xi_y * tyz + xi_z * tzz;
+  z.gF[g + sz] = eta_x * txx + eta_y * txy + eta_z * txz;
+  z.gF[g + 2 * sz] = eta_x * txy + eta_y * tyy + eta_z * tyz;
+  z.gF[g + 3 * sz] = eta_x * txz + eta_y * tyz + eta_z * tzz;
+  z.hF[g + sz] = zeta_x * txx + zeta_y * txy + zeta_z * txz;
+  z.hF[g + 2 * sz] = zeta_x * txy + zeta_y * tyy + zeta_z * tyz;
+  z.hF[g + 3 * sz] = zeta_x * txz + zeta_y * tyz + zeta_z * tzz;
+  z.fF[g + 4 * sz] = xi_x * Ex + xi_y * Ey + xi_z * Ez;
+  z.gF[g + 4 * sz] = eta_x * Ex + eta_y * Ey + eta_z * Ez;
+  z.hF[g + 4 * sz] = zeta_x * Ex + zeta_y * Ey + zeta_z * Ez;
 }
 
 // The divergence reads each flux array along one direction only; rows of kVisRow i-nodes
@@ -347,8 +317,7 @@ int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_fac
   if (p.viscous_order == 0) return CB2_OK;
   if (p.viscous_order == 8) {
     if (p.n_spec != 0) return CB2_ERR_UNSUPPORTED;
-    const dim3 grid((z.mx + kVmTI - 1) / kVmTI, (z.my + kVmTJ - 1) / kVmTJ, (z.mz + kVmKC - 1) / kVmKC);
-    const dim3 block(kVmTI, kVmTJ);
+    const dim3 grid((z.mx + kVisTI - 1) / kVisTI, (z.my + kVisTJ - 1) / kVisTJ, z.mz), block(kVisTI, kVisTJ);
     {
       ProfScope prof("visc8_node_flux", s);
       if (p.precision == CB2_PREC_MIXED) k_visc8_node_flux_air<float><<<grid, block, 0, s>>>(z, p);
