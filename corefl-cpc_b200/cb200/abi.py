@@ -1,7 +1,7 @@
 """ctypes mirror of include/cb200.h (structs and constants)."""
 import ctypes as C
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 OK = 0
 ERR_CUDA, ERR_INVALID, ERR_NONPHYSICAL, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_NOMEM = -1, -2, -3, -4, -5, -6
@@ -18,7 +18,7 @@ _ip = C.POINTER(C.c_int)
 
 ZONE_ARRAYS = ("cv", "bv", "sv", "qn", "dq", "metric", "jac", "mul", "thermal_conductivity", "rho_D",
                "acoustic_speed", "gamma", "mach", "fFlux", "gFlux", "hFlux", "vis_flux", "shock_sensor",
-               "dt_local", "reaction_timeScale", "entropy_fix_delta")
+               "dt_local", "reaction_timeScale", "entropy_fix_delta", "temperature_ve")
 
 
 class ZoneView(C.Structure):
@@ -45,6 +45,12 @@ class Mechanism(C.Structure):
                [(n, _dp) for n in MECH_DOUBLE] + [(n, _ip) for n in MECH_INT] + [(n, _dp) for n in MECH_REAC]
 
 
+class TwoTemperature(C.Structure):
+    _fields_ = [("n_spec", C.c_int), ("max_level", C.c_int), ("theta_v", _dp), ("n_level", _ip),
+                ("elec_theta", _dp), ("elec_g", _dp), ("lt_a", _dp), ("lt_b", _dp), ("park_sigma", _dp),
+                ("enable_vt_relaxation", C.c_int)]
+
+
 class ParamView(C.Structure):
     _fields_ = [("abi_version", C.c_int), ("dim", C.c_int), ("n_var", C.c_int), ("n_spec", C.c_int),
                 ("n_scalar", C.c_int), ("n_scalar_transported", C.c_int), ("inviscid_scheme", C.c_int),
@@ -54,7 +60,7 @@ class ParamView(C.Structure):
                 ("entropy_fix_factor", C.c_double), ("Pr", C.c_double), ("cfl", C.c_double),
                 ("rho_ref", C.c_double), ("v_ref", C.c_double), ("mu_constant", C.c_double),
                 ("precision", C.c_int), ("mech", C.POINTER(Mechanism)), ("limit_flow", C.c_int), ("p_ref", C.c_double),
-                ("c_ref", C.c_double), ("dt", C.c_double)]
+                ("c_ref", C.c_double), ("dt", C.c_double), ("two_t", C.POINTER(TwoTemperature))]
 
 
 # ---- batched solves (include/cb200_serve.h) ---------------------------------------------------

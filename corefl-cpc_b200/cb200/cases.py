@@ -36,7 +36,7 @@ class Case:
 
 def make_param(n_var=5, n_spec=0, dim=3, inviscid_scheme=abi.INV_WENO5_CH, reconstruction=abi.REC_MUSCL,
                viscous_order=0, Pr=0.72, cfl=0.5, rho_ref=1.0, v_ref=1.0, mu_constant=0.0,
-               entropy_fix_factor=0.125, mech=None, precision=abi.PREC_FP64):
+               entropy_fix_factor=0.125, mech=None, precision=abi.PREC_FP64, two_t=None):
     p = abi.ParamView()
     p.abi_version = abi.ABI_VERSION
     p.dim = dim
@@ -66,6 +66,11 @@ def make_param(n_var=5, n_spec=0, dim=3, inviscid_scheme=abi.INV_WENO5_CH, recon
     p.p_ref = 0.0
     p.c_ref = 0.0
     p.dt = 0.0
+    if two_t is not None:
+        # e_ve is the scalar after the species (i_eve = n_spec, src/Parameter.cpp:647-656)
+        p.two_t = two_t
+        p.n_scalar = n_spec + 1
+        p.n_scalar_transported = n_spec + 1
     return p
 
 
@@ -282,6 +287,36 @@ def h2_air_box(mech, n_nodes=192, ngg=3, length=1e-3, seed=2024, scheme=abi.INV_
                      rho_ref=float(rho.mean()), v_ref=c0, mech=mech.ptr())
     par.reaction = 1 if reaction else 0
     return Case("h2_air_box", par, [b], [faces], {"dt": 2e-9, "mech": mech, "dx": dx})
+
+
+def h2_air_box_2t(mech, tt, n_nodes=10, ngg=3, length=1e-3, seed=77, t_ve_ratio=0.6):
+    """Two-temperature H2/air box out of vibrational equilibrium: the reacting box's state
+    (velocity field, hot spots, 1 atm, stoichiometric mixture with 2 % of it moved to H, O and
+    OH) with T_ve = t_ve_ratio * T + 300 K at every node.  e_ve is left at zero, so a
+    cv-from-bv pass fills it from T_ve (sync_two_temperature_state_from_sv)."""
+    base = h2_air_box(mech, n_nodes=n_nodes, ngg=ngg, length=length, seed=seed, viscous_order=0, reaction=False)
+    hb0 = base.blocks[0]
+    m = n_nodes
+    ns = mech.ns
+    specs = array_specs(m, m, m, ngg, 6 + ns, ns + 1)
+    specs["temperature_ve"] = (1, ngg)
+    b = HostBlock(m, m, m, ngg, specs)
+    for name in ("bv", "metric", "jac", "mul", "mach", "thermal_conductivity", "acoustic_speed", "gamma"):
+        if name in hb0.a and name in b.a:
+            b.a[name][...] = hb0.a[name]
+    y = hb0.a["sv"].copy()
+    rng = np.random.default_rng(seed + 5)
+    moved = 0.02 * y[mech.index("O2")]
+    for name, share in (("H", 0.2), ("O", 0.3), ("OH", 0.5)):
+        y[mech.index(name)] += share * moved * rng.uniform(0.5, 1.5, moved.shape)
+    y[mech.index("O2")] -= moved
+    y /= y.sum(axis=0, keepdims=True)
+    b.a["sv"][:ns] = y
+    b.a["sv"][ns] = 0.0
+    b.a["temperature_ve"][0] = t_ve_ratio * b.a["bv"][5] + 300.0
+    par = make_param(n_var=6 + ns, n_spec=ns, dim=3, inviscid_scheme=abi.INV_HLLC, reconstruction=abi.REC_WENO5,
+                     cfl=0.5, rho_ref=base.param.rho_ref, v_ref=base.param.v_ref, mech=mech.ptr(), two_t=tt.ptr())
+    return Case("h2_air_box_2t", par, [b], base.faces, {"mech": mech, "two_t": tt, "dx": base.meta["dx"]})
 
 
 def reactive_shock_tube(mech, n_nodes=400, ngg=3, length=0.1, scheme=abi.INV_HLLC,

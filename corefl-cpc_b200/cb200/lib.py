@@ -41,6 +41,7 @@ def load():
         "cb2_shock_sensor": (C.c_int, [vp, C.c_int, vp]),
         "cb2_stage_update": (C.c_int, [vp, C.c_int, C.c_double, C.c_int, vp]),
         "cb2_boundary": (C.c_int, [vp, C.c_int, vp]),
+        "cb2_vt_relaxation": (C.c_int, [vp, C.c_int, C.c_double, vp]),
         "cb2_properties": (C.c_int, [vp, C.c_int, vp]),
         "cb2_cv_from_bv": (C.c_int, [vp, C.c_int, vp]),
         "cb2_cfl_dt": (C.c_int, [vp, P(C.c_double), vp]),
@@ -96,6 +97,9 @@ class Context:
 
     def stage_update(self, blk, dt, rk, stream=None):
         check(self.lib.cb2_stage_update(self.h, blk, dt, rk, stream), "cb2_stage_update")
+
+    def vt_relaxation(self, blk, dt_stage, stream=None):
+        check(self.lib.cb2_vt_relaxation(self.h, blk, dt_stage, stream), "cb2_vt_relaxation")
 
     def boundary(self, blk, stream=None):
         check(self.lib.cb2_boundary(self.h, blk, stream), "cb2_boundary")

@@ -62,3 +62,33 @@ def stoich_h2_air(mech):
     for n, v in x.items():
         y[mech.index(n)] = v * w[mech.index(n)] / tot
     return y
+
+
+class TwoTemperatureStruct:
+    """cb2_two_temperature from the JSON the reference's two-temperature parser writes
+    (tests/golden/h2_two_temperature.json); keeps the arrays alive like MechStruct."""
+
+    def __init__(self, d, enable_vt_relaxation=True):
+        self.d = d
+        ns = int(d["n_spec"])
+        s = abi.TwoTemperature()
+        s.n_spec = ns
+        s.max_level = int(d["max_level"])
+        s.enable_vt_relaxation = 1 if enable_vt_relaxation else 0
+        self.arrays = {}
+        for name in ("theta_v", "elec_theta", "elec_g", "lt_a", "lt_b", "park_sigma"):
+            a = np.ascontiguousarray(np.asarray(d[name], dtype=np.float64))
+            self.arrays[name] = a
+            setattr(s, name, a.ctypes.data_as(C.POINTER(C.c_double)))
+        a = np.ascontiguousarray(np.asarray(d["n_level"], dtype=np.int32))
+        self.arrays["n_level"] = a
+        s.n_level = a.ctypes.data_as(C.POINTER(C.c_int))
+        self.struct = s
+
+    def ptr(self):
+        return C.pointer(self.struct)
+
+
+def load_two_temperature_json(path, enable_vt_relaxation=True):
+    with open(path) as f:
+        return TwoTemperatureStruct(json.load(f), enable_vt_relaxation)

@@ -129,7 +129,7 @@ int fail_cuda(cudaError_t e) {
 }
 
 // Copies the mechanism into one device allocation and fills the device pointers of Mech.
-int upload_mechanism(const cb2_mechanism &m, cb2_ctx *ctx) {
+int upload_mechanism(const cb2_mechanism &m, const cb2_two_temperature *tt, cb2_ctx *ctx) {
   const int ns = m.n_spec, nr = m.n_reac;
   std::vector<double> buf;
   std::vector<int> ibuf;
@@ -185,6 +185,16 @@ int upload_mechanism(const cb2_mechanism &m, cb2_ctx *ctx) {
   addi(&d.stoi_f, m.stoi_f, (size_t)nr * ns);
   addi(&d.stoi_b, m.stoi_b, (size_t)nr * ns);
   addi(&d.reac_order, m.reac_order, nr);
+  if (tt) {
+    const size_t ml = (size_t)tt->max_level;
+    addd(&d.theta_v, tt->theta_v, ns);
+    addd(&d.elec_theta, tt->elec_theta, ns * ml);
+    addd(&d.elec_g, tt->elec_g, ns * ml);
+    addd(&d.lt_a, tt->lt_a, (size_t)ns * ns);
+    addd(&d.lt_b, tt->lt_b, (size_t)ns * ns);
+    addd(&d.park_sigma, tt->park_sigma, ns);
+    addi(&d.n_level, tt->n_level, ns);
+  }
   const size_t bd = buf.size() * sizeof(double), bi = ibuf.size() * sizeof(int);
   char *dev = nullptr;
   cudaError_t e = cudaMalloc(&dev, bd + bi + 16);
@@ -196,6 +206,8 @@ int upload_mechanism(const cb2_mechanism &m, cb2_ctx *ctx) {
   for (auto &s : is) *s.dst = reinterpret_cast<const int *>(dev + bd) + s.off;
   d.n_spec = ns;
   d.n_reac = nr;
+  d.max_level = tt ? tt->max_level : 0;
+  d.enable_vt = tt && tt->enable_vt_relaxation ? 1 : 0;
   return CB2_OK;
 }
 
@@ -230,6 +242,7 @@ Zone make_zone(const cb2_zone_view &v) {
   z.mul = v.mul; z.kappa = v.thermal_conductivity; z.rhoD = v.rho_D; z.acoustic = v.acoustic_speed;
   z.gamma = v.gamma; z.mach = v.mach; z.fF = v.fFlux; z.gF = v.gFlux; z.hF = v.hFlux; z.visf = v.vis_flux;
   z.shock = v.shock_sensor; z.dtl = v.dt_local; z.rts = v.reaction_timeScale; z.efd = v.entropy_fix_delta;
+  z.tve = v.temperature_ve;
   return z;
 }
 
@@ -237,6 +250,10 @@ Block *get_block(cb2_ctx *ctx, int blk) {
   if (!ctx || blk < 0 || blk >= (int)ctx->blocks.size() || !ctx->blocks[blk].bound) return nullptr;
   return &ctx->blocks[blk];
 }
+
+// The two-temperature model is built for the pointwise stage operations (stage update with
+// the VT relaxation, cv from bv); its flux terms are not, so the other entry points refuse it.
+bool two_temperature(const cb2_ctx *ctx) { return ctx && ctx->p.i_eve >= 0; }
 
 int count(cb2_ctx *ctx, int n) {
   ctx->n_launch += (unsigned long long)n;
@@ -271,7 +288,20 @@ int cb2_init(const cb2_param_view *pv, cb2_ctx **out) {
   const int ns = pv->mech ? pv->mech->n_spec : 0;
   if (pv->n_spec != ns) return CB2_ERR_INVALID;
   if (ns != 0 && ns != 5 && ns != 9) return CB2_ERR_UNSUPPORTED;
-  if (pv->n_var != 5 + ns || pv->n_scalar != ns) return CB2_ERR_UNSUPPORTED;
+  // two-temperature: e_ve is the scalar after the species (i_eve = n_spec)
+  const cb2_two_temperature *tt = pv->two_t;
+  if (tt) {
+    if (ns == 0 || tt->n_spec != ns || tt->max_level < 1 || !tt->theta_v || !tt->n_level || !tt->elec_theta ||
+        !tt->elec_g || !tt->lt_a || !tt->lt_b || !tt->park_sigma)
+      return CB2_ERR_INVALID;
+    for (int s = 0; s < ns; ++s)
+      if (tt->n_level[s] < 0 || tt->n_level[s] > tt->max_level) return CB2_ERR_INVALID;
+    if (pv->n_var != 6 + ns || pv->n_scalar != ns + 1 || pv->n_scalar_transported != ns + 1)
+      return CB2_ERR_INVALID;
+    if (pv->precision != CB2_PREC_FP64) return CB2_ERR_UNSUPPORTED;
+  } else if (pv->n_var != 5 + ns || pv->n_scalar != ns) {
+    return CB2_ERR_UNSUPPORTED;
+  }
   const int sch = pv->inviscid_scheme;
   const bool weno_ch = sch == CB2_INV_WENO5_CH || sch == CB2_INV_WENO7_CH || sch == CB2_INV_WENO5_CP ||
                        sch == CB2_INV_WENO7_CP;
@@ -336,7 +366,8 @@ int cb2_init(const cb2_param_view *pv, cb2_ctx **out) {
     p.lf_ul[4] = 1e+3 * pv->p_ref;
   }
   int rc = CB2_OK;
-  if (pv->mech) rc = upload_mechanism(*pv->mech, ctx);
+  p.i_eve = tt ? ns : -1;
+  if (pv->mech) rc = upload_mechanism(*pv->mech, tt, ctx);
   if (rc == CB2_OK) {
     cudaError_t e = cudaMalloc(&ctx->d_status, sizeof(unsigned) + 2 * sizeof(double));
     if (e != cudaSuccess) rc = fail_cuda(e);
@@ -425,6 +456,7 @@ int cb2_bind_block(cb2_ctx *ctx, int blk, const cb2_zone_view *v, const cb2_face
   if (p.n_spec > 0 && (!v->sv || !v->acoustic_speed || !v->gamma || !v->mul || !v->thermal_conductivity ||
                        !v->rho_D))
     return CB2_ERR_INVALID;
+  if (p.i_eve >= 0 && (!v->sv || !v->temperature_ve)) return CB2_ERR_INVALID;
   if (p.viscous_order > 0 && !v->mul) return CB2_ERR_INVALID;
   if (p.viscous_order == 8 && (!v->fFlux || !v->gFlux || !v->hFlux)) return CB2_ERR_INVALID;
   if (p.inviscid_scheme == CB2_INV_ROE && !v->entropy_fix_delta) return CB2_ERR_INVALID;
@@ -511,6 +543,7 @@ int cb2_store_qn(cb2_ctx *ctx, int blk, void *stream) {
 int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream) {
   Block *B = get_block(ctx, blk);
   if (!B) return CB2_ERR_INVALID;
+  if (two_temperature(ctx)) return CB2_ERR_UNSUPPORTED;
   ProfGuard pg(ctx);
   cudaStream_t s = (cudaStream_t)stream;
   const Param &p = ctx->p;
@@ -537,6 +570,7 @@ int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream) {
 int cb2_shock_sensor(cb2_ctx *ctx, int blk, void *stream) {
   Block *B = get_block(ctx, blk);
   if (!B || !B->z.shock) return CB2_ERR_INVALID;
+  if (two_temperature(ctx)) return CB2_ERR_UNSUPPORTED;
   ProfGuard pg(ctx);
   int nl = 0;
   CB2_TRY(launch_shock_sensor(B->z, ctx->p, (cudaStream_t)stream, nl));
@@ -552,9 +586,20 @@ int cb2_stage_update(cb2_ctx *ctx, int blk, double dt, int rk, void *stream) {
   return count(ctx, nl);
 }
 
+int cb2_vt_relaxation(cb2_ctx *ctx, int blk, double dt_stage, void *stream) {
+  Block *B = get_block(ctx, blk);
+  if (!B || !(dt_stage >= 0.0)) return CB2_ERR_INVALID;
+  if (!two_temperature(ctx)) return CB2_ERR_UNSUPPORTED;
+  ProfGuard pg(ctx);
+  int nl = 0;
+  CB2_TRY(launch_vt_relaxation(B->z, ctx->p, dt_stage, (cudaStream_t)stream, nl));
+  return count(ctx, nl);
+}
+
 int cb2_boundary(cb2_ctx *ctx, int blk, void *stream) {
   Block *B = get_block(ctx, blk);
   if (!B) return CB2_ERR_INVALID;
+  if (two_temperature(ctx)) return CB2_ERR_UNSUPPORTED;
   ProfGuard pg(ctx);
   int nl = 0;
   cudaStream_t s = (cudaStream_t)stream;
@@ -566,6 +611,7 @@ int cb2_boundary(cb2_ctx *ctx, int blk, void *stream) {
 int cb2_properties(cb2_ctx *ctx, int blk, void *stream) {
   Block *B = get_block(ctx, blk);
   if (!B) return CB2_ERR_INVALID;
+  if (two_temperature(ctx)) return CB2_ERR_UNSUPPORTED;
   ProfGuard pg(ctx);
   int nl = 0;
   CB2_TRY(launch_properties(B->z, ctx->p, (cudaStream_t)stream, nl));
@@ -583,6 +629,7 @@ int cb2_cv_from_bv(cb2_ctx *ctx, int blk, void *stream) {
 
 // Enqueues the CFL dt of every bound block and their minimum into ctx->d_dtmin.
 static int enqueue_cfl_dt(cb2_ctx *ctx, cudaStream_t s) {
+  if (two_temperature(ctx)) return CB2_ERR_UNSUPPORTED;
   int nl = 0;
   CB2_TRY(launch_set_value(ctx->d_dtmin, 1e+6, s, nl));
   for (auto &B : ctx->blocks) {
@@ -708,6 +755,7 @@ extern "C" {
 
 int cb2_rk3_step(cb2_ctx *ctx, double *dt_inout, int fixed_dt, void *stream) {
   if (!ctx || !dt_inout) return CB2_ERR_INVALID;
+  if (two_temperature(ctx)) return CB2_ERR_UNSUPPORTED;
   ProfGuard pg(ctx);
   CB2_TRY(enqueue_step_head(ctx, stream));
   double dt = *dt_inout;
@@ -722,6 +770,7 @@ int cb2_rk3_step(cb2_ctx *ctx, double *dt_inout, int fixed_dt, void *stream) {
 int cb2_rk3_run(cb2_ctx *ctx, double dt, int fixed_dt, long long max_steps, double t_end, double *time_inout,
                 long long *steps_out, double *dt_last_out, void *stream) {
   if (!ctx || !time_inout || !steps_out || max_steps < 0 || std::isnan(t_end)) return CB2_ERR_INVALID;
+  if (two_temperature(ctx)) return CB2_ERR_UNSUPPORTED;
   if (fixed_dt && !(dt > 0.0 && dt < 1e300)) return CB2_ERR_INVALID;
   *steps_out = 0;
   if (max_steps == 0 || !(*time_inout < t_end)) return CB2_OK;
@@ -754,6 +803,7 @@ int cb2_rk3_run(cb2_ctx *ctx, double dt, int fixed_dt, long long max_steps, doub
 int cb2_reactor_setup(cb2_ctx *ctx, cb2_reactor *reactors, int n, const double *T0, const double *p0,
                       const double *Y, const double *t_end, double h0, void *stream) {
   if (!ctx || !reactors || n < 0 || !T0 || !p0 || !Y || !t_end || !(h0 > 0)) return CB2_ERR_INVALID;
+  if (two_temperature(ctx)) return CB2_ERR_UNSUPPORTED;
   if (ctx->p.n_spec == 0) return CB2_ERR_UNSUPPORTED;
   if (n == 0) return CB2_OK;
   ProfGuard pg(ctx);
@@ -764,6 +814,7 @@ int cb2_reactor_setup(cb2_ctx *ctx, cb2_reactor *reactors, int n, const double *
 int cb2_reactor_advance(cb2_ctx *ctx, cb2_reactor *reactors, int n, int max_attempts, double rtol, double atol,
                         void *stream) {
   if (!ctx || !reactors || n < 0 || max_attempts < 1 || !(rtol > 0) || !(atol > 0)) return CB2_ERR_INVALID;
+  if (two_temperature(ctx)) return CB2_ERR_UNSUPPORTED;
   if (ctx->p.n_spec == 0) return CB2_ERR_UNSUPPORTED;
   if (n == 0) return CB2_OK;
   ProfGuard pg(ctx);

@@ -163,7 +163,7 @@ int launch_line_batch(LineCase *cases, int n, const Param &p, int max_steps, cud
 }
 
 bool line_batch_supported(const Param &p) {
-  return p.viscous_order == 0 && p.precision == CB2_PREC_FP64 && p.n_spec == 9 &&
+  return p.viscous_order == 0 && p.precision == CB2_PREC_FP64 && p.n_spec == 9 && p.i_eve < 0 &&
          p.reconstruction == CB2_REC_WENO5 && (p.inviscid_scheme == CB2_INV_HLLC || p.inviscid_scheme == CB2_INV_AUSMP);
 }
 

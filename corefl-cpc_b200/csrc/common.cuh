@@ -69,6 +69,7 @@ struct Zone {
   Layout L1;  // ghost 1 (vis_flux, entropy_fix_delta)
   double *cv, *bv, *sv, *qn, *dq, *metric, *jac, *mul, *kappa, *rhoD, *acoustic, *gamma, *mach;
   double *fF, *gF, *hF, *visf, *shock, *dtl, *rts, *efd;
+  double *tve;  // two-temperature: T_ve, ghost ngg
   BTypes bt;
 };
 
@@ -83,11 +84,16 @@ struct Mech {
   const double *zrot;
   const int *reac_type, *rev_type, *stoi_f, *stoi_b, *reac_order;
   const double *A, *b, *Ea, *A2, *b2, *Ea2, *tbc, *troe_alpha, *troe_t3, *troe_t1, *troe_t2;
+  // two-temperature data (null / 0 for one temperature)
+  int max_level, enable_vt;
+  const double *theta_v, *elec_theta, *elec_g, *lt_a, *lt_b, *park_sigma;
+  const int *n_level;
 };
 
 // Scalar settings passed by value to kernels.
 struct Param {
   int dim, n_var, n_spec, n_scalar, n_scalar_transported, n_reac;
+  int i_eve;  // two-temperature: e_ve's index in sv (= n_spec); -1 for one temperature
   int inviscid_scheme, reconstruction, limiter, viscous_order, positive_preserving;
   int gradP, reaction, shock_sensor;
   double sensor_eps, sensor_threshold, entropy_fix_factor, Pr, cfl;
@@ -110,7 +116,7 @@ __device__ __forceinline__ void flag_status(const Param &p, unsigned bits) {
 __device__ __forceinline__ double step_dt(const Param &p, double dt) { return p.dt_dev ? *p.dt_dev : dt; }
 
 // SSP-RK3 Shu-Osher coefficients (src/RK.cuh:12-16).
-__device__ __forceinline__ void ssprk3_coeff(int rk, double &a, double &b, double &c) {
+__host__ __device__ __forceinline__ void ssprk3_coeff(int rk, double &a, double &b, double &c) {
   if (rk == 0) { a = 1.0; b = 0.0; c = 1.0; }
   else if (rk == 1) { a = 0.75; b = 0.25; c = 0.25; }
   else { a = 1.0 / 3.0; b = 2.0 / 3.0; c = 2.0 / 3.0; }

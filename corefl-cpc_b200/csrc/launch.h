@@ -72,6 +72,9 @@ int launch_inviscid_pv(const Zone &z, const Param &p, cudaStream_t s, int &n_lau
 int launch_inviscid_pv_f32(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
 int launch_stage_update(const Zone &z, const Param &p, double dt, int rk, cudaStream_t s, int &n_launch);
 int launch_cv_from_bv(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
+// two-temperature VT relaxation over dt_stage of every interior node (a standalone
+// apply_vt_relaxation_rk; launch_stage_update runs it itself for two-temperature contexts)
+int launch_vt_relaxation(const Zone &z, const Param &p, double dt_stage, cudaStream_t s, int &n_launch);
 int launch_properties(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
 int launch_boundary(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, cudaStream_t s,
                     int &n_launch);

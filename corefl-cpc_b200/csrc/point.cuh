@@ -5,6 +5,7 @@
 #pragma once
 #include "common.cuh"
 #include "thermo.cuh"
+#include "thermo_2t.cuh"
 #include "transport.cuh"
 
 namespace cb2 {
@@ -35,10 +36,13 @@ __device__ __forceinline__ double newton_temperature(double e, const double *y, 
 }
 
 // SSP-RK3 stage update of one interior node (update_cv_and_bv_rk<mix>, src/RK.cuh:277-367).
-template <int NS>
+// TT: two-temperature model, rho*e_ve at cv comp 5 + NS (clipped at zero), e_ve at sv comp NS,
+// T_ve and T from the two-temperature inversion.
+template <int NS, bool TT = false>
 __device__ __forceinline__ void stage_update_point(const Zone &z, const Param &p, double dt, int rk, int i, int j,
                                                    int k) {
-  constexpr int NV = 5 + NS;
+  static_assert(!TT || NS > 0, "the two-temperature model needs species");
+  constexpr int NV = 5 + NS + (TT ? 1 : 0);
   double a, b, c;
   ssprk3_coeff(rk, a, b, c);
   const idx_t g = z.L.at(i, j, k), sz = z.L.sz;
@@ -70,6 +74,7 @@ __device__ __forceinline__ void stage_update_point(const Zone &z, const Param &p
       if (q[5 + s] < 0) q[5 + s] = 0;
       else sum += q[5 + s];
     }
+    if constexpr (TT) q[5 + NS] = fmax(q[5 + NS], 0.0);
     sum = 1.0 / sum;
     const double scale = rho * sum;
     double y[NS], r_mix = 0;
@@ -78,6 +83,13 @@ __device__ __forceinline__ void stage_update_point(const Zone &z, const Param &p
       y[s] = q[5 + s] * sum;
       q[5 + s] *= scale;
       z.sv[g + s * sz] = y[s];
+    }
+    if constexpr (TT) {
+      z.sv[g + NS * sz] = q[5 + NS] * dinv;
+#pragma unroll
+      for (int l = 0; l < NV; ++l) z.cv[g + l * sz] = q[l];
+      temperature_2t<NS>(z, p, g, q[4]);
+      return;
     }
 #pragma unroll
     for (int s = 0; s < NS; ++s) r_mix += y[s] * __ldg(p.mech.gas_const + s);
@@ -195,6 +207,12 @@ __device__ __forceinline__ void cv_point(const Zone &z, const Param &p, idx_t g)
   if constexpr (NS == 0) {
     E *= rho;
     E += z.bv[g + 4 * sz] / (kGammaAir - 1);
+  } else if (p.i_eve >= 0) {
+    // two-temperature (src/FieldOperation.cuh:154-158, 97-109)
+    sync_two_temperature<NS>(z, p, g);
+#pragma unroll
+    for (int s = 0; s <= NS; ++s) z.cv[g + (5 + s) * sz] = rho * z.sv[g + s * sz];
+    E = total_energy_2t<NS>(z, p, g);
   } else {
     double h[NS];
     nasa7_h<NS>(z.bv[g + 5 * sz], p.mech, h);

@@ -160,7 +160,7 @@ extern "C" int cb2_serve_run(cb2_ctx *ctx_reactor, cb2_ctx *ctx_tube, const cb2_
   if ((need_r && !ctx_reactor) || (need_t && (!ctx_tube || !opt->tube_Y))) return CB2_ERR_INVALID;
   const Param *pr = need_r ? ctx_param(ctx_reactor) : nullptr;
   const Param *pt = need_t ? ctx_param(ctx_tube) : nullptr;
-  if (pr && pr->n_spec == 0) return CB2_ERR_UNSUPPORTED;
+  if (pr && (pr->n_spec == 0 || pr->i_eve >= 0)) return CB2_ERR_UNSUPPORTED;
   if (pt && !line_batch_supported(*pt)) return CB2_ERR_UNSUPPORTED;
   const int nsr = pr ? pr->n_spec : 0, nst = pt ? pt->n_spec : 0;
   const int g = 3;  // ghost nodes of a WENO5 line

@@ -10,12 +10,22 @@ namespace cb2 {
 
 constexpr int kPtThreads = 128;
 
-template <int NS>
+template <int NS, bool TT>
 __global__ void __launch_bounds__(kPtThreads) k_stage_update(Zone z, Param p, double dt, int rk) {
   const int i = blockIdx.x * kPtThreads + threadIdx.x;
   const int j = blockIdx.y, k = blockIdx.z;
   if (i >= z.mx) return;
-  stage_update_point<NS>(z, p, step_dt(p, dt), rk, i, j, k);
+  stage_update_point<NS, TT>(z, p, step_dt(p, dt), rk, i, j, k);
+}
+
+// VT relaxation of every interior node over dt_scale x the step's dt (apply_vt_relaxation_rk,
+// src/RK.cuh:20-28; dt_stage = rk_stage_dt_scale[rk] * dt, :91, 202).
+template <int NS>
+__global__ void __launch_bounds__(kPtThreads) k_vt_relaxation(Zone z, Param p, double dt, double dt_scale) {
+  const int i = blockIdx.x * kPtThreads + threadIdx.x;
+  const int j = blockIdx.y, k = blockIdx.z;
+  if (i >= z.mx) return;
+  vt_relax_point<NS>(z, p, z.L.at(i, j, k), dt_scale * step_dt(p, dt));
 }
 
 template <int NS>
@@ -127,13 +137,37 @@ __global__ void __launch_bounds__(kPtThreads) k_limit_flow_apply(Zone z, Param p
 }
 
 template <int NS>
+static int launch_vt_ns(const Zone &z, const Param &p, double dt, double dt_scale, cudaStream_t s, int &nl) {
+  if (!p.mech.enable_vt) return CB2_OK;
+  dim3 grid((z.mx + kPtThreads - 1) / kPtThreads, z.my, z.mz);
+  ProfScope prof("vt_relaxation", s);
+  k_vt_relaxation<NS><<<grid, kPtThreads, 0, s>>>(z, p, dt, dt_scale);
+  ++nl;
+  return check_launch();
+}
+
+template <int NS>
 static int launch_update_ns(const Zone &z, const Param &p, double dt, int rk, cudaStream_t s, int &nl) {
   dim3 grid((z.mx + kPtThreads - 1) / kPtThreads, z.my, z.mz);
+  const bool tt = p.i_eve >= 0;
   {
     ProfScope prof("stage_update", s);
-    k_stage_update<NS><<<grid, kPtThreads, 0, s>>>(z, p, dt, rk);
+    if constexpr (NS > 0) {
+      if (tt) k_stage_update<NS, true><<<grid, kPtThreads, 0, s>>>(z, p, dt, rk);
+      else k_stage_update<NS, false><<<grid, kPtThreads, 0, s>>>(z, p, dt, rk);
+    } else {
+      k_stage_update<NS, false><<<grid, kPtThreads, 0, s>>>(z, p, dt, rk);
+    }
   }
   CB2_TRY(check_launch());
+  if constexpr (NS > 0) {
+    // the stage's VT relaxation follows its update and precedes limit_flow (src/RK.cuh:198-207)
+    if (tt) {
+      double a, b, c;
+      ssprk3_coeff(rk, a, b, c);
+      CB2_TRY(launch_vt_ns<NS>(z, p, dt, c, s, nl));
+    }
+  }
   if (p.limit_flow) {
     ProfScope prof("limit_flow", s);
     k_limit_flow_mean<<<grid, kPtThreads, 0, s>>>(z, p);
@@ -150,6 +184,15 @@ int launch_stage_update(const Zone &z, const Param &p, double dt, int rk, cudaSt
     case 0: return launch_update_ns<0>(z, p, dt, rk, s, n_launch);
     case 5: return launch_update_ns<5>(z, p, dt, rk, s, n_launch);
     case 9: return launch_update_ns<9>(z, p, dt, rk, s, n_launch);
+    default: return CB2_ERR_UNSUPPORTED;
+  }
+}
+
+int launch_vt_relaxation(const Zone &z, const Param &p, double dt_stage, cudaStream_t s, int &n_launch) {
+  if (p.i_eve < 0) return CB2_ERR_UNSUPPORTED;
+  switch (p.n_spec) {
+    case 5: return launch_vt_ns<5>(z, p, dt_stage, 1.0, s, n_launch);
+    case 9: return launch_vt_ns<9>(z, p, dt_stage, 1.0, s, n_launch);
     default: return CB2_ERR_UNSUPPORTED;
   }
 }

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define CB2_ABI_VERSION 2
+#define CB2_ABI_VERSION 3
 
 /* ---- status codes ---------------------------------------------------------------- */
 #define CB2_OK 0
@@ -96,6 +96,7 @@ typedef struct cb2_zone_view {
   double *dt_local;             /* ghost 0                                  */
   double *reaction_timeScale;   /* ghost ngg, reacting cases                */
   double *entropy_fix_delta;    /* ghost 1, Roe                             */
+  double *temperature_ve;       /* ghost ngg, two-temperature cases (DZone::temperature_ve) */
 } cb2_zone_view;
 
 /* One face boundary condition of a block (cfd::Boundary, src/Mesh.h:8-30, after
@@ -140,6 +141,21 @@ typedef struct cb2_mechanism {
   const double *troe_alpha, *troe_t3, *troe_t1, *troe_t2; /* [n_reac] */
 } cb2_mechanism;
 
+/* Vibrational-electronic data of the species for the two-temperature model, as
+ * cfd::Species::read_two_temperature parses two_temperature.dat (src/ChemData.cpp:130-233).
+ * Host arrays, row-major, in the mechanism's species order. */
+typedef struct cb2_two_temperature {
+  int n_spec;                /* must equal the mechanism's n_spec                       */
+  int max_level;             /* row length of elec_theta / elec_g (>= 1)                */
+  const double *theta_v;     /* [n_spec] characteristic vibrational temperature, K; <= 0: none */
+  const int *n_level;        /* [n_spec] electronic levels of each species              */
+  const double *elec_theta;  /* [n_spec*max_level] electronic level temperatures, K     */
+  const double *elec_g;      /* [n_spec*max_level] degeneracies                         */
+  const double *lt_a, *lt_b; /* [n_spec*n_spec] Millikan-White A_ij, B_ij; <= 0: default */
+  const double *park_sigma;  /* [n_spec] Park limiting cross-section, m^2               */
+  int enable_vt_relaxation;  /* DParameter::enable_vt_relaxation                        */
+} cb2_two_temperature;
+
 /* Scalar settings (the scalar fields of `DParameter`, src/DParameter.cuh:13-160, with the
  * setup.txt meaning given in src/Parameter.cpp:358-546). */
 typedef struct cb2_param_view {
@@ -172,6 +188,11 @@ typedef struct cb2_param_view {
   /* time step the positivity limiter starts with (DParameter::dt, the setup's fixed step);
    * cb2_cfl_dt and cb2_rk3_step replace it with the step they take */
   double dt;
+  /* two-temperature model (the reference's COREFL_ENABLE_TWO_TEMPERATURE build): NULL for one
+   * temperature.  With it the last scalar is the vibrational-electronic energy e_ve
+   * (i_eve = n_spec, src/Parameter.cpp:647-656): n_scalar = n_scalar_transported = n_spec + 1,
+   * n_var = 6 + n_spec, cv holds rho*e_ve at 5 + n_spec, and zones carry temperature_ve. */
+  const cb2_two_temperature *two_t;
 } cb2_param_view;
 
 typedef struct cb2_ctx cb2_ctx;
@@ -207,8 +228,22 @@ int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream);
 int cb2_shock_sensor(cb2_ctx *ctx, int blk, void *stream);
 
 /* Shu-Osher stage `rk` (0,1,2) with time step dt, species clipping and primitive recovery:
- * replaces update_cv_and_bv_rk<mix> (src/RK.cuh:277-367). */
+ * replaces update_cv_and_bv_rk<mix> (src/RK.cuh:277-367), followed by limit_flow when set.
+ * Two-temperature contexts recover T_ve and T with the two-temperature inversion
+ * (src/FieldOperation.cu:24-63) and relax e_ve over {1, 1/4, 2/3}[rk] x dt before limit_flow,
+ * as RK3 does (apply_vt_relaxation_rk, src/RK.cuh:199-203). */
 int cb2_stage_update(cb2_ctx *ctx, int blk, double dt, int rk, void *stream);
+
+/* Two-temperature VT relaxation of every interior node over dt_stage alone: replaces
+ * apply_vt_relaxation_rk (src/RK.cuh:20-28, apply_vt_relaxation_1_point,
+ * src/FieldOperation.cuh:60-88), for callers that run their own stage update.  e_v relaxes
+ * towards equilibrium at T with the Millikan-White + Park time, then T_ve and T follow.
+ * CB2_ERR_UNSUPPORTED for one-temperature contexts.
+ *
+ * Two-temperature contexts (cb2_param_view::two_t) are built for the pointwise stage
+ * operations: cb2_stage_update, cb2_vt_relaxation and cb2_cv_from_bv.  The flux, boundary,
+ * property, time-step, whole-step and batched entry points return CB2_ERR_UNSUPPORTED for them. */
+int cb2_vt_relaxation(cb2_ctx *ctx, int blk, double dt_stage, void *stream);
 
 /* Ghost fill of bv/sv/cv from the face conditions bound with the block (periodic,
  * outflow, ...): replaces DBoundCond::apply_boundary_conditions (src/BoundCond.cu:3846). */
@@ -219,7 +254,8 @@ int cb2_boundary(cb2_ctx *ctx, int blk, void *stream);
 int cb2_properties(cb2_ctx *ctx, int blk, void *stream);
 
 /* cv from bv/sv over interior and ghosts: replaces compute_cv_from_bv<mix>
- * (src/FieldOperation.cuh:136-161). */
+ * (src/FieldOperation.cuh:136-161); two-temperature contexts first bring e_ve and T_ve into
+ * agreement (sync_two_temperature_state_from_sv, :28-58). */
 int cb2_cv_from_bv(cb2_ctx *ctx, int blk, void *stream);
 
 /* Local CFL time step of every node and the min over all bound blocks, returned to the

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "liboracle.so")
-SRCS = [os.path.join(HERE, f) for f in ("oracle.cpp", "reactor.cpp", "oracle_capi.cpp")]
+SRCS = [os.path.join(HERE, f) for f in ("oracle.cpp", "reactor.cpp", "two_temp.cpp", "oracle_capi.cpp")]
 HDRS = [os.path.join(HERE, "oracle.hpp"), os.path.join(REPO, "include", "cb200.h"),
         os.path.join(REPO, "include", "cb200_serve.h")]
 

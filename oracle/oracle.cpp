@@ -1296,7 +1296,12 @@ void cv_point(Zone &z, const Param &p, int i, int j, int k) {
   z.cv(i, j, k, 1) = rho * z.bv(i, j, k, 1);
   z.cv(i, j, k, 2) = rho * z.bv(i, j, k, 2);
   z.cv(i, j, k, 3) = rho * z.bv(i, j, k, 3);
+  if (p.i_eve >= 0) sync_two_temperature(z, p, i, j, k);
   for (int l = 0; l < p.n_scalar; ++l) z.cv(i, j, k, 5 + l) = rho * z.sv(i, j, k, l);
+  if (p.i_eve >= 0) {
+    z.cv(i, j, k, 4) = total_energy_2t(z, p, i, j, k);
+    return;
+  }
   const double V2 = z.bv(i, j, k, 1) * z.bv(i, j, k, 1) + z.bv(i, j, k, 2) * z.bv(i, j, k, 2) +
                     z.bv(i, j, k, 3) * z.bv(i, j, k, 3);
   double E = 0.5 * V2;
@@ -1425,6 +1430,24 @@ Param make_param(const cb2_param_view &pv) {
     o.troe_t1 = cp(m.troe_t1, nr);
     o.troe_t2 = cp(m.troe_t2, nr);
   }
+  if (pv.two_t && pv.mech) {
+    // DParameter two-temperature tables (src/DParameter.cu:150-200); i_eve = n_spec
+    // (src/Parameter.cpp:647-656)
+    const cb2_two_temperature &t = *pv.two_t;
+    const int ns = t.n_spec, ml = t.max_level;
+    TwoTemperature &o = p.tt;
+    o.on = true;
+    o.enable_vt = t.enable_vt_relaxation != 0;
+    o.max_level = ml;
+    o.theta_v.assign(t.theta_v, t.theta_v + ns);
+    o.n_level.assign(t.n_level, t.n_level + ns);
+    o.elec_theta.assign(t.elec_theta, t.elec_theta + ns * ml);
+    o.elec_g.assign(t.elec_g, t.elec_g + ns * ml);
+    o.lt_a.assign(t.lt_a, t.lt_a + ns * ns);
+    o.lt_b.assign(t.lt_b, t.lt_b + ns * ns);
+    o.park_sigma.assign(t.park_sigma, t.park_sigma + ns);
+    p.i_eve = p.n_spec;
+  }
   return p;
 }
 
@@ -1439,6 +1462,7 @@ Zone make_zone(const cb2_zone_view &v, const cb2_face_bc *faces, int n_faces, co
   z.fF = A(v.fFlux, g); z.gF = A(v.gFlux, g); z.hF = A(v.hFlux, g); z.visf = A(v.vis_flux, 1);
   z.shock = A(v.shock_sensor, g); z.dtl = A(v.dt_local, 0); z.rts = A(v.reaction_timeScale, g);
   z.efd = A(v.entropy_fix_delta, 1);
+  z.tve = A(v.temperature_ve, g);
   const int mx = v.mx, my = v.my, mz = v.mz;
   z.il.assign(my * mz, 0); z.ir.assign(my * mz, 0); z.jl.assign(mx * mz, 0); z.jr.assign(mx * mz, 0);
   z.kl.assign(mx * my, 0); z.kr.assign(mx * my, 0);
@@ -1566,11 +1590,17 @@ void update_cv_and_bv_rk(Zone &z, const Param &p, double dt, int rk) {
           if (z.cv(i, j, k, 5 + l) < 0) z.cv(i, j, k, 5 + l) = 0;
           else sum += z.cv(i, j, k, l + 5);
         }
+        if (p.i_eve >= 0) z.cv(i, j, k, 5 + p.i_eve) = std::max(z.cv(i, j, k, 5 + p.i_eve), 0.0);
         sum = 1.0 / sum;
         const double scale = z.cv(i, j, k, 0) * sum;
         for (int l = 0; l < p.n_spec; ++l) {
           z.sv(i, j, k, l) = z.cv(i, j, k, 5 + l) * sum;
           z.cv(i, j, k, 5 + l) *= scale;
+        }
+        for (int l = p.n_spec; l < p.n_scalar; ++l) z.sv(i, j, k, l) = z.cv(i, j, k, 5 + l) * dinv;
+        if (p.i_eve >= 0) {
+          temperature_2t(z, p, i, j, k, z.cv(i, j, k, 4));
+          continue;
         }
         // Newton T from e (1T), |1 - T1/T| < 1e-5, at most 1000 iterations
         double gc = 0;
@@ -1595,6 +1625,9 @@ void update_cv_and_bv_rk(Zone &z, const Param &p, double dt, int rk) {
         z.bv(i, j, k, 5) = t;
         z.bv(i, j, k, 4) = rho * t * gc;
       }
+  // two-temperature: VT relaxation over the stage's share of the step, rk_stage_dt_scale
+  // {1, 1/4, 2/3} (src/RK.cuh:91, 199-203)
+  if (p.i_eve >= 0) apply_vt_relaxation(z, p, C[rk] * dt);
   if (p.limit_flow) limit_flow(z, p);
 }
 

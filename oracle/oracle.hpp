@@ -52,8 +52,19 @@ struct Mechanism {
   std::vector<double> A, b, Ea, A2, b2, Ea2, tbc, troe_alpha, troe_t3, troe_t1, troe_t2;
 };
 
+// Vibrational-electronic data of the two-temperature model (cfd::Species::read_two_temperature,
+// src/ChemData.cpp:130-233; DParameter copies, src/DParameter.cu:150-200)
+struct TwoTemperature {
+  bool on = false;
+  bool enable_vt = true;
+  int max_level = 1;
+  std::vector<double> theta_v, elec_theta, elec_g, lt_a, lt_b, park_sigma;
+  std::vector<int> n_level;
+};
+
 struct Param {
   int dim = 3, n_var = 5, n_spec = 0, n_scalar = 0, n_scalar_transported = 0, n_reac = 0;
+  int i_eve = -1;  // index of e_ve in sv (two-temperature), -1 otherwise
   int inviscid_scheme = 52, reconstruction = 2, limiter = 0, viscous_order = 0;
   int positive_preserving = 0, gradP = 0, reaction = 0, shock_sensor = 0;
   double sensor_eps = 0, sensor_threshold = 0, entropy_fix_factor = 0.125, Pr = 0.72, cfl = 0.5;
@@ -62,6 +73,7 @@ struct Param {
   double dt = 0;  // the step's time step (positivity limiter)
   double lf_ll[5] = {0, 0, 0, 0, 0}, lf_ul[5] = {0, 0, 0, 0, 0};
   Mechanism mech;
+  TwoTemperature tt;
 };
 
 struct FaceBC {
@@ -73,7 +85,7 @@ struct FaceBC {
 struct Zone {
   int mx = 0, my = 0, mz = 0, ngg = 0;
   Arr cv, bv, sv, qn, dq, metric, jac, mul, kappa, rhoD, acoustic, gamma, mach, fF, gF, hF, visf, shock, dtl, rts,
-      efd;
+      efd, tve;
   std::vector<int> il, ir, jl, jr, kl, kr;  // physical-boundary flags per face node
   std::vector<FaceBC> faces;
 };
@@ -99,6 +111,18 @@ void nasa7_h_cp(double t, const Mechanism &m, double *h, double *cp);
 
 // forward/backward rates of progress [mol/(cm^3 s)] of every reaction at t and c [mol/cm^3]
 void reaction_rates(const Mechanism &m, double t, const double *c, double *q1, double *q2);
+
+// two-temperature model (two_temp.cpp)
+double ve_energy(const Param &p, int i, double t);
+double ve_cv(const Param &p, int i, double t);
+double mixture_ve_energy(const Param &p, double t, const double *y, double *cv_ve);
+double invert_tve_from_eve(const Param &p, double eve_target, const double *y, double t_init);
+double vt_relaxation_source(const Param &p, double density, double t, double tve, const double *y, double *eve_eq,
+                            double *tau_eff);
+void temperature_2t(Zone &z, const Param &p, int i, int j, int k, double total_energy);
+void sync_two_temperature(Zone &z, const Param &p, int i, int j, int k);
+double total_energy_2t(Zone &z, const Param &p, int i, int j, int k);
+void apply_vt_relaxation(Zone &z, const Param &p, double dt_stage);
 
 // 0-D constant-volume reactor (reactor.cpp)
 struct ReactorState {

@@ -37,6 +37,34 @@ int oracle_stage_update(const cb2_param_view *pv, const cb2_zone_view *zv, doubl
   return 0;
 }
 
+int oracle_vt_relaxation(const cb2_param_view *pv, const cb2_zone_view *zv, double dt_stage) {
+  Param p = make_param(*pv);
+  Zone z = make_zone(*zv, nullptr, 0, p);
+  apply_vt_relaxation(z, p, dt_stage);
+  return 0;
+}
+
+// Two-temperature functions at one state (for the golden-fixture checks): out[0..3] = mixture
+// e_ve(T), cv_ve(T), e_ve(Tve), cv_ve(Tve); out[4] = T_ve inverted from e_ve(Tve) starting at T;
+// out[5..7] = VT source, e_ve equilibrium, effective relaxation time.
+void oracle_two_temperature_state(const cb2_param_view *pv, double rho, double t, double tve, const double *y,
+                                  double *out) {
+  Param p = make_param(*pv);
+  out[0] = mixture_ve_energy(p, t, y, &out[1]);
+  out[2] = mixture_ve_energy(p, tve, y, &out[3]);
+  out[4] = invert_tve_from_eve(p, out[2], y, t);
+  out[5] = vt_relaxation_source(p, rho, t, tve, y, &out[6], &out[7]);
+}
+
+// Species e_ve and cv_ve at t: e[n_spec], cv[n_spec]
+void oracle_species_ve(const cb2_param_view *pv, double t, double *e, double *cv) {
+  Param p = make_param(*pv);
+  for (int s = 0; s < p.n_spec; ++s) {
+    e[s] = ve_energy(p, s, t);
+    cv[s] = ve_cv(p, s, t);
+  }
+}
+
 int oracle_cv_from_bv(const cb2_param_view *pv, const cb2_zone_view *zv) {
   Param p = make_param(*pv);
   Zone z = make_zone(*zv, nullptr, 0, p);

@@ -7,6 +7,8 @@ import ctypes as C
 import os
 import sys
 
+import numpy as np
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(os.path.dirname(HERE), "corefl-cpc_b200"))
 from cb200 import abi  # noqa: E402
@@ -39,6 +41,10 @@ def load():
             "oracle_rk3_step": (C.c_int, [P(abi.ParamView), P(abi.ZoneView), P(abi.FaceBC), P(C.c_int), C.c_int,
                                           P(C.c_double), C.c_int]),
             "oracle_nasa7_h_cp": (None, [P(abi.Mechanism), C.c_double, P(C.c_double), P(C.c_double)]),
+            "oracle_vt_relaxation": (C.c_int, [P(abi.ParamView), P(abi.ZoneView), C.c_double]),
+            "oracle_two_temperature_state": (None, [P(abi.ParamView), C.c_double, C.c_double, C.c_double,
+                                                    P(C.c_double), P(C.c_double)]),
+            "oracle_species_ve": (None, [P(abi.ParamView), C.c_double, P(C.c_double), P(C.c_double)]),
         }
         for n, (r, a) in sig.items():
             f = getattr(lib, n)
@@ -86,6 +92,29 @@ def shock_sensor(param, block):
 def properties(param, block):
     v = block.view()
     load().oracle_properties(C.byref(param), C.byref(v))
+
+
+def vt_relaxation(param, block, dt_stage):
+    v = block.view()
+    load().oracle_vt_relaxation(C.byref(param), C.byref(v), dt_stage)
+
+
+def two_temperature_state(param, rho, t, tve, y):
+    """(e_ve(T), cv_ve(T), e_ve(Tve), cv_ve(Tve), Tve inverted from e_ve(Tve) starting at T,
+    VT source, e_ve equilibrium, effective relaxation time)"""
+    yy = np.ascontiguousarray(np.asarray(y, dtype=np.float64))
+    out = np.zeros(8)
+    P = C.POINTER(C.c_double)
+    load().oracle_two_temperature_state(C.byref(param), rho, t, tve, yy.ctypes.data_as(P), out.ctypes.data_as(P))
+    return out
+
+
+def species_ve(param, t):
+    ns = param.n_spec
+    e, cv = np.zeros(ns), np.zeros(ns)
+    P = C.POINTER(C.c_double)
+    load().oracle_species_ve(C.byref(param), t, e.ctypes.data_as(P), cv.ctypes.data_as(P))
+    return e, cv
 
 
 def cv_from_bv(param, block):

@@ -23,7 +23,8 @@ def build(ref="/root/reference", force=False):
     os.makedirs(OUT, exist_ok=True)
     exe = os.path.join(OUT, "dump_mech")
     mine = [os.path.join(HERE, "ref", f) for f in ("stubs.cpp", "dump_mech.cpp", "mpi.h")]
-    drivers = [os.path.join(HERE, "ref", f) for f in ("dump_chem.cpp", "dump_reactor.cpp", "chem_stubs.cpp")]
+    drivers = [os.path.join(HERE, "ref", f) for f in ("dump_chem.cpp", "dump_reactor.cpp", "chem_stubs.cpp",
+                                                       "dump_2t.cpp")]
     theirs = [os.path.join(src, f) for f in ("ChemData.cpp", "Parameter.cpp", "Element.cpp",
                                              os.path.join("gxl_lib", "MyString.cpp"))]
     if not force and os.path.exists(exe) and os.path.getmtime(exe) >= max(os.path.getmtime(f) for f in mine + drivers):
@@ -50,6 +51,15 @@ def build(ref="/root/reference", force=False):
     r = subprocess.run(cmd3, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("reference reactor driver build failed:\n" + r.stderr[-4000:])
+    # dump_2t: the parser and host chemistry rebuilt with the reference's two-temperature switch on
+    # (COREFL_ENABLE_TWO_TEMPERATURE, src/Define.h:10-12), so Species reads two_temperature.dat
+    exe4 = os.path.join(OUT, "dump_2t")
+    cmd4 = [c if not c.endswith("dump_chem.cpp") else os.path.join(HERE, "ref", "dump_2t.cpp") for c in cmd2]
+    cmd4.insert(1, "-DCOREFL_ENABLE_TWO_TEMPERATURE=1")
+    cmd4[-1] = exe4
+    r = subprocess.run(cmd4, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("reference two-temperature driver build failed:\n" + r.stderr[-4000:])
     return exe
 
 

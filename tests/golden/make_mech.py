@@ -9,6 +9,12 @@ oracle/ref_build.py) on the reference's example data files and keeps its JSON ou
   h2_chem_states.json : 48 seeded (rho, T, Y) states with the reference's host chemistry
                    source cfd::compute_src, h_k/cp_k from Species::compute_enthalpy_and_cp and
                    the Newton temperature of cfd::update_t (src/ConstVolumeReactor.cpp)
+  h2_two_temperature.json : the vibrational-electronic data of two_temperature.dat
+                   (example/squareCylinder2D_M10_air5_dns/input/chemistry/) as
+                   Species::read_two_temperature parses it for the 9 H2/air species, the
+                   species e_ve / cv_ve of Species::compute_ve_energy / compute_ve_cv on a
+                   temperature ladder, and on 40 seeded (rho, T, Tve, Y) states the mixture
+                   e_ve, Species::invert_tve_from_eve and cfd::compute_vt_relaxation_source
   h2_reactor_runs.json : 0-D reactors run with the reference's host chemistry, Jacobian, LU
                    and Newton through the adaptive ROK4E sequence (RTol 1e-6, ATol 1e-12,
                    first step 1e-8): the reference's example case to 1.2 ms and 8 seeded
@@ -58,6 +64,9 @@ def main(ref):
     print(run(ref, "h2_li2004.json", files, 7))
     print(run(ref, "h2_chem_states.json", files, 7, prog="dump_chem", extra=("48",)))
     print(run(ref, "h2_reactor_runs.json", files, 7, prog="dump_reactor", extra=("9",)))
+    files_2t = dict(files, two_temperature_file="example/squareCylinder2D_M10_air5_dns/input/chemistry/"
+                                                "two_temperature.dat")
+    print(run(ref, "h2_two_temperature.json", files_2t, 7, prog="dump_2t", extra=("40",)))
 
 
 if __name__ == "__main__":

@@ -7,7 +7,7 @@ import re
 import pytest
 
 import cb200
-from cb200 import abi, cases
+from cb200 import abi, cases, mech as mechmod
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -30,8 +30,10 @@ def test_library_exports_every_declared_symbol(cb200_lib):
 
 
 def test_struct_sizes_match_header():
-    # 4 ints + 21 pointers; 3 ints + 6 ints + 7 doubles; versioned param view
-    assert C.sizeof(abi.ZoneView) == 4 * 4 + 21 * 8
+    # 4 ints + 22 pointers; 3 ints + 6 ints + 7 doubles; versioned param view
+    assert C.sizeof(abi.ZoneView) == 4 * 4 + 22 * 8
+    # 2 ints, 7 pointers, 1 int (padded to 8)
+    assert C.sizeof(abi.TwoTemperature) == 2 * 4 + 7 * 8 + 8
     assert C.sizeof(abi.FaceBC) == 4 * 9 + 4 + 7 * 8  # 36 bytes of ints, padded to 8
     assert abi.ParamView.abi_version.offset == 0
 
@@ -79,6 +81,18 @@ def test_init_rejects_bad_arguments(cb200_lib):
     assert cb200_lib.cb2_init(C.byref(p), C.byref(h)) == abi.ERR_UNSUPPORTED
     p = cases.make_param(inviscid_scheme=abi.INV_AUSMP, reconstruction=abi.REC_MUSCL, precision=abi.PREC_MIXED)
     assert cb200_lib.cb2_init(C.byref(p), C.byref(h)) == abi.ERR_UNSUPPORTED
+    # two-temperature: e_ve is one more scalar and conservative variable, FP64 only
+    gold = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    h2 = mechmod.load_json(os.path.join(gold, "h2_li2004.json"))
+    tt = mechmod.load_two_temperature_json(os.path.join(gold, "h2_two_temperature.json"))
+    p = cases.make_param(n_var=5 + h2.ns, n_spec=h2.ns, mech=h2.ptr(), two_t=tt.ptr(), inviscid_scheme=abi.INV_HLLC,
+                         reconstruction=abi.REC_WENO5)
+    assert cb200_lib.cb2_init(C.byref(p), C.byref(h)) == abi.ERR_INVALID
+    p = cases.make_param(n_var=6 + h2.ns, n_spec=h2.ns, mech=h2.ptr(), two_t=tt.ptr(), inviscid_scheme=abi.INV_HLLC,
+                         reconstruction=abi.REC_WENO5, precision=abi.PREC_MIXED)
+    assert cb200_lib.cb2_init(C.byref(p), C.byref(h)) == abi.ERR_UNSUPPORTED
+    p = cases.make_param(n_var=6, n_spec=0, two_t=tt.ptr())  # needs a mechanism
+    assert cb200_lib.cb2_init(C.byref(p), C.byref(h)) == abi.ERR_INVALID
     assert not h.value
 
 
