@@ -214,6 +214,7 @@ def gpu_arm(args, rank, world, local_rank):
     sh = stream.cuda_stream
     ctx.properties(0, sh)
     dt = ctx.cfl_dt(sh)
+    tile_widths = ctx.autotune(0, sh)  # y/z sweep tile widths, timed on this block
     nodes = (args.n + 1) ** 3
 
     for _ in range(args.warmup):
@@ -315,6 +316,7 @@ def gpu_arm(args, rank, world, local_rank):
                                    f"({args.n + 1}^3 nodes, 4 ghost layers), WENO7 reconstruction + AUSM+, "
                                    f"8th-order collocated viscous (mu=1e-4, Pr=0.72), SSP-RK3 fixed dt",
                        "dt": dt, "precision": "plain FP64", "per_gpu_nodes": nodes,
+                       "sweep_tile_widths": tile_widths,
                        "l2": "inputs larger than L2 (about 7 GB of field arrays per GPU)",
                        "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
             "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
@@ -337,6 +339,7 @@ def mixed_form(args, p, dev, faces, host_state, xyz, dt, ctx64, stream, nodes, w
     pm.precision = abi.PREC_MIXED
     ctx32 = cb200.Context(pm)
     ctx32.bind(0, dev.view(), faces)
+    ctx32.autotune(0, sh)
     dev_init = {n: torch.from_numpy(a).to(dev.t[n].device) for n, a in host_state.items()}
     g = (dev.t["bv"].shape[-1] - int(round(xyz.shape[-1]))) // 2
 

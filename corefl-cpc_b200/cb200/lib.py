@@ -42,6 +42,8 @@ def load():
         "cb2_stage_update": (C.c_int, [vp, C.c_int, C.c_double, C.c_int, vp]),
         "cb2_boundary": (C.c_int, [vp, C.c_int, vp]),
         "cb2_vt_relaxation": (C.c_int, [vp, C.c_int, C.c_double, vp]),
+        "cb2_autotune": (C.c_int, [vp, C.c_int, P(C.c_int), vp]),
+        "cb2_set_tile_widths": (C.c_int, [vp, C.c_int, P(C.c_int)]),
         "cb2_properties": (C.c_int, [vp, C.c_int, vp]),
         "cb2_cv_from_bv": (C.c_int, [vp, C.c_int, vp]),
         "cb2_cfl_dt": (C.c_int, [vp, P(C.c_double), vp]),
@@ -97,6 +99,16 @@ class Context:
 
     def stage_update(self, blk, dt, rk, stream=None):
         check(self.lib.cb2_stage_update(self.h, blk, dt, rk, stream), "cb2_stage_update")
+
+    def autotune(self, blk=0, stream=None):
+        """Tile widths of the block's y/z sweeps picked by timing (cb2_autotune)."""
+        out = (C.c_int * 3)()
+        check(self.lib.cb2_autotune(self.h, blk, out, stream), "cb2_autotune")
+        return list(out)
+
+    def set_tile_widths(self, blk, widths):
+        arr = (C.c_int * 3)(*widths)
+        check(self.lib.cb2_set_tile_widths(self.h, blk, arr), "cb2_set_tile_widths")
 
     def vt_relaxation(self, blk, dt_stage, stream=None):
         check(self.lib.cb2_vt_relaxation(self.h, blk, dt_stage, stream), "cb2_vt_relaxation")

@@ -7,6 +7,7 @@
 #include <vector>
 #include "common.cuh"
 #include "launch.h"
+#include "sweep.cuh"
 
 namespace cb2 {
 
@@ -584,6 +585,75 @@ int cb2_stage_update(cb2_ctx *ctx, int blk, double dt, int rk, void *stream) {
   int nl = 0;
   CB2_TRY(launch_stage_update(B->z, ctx->p, dt, rk, (cudaStream_t)stream, nl));
   return count(ctx, nl);
+}
+
+int cb2_autotune(cb2_ctx *ctx, int blk, int *tile_ni_out, void *stream) {
+  Block *B = get_block(ctx, blk);
+  if (!B) return CB2_ERR_INVALID;
+  if (two_temperature(ctx)) return CB2_ERR_UNSUPPORTED;
+  const Param &p = ctx->p;
+  Zone &z = B->z;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int sch = p.inviscid_scheme;
+  const bool tunable = (sch == CB2_INV_AUSMP || sch == CB2_INV_HLLC || sch == CB2_INV_ROE) && p.n_spec == 0 &&
+                       (p.reconstruction == CB2_REC_WENO5 || p.reconstruction == CB2_REC_WENO7);
+  const int ndir = z.mz > 1 ? 3 : 2;
+  if (tunable) {
+    // candidates run on a scratch residual, so the caller's dq is untouched
+    double *scratch = nullptr;
+    CB2_TRY(check_cuda(cudaMalloc(&scratch, (size_t)z.L0.sz * p.n_var * sizeof(double))));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = check_cuda(cudaEventCreate(&e0));
+    if (rc == CB2_OK) rc = check_cuda(cudaEventCreate(&e1));
+    Zone zt = z;
+    zt.dq = scratch;
+    Profiler *saved = ctx->prof;
+    ctx->prof = nullptr;  // the trial launches are not part of the profile
+    ProfGuard pg(ctx);
+    for (int d = 1; d < ndir && rc == CB2_OK; ++d) {
+      float best_ms = 1e30f;
+      int best = 0;
+      zt.sweep_mask = 1u << d;
+      for (int c = 0; c < 3 && rc == CB2_OK; ++c) {
+        zt.tile_ni[d] = kTileNI[c];
+        int nl = 0;
+        rc = launch_inviscid_pv(zt, p, s, nl);  // warm-up (also sets the shared-memory limit)
+        if (rc == CB2_OK) rc = check_cuda(cudaEventRecord(e0, s));
+        for (int r = 0; r < 3 && rc == CB2_OK; ++r) rc = launch_inviscid_pv(zt, p, s, nl);
+        if (rc == CB2_OK) rc = check_cuda(cudaEventRecord(e1, s));
+        if (rc == CB2_OK) rc = check_cuda(cudaEventSynchronize(e1));
+        float ms = 0;
+        if (rc == CB2_OK) rc = check_cuda(cudaEventElapsedTime(&ms, e0, e1));
+        if (rc == CB2_OK && ms < best_ms) {
+          best_ms = ms;
+          best = kTileNI[c];
+        }
+      }
+      if (rc == CB2_OK) z.tile_ni[d] = best;
+    }
+    ctx->prof = saved;
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(scratch);
+    if (rc != CB2_OK) return rc;
+    ++ctx->bind_gen;  // a captured step graph holds the old tile widths
+  }
+  if (tile_ni_out)
+    for (int d = 0; d < 3; ++d) tile_ni_out[d] = d == 0 ? 0 : (z.tile_ni[d] ? z.tile_ni[d] : kNI);
+  return CB2_OK;
+}
+
+int cb2_set_tile_widths(cb2_ctx *ctx, int blk, const int *tile_ni) {
+  Block *B = get_block(ctx, blk);
+  if (!B || !tile_ni) return CB2_ERR_INVALID;
+  for (int d = 1; d < 3; ++d) {
+    bool ok = tile_ni[d] == 0;
+    for (int c = 0; c < 3; ++c) ok = ok || tile_ni[d] == kTileNI[c];
+    if (!ok) return CB2_ERR_INVALID;
+  }
+  for (int d = 1; d < 3; ++d) B->z.tile_ni[d] = tile_ni[d];
+  ++ctx->bind_gen;
+  return CB2_OK;
 }
 
 int cb2_vt_relaxation(cb2_ctx *ctx, int blk, double dt_stage, void *stream) {

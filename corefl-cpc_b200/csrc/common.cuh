@@ -71,6 +71,8 @@ struct Zone {
   double *fF, *gF, *hF, *visf, *shock, *dtl, *rts, *efd;
   double *tve;  // two-temperature: T_ve, ghost ngg
   BTypes bt;
+  int tile_ni[3];       // i-columns of the y/z sweep tiles (0: the default), set by the autotuner
+  unsigned sweep_mask;  // primitive sweeps to run (bit d: direction d; 0: all)
 };
 
 // Mechanism tables in device memory (copied from cb2_mechanism by cb2_init).

@@ -379,10 +379,10 @@ __host__ __device__ constexpr int pv_half_width() { return REC == 1 ? 0 : (REC <
 
 // Shared-memory bytes of one sweep tile.
 template <typename T, int NS, int REC, int SOLVER>
-__host__ __device__ constexpr size_t pv_tile_smem(int dir) {
+__host__ __device__ constexpr size_t pv_tile_smem(int dir, int ni = kNI) {
   return sizeof(T) * ((size_t)(5 + NS + 4 + (SOLVER == CB2_INV_ROE ? 1 : 0)) *
                           (dir == 0 ? (kSweepThreads + 2 * pv_half_width<REC>())
-                                    : kNI * (kNS + 2 * pv_half_width<REC>())) +
+                                    : ni * (kSweepThreads / ni + 2 * pv_half_width<REC>())) +
                       (size_t)(2 * (5 + NS) + 2) * kSweepThreads);
 }
 
@@ -390,12 +390,13 @@ __host__ __device__ constexpr size_t pv_tile_smem(int dir) {
 // CTA of kSweepThreads threads; sN holds the node data [NSLOT][NN], sR the right states
 // [NV+2][kSweepThreads], sF the interface fluxes [NV][kSweepThreads].  The tile ends with the
 // whole CTA in step, so a CTA may run several tiles back to back.
-template <typename T, int NS, int DIR, int REC, int SOLVER>
+template <typename T, int NS, int DIR, int REC, int SOLVER, int NI = kNI>
 __device__ __forceinline__ void pv_tile_body(const Zone &z, const Param &p, idx_t run, int bx, int by, int bz,
                                              T *sN, T *sR, T *sF) {
   constexpr int NV = 5 + NS;
   constexpr int RH = pv_half_width<REC>();
-  constexpr int NN = DIR == 0 ? (kSweepThreads + 2 * RH) : kNI * (kNS + 2 * RH);
+  constexpr int NSW = kSweepThreads / NI;  // y/z tile: nodes along the sweep
+  constexpr int NN = DIR == 0 ? (kSweepThreads + 2 * RH) : NI * (NSW + 2 * RH);
   const int tid = threadIdx.x;
   const int g = z.ngg;
   const Layout &L = z.L;
@@ -451,27 +452,27 @@ __device__ __forceinline__ void pv_tile_body(const Zone &z, const Param &p, idx_
     c = tid + RH;
     st = 1;
   } else {
-    const int ti = tid % kNI, ts = tid / kNI;
-    i = bx * kNI + ti;
-    const int s0 = by * (kNS - 2) - 1;
+    const int ti = tid % NI, ts = tid / NI;
+    i = bx * NI + ti;
+    const int s0 = by * (NSW - 2) - 1;
     ms = DIR == 1 ? L.my : L.mz;
     if (DIR == 1) k = bz; else j = bz;
-    for (int s = ts; s < kNS + 2 * RH; s += kNS) {
+    for (int s = ts; s < NSW + 2 * RH; s += NSW) {
       const int nn = s0 - RH + s;
       if (i < L.mx && nn < ms + g) {
-        if (DIR == 1) load(L.at(i, nn, k), s * kNI + ti, i, nn, k);
-        else load(L.at(i, j, nn), s * kNI + ti, i, j, nn);
+        if (DIR == 1) load(L.at(i, nn, k), s * NI + ti, i, nn, k);
+        else load(L.at(i, j, nn), s * NI + ti, i, j, nn);
       }
     }
     n = s0 + ts;
     if (DIR == 1) j = n; else k = n;
     inside = i < L.mx;
     tpos = ts;
-    c = (ts + RH) * kNI + ti;
-    st = kNI;
+    c = (ts + RH) * NI + ti;
+    st = NI;
   }
   const bool rec = inside && n >= -1 && n <= ms;
-  const bool face = rec && n <= ms - 1 && tpos < (DIR == 0 ? kSweepThreads : kNS) - 1;
+  const bool face = rec && n <= ms - 1 && tpos < (DIR == 0 ? kSweepThreads : NSW) - 1;
   const bool upd = face && n >= 0 && tpos >= 1;
   __syncthreads();
 
@@ -487,7 +488,7 @@ __device__ __forceinline__ void pv_tile_body(const Zone &z, const Param &p, idx_
   __syncthreads();
 
   if (face) {
-    const int tn = tid + st;  // the thread of node n+1 (st is 1 or kNI, as the thread layout)
+    const int tn = tid + st;  // the thread of node n+1 (st is 1 or NI, as the thread layout)
     T pr[NV + 2];
 #pragma unroll
     for (int v = 0; v < NV + 2; ++v) pr[v] = sR[v * kSweepThreads + tn];
@@ -517,23 +518,23 @@ __device__ __forceinline__ void pv_tile_body(const Zone &z, const Param &p, idx_
 }
 
 // One whole tile with pv_tile_smem bytes at pv_smem.
-template <typename T, int NS, int DIR, int REC, int SOLVER>
+template <typename T, int NS, int DIR, int REC, int SOLVER, int NI = kNI>
 __device__ __forceinline__ void pv_tile(const Zone &z, const Param &p, idx_t run, int bx, int by, int bz,
                                         unsigned char *pv_smem) {
   constexpr int NV = 5 + NS;
   constexpr int RH = pv_half_width<REC>();
-  constexpr int NN = DIR == 0 ? (kSweepThreads + 2 * RH) : kNI * (kNS + 2 * RH);
+  constexpr int NN = DIR == 0 ? (kSweepThreads + 2 * RH) : NI * (kSweepThreads / NI + 2 * RH);
   constexpr int NSLOT = NV + 4 + (SOLVER == CB2_INV_ROE ? 1 : 0);
   T *sN = reinterpret_cast<T *>(pv_smem);
   T *sR = sN + NSLOT * NN;
   T *sF = sR + (NV + 2) * kSweepThreads;
-  pv_tile_body<T, NS, DIR, REC, SOLVER>(z, p, run, bx, by, bz, sN, sR, sF);
+  pv_tile_body<T, NS, DIR, REC, SOLVER, NI>(z, p, run, bx, by, bz, sN, sR, sF);
 }
 
-template <typename T, int NS, int DIR, int REC, int SOLVER>
+template <typename T, int NS, int DIR, int REC, int SOLVER, int NI = kNI>
 __global__ void __launch_bounds__(kSweepThreads) k_inviscid_pv(Zone z, Param p, idx_t run) {
   extern __shared__ __align__(16) unsigned char pv_smem[];
-  pv_tile<T, NS, DIR, REC, SOLVER>(z, p, run, blockIdx.x, blockIdx.y, blockIdx.z, pv_smem);
+  pv_tile<T, NS, DIR, REC, SOLVER, NI>(z, p, run, blockIdx.x, blockIdx.y, blockIdx.z, pv_smem);
 }
 
 // Entropy-fix delta of the Roe scheme on [-1, m] in every direction (ghost width 1), FP64.
@@ -559,6 +560,29 @@ __global__ void k_entropy_fix_delta(Zone z, Param p) {
   z.efd[z.L1.at(i, j, k)] = d;
 }
 
+template <typename T, int NS, int DIR, int REC, int SOLVER, int NI>
+static int launch_pv_yz(const Zone &z, const Param &p, cudaStream_t s) {
+  SweepGeom geo;
+  const dim3 grid = node_sweep_grid(DIR, z.L, geo, NI);
+  const size_t smem = pv_tile_smem<T, NS, REC, SOLVER>(DIR, NI);
+  auto kern = k_inviscid_pv<T, NS, DIR, REC, SOLVER, NI>;
+  CB2_TRY(prepare_smem(kern, smem));
+  kern<<<grid, kSweepThreads, smem, s>>>(z, p, 0);
+  return check_launch();
+}
+
+// y/z sweep with the block's tile width: the autotuned widths exist for the WENO5/7 air sweeps
+// (the bench's kernels); every other combination uses kNI.
+template <typename T, int NS, int DIR, int REC, int SOLVER>
+static int launch_pv_yz_ni(const Zone &z, const Param &p, cudaStream_t s) {
+  if constexpr ((REC == 5 || REC == 7) && NS == 0) {
+    const int ni = z.tile_ni[DIR];
+    if (ni == 4) return launch_pv_yz<T, NS, DIR, REC, SOLVER, 4>(z, p, s);
+    if (ni == 16) return launch_pv_yz<T, NS, DIR, REC, SOLVER, 16>(z, p, s);
+  }
+  return launch_pv_yz<T, NS, DIR, REC, SOLVER, kNI>(z, p, s);
+}
+
 template <typename T, int NS, int REC, int SOLVER>
 static int launch_pv_dirs(const Zone &z, const Param &p, cudaStream_t s, int &nl) {
   if (SOLVER == CB2_INV_ROE) {
@@ -570,26 +594,23 @@ static int launch_pv_dirs(const Zone &z, const Param &p, cudaStream_t s, int &nl
   }
   const int ndir = z.mz > 1 ? 3 : 2;
   for (int d = 0; d < ndir; ++d) {
-    SweepGeom geo;
-    const dim3 grid = node_sweep_grid(d, z.L, geo);
-    const size_t smem = pv_tile_smem<T, NS, REC, SOLVER>(d);
+    if (z.sweep_mask && !(z.sweep_mask & (1u << d))) continue;
     static const char *names[3] = {"pv_flux_x", "pv_flux_y", "pv_flux_z"};
     ProfScope prof(names[d], s);
     if (d == 0) {
+      SweepGeom geo;
+      const dim3 grid = node_sweep_grid(0, z.L, geo);
+      const size_t smem = pv_tile_smem<T, NS, REC, SOLVER>(0);
       auto kern = k_inviscid_pv<T, NS, 0, REC, SOLVER>;
       CB2_TRY(prepare_smem(kern, smem));
       kern<<<grid, kSweepThreads, smem, s>>>(z, p, geo.run);
+      CB2_TRY(check_launch());
     } else if (d == 1) {
-      auto kern = k_inviscid_pv<T, NS, 1, REC, SOLVER>;
-      CB2_TRY(prepare_smem(kern, smem));
-      kern<<<grid, kSweepThreads, smem, s>>>(z, p, 0);
+      CB2_TRY((launch_pv_yz_ni<T, NS, 1, REC, SOLVER>(z, p, s)));
     } else {
-      auto kern = k_inviscid_pv<T, NS, 2, REC, SOLVER>;
-      CB2_TRY(prepare_smem(kern, smem));
-      kern<<<grid, kSweepThreads, smem, s>>>(z, p, 0);
+      CB2_TRY((launch_pv_yz_ni<T, NS, 2, REC, SOLVER>(z, p, s)));
     }
     ++nl;
-    CB2_TRY(check_launch());
   }
   return CB2_OK;
 }

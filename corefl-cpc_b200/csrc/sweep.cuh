@@ -44,16 +44,21 @@ __host__ __device__ __forceinline__ int node_sweep_nodes(int dir, int r) {
   return dir == 0 ? (kSweepThreads + 2 * r) : kNI * (kNS + 2 * r);
 }
 
-inline dim3 node_sweep_grid(int dir, const Layout &L, SweepGeom &g) {
+// ni: i-columns of a y/z tile (kSweepThreads / ni nodes along the sweep); the autotuner picks
+// it per block and direction among kTileNI.
+constexpr int kTileNI[3] = {4, 8, 16};
+
+inline dim3 node_sweep_grid(int dir, const Layout &L, SweepGeom &g, int ni = kNI) {
   g.dir = dir;
   if (dir == 0) {
     g.run = (idx_t)L.my * L.disp2;
     const idx_t per = kSweepThreads - 2;
     return dim3((unsigned)((g.run + per - 1) / per), 1, (unsigned)L.mz);
   }
-  g.n_itile = (L.mx + kNI - 1) / kNI;
+  const int ns = kSweepThreads / ni;
+  g.n_itile = (L.mx + ni - 1) / ni;
   const int ms = dir == 1 ? L.my : L.mz;
-  g.n_stile = (ms + kNS - 3) / (kNS - 2);
+  g.n_stile = (ms + ns - 3) / (ns - 2);
   const int other = dir == 1 ? L.mz : L.my;
   return dim3((unsigned)g.n_itile, (unsigned)g.n_stile, (unsigned)other);
 }

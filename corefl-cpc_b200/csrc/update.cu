@@ -34,30 +34,7 @@ __global__ void __launch_bounds__(kPtThreads) k_cv_from_bv(Zone z, Param p) {
   const int i = blockIdx.x * kPtThreads + threadIdx.x - g_;
   const int j = blockIdx.y - g_, k = blockIdx.z - g_;
   if (i >= z.mx + g_) return;
-  const idx_t g = z.L.at(i, j, k), sz = z.L.sz;
-  const double rho = z.bv[g], u = z.bv[g + sz], v = z.bv[g + 2 * sz], w = z.bv[g + 3 * sz];
-  const double pr = z.bv[g + 4 * sz];
-  z.cv[g] = rho;
-  z.cv[g + sz] = rho * u;
-  z.cv[g + 2 * sz] = rho * v;
-  z.cv[g + 3 * sz] = rho * w;
-  double E = 0.5 * (u * u + v * v + w * w);
-  if constexpr (NS == 0) {
-    E *= rho;
-    E += pr / (kGammaAir - 1);
-  } else {
-    double h[NS];
-    nasa7_h<NS>(z.bv[g + 5 * sz], p.mech, h);
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      const double y = z.sv[g + s * sz];
-      z.cv[g + (5 + s) * sz] = rho * y;
-      E += h[s] * y;
-    }
-    E *= rho;
-    E -= pr;
-  }
-  z.cv[g + 4 * sz] = E;
+  cv_point<NS>(z, p, z.L.at(i, j, k));
 }
 
 // ---- limit_flow (src/TimeAdvanceFunc.cuh:129-232) --------------------------------------------

@@ -301,6 +301,22 @@ int cb2_rk3_step(cb2_ctx *ctx, double *dt_inout, int fixed_dt, void *stream);
 int cb2_rk3_run(cb2_ctx *ctx, double dt, int fixed_dt, long long max_steps, double t_end, double *time_inout,
                 long long *steps_out, double *dt_last_out, void *stream);
 
+/* ---- autotuning (no counterpart in the reference) ----------------------------------------- */
+
+/* Picks, for block `blk`, the y and z sweep tile widths of the primitive-variable WENO5/WENO7
+ * air sweeps (4, 8 or 16 i-columns by 64, 32 or 16 nodes along the sweep) by timing every
+ * candidate three times with CUDA events on the block's own data.  The candidates write a
+ * scratch residual that is allocated for the call and freed after it, so the caller's arrays
+ * are untouched.  The widths stay with the block until it is rebound; every width gives the
+ * same results bit for bit.  Writes the chosen widths to tile_ni_out[3] (x: 0, the x sweep
+ * streams k-planes) when it is not NULL.  Other schemes keep their fixed tiles (CB2_OK).
+ * Synchronises `stream`; call it outside stream capture. */
+int cb2_autotune(cb2_ctx *ctx, int blk, int *tile_ni_out, void *stream);
+
+/* Sets the widths cb2_autotune would pick (tile_ni[1], tile_ni[2] in {0 = default, 4, 8, 16};
+ * tile_ni[0] is ignored), e.g. to reuse the result of an earlier tuning run. */
+int cb2_set_tile_widths(cb2_ctx *ctx, int blk, const int *tile_ni);
+
 /* ---- diagnostics --------------------------------------------------------------------- */
 
 /* Reads and clears the device status word that kernels set on non-physical states
