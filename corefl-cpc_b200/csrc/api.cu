@@ -79,6 +79,7 @@ struct Block {
   Zone z{};
   std::vector<FaceBC> faces;
   int *d_btype = nullptr;  // six face flag arrays, one allocation
+  float *d_f32 = nullptr;  // mixed form: bv32 and met32, one allocation
 };
 
 }  // namespace cb2
@@ -393,7 +394,10 @@ void cb2_destroy(cb2_ctx *ctx) {
   if (ctx->sg.graph) cudaGraphDestroy(ctx->sg.graph);
   if (ctx->sg.capture) cudaStreamDestroy(ctx->sg.capture);
   cudaFree(ctx->d_run);
-  for (auto &b : ctx->blocks) cudaFree(b.d_btype);
+  for (auto &b : ctx->blocks) {
+    cudaFree(b.d_btype);
+    cudaFree(b.d_f32);
+  }
   cudaFree(ctx->d_tables);
   cudaFree(ctx->d_status);
   cudaFree(ctx->d_partial);
@@ -473,6 +477,8 @@ int cb2_bind_block(cb2_ctx *ctx, int blk, const cb2_zone_view *v, const cb2_face
   Block &B = ctx->blocks[blk];
   cudaFree(B.d_btype);
   B.d_btype = nullptr;
+  cudaFree(B.d_f32);
+  B.d_f32 = nullptr;
   B.v = *v;
   B.z = make_zone(*v);
   B.faces.clear();
@@ -526,6 +532,19 @@ int cb2_bind_block(cb2_ctx *ctx, int blk, const cb2_zone_view *v, const cb2_face
     if (e != cudaSuccess) { ctx->n_partial = 0; return fail_cuda(e); }
     ctx->n_partial = np;
   }
+  if (p.precision == CB2_PREC_MIXED) {
+    // FP32 copies: bv (refreshed per residual) and metric + J (snapshot of the bound block)
+    const size_t sz = (size_t)B.z.L.sz;
+    const size_t off = (6 * sz + 63) / 64 * 64;  // met32 starts on a 256-byte boundary
+    e = cudaMalloc(&B.d_f32, (off + 10 * sz) * sizeof(float));
+    if (e != cudaSuccess) return fail_cuda(e);
+    B.z.bv32 = B.d_f32;
+    B.z.met32 = B.d_f32 + off;
+    int nl = 0;
+    CB2_TRY(launch_to_f32(v->metric, B.z.met32, 9 * sz, nullptr, nl));
+    CB2_TRY(launch_to_f32(v->jac, B.z.met32 + 9 * sz, sz, nullptr, nl));
+    CB2_TRY(check_cuda(cudaDeviceSynchronize()));
+  }
   B.bound = true;
   ++ctx->bind_gen;
   return CB2_OK;
@@ -549,6 +568,10 @@ int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream) {
   cudaStream_t s = (cudaStream_t)stream;
   const Param &p = ctx->p;
   int nl = 0;
+  if (p.precision == CB2_PREC_MIXED) {
+    ProfScope prof("bv_to_f32", s);
+    CB2_TRY(launch_to_f32(B->z.bv, B->z.bv32, 6 * (size_t)B->z.L.sz, s, nl));
+  }
   const bool visc = (mask & CB2_RHS_VISCOUS) && p.viscous_order > 0;
   const bool assign = visc && viscous_assigns_dq(p);  // the viscous term writes dq: no zeroing
   if (!assign) {

@@ -404,13 +404,22 @@ __device__ __forceinline__ void pv_tile_body(const Zone &z, const Param &p, idx_
 
   auto put = [&](int idx, const double *src) { sN[idx] = T(*src); };
   auto load = [&](idx_t gi, int slot, int i, int j, int k) {
+    if constexpr (sizeof(T) == 4) {
+      // mixed form: the FP32 copies of bv, the metric and J
 #pragma unroll
-    for (int l = 0; l < 5; ++l) put(l * NN + slot, z.bv + gi + l * sz);
+      for (int l = 0; l < 5; ++l) sN[l * NN + slot] = z.bv32[gi + l * sz];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) sN[(NV + c) * NN + slot] = z.met32[gi + (3 * DIR + c) * sz];
+      sN[(NV + 3) * NN + slot] = z.met32[gi + 9 * sz];
+    } else {
+#pragma unroll
+      for (int l = 0; l < 5; ++l) put(l * NN + slot, z.bv + gi + l * sz);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) put((NV + c) * NN + slot, z.metric + gi + (3 * DIR + c) * sz);
+      put((NV + 3) * NN + slot, z.jac + gi);
+    }
 #pragma unroll
     for (int s = 0; s < NS; ++s) put((5 + s) * NN + slot, z.sv + gi + s * sz);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) put((NV + c) * NN + slot, z.metric + gi + (3 * DIR + c) * sz);
-    put((NV + 3) * NN + slot, z.jac + gi);
     if constexpr (SOLVER == CB2_INV_ROE) {
       // entropy-fix delta exists on [-1, m] only (ghost width 1)
       const bool in1 = i >= -1 && i <= z.mx && j >= -1 && j <= z.my && k >= -1 && k <= z.mz;

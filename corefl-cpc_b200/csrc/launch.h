@@ -93,6 +93,8 @@ int launch_min_reduce(const double *src, long long n, double *partial, int n_par
                       cudaStream_t s, int &n_launch);
 int min_reduce_partials(long long n);
 int launch_set_value(double *dst, double v, cudaStream_t s, int &n_launch);
+// dst[i] = float(src[i]) for i < n (the mixed form's FP32 copies)
+int launch_to_f32(const double *src, float *dst, size_t n, cudaStream_t s, int &n_launch);
 
 // State of the device-driven step loop (cb2_rk3_run, graph.cu): the loop repeats while
 // step < max_steps, time < t_end, dt is positive and finite and the status word is clear.

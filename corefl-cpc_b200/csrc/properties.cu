@@ -2,6 +2,7 @@
 // src/FieldOperation.cuh:183-247), the local CFL time step (local_time_step<mix>,
 // src/TimeAdvanceFunc.cuh:28-127) and its global minimum (min_of_arr + global_time_step,
 // src/TimeAdvanceFunc.cu:114-164).
+#include <algorithm>
 #include "point.cuh"
 #include "launch.h"
 
@@ -100,6 +101,20 @@ __global__ void k_set_value(double *dst, double v) { *dst = v; }
 
 int launch_set_value(double *dst, double v, cudaStream_t s, int &n_launch) {
   k_set_value<<<1, 1, 0, s>>>(dst, v);
+  ++n_launch;
+  return check_launch();
+}
+
+// Grid-stride FP64 -> FP32 conversion (coalesced 8-byte loads and 4-byte stores).
+__global__ void k_to_f32(const double *__restrict__ src, float *__restrict__ dst, size_t n) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) dst[i] = (float)src[i];
+}
+
+int launch_to_f32(const double *src, float *dst, size_t n, cudaStream_t s, int &n_launch) {
+  if (n == 0) return CB2_OK;
+  const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 32);
+  k_to_f32<<<blocks, 256, 0, s>>>(src, dst, n);
   ++n_launch;
   return check_launch();
 }
