@@ -9,6 +9,7 @@
 //   :86-138): face fluxes from face-averaged metrics/coefficients and compact differences,
 //   mixture species diffusion with the correction velocity and the h_k J_k energy term;
 //   the face difference is taken in the same kernel as the face flux through shared memory.
+#include <type_traits>
 #include "common.cuh"
 #include "thermo.cuh"
 #include "launch.h"
@@ -58,7 +59,7 @@ constexpr int kVisTI = 32, kVisTJ = 8, kVisThreads = kVisTI * kVisTJ;
 // T is the arithmetic type (double: plain form; float: mixed form, FP64 arrays read and
 // written, the stencils, stresses and fluxes evaluated in FP32).
 template <typename T>
-__global__ void __launch_bounds__(kVisThreads) k_visc8_node_flux_air(Zone z, Param p) {
+__global__ void __launch_bounds__(kVisThreads, 3) k_visc8_node_flux_air(Zone z, Param p) {
   const int i = blockIdx.x * kVisTI + threadIdx.x, j = blockIdx.y * kVisTJ + threadIdx.y, k = blockIdx.z;
   if (i >= z.mx || j >= z.my) return;
   const Layout &L = z.L;
@@ -66,35 +67,29 @@ __global__ void __launch_bounds__(kVisThreads) k_visc8_node_flux_air(Zone z, Par
   const BFlags b = bflags(z, i, j, k);
   const idx_t si = 1, sj = L.disp2, sk = L.disp1;
   // the mixed form reads the FP32 copies of bv, the metric and J
+  using Src = std::conditional_t<sizeof(T) == 4, const float *, const double *>;
+  Src BV, M;
+  if constexpr (sizeof(T) == 4) {
+    BV = z.bv32;
+    M = z.met32 + g;
+  } else {
+    BV = z.bv;
+    M = z.metric + g;
+  }
   auto der = [&](int comp, T &dxi, T &deta, T &dzeta) {
-    if constexpr (sizeof(T) == 4) {
-      const float *f = z.bv32 + comp * sz + g;
-      dxi = d8<T>([&](int m) { return f[m * si]; }, i, z.mx, b.il, b.ir);
-      deta = d8<T>([&](int m) { return f[m * sj]; }, j, z.my, b.jl, b.jr);
-      dzeta = d8<T>([&](int m) { return f[m * sk]; }, k, z.mz, b.kl, b.kr);
-    } else {
-      const double *f = z.bv + comp * sz + g;
-      dxi = d8<T>([&](int m) { return T(f[m * si]); }, i, z.mx, b.il, b.ir);
-      deta = d8<T>([&](int m) { return T(f[m * sj]); }, j, z.my, b.jl, b.jr);
-      dzeta = d8<T>([&](int m) { return T(f[m * sk]); }, k, z.mz, b.kl, b.kr);
-    }
+    const Src f = BV + comp * sz + g;
+    dxi = d8<T>([&](int m) { return T(f[m * si]); }, i, z.mx, b.il, b.ir);
+    deta = d8<T>([&](int m) { return T(f[m * sj]); }, j, z.my, b.jl, b.jr);
+    dzeta = d8<T>([&](int m) { return T(f[m * sk]); }, k, z.mz, b.kl, b.kr);
   };
   T u_xi, u_eta, u_zeta, v_xi, v_eta, v_zeta, w_xi, w_eta, w_zeta, t_xi, t_eta, t_zeta;
   der(1, u_xi, u_eta, u_zeta);
   der(2, v_xi, v_eta, v_zeta);
   der(3, w_xi, w_eta, w_zeta);
   der(5, t_xi, t_eta, t_zeta);
-  T mt[9];
-  if constexpr (sizeof(T) == 4) {
-#pragma unroll
-    for (int c = 0; c < 9; ++c) mt[c] = z.met32[g + c * sz];
-  } else {
-#pragma unroll
-    for (int c = 0; c < 9; ++c) mt[c] = z.metric[g + c * sz];
-  }
-  const T xi_x = mt[0], xi_y = mt[1], xi_z = mt[2];
-  const T eta_x = mt[3], eta_y = mt[4], eta_z = mt[5];
-  const T zeta_x = mt[6], zeta_y = mt[7], zeta_z = mt[8];
+  const T xi_x = T(M[0]), xi_y = T(M[sz]), xi_z = T(M[2 * sz]);
+  const T eta_x = T(M[3 * sz]), eta_y = T(M[4 * sz]), eta_z = T(M[5 * sz]);
+  const T zeta_x = T(M[6 * sz]), zeta_y = T(M[7 * sz]), zeta_z = T(M[8 * sz]);
   const T u_x = u_xi * xi_x + u_eta * eta_x + u_zeta * zeta_x;
   const T u_y = u_xi * xi_y + u_eta * eta_y + u_zeta * zeta_y;
   const T u_z = u_xi * xi_z + u_eta * eta_z + u_zeta * zeta_z;
@@ -114,16 +109,7 @@ __global__ void __launch_bounds__(kVisThreads) k_visc8_node_flux_air(Zone z, Par
   const T t_z = t_xi * xi_z + t_eta * eta_z + t_zeta * zeta_z;
   const T cp = T(kGammaAir * kRAir / (kGammaAir - 1));
   const T kap = mu / T(p.Pr) * cp;
-  T u, v, w;
-  if constexpr (sizeof(T) == 4) {
-    u = z.bv32[g + sz];
-    v = z.bv32[g + 2 * sz];
-    w = z.bv32[g + 3 * sz];
-  } else {
-    u = z.bv[g + sz];
-    v = z.bv[g + 2 * sz];
-    w = z.bv[g + 3 * sz];
-  }
+  const T u = T(BV[g + sz]), v = T(BV[g + 2 * sz]), w = T(BV[g + 3 * sz]);
   const T Ex = u * txx + v * txy + w * txz + kap * t_x;
   const T Ey = u * txy + v * tyy + w * tyz + kap * t_y;
   const T Ez = u * txz + v * tyz + w * tzz + kap * t_z;
