@@ -535,11 +535,18 @@ int cb2_bind_block(cb2_ctx *ctx, int blk, const cb2_zone_view *v, const cb2_face
   if (p.precision == CB2_PREC_MIXED) {
     // FP32 copies: bv (refreshed per residual) and metric + J (snapshot of the bound block)
     const size_t sz = (size_t)B.z.L.sz;
-    const size_t off = (6 * sz + 63) / 64 * 64;  // met32 starts on a 256-byte boundary
-    e = cudaMalloc(&B.d_f32, (off + 10 * sz) * sizeof(float));
+    auto up = [](size_t n) { return (n + 63) / 64 * 64; };  // each copy starts on a 256-byte boundary
+    const size_t off = up(6 * sz), offf = off + up(10 * sz);
+    const size_t nflux = p.viscous_order == 8 ? up((size_t)p.n_var * sz) : 0;
+    e = cudaMalloc(&B.d_f32, (offf + 3 * nflux) * sizeof(float));
     if (e != cudaSuccess) return fail_cuda(e);
     B.z.bv32 = B.d_f32;
     B.z.met32 = B.d_f32 + off;
+    if (nflux) {
+      B.z.fF32 = B.d_f32 + offf;
+      B.z.gF32 = B.z.fF32 + nflux;
+      B.z.hF32 = B.z.gF32 + nflux;
+    }
     int nl = 0;
     CB2_TRY(launch_to_f32(v->metric, B.z.met32, 9 * sz, nullptr, nl));
     CB2_TRY(launch_to_f32(v->jac, B.z.met32 + 9 * sz, sz, nullptr, nl));

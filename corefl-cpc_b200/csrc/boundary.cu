@@ -240,6 +240,18 @@ __global__ void k_eliminate_k_gradient(Zone z, Param p) {
 
 // Periodic exchange of the 8th-order viscous node fluxes (periodic_exchange task 1,
 // src/DataCommunication.cu:665-712).
+// The node-flux arrays the periodic exchange works on: the caller's FP64 arrays, or the
+// mixed form's FP32 copies.
+template <typename F>
+__device__ __forceinline__ void flux_arrays(const Zone &z, F *arr[3]) {
+  if constexpr (sizeof(F) == 4) {
+    arr[0] = z.fF32; arr[1] = z.gF32; arr[2] = z.hF32;
+  } else {
+    arr[0] = z.fF; arr[1] = z.gF; arr[2] = z.hF;
+  }
+}
+
+template <typename F>
 __global__ void k_periodic_flux(Zone z, Param p, FaceBC f) {
   int i, j, k;
   if (!face_point(f, i, j, k)) return;
@@ -250,10 +262,11 @@ __global__ void k_periodic_flux(Zone z, Param p, FaceBC f) {
   o[f.face] = f.direction < 0 ? ext[f.face] - 1 : 0;
   const idx_t sz = z.L.sz;
   const idx_t gb = z.L.at(i, j, k), go = z.L.at(o[0], o[1], o[2]);
-  double *arr[3] = {z.fF, z.gF, z.hF};
+  F *arr[3];
+  flux_arrays<F>(z, arr);
   for (int l = 0; l < p.n_var; ++l)
     for (int a = 0; a < 3; ++a) {
-      const double ave = 0.5 * (arr[a][gb + l * sz] + arr[a][go + l * sz]);
+      const F ave = F(0.5) * (arr[a][gb + l * sz] + arr[a][go + l * sz]);
       arr[a][gb + l * sz] = ave;
       arr[a][go + l * sz] = ave;
     }
@@ -341,18 +354,20 @@ __global__ void k_bc_periodic_pair(Zone z, Param p, FaceBC f) {
 
 // The same pairing for the 8th-order viscous node fluxes (components 1..n_var-1 of the three
 // flux arrays; component 0 carries no viscous flux and is never read).
+template <typename F>
 __global__ void k_periodic_flux_pair(Zone z, Param p, FaceBC f) {
   PairItem it;
   const int g = z.ngg;
   if (!pair_item(f, g, it)) return;
   const int m = f.face == 0 ? z.mx : (f.face == 1 ? z.my : z.mz);
   const idx_t sz = z.L.sz;
-  double *arr[3] = {z.fF, z.gF, z.hF};
+  F *arr[3];
+  flux_arrays<F>(z, arr);
   if (it.p == 0) {
     const idx_t ga = along(z.L, f.face, it.i, it.j, it.k, 0), gb = along(z.L, f.face, it.i, it.j, it.k, m - 1);
     for (int l = 1; l < p.n_var; ++l)
       for (int a = 0; a < 3; ++a) {
-        const double ave = 0.5 * (arr[a][ga + l * sz] + arr[a][gb + l * sz]);
+        const F ave = F(0.5) * (arr[a][ga + l * sz] + arr[a][gb + l * sz]);
         arr[a][ga + l * sz] = ave;
         arr[a][gb + l * sz] = ave;
       }
@@ -454,7 +469,10 @@ int launch_periodic_flux_exchange(const Zone &z, const Param &p, const FaceBC *f
     if (lf >= 0) {
       const long long np = face_points(faces[lf]) * (2 * z.ngg + 1);
       ProfScope prof("periodic_flux_exchange", s);
-      k_periodic_flux_pair<<<(unsigned)((np + 127) / 128), 128, 0, s>>>(z, p, faces[lf]);
+      if (p.precision == CB2_PREC_MIXED)
+        k_periodic_flux_pair<float><<<(unsigned)((np + 127) / 128), 128, 0, s>>>(z, p, faces[lf]);
+      else
+        k_periodic_flux_pair<double><<<(unsigned)((np + 127) / 128), 128, 0, s>>>(z, p, faces[lf]);
       ++n_launch;
       CB2_TRY(check_launch());
       f = q;
@@ -464,7 +482,8 @@ int launch_periodic_flux_exchange(const Zone &z, const Param &p, const FaceBC *f
     const unsigned blocks = (unsigned)((np + 127) / 128);
     if (!blocks) continue;
     ProfScope prof("periodic_flux_exchange", s);
-    k_periodic_flux<<<blocks, 128, 0, s>>>(z, p, faces[f]);
+    if (p.precision == CB2_PREC_MIXED) k_periodic_flux<float><<<blocks, 128, 0, s>>>(z, p, faces[f]);
+    else k_periodic_flux<double><<<blocks, 128, 0, s>>>(z, p, faces[f]);
     ++n_launch;
     CB2_TRY(check_launch());
   }

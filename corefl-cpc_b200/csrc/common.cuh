@@ -74,6 +74,7 @@ struct Zone {
   // same padded layout): bv (6 comps, refreshed at the start of every residual) and the
   // metric (9 comps) followed by J, taken when the block is bound
   float *bv32, *met32;
+  float *fF32, *gF32, *hF32;  // mixed form: 8th-order viscous node fluxes (n_var comps, ghost ngg)
   BTypes bt;
   int tile_ni[3];       // i-columns of the y/z sweep tiles (0: the default), set by the autotuner
   unsigned sweep_mask;  // primitive sweeps to run (bit d: direction d; 0: all)

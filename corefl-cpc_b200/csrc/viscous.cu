@@ -59,7 +59,7 @@ constexpr int kVisTI = 32, kVisTJ = 8, kVisThreads = kVisTI * kVisTJ;
 // T is the arithmetic type (double: plain form; float: mixed form, FP64 arrays read and
 // written, the stencils, stresses and fluxes evaluated in FP32).
 template <typename T>
-__global__ void __launch_bounds__(kVisThreads, 3) k_visc8_node_flux_air(Zone z, Param p) {
+__global__ void __launch_bounds__(kVisThreads, sizeof(T) == 8 ? 3 : 4) k_visc8_node_flux_air(Zone z, Param p) {
   const int i = blockIdx.x * kVisTI + threadIdx.x, j = blockIdx.y * kVisTJ + threadIdx.y, k = blockIdx.z;
   if (i >= z.mx || j >= z.my) return;
   const Layout &L = z.L;
@@ -113,18 +113,25 @@ __global__ void __launch_bounds__(kVisThreads, 3) k_visc8_node_flux_air(Zone z, 
   const T Ex = u * txx + v * txy + w * txz + kap * t_x;
   const T Ey = u * txy + v * tyy + w * tyz + kap * t_y;
   const T Ez = u * txz + v * tyz + w * tzz + kap * t_z;
-  z.fF[g + sz] = xi_x * txx + xi_y * txy + xi_z * txz;
-  z.fF[g + 2 * sz] = xi_x * txy + xi_y * tyy + xi_z * tyz;
-  z.fF[g + 3 * sz] = xi_x * txz + xi_y * tyz + xi_z * tzz;
-  z.gF[g + sz] = eta_x * txx + eta_y * txy + eta_z * txz;
-  z.gF[g + 2 * sz] = eta_x * txy + eta_y * tyy + eta_z * tyz;
-  z.gF[g + 3 * sz] = eta_x * txz + eta_y * tyz + eta_z * tzz;
-  z.hF[g + sz] = zeta_x * txx + zeta_y * txy + zeta_z * txz;
-  z.hF[g + 2 * sz] = zeta_x * txy + zeta_y * tyy + zeta_z * tyz;
-  z.hF[g + 3 * sz] = zeta_x * txz + zeta_y * tyz + zeta_z * tzz;
-  z.fF[g + 4 * sz] = xi_x * Ex + xi_y * Ey + xi_z * Ez;
-  z.gF[g + 4 * sz] = eta_x * Ex + eta_y * Ey + eta_z * Ez;
-  z.hF[g + 4 * sz] = zeta_x * Ex + zeta_y * Ey + zeta_z * Ez;
+  // node fluxes: the caller's FP64 arrays, or the FP32 copies the mixed form's divergence reads
+  T *FF, *GF, *HF;
+  if constexpr (sizeof(T) == 4) {
+    FF = z.fF32; GF = z.gF32; HF = z.hF32;
+  } else {
+    FF = z.fF; GF = z.gF; HF = z.hF;
+  }
+  FF[g + sz] = xi_x * txx + xi_y * txy + xi_z * txz;
+  FF[g + 2 * sz] = xi_x * txy + xi_y * tyy + xi_z * tyz;
+  FF[g + 3 * sz] = xi_x * txz + xi_y * tyz + xi_z * tzz;
+  GF[g + sz] = eta_x * txx + eta_y * txy + eta_z * txz;
+  GF[g + 2 * sz] = eta_x * txy + eta_y * tyy + eta_z * tyz;
+  GF[g + 3 * sz] = eta_x * txz + eta_y * tyz + eta_z * tzz;
+  HF[g + sz] = zeta_x * txx + zeta_y * txy + zeta_z * txz;
+  HF[g + 2 * sz] = zeta_x * txy + zeta_y * tyy + zeta_z * tyz;
+  HF[g + 3 * sz] = zeta_x * txz + zeta_y * tyz + zeta_z * tzz;
+  FF[g + 4 * sz] = xi_x * Ex + xi_y * Ey + xi_z * Ez;
+  GF[g + 4 * sz] = eta_x * Ex + eta_y * Ey + eta_z * Ez;
+  HF[g + 4 * sz] = zeta_x * Ex + zeta_y * Ey + zeta_z * Ez;
 }
 
 // The divergence reads each flux array along one direction only; rows of kVisRow i-nodes
@@ -134,7 +141,7 @@ constexpr int kVisRow = 128;
 // ASSIGN: the divergence is the first term of the residual, so it writes dq (the mass row
 // gets zero) instead of adding to a zeroed dq.
 template <typename T, bool ASSIGN>
-__global__ void __launch_bounds__(kVisRow) k_visc8_divergence(Zone z, Param p) {
+__global__ void __launch_bounds__(kVisRow, sizeof(T) == 8 ? 16 : 12) k_visc8_divergence(Zone z, Param p) {
   const int i = blockIdx.x * kVisRow + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
   if (i >= z.mx) return;
   const Layout &L = z.L;
@@ -144,8 +151,15 @@ __global__ void __launch_bounds__(kVisRow) k_visc8_divergence(Zone z, Param p) {
   const T jac = T(z.jac[g]);
   const idx_t g0 = z.L0.at(i, j, k), sz0 = z.L0.sz;
   if (ASSIGN) z.dq[g0] = 0.0;
+  using Src = std::conditional_t<sizeof(T) == 4, const float *, const double *>;
+  Src F0, G0, H0;
+  if constexpr (sizeof(T) == 4) {
+    F0 = z.fF32; G0 = z.gF32; H0 = z.hF32;
+  } else {
+    F0 = z.fF; G0 = z.gF; H0 = z.hF;
+  }
   for (int l = 1; l < p.n_var; ++l) {
-    const double *f = z.fF + l * sz + g, *gg = z.gF + l * sz + g, *h = z.hF + l * sz + g;
+    const Src f = F0 + l * sz + g, gg = G0 + l * sz + g, h = H0 + l * sz + g;
     const T d = d8<T>([&](int m) { return T(f[m]); }, i, z.mx, b.il, b.ir) +
                 d8<T>([&](int m) { return T(gg[m * sj]); }, j, z.my, b.jl, b.jr) +
                 d8<T>([&](int m) { return T(h[m * sk]); }, k, z.mz, b.kl, b.kr);
@@ -338,10 +352,16 @@ int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_fac
     CB2_TRY(launch_periodic_flux_exchange(z, p, faces, n_faces, s, nl));
     {
       ProfScope prof("visc8_divergence", s);
-      // the divergence is a load-bound sum of four 9-point stencils: FP64 in both forms
+      // the mixed form sums the FP32 node fluxes in FP32 and adds the result to the FP64 dq
       const dim3 grow((z.mx + kVisRow - 1) / kVisRow, z.my, z.mz);
-      if (assign) k_visc8_divergence<double, true><<<grow, kVisRow, 0, s>>>(z, p);
-      else k_visc8_divergence<double, false><<<grow, kVisRow, 0, s>>>(z, p);
+      if (p.precision == CB2_PREC_MIXED) {
+        if (assign) k_visc8_divergence<float, true><<<grow, kVisRow, 0, s>>>(z, p);
+        else k_visc8_divergence<float, false><<<grow, kVisRow, 0, s>>>(z, p);
+      } else if (assign) {
+        k_visc8_divergence<double, true><<<grow, kVisRow, 0, s>>>(z, p);
+      } else {
+        k_visc8_divergence<double, false><<<grow, kVisRow, 0, s>>>(z, p);
+      }
     }
     ++nl;
     return check_launch();
