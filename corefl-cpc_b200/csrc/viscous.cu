@@ -59,7 +59,7 @@ constexpr int kVisTI = 32, kVisTJ = 8, kVisThreads = kVisTI * kVisTJ;
 // T is the arithmetic type (double: plain form; float: mixed form, FP64 arrays read and
 // written, the stencils, stresses and fluxes evaluated in FP32).
 template <typename T>
-__global__ void __launch_bounds__(kVisThreads, sizeof(T) == 8 ? 3 : 4) k_visc8_node_flux_air(Zone z, Param p) {
+__device__ __forceinline__ void visc8_node_flux_air(const Zone &z, const Param &p) {
   const int i = blockIdx.x * kVisTI + threadIdx.x, j = blockIdx.y * kVisTJ + threadIdx.y, k = blockIdx.z;
   if (i >= z.mx || j >= z.my) return;
   const Layout &L = z.L;
@@ -134,6 +134,14 @@ __global__ void __launch_bounds__(kVisThreads, sizeof(T) == 8 ? 3 : 4) k_visc8_n
   HF[g + 4 * sz] = zeta_x * Ex + zeta_y * Ey + zeta_z * Ez;
 }
 
+__global__ void __launch_bounds__(kVisThreads) k_visc8_node_flux_air_f64(Zone z, Param p) {
+  visc8_node_flux_air<double>(z, p);
+}
+// bounded to 64 registers: four CTAs of 256 threads per SM
+__global__ void __launch_bounds__(kVisThreads, 4) k_visc8_node_flux_air_f32(Zone z, Param p) {
+  visc8_node_flux_air<float>(z, p);
+}
+
 // The divergence reads each flux array along one direction only; rows of kVisRow i-nodes
 // measured faster than 2-D tiles for it.
 constexpr int kVisRow = 128;
@@ -141,7 +149,7 @@ constexpr int kVisRow = 128;
 // ASSIGN: the divergence is the first term of the residual, so it writes dq (the mass row
 // gets zero) instead of adding to a zeroed dq.
 template <typename T, bool ASSIGN>
-__global__ void __launch_bounds__(kVisRow, sizeof(T) == 8 ? 16 : 12) k_visc8_divergence(Zone z, Param p) {
+__device__ __forceinline__ void visc8_divergence_row(const Zone &z, const Param &p) {
   const int i = blockIdx.x * kVisRow + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
   if (i >= z.mx) return;
   const Layout &L = z.L;
@@ -158,6 +166,7 @@ __global__ void __launch_bounds__(kVisRow, sizeof(T) == 8 ? 16 : 12) k_visc8_div
   } else {
     F0 = z.fF; G0 = z.gF; H0 = z.hF;
   }
+#pragma unroll 1
   for (int l = 1; l < p.n_var; ++l) {
     const Src f = F0 + l * sz + g, gg = G0 + l * sz + g, h = H0 + l * sz + g;
     const T d = d8<T>([&](int m) { return T(f[m]); }, i, z.mx, b.il, b.ir) +
@@ -166,6 +175,16 @@ __global__ void __launch_bounds__(kVisRow, sizeof(T) == 8 ? 16 : 12) k_visc8_div
     if (ASSIGN) z.dq[g0 + l * sz0] = double(d * jac);
     else z.dq[g0 + l * sz0] += double(d * jac);
   }
+}
+
+// Both sums fit in 32 registers (16 rows of 128 threads per SM); the FP32 one needs the bound.
+template <bool ASSIGN>
+__global__ void __launch_bounds__(kVisRow) k_visc8_divergence_f64(Zone z, Param p) {
+  visc8_divergence_row<double, ASSIGN>(z, p);
+}
+template <bool ASSIGN>
+__global__ void __launch_bounds__(kVisRow, 16) k_visc8_divergence_f32(Zone z, Param p) {
+  visc8_divergence_row<float, ASSIGN>(z, p);
 }
 
 // ---- 2nd-order face fluxes ----------------------------------------------------------------
@@ -344,8 +363,8 @@ int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_fac
     const dim3 grid((z.mx + kVisTI - 1) / kVisTI, (z.my + kVisTJ - 1) / kVisTJ, z.mz), block(kVisTI, kVisTJ);
     {
       ProfScope prof("visc8_node_flux", s);
-      if (p.precision == CB2_PREC_MIXED) k_visc8_node_flux_air<float><<<grid, block, 0, s>>>(z, p);
-      else k_visc8_node_flux_air<double><<<grid, block, 0, s>>>(z, p);
+      if (p.precision == CB2_PREC_MIXED) k_visc8_node_flux_air_f32<<<grid, block, 0, s>>>(z, p);
+      else k_visc8_node_flux_air_f64<<<grid, block, 0, s>>>(z, p);
     }
     ++nl;
     CB2_TRY(check_launch());
@@ -355,12 +374,12 @@ int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_fac
       // the mixed form sums the FP32 node fluxes in FP32 and adds the result to the FP64 dq
       const dim3 grow((z.mx + kVisRow - 1) / kVisRow, z.my, z.mz);
       if (p.precision == CB2_PREC_MIXED) {
-        if (assign) k_visc8_divergence<float, true><<<grow, kVisRow, 0, s>>>(z, p);
-        else k_visc8_divergence<float, false><<<grow, kVisRow, 0, s>>>(z, p);
+        if (assign) k_visc8_divergence_f32<true><<<grow, kVisRow, 0, s>>>(z, p);
+        else k_visc8_divergence_f32<false><<<grow, kVisRow, 0, s>>>(z, p);
       } else if (assign) {
-        k_visc8_divergence<double, true><<<grow, kVisRow, 0, s>>>(z, p);
+        k_visc8_divergence_f64<true><<<grow, kVisRow, 0, s>>>(z, p);
       } else {
-        k_visc8_divergence<double, false><<<grow, kVisRow, 0, s>>>(z, p);
+        k_visc8_divergence_f64<false><<<grow, kVisRow, 0, s>>>(z, p);
       }
     }
     ++nl;
