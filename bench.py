@@ -31,15 +31,43 @@ sys.path.insert(0, os.path.join(REPO, "corefl-cpc_b200"))
 METRIC = "RK3 cell-updates/s, mixed vs FP64 at equal L1 error; p50/p99 solve latency"
 UNIT = "cell-updates/s"
 
-# Compulsory FP64 HBM traffic of each kernel per node it processes (every array it reads or
-# writes counted once), used for the roofline of the dominant kernel.
+# Compulsory HBM traffic of each kernel per interior node it processes (every array it reads or
+# writes counted once), for the per-kernel rooflines.  Plain form: FP64 arrays.
 KERNEL_BYTES_PER_NODE = {
     "pv_flux_x": 8 * (5 + 3 + 1 + 10), "pv_flux_y": 8 * (5 + 3 + 1 + 10), "pv_flux_z": 8 * (5 + 3 + 1 + 10),
     "weno_char_x": 8 * (5 + 2 + 3 + 1 + 10), "weno_char_y": 8 * (5 + 2 + 3 + 1 + 10),
     "weno_char_z": 8 * (5 + 2 + 3 + 1 + 10),
-    "visc8_node_flux": 8 * (4 + 9 + 1 + 12), "visc8_divergence": 8 * (12 + 1 + 8),
+    # u, v, w, T + 9 metric + mu read, 12 node fluxes written
+    "visc8_node_flux": 8 * (4 + 9 + 1 + 12),
+    # 12 node fluxes + J read, dq (5) written: the divergence assigns dq
+    "visc8_divergence": 8 * (12 + 1 + 5),
     "stage_update": 8 * (5 + 5 + 5 + 1 + 5 + 6),
 }
+# Mixed form: the sweeps and node fluxes read the FP32 copies of bv, the metric and J, the node
+# fluxes live in FP32 scratch; dq, the state and mu stay FP64.
+KERNEL_BYTES_PER_NODE_MIXED = dict(KERNEL_BYTES_PER_NODE, **{
+    "pv_flux_x": 4 * (5 + 3 + 1) + 8 * 10, "pv_flux_y": 4 * (5 + 3 + 1) + 8 * 10,
+    "pv_flux_z": 4 * (5 + 3 + 1) + 8 * 10,
+    "visc8_node_flux": 4 * (4 + 9 + 12) + 8, "visc8_divergence": 4 * (12 + 1) + 8 * 5,
+})
+# per padded node (kernels that sweep the ghost layers too)
+KERNEL_BYTES_PER_PADDED_NODE = {"bv_to_f32": 6 * (8 + 4), "store_qn": 5 * 16, "properties": 8 * (4 + 2)}
+
+
+def kernel_rooflines(prof, nodes, padded, bytes_map, peak):
+    """Achieved algorithmic GB/s of every profiled kernel whose compulsory bytes are known."""
+    out = {}
+    for name, (count, ms) in prof.items():
+        per = bytes_map.get(name)
+        n = nodes
+        if per is None:
+            per, n = KERNEL_BYTES_PER_PADDED_NODE.get(name), padded
+        if per is None or ms <= 0:
+            continue
+        gbs = per * n * count / (ms * 1e-3) / 1e9
+        out[name] = {"ms_per_step": ms, "launches": count, "bytes_per_node": per, "achieved_GBps": gbs,
+                     "frac": gbs / peak}
+    return out
 
 
 def parse():
@@ -266,6 +294,8 @@ def gpu_arm(args, rank, world, local_rank):
                 "traffic": (traffic * nodes if traffic else None),
                 "algorithmic_bytes": bpn * nodes, "avg_launch_ms": avg_ms,
                 "share": kms / total}
+    padded = (args.n + 1 + 8) ** 3
+    kernel_roofs = kernel_rooflines(prof, nodes, padded, KERNEL_BYTES_PER_NODE, peak)
 
     e2e = None
     if not args.no_e2e:
@@ -321,7 +351,8 @@ def gpu_arm(args, rank, world, local_rank):
                        "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
             "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
             "clocks": clocks, "status_flags": status, "mixed": mixed, "serve": served,
-            "kernel_ms_per_step": {k: v[1] for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}}
+            "kernel_ms_per_step": {k: v[1] for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
+            "kernel_rooflines": kernel_roofs}
     print(json.dumps(line), flush=True)
 
 
@@ -399,6 +430,9 @@ def mixed_form(args, p, dev, faces, host_state, xyz, dt, ctx64, stream, nodes, w
            "t_end": t_end, "status_flags": status32,
            "accuracy_bound_l1": 1e-6,
            "kernel_ms_per_step": {k: v[1] for k, v in sorted(prof32.items(), key=lambda kv: -kv[1][1])}}
+    peak, _ = measured_peaks()
+    n_side = round(nodes ** (1.0 / 3.0))
+    out["kernel_rooflines"] = kernel_rooflines(prof32, nodes, (n_side + 8) ** 3, KERNEL_BYTES_PER_NODE_MIXED, peak)
     out["meets_accuracy_bound"] = out["l1_rho_vs_fp64"] <= 1e-6
     return out
 
