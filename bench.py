@@ -83,6 +83,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
     ap.add_argument("--no-serve", action="store_true", help="skip the served reactor/shock-tube workload")
+    ap.add_argument("--no-reacting", action="store_true", help="skip the reacting H2/air box")
+    ap.add_argument("--reacting-n", type=int, default=192, help="nodes per side of the reacting H2/air box")
+    ap.add_argument("--reacting-steps", type=int, default=5, help="timed steps of the reacting H2/air box")
     ap.add_argument("--serve-seconds", type=float, default=0.05,
                     help="length of the seeded Poisson arrival window of the served workload")
     ap.add_argument("--serve-tube-t-end", type=float, default=1e-6,
@@ -331,6 +334,7 @@ def gpu_arm(args, rank, world, local_rank):
     ctx.close()
     del dev, xyz
     torch.cuda.empty_cache()
+    reacting = None if args.no_reacting else reacting_box(args, local_rank)
     served = None if args.no_serve else serve_workload(args)
     if dist:
         dist.barrier()
@@ -350,7 +354,7 @@ def gpu_arm(args, rank, world, local_rank):
                        "l2": "inputs larger than L2 (about 7 GB of field arrays per GPU)",
                        "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
             "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clocks, "status_flags": status, "mixed": mixed, "serve": served,
+            "clocks": clocks, "status_flags": status, "mixed": mixed, "serve": served, "reacting_box": reacting,
             "kernel_ms_per_step": {k: v[1] for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
             "kernel_rooflines": kernel_roofs}
     print(json.dumps(line), flush=True)
@@ -434,6 +438,65 @@ def mixed_form(args, p, dev, faces, host_state, xyz, dt, ctx64, stream, nodes, w
     n_side = round(nodes ** (1.0 / 3.0))
     out["kernel_rooflines"] = kernel_rooflines(prof32, nodes, (n_side + 8) ** 3, KERNEL_BYTES_PER_NODE_MIXED, peak)
     out["meets_accuracy_bound"] = out["l1_rho_vs_fp64"] <= 1e-6
+    return out
+
+
+def reacting_box(args, local_rank):
+    """The reacting H2/air box (3-D periodic, --reacting-n nodes per side, L = 1 mm, random-phase
+    velocity with u_rms = 10 m/s, 1200 K with five 300 K hot spots, 1 atm, stoichiometric
+    premixed H2/air, 9 species / 19 reactions): WENO5 + HLLC, 2nd-order mixture-averaged
+    viscous terms, finite-rate chemistry, fixed dt = 2e-9 s, in the plain and the mixed form
+    (FP32 sweeps; viscous, chemistry and transport FP64).  Timed with CUDA events over
+    --reacting-steps steps after 2 warm-up steps, each form from the same initial state."""
+    import torch
+    import cb200
+    from cb200 import abi, cases
+    from cb200 import mech as mechmod
+    from cb200.field import DeviceBlock
+    h2 = mechmod.load_json(os.path.join(REPO, "tests", "golden", "h2_li2004.json"))
+    case = cases.h2_air_box(h2, n_nodes=args.reacting_n)
+    p, hb, faces = case.param, case.blocks[0], case.faces[0]
+    dev = DeviceBlock(hb, device=f"cuda:{local_rank}")
+    init = {n: dev.t[n].clone() for n in ("cv", "bv", "sv")}
+    del case, hb
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    nodes = args.reacting_n ** 3
+    dt = 2e-9
+    out = {"workload": f"reacting H2/air box {args.reacting_n}^3 nodes, WENO5 + HLLC, 2nd-order viscous, "
+                       f"finite-rate chemistry (9 species, 19 reactions), fixed dt 2e-9 s",
+           "steps": args.reacting_steps}
+    for name, prec in (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED)):
+        pv = abi.ParamView.from_buffer_copy(p)
+        pv.precision = prec
+        for n, t in init.items():
+            dev.t[n].copy_(t)
+        ctx = cb200.Context(pv)
+        ctx.bind(0, dev.view(), faces)
+        ctx.properties(0, sh)
+        for _ in range(2):
+            ctx.rk3_step(dt, True, sh)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.reacting_steps):
+            ctx.rk3_step(dt, True, sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.reacting_steps
+        ctx.profile(True)
+        ctx.rk3_step(dt, True, sh)
+        torch.cuda.synchronize()
+        prof = ctx.profile_read()
+        ctx.profile(False)
+        status = ctx.read_status(sh)
+        ctx.close()
+        top = sorted(prof.items(), key=lambda kv: -kv[1][1])[:8]
+        out[name] = {"value": nodes / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "status_flags": status,
+                     "kernel_ms_per_step": {k: v[1] for k, v in top}}
+    out["speedup_mixed_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    del dev, init
+    torch.cuda.empty_cache()
     return out
 
 
