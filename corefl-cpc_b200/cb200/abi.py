@@ -101,3 +101,11 @@ class ServeOptions(C.Structure):
                 ("tube_TL", C.c_double), ("tube_pL", C.c_double), ("tube_TR", C.c_double),
                 ("tube_pR", C.c_double), ("tube_Y", C.POINTER(C.c_double)), ("time_limit_s", C.c_double),
                 ("stats", C.POINTER(ServeStats))]
+
+
+BLOCK_DONE, BLOCK_FAILED = 1, 2
+
+
+class BlockCase(C.Structure):
+    _fields_ = [("zone", ZoneView), ("time", C.c_double), ("t_end", C.c_double), ("dt", C.c_double),
+                ("last_dt", C.c_double), ("steps", C.c_int), ("status", C.c_int)]

@@ -43,6 +43,9 @@ def load():
         "cb2_boundary": (C.c_int, [vp, C.c_int, vp]),
         "cb2_vt_relaxation": (C.c_int, [vp, C.c_int, C.c_double, vp]),
         "cb2_autotune": (C.c_int, [vp, C.c_int, P(C.c_int), vp]),
+        "cb2_block_batch_advance": (C.c_int, [vp, vp, C.c_int, C.c_int, vp]),
+        "cb2_block_batch_autotune": (C.c_int, [vp, vp, C.c_int, P(C.c_int), vp]),
+        "cb2_block_batch_set_tile_width": (C.c_int, [vp, C.c_int]),
         "cb2_set_tile_widths": (C.c_int, [vp, C.c_int, P(C.c_int)]),
         "cb2_properties": (C.c_int, [vp, C.c_int, vp]),
         "cb2_cv_from_bv": (C.c_int, [vp, C.c_int, vp]),
@@ -105,6 +108,20 @@ class Context:
         out = (C.c_int * 3)()
         check(self.lib.cb2_autotune(self.h, blk, out, stream), "cb2_autotune")
         return list(out)
+
+    def block_batch_advance(self, cases, max_steps, stream=None):
+        """Advance a ctypes array of abi.BlockCase in one persistent launch (cb2_block_batch_advance)."""
+        check(self.lib.cb2_block_batch_advance(self.h, C.cast(cases, C.c_void_p), len(cases), max_steps, stream),
+              "cb2_block_batch_advance")
+
+    def block_batch_autotune(self, cases, stream=None):
+        ni = C.c_int(0)
+        check(self.lib.cb2_block_batch_autotune(self.h, C.cast(cases, C.c_void_p), len(cases), C.byref(ni), stream),
+              "cb2_block_batch_autotune")
+        return ni.value
+
+    def block_batch_set_tile_width(self, ni):
+        check(self.lib.cb2_block_batch_set_tile_width(self.h, ni), "cb2_block_batch_set_tile_width")
 
     def set_tile_widths(self, blk, widths):
         arr = (C.c_int * 3)(*widths)

@@ -1,5 +1,6 @@
 // extern "C" entry points of libcb200 (declared in include/cb200.h) and the RK3 step
 // orchestration (the stage body of RK3<mix>, src/RK.cuh:107-237).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -8,6 +9,8 @@
 #include "common.cuh"
 #include "launch.h"
 #include "sweep.cuh"
+#include "block_batch.h"
+#include "cb200_serve.h"
 
 namespace cb2 {
 
@@ -108,6 +111,11 @@ struct cb2_ctx {
     unsigned long long launches = 0; // kernels per step inside the graph
   } sg;
   RunState *d_run = nullptr;  // time, t_end, dt, step counter of the graph loop
+  // batched closed blocks (cb2_block_batch_*)
+  BlockCase *d_batch = nullptr;
+  int n_batch = 0;            // capacity of d_batch
+  int *d_queue = nullptr;     // work counter of the persistent batch grid
+  int batch_ni = kNI;         // y/z tile width of the batch kernel (cb2_block_batch_autotune)
 };
 
 namespace cb2 {
@@ -394,6 +402,8 @@ void cb2_destroy(cb2_ctx *ctx) {
   if (ctx->sg.graph) cudaGraphDestroy(ctx->sg.graph);
   if (ctx->sg.capture) cudaStreamDestroy(ctx->sg.capture);
   cudaFree(ctx->d_run);
+  cudaFree(ctx->d_batch);
+  cudaFree(ctx->d_queue);
   for (auto &b : ctx->blocks) {
     cudaFree(b.d_btype);
     cudaFree(b.d_f32);
@@ -920,6 +930,137 @@ int cb2_reactor_advance(cb2_ctx *ctx, cb2_reactor *reactors, int n, int max_atte
   ProfGuard pg(ctx);
   ++ctx->n_launch;
   return launch_reactor_advance(ctx->p, reactors, n, max_attempts, rtol, atol, (cudaStream_t)stream);
+}
+
+}  // extern "C"
+
+// Host records of a batch, largest block first (the persistent grid's work order), in
+// ctx->d_batch; order[pos] is the caller's index of record pos.
+static int build_block_batch(cb2_ctx *ctx, const cb2_block_case *cases, int n, std::vector<BlockCase> &h,
+                             std::vector<int> &order) {
+  const Param &p = ctx->p;
+  const int need_g = p.reconstruction == CB2_REC_WENO7 ? 4 : 3;
+  order.resize(n);
+  for (int i = 0; i < n; ++i) {
+    const cb2_zone_view &v = cases[i].zone;
+    if (v.mx < 1 || v.my < 1 || v.mz < 1 || v.ngg < need_g) return CB2_ERR_INVALID;
+    if (!v.cv || !v.bv || !v.qn || !v.dq || !v.metric || !v.jac || !v.mul) return CB2_ERR_INVALID;
+    if (!(cases[i].dt >= 0.0)) return CB2_ERR_INVALID;
+    if ((long long)(v.mx + 2 * v.ngg) * (v.my + 2 * v.ngg) >= (1LL << 31)) return CB2_ERR_UNSUPPORTED;
+    const int ms[3] = {v.mx, v.my, v.mz};
+    for (int d = 0; d < (v.mz > 1 ? 3 : 2); ++d)
+      if (ms[d] < v.ngg + 2) return CB2_ERR_UNSUPPORTED;  // the periodic pair needs m >= g + 2
+    order[i] = i;
+  }
+  auto work = [&](int i) { return (long long)cases[i].zone.mx * cases[i].zone.my * cases[i].zone.mz; };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
+  if (n > ctx->n_batch) {
+    cudaFree(ctx->d_batch);
+    ctx->d_batch = nullptr;
+    ctx->n_batch = 0;
+    CB2_TRY(check_cuda(cudaMalloc(&ctx->d_batch, sizeof(BlockCase) * n)));
+    ctx->n_batch = n;
+  }
+  if (!ctx->d_queue) CB2_TRY(check_cuda(cudaMalloc(&ctx->d_queue, sizeof(int))));
+  h.assign(n, BlockCase{});
+  for (int pos = 0; pos < n; ++pos) {
+    const cb2_block_case &c = cases[order[pos]];
+    BlockCase &b = h[pos];
+    b.z = make_zone(c.zone);
+    b.p = p;
+    b.p.dim = c.zone.mz == 1 ? 2 : 3;
+    b.p.status = &ctx->d_batch[pos].flags;
+    const int mx = c.zone.mx, my = c.zone.my, mz = c.zone.mz;
+    b.n_pairs = 0;
+    for (int d = 0; d < (mz > 1 ? 3 : 2); ++d) {
+      // the low periodic face of direction d over the whole block (the register_face ranges)
+      FaceBC f{};
+      f.type = CB2_BC_PERIODIC;
+      f.face = d;
+      f.direction = -1;
+      f.end[0] = d == 0 ? 0 : mx - 1;
+      f.end[1] = d == 1 ? 0 : my - 1;
+      f.end[2] = d == 2 ? 0 : mz - 1;
+      b.pairs[b.n_pairs++] = f;
+    }
+    b.time = c.time;
+    b.t_end = c.t_end;
+    b.dt_fixed = c.dt;
+    b.last_dt = 0.0;
+    b.steps = 0;
+    b.status = 0;
+    b.flags = 0u;
+  }
+  return CB2_OK;
+}
+
+extern "C" {
+
+int cb2_block_batch_advance(cb2_ctx *ctx, cb2_block_case *cases, int n, int max_steps, void *stream) {
+  if (!ctx || (n > 0 && !cases) || n < 0 || max_steps < 0) return CB2_ERR_INVALID;
+  if (!block_batch_supported(ctx->p)) return CB2_ERR_UNSUPPORTED;
+  if (n == 0) return CB2_OK;
+  std::vector<BlockCase> h;
+  std::vector<int> order;
+  CB2_TRY(build_block_batch(ctx, cases, n, h, order));
+  ProfGuard pg(ctx);
+  cudaStream_t s = (cudaStream_t)stream;
+  CB2_TRY(check_cuda(cudaMemcpyAsync(ctx->d_batch, h.data(), sizeof(BlockCase) * n, cudaMemcpyHostToDevice, s)));
+  CB2_TRY(launch_block_batch(ctx->d_batch, n, ctx->p, max_steps, 0, ctx->batch_ni, ctx->d_queue, s));
+  ++ctx->n_launch;
+  CB2_TRY(check_cuda(cudaMemcpyAsync(h.data(), ctx->d_batch, sizeof(BlockCase) * n, cudaMemcpyDeviceToHost, s)));
+  CB2_TRY(check_cuda(cudaStreamSynchronize(s)));
+  for (int pos = 0; pos < n; ++pos) {
+    cb2_block_case &c = cases[order[pos]];
+    c.time = h[pos].time;
+    c.last_dt = h[pos].last_dt;
+    c.steps = h[pos].steps;
+    c.status = h[pos].status;
+  }
+  return CB2_OK;
+}
+
+int cb2_block_batch_autotune(cb2_ctx *ctx, cb2_block_case *cases, int n, int *tile_ni_out, void *stream) {
+  if (!ctx || (n > 0 && !cases) || n < 0) return CB2_ERR_INVALID;
+  if (!block_batch_supported(ctx->p)) return CB2_ERR_UNSUPPORTED;
+  if (n > 0) {
+    std::vector<BlockCase> h;
+    std::vector<int> order;
+    CB2_TRY(build_block_batch(ctx, cases, n, h, order));
+    cudaStream_t s = (cudaStream_t)stream;
+    CB2_TRY(check_cuda(cudaMemcpyAsync(ctx->d_batch, h.data(), sizeof(BlockCase) * n, cudaMemcpyHostToDevice, s)));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = check_cuda(cudaEventCreate(&e0));
+    if (rc == CB2_OK) rc = check_cuda(cudaEventCreate(&e1));
+    float best_ms = 1e30f;
+    int best = kNI;
+    for (int c = 0; c < 3 && rc == CB2_OK; ++c) {
+      const int ni = kTileNI[c];
+      rc = launch_block_batch(ctx->d_batch, n, ctx->p, 0, 1, ni, ctx->d_queue, s);  // warm-up
+      if (rc == CB2_OK) rc = check_cuda(cudaEventRecord(e0, s));
+      for (int r = 0; r < 2 && rc == CB2_OK; ++r) rc = launch_block_batch(ctx->d_batch, n, ctx->p, 0, 1, ni, ctx->d_queue, s);
+      if (rc == CB2_OK) rc = check_cuda(cudaEventRecord(e1, s));
+      if (rc == CB2_OK) rc = check_cuda(cudaEventSynchronize(e1));
+      float ms = 0;
+      if (rc == CB2_OK) rc = check_cuda(cudaEventElapsedTime(&ms, e0, e1));
+      if (rc == CB2_OK && ms < best_ms) {
+        best_ms = ms;
+        best = ni;
+      }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (rc != CB2_OK) return rc;
+    ctx->batch_ni = best;
+  }
+  if (tile_ni_out) *tile_ni_out = ctx->batch_ni;
+  return CB2_OK;
+}
+
+int cb2_block_batch_set_tile_width(cb2_ctx *ctx, int tile_ni) {
+  if (!ctx || !(tile_ni == 4 || tile_ni == 8 || tile_ni == 16)) return CB2_ERR_INVALID;
+  ctx->batch_ni = tile_ni;
+  return CB2_OK;
 }
 
 int cb2_read_status(cb2_ctx *ctx, unsigned *flags_out, void *stream) {
