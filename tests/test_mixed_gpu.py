@@ -101,3 +101,63 @@ def test_mixed_sine_wave_l1_density_within_1e6():
     assert abs(e32 - e64) <= 1e-3 * e64, (e32, e64)
     c64.close()
     c32.close()
+
+
+def _h2():
+    import os
+    from cb200 import mech as mechmod
+    return mechmod.load_json(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "h2_li2004.json"))
+
+
+@pytest.mark.parametrize("scheme,rec", [(abi.INV_HLLC, abi.REC_WENO5), (abi.INV_AUSMP, abi.REC_WENO7)],
+                         ids=["hllc_weno5", "ausm_weno7"])
+def test_mixed_mixture_rhs_close_to_fp64_oracle(oracle_lib, scheme, rec):
+    """The H2/air box (9 species): one inviscid right-hand side of the mixed form against the FP64
+    oracle, every variable within RHS_TOL of its largest |dq|."""
+    h2 = _h2()
+    case = cases.h2_air_box(h2, n_nodes=14, scheme=scheme, reconstruction=rec, viscous_order=0, reaction=False)
+    p, hb, faces = case.param, case.blocks[0], case.faces[0]
+    oracle_lib.boundary(p, hb, faces)
+    oracle_lib.properties(p, hb)
+    dev = DeviceBlock(hb)
+    pm = abi.ParamView.from_buffer_copy(p)
+    pm.precision = abi.PREC_MIXED
+    ctx = cb200.Context(pm)
+    ctx.bind(0, dev.view(), faces)
+    ctx.rhs(0, mask=abi.RHS_INVISCID)
+    _sync()
+    oracle_lib.rhs(p, hb, faces, mask=abi.RHS_INVISCID)
+    dq = dev.to_host(["dq"])["dq"]
+    ref = hb.a["dq"]
+    per_var = [float(np.abs(dq[v] - ref[v]).max() / max(np.abs(ref[v]).max(), 1e-300)) for v in range(dq.shape[0])]
+    assert np.isfinite(dq).all()
+    assert max(per_var) < RHS_TOL, per_var
+    ctx.close()
+
+
+def test_mixed_reacting_box_steps_stay_physical():
+    """Three mixed-form RK3 steps of the reacting H2/air box (viscous, chemistry) keep every node
+    physical and stay within 1e-6 (L1, relative) of the FP64 path in density and temperature."""
+    import torch
+    h2 = _h2()
+    case = cases.h2_air_box(h2, n_nodes=24, scheme=abi.INV_HLLC, reconstruction=abi.REC_WENO5, viscous_order=2,
+                            reaction=True)
+    p, hb, faces = case.param, case.blocks[0], case.faces[0]
+    res = {}
+    for name, prec in (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED)):
+        dev = DeviceBlock(hb)
+        pv = abi.ParamView.from_buffer_copy(p)
+        pv.precision = prec
+        ctx = cb200.Context(pv)
+        ctx.bind(0, dev.view(), faces)
+        ctx.properties(0)
+        for _ in range(3):
+            ctx.rk3_step(2e-9, True)
+        _sync()
+        assert ctx.read_status() == 0, name
+        res[name] = dev.to_host(["bv"])["bv"]
+        ctx.close()
+    g = hb.ngg
+    for c in (0, 5):
+        a, b = res["mixed"][c, g:-g, g:-g, g:-g], res["fp64"][c, g:-g, g:-g, g:-g]
+        assert np.abs(a - b).mean() / np.abs(b).mean() < 1e-6, c
