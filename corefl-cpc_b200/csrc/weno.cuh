@@ -122,9 +122,13 @@ __device__ __forceinline__ T weno7_minus(const T *v, T eps, bool shock) {
 
 // FP32 weights.  The single-division product form needs the product of three or four
 // (eps + beta)^2 terms, which FP32 cannot hold across the dynamic range of a discontinuity.  The
-// FP32 path normalises by the smallest term instead: with r_s = D_min / D_s in (0, 1],
-//   WENO-JS  alpha_s ~ c_s r_s,   WENO-Z  alpha_s ~ c_s (D_min + tau r_s),
-// the same weights up to a common factor, every term bounded by c_s (D_min + tau).
+// FP32 path normalises by the smallest term instead, and takes every ratio before squaring so
+// that nothing underflows: with A_s = eps + beta_s (D_s = A_s^2), q_s = (A_min / A_s)^2 in (0, 1],
+// T = |b0 + 3 b1 - 3 b2 - b3| (tau = T^2) and t = 1 / (1 + (A_min / T)^2) = tau / (D_min + tau),
+//   WENO-JS  alpha_s ~ c_s q_s,   WENO-Z  alpha_s ~ c_s ((1 - t) + t q_s),
+// the same weights up to a common factor, every term bounded by c_s.  (The square of a small A_s,
+// e.g. eps + 0 for a uniform density of 0.3, is below the smallest normal FP32 number, and the
+// paired FP32 instructions flush such results to zero.)
 __device__ __forceinline__ float rcp32(float x) { return __frcp_rn(x); }
 
 // ---- node-centred pair ---------------------------------------------------------------
@@ -150,8 +154,9 @@ __device__ __forceinline__ void weno5_node(const T *v, T eps, T &lp, T &rm) {
   T D0 = sq(eps + b0), D1 = sq(eps + b1), D2 = sq(eps + b2);
   T E0, E1, E2;  // weights of the sub-stencils up to a common factor
   if constexpr (sizeof(T) == 4) {
-    const T Dm = fmin(fmin(D0, D1), D2);
-    E0 = Dm * rcp32(D0); E1 = Dm * rcp32(D1); E2 = Dm * rcp32(D2);
+    const T A0 = eps + b0, A1 = eps + b1, A2 = eps + b2;
+    const T Am = fmin(fmin(A0, A1), A2);
+    E0 = sq(Am * rcp32(A0)); E1 = sq(Am * rcp32(A1)); E2 = sq(Am * rcp32(A2));
   } else {
     const T sc = binade_inv(fmax(fmax(D0, D1), D2));
     D0 *= sc; D1 *= sc; D2 *= sc;
@@ -187,9 +192,12 @@ __device__ __forceinline__ void weno7_node(const T *u, T eps, T &lp, T &rm) {
   T D0 = sq(eps + b0), D1 = sq(eps + b1), D2 = sq(eps + b2), D3 = sq(eps + b3);
   T E0, E1, E2, E3;  // Z weights of the sub-stencils up to a common factor
   if constexpr (sizeof(T) == 4) {
-    const T Dm = fmin(fmin(D0, D1), fmin(D2, D3));
-    E0 = Dm + tau * (Dm * rcp32(D0)); E1 = Dm + tau * (Dm * rcp32(D1));
-    E2 = Dm + tau * (Dm * rcp32(D2)); E3 = Dm + tau * (Dm * rcp32(D3));
+    const T A0 = eps + b0, A1 = eps + b1, A2 = eps + b2, A3 = eps + b3;
+    const T Am = fmin(fmin(A0, A1), fmin(A2, A3));
+    const T rz = Am * rcp32(fabs(b0 + 3 * b1 - 3 * b2 - b3));
+    const T t = rcp32(1 + rz * rz), u = 1 - t;
+    E0 = u + t * sq(Am * rcp32(A0)); E1 = u + t * sq(Am * rcp32(A1));
+    E2 = u + t * sq(Am * rcp32(A2)); E3 = u + t * sq(Am * rcp32(A3));
   } else {
     const T sc = binade_inv(fmax(fmax(D0, D1), fmax(D2, D3)));
     D0 *= sc; D1 *= sc; D2 *= sc; D3 *= sc; tau *= sc;
@@ -242,11 +250,12 @@ __device__ __forceinline__ void weno5_node_x2(const float *v, float eps, float &
   const float2 B0 = fma2(p2(13.0f / 12), mul2(e0, e0), mul2(p2(0.25f), mul2(f0, f0)));  // (b0, b2)
   const float e1 = v[1] + v[3] - 2 * v[2], f1 = v[1] - v[3];
   const float b1 = 13.0f / 12 * (e1 * e1) + 0.25f * (f1 * f1);
-  const float2 DA = mul2(add2(p2(eps), B0), add2(p2(eps), B0));  // (D0, D2)
-  const float D1 = (eps + b1) * (eps + b1);
-  const float Dm = fminf(fminf(DA.x, DA.y), D1);
-  const float2 EA = mul2(p2(Dm), rcp2(DA));  // (E0, E2)
-  const float E1 = Dm * rcp32(D1);
+  const float2 AA = add2(p2(eps), B0);  // (A0, A2)
+  const float A1 = eps + b1;
+  const float Am = fminf(fminf(AA.x, AA.y), A1);
+  const float2 RA = mul2(p2(Am), rcp2(AA));
+  const float2 EA = mul2(RA, RA);  // (E0, E2)
+  const float R1 = Am * rcp32(A1), E1 = R1 * R1;
   const float2 W0 = mul2(p2(0.1f), EA), W1 = p2(0.6f * E1), W2 = mul2(p2(0.3f), swap2(EA));
   const float2 num = fma2(W2, Q2, fma2(W1, Q1, mul2(W0, Q0)));
   const float2 den = add2(add2(W0, W1), W2);
@@ -269,13 +278,14 @@ __device__ __forceinline__ void weno7_node_x2(const float *u, float eps, float &
   const float2 B1 = beta7_x2(lin4(k6, U[1], -6 * k6, U[2], 3 * k6, U[3], 2 * k6, U[4]), lin3(1, U[2], -2, U[3], 1, U[4]),
                              lin4(-1, U[1], 3, U[2], -3, U[3], 1, U[4]));
   // plus side: b0 = B0.x, b1 = B1.x, b2 = B1.y, b3 = B0.y
-  const float t = (B0.x - B0.y) + 3 * (B1.x - B1.y);
-  const float tau = t * t;  // unchanged by the mirroring
-  const float2 A0 = add2(p2(eps), B0), A1 = add2(p2(eps), B1);
-  const float2 DA = mul2(A0, A0), DB = mul2(A1, A1);  // (D0, D3), (D1, D2)
-  const float Dm = fminf(fminf(DA.x, DA.y), fminf(DB.x, DB.y));
-  const float2 EA = fma2(p2(tau), mul2(p2(Dm), rcp2(DA)), p2(Dm));  // (E0, E3)
-  const float2 EB = fma2(p2(tau), mul2(p2(Dm), rcp2(DB)), p2(Dm));  // (E1, E2)
+  const float2 A0 = add2(p2(eps), B0), A1 = add2(p2(eps), B1);  // (A0, A3), (A1, A2)
+  const float Am = fminf(fminf(A0.x, A0.y), fminf(A1.x, A1.y));
+  const float2 R0 = mul2(p2(Am), rcp2(A0)), R1 = mul2(p2(Am), rcp2(A1));
+  // t = tau / (D_min + tau), tau unchanged by the mirroring; T = 0 gives rz = inf and t = 0
+  const float rz = Am * rcp32(fabsf((B0.x - B0.y) + 3 * (B1.x - B1.y)));
+  const float t = rcp32(1.0f + rz * rz);
+  const float2 EA = fma2(p2(t), mul2(R0, R0), p2(1.0f - t));  // (E0, E3)
+  const float2 EB = fma2(p2(t), mul2(R1, R1), p2(1.0f - t));  // (E1, E2)
   const float2 W0 = mul2(p2(1.0f / 35), EA), W1 = mul2(p2(12.0f / 35), EB);
   const float2 W2 = mul2(p2(18.0f / 35), swap2(EB)), W3 = mul2(p2(4.0f / 35), swap2(EA));
   const float2 num = fma2(W3, Q3, fma2(W2, Q2, fma2(W1, Q1, mul2(W0, Q0))));
