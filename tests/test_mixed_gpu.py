@@ -115,7 +115,8 @@ def test_mixed_mixture_rhs_close_to_fp64_oracle(oracle_lib, scheme, rec):
     """The H2/air box (9 species): one inviscid right-hand side of the mixed form against the FP64
     oracle, every variable within RHS_TOL of its largest |dq|."""
     h2 = _h2()
-    case = cases.h2_air_box(h2, n_nodes=14, scheme=scheme, reconstruction=rec, viscous_order=0, reaction=False)
+    case = cases.h2_air_box(h2, n_nodes=14, ngg=4 if rec == abi.REC_WENO7 else 3, scheme=scheme, reconstruction=rec,
+                            viscous_order=0, reaction=False)
     p, hb, faces = case.param, case.blocks[0], case.faces[0]
     oracle_lib.boundary(p, hb, faces)
     oracle_lib.properties(p, hb)
