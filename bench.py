@@ -306,26 +306,61 @@ def gpu_arm(args, rank, world, local_rank):
         out_cv = torch.empty_like(pin["cv"]).pin_memory()
         h2d = sum(t.numel() * 8 for t in pin.values())
         d2h = out_cv.numel() * 8
-        k_e2e = max(1, min(args.steps, 5))
+        k_e2e = max(1, min(args.steps, 10))
+        # Every step copies its input state in from pinned host memory and its result out, as a
+        # caller holding the state on the host would.  The transfers run on their own streams,
+        # double-buffered through device staging arrays, so step k+1's input crosses PCIe while
+        # step k computes and step k-1's result crosses back.
+        s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+        stage = {n: torch.empty_like(dev.t[n]) for n in ("cv", "bv")}
+        outs = [torch.empty_like(dev.t["cv"]) for _ in range(2)]
+        ev = lambda: torch.cuda.Event()  # noqa: E731
+        ev_in = [ev() for _ in range(k_e2e)]
+        ev_staged = [ev() for _ in range(k_e2e)]
+        ev_done = [ev() for _ in range(k_e2e)]
+        ev_out = [ev() for _ in range(k_e2e)]
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
         e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e2.record(stream)
-        for _ in range(k_e2e):
-            dev.t["cv"].copy_(pin["cv"], non_blocking=True)
-            dev.t["bv"].copy_(pin["bv"], non_blocking=True)
+        e2.record(s_in)
+        with torch.cuda.stream(s_in):
+            for n in ("cv", "bv"):
+                stage[n].copy_(pin[n], non_blocking=True)
+            ev_in[0].record(s_in)
+        for k in range(k_e2e):
+            stream.wait_event(ev_in[k])
+            for n in ("cv", "bv"):
+                dev.t[n].copy_(stage[n])
+            ev_staged[k].record(stream)
+            if k + 1 < k_e2e:
+                s_in.wait_event(ev_staged[k])
+                with torch.cuda.stream(s_in):
+                    for n in ("cv", "bv"):
+                        stage[n].copy_(pin[n], non_blocking=True)
+                    ev_in[k + 1].record(s_in)
             ctx.rk3_step(dt, True, sh)
-            out_cv.copy_(dev.t["cv"], non_blocking=True)
-        e3.record(stream)
+            if k >= 2:
+                stream.wait_event(ev_out[k - 2])  # the transfer that last read this buffer
+            outs[k % 2].copy_(dev.t["cv"])
+            ev_done[k].record(stream)
+            s_out.wait_event(ev_done[k])
+            with torch.cuda.stream(s_out):
+                out_cv.copy_(outs[k % 2], non_blocking=True)
+                ev_out[k].record(s_out)
+        s_out.wait_event(ev_done[k_e2e - 1])
+        e3.record(s_out)
         torch.cuda.synchronize()
         ms_e = e2.elapsed_time(e3)
+        del stage, outs
         if dist:
             t = torch.tensor([ms_e], device=f"cuda:{local_rank}")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms_e = float(t.item())
         e2e = {"value": world * nodes * k_e2e / (ms_e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "steps": k_e2e, "ms_per_step": ms_e / k_e2e}
+               "d2h_bytes_per_step": d2h, "steps": k_e2e, "ms_per_step": ms_e / k_e2e,
+               "transfers": "pinned host state in and result out every step, on their own streams, "
+                            "overlapped with the neighbouring steps' compute"}
 
     mixed = None
     if not args.no_mixed:
