@@ -99,7 +99,7 @@ __device__ __forceinline__ void state_energy(T *pv, const Mech &m) {
   constexpr int NV = 5 + NS;
   const T ek = T(0.5) * (pv[1] * pv[1] + pv[2] * pv[2] + pv[3] * pv[3]);
   if constexpr (NS == 0) {
-    pv[NV] = ek * pv[0] + pv[4] / T(kGammaAir - 1);
+    pv[NV] = ek * pv[0] + pv[4] * T(1.0 / (kGammaAir - 1));
     pv[NV + 1] = T(kGammaAir);
   } else {
     double y[NS], r = 0;
@@ -124,15 +124,19 @@ __device__ __forceinline__ void ausm_plus(const T *pl, const T *pr, const T *ml,
   const T k2 = half * (jl * ml[1] + jr * mr[1]);
   const T k3 = half * (jl * ml[2] + jr * mr[2]);
   const T gk = sqrt(k1 * k1 + k2 * k2 + k3 * k3);
-  const T ul = (k1 * pl[1] + k2 * pl[2] + k3 * pl[3]) / gk;
-  const T ur = (k1 * pr[1] + k2 * pr[2] + k3 * pr[3]) / gk;
+  // one reciprocal each for |grad xi| and c instead of two divisions
+  const T igk = T(1) / gk;
+  const T ul = (k1 * pl[1] + k2 * pl[2] + k3 * pl[3]) * igk;
+  const T ur = (k1 * pr[1] + k2 * pr[2] + k3 * pr[3]) * igk;
   const T c = half * (sqrt(pl[NV + 1] * pl[4] / pl[0]) + sqrt(pr[NV + 1] * pr[4] / pr[0]));
-  const T Ml = ul / c, Mr = ur / c;
+  const T ic = T(1) / c;
+  const T Ml = ul * ic, Mr = ur * ic;
   const T alpha = T(3 / 16.0);
   T mlp, plp, mrn, prn;
+  // supersonic: M+ = (M + |M|)/2 and P+ = M+/M, which is exactly 1 (M > 1) or 0 (M < -1)
   if (fabs(Ml) > 1) {
     mlp = half * (Ml + fabs(Ml));
-    plp = mlp / Ml;
+    plp = Ml > 0 ? T(1) : T(0);
   } else {
     const T a = (Ml + 1) * (Ml + 1) * T(0.25), b = (Ml * Ml - 1) * (Ml * Ml - 1);
     mlp = a + T(0.125) * b;
@@ -140,7 +144,7 @@ __device__ __forceinline__ void ausm_plus(const T *pl, const T *pr, const T *ml,
   }
   if (fabs(Mr) > 1) {
     mrn = half * (Mr - fabs(Mr));
-    prn = mrn / Mr;
+    prn = Mr < 0 ? T(1) : T(0);
   } else {
     const T a = (Mr - 1) * (Mr - 1) * T(0.25), b = (Mr * Mr - 1) * (Mr * Mr - 1);
     mrn = -a - T(0.125) * b;
@@ -166,7 +170,8 @@ __device__ __forceinline__ void hllc(const T *pl, const T *pr, const T *ml, cons
   constexpr int NV = 5 + NS;
   const T half = T(0.5);
   const T sl0 = sqrt(pl[0]), sr0 = sqrt(pr[0]);
-  const T rlc = sl0 / (sl0 + sr0), rrc = sr0 / (sl0 + sr0);
+  const T isum = T(1) / (sl0 + sr0);
+  const T rlc = sl0 * isum, rrc = sr0 * isum;
   const T ut = pl[1] * rlc + pr[1] * rrc, vt = pl[2] * rlc + pr[2] * rrc, wt = pl[3] * rlc + pr[3] * rrc;
   T ct;
   if constexpr (NS == 0) {
@@ -188,11 +193,13 @@ __device__ __forceinline__ void hllc(const T *pl, const T *pr, const T *ml, cons
   }
   const T kx = half * (ml[0] + mr[0]), ky = half * (ml[1] + mr[1]), kz = half * (ml[2] + mr[2]);
   const T gk = sqrt(kx * kx + ky * ky + kz * kz);
-  const T Ut = (kx * ut + ky * vt + kz * wt) / gk;
+  const T igk = T(1) / gk;
+  const T Ut = (kx * ut + ky * vt + kz * wt) * igk;
   const T ja = half * (jl + jr);
   const T Ul = kx * pl[1] + ky * pl[2] + kz * pl[3];
   const T cl = sqrt(pl[NV + 1] * pl[4] / pl[0]);
-  const T sl = fmin(Ul / gk - cl, Ut - ct);
+  const T Uln = Ul * igk;  // normal velocities
+  const T sl = fmin(Uln - cl, Ut - ct);
   if (sl >= 0) {
     const T rU = pl[0] * Ul;
     fc[0] = ja * rU;
@@ -206,7 +213,8 @@ __device__ __forceinline__ void hllc(const T *pl, const T *pr, const T *ml, cons
   }
   const T Ur = kx * pr[1] + ky * pr[2] + kz * pr[3];
   const T cr = sqrt(pr[NV + 1] * pr[4] / pr[0]);
-  const T sr = fmax(Ur / gk + cr, Ut + ct);
+  const T Urn = Ur * igk;
+  const T sr = fmax(Urn + cr, Ut + ct);
   if (sr < 0) {
     const T rU = pr[0] * Ur;
     fc[0] = ja * rU;
@@ -218,9 +226,9 @@ __device__ __forceinline__ void hllc(const T *pl, const T *pr, const T *ml, cons
     for (int l = 5; l < NV; ++l) fc[l] = ja * rU * pr[l];
     return;
   }
-  const T sm = ((pr[0] * Ur * (sr - Ur / gk) - pl[0] * Ul * (sl - Ul / gk)) / gk + pl[4] - pr[4]) /
-               (pr[0] * (sr - Ur / gk) - pl[0] * (sl - Ul / gk));
-  const T pm = pl[0] * (sl - Ul / gk) * (sm - Ul / gk) + pl[4];
+  const T sm = ((pr[0] * Ur * (sr - Urn) - pl[0] * Ul * (sl - Uln)) * igk + pl[4] - pr[4]) /
+               (pr[0] * (sr - Urn) - pl[0] * (sl - Uln));
+  const T pm = pl[0] * (sl - Uln) * (sm - Uln) + pl[4];
   const bool left = sm >= 0;
   const T *ps = left ? pl : pr;
   const T ss = left ? sl : sr, Us = left ? Ul : Ur;
