@@ -84,6 +84,9 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
     ap.add_argument("--no-serve", action="store_true", help="skip the served reactor/shock-tube workload")
     ap.add_argument("--no-reacting", action="store_true", help="skip the reacting H2/air box")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-blocks form")
+    ap.add_argument("--batch-blocks", type=int, default=296, help="blocks of the batched-blocks form")
+    ap.add_argument("--batch-steps", type=int, default=5, help="steps of the batched-blocks form")
     ap.add_argument("--reacting-n", type=int, default=192, help="nodes per side of the reacting H2/air box")
     ap.add_argument("--reacting-steps", type=int, default=5, help="timed steps of the reacting H2/air box")
     ap.add_argument("--serve-seconds", type=float, default=0.05,
@@ -370,6 +373,7 @@ def gpu_arm(args, rank, world, local_rank):
     del dev, xyz
     torch.cuda.empty_cache()
     reacting = None if args.no_reacting else reacting_box(args, local_rank)
+    batched = None if args.no_batch else batched_blocks(args, local_rank)
     served = None if args.no_serve else serve_workload(args)
     if dist:
         dist.barrier()
@@ -390,6 +394,7 @@ def gpu_arm(args, rank, world, local_rank):
                        "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
             "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
             "clocks": clocks, "status_flags": status, "mixed": mixed, "serve": served, "reacting_box": reacting,
+            "batched_blocks": batched,
             "kernel_ms_per_step": {k: v[1] for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
             "kernel_rooflines": kernel_roofs}
     print(json.dumps(line), flush=True)
@@ -531,6 +536,70 @@ def reacting_box(args, local_rank):
                      "kernel_ms_per_step": {k: v[1] for k, v in top}}
     out["speedup_mixed_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
     del dev, init
+    torch.cuda.empty_cache()
+    return out
+
+
+def batched_blocks(args, local_rank):
+    """Batched form: --batch-blocks closed periodic sine-wave blocks (WENO7 + AUSM+, inviscid,
+    FP64) of seeded uneven sizes n^3 nodes, n ~ U{12..40}, advanced --batch-steps CFL steps
+    (a) in one persistent launch (cb2_block_batch_advance, tile width tuned first) and (b) one
+    block after another through cb2_rk3_step, each from the same initial states.  Wall clock
+    around each form (the batch call synchronises; the loop ends with a synchronise)."""
+    import numpy as np
+    import torch
+    import cb200
+    from cb200 import abi, cases
+    from cb200.field import DeviceBlock
+    rng = np.random.default_rng(2027)
+    sizes = rng.integers(12, 41, args.batch_blocks)
+    blocks = []
+    for n in sizes:
+        c = cases.sine_wave(n=int(n) - 1, viscous_order=0)
+        blocks.append((c.param, c.blocks[0], c.faces[0]))
+    p0 = blocks[0][0]
+    nodes = int(sum(int(n) ** 3 for n in sizes))
+    S = args.batch_steps
+    out = {"workload": f"{args.batch_blocks} periodic sine-wave blocks of n^3 nodes, n ~ U{{12..40}} (seeded), "
+                       f"WENO7 + AUSM+, inviscid, CFL 0.5 steps, FP64", "blocks": args.batch_blocks,
+           "nodes": nodes, "steps": S}
+    # (a) one persistent launch
+    devs = [DeviceBlock(hb, device=f"cuda:{local_rank}") for _, hb, _ in blocks]
+    ctx = cb200.Context(p0)
+    cs = (abi.BlockCase * len(blocks))()
+    for c, d in zip(cs, devs):
+        c.zone = d.view()
+        c.time, c.t_end, c.dt = 0.0, 1e30, 0.0
+    out["tile_width"] = ctx.block_batch_autotune(cs)
+    for d, (_, hb, _) in zip(devs, blocks):
+        d.load(hb, ["cv", "bv"])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ctx.block_batch_advance(cs, S)
+    t_batch = time.perf_counter() - t0
+    failed = sum(1 for c in cs if c.status & abi.BLOCK_FAILED)
+    ctx.close()
+    # (b) the same blocks one by one through the block path
+    for d, (_, hb, _) in zip(devs, blocks):
+        d.load(hb, ["cv", "bv"])
+    ctxs = []
+    for (p, _, faces), d in zip(blocks, devs):
+        cx = cb200.Context(p)
+        cx.bind(0, d.view(), faces)
+        ctxs.append(cx)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for cx in ctxs:
+        for _ in range(S):
+            cx.rk3_step(0.0, fixed_dt=False)
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    for cx in ctxs:
+        cx.close()
+    out["batched"] = {"value": nodes * S / t_batch, "unit": UNIT, "seconds": t_batch, "failed_blocks": failed}
+    out["one_by_one"] = {"value": nodes * S / t_seq, "unit": UNIT, "seconds": t_seq}
+    out["speedup_batched"] = t_seq / t_batch
+    del devs
     torch.cuda.empty_cache()
     return out
 

@@ -25,6 +25,13 @@
 
 namespace cb2 {
 
+// A product rounded on its own (never fused into a following add).  The reciprocal-times
+// products below feed sums; pinning their rounding keeps every kernel that inlines these solvers
+// (the block sweeps, the batched kernels) bitwise identical.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+
+
 template <typename T>
 __device__ __forceinline__ T sgn1(T a) { return a < 0 ? T(-1) : T(1); }
 template <typename T>
@@ -99,7 +106,7 @@ __device__ __forceinline__ void state_energy(T *pv, const Mech &m) {
   constexpr int NV = 5 + NS;
   const T ek = T(0.5) * (pv[1] * pv[1] + pv[2] * pv[2] + pv[3] * pv[3]);
   if constexpr (NS == 0) {
-    pv[NV] = ek * pv[0] + pv[4] * T(1.0 / (kGammaAir - 1));
+    pv[NV] = ek * pv[0] + mul_rn(pv[4], T(1.0 / (kGammaAir - 1)));
     pv[NV + 1] = T(kGammaAir);
   } else {
     double y[NS], r = 0;
@@ -126,11 +133,11 @@ __device__ __forceinline__ void ausm_plus(const T *pl, const T *pr, const T *ml,
   const T gk = sqrt(k1 * k1 + k2 * k2 + k3 * k3);
   // one reciprocal each for |grad xi| and c instead of two divisions
   const T igk = T(1) / gk;
-  const T ul = (k1 * pl[1] + k2 * pl[2] + k3 * pl[3]) * igk;
-  const T ur = (k1 * pr[1] + k2 * pr[2] + k3 * pr[3]) * igk;
+  const T ul = mul_rn(k1 * pl[1] + k2 * pl[2] + k3 * pl[3], igk);
+  const T ur = mul_rn(k1 * pr[1] + k2 * pr[2] + k3 * pr[3], igk);
   const T c = half * (sqrt(pl[NV + 1] * pl[4] / pl[0]) + sqrt(pr[NV + 1] * pr[4] / pr[0]));
   const T ic = T(1) / c;
-  const T Ml = ul * ic, Mr = ur * ic;
+  const T Ml = mul_rn(ul, ic), Mr = mul_rn(ur, ic);
   const T alpha = T(3 / 16.0);
   T mlp, plp, mrn, prn;
   // supersonic: M+ = (M + |M|)/2 and P+ = M+/M, which is exactly 1 (M > 1) or 0 (M < -1)
@@ -171,7 +178,7 @@ __device__ __forceinline__ void hllc(const T *pl, const T *pr, const T *ml, cons
   const T half = T(0.5);
   const T sl0 = sqrt(pl[0]), sr0 = sqrt(pr[0]);
   const T isum = T(1) / (sl0 + sr0);
-  const T rlc = sl0 * isum, rrc = sr0 * isum;
+  const T rlc = mul_rn(sl0, isum), rrc = mul_rn(sr0, isum);
   const T ut = pl[1] * rlc + pr[1] * rrc, vt = pl[2] * rlc + pr[2] * rrc, wt = pl[3] * rlc + pr[3] * rrc;
   T ct;
   if constexpr (NS == 0) {
@@ -194,11 +201,11 @@ __device__ __forceinline__ void hllc(const T *pl, const T *pr, const T *ml, cons
   const T kx = half * (ml[0] + mr[0]), ky = half * (ml[1] + mr[1]), kz = half * (ml[2] + mr[2]);
   const T gk = sqrt(kx * kx + ky * ky + kz * kz);
   const T igk = T(1) / gk;
-  const T Ut = (kx * ut + ky * vt + kz * wt) * igk;
+  const T Ut = mul_rn(kx * ut + ky * vt + kz * wt, igk);
   const T ja = half * (jl + jr);
   const T Ul = kx * pl[1] + ky * pl[2] + kz * pl[3];
   const T cl = sqrt(pl[NV + 1] * pl[4] / pl[0]);
-  const T Uln = Ul * igk;  // normal velocities
+  const T Uln = mul_rn(Ul, igk);  // normal velocities
   const T sl = fmin(Uln - cl, Ut - ct);
   if (sl >= 0) {
     const T rU = pl[0] * Ul;
@@ -213,7 +220,7 @@ __device__ __forceinline__ void hllc(const T *pl, const T *pr, const T *ml, cons
   }
   const T Ur = kx * pr[1] + ky * pr[2] + kz * pr[3];
   const T cr = sqrt(pr[NV + 1] * pr[4] / pr[0]);
-  const T Urn = Ur * igk;
+  const T Urn = mul_rn(Ur, igk);
   const T sr = fmax(Urn + cr, Ut + ct);
   if (sr < 0) {
     const T rU = pr[0] * Ur;
@@ -226,7 +233,7 @@ __device__ __forceinline__ void hllc(const T *pl, const T *pr, const T *ml, cons
     for (int l = 5; l < NV; ++l) fc[l] = ja * rU * pr[l];
     return;
   }
-  const T sm = ((pr[0] * Ur * (sr - Urn) - pl[0] * Ul * (sl - Uln)) * igk + pl[4] - pr[4]) /
+  const T sm = (mul_rn(pr[0] * Ur * (sr - Urn) - pl[0] * Ul * (sl - Uln), igk) + pl[4] - pr[4]) /
                (pr[0] * (sr - Urn) - pl[0] * (sl - Uln));
   const T pm = pl[0] * (sl - Uln) * (sm - Uln) + pl[4];
   const bool left = sm >= 0;
