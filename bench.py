@@ -543,7 +543,7 @@ def reacting_box(args, local_rank):
 def batched_blocks(args, local_rank):
     """Batched form: --batch-blocks closed periodic sine-wave blocks (WENO7 + AUSM+, inviscid,
     FP64) of seeded uneven sizes n^3 nodes, n ~ U{12..40}, advanced --batch-steps CFL steps
-    (a) in one persistent launch (cb2_block_batch_advance, tile width tuned first) and (b) one
+    (a) in one persistent launch (cb2_block_batch_advance, tile width and cluster size tuned first) and (b) one
     block after another through cb2_rk3_step, each from the same initial states.  Wall clock
     around each form (the batch call synchronises; the loop ends with a synchronise)."""
     import numpy as np
@@ -570,7 +570,8 @@ def batched_blocks(args, local_rank):
     for c, d in zip(cs, devs):
         c.zone = d.view()
         c.time, c.t_end, c.dt = 0.0, 1e30, 0.0
-    out["tile_width"] = ctx.block_batch_autotune(cs)
+    ni, cl = ctx.block_batch_autotune(cs)
+    out["schedule"] = {"tile_width": ni, "cluster_ctas": cl}
     for d, (_, hb, _) in zip(devs, blocks):
         d.load(hb, ["cv", "bv"])
     torch.cuda.synchronize()

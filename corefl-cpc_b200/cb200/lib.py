@@ -45,7 +45,7 @@ def load():
         "cb2_autotune": (C.c_int, [vp, C.c_int, P(C.c_int), vp]),
         "cb2_block_batch_advance": (C.c_int, [vp, vp, C.c_int, C.c_int, vp]),
         "cb2_block_batch_autotune": (C.c_int, [vp, vp, C.c_int, P(C.c_int), vp]),
-        "cb2_block_batch_set_tile_width": (C.c_int, [vp, C.c_int]),
+        "cb2_block_batch_set_schedule": (C.c_int, [vp, C.c_int, C.c_int]),
         "cb2_set_tile_widths": (C.c_int, [vp, C.c_int, P(C.c_int)]),
         "cb2_properties": (C.c_int, [vp, C.c_int, vp]),
         "cb2_cv_from_bv": (C.c_int, [vp, C.c_int, vp]),
@@ -115,13 +115,14 @@ class Context:
               "cb2_block_batch_advance")
 
     def block_batch_autotune(self, cases, stream=None):
-        ni = C.c_int(0)
-        check(self.lib.cb2_block_batch_autotune(self.h, C.cast(cases, C.c_void_p), len(cases), C.byref(ni), stream),
+        """(tile width, cluster size) picked by timing the batch's residual phase."""
+        out = (C.c_int * 2)()
+        check(self.lib.cb2_block_batch_autotune(self.h, C.cast(cases, C.c_void_p), len(cases), out, stream),
               "cb2_block_batch_autotune")
-        return ni.value
+        return out[0], out[1]
 
-    def block_batch_set_tile_width(self, ni):
-        check(self.lib.cb2_block_batch_set_tile_width(self.h, ni), "cb2_block_batch_set_tile_width")
+    def block_batch_set_schedule(self, ni, cluster):
+        check(self.lib.cb2_block_batch_set_schedule(self.h, ni, cluster), "cb2_block_batch_set_schedule")
 
     def set_tile_widths(self, blk, widths):
         arr = (C.c_int * 3)(*widths)

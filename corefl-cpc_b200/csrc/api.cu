@@ -116,6 +116,7 @@ struct cb2_ctx {
   int n_batch = 0;            // capacity of d_batch
   int *d_queue = nullptr;     // work counter of the persistent batch grid
   int batch_ni = kNI;         // y/z tile width of the batch kernel (cb2_block_batch_autotune)
+  int batch_cs = 8;           // CTAs per thread-block cluster sharing one batched block
 };
 
 namespace cb2 {
@@ -1006,7 +1007,7 @@ int cb2_block_batch_advance(cb2_ctx *ctx, cb2_block_case *cases, int n, int max_
   ProfGuard pg(ctx);
   cudaStream_t s = (cudaStream_t)stream;
   CB2_TRY(check_cuda(cudaMemcpyAsync(ctx->d_batch, h.data(), sizeof(BlockCase) * n, cudaMemcpyHostToDevice, s)));
-  CB2_TRY(launch_block_batch(ctx->d_batch, n, ctx->p, max_steps, 0, ctx->batch_ni, ctx->d_queue, s));
+  CB2_TRY(launch_block_batch(ctx->d_batch, n, ctx->p, max_steps, 0, ctx->batch_ni, ctx->batch_cs, ctx->d_queue, s));
   ++ctx->n_launch;
   CB2_TRY(check_cuda(cudaMemcpyAsync(h.data(), ctx->d_batch, sizeof(BlockCase) * n, cudaMemcpyDeviceToHost, s)));
   CB2_TRY(check_cuda(cudaStreamSynchronize(s)));
@@ -1033,33 +1034,43 @@ int cb2_block_batch_autotune(cb2_ctx *ctx, cb2_block_case *cases, int n, int *ti
     int rc = check_cuda(cudaEventCreate(&e0));
     if (rc == CB2_OK) rc = check_cuda(cudaEventCreate(&e1));
     float best_ms = 1e30f;
-    int best = kNI;
-    for (int c = 0; c < 3 && rc == CB2_OK; ++c) {
-      const int ni = kTileNI[c];
-      rc = launch_block_batch(ctx->d_batch, n, ctx->p, 0, 1, ni, ctx->d_queue, s);  // warm-up
-      if (rc == CB2_OK) rc = check_cuda(cudaEventRecord(e0, s));
-      for (int r = 0; r < 2 && rc == CB2_OK; ++r) rc = launch_block_batch(ctx->d_batch, n, ctx->p, 0, 1, ni, ctx->d_queue, s);
-      if (rc == CB2_OK) rc = check_cuda(cudaEventRecord(e1, s));
-      if (rc == CB2_OK) rc = check_cuda(cudaEventSynchronize(e1));
-      float ms = 0;
-      if (rc == CB2_OK) rc = check_cuda(cudaEventElapsedTime(&ms, e0, e1));
-      if (rc == CB2_OK && ms < best_ms) {
-        best_ms = ms;
-        best = ni;
+    int best = kNI, best_cs = 8;
+    const int cluster[4] = {1, 2, 4, 8};
+    for (int c = 0; c < 3 && rc == CB2_OK; ++c)
+      for (int q = 0; q < 4 && rc == CB2_OK; ++q) {
+        const int ni = kTileNI[c], cs = cluster[q];
+        rc = launch_block_batch(ctx->d_batch, n, ctx->p, 0, 1, ni, cs, ctx->d_queue, s);  // warm-up
+        if (rc == CB2_OK) rc = check_cuda(cudaEventRecord(e0, s));
+        for (int r = 0; r < 2 && rc == CB2_OK; ++r)
+          rc = launch_block_batch(ctx->d_batch, n, ctx->p, 0, 1, ni, cs, ctx->d_queue, s);
+        if (rc == CB2_OK) rc = check_cuda(cudaEventRecord(e1, s));
+        if (rc == CB2_OK) rc = check_cuda(cudaEventSynchronize(e1));
+        float ms = 0;
+        if (rc == CB2_OK) rc = check_cuda(cudaEventElapsedTime(&ms, e0, e1));
+        if (rc == CB2_OK && ms < best_ms) {
+          best_ms = ms;
+          best = ni;
+          best_cs = cs;
+        }
       }
-    }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (rc != CB2_OK) return rc;
     ctx->batch_ni = best;
+    ctx->batch_cs = best_cs;
   }
-  if (tile_ni_out) *tile_ni_out = ctx->batch_ni;
+  if (tile_ni_out) {
+    tile_ni_out[0] = ctx->batch_ni;
+    tile_ni_out[1] = ctx->batch_cs;
+  }
   return CB2_OK;
 }
 
-int cb2_block_batch_set_tile_width(cb2_ctx *ctx, int tile_ni) {
+int cb2_block_batch_set_schedule(cb2_ctx *ctx, int tile_ni, int cluster_ctas) {
   if (!ctx || !(tile_ni == 4 || tile_ni == 8 || tile_ni == 16)) return CB2_ERR_INVALID;
+  if (!(cluster_ctas == 1 || cluster_ctas == 2 || cluster_ctas == 4 || cluster_ctas == 8)) return CB2_ERR_INVALID;
   ctx->batch_ni = tile_ni;
+  ctx->batch_cs = cluster_ctas;
   return CB2_OK;
 }
 

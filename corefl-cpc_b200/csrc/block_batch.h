@@ -18,8 +18,9 @@ struct BlockCase {
 
 bool block_batch_supported(const Param &p);
 // mode 0: advance by up to max_steps steps; mode 1: one residual (dq) of every block, for timing.
-// queue: one device int, the work counter of the persistent grid.
-int launch_block_batch(BlockCase *cases, int n, const Param &p, int max_steps, int mode, int ni, int *queue,
-                       cudaStream_t s);
+// cs: CTAs per thread-block cluster, which shares one block (1..8).  queue: one device int, the
+// work counter of the persistent grid.
+int launch_block_batch(BlockCase *cases, int n, const Param &p, int max_steps, int mode, int ni, int cs,
+                       int *queue, cudaStream_t s);
 
 }  // namespace cb2

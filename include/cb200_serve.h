@@ -119,25 +119,29 @@ typedef struct cb2_block_case {
 #define CB2_BLOCK_FAILED 2 /* a non-finite or non-positive step, or a non-physical state */
 
 /* Advances every block of cases[0..n) (host array) by up to max_steps SSP-RK3 steps, stopping
- * each at its own t_end, in ONE persistent launch: each CTA takes the next block from a work
- * queue ordered by decreasing size (largest first), runs its whole steps (qn copy, dt, three
- * stages of zeroed residual, x/y/z primitive sweeps, stage update, periodic ghost fill,
- * properties) with CTA barriers between the phases, then takes the next block.  The arithmetic
+ * each at its own t_end, in ONE persistent launch: each thread-block cluster takes the next
+ * block from a work queue ordered by decreasing size (largest first), runs its whole steps (qn
+ * copy, dt, three stages of zeroed residual, x/y/z primitive sweeps, stage update, periodic
+ * ghost fill, properties) with the phases' tiles and nodes spread over its CTAs and cluster
+ * barriers between the phases, then takes the next block.  The arithmetic
  * per node is the block path's: a block's results equal cb2_rk3_step on the same block bit for
  * bit and do not depend on the other blocks of the batch.  Built for the air model, inviscid,
  * WENO5/WENO7 primitive reconstruction with AUSM+ or HLLC, FP64; every block needs
- * m >= ngg + 2 nodes along each periodic direction.  The y/z sweep tiles use the width
- * cb2_block_batch_autotune picked for this context (8 until then).  Synchronises `stream`. */
+ * m >= ngg + 2 nodes along each periodic direction.  The y/z sweep tile width and the cluster
+ * size are the ones cb2_block_batch_autotune picked for this context (8 and 8 until then).
+ * Synchronises `stream`. */
 int cb2_block_batch_advance(cb2_ctx *ctx, cb2_block_case *cases, int n, int max_steps, void *stream);
 
 /* Times the batch's residual phase (zeroed dq and the three sweeps of every block, one
- * persistent launch per candidate) for the y/z tile widths 4, 8 and 16 and keeps the fastest
- * for this context's later batches; writes it to *tile_ni_out when not NULL.  Only the blocks'
- * dq (a per-stage scratch) changes.  Synchronises `stream`. */
-int cb2_block_batch_autotune(cb2_ctx *ctx, cb2_block_case *cases, int n, int *tile_ni_out, void *stream);
+ * persistent launch per candidate) for every y/z tile width (4, 8, 16) and cluster size (1, 2,
+ * 4, 8 CTAs per block) and keeps the fastest pair for this context's later batches; writes it
+ * to schedule_out[2] = {tile width, cluster size} when not NULL.  Only the blocks' dq (a
+ * per-stage scratch) changes.  Synchronises `stream`. */
+int cb2_block_batch_autotune(cb2_ctx *ctx, cb2_block_case *cases, int n, int *schedule_out, void *stream);
 
-/* Sets the batch's y/z tile width (4, 8 or 16) directly, e.g. from an earlier tuning run. */
-int cb2_block_batch_set_tile_width(cb2_ctx *ctx, int tile_ni);
+/* Sets the batch's y/z tile width (4, 8 or 16) and cluster size (1, 2, 4 or 8) directly, e.g.
+ * from an earlier tuning run.  Every choice gives the same results bit for bit. */
+int cb2_block_batch_set_schedule(cb2_ctx *ctx, int tile_ni, int cluster_ctas);
 
 #ifdef __cplusplus
 }

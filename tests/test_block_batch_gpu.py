@@ -1,7 +1,7 @@
 """Batched closed blocks (cb2_block_batch_advance): uneven 2-D and 3-D periodic air blocks in one
 persistent launch must give, block by block, the same bits as cb2_rk3_step on that block, with
-fixed and CFL steps, whatever other blocks share the batch and whatever tile width the autotuner
-picks."""
+fixed and CFL steps, whatever other blocks share the batch and whatever tile width and cluster
+size the autotuner picks."""
 import numpy as np
 import pytest
 
@@ -97,12 +97,13 @@ def test_batch_result_independent_of_company_and_tiles(oracle_lib):
     alone, _ = _batch(ctx, blocks[1:2], 3, dt)
     ref = alone[0].to_host(["cv"])["cv"]
     for w in (4, 8, 16):
-        ctx.block_batch_set_tile_width(w)
-        together, cases = _batch(ctx, blocks, 3, dt)
-        assert np.array_equal(together[1].to_host(["cv"])["cv"], ref), w
+        for cs in (1, 2, 4, 8):
+            ctx.block_batch_set_schedule(w, cs)
+            together, cases = _batch(ctx, blocks, 3, dt)
+            assert np.array_equal(together[1].to_host(["cv"])["cv"], ref), (w, cs)
     tune_cases, keep = _cases_for(blocks, dt)
-    ni = ctx.block_batch_autotune(tune_cases)
-    assert ni in (4, 8, 16)
+    ni, cs = ctx.block_batch_autotune(tune_cases)
+    assert ni in (4, 8, 16) and cs in (1, 2, 4, 8)
     # tuning touched only the residual scratch dq
     for (_, hb, _), d in zip(blocks, keep):
         assert np.array_equal(d.to_host(["cv"])["cv"], hb.a["cv"])
