@@ -96,6 +96,9 @@ def parse():
     ap.add_argument("--serve-reactor-t-end", type=float, default=1e-3,
                     help="physical end time of the served 0-D reactors")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="mean arrivals per second")
+    ap.add_argument("--schedule", default=None,
+                    help="use these tile widths instead of timing them: 'NI' for the y/z sweeps and the "
+                         "batch, or 'NI,CS' to also fix the batch's cluster size (e.g. from an earlier run)")
     ap.add_argument("--accuracy-steps", type=int, default=100,
                     help="RK3 steps of the mixed-vs-FP64 accuracy run (the workload's 100 steps)")
     return ap.parse_args()
@@ -222,6 +225,15 @@ def load_traffic():
         return {}
 
 
+def tune_sweeps(ctx, args, stream):
+    """The block's sweep tile widths: timed on the block (cb2_autotune), or fixed by --schedule."""
+    if args.schedule:
+        ni = int(args.schedule.split(",")[0])
+        ctx.set_tile_widths(0, [0, ni, ni])
+        return [0, ni, ni]
+    return ctx.autotune(0, stream)
+
+
 def gpu_arm(args, rank, world, local_rank):
     import torch
     import cb200
@@ -248,7 +260,7 @@ def gpu_arm(args, rank, world, local_rank):
     sh = stream.cuda_stream
     ctx.properties(0, sh)
     dt = ctx.cfl_dt(sh)
-    tile_widths = ctx.autotune(0, sh)  # y/z sweep tile widths, timed on this block
+    tile_widths = tune_sweeps(ctx, args, sh)  # y/z sweep tile widths, timed on this block
     nodes = (args.n + 1) ** 3
 
     for _ in range(args.warmup):
@@ -414,7 +426,7 @@ def mixed_form(args, p, dev, faces, host_state, xyz, dt, ctx64, stream, nodes, w
     pm.precision = abi.PREC_MIXED
     ctx32 = cb200.Context(pm)
     ctx32.bind(0, dev.view(), faces)
-    ctx32.autotune(0, sh)
+    tune_sweeps(ctx32, args, sh)
     dev_init = {n: torch.from_numpy(a).to(dev.t[n].device) for n, a in host_state.items()}
     g = (dev.t["bv"].shape[-1] - int(round(xyz.shape[-1]))) // 2
 
@@ -570,7 +582,12 @@ def batched_blocks(args, local_rank):
     for c, d in zip(cs, devs):
         c.zone = d.view()
         c.time, c.t_end, c.dt = 0.0, 1e30, 0.0
-    ni, cl = ctx.block_batch_autotune(cs)
+    if args.schedule:
+        fixed = [int(v) for v in args.schedule.split(",")]
+        ni, cl = fixed[0], fixed[1] if len(fixed) > 1 else 8
+        ctx.block_batch_set_schedule(ni, cl)
+    else:
+        ni, cl = ctx.block_batch_autotune(cs)
     out["schedule"] = {"tile_width": ni, "cluster_ctas": cl}
     for d, (_, hb, _) in zip(devs, blocks):
         d.load(hb, ["cv", "bv"])

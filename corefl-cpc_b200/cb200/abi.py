@@ -1,7 +1,7 @@
 """ctypes mirror of include/cb200.h (structs and constants)."""
 import ctypes as C
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 OK = 0
 ERR_CUDA, ERR_INVALID, ERR_NONPHYSICAL, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_NOMEM = -1, -2, -3, -4, -5, -6
@@ -40,9 +40,16 @@ MECH_INT = ("reac_type", "rev_type", "stoi_f", "stoi_b", "reac_order")
 MECH_REAC = ("A", "b", "Ea", "A2", "b2", "Ea2", "third_body_coeff", "troe_alpha", "troe_t3", "troe_t1", "troe_t2")
 
 
+MECH_NASA9 = ("temperature_range", "therm_poly_coeff")
+MECH_RT = ("tcf_a", "tcf_b", "tcb_a", "tcb_b")
+
+
 class Mechanism(C.Structure):
     _fields_ = [("n_spec", C.c_int), ("n_reac", C.c_int)] + \
-               [(n, _dp) for n in MECH_DOUBLE] + [(n, _ip) for n in MECH_INT] + [(n, _dp) for n in MECH_REAC]
+               [(n, _dp) for n in MECH_DOUBLE] + [(n, _ip) for n in MECH_INT] + [(n, _dp) for n in MECH_REAC] + \
+               [("therm_nasa_7_9", C.c_int), ("max_range", C.c_int), ("n_temperature_range", _ip)] + \
+               [(n, _dp) for n in MECH_NASA9] + [("two_temperature_reaction_temperature", C.c_int)] + \
+               [(n, _dp) for n in MECH_RT]
 
 
 class TwoTemperature(C.Structure):

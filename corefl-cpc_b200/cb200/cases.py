@@ -319,6 +319,57 @@ def h2_air_box_2t(mech, tt, n_nodes=10, ngg=3, length=1e-3, seed=77, t_ve_ratio=
     return Case("h2_air_box_2t", par, [b], base.faces, {"mech": mech, "two_t": tt, "dx": base.meta["dx"]})
 
 
+def air5_box_2t(mech, tt, n_nodes=10, ngg=3, length=1e-2, seed=91, viscous_order=0, reaction=True,
+                scheme=abi.INV_WENO5_CH, reconstruction=abi.REC_WENO5):
+    """Two-temperature AIR5 periodic box with the post-shock conditions of a Mach-10 body: a
+    uniform n_nodes^3 grid with sides L, random-phase velocity (u_rms = 400 m/s), T = 6000 K +
+    three 2500 K Gaussian spots, T_ve = 0.45 T + 600 K (vibration lagging), p = 20 kPa, and
+    partly dissociated air (N2 0.70, O2 0.10, NO 0.05, N 0.05, O 0.10 by mass, +-30 % seeded
+    noise, renormalised).  bv, sv, T_ve and the geometry are set; cv and e_ve are left to a
+    cv-from-bv pass."""
+    m = n_nodes
+    nper = m - 1
+    dx = length / nper
+    ns = mech.ns
+    specs = array_specs(m, m, m, ngg, 6 + ns, ns + 1, viscous_order=viscous_order, reaction=reaction)
+    specs["temperature_ve"] = (1, ngg)
+    b = HostBlock(m, m, m, ngg, specs)
+    idx = (np.arange(-ngg, m + ngg)) % nper
+    u, v, w = turbulence_field(nper, 400.0, k_max=3, k0=2.0, seed=seed)
+    U = [f[np.ix_(idx, idx, idx)] for f in (u, v, w)]
+    rng = np.random.default_rng(seed + 1)
+    q = idx * dx
+    Z, Y, X = np.meshgrid(q, q, q, indexing="ij")
+    T = np.full(X.shape, 6000.0)
+    for c in rng.uniform(0, length, (3, 3)):
+        d2 = 0
+        for coord, cc in zip((X, Y, Z), c):
+            dd = np.abs(coord - cc)
+            dd = np.minimum(dd, length - dd)
+            d2 = d2 + dd ** 2
+        T += 2500.0 * np.exp(-d2 / (0.2 * length) ** 2)
+    base = {"N2": 0.70, "O2": 0.10, "NO": 0.05, "N": 0.05, "O": 0.10}
+    y = np.stack([base[n] * (1 + 0.3 * rng.uniform(-1, 1, X.shape)) for n in mech.species])
+    y /= y.sum(axis=0, keepdims=True)
+    p = np.full(X.shape, 2.0e4)
+    rho = p / ((y * (8314.462618 / mech.mw)[:, None, None, None]).sum(axis=0) * T)
+    bv = b.a["bv"]
+    bv[0], bv[1], bv[2], bv[3], bv[4], bv[5] = rho, U[0], U[1], U[2], p, T
+    b.a["sv"][:ns] = y
+    b.a["sv"][ns] = 0.0
+    b.a["temperature_ve"][0] = 0.45 * T + 600.0
+    mt = b.a["metric"]
+    mt[0] = mt[4] = mt[8] = 1.0 / dx
+    b.a["jac"][0] = dx ** 3
+    faces = box_faces(m, m, m, {(d, s): abi.BC_PERIODIC for d in range(3) for s in (-1, 1)})
+    c0 = math.sqrt(1.3 * 2.0e4 / float(rho.mean()))
+    par = make_param(n_var=6 + ns, n_spec=ns, dim=3, inviscid_scheme=scheme, reconstruction=reconstruction,
+                     viscous_order=viscous_order, cfl=0.3, rho_ref=float(rho.mean()), v_ref=c0, mech=mech.ptr(),
+                     two_t=tt.ptr())
+    par.reaction = 1 if reaction else 0
+    return Case("air5_box_2t", par, [b], [faces], {"mech": mech, "two_t": tt, "dx": dx})
+
+
 def reactive_shock_tube(mech, n_nodes=400, ngg=3, length=0.1, scheme=abi.INV_HLLC,
                         reconstruction=abi.REC_WENO5, reaction=True):
     """1-D reactive shock tube, stoichiometric H2/air: (T, p) = (1500 K, 5 atm) left of

@@ -26,11 +26,20 @@ class MechStruct:
                 a = np.ascontiguousarray(np.asarray(d[name], dtype=np.float64))
                 self.arrays[name] = a
                 setattr(s, name, a.ctypes.data_as(C.POINTER(C.c_double)))
-        for name in abi.MECH_INT:
+        for name in abi.MECH_INT + ("n_temperature_range",):
             if name in d:
                 a = np.ascontiguousarray(np.asarray(d[name], dtype=np.int32))
                 self.arrays[name] = a
                 setattr(s, name, a.ctypes.data_as(C.POINTER(C.c_int)))
+        for name in abi.MECH_NASA9 + abi.MECH_RT:
+            if name in d:
+                a = np.ascontiguousarray(np.asarray(d[name], dtype=np.float64))
+                self.arrays[name] = a
+                setattr(s, name, a.ctypes.data_as(C.POINTER(C.c_double)))
+        # NASA9 multi-range thermo and the two-temperature control temperatures, when present
+        s.therm_nasa_7_9 = int(d.get("nasa_7_or_9", 7))
+        s.max_range = int(d.get("max_range", 0))
+        s.two_temperature_reaction_temperature = int(d.get("two_temperature_reaction_temperature", 0))
         self.struct = s
 
     @property

@@ -196,6 +196,20 @@ int upload_mechanism(const cb2_mechanism &m, const cb2_two_temperature *tt, cb2_
   addi(&d.stoi_f, m.stoi_f, (size_t)nr * ns);
   addi(&d.stoi_b, m.stoi_b, (size_t)nr * ns);
   addi(&d.reac_order, m.reac_order, nr);
+  const bool nasa9 = m.therm_nasa_7_9 == 9;
+  if (nasa9) {
+    const size_t mr = (size_t)m.max_range;
+    addd(&d.t_cut, m.temperature_range, ns * (mr + 1));
+    addd(&d.poly9, m.therm_poly_coeff, ns * mr * 9);
+    addi(&d.n_range, m.n_temperature_range, ns);
+  }
+  const bool park = m.two_temperature_reaction_temperature != 0 && nr > 0;
+  if (park) {
+    addd(&d.tcf_a, m.tcf_a, nr);
+    addd(&d.tcf_b, m.tcf_b, nr);
+    addd(&d.tcb_a, m.tcb_a, nr);
+    addd(&d.tcb_b, m.tcb_b, nr);
+  }
   if (tt) {
     const size_t ml = (size_t)tt->max_level;
     addd(&d.theta_v, tt->theta_v, ns);
@@ -217,6 +231,9 @@ int upload_mechanism(const cb2_mechanism &m, const cb2_two_temperature *tt, cb2_
   for (auto &s : is) *s.dst = reinterpret_cast<const int *>(dev + bd) + s.off;
   d.n_spec = ns;
   d.n_reac = nr;
+  d.nasa9 = nasa9 ? 1 : 0;
+  d.max_range = nasa9 ? m.max_range : 0;
+  d.park = park ? 1 : 0;
   d.max_level = tt ? tt->max_level : 0;
   d.enable_vt = tt && tt->enable_vt_relaxation ? 1 : 0;
   return CB2_OK;
@@ -266,6 +283,10 @@ Block *get_block(cb2_ctx *ctx, int blk) {
 // the VT relaxation, cv from bv); its flux terms are not, so the other entry points refuse it.
 bool two_temperature(const cb2_ctx *ctx) { return ctx && ctx->p.i_eve >= 0; }
 
+// The residual terms built for two-temperature contexts: the chemistry source with the control
+// temperatures and the e_ve source.
+unsigned two_temperature_rhs_terms(const cb2_ctx *) { return CB2_RHS_CHEMISTRY; }
+
 int count(cb2_ctx *ctx, int n) {
   ctx->n_launch += (unsigned long long)n;
   return CB2_OK;
@@ -299,6 +320,29 @@ int cb2_init(const cb2_param_view *pv, cb2_ctx **out) {
   const int ns = pv->mech ? pv->mech->n_spec : 0;
   if (pv->n_spec != ns) return CB2_ERR_INVALID;
   if (ns != 0 && ns != 5 && ns != 9) return CB2_ERR_UNSUPPORTED;
+  if (ns > 0) {
+    const cb2_mechanism &m = *pv->mech;
+    if (m.therm_nasa_7_9 == 9) {
+      // NASA9 multi-range tables: every species has 1..max_range ranges with rising boundaries
+      if (m.max_range < 1 || m.max_range > 4 || !m.n_temperature_range || !m.temperature_range ||
+          !m.therm_poly_coeff)
+        return CB2_ERR_INVALID;
+      for (int s = 0; s < ns; ++s) {
+        const int n = m.n_temperature_range[s];
+        if (n < 1 || n > m.max_range) return CB2_ERR_INVALID;
+        const double *cut = m.temperature_range + s * (m.max_range + 1);
+        for (int r = 0; r < n; ++r)
+          if (!(cut[r] > 0 && cut[r] < cut[r + 1])) return CB2_ERR_INVALID;
+      }
+    } else if (m.therm_nasa_7_9 != 0 && m.therm_nasa_7_9 != 7) {
+      return CB2_ERR_INVALID;
+    } else if (!m.low_temp_coeff || !m.high_temp_coeff || !m.t_low || !m.t_mid || !m.t_high) {
+      return CB2_ERR_INVALID;
+    }
+    if (m.two_temperature_reaction_temperature && m.n_reac > 0 &&
+        (!m.tcf_a || !m.tcf_b || !m.tcb_a || !m.tcb_b))
+      return CB2_ERR_INVALID;
+  }
   // two-temperature: e_ve is the scalar after the species (i_eve = n_spec)
   const cb2_two_temperature *tt = pv->two_t;
   if (tt) {
@@ -581,7 +625,7 @@ int cb2_store_qn(cb2_ctx *ctx, int blk, void *stream) {
 int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream) {
   Block *B = get_block(ctx, blk);
   if (!B) return CB2_ERR_INVALID;
-  if (two_temperature(ctx)) return CB2_ERR_UNSUPPORTED;
+  if (two_temperature(ctx) && (mask & ~two_temperature_rhs_terms(ctx))) return CB2_ERR_UNSUPPORTED;
   ProfGuard pg(ctx);
   cudaStream_t s = (cudaStream_t)stream;
   const Param &p = ctx->p;

@@ -1,7 +1,9 @@
 // Finite-rate chemistry of one state: concentrations -> forward/backward rates -> rates of
 // progress -> species creation and destruction (finite_rate_chemistry, generic-mechanism branch,
 // src/FiniteRateChem.cu:1406-1488; forward_reaction_rate :1505-1554 with Troe :1536-1549;
-// backward_reaction_rate :1560-1636; rate_of_progress :1638-1663; chemical_source :1665-1681).
+// backward_reaction_rate :1560-1636; rate_of_progress :1638-1663; chemical_source :1665-1681;
+// the two-temperature control temperatures reaction_temperature :1490-1503 and the e_ve
+// source compute_two_temperature_chemical_source :19-31).
 //
 // The reaction loop is fused: each reaction's rate of progress is added to the per-species
 // creation/destruction accumulators as soon as it is known, so no per-reaction arrays are
@@ -11,6 +13,7 @@
 #pragma once
 #include "common.cuh"
 #include "thermo.cuh"
+#include "thermo_2t.cuh"
 
 namespace cb2 {
 
@@ -25,14 +28,26 @@ __device__ __forceinline__ double ipow(double c, int n) {
   return r;
 }
 
+// Smoothed control temperature T^a Tve^b of a two-temperature reaction rate
+// (reaction_temperature / smooth_reaction_temperature, src/FiniteRateChem.cu:1490-1503).
+__device__ __forceinline__ double reaction_temperature(double t, double tve, double a, double b) {
+  const double trx = pow(fmax(t, 1.0), a) * pow(fmax(tve, 1.0), b);
+  constexpr double t_min = 800.0, eps = 80.0;
+  return 0.5 * (trx + t_min + sqrt((trx - t_min) * (trx - t_min) + eps * eps));
+}
+
 // Forward and backward rates of progress of reaction r at t, concentrations c and
 // g/(RT) of every species (used only for reactions whose backward rate follows from the
-// equilibrium constant); temp_t = p_atm / (R_u T) * 1e-3.
+// equilibrium constant); temp_t = p_atm / (R_u T) * 1e-3.  With the mechanism's
+// control-temperature model the forward rate runs at smooth(T^tcf_a Tve^tcf_b) and the backward
+// rate at smooth(T^tcb_a Tve^tcb_b), its g/(RT) evaluated there (gibbs is then unused).
 template <int NS>
-__device__ __forceinline__ void reaction_progress(int r, double t, const double *c, const double *gibbs,
-                                                  double temp_t, const Mech &m, double &q1_out, double &q2_out) {
+__device__ __forceinline__ void reaction_progress(int r, double t0, double tve, const double *c,
+                                                  const double *gibbs, double temp_t, const Mech &m,
+                                                  double &q1_out, double &q2_out) {
   const int ty = __ldg(m.reac_type + r);
   const int *sf = m.stoi_f + r * NS, *sb = m.stoi_b + r * NS;
+  const double t = m.park ? reaction_temperature(t0, tve, __ldg(m.tcf_a + r), __ldg(m.tcf_b + r)) : t0;
   // forward rate
   double kf = arrhenius(t, __ldg(m.A + r), __ldg(m.b + r), __ldg(m.Ea + r));
   double cc = 0;
@@ -68,7 +83,24 @@ __device__ __forceinline__ void reaction_progress(int r, double t, const double 
   }
   // backward rate
   double kb = 0;
-  if (ty != 0) {
+  if (m.park) {
+    if (ty != 0) {
+      const double thb = reaction_temperature(t0, tve, __ldg(m.tcb_a + r), __ldg(m.tcb_b + r));
+      if (__ldg(m.rev_type + r) == 1) {
+        kb = arrhenius(thb, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
+        if (ty == 4) kb *= cc;
+      } else {
+        double g[NS];
+        species_gibbs_rt<NS>(thb, m, g);
+        double dg = 0;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) dg += g[s] * (__ldg(sb + s) - __ldg(sf + s));
+        constexpr double temp_p = kPatm / kRu * 1e-3;
+        const double kc = pow(temp_p / thb, __ldg(m.reac_order + r)) * exp(-dg);
+        kb = kf / kc;
+      }
+    }
+  } else if (ty != 0) {
     if (__ldg(m.rev_type + r) == 1) {
       kb = arrhenius(t, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
       if (ty == 4) kb *= cc;
@@ -106,10 +138,10 @@ __device__ __forceinline__ bool mech_needs_gibbs(const Mech &m) {
 // q1 nu_f + q2 nu_b [mol/(cm^3 s)]; q1r/q2r (may be null) receive the forward and backward
 // rates of progress of every reaction.
 template <int NS>
-__device__ __forceinline__ void chem_rates(double t, const double *c, const Mech &m, double *creation,
+__device__ __forceinline__ void chem_rates(double t, double tve, const double *c, const Mech &m, double *creation,
                                            double *destruction, double *q1r, double *q2r) {
   double gibbs[NS];
-  if (mech_needs_gibbs(m)) nasa7_gibbs_rt<NS>(t, m, gibbs);
+  if (!m.park && mech_needs_gibbs(m)) species_gibbs_rt<NS>(t, m, gibbs);
   constexpr double temp_p = kPatm / kRu * 1e-3;
   const double temp_t = temp_p / t;
 #pragma unroll
@@ -117,7 +149,7 @@ __device__ __forceinline__ void chem_rates(double t, const double *c, const Mech
 
   for (int r = 0; r < m.n_reac; ++r) {
     double q1, q2;
-    reaction_progress<NS>(r, t, c, gibbs, temp_t, m, q1, q2);
+    reaction_progress<NS>(r, t, tve, c, gibbs, temp_t, m, q1, q2);
     if (q1r) {
       q1r[r] = q1;
       q2r[r] = q2;
@@ -144,11 +176,16 @@ __device__ __forceinline__ void chemistry_point(const Zone &z, const Param &p, i
     y[s] = z.sv[g + s * sz];
     c[s] = rho * y[s] * __ldg(m.imw + s) * 1e-3;
   }
+  // two-temperature: the rates see max(T_ve, 1) (src/FiniteRateChem.cu:1450-1451)
+  const bool tt = p.i_eve >= 0;
+  const double tve_raw = tt ? z.tve[g] : t;
   double creation[NS], destruction[NS];
-  chem_rates<NS>(t, c, m, creation, destruction, nullptr, nullptr);
+  chem_rates<NS>(t, tt ? fmax(tve_raw, 1.0) : t, c, m, creation, destruction, nullptr, nullptr);
   const double jac = z.jac[g];
   const idx_t g0 = z.L0.at(i, j, k), sz0 = z.L0.sz;
-  double ts = 1e+6;
+  // e_ve source sum_s omega_s e_ve,s(T_ve), T_ve replaced by max(T, 1) when not positive
+  const double tve_src = tve_raw > 0.0 ? tve_raw : fmax(t, 1.0);
+  double ts = 1e+6, eve_src = 0.0;
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
     const double w = 1e+3 / __ldg(m.imw + s);
@@ -156,7 +193,9 @@ __device__ __forceinline__ void chemistry_point(const Zone &z, const Param &p, i
     const double om = creation[s] * w - od;
     z.dq[g0 + (5 + s) * sz0] += jac * om;
     if (y[s] > 1e-25 && fabs(od) > 1e-25) ts = fmin(ts, fabs(rho * y[s] / od));
+    if (tt) eve_src += om * ve_energy(s, tve_src, m, nullptr);
   }
+  if (tt) z.dq[g0 + (5 + NS) * sz0] += jac * eve_src;
   if (z.rts) z.rts[g] = ts;
 }
 

@@ -91,6 +91,14 @@ struct Mech {
   const double *zrot;
   const int *reac_type, *rev_type, *stoi_f, *stoi_b, *reac_order;
   const double *A, *b, *Ea, *A2, *b2, *Ea2, *tbc, *troe_alpha, *troe_t3, *troe_t1, *troe_t2;
+  // NASA9 multi-range thermo (nasa9 = 1): cuts [n_spec][max_range+1], coefficients
+  // [n_spec][max_range][9] (a0..a6, b1, b2)
+  int nasa9, max_range;
+  const int *n_range;
+  const double *t_cut, *poly9;
+  // control temperatures of the two-temperature reaction rates (park = 1)
+  int park;
+  const double *tcf_a, *tcf_b, *tcb_a, *tcb_b;
   // two-temperature data (null / 0 for one temperature)
   int max_level, enable_vt;
   const double *theta_v, *elec_theta, *elec_g, *lt_a, *lt_b, *park_sigma;

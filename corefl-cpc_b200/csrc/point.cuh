@@ -19,7 +19,7 @@ __device__ __forceinline__ double newton_temperature(double e, const double *y, 
   int iter = 0;
   double h[NS], cp[NS];
   while (err > 1e-5 && iter++ < 1000) {
-    nasa7_h_cp<NS>(t, m, h, cp);
+    species_h_cp<NS>(t, m, h, cp);
     double cpt = 0, ht = 0;
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
@@ -118,7 +118,7 @@ __device__ __forceinline__ void properties_point(const Zone &z, const Param &p, 
     if (z.mach) z.mach[g] = V / sqrt(kGammaAir * kRu / kMwAir * t);
   } else {
     double cp[NS], y[NS];
-    nasa7_cp<NS>(t, p.mech, cp);
+    species_cp<NS>(t, p.mech, cp);
     double imw = 0, cpt = 0;
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
@@ -171,7 +171,7 @@ __device__ __forceinline__ double local_dt_point(const Zone &z, const Param &p, 
       dv *= z.mul[g] / p.Pr;
     } else {
       double cp[NS];
-      nasa7_cp<NS>(z.bv[g + 5 * sz], p.mech, cp);
+      species_cp<NS>(z.bv[g + 5 * sz], p.mech, cp);
       double cpt = 0, mrd = 0;
       for (int s = 0; s < NS; ++s) {
         cpt += cp[s] * z.sv[g + s * sz];
@@ -215,7 +215,7 @@ __device__ __forceinline__ void cv_point(const Zone &z, const Param &p, idx_t g)
     E = total_energy_2t<NS>(z, p, g);
   } else {
     double h[NS];
-    nasa7_h<NS>(z.bv[g + 5 * sz], p.mech, h);
+    species_h<NS>(z.bv[g + 5 * sz], p.mech, h);
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
       const double y = z.sv[g + s * sz];

@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(kReactorThreads) k_reactor_setup(cb2_reactor *
   }
   const double rho = p / (t * kRu * imw);
   double h[NS];
-  nasa7_h<NS>(t, m, h);
+  species_h<NS>(t, m, h);
   double E = 0;
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
@@ -116,6 +116,11 @@ __device__ __forceinline__ Mech mech_species(const Mech &m, int s) {
   o.t_low += s; o.t_mid += s; o.t_high += s;
   o.lo += 7 * s; o.hi += 7 * s;
   o.gas_const += s; o.imw += s; o.mw += s;
+  if (m.nasa9) {
+    o.n_range += s;
+    o.t_cut += s * (m.max_range + 1);
+    o.poly9 += s * m.max_range * 9;
+  }
   return o;
 }
 
@@ -125,12 +130,12 @@ __device__ __forceinline__ void warp_source(double t, const double *y, const Mec
                                             ReactorShared<NS> &S, int lane) {
   if (lane < NS) {
     S.c[lane] = y[lane] / __ldg(m.mw + lane) * 1e-3;
-    if (gibbs_needed) nasa7_gibbs_rt<1>(t, mech_species(m, lane), &S.gibbs[lane]);
+    if (gibbs_needed) species_gibbs_rt<1>(t, mech_species(m, lane), &S.gibbs[lane]);
   }
   __syncwarp();
   constexpr double temp_p = kPatm / kRu * 1e-3;
   const double temp_t = temp_p / t;
-  for (int r = lane; r < m.n_reac; r += 32) reaction_progress<NS>(r, t, S.c, S.gibbs, temp_t, m, S.q1[r], S.q2[r]);
+  for (int r = lane; r < m.n_reac; r += 32) reaction_progress<NS>(r, t, t, S.c, S.gibbs, temp_t, m, S.q1[r], S.q2[r]);
   __syncwarp();
   if (lane < NS) {
     double cre = 0, des = 0;
@@ -156,7 +161,7 @@ __device__ __forceinline__ double warp_temperature(double t0, double imw, double
   while (err > 1e-8 && iter++ < 100) {
     if (lane < NS) {
       double h, cp;
-      nasa7_h_cp<1>(t, mech_species(m, lane), &h, &cp);
+      species_h_cp<1>(t, mech_species(m, lane), &h, &cp);
       S.ta[lane] = cp * S.yk[lane];
       S.tb[lane] = h * S.yk[lane];
     }

@@ -1,17 +1,96 @@
-// NASA7 two-range thermodynamics of a thermally perfect mixture (the Combustion2Part
-// branch of src/Thermo.cu:386-632) and the Roe-state "characteristic thermo" helper
-// (src/Thermo.cuh:49-110, one-temperature form).  Coefficients are read from the device
-// copy of the mechanism; outside [t_low, t_high] the enthalpy is extended linearly with
-// the edge cp and cp is held constant, as the reference does.
+// Species thermodynamics of a thermally perfect mixture: NASA7 two-range polynomials (the
+// Combustion2Part branch of src/Thermo.cu:386-632) or NASA9 multi-range polynomials (the
+// HighTempMultiPart branch with therm_nasa_7_9 = 9, src/Thermo.cu:76-112, 201-238, 288-320,
+// 352-384), chosen by the mechanism; and the Roe-state "characteristic thermo" helper
+// (src/Thermo.cuh:49-110).  Coefficients are read from the device copy of the mechanism;
+// outside the fitted range the enthalpy is extended linearly with the edge cp and cp is held
+// constant, as the reference does.
 #pragma once
 #include "common.cuh"
 
 namespace cb2 {
 
+// NASA9: the range of species s that holds t, or the edge range and its boundary outside.
+__device__ __forceinline__ const double *nasa9_range(const Mech &m, int s, double t, double &tt, bool &outside) {
+  const double *cut = m.t_cut + s * (m.max_range + 1);
+  const int n = __ldg(m.n_range + s);
+  const double *a = m.poly9 + s * m.max_range * 9;
+  outside = true;
+  if (t < __ldg(cut)) { tt = __ldg(cut); return a; }
+  if (t > __ldg(cut + n)) { tt = __ldg(cut + n); return a + (n - 1) * 9; }
+  outside = false;
+  tt = t;
+  int j = n - 1;
+  for (int r = 0; r < n; ++r)
+    if (__ldg(cut + r) <= t && t <= __ldg(cut + r + 1)) { j = r; break; }
+  return a + j * 9;
+}
+
+// NASA9 h/R at tt (1/tt and ln tt given) and cp/R at tt (1/tt^2 and 1/tt given)
+__device__ __forceinline__ double nasa9_h(const double *a, double tt, double itt, double lntt) {
+  const double tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt, tt5 = tt4 * tt;
+  return -__ldg(a + 0) * itt + __ldg(a + 1) * lntt + __ldg(a + 2) * tt + 0.5 * __ldg(a + 3) * tt2 +
+         __ldg(a + 4) * tt3 / 3 + 0.25 * __ldg(a + 5) * tt4 + 0.2 * __ldg(a + 6) * tt5 + __ldg(a + 7);
+}
+__device__ __forceinline__ double nasa9_cp(const double *a, double tt, double itt2, double itt) {
+  const double tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt;
+  return __ldg(a + 0) * itt2 + __ldg(a + 1) * itt + __ldg(a + 2) + __ldg(a + 3) * tt + __ldg(a + 4) * tt2 +
+         __ldg(a + 5) * tt3 + __ldg(a + 6) * tt4;
+}
+
+// NASA9 h_k and cp_k (compute_enthalpy_and_cp, src/Thermo.cu:201-238)
+template <int NS>
+__device__ __forceinline__ void nasa9_h_cp(double t, const Mech &m, double *h, double *cp) {
+  const double it = 1.0 / t, lnt = log(t), it2 = it * it;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    double tt;
+    bool outside;
+    const double *a = nasa9_range(m, s, t, tt, outside);
+    double hs, cps;
+    if (outside) {
+      const double tt2 = tt * tt, itt2 = 1.0 / tt2, itt = 1.0 / tt;
+      cps = nasa9_cp(a, tt, itt2, itt);
+      hs = nasa9_h(a, tt, itt, log(tt)) + cps * (t - tt);
+    } else {
+      hs = nasa9_h(a, t, it, lnt);
+      cps = nasa9_cp(a, t, it2, it);
+    }
+    cp[s] = cps * __ldg(m.gas_const + s);
+    h[s] = hs * __ldg(m.gas_const + s);
+  }
+}
+
+// NASA9 g_k/(R_k T) (compute_gibbs_div_rt, src/Thermo.cu:352-384)
+template <int NS>
+__device__ __forceinline__ void nasa9_gibbs_rt(double t, const Mech &m, double *g) {
+  const double it = 1.0 / t, lnt = log(t), it2 = it * it;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    double tt;
+    bool outside;
+    const double *a = nasa9_range(m, s, t, tt, outside);
+    double itt = it, lntt = lnt, itt2 = it2;
+    if (outside) {
+      itt = 1 / tt;
+      lntt = log(tt);
+      itt2 = itt * itt;
+    }
+    const double tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt;
+    g[s] = -0.5 * __ldg(a + 0) * itt2 + __ldg(a + 1) * itt * (lntt + 1) + __ldg(a + 2) * (1.0 - lntt) -
+           0.5 * __ldg(a + 3) * tt - __ldg(a + 4) * tt2 / 6.0 - __ldg(a + 5) * tt3 / 12.0 -
+           __ldg(a + 6) * tt4 * 0.05 + __ldg(a + 7) * itt - __ldg(a + 8);
+  }
+}
+
 // h_k [J/kg] and cp_k [J/(kg K)] of every species at temperature t
 // (compute_enthalpy_and_cp, src/Thermo.cu:453-523).
 template <int NS>
-__device__ __forceinline__ void nasa7_h_cp(double t, const Mech &m, double *h, double *cp) {
+__device__ __forceinline__ void species_h_cp(double t, const Mech &m, double *h, double *cp) {
+  if (m.nasa9) {
+    nasa9_h_cp<NS>(t, m, h, cp);
+    return;
+  }
   const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, t5 = t4 * t;
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
@@ -39,7 +118,12 @@ __device__ __forceinline__ void nasa7_h_cp(double t, const Mech &m, double *h, d
 
 // h_k only (compute_enthalpy, src/Thermo.cu:386-451).
 template <int NS>
-__device__ __forceinline__ void nasa7_h(double t, const Mech &m, double *h) {
+__device__ __forceinline__ void species_h(double t, const Mech &m, double *h) {
+  if (m.nasa9) {
+    double cp[NS];
+    nasa9_h_cp<NS>(t, m, h, cp);
+    return;
+  }
   const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, t5 = t4 * t;
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
@@ -64,7 +148,12 @@ __device__ __forceinline__ void nasa7_h(double t, const Mech &m, double *h) {
 
 // cp_k only (compute_cp, src/Thermo.cu:525-574).
 template <int NS>
-__device__ __forceinline__ void nasa7_cp(double t, const Mech &m, double *cp) {
+__device__ __forceinline__ void species_cp(double t, const Mech &m, double *cp) {
+  if (m.nasa9) {
+    double h[NS];
+    nasa9_h_cp<NS>(t, m, h, cp);
+    return;
+  }
   const double t2 = t * t, t3 = t2 * t, t4 = t3 * t;
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
@@ -87,7 +176,11 @@ __device__ __forceinline__ void nasa7_cp(double t, const Mech &m, double *cp) {
 // g_k/(R_k T) of every species (compute_gibbs_div_rt, src/Thermo.cu:576-632, NASA7 branch);
 // outside [t_low, t_high] the polynomial is evaluated at the range edge.
 template <int NS>
-__device__ __forceinline__ void nasa7_gibbs_rt(double t, const Mech &m, double *g) {
+__device__ __forceinline__ void species_gibbs_rt(double t, const Mech &m, double *g) {
+  if (m.nasa9) {
+    nasa9_gibbs_rt<NS>(t, m, g);
+    return;
+  }
   const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, t_inv = 1 / t, log_t = log(t);
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
@@ -114,7 +207,7 @@ __device__ __forceinline__ void characteristic_thermo(double t, const double *y,
                                                       double &c, double *alpha, double *ecoef, double *e_tr_out) {
   const double te = fmax(t, 1.0);
   double h[NS], cp[NS];
-  nasa7_h_cp<NS>(te, m, h, cp);
+  species_h_cp<NS>(te, m, h, cp);
   double e_tr = 0, r = 0, cpm = 0, cvm = 0;
 #pragma unroll
   for (int s = 0; s < NS; ++s) {

@@ -98,7 +98,7 @@ __device__ __forceinline__ double mixture_vib_energy(double t, const double *y, 
 template <int NS>
 __device__ __forceinline__ double mixture_tr_energy(double t, const double *y, const Mech &m, double &cv_tr) {
   double h[NS], cp[NS];
-  nasa7_h_cp<NS>(t, m, h, cp);
+  species_h_cp<NS>(t, m, h, cp);
   double e = 0.0, cpm = 0.0, rm = 0.0;
 #pragma unroll
   for (int i = 0; i < NS; ++i) {
@@ -287,7 +287,7 @@ __device__ __forceinline__ double total_energy_2t(const Zone &z, const Param &p,
   const double u = z.bv[g + sz], v = z.bv[g + 2 * sz], w = z.bv[g + 3 * sz], t = z.bv[g + 5 * sz];
   double E = 0.5 * (u * u + v * v + w * w);
   double h[NS], cp[NS], y[NS];
-  nasa7_h_cp<NS>(t, p.mech, h, cp);
+  species_h_cp<NS>(t, p.mech, h, cp);
 #pragma unroll
   for (int l = 0; l < NS; ++l) {
     y[l] = z.sv[g + l * sz];

@@ -290,7 +290,7 @@ __device__ __forceinline__ void visc2_face(const Zone &z, const Param &p, int i,
       }
     }
     double h[NS];
-    nasa7_h<NS>(0.5 * (z.bv[g + 5 * sz] + z.bv[gn + 5 * sz]), m, h);
+    species_h<NS>(0.5 * (z.bv[g + 5 * sz] + z.bv[gn + 5 * sz]), m, h);
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
       const double jd = dif[s] * (force[s] - mwt * yk[s] * sum_gy_w) - yk[s] * corr;

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define CB2_ABI_VERSION 3
+#define CB2_ABI_VERSION 4
 
 /* ---- status codes ---------------------------------------------------------------- */
 #define CB2_OK 0
@@ -139,6 +139,21 @@ typedef struct cb2_mechanism {
   const double *A2, *b2, *Ea2;       /* [n_reac] low-pressure / reverse Arrhenius        */
   const double *third_body_coeff;    /* [n_reac*n_spec] */
   const double *troe_alpha, *troe_t3, *troe_t1, *troe_t2; /* [n_reac] */
+  /* NASA9 multi-range polynomials (the reference's high-temperature build, therm_nasa_7_9 = 9,
+   * Species::read_therm_nasa9, src/ChemData.cpp:865-1034); replace the NASA7 tables above when
+   * therm_nasa_7_9 == 9.  Below the first and above the last boundary h is extended linearly
+   * with the edge cp and cp is held (src/Thermo.cu:76-112). */
+  int therm_nasa_7_9;                 /* 0 or 7: the NASA7 two-range tables; 9: the tables below */
+  int max_range;                      /* most temperature ranges of any species (1..4)           */
+  const int *n_temperature_range;     /* [n_spec]                                                */
+  const double *temperature_range;    /* [n_spec*(max_range+1)] range boundaries [K]             */
+  const double *therm_poly_coeff;     /* [n_spec*max_range*9]: a0..a6, b1, b2 of each range      */
+  /* Control temperatures of the two-temperature reaction rates (Reaction::tcf_a .. tcb_b, the
+   * AIR5 model of src/ChemData.cpp:1247-1262): with the switch on, reaction i runs forward at
+   * smooth(T^tcf_a Tve^tcf_b) and backward at smooth(T^tcb_a Tve^tcb_b)
+   * (src/FiniteRateChem.cu:1490-1503). */
+  int two_temperature_reaction_temperature;
+  const double *tcf_a, *tcf_b, *tcb_a, *tcb_b; /* [n_reac] */
 } cb2_mechanism;
 
 /* Vibrational-electronic data of the species for the two-temperature model, as

@@ -12,9 +12,88 @@ namespace {
 inline double sqr(double x) { return x * x; }
 
 // ---------------------------------------------------------------------------------------
+// Thermodynamics, NASA9 multi-range (the HighTempMultiPart build with therm_nasa_7_9 = 9:
+// compute_enthalpy src/Thermo.cu:76-112, compute_enthalpy_and_cp :201-238, compute_cp
+// :288-320, compute_gibbs_div_rt :352-384).  Outside the first / last boundary the polynomial
+// is evaluated at the boundary; h is then extended linearly with that cp.
+// ---------------------------------------------------------------------------------------
+struct Range9 {
+  const double *a;  // a0..a6, b1, b2 of the range used
+  double tt;        // evaluation temperature (t, or the boundary outside)
+  bool outside;
+};
+
+Range9 range9(const Mechanism &m, int s, double t) {
+  const double *cut = m.t_cut.data() + s * (m.max_range + 1);
+  const int n = m.n_range[s];
+  const double *a = m.poly9.data() + (size_t)s * m.max_range * 9;
+  if (t < cut[0]) return {a, cut[0], true};
+  if (t > cut[n]) return {a + (n - 1) * 9, cut[n], true};
+  int j = n - 1;
+  for (int r = 0; r < n; ++r)
+    if (cut[r] <= t && t <= cut[r + 1]) {
+      j = r;
+      break;
+    }
+  return {a + j * 9, t, false};
+}
+
+// h/R at tt with 1/tt and ln tt given
+double h9(const double *a, double tt, double itt, double lntt) {
+  const double tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt, tt5 = tt4 * tt;
+  return -a[0] * itt + a[1] * lntt + a[2] * tt + 0.5 * a[3] * tt2 + a[4] * tt3 / 3 + 0.25 * a[5] * tt4 +
+         0.2 * a[6] * tt5 + a[7];
+}
+// cp/R at tt with 1/tt^2 and 1/tt given
+double cp9(const double *a, double tt, double itt2, double itt) {
+  const double tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt;
+  return a[0] * itt2 + a[1] * itt + a[2] + a[3] * tt + a[4] * tt2 + a[5] * tt3 + a[6] * tt4;
+}
+
+void nasa9_h_cp(double t, const Mechanism &m, double *h, double *cp) {
+  const double it = 1.0 / t, lnt = std::log(t), it2 = it * it;
+  for (int i = 0; i < m.n_spec; ++i) {
+    const Range9 r = range9(m, i, t);
+    if (r.outside) {
+      const double tt2 = r.tt * r.tt, itt2 = 1.0 / tt2, itt = 1.0 / r.tt;
+      const double c = cp9(r.a, r.tt, itt2, itt);
+      h[i] = h9(r.a, r.tt, itt, std::log(r.tt)) + c * (t - r.tt);
+      cp[i] = c;
+    } else {
+      h[i] = h9(r.a, t, it, lnt);
+      cp[i] = cp9(r.a, t, it2, it);
+    }
+    cp[i] *= m.gas_const[i];
+    h[i] *= m.gas_const[i];
+  }
+}
+
+void nasa9_gibbs_rt(double t, const Mechanism &m, double *g) {
+  const double it = 1.0 / t, lnt = std::log(t), it2 = it * it;
+  for (int i = 0; i < m.n_spec; ++i) {
+    const Range9 r = range9(m, i, t);
+    double itt = it, lntt = lnt, itt2 = it2;
+    if (r.outside) {
+      itt = 1 / r.tt;
+      lntt = std::log(r.tt);
+      itt2 = itt * itt;
+    }
+    const double tt = r.tt, tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt;
+    const double *a = r.a;
+    g[i] = -0.5 * a[0] * itt2 + a[1] * itt * (lntt + 1) + a[2] * (1.0 - lntt) - 0.5 * a[3] * tt - a[4] * tt2 / 6.0 -
+           a[5] * tt3 / 12.0 - a[6] * tt4 * 0.05 + a[7] * itt - a[8];
+  }
+}
+
+// ---------------------------------------------------------------------------------------
 // Thermodynamics, NASA7 two-range (src/Thermo.cu:386-574, Combustion2Part branch)
 // ---------------------------------------------------------------------------------------
 void nasa7_h(double t, const Mechanism &m, double *h) {
+  if (m.nasa == 9) {
+    double cp[16];
+    nasa9_h_cp(t, m, h, cp);
+    return;
+  }
   const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, t5 = t4 * t;
   for (int i = 0; i < m.n_spec; ++i) {
     if (t < m.t_low[i] || t > m.t_high[i]) {
@@ -33,6 +112,11 @@ void nasa7_h(double t, const Mechanism &m, double *h) {
 }
 
 void nasa7_cp(double t, const Mechanism &m, double *cp) {
+  if (m.nasa == 9) {
+    double h[16];
+    nasa9_h_cp(t, m, h, cp);
+    return;
+  }
   const double t2 = t * t, t3 = t2 * t, t4 = t3 * t;
   for (int i = 0; i < m.n_spec; ++i) {
     if (t < m.t_low[i] || t > m.t_high[i]) {
@@ -1148,6 +1232,10 @@ void transport(double t, double mw_total, const double *y, const double *cp, con
 // ---------------------------------------------------------------------------------------
 void gibbs_div_rt(double t, const Mechanism &m, double *g) {
   // compute_gibbs_div_rt (src/Thermo.cu:576-605)
+  if (m.nasa == 9) {
+    nasa9_gibbs_rt(t, m, g);
+    return;
+  }
   const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, t_inv = 1 / t, log_t = std::log(t);
   for (int i = 0; i < m.n_spec; ++i) {
     if (t < m.t_low[i] || t > m.t_high[i]) {
@@ -1168,11 +1256,20 @@ double arrhenius(double t, double A, double b, double Ea) { return A * std::pow(
 
 // Forward and backward rates of progress q1, q2 [mol/(cm^3 s)] of every reaction at t [K] and
 // concentrations c [mol/cm^3].
-void rates_of_progress(const Mechanism &m, double t, const double *c, double *q1, double *q2) {
+// reaction_temperature / smooth_reaction_temperature (src/FiniteRateChem.cu:1490-1503)
+double reaction_temperature(double t, double tve, double a, double b) {
+  const double trx = std::pow(std::max(t, 1.0), a) * std::pow(std::max(tve, 1.0), b);
+  constexpr double t_min = 800.0, eps = 80.0;
+  return 0.5 * (trx + t_min + std::sqrt((trx - t_min) * (trx - t_min) + eps * eps));
+}
+
+void rates_of_progress(const Mechanism &m, double t0, double tve, const double *c, double *q1, double *q2) {
   const int ns = m.n_spec, nr = m.n_reac;
   double kf[32], kb[32];
-  // forward_reaction_rate (:1505-1554), 1T reaction temperature
+  // forward_reaction_rate (:1505-1554); with the control-temperature model each reaction runs
+  // at its own smoothed T^a Tve^b
   for (int i = 0; i < nr; ++i) {
+    const double t = m.park ? reaction_temperature(t0, tve, m.tcf_a[i], m.tcf_b[i]) : t0;
     kf[i] = arrhenius(t, m.A[i], m.b[i], m.Ea[i]);
     const int ty = m.reac_type[i];
     if (ty == 3) {
@@ -1206,9 +1303,37 @@ void rates_of_progress(const Mechanism &m, double t, const double *c, double *q1
       }
     }
   }
+  // backward_reaction_rate (:1560-1592) with the control-temperature model: per reaction at
+  // its own backward temperature, g/RT evaluated there
+  if (m.park) {
+    for (int i = 0; i < nr; ++i) {
+      const double thb = reaction_temperature(t0, tve, m.tcb_a[i], m.tcb_b[i]);
+      if (m.reac_type[i] == 0) {
+        kb[i] = 0;
+        continue;
+      }
+      if (m.rev_type[i] == 1) {
+        kb[i] = arrhenius(thb, m.A2[i], m.b2[i], m.Ea2[i]);
+        if (m.reac_type[i] == 4) {
+          double cc = 0;
+          for (int l = 0; l < ns; ++l) cc += c[l] * m.tbc[i * ns + l];
+          kb[i] *= cc;
+        }
+        continue;
+      }
+      double g[16];
+      gibbs_div_rt(thb, m, g);
+      const double temp_t = p_atm / R_u * 1e-3 / thb;
+      double dg = 0;
+      for (int l = 0; l < ns; ++l) dg += g[l] * (m.stoi_b[i * ns + l] - m.stoi_f[i * ns + l]);
+      const double kc = std::pow(temp_t, m.reac_order[i]) * std::exp(-dg);
+      kb[i] = kf[i] / kc;
+    }
+  }
   // backward_reaction_rate (:1593-1636)
-  int n_gibbs = nr;
-  for (int i = 0; i < nr; ++i) {
+  const double t = t0;
+  int n_gibbs = m.park ? 0 : nr;
+  for (int i = 0; i < nr && !m.park; ++i) {
     if (m.reac_type[i] == 0) {
       kb[i] = 0;
       --n_gibbs;
@@ -1249,11 +1374,12 @@ void rates_of_progress(const Mechanism &m, double t, const double *c, double *q1
   }
 }
 
-void chemistry_point(const Mechanism &m, double rho, double t, const double *y, double *omega, double *omega_d) {
+void chemistry_point(const Mechanism &m, double rho, double t, double tve, const double *y, double *omega,
+                     double *omega_d) {
   const int ns = m.n_spec, nr = m.n_reac;
   double c[16], q1[32], q2[32];
   for (int l = 0; l < ns; ++l) c[l] = rho * y[l] * m.imw[l] * 1e-3;
-  rates_of_progress(m, t, c, q1, q2);
+  rates_of_progress(m, t, tve, c, q1, q2);
   // chemical_source (:1665-1681)
   for (int i = 0; i < ns; ++i) {
     double creation = 0;
@@ -1276,12 +1402,22 @@ void finite_rate_chemistry(Zone &z, const Param &p) {
         const int ns = p.n_spec;
         double y[16], om[16], od[16];
         for (int l = 0; l < ns; ++l) y[l] = z.sv(i, j, k, l);
-        const double rho = z.bv(i, j, k, 0);
-        chemistry_point(p.mech, rho, z.bv(i, j, k, 5), y, om, od);
+        const double rho = z.bv(i, j, k, 0), t = z.bv(i, j, k, 5);
+        // the rates see max(T_ve, 1) (:1450-1451)
+        const double tve = p.i_eve >= 0 ? std::max(z.tve(i, j, k), 1.0) : t;
+        chemistry_point(p.mech, rho, t, tve, y, om, od);
         double ts = 1e+6;
         for (int l = 0; l < ns; ++l) {
           z.dq(i, j, k, l + 5) += z.jac(i, j, k) * om[l];
           if (y[l] > 1e-25 && std::fabs(od[l]) > 1e-25) ts = std::min(ts, std::fabs(rho * y[l] / od[l]));
+        }
+        if (p.i_eve >= 0) {
+          // compute_two_temperature_chemical_source (:19-31): sum_l omega_l e_ve,l(T_ve)
+          double tv = z.tve(i, j, k);
+          if (tv <= 0.0) tv = std::max(t, 1.0);
+          double src = 0.0;
+          for (int l = 0; l < ns; ++l) src += om[l] * ve_energy(p, l, tv);
+          z.dq(i, j, k, 5 + p.i_eve) += z.jac(i, j, k) * src;
         }
         if (z.rts) z.rts(i, j, k) = ts;
       }
@@ -1321,11 +1457,15 @@ void cv_point(Zone &z, const Param &p, int i, int j, int k) {
 }  // namespace
 
 void reaction_rates(const Mechanism &m, double t, const double *c, double *q1, double *q2) {
-  rates_of_progress(m, t, c, q1, q2);
+  rates_of_progress(m, t, t, c, q1, q2);
 }
 
 void nasa7_h_cp(double t, const Mechanism &m, double *h, double *cp) {
   // compute_enthalpy_and_cp (src/Thermo.cu:453-523)
+  if (m.nasa == 9) {
+    nasa9_h_cp(t, m, h, cp);
+    return;
+  }
   const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, t5 = t4 * t;
   for (int i = 0; i < m.n_spec; ++i) {
     if (t < m.t_low[i] || t > m.t_high[i]) {
@@ -1399,6 +1539,20 @@ Param make_param(const cb2_param_view &pv) {
       o.imw[s] = 1.0 / m.mw[s];              // src/DParameter.cu:96
       o.gas_const[s] = R_u / m.mw[s];        // src/DParameter.cu:97
       o.mw[s] = 1.0 / o.imw[s];              // src/Transport.cu:57
+    }
+    if (m.therm_nasa_7_9 == 9) {
+      o.nasa = 9;
+      o.max_range = m.max_range;
+      o.n_range = cpi(m.n_temperature_range, ns);
+      o.t_cut = cp(m.temperature_range, ns * (m.max_range + 1));
+      o.poly9 = cp(m.therm_poly_coeff, ns * m.max_range * 9);
+    }
+    o.park = m.two_temperature_reaction_temperature != 0;
+    if (o.park) {
+      o.tcf_a = cp(m.tcf_a, nr);
+      o.tcf_b = cp(m.tcf_b, nr);
+      o.tcb_a = cp(m.tcb_a, nr);
+      o.tcb_b = cp(m.tcb_b, nr);
     }
     o.lo = cp(m.low_temp_coeff, ns * 7);
     o.hi = cp(m.high_temp_coeff, ns * 7);
@@ -1654,7 +1808,14 @@ void compute_inviscid_flux(Zone &z, const Param &p) {
 void compute_chemistry(Zone &z, const Param &p) { finite_rate_chemistry(z, p); }
 
 void chemistry_source(const Mechanism &m, double rho, double t, const double *y, double *omega, double *omega_d) {
-  chemistry_point(m, rho, t, y, omega, omega_d);
+  chemistry_point(m, rho, t, t, y, omega, omega_d);
+}
+
+void species_gibbs_rt(double t, const Mechanism &m, double *g) { gibbs_div_rt(t, m, g); }
+
+void chemistry_source_2t(const Mechanism &m, double rho, double t, double tve, const double *y, double *omega,
+                         double *omega_d) {
+  chemistry_point(m, rho, t, tve, y, omega, omega_d);
 }
 
 void compute_viscous_flux(Zone &z, const Param &p) {

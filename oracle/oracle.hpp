@@ -50,6 +50,14 @@ struct Mechanism {
   std::vector<double> geometry, lj_inv, vis_coeff, wjwi14, sqwiwj8, bdc, kbe, zrot;
   std::vector<int> reac_type, rev_type, stoi_f, stoi_b, reac_order;
   std::vector<double> A, b, Ea, A2, b2, Ea2, tbc, troe_alpha, troe_t3, troe_t1, troe_t2;
+  // NASA9 multi-range thermo (nasa == 9): cuts [n_spec][max_range+1], coefficients
+  // [n_spec][max_range][9]
+  int nasa = 7, max_range = 0;
+  std::vector<int> n_range;
+  std::vector<double> t_cut, poly9;
+  // two-temperature control temperatures of the reaction rates
+  bool park = false;
+  std::vector<double> tcf_a, tcf_b, tcb_a, tcb_b;
 };
 
 // Vibrational-electronic data of the two-temperature model (cfd::Species::read_two_temperature,
@@ -100,6 +108,11 @@ void compute_inviscid_flux(Zone &z, const Param &p);
 void compute_viscous_flux(Zone &z, const Param &p);
 void compute_chemistry(Zone &z, const Param &p);
 void chemistry_source(const Mechanism &m, double rho, double t, const double *y, double *omega, double *omega_d);
+// g_k/(R_k T) of every species (compute_gibbs_div_rt)
+void species_gibbs_rt(double t, const Mechanism &m, double *g);
+// the same at (T, Tve): the control temperatures of the two-temperature reaction rates
+void chemistry_source_2t(const Mechanism &m, double rho, double t, double tve, const double *y, double *omega,
+                         double *omega_d);
 void update_physical_properties(Zone &z, const Param &p);
 void compute_shock_sensor(Zone &z, const Param &p);
 void apply_boundary_conditions(Zone &z, const Param &p);

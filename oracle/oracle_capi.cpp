@@ -143,6 +143,25 @@ void oracle_chemistry_source(const cb2_mechanism *m, double rho, double t, const
   chemistry_source(p.mech, rho, t, y, omega, omega_d);
 }
 
+void oracle_gibbs_rt(const cb2_mechanism *m, double t, double *g) {
+  cb2_param_view pv{};
+  pv.mech = m;
+  pv.n_spec = m->n_spec;
+  Param p = make_param(pv);
+  species_gibbs_rt(t, p.mech, g);
+}
+
+// The same at (T, Tve): with the mechanism's control-temperature model each reaction runs at its
+// own smoothed T^a Tve^b.
+void oracle_chemistry_source_2t(const cb2_mechanism *m, double rho, double t, double tve, const double *y,
+                                double *omega, double *omega_d) {
+  cb2_param_view pv{};
+  pv.mech = m;
+  pv.n_spec = m->n_spec;
+  Param p = make_param(pv);
+  chemistry_source_2t(p.mech, rho, t, tve, y, omega, omega_d);
+}
+
 // A 0-D reactor from (T0, p0, Y) advanced by at most max_attempts ROK4E attempts (or to t_end);
 // the state is returned in the cb2_reactor layout of include/cb200_serve.h.
 void oracle_reactor_run(const cb2_mechanism *m, double T0, double p0, const double *Y, double t_end, double h0,

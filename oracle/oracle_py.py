@@ -45,6 +45,7 @@ def load():
             "oracle_two_temperature_state": (None, [P(abi.ParamView), C.c_double, C.c_double, C.c_double,
                                                     P(C.c_double), P(C.c_double)]),
             "oracle_species_ve": (None, [P(abi.ParamView), C.c_double, P(C.c_double), P(C.c_double)]),
+            "oracle_gibbs_rt": (None, [P(abi.Mechanism), C.c_double, P(C.c_double)]),
         }
         for n, (r, a) in sig.items():
             f = getattr(lib, n)
@@ -150,6 +151,28 @@ def chemistry_source(mech, rho, t, y):
     od = np.zeros(mech.ns)
     lib.oracle_chemistry_source(mech.ptr(), rho, t, y.ctypes.data_as(P), om.ctypes.data_as(P), od.ctypes.data_as(P))
     return om, od
+
+
+def chemistry_source_2t(mech, rho, t, tve, y):
+    """(omega, omega_d) of one state at (T, Tve) (the control-temperature rates when the mechanism
+    has them)."""
+    lib = load()
+    lib.oracle_chemistry_source_2t.restype = None
+    P = C.POINTER(C.c_double)
+    lib.oracle_chemistry_source_2t.argtypes = [C.POINTER(abi.Mechanism), C.c_double, C.c_double, C.c_double, P, P, P]
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    om = np.zeros(mech.ns)
+    od = np.zeros(mech.ns)
+    lib.oracle_chemistry_source_2t(mech.ptr(), rho, t, tve, y.ctypes.data_as(P), om.ctypes.data_as(P),
+                                   od.ctypes.data_as(P))
+    return om, od
+
+
+def gibbs_rt(mech, t):
+    g = np.zeros(mech.ns)
+    P = C.POINTER(C.c_double)
+    load().oracle_gibbs_rt(mech.ptr(), C.c_double(t), g.ctypes.data_as(P))
+    return g
 
 
 def nasa7_h_cp(mech, t):

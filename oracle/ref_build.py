@@ -24,7 +24,7 @@ def build(ref="/root/reference", force=False):
     exe = os.path.join(OUT, "dump_mech")
     mine = [os.path.join(HERE, "ref", f) for f in ("stubs.cpp", "dump_mech.cpp", "mpi.h")]
     drivers = [os.path.join(HERE, "ref", f) for f in ("dump_chem.cpp", "dump_reactor.cpp", "chem_stubs.cpp",
-                                                       "dump_2t.cpp")]
+                                                       "dump_2t.cpp", "dump_air5.cpp")]
     theirs = [os.path.join(src, f) for f in ("ChemData.cpp", "Parameter.cpp", "Element.cpp",
                                              os.path.join("gxl_lib", "MyString.cpp"))]
     if not force and os.path.exists(exe) and os.path.getmtime(exe) >= max(os.path.getmtime(f) for f in mine + drivers):
@@ -60,6 +60,15 @@ def build(ref="/root/reference", force=False):
     r = subprocess.run(cmd4, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("reference two-temperature driver build failed:\n" + r.stderr[-4000:])
+    # dump_air5: the same two-temperature build driven on the AIR5 data; the host Species thermo
+    # and compute_gibbs_div_rt evaluate NASA9 multi-range polynomials whenever therm_nasa_7_9 = 9
+    # (src/ChemData.cpp:326-520, src/ConstVolumeReactor.cpp:1401-1454)
+    exe5 = os.path.join(OUT, "dump_air5")
+    cmd5 = [c if not c.endswith("dump_2t.cpp") else os.path.join(HERE, "ref", "dump_air5.cpp") for c in cmd4]
+    cmd5[-1] = exe5
+    r = subprocess.run(cmd5, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("reference AIR5 driver build failed:\n" + r.stderr[-4000:])
     return exe
 
 

@@ -15,6 +15,12 @@ oracle/ref_build.py) on the reference's example data files and keeps its JSON ou
                    species e_ve / cv_ve of Species::compute_ve_energy / compute_ve_cv on a
                    temperature ladder, and on 40 seeded (rho, T, Tve, Y) states the mixture
                    e_ve, Species::invert_tve_from_eve and cfd::compute_vt_relaxation_source
+  air5_park.json : the AIR5 two-temperature case (5 species, Park's 17 dissociation and exchange
+                   reactions of example/squareCylinder2D_M10_air5_dns/input/chemistry/) with NASA9
+                   multi-range thermo and the AIR5 control-temperature model: the tables, species
+                   h / cp / g/RT / e_ve / cv_ve on a temperature ladder, and on 32 seeded
+                   (rho, T, Tve, Y) states the source of compute_src(T, Tve), the e_ve chemical
+                   source and update_t_two_temperature
   h2_reactor_runs.json : 0-D reactors run with the reference's host chemistry, Jacobian, LU
                    and Newton through the adaptive ROK4E sequence (RTol 1e-6, ATol 1e-12,
                    first step 1e-8): the reference's example case to 1.2 ms and 8 seeded
@@ -67,6 +73,10 @@ def main(ref):
     files_2t = dict(files, two_temperature_file="example/squareCylinder2D_M10_air5_dns/input/chemistry/"
                                                 "two_temperature.dat")
     print(run(ref, "h2_two_temperature.json", files_2t, 7, prog="dump_2t", extra=("40",)))
+    air = "example/squareCylinder2D_M10_air5_dns/input/chemistry/"
+    files_air5 = {"mechanism_file": air + "air5_park.inp", "therm_file": air + "therm.dat",
+                  "transport_file": air + "tran.dat", "two_temperature_file": air + "two_temperature.dat"}
+    print(run(ref, "air5_park.json", files_air5, 9, prog="dump_air5", extra=("32",)))
 
 
 if __name__ == "__main__":
