@@ -18,7 +18,8 @@ _ip = C.POINTER(C.c_int)
 
 ZONE_ARRAYS = ("cv", "bv", "sv", "qn", "dq", "metric", "jac", "mul", "thermal_conductivity", "rho_D",
                "acoustic_speed", "gamma", "mach", "fFlux", "gFlux", "hFlux", "vis_flux", "shock_sensor",
-               "dt_local", "reaction_timeScale", "entropy_fix_delta", "temperature_ve")
+               "dt_local", "reaction_timeScale", "entropy_fix_delta", "temperature_ve",
+               "thermal_conductivity_ve")
 
 
 class ZoneView(C.Structure):

@@ -333,6 +333,8 @@ def air5_box_2t(mech, tt, n_nodes=10, ngg=3, length=1e-2, seed=91, viscous_order
     ns = mech.ns
     specs = array_specs(m, m, m, ngg, 6 + ns, ns + 1, viscous_order=viscous_order, reaction=reaction)
     specs["temperature_ve"] = (1, ngg)
+    if viscous_order:
+        specs["thermal_conductivity_ve"] = (1, ngg)
     b = HostBlock(m, m, m, ngg, specs)
     idx = (np.arange(-ngg, m + ngg)) % nper
     u, v, w = turbulence_field(nper, 400.0, k_max=3, k0=2.0, seed=seed)

@@ -271,6 +271,7 @@ Zone make_zone(const cb2_zone_view &v) {
   z.gamma = v.gamma; z.mach = v.mach; z.fF = v.fFlux; z.gF = v.gFlux; z.hF = v.hFlux; z.visf = v.vis_flux;
   z.shock = v.shock_sensor; z.dtl = v.dt_local; z.rts = v.reaction_timeScale; z.efd = v.entropy_fix_delta;
   z.tve = v.temperature_ve;
+  z.kappa_ve = v.thermal_conductivity_ve;
   return z;
 }
 
@@ -285,7 +286,11 @@ bool two_temperature(const cb2_ctx *ctx) { return ctx && ctx->p.i_eve >= 0; }
 
 // The residual terms built for two-temperature contexts: the chemistry source with the control
 // temperatures and the e_ve source.
-unsigned two_temperature_rhs_terms(const cb2_ctx *) { return CB2_RHS_CHEMISTRY; }
+unsigned two_temperature_rhs_terms(const cb2_ctx *ctx) {
+  unsigned m = CB2_RHS_CHEMISTRY;
+  if (ctx->p.viscous_order == 2) m |= CB2_RHS_VISCOUS;
+  return m;
+}
 
 int count(cb2_ctx *ctx, int n) {
   ctx->n_launch += (unsigned long long)n;
@@ -766,7 +771,6 @@ int cb2_boundary(cb2_ctx *ctx, int blk, void *stream) {
 int cb2_properties(cb2_ctx *ctx, int blk, void *stream) {
   Block *B = get_block(ctx, blk);
   if (!B) return CB2_ERR_INVALID;
-  if (two_temperature(ctx)) return CB2_ERR_UNSUPPORTED;
   ProfGuard pg(ctx);
   int nl = 0;
   CB2_TRY(launch_properties(B->z, ctx->p, (cudaStream_t)stream, nl));
@@ -784,7 +788,6 @@ int cb2_cv_from_bv(cb2_ctx *ctx, int blk, void *stream) {
 
 // Enqueues the CFL dt of every bound block and their minimum into ctx->d_dtmin.
 static int enqueue_cfl_dt(cb2_ctx *ctx, cudaStream_t s) {
-  if (two_temperature(ctx)) return CB2_ERR_UNSUPPORTED;
   int nl = 0;
   CB2_TRY(launch_set_value(ctx->d_dtmin, 1e+6, s, nl));
   for (auto &B : ctx->blocks) {

@@ -70,6 +70,7 @@ struct Zone {
   double *cv, *bv, *sv, *qn, *dq, *metric, *jac, *mul, *kappa, *rhoD, *acoustic, *gamma, *mach;
   double *fF, *gF, *hF, *visf, *shock, *dtl, *rts, *efd;
   double *tve;  // two-temperature: T_ve, ghost ngg
+  double *kappa_ve;  // two-temperature: vibrational-electronic conductivity, ghost ngg
   // mixed form: FP32 copies the FP32 kernels read instead of the FP64 arrays (private scratch,
   // same padded layout): bv (6 comps, refreshed at the start of every residual) and the
   // metric (9 comps) followed by J, taken when the block is bound

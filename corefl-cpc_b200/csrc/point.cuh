@@ -128,11 +128,25 @@ __device__ __forceinline__ void properties_point(const Zone &z, const Param &p, 
     }
     const double mw = 1 / fmax(imw, 1e-12);
     const double R = kRu * imw;
-    const double gam = cpt / (cpt - R);
-    z.gamma[g] = gam;
-    const double c = sqrt(gam * R * t);
-    z.acoustic[g] = c;
-    if (z.mach) z.mach[g] = V / c;
+    const bool tt = p.i_eve >= 0;
+    if (tt) {
+      // two-temperature (src/FieldOperation.cuh:207-226): gamma and c of the
+      // translational-rotational mode; T_ve defaults to T
+      double cv_tr, cp_tr, r_mix;
+      tr_heat_capacities<NS>(t, y, p.mech, cv_tr, cp_tr, r_mix);
+      const double gam = cp_tr / fmax(cv_tr, 1e-8);
+      z.gamma[g] = gam;
+      const double a = sqrt(fmax(gam * r_mix * t, 1e-12));
+      z.acoustic[g] = a;
+      if (z.mach) z.mach[g] = V / a;
+      if (z.tve[g] <= 0) z.tve[g] = t;
+    } else {
+      const double gam = cpt / (cpt - R);
+      z.gamma[g] = gam;
+      const double c = sqrt(gam * R * t);
+      z.acoustic[g] = c;
+      if (z.mach) z.mach[g] = V / c;
+    }
     if (!transport) return;
     double mu, kappa, rhoD[NS];
     transport_properties<NS>(t, z.bv[g + 4 * sz], mw, y, cp, p.mech, mu, kappa, rhoD);
@@ -140,6 +154,12 @@ __device__ __forceinline__ void properties_point(const Zone &z, const Param &p, 
     z.kappa[g] = kappa;
 #pragma unroll
     for (int s = 0; s < NS; ++s) z.rhoD[g + s * sz] = rhoD[s];
+    if (tt && z.kappa_ve) {
+      // kappa_ve = kappa cv_ve(T_ve) / cp
+      double cv_ve;
+      mixture_ve_energy<NS>(z.tve[g], y, p.mech, &cv_ve);
+      z.kappa_ve[g] = kappa * cv_ve / fmax(cpt, 1e-8);
+    }
   }
 }
 
@@ -180,6 +200,15 @@ __device__ __forceinline__ double local_dt_point(const Zone &z, const Param &p, 
       dv = z.mul[g] * irho;
       dv = fmax(dv, z.kappa[g] * irho * z.gamma[g] / cpt);
       dv = fmax(dv, mrd * irho);
+      if (p.i_eve >= 0 && z.kappa_ve) {
+        // two-temperature: the e_ve conduction kappa_ve / (rho cv_ve) (src/TimeAdvanceFunc.cuh:95-106)
+        const double tve = z.tve[g] > 0.0 ? z.tve[g] : fmax(z.bv[g + 5 * sz], 1.0);
+        double y[NS], cv_ve;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) y[s] = z.sv[g + s * sz];
+        mixture_ve_energy<NS>(tve, y, p.mech, &cv_ve);
+        dv = fmax(dv, z.kappa_ve[g] * irho / fmax(cv_ve, 1e-8));
+      }
     }
     lam = fmax(lam, len * len * dv);
   }

@@ -113,6 +113,26 @@ __device__ __forceinline__ double mixture_tr_energy(double t, const double *y, c
   return e - eve_eq;
 }
 
+// cv_tr, cp_tr and R of the mixture at t (the heat capacities compute_mixture_tr_energy returns,
+// src/Thermo.cu:739-761).
+template <int NS>
+__device__ __forceinline__ void tr_heat_capacities(double t, const double *y, const Mech &m, double &cv_tr,
+                                                   double &cp_tr, double &r_mix) {
+  double h[NS], cp[NS];
+  species_h_cp<NS>(t, m, h, cp);
+  double cpm = 0.0, rm = 0.0;
+#pragma unroll
+  for (int i = 0; i < NS; ++i) {
+    cpm += y[i] * cp[i];
+    rm += y[i] * __ldg(m.gas_const + i);
+  }
+  double cv_eq;
+  mixture_ve_energy<NS>(t, y, m, &cv_eq);
+  cv_tr = (cpm - rm) - cv_eq;
+  cp_tr = cpm - cv_eq;
+  r_mix = rm;
+}
+
 // Newton inversion of T_ve from e_ve, at most 80 iterations (invert_tve_from_eve,
 // src/Thermo.cu:763-779).
 template <int NS>

@@ -12,6 +12,7 @@
 #include <type_traits>
 #include "common.cuh"
 #include "thermo.cuh"
+#include "thermo_2t.cuh"
 #include "launch.h"
 
 namespace cb2 {
@@ -190,7 +191,7 @@ __global__ void __launch_bounds__(kVisRow, 16) k_visc8_divergence_f32(Zone z, Pa
 // ---- 2nd-order face fluxes ----------------------------------------------------------------
 // Face between node (i,j,k) and its +1 neighbour along DIR.  The compact difference is taken
 // along DIR and the two transverse derivatives are averaged over the two nodes (4-point).
-template <int NS, int DIR>
+template <int NS, int DIR, bool TT = false>
 __device__ __forceinline__ void visc2_face(const Zone &z, const Param &p, int i, int j, int k, double *fv) {
   const Layout &L = z.L;
   const idx_t sz = L.sz;
@@ -290,12 +291,33 @@ __device__ __forceinline__ void visc2_face(const Zone &z, const Param &p, int i,
       }
     }
     double h[NS];
-    species_h<NS>(0.5 * (z.bv[g + 5 * sz] + z.bv[gn + 5 * sz]), m, h);
+    const double tm = 0.5 * (z.bv[g + 5 * sz] + z.bv[gn + 5 * sz]);
+    species_h<NS>(tm, m, h);
+    const double tve_m = TT ? 0.5 * (z.tve[g] + z.tve[gn]) : tm;
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
       const double jd = dif[s] * (force[s] - mwt * yk[s] * sum_gy_w) - yk[s] * corr;
       fv[4 + s] = jd;
-      fv[3] += h[s] * jd;
+      // two-temperature: the diffusing enthalpy carries e_ve at T_ve
+      // (compute_nonequilibrium_diffusion_enthalpy, src/Thermo.cuh:43-47)
+      const double hd = TT ? h[s] - ve_energy(s, tm, m, nullptr) + ve_energy(s, tve_m, m, nullptr) : h[s];
+      fv[3] += hd * jd;
+    }
+    if constexpr (TT) {
+      // e_ve conduction kappa_ve grad T_ve in the energy flux, and the e_ve flux
+      // (src/ViscousScheme.cu:1024-1039)
+      double v_xi, v_eta, v_zeta;
+      grad(z.tve, v_xi, v_eta, v_zeta);
+      const double v_x = v_xi * xi_x + v_eta * eta_x + v_zeta * zeta_x;
+      const double v_y = v_xi * xi_y + v_eta * eta_y + v_zeta * zeta_y;
+      const double v_z = v_xi * xi_z + v_eta * eta_z + v_zeta * zeta_z;
+      const double kve = 0.5 * (z.kappa_ve[g] + z.kappa_ve[gn]);
+      const double cond_ve = kve * (kxj * v_x + kyj * v_y + kzj * v_z);
+      fv[3] += cond_ve;
+      double ef = cond_ve;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) ef += ve_energy(s, tve_m, m, nullptr) * fv[4 + s];
+      fv[4 + NS] = ef;
     }
   }
 }
@@ -304,9 +326,9 @@ constexpr int kV2TI = 16, kV2TS = 16;  // tile of 16 transverse x 16 faces along
 
 // Face fluxes of a tile and their difference: a CTA owns kV2TS faces along DIR (the first
 // one is the left face of the first node) for kV2TI positions of the transverse index.
-template <int NS, int DIR>
+template <int NS, int DIR, bool TT = false>
 __global__ void __launch_bounds__(kV2TI *kV2TS) k_visc2(Zone z, Param p) {
-  constexpr int NF = 4 + NS;
+  constexpr int NF = 4 + NS + (TT ? 1 : 0);
   __shared__ double sfv[NF][kV2TI * kV2TS];
   const int tid = threadIdx.x;
   const int tt = tid % kV2TI, ts = tid / kV2TI;
@@ -322,7 +344,7 @@ __global__ void __launch_bounds__(kV2TI *kV2TS) k_visc2(Zone z, Param p) {
   const bool valid = tr < trmax && n <= ext[DIR] - 1;
   if (valid) {
     double fv[NF];
-    visc2_face<NS, DIR>(z, p, i, j, k, fv);
+    visc2_face<NS, DIR, TT>(z, p, i, j, k, fv);
 #pragma unroll
     for (int c = 0; c < NF; ++c) sfv[c][tid] = fv[c];
   }
@@ -334,7 +356,7 @@ __global__ void __launch_bounds__(kV2TI *kV2TS) k_visc2(Zone z, Param p) {
   }
 }
 
-template <int NS>
+template <int NS, bool TT = false>
 static int launch_visc2_ns(const Zone &z, const Param &p, cudaStream_t s, int &nl) {
   const int ndir = z.mz > 1 ? 3 : 2;
   for (int d = 0; d < ndir; ++d) {
@@ -344,9 +366,9 @@ static int launch_visc2_ns(const Zone &z, const Param &p, cudaStream_t s, int &n
     dim3 grid((tr + kV2TI - 1) / kV2TI, (ext[d] + kV2TS - 2) / (kV2TS - 1), other);
     static const char *names[3] = {"visc2_x", "visc2_y", "visc2_z"};
     ProfScope prof(names[d], s);
-    if (d == 0) k_visc2<NS, 0><<<grid, kV2TI * kV2TS, 0, s>>>(z, p);
-    else if (d == 1) k_visc2<NS, 1><<<grid, kV2TI * kV2TS, 0, s>>>(z, p);
-    else k_visc2<NS, 2><<<grid, kV2TI * kV2TS, 0, s>>>(z, p);
+    if (d == 0) k_visc2<NS, 0, TT><<<grid, kV2TI * kV2TS, 0, s>>>(z, p);
+    else if (d == 1) k_visc2<NS, 1, TT><<<grid, kV2TI * kV2TS, 0, s>>>(z, p);
+    else k_visc2<NS, 2, TT><<<grid, kV2TI * kV2TS, 0, s>>>(z, p);
     ++nl;
     CB2_TRY(check_launch());
   }
@@ -386,6 +408,13 @@ int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_fac
     return check_launch();
   }
   if (p.viscous_order == 2) {
+    if (p.i_eve >= 0) {
+      // two-temperature: the e_ve conduction and flux, T_ve in the diffusing enthalpy
+      if (!z.tve || !z.kappa_ve) return CB2_ERR_INVALID;
+      if (p.n_spec == 5) return launch_visc2_ns<5, true>(z, p, s, nl);
+      if (p.n_spec == 9) return launch_visc2_ns<9, true>(z, p, s, nl);
+      return CB2_ERR_UNSUPPORTED;
+    }
     switch (p.n_spec) {
       case 0: return launch_visc2_ns<0>(z, p, s, nl);
       case 5: return launch_visc2_ns<5>(z, p, s, nl);

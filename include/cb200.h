@@ -97,6 +97,8 @@ typedef struct cb2_zone_view {
   double *reaction_timeScale;   /* ghost ngg, reacting cases                */
   double *entropy_fix_delta;    /* ghost 1, Roe                             */
   double *temperature_ve;       /* ghost ngg, two-temperature cases (DZone::temperature_ve) */
+  double *thermal_conductivity_ve; /* ghost ngg, two-temperature mixtures with viscous terms
+                                    * (DZone::thermal_conductivity_ve)                          */
 } cb2_zone_view;
 
 /* One face boundary condition of a block (cfd::Boundary, src/Mesh.h:8-30, after

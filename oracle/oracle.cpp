@@ -1126,11 +1126,29 @@ void viscous_face_2nd(const Zone &z, const Param &p, int dir, int i, int j, int 
       }
     }
     double h[16];
-    nasa7_h(0.5 * (z.bv(i, j, k, 5) + z.bv(in, jn, kn, 5)), p.mech, h);
+    const double tm = 0.5 * (z.bv(i, j, k, 5) + z.bv(in, jn, kn, 5));
+    nasa7_h(tm, p.mech, h);
+    const bool tt = p.i_eve >= 0;
+    const double tve_m = tt ? 0.5 * (z.tve(i, j, k) + z.tve(in, jn, kn)) : tm;
     for (int l = 0; l < ns; ++l) {
       const double jd = dif[l] * (force[l] - mwt * yk[l] * sum_gy_w) - yk[l] * corr;
       fv[4 + l] = jd;
-      fv[3] += h[l] * jd;
+      // two-temperature: the diffusing enthalpy carries e_ve at T_ve
+      // (compute_nonequilibrium_diffusion_enthalpy, src/Thermo.cuh:43-47)
+      const double hd = tt ? h[l] - ve_energy(p, l, tm) + ve_energy(p, l, tve_m) : h[l];
+      fv[3] += hd * jd;
+    }
+    if (tt) {
+      // e_ve conduction kappa_ve grad T_ve in the energy flux, and the e_ve flux
+      // (src/ViscousScheme.cu:1024-1039)
+      double dtv[3];
+      der(z.tve, 0, dtv);
+      const double kve = 0.5 * (z.kappa_ve(i, j, k) + z.kappa_ve(in, jn, kn));
+      const double cond_ve = kve * (kxj * cx(dtv) + kyj * cy(dtv) + kzj * cz(dtv));
+      fv[3] += cond_ve;
+      double ef = cond_ve;
+      for (int l = 0; l < ns; ++l) ef += ve_energy(p, l, tve_m) * fv[4 + l];
+      fv[4 + p.i_eve] = ef;
     }
   }
 }
@@ -1617,6 +1635,7 @@ Zone make_zone(const cb2_zone_view &v, const cb2_face_bc *faces, int n_faces, co
   z.shock = A(v.shock_sensor, g); z.dtl = A(v.dt_local, 0); z.rts = A(v.reaction_timeScale, g);
   z.efd = A(v.entropy_fix_delta, 1);
   z.tve = A(v.temperature_ve, g);
+  z.kappa_ve = A(v.thermal_conductivity_ve, g);
   const int mx = v.mx, my = v.my, mz = v.mz;
   z.il.assign(my * mz, 0); z.ir.assign(my * mz, 0); z.jl.assign(mx * mz, 0); z.jr.assign(mx * mz, 0);
   z.kl.assign(mx * my, 0); z.kr.assign(mx * my, 0);
@@ -1847,16 +1866,34 @@ void update_physical_properties(Zone &z, const Param &p) {
         }
         const double mw = 1 / std::max(imw, 1e-12);
         const double R = R_u * imw;
-        const double gam = cpt / (cpt - R);
-        z.gamma(i, j, k) = gam;
-        const double c = std::sqrt(gam * R * t);
-        z.acoustic(i, j, k) = c;
-        if (z.mach) z.mach(i, j, k) = V / c;
+        if (p.i_eve >= 0) {
+          // two-temperature (src/FieldOperation.cuh:207-226): gamma and c of the
+          // translational-rotational mode, T_ve defaulted to T, kappa_ve = kappa cv_ve(T_ve) / cp
+          double cv_tr, cp_tr, r_mix;
+          tr_heat_capacities(p, t, y, cv_tr, cp_tr, r_mix);
+          const double gam = cp_tr / std::max(cv_tr, 1e-8);
+          z.gamma(i, j, k) = gam;
+          const double a = std::sqrt(std::max(gam * r_mix * t, 1e-12));
+          z.acoustic(i, j, k) = a;
+          if (z.mach) z.mach(i, j, k) = V / a;
+          if (z.tve(i, j, k) <= 0) z.tve(i, j, k) = t;
+        } else {
+          const double gam = cpt / (cpt - R);
+          z.gamma(i, j, k) = gam;
+          const double c = std::sqrt(gam * R * t);
+          z.acoustic(i, j, k) = c;
+          if (z.mach) z.mach(i, j, k) = V / c;
+        }
         double mu, kap, rd[16];
         transport(t, mw, y, cp, p.mech, mu, kap, rd);
         z.mul(i, j, k) = mu;
         z.kappa(i, j, k) = kap;
         for (int l = 0; l < ns; ++l) z.rhoD(i, j, k, l) = rd[l];
+        if (p.i_eve >= 0 && z.kappa_ve) {
+          double cv_ve = 0;
+          mixture_ve_energy(p, z.tve(i, j, k), y, &cv_ve);
+          z.kappa_ve(i, j, k) = kap * cv_ve / std::max(cpt, 1e-8);
+        }
       }
 }
 
@@ -2045,6 +2082,14 @@ double local_time_step_min(Zone &z, const Param &p) {
             dv = z.mul(i, j, k) * irho;
             dv = std::max(dv, z.kappa(i, j, k) * irho * z.gamma(i, j, k) / cp);
             dv = std::max(dv, mrd * irho);
+            if (p.i_eve >= 0 && z.kappa_ve) {
+              // two-temperature e_ve conduction (src/TimeAdvanceFunc.cuh:95-106)
+              const double tve = z.tve(i, j, k) > 0.0 ? z.tve(i, j, k) : std::max(z.bv(i, j, k, 5), 1.0);
+              double y[16], cv_ve = 0;
+              for (int l = 0; l < p.n_spec; ++l) y[l] = z.sv(i, j, k, l);
+              mixture_ve_energy(p, tve, y, &cv_ve);
+              dv = std::max(dv, z.kappa_ve(i, j, k) * irho / std::max(cv_ve, 1e-8));
+            }
           }
           lam = std::max(lam, len * len * dv);
         }

@@ -93,7 +93,7 @@ struct FaceBC {
 struct Zone {
   int mx = 0, my = 0, mz = 0, ngg = 0;
   Arr cv, bv, sv, qn, dq, metric, jac, mul, kappa, rhoD, acoustic, gamma, mach, fF, gF, hF, visf, shock, dtl, rts,
-      efd, tve;
+      efd, tve, kappa_ve;
   std::vector<int> il, ir, jl, jr, kl, kr;  // physical-boundary flags per face node
   std::vector<FaceBC> faces;
 };
@@ -129,6 +129,8 @@ void reaction_rates(const Mechanism &m, double t, const double *c, double *q1, d
 double ve_energy(const Param &p, int i, double t);
 double ve_cv(const Param &p, int i, double t);
 double mixture_ve_energy(const Param &p, double t, const double *y, double *cv_ve);
+// cv_tr, cp_tr and R of the mixture at t (compute_mixture_tr_energy's heat capacities)
+void tr_heat_capacities(const Param &p, double t, const double *y, double &cv_tr, double &cp_tr, double &r_mix);
 double invert_tve_from_eve(const Param &p, double eve_target, const double *y, double t_init);
 double vt_relaxation_source(const Param &p, double density, double t, double tve, const double *y, double *eve_eq,
                             double *tau_eff);

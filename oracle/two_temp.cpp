@@ -57,8 +57,9 @@ double mixture_vib_energy(const Param &p, double t, const double *y, double *cv_
   return ev;
 }
 
-double mixture_tr_energy(const Param &p, double t, const double *y, double *cv_tr) {
-  // compute_mixture_tr_energy (src/Thermo.cu:739-761); only e and cv_tr are used here
+double mixture_tr_energy(const Param &p, double t, const double *y, double *cv_tr, double *cp_tr = nullptr,
+                         double *r_mix = nullptr) {
+  // compute_mixture_tr_energy (src/Thermo.cu:739-761)
   double h[16], cp[16];
   nasa7_h_cp(t, p.mech, h, cp);
   double e = 0.0, cpm = 0.0, rm = 0.0;
@@ -71,6 +72,8 @@ double mixture_tr_energy(const Param &p, double t, const double *y, double *cv_t
   const double eve_eq = mixture_ve_energy(p, t, y, &cv_eq);
   const double cv_total = cpm - rm;
   if (cv_tr) *cv_tr = cv_total - cv_eq;
+  if (cp_tr) *cp_tr = cpm - cv_eq;
+  if (r_mix) *r_mix = rm;
   return e - eve_eq;
 }
 
@@ -333,6 +336,10 @@ void apply_vt_relaxation(Zone &z, const Param &p, double dt_stage) {
         z.tve(i, j, k) = invert_tve_from_eve(p, z.sv(i, j, k, p.i_eve), y, tve);
         temperature_2t(z, p, i, j, k, z.cv(i, j, k, 4));
       }
+}
+
+void tr_heat_capacities(const Param &p, double t, const double *y, double &cv_tr, double &cp_tr, double &r_mix) {
+  mixture_tr_energy(p, t, y, &cv_tr, &cp_tr, &r_mix);
 }
 
 }  // namespace oracle

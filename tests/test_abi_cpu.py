@@ -31,7 +31,11 @@ def test_library_exports_every_declared_symbol(cb200_lib):
 
 def test_struct_sizes_match_header():
     # 4 ints + 22 pointers; 3 ints + 6 ints + 7 doubles; versioned param view
-    assert C.sizeof(abi.ZoneView) == 4 * 4 + 22 * 8
+    assert C.sizeof(abi.ZoneView) == 4 * 4 + 23 * 8
+    # n_spec, n_reac; the NASA7, transport and reaction tables; the NASA9 header (two ints), its
+    # three tables; the control-temperature switch (padded) and its four tables
+    n_tab = len(abi.MECH_DOUBLE) + len(abi.MECH_INT) + len(abi.MECH_REAC)
+    assert C.sizeof(abi.Mechanism) == 2 * 4 + n_tab * 8 + 2 * 4 + 3 * 8 + 8 + 4 * 8
     # 2 ints, 7 pointers, 1 int (padded to 8)
     assert C.sizeof(abi.TwoTemperature) == 2 * 4 + 7 * 8 + 8
     assert C.sizeof(abi.FaceBC) == 4 * 9 + 4 + 7 * 8  # 36 bytes of ints, padded to 8

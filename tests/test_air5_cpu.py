@@ -123,3 +123,25 @@ def test_air5_box_oracle_chemistry_rows(oracle_lib, air5, tt):
         oracle_lib.stage_update(p, b, 1e-9, rk)
     assert np.isfinite(b.a["bv"][:, g:-g, g:-g, g:-g]).all()
     assert (b.a["temperature_ve"][0][g:-g, g:-g, g:-g] > 0).all()
+
+
+def test_air5_box_oracle_viscous_two_temperature(oracle_lib, air5, tt):
+    """Properties (gamma of the trans-rot mode, kappa_ve = kappa cv_ve / cp) and the 2nd-order
+    viscous residual with the e_ve rows on the AIR5 box: finite, and the e_ve conduction acts."""
+    case = cases.air5_box_2t(air5, tt, n_nodes=6, viscous_order=2)
+    p, b, faces = case.param, case.blocks[0], case.faces[0]
+    oracle_lib.cv_from_bv(p, b)
+    oracle_lib.properties(p, b)
+    g = b.ngg
+    inner = (slice(None), slice(g, -g), slice(g, -g), slice(g, -g))
+    kve, kap = b.a["thermal_conductivity_ve"][inner], b.a["thermal_conductivity"][inner]
+    assert (kve > 0).all() and (kve < kap).all()
+    # the trans-rot gamma of partly dissociated air: near 1.4 (diatomic; the NASA9 cp is not
+    # exactly the harmonic-oscillator split) and below 5/3 (atoms)
+    gam = b.a["gamma"][inner]
+    assert (gam > 1.35).all() and (gam < 1.67).all()
+    oracle_lib.rhs(p, b, faces, abi.RHS_VISCOUS)
+    assert np.isfinite(b.a["dq"]).all()
+    assert np.abs(b.a["dq"][5 + air5.ns]).max() > 0
+    dt = oracle_lib.cfl_dt(p, b)
+    assert 0 < dt < 1e-3
