@@ -93,10 +93,13 @@ def test_vt_relaxation_parity(oracle_lib, h2, tt):
     assert np.abs(_inner(b.a["temperature_ve"], g) - _inner(before, g)).max() > 1.0
 
 
-def test_two_temperature_context_refuses_flux_paths(oracle_lib, h2, tt):
+def test_two_temperature_context_refuses_unbuilt_paths(oracle_lib, h2, tt):
+    """The inviscid two-temperature flux is not built: the residual with it, the boundary fill and
+    the whole step refuse the context; the chemistry-only residual runs."""
     p, b, faces, dev, ctx = _setup(oracle_lib, h2, tt)
-    for call in (lambda: ctx.rhs(0), lambda: ctx.boundary(0), lambda: ctx.properties(0),
-                 lambda: ctx.rk3_step(1e-9, fixed_dt=True), lambda: ctx.cfl_dt()):
+    for call in (lambda: ctx.rhs(0), lambda: ctx.rhs(0, abi.RHS_INVISCID), lambda: ctx.boundary(0),
+                 lambda: ctx.rk3_step(1e-9, fixed_dt=True)):
         with pytest.raises(cb200.CB2Error) as e:
             call()
         assert e.value.code == abi.ERR_UNSUPPORTED
+    ctx.rhs(0, abi.RHS_CHEMISTRY)
