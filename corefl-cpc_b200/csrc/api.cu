@@ -284,11 +284,36 @@ Block *get_block(cb2_ctx *ctx, int blk) {
 // the VT relaxation, cv from bv); its flux terms are not, so the other entry points refuse it.
 bool two_temperature(const cb2_ctx *ctx) { return ctx && ctx->p.i_eve >= 0; }
 
+unsigned two_temperature_rhs_terms(const cb2_ctx *ctx);
+
+// Faces whose ghost fill is built for two temperatures: periodic and outflow copy bv and every
+// scalar (e_ve included) and rebuild cv with the T_ve sync, as the reference's apply_periodic /
+// apply_outflow do (src/BoundCond.cu:2204-2350, 3390-3440).
+bool two_temperature_faces(const Block &B) {
+  for (const FaceBC &f : B.faces)
+    if (f.type != CB2_BC_PERIODIC && f.type != CB2_BC_OUTFLOW) return false;
+  return true;
+}
+
+// Whether the whole two-temperature step is built for this context: every residual term the
+// settings ask for and the ghost fill of every bound block.
+bool two_temperature_step(const cb2_ctx *ctx) {
+  unsigned need = CB2_RHS_INVISCID;
+  if (ctx->p.viscous_order > 0) need |= CB2_RHS_VISCOUS;
+  if (ctx->p.reaction) need |= CB2_RHS_CHEMISTRY;
+  if ((need & ~two_temperature_rhs_terms(ctx)) != 0) return false;
+  for (const Block &B : ctx->blocks)
+    if (B.bound && !two_temperature_faces(B)) return false;
+  return true;
+}
+
 // The residual terms built for two-temperature contexts: the chemistry source with the control
-// temperatures and the e_ve source.
+// temperatures and the e_ve source, the 2nd-order viscous fluxes with the e_ve terms, and the
+// characteristic WENO fluxes with rho e_ve as a scalar row.
 unsigned two_temperature_rhs_terms(const cb2_ctx *ctx) {
   unsigned m = CB2_RHS_CHEMISTRY;
   if (ctx->p.viscous_order == 2) m |= CB2_RHS_VISCOUS;
+  if (ctx->p.inviscid_scheme == CB2_INV_WENO5_CH || ctx->p.inviscid_scheme == CB2_INV_WENO7_CH) m |= CB2_RHS_INVISCID;
   return m;
 }
 
@@ -759,7 +784,7 @@ int cb2_vt_relaxation(cb2_ctx *ctx, int blk, double dt_stage, void *stream) {
 int cb2_boundary(cb2_ctx *ctx, int blk, void *stream) {
   Block *B = get_block(ctx, blk);
   if (!B) return CB2_ERR_INVALID;
-  if (two_temperature(ctx)) return CB2_ERR_UNSUPPORTED;
+  if (two_temperature(ctx) && !two_temperature_faces(*B)) return CB2_ERR_UNSUPPORTED;
   ProfGuard pg(ctx);
   int nl = 0;
   cudaStream_t s = (cudaStream_t)stream;
@@ -913,7 +938,7 @@ extern "C" {
 
 int cb2_rk3_step(cb2_ctx *ctx, double *dt_inout, int fixed_dt, void *stream) {
   if (!ctx || !dt_inout) return CB2_ERR_INVALID;
-  if (two_temperature(ctx)) return CB2_ERR_UNSUPPORTED;
+  if (two_temperature(ctx) && !two_temperature_step(ctx)) return CB2_ERR_UNSUPPORTED;
   ProfGuard pg(ctx);
   CB2_TRY(enqueue_step_head(ctx, stream));
   double dt = *dt_inout;

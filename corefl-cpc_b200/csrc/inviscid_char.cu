@@ -9,9 +9,12 @@
 // max over the stencil of |U_k| + c|grad k|, projection of F and Q onto the left
 // eigenvectors at every stencil node, WENO on the split characteristic fluxes, and the
 // explicit back-projection.  The y/z face metric is averaged with the i+1 neighbour, as
-// the reference does (src/WENO.cu:1615-1617, 2280-2282).
+// the reference does (src/WENO.cu:1615-1617, 2280-2282).  Two-temperature mixtures carry
+// rho e_ve as one more scalar row, with the Roe-state thermo of the translational-rotational
+// mode (TT).
 #include "common.cuh"
 #include "thermo.cuh"
+#include "thermo_2t.cuh"
 #include "weno.cuh"
 #include "sweep.cuh"
 #include "launch.h"
@@ -22,11 +25,12 @@ namespace cb2 {
 // 0 U_k = (rho u . grad k)/rho, 1-3 rho u_m U_k + p k_m, 4 p, 5 c |grad k|, 6 J.
 constexpr int kNF = 7;
 
-template <int NS, int ORDER>
+template <int NS, int ORDER, bool TT = false>
 __device__ __forceinline__ void char_flux(const double *__restrict__ sQ, const double *__restrict__ sF, int NN,
                                           int c, int st, double kx, double ky, double kz, double eps,
                                           bool shock, const Mech &mech, double *fc) {
-  constexpr int NV = 5 + NS;
+  constexpr int NSC = NS + (TT ? 1 : 0);  // transported scalars: species (+ e_ve)
+  constexpr int NV = 5 + NSC;
   constexpr int R = ORDER / 2 + 1;  // nodes on each side of the interface
   constexpr int NW = 2 * R - 1;     // values per WENO side
 #define Qv(v, m) sQ[(v) * NN + c + (m) * st]
@@ -39,7 +43,7 @@ __device__ __forceinline__ void char_flux(const double *__restrict__ sQ, const d
   const double vm = rlc * Qv(2, 0) + rrc * Qv(2, 1);
   const double wm = rlc * Qv(3, 0) + rrc * Qv(3, 1);
   double cm, gm1;
-  double svm[NS > 0 ? NS : 1], alpha[NS > 0 ? NS : 1], ecoef[NS > 0 ? NS : 1];
+  double svm[NSC > 0 ? NSC : 1], alpha[NSC > 0 ? NSC : 1], ecoef[NSC > 0 ? NSC : 1];
   if constexpr (NS == 0) {
     const double t_roe = (rlc * Fv(4, 0) + rrc * Fv(4, 1)) / kRAir;
     cm = sqrt(kGammaAir * kRAir * t_roe);
@@ -47,13 +51,13 @@ __device__ __forceinline__ void char_flux(const double *__restrict__ sQ, const d
   } else {
     double rmix = 0;
 #pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      svm[s] = rlc * Qv(5 + s, 0) + rrc * Qv(5 + s, 1);
-      rmix += svm[s] * __ldg(mech.gas_const + s);
-    }
+    for (int s = 0; s < NSC; ++s) svm[s] = rlc * Qv(5 + s, 0) + rrc * Qv(5 + s, 1);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) rmix += svm[s] * __ldg(mech.gas_const + s);
     const double t_roe = (rlc * Fv(4, 0) + rrc * Fv(4, 1)) / fmax(rmix, 1e-12);
     double gamma;
-    characteristic_thermo<NS>(t_roe, svm, mech, gamma, cm, alpha, ecoef, nullptr);
+    if constexpr (TT) characteristic_thermo_2t<NS>(t_roe, svm, mech, gamma, cm, alpha, ecoef);
+    else characteristic_thermo<NS>(t_roe, svm, mech, gamma, cm, alpha, ecoef, nullptr);
     gm1 = gamma - 1;
   }
   // orthonormal basis (k, n, q)
@@ -87,7 +91,7 @@ __device__ __forceinline__ void char_flux(const double *__restrict__ sQ, const d
     for (int m = 0; m < 2 * R; ++m) {
       double sp = 0, sm = 0;
 #pragma unroll
-      for (int s = 0; s < NS; ++s) {
+      for (int s = 0; s < NSC; ++s) {
         sp = fma(alpha[s], Qv(5 + s, m - R + 1), sp);
         sm = fma(alpha[s], Qv(5 + s, m - R + 1) * Fv(0, m - R + 1), sm);
       }
@@ -136,7 +140,7 @@ __device__ __forceinline__ void char_flux(const double *__restrict__ sQ, const d
   }
   if constexpr (NS > 0) {
 #pragma unroll 1
-    for (int s = 0; s < NS; ++s) {
+    for (int s = 0; s < NSC; ++s) {
       double vp[NW], vmn[NW];
 #pragma unroll
       for (int m = 0; m < 2 * R; ++m) {
@@ -162,7 +166,7 @@ __device__ __forceinline__ void char_flux(const double *__restrict__ sQ, const d
   if constexpr (NS > 0) {
     double e = 0;
 #pragma unroll
-    for (int s = 0; s < NS; ++s) {
+    for (int s = 0; s < NSC; ++s) {
       fc[5 + s] = svm[s] * f034 + fch[5 + s];
       e += ecoef[s] * fch[5 + s];
     }
@@ -173,9 +177,9 @@ __device__ __forceinline__ void char_flux(const double *__restrict__ sQ, const d
 }
 
 // Loads node data of one slot: conservative variables, U_k, momentum fluxes, p, c|grad k|, J.
-template <int NS, int DIR>
+template <int NS, int DIR, bool TT = false>
 __device__ __forceinline__ void load_node(const Zone &z, idx_t g, double *sQ, double *sF, int NN, int slot) {
-  constexpr int NV = 5 + NS;
+  constexpr int NV = 5 + NS + (TT ? 1 : 0);
   const idx_t sz = z.L.sz;
   const double q0 = z.cv[g], q1 = z.cv[g + sz], q2 = z.cv[g + 2 * sz], q3 = z.cv[g + 3 * sz], q4 = z.cv[g + 4 * sz];
   const double m0 = z.metric[g + (3 * DIR) * sz], m1 = z.metric[g + (3 * DIR + 1) * sz],
@@ -204,7 +208,8 @@ __device__ __forceinline__ void load_node(const Zone &z, idx_t g, double *sQ, do
 // Positivity limiter of the species rows of an interface flux (src/WENO.cu:1459-1528): with
 // alpha = 1/3 (3-D) or 1/2, every species flux is blended with a first-order flux f1 by
 // theta = min(theta_p, theta_m) so that the one-sided updates alpha J rhoY -+ dt f of the left
-// and right nodes stay non-negative.  Slots cl / cr of the left / right node.
+// and right nodes stay non-negative; NS counts every transported scalar (species and, in two
+// temperatures, e_ve).  Slots cl / cr of the left / right node.
 template <int NS>
 __device__ __forceinline__ void positive_limit(const double *sQ, const double *sF, int NN, int cl, int cr,
                                                const Param &p, double *fc) {
@@ -255,9 +260,9 @@ __device__ __forceinline__ void positive_limit(const double *sQ, const double *s
   }
 }
 
-template <int NS, int DIR, int ORDER>
+template <int NS, int DIR, int ORDER, bool TT = false>
 __global__ void __launch_bounds__(kSweepThreads) k_weno_char(Zone z, Param p, idx_t run) {
-  constexpr int NV = 5 + NS;
+  constexpr int NV = 5 + NS + (TT ? 1 : 0);
   constexpr int R = ORDER / 2 + 1;
   constexpr int NN = DIR == 0 ? (kSweepThreads + 2 * R - 1) : kTI * (kTS + 2 * R - 1);
   extern __shared__ double smem[];
@@ -280,7 +285,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_weno_char(Zone z, Param p, id
     const idx_t qmin = -(idx_t)g * L.disp2, qmax = (idx_t)(L.my + g) * L.disp2;
     for (int s = tid; s < NN; s += kSweepThreads) {
       const idx_t q = qlo + s;
-      if (q >= qmin && q < qmax) load_node<NS, 0>(z, base + q, sQ, sF, NN, s);
+      if (q >= qmin && q < qmax) load_node<NS, 0, TT>(z, base + q, sQ, sF, NN, s);
     }
     const idx_t q = q0 + tid;
     const idx_t jj = q >= 0 ? q / L.disp2 : -1;
@@ -299,7 +304,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_weno_char(Zone z, Param p, id
       const int n = s0 - R + s;  // sweep index of this node slot
       if (i < L.mx && n < ms + g) {
         const idx_t gi = DIR == 1 ? L.at(i, n, k) : L.at(i, j, n);
-        load_node<NS, DIR>(z, gi, sQ, sF, NN, s * kTI + ti);
+        load_node<NS, DIR, TT>(z, gi, sQ, sF, NN, s * kTI + ti);
       }
     }
     const int n_if = s0 - 1 + ts;  // interface n_if + 1/2
@@ -328,9 +333,9 @@ __global__ void __launch_bounds__(kSweepThreads) k_weno_char(Zone z, Param p, id
       }
     }
     double fc[NV];
-    char_flux<NS, ORDER>(sQ, sF, NN, c, st, kx, ky, kz, kWenoEps * p.weno_eps_scale, shock, p.mech, fc);
+    char_flux<NS, ORDER, TT>(sQ, sF, NN, c, st, kx, ky, kz, kWenoEps * p.weno_eps_scale, shock, p.mech, fc);
     if constexpr (NS > 0) {
-      if (p.positive_preserving) positive_limit<NS>(sQ, sF, NN, c, c + st, p, fc);
+      if (p.positive_preserving) positive_limit<NS + (TT ? 1 : 0)>(sQ, sF, NN, c, c + st, p, fc);
     }
 #pragma unroll
     for (int v = 0; v < NV; ++v) sFl[v * kSweepThreads + tid] = fc[v];
@@ -532,9 +537,9 @@ int launch_inviscid_comp(const Zone &z, const Param &p, cudaStream_t s, int &n_l
   }
 }
 
-template <int NS, int ORDER>
+template <int NS, int ORDER, bool TT = false>
 static int launch_dir(int dir, const Zone &z, const Param &p, cudaStream_t s) {
-  constexpr int NV = 5 + NS;
+  constexpr int NV = 5 + NS + (TT ? 1 : 0);
   constexpr int R = ORDER / 2 + 1;
   SweepGeom geo;
   const dim3 grid = sweep_grid(dir, z.L, geo);
@@ -543,26 +548,26 @@ static int launch_dir(int dir, const Zone &z, const Param &p, cudaStream_t s) {
   static const char *names[3] = {"weno_char_x", "weno_char_y", "weno_char_z"};
   ProfScope prof(names[dir], s);
   if (dir == 0) {
-    auto kern = k_weno_char<NS, 0, ORDER>;
+    auto kern = k_weno_char<NS, 0, ORDER, TT>;
     CB2_TRY(prepare_smem(kern, smem));
     kern<<<grid, kSweepThreads, smem, s>>>(z, p, geo.run);
   } else if (dir == 1) {
-    auto kern = k_weno_char<NS, 1, ORDER>;
+    auto kern = k_weno_char<NS, 1, ORDER, TT>;
     CB2_TRY(prepare_smem(kern, smem));
     kern<<<grid, kSweepThreads, smem, s>>>(z, p, 0);
   } else {
-    auto kern = k_weno_char<NS, 2, ORDER>;
+    auto kern = k_weno_char<NS, 2, ORDER, TT>;
     CB2_TRY(prepare_smem(kern, smem));
     kern<<<grid, kSweepThreads, smem, s>>>(z, p, 0);
   }
   return check_launch();
 }
 
-template <int NS>
+template <int NS, bool TT = false>
 static int launch_char_ns(const Zone &z, const Param &p, int order, cudaStream_t s, int &n_launch) {
   const int ndir = z.mz > 1 ? 3 : 2;
   for (int d = 0; d < ndir; ++d) {
-    int rc = order == 5 ? launch_dir<NS, 5>(d, z, p, s) : launch_dir<NS, 7>(d, z, p, s);
+    int rc = order == 5 ? launch_dir<NS, 5, TT>(d, z, p, s) : launch_dir<NS, 7, TT>(d, z, p, s);
     if (rc) return rc;
     ++n_launch;
   }
@@ -571,6 +576,11 @@ static int launch_char_ns(const Zone &z, const Param &p, int order, cudaStream_t
 
 int launch_inviscid_char(const Zone &z, const Param &p, cudaStream_t s, int &n_launch) {
   const int order = (p.inviscid_scheme == CB2_INV_WENO5_CH) ? 5 : 7;
+  if (p.i_eve >= 0) {
+    if (p.n_spec == 5) return launch_char_ns<5, true>(z, p, order, s, n_launch);
+    if (p.n_spec == 9) return launch_char_ns<9, true>(z, p, order, s, n_launch);
+    return CB2_ERR_UNSUPPORTED;
+  }
   switch (p.n_spec) {
     case 0: return launch_char_ns<0>(z, p, order, s, n_launch);
     case 5: return launch_char_ns<5>(z, p, order, s, n_launch);

@@ -345,4 +345,41 @@ __device__ __forceinline__ void vt_relax_point(const Zone &z, const Param &p, id
   temperature_2t<NS>(z, p, g, z.cv[g + 4 * sz]);
 }
 
+// Roe-state characteristic thermo of the two-temperature model (src/Thermo.cuh:49-110 with
+// two_temperature on): gamma and c of the translational-rotational mode, h_tr = h - e_ve(T),
+// cp_tr = cp - cv_ve(T); the species rows alpha_s and energy coefficients as in one temperature,
+// and the e_ve scalar's row alpha = -(gamma - 1)/c^2 with energy coefficient 1.
+template <int NS>
+__device__ __forceinline__ void characteristic_thermo_2t(double t, const double *y, const Mech &m, double &gamma,
+                                                         double &c, double *alpha, double *ecoef) {
+  const double te = fmax(t, 1.0);
+  double h[NS], cp[NS], htr[NS];
+  species_h_cp<NS>(te, m, h, cp);
+  double r = 0, cpm = 0, cvm = 0;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    double cv_ve;
+    const double e_ve = ve_energy(s, te, m, &cv_ve);
+    const double rs = __ldg(m.gas_const + s);
+    htr[s] = h[s] - e_ve;
+    const double cp_tr = cp[s] - cv_ve;
+    r += y[s] * rs;
+    cpm += y[s] * cp_tr;
+    cvm += y[s] * (cp_tr - rs);
+  }
+  gamma = cpm / fmax(cvm, 1e-8);
+  c = sqrt(fmax(gamma * r * te, 1e-12));
+  const double gm1 = gamma - 1.0;
+  const double c2 = fmax(c * c, 1e-30);
+  const double inv_gm1 = 1.0 / fmax(gm1, 1e-12);
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const double a = (gamma * __ldg(m.gas_const + s) * te - gm1 * htr[s]) / c2;
+    alpha[s] = a;
+    ecoef[s] = -a * c2 * inv_gm1;
+  }
+  alpha[NS] = -gm1 / c2;
+  ecoef[NS] = 1.0;
+}
+
 }  // namespace cb2

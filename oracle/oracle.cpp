@@ -258,7 +258,8 @@ void weno_char_interface(const Param &p, int order, double Q[][8], double F[][8]
     for (int l = 0; l < ns; ++l) rg += svm[l] * p.mech.gas_const[l];
     const double temp3 = (rlc * F[4][ic] + rrc * F[4][ic + 1]) / std::max(rg, 1e-12);
     double gamma;
-    characteristic_thermo(temp3, svm, p.mech, &gamma, &cm, alpha, ecoef, nullptr);
+    if (p.i_eve >= 0) characteristic_thermo_2t(p, temp3, svm, &gamma, &cm, alpha, ecoef);
+    else characteristic_thermo(temp3, svm, p.mech, &gamma, &cm, alpha, ecoef, nullptr);
     gm1 = gamma - 1;
   }
   temp1 = 1.0 / std::sqrt(kx * kx + ky * ky + kz * kz);
@@ -379,8 +380,10 @@ void positive_limit(const Param &p, const double Q[][8], const double F[][8], in
   const double alpha = p.dim == 3 ? 1.0 / 3.0 : 0.5;
   const double jl = F[6][l], jr = F[6][l + 1];
   const double alphaL = 0.5 * alpha * jl, alphaR = 0.5 * alpha * jr;
+  // every transported scalar: the species and, in two temperatures, e_ve (src/WENO.cu:1471)
+  const int nsc = p.n_var - 5;
   int start = -1;
-  for (int s = 0; s < p.n_spec; ++s) {
+  for (int s = 0; s < nsc; ++s) {
     const double up = alphaL * Q[s + 5][l] - dt * fc[s + 5];
     const double um = alphaR * Q[s + 5][l + 1] + dt * fc[s + 5];
     if (up < 0 || um < 0) {
@@ -390,7 +393,7 @@ void positive_limit(const Param &p, const double Q[][8], const double F[][8], in
   }
   if (start < 0) return;
   const double U1 = F[0][l] * jl, U2 = F[0][l + 1] * jr;
-  for (int s = start; s < p.n_spec; ++s) {
+  for (int s = start; s < nsc; ++s) {
     double f1 = 0, theta_p = 1, theta_m = 1;
     bool have_f1 = false;
     const double yl = Q[s + 5][l], yr = Q[s + 5][l + 1];

@@ -145,3 +145,20 @@ def test_air5_box_oracle_viscous_two_temperature(oracle_lib, air5, tt):
     assert np.abs(b.a["dq"][5 + air5.ns]).max() > 0
     dt = oracle_lib.cfl_dt(p, b)
     assert 0 < dt < 1e-3
+
+
+def test_air5_box_oracle_step_two_temperature(oracle_lib, air5, tt):
+    """A whole oracle step of the AIR5 box with every two-temperature term: finite and T_ve moves
+    towards T (the VT relaxation and the e_ve conduction act)."""
+    case = cases.air5_box_2t(air5, tt, n_nodes=6, viscous_order=2)
+    p, b, faces = case.param, case.blocks[0], case.faces[0]
+    oracle_lib.cv_from_bv(p, b)
+    oracle_lib.properties(p, b)
+    g = b.ngg
+    inner = (0, slice(g, -g), slice(g, -g), slice(g, -g))
+    gap0 = (b.a["bv"][5] - b.a["temperature_ve"][0])[inner[1:]]
+    for _ in range(3):
+        oracle_lib.rk3_step(p, [b], [faces], 2e-9, True)
+    assert np.isfinite(b.a["cv"]).all()
+    gap = (b.a["bv"][5] - b.a["temperature_ve"][0])[inner[1:]]
+    assert np.abs(gap).mean() < np.abs(gap0).mean()

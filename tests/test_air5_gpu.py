@@ -134,3 +134,36 @@ def test_cfl_two_temperature_parity(oracle_lib, air5, tt):
     dt = ctx.cfl_dt()
     ref = oracle_lib.cfl_dt(p, b)
     assert abs(dt - ref) <= 1e-13 * ref
+
+
+@pytest.mark.parametrize("scheme,ngg", [(abi.INV_WENO5_CH, 3), (abi.INV_WENO7_CH, 4)], ids=["weno5_ch", "weno7_ch"])
+def test_inviscid_char_two_temperature_parity(oracle_lib, air5, tt, scheme, ngg):
+    """Characteristic WENO with rho e_ve as a scalar row and the trans-rot Roe-state thermo."""
+    p, b, faces, dev, ctx = _setup(oracle_lib, air5, tt, n=10, scheme=scheme, ngg=ngg)
+    oracle_lib.properties(p, b)
+    dev.load(b, ["gamma", "acoustic_speed", "mach", "mul", "thermal_conductivity", "rho_D"])
+    ctx.rhs(0, abi.RHS_INVISCID)
+    _sync()
+    oracle_lib.rhs(p, b, faces, abi.RHS_INVISCID)
+    out = dev.to_host(["dq"])
+    assert helpers.rel_err(out["dq"], b.a["dq"]) < 1e-11
+    assert np.abs(b.a["dq"][5 + air5.ns]).max() > 0
+
+
+def test_rk3_step_two_temperature_parity(oracle_lib, air5, tt):
+    """Whole SSP-RK3 steps of the two-temperature AIR5 box: WENO5-ch fluxes with the e_ve row,
+    2nd-order viscous terms with the e_ve conduction, Park chemistry with the e_ve source, the
+    stage update with the VT relaxation, periodic ghost fill and the two-temperature properties."""
+    p, b, faces, dev, ctx = _setup(oracle_lib, air5, tt, n=8, viscous_order=2)
+    oracle_lib.properties(p, b)
+    dev.load(b, list(PROPS))
+    dt = 2e-9
+    for _ in range(2):
+        ctx.rk3_step(dt, fixed_dt=True)
+        oracle_lib.rk3_step(p, [b], [faces], dt, True)
+    _sync()
+    assert ctx.read_status() == 0
+    g = b.ngg
+    out = dev.to_host(["cv", "bv", "sv", "temperature_ve"])
+    for n in ("cv", "bv", "sv", "temperature_ve"):
+        assert helpers.rel_err(_inner(out[n], g), _inner(b.a[n], g)) < 1e-10, n

@@ -94,10 +94,11 @@ def test_vt_relaxation_parity(oracle_lib, h2, tt):
 
 
 def test_two_temperature_context_refuses_unbuilt_paths(oracle_lib, h2, tt):
-    """The inviscid two-temperature flux is not built: the residual with it, the boundary fill and
-    the whole step refuse the context; the chemistry-only residual runs."""
+    """The two-temperature primitive-variable (HLLC) flux is not built: the residual with it and the
+    whole step refuse the context; the chemistry-only residual and the periodic ghost fill run."""
     p, b, faces, dev, ctx = _setup(oracle_lib, h2, tt)
-    for call in (lambda: ctx.rhs(0), lambda: ctx.rhs(0, abi.RHS_INVISCID), lambda: ctx.boundary(0),
+    ctx.boundary(0)
+    for call in (lambda: ctx.rhs(0), lambda: ctx.rhs(0, abi.RHS_INVISCID),
                  lambda: ctx.rk3_step(1e-9, fixed_dt=True)):
         with pytest.raises(cb200.CB2Error) as e:
             call()
