@@ -88,6 +88,9 @@ def parse():
     ap.add_argument("--batch-blocks", type=int, default=296, help="blocks of the batched-blocks form")
     ap.add_argument("--batch-steps", type=int, default=5, help="steps of the batched-blocks form")
     ap.add_argument("--reacting-n", type=int, default=192, help="nodes per side of the reacting H2/air box")
+    ap.add_argument("--no-air5", action="store_true", help="skip the two-temperature AIR5 box")
+    ap.add_argument("--air5-n", type=int, default=80, help="nodes per side of the two-temperature AIR5 box")
+    ap.add_argument("--air5-steps", type=int, default=5, help="timed steps of the two-temperature AIR5 box")
     ap.add_argument("--reacting-steps", type=int, default=5, help="timed steps of the reacting H2/air box")
     ap.add_argument("--serve-seconds", type=float, default=0.05,
                     help="length of the seeded Poisson arrival window of the served workload")
@@ -386,6 +389,7 @@ def gpu_arm(args, rank, world, local_rank):
     torch.cuda.empty_cache()
     reacting = None if args.no_reacting else reacting_box(args, local_rank)
     batched = None if args.no_batch else batched_blocks(args, local_rank)
+    air5 = None if args.no_air5 else air5_box(args, local_rank)
     served = None if args.no_serve else serve_workload(args)
     if dist:
         dist.barrier()
@@ -406,7 +410,7 @@ def gpu_arm(args, rank, world, local_rank):
                        "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
             "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
             "clocks": clocks, "status_flags": status, "mixed": mixed, "serve": served, "reacting_box": reacting,
-            "batched_blocks": batched,
+            "batched_blocks": batched, "two_temperature_air5": air5,
             "kernel_ms_per_step": {k: v[1] for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
             "kernel_rooflines": kernel_roofs}
     print(json.dumps(line), flush=True)
@@ -548,6 +552,63 @@ def reacting_box(args, local_rank):
                      "kernel_ms_per_step": {k: v[1] for k, v in top}}
     out["speedup_mixed_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
     del dev, init
+    torch.cuda.empty_cache()
+    return out
+
+
+def air5_box(args, local_rank):
+    """The two-temperature AIR5 box (3-D periodic, --air5-n nodes per side; 80^3 = 0.51 M nodes,
+    the node count of the 1024 x 512 square-cylinder grid): post-shock air at 20 kPa, T = 6000 K
+    with 2500 K hot spots, T_ve = 0.45 T + 600 K, partly dissociated (N2, O2, NO, N, O), random
+    400 m/s velocity; characteristic WENO5 with the rho e_ve row, 2nd-order viscous terms with
+    the e_ve conduction, Park's 17 reactions with the AIR5 control temperatures and the e_ve
+    source, VT relaxation in every stage, NASA9 thermo; FP64, fixed dt = 2e-9 s.  The state is
+    completed on the device (cb2_cv_from_bv: cv and e_ve from the primitives and T_ve)."""
+    import torch
+    import cb200
+    from cb200 import cases
+    from cb200 import mech as mechmod
+    from cb200.field import DeviceBlock
+    gold = os.path.join(REPO, "tests", "golden", "air5_park.json")
+    air5 = mechmod.load_json(gold)
+    tt = mechmod.load_two_temperature_json(gold)
+    case = cases.air5_box_2t(air5, tt, n_nodes=args.air5_n, viscous_order=2)
+    p, hb, faces = case.param, case.blocks[0], case.faces[0]
+    p.positive_preserving = 1
+    dev = DeviceBlock(hb, device=f"cuda:{local_rank}")
+    del hb
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    ctx = cb200.Context(p)
+    ctx.bind(0, dev.view(), faces)
+    ctx.cv_from_bv(0, sh)
+    ctx.properties(0, sh)
+    dt = 2e-9
+    for _ in range(2):
+        ctx.rk3_step(dt, True, sh)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.air5_steps):
+        ctx.rk3_step(dt, True, sh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.air5_steps
+    ctx.profile(True)
+    ctx.rk3_step(dt, True, sh)
+    torch.cuda.synchronize()
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    status = ctx.read_status(sh)
+    ctx.close()
+    top = sorted(prof.items(), key=lambda kv: -kv[1][1])[:8]
+    nodes = args.air5_n ** 3
+    out = {"workload": f"two-temperature AIR5 box {args.air5_n}^3 nodes, WENO5-ch with the rho e_ve row, "
+                       f"2nd-order viscous, Park chemistry (5 species, 17 reactions), VT relaxation, NASA9, "
+                       f"fixed dt 2e-9 s, FP64", "steps": args.air5_steps,
+           "value": nodes / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "status_flags": status,
+           "kernel_ms_per_step": {k: v[1] for k, v in top}}
+    del dev
     torch.cuda.empty_cache()
     return out
 
