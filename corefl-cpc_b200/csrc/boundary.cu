@@ -42,6 +42,9 @@ __global__ void k_bc_outflow(Zone z, Param p, FaceBC f) {
     const idx_t gg = z.L.at(i + gl * d[0], j + gl * d[1], k + gl * d[2]);
     for (int l = 0; l < 6; ++l) z.bv[gg + l * sz] = z.bv[gb + l * sz];
     for (int l = 0; l < p.n_scalar; ++l) z.sv[gg + l * sz] = z.sv[gb + l * sz];
+    // two-temperature: the ghost T_ve (the starting guess of its inversion from e_ve) is the
+    // face node's, or its T when unset (src/BoundCond.cu:2339-2345)
+    if (p.i_eve >= 0) z.tve[gg] = z.tve[gb] > 0.0 ? z.tve[gb] : z.bv[gb + 5 * sz];
     cv_point<NS>(z, p, gg);
   }
 }

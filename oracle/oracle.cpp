@@ -1938,6 +1938,8 @@ void apply_boundary_conditions(Zone &z, const Param &p) {
                 const int gi = i + g * dir[0], gj = j + g * dir[1], gk = k + g * dir[2];
                 for (int l = 0; l < 6; ++l) z.bv(gi, gj, gk, l) = z.bv(i, j, k, l);
                 for (int l = 0; l < p.n_scalar; ++l) z.sv(gi, gj, gk, l) = z.sv(i, j, k, l);
+                // two-temperature ghost T_ve, the starting guess of its inversion (:2339-2345)
+                if (p.i_eve >= 0) z.tve(gi, gj, gk) = z.tve(i, j, k) > 0.0 ? z.tve(i, j, k) : z.bv(i, j, k, 5);
                 cv_point(z, p, gi, gj, gk);
               }
             } else if (type == CB2_BC_INFLOW) {  // constant supersonic state

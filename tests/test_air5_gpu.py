@@ -167,3 +167,27 @@ def test_rk3_step_two_temperature_parity(oracle_lib, air5, tt):
     out = dev.to_host(["cv", "bv", "sv", "temperature_ve"])
     for n in ("cv", "bv", "sv", "temperature_ve"):
         assert helpers.rel_err(_inner(out[n], g), _inner(b.a[n], g)) < 1e-10, n
+
+
+def test_rk3_step_two_temperature_outflow_parity(oracle_lib, air5, tt):
+    """The same steps with outflow faces along x (zeroth-order extrapolation of bv and every scalar,
+    the ghost T_ve starting its inversion from the face node's)."""
+    case = cases.air5_box_2t(air5, tt, n_nodes=8, viscous_order=2)
+    p, b, faces = case.param, case.blocks[0], case.faces[0]
+    for f in faces:
+        if f.face == 0:
+            f.type = abi.BC_OUTFLOW
+    oracle_lib.cv_from_bv(p, b)
+    oracle_lib.properties(p, b)
+    dev = DeviceBlock(b)
+    ctx = cb200.Context(p)
+    ctx.bind(0, dev.view(), faces)
+    for _ in range(2):
+        ctx.rk3_step(2e-9, fixed_dt=True)
+        oracle_lib.rk3_step(p, [b], [faces], 2e-9, True)
+    _sync()
+    assert ctx.read_status() == 0
+    g = b.ngg
+    out = dev.to_host(["cv", "bv", "sv", "temperature_ve"])
+    for n in ("cv", "bv", "sv", "temperature_ve"):
+        assert helpers.rel_err(_inner(out[n], g), _inner(b.a[n], g)) < 1e-10, n
