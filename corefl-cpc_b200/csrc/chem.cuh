@@ -41,13 +41,38 @@ __device__ __forceinline__ double reaction_temperature(double t, double tve, dou
 // equilibrium constant); temp_t = p_atm / (R_u T) * 1e-3.  With the mechanism's
 // control-temperature model the forward rate runs at smooth(T^tcf_a Tve^tcf_b) and the backward
 // rate at smooth(T^tcb_a Tve^tcb_b), its g/(RT) evaluated there (gibbs is then unused).
+// The control temperatures and the backward g/(RT) of the last reaction, reused by the next one
+// when its exponents are the same (the AIR5 model has two forward pairs and one backward pair):
+// the same inputs give the same values, so the rates do not change.
+template <int NS>
+struct ParkCache {
+  double fa, fb, tf, ba, bb, tb;
+  bool have_g;
+  double g[NS];
+  __device__ __forceinline__ ParkCache() {
+    const double qnan = __longlong_as_double(0x7ff8000000000000ll);
+    fa = fb = ba = bb = qnan;
+    tf = tb = 0;
+    have_g = false;
+  }
+};
+
 template <int NS>
 __device__ __forceinline__ void reaction_progress(int r, double t0, double tve, const double *c,
                                                   const double *gibbs, double temp_t, const Mech &m,
-                                                  double &q1_out, double &q2_out) {
+                                                  double &q1_out, double &q2_out, ParkCache<NS> *pc = nullptr) {
   const int ty = __ldg(m.reac_type + r);
   const int *sf = m.stoi_f + r * NS, *sb = m.stoi_b + r * NS;
-  const double t = m.park ? reaction_temperature(t0, tve, __ldg(m.tcf_a + r), __ldg(m.tcf_b + r)) : t0;
+  double t = t0;
+  if (m.park) {
+    const double a = __ldg(m.tcf_a + r), b = __ldg(m.tcf_b + r);
+    if (pc && pc->fa == a && pc->fb == b) {
+      t = pc->tf;
+    } else {
+      t = reaction_temperature(t0, tve, a, b);
+      if (pc) { pc->fa = a; pc->fb = b; pc->tf = t; }
+    }
+  }
   // forward rate
   double kf = arrhenius(t, __ldg(m.A + r), __ldg(m.b + r), __ldg(m.Ea + r));
   double cc = 0;
@@ -85,13 +110,29 @@ __device__ __forceinline__ void reaction_progress(int r, double t0, double tve, 
   double kb = 0;
   if (m.park) {
     if (ty != 0) {
-      const double thb = reaction_temperature(t0, tve, __ldg(m.tcb_a + r), __ldg(m.tcb_b + r));
+      const double a = __ldg(m.tcb_a + r), b = __ldg(m.tcb_b + r);
+      double thb;
+      if (pc && pc->ba == a && pc->bb == b) {
+        thb = pc->tb;
+      } else {
+        thb = reaction_temperature(t0, tve, a, b);
+        if (pc) { pc->ba = a; pc->bb = b; pc->tb = thb; pc->have_g = false; }
+      }
       if (__ldg(m.rev_type + r) == 1) {
         kb = arrhenius(thb, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
         if (ty == 4) kb *= cc;
       } else {
-        double g[NS];
-        species_gibbs_rt<NS>(thb, m, g);
+        double gl[NS];
+        const double *g = gl;
+        if (pc) {
+          if (!pc->have_g) {
+            species_gibbs_rt<NS>(thb, m, pc->g);
+            pc->have_g = true;
+          }
+          g = pc->g;
+        } else {
+          species_gibbs_rt<NS>(thb, m, gl);
+        }
         double dg = 0;
 #pragma unroll
         for (int s = 0; s < NS; ++s) dg += g[s] * (__ldg(sb + s) - __ldg(sf + s));
@@ -147,19 +188,38 @@ __device__ __forceinline__ void chem_rates(double t, double tve, const double *c
 #pragma unroll
   for (int s = 0; s < NS; ++s) creation[s] = destruction[s] = 0;
 
-  for (int r = 0; r < m.n_reac; ++r) {
-    double q1, q2;
-    reaction_progress<NS>(r, t, tve, c, gibbs, temp_t, m, q1, q2);
-    if (q1r) {
-      q1r[r] = q1;
-      q2r[r] = q2;
-    }
-    const int *sf = m.stoi_f + r * NS, *sb = m.stoi_b + r * NS;
+  if (m.park) {
+    ParkCache<NS> pc;
+    for (int r = 0; r < m.n_reac; ++r) {
+      double q1, q2;
+      reaction_progress<NS>(r, t, tve, c, gibbs, temp_t, m, q1, q2, &pc);
+      if (q1r) {
+        q1r[r] = q1;
+        q2r[r] = q2;
+      }
+      const int *sf = m.stoi_f + r * NS, *sb = m.stoi_b + r * NS;
 #pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      const double f = __ldg(sf + s), b = __ldg(sb + s);
-      creation[s] += q2 * f + q1 * b;
-      destruction[s] += q1 * f + q2 * b;
+      for (int s = 0; s < NS; ++s) {
+        const double f = __ldg(sf + s), b = __ldg(sb + s);
+        creation[s] += q2 * f + q1 * b;
+        destruction[s] += q1 * f + q2 * b;
+      }
+    }
+  } else {
+    for (int r = 0; r < m.n_reac; ++r) {
+      double q1, q2;
+      reaction_progress<NS>(r, t, tve, c, gibbs, temp_t, m, q1, q2);
+      if (q1r) {
+        q1r[r] = q1;
+        q2r[r] = q2;
+      }
+      const int *sf = m.stoi_f + r * NS, *sb = m.stoi_b + r * NS;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const double f = __ldg(sf + s), b = __ldg(sb + s);
+        creation[s] += q2 * f + q1 * b;
+        destruction[s] += q1 * f + q2 * b;
+      }
     }
   }
 }
