@@ -309,10 +309,11 @@ bool two_temperature_step(const cb2_ctx *ctx) {
 
 // The residual terms built for two-temperature contexts: the chemistry source with the control
 // temperatures and the e_ve source, the 2nd-order viscous fluxes with the e_ve terms, and the
-// characteristic WENO fluxes with rho e_ve as a scalar row.
+// characteristic WENO fluxes with rho e_ve as a scalar row.  An inviscid context has no viscous
+// term to build, so asking for it (CB2_RHS_ALL) is no refusal.
 unsigned two_temperature_rhs_terms(const cb2_ctx *ctx) {
   unsigned m = CB2_RHS_CHEMISTRY;
-  if (ctx->p.viscous_order == 2) m |= CB2_RHS_VISCOUS;
+  if (ctx->p.viscous_order == 2 || ctx->p.viscous_order == 0) m |= CB2_RHS_VISCOUS;
   if (ctx->p.inviscid_scheme == CB2_INV_WENO5_CH || ctx->p.inviscid_scheme == CB2_INV_WENO7_CH) m |= CB2_RHS_INVISCID;
   return m;
 }

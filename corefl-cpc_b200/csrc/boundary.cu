@@ -340,7 +340,11 @@ static int launch_bc_ns(const Zone &z, const Param &p, const FaceBC *faces, int 
   for (int t : order) {
     for (int f = 0; f < n; ++f) {
       if (faces[f].type != t) continue;
-      if (t == CB2_BC_PERIODIC) {
+      // Two temperatures: face by face, as the reference.  Rebuilding cv syncs e_ve and T_ve
+      // (sync_two_temperature_state_from_sv), and the reference's order of those syncs -- the low
+      // face's nodes and ghosts first, then the high face averaging with the synced low nodes --
+      // decides T_ve wherever e_ve and T_ve disagree on entry (an e_ve left at zero).
+      if (t == CB2_BC_PERIODIC && p.i_eve < 0) {
         int q = -1;
         const int lf = periodic_pair(z, faces, n, f, &q);
         if (lf >= 0) {

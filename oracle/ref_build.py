@@ -6,7 +6,8 @@ Compiles, straight from the reference source tree (never copied into this reposi
               single-process oracle/ref/mpi.h, oracle/ref/stubs.cpp and
               oracle/ref/dump_mech.cpp; it writes the mechanism tables as JSON.
 The reference's CMake build needs MPI and is not used.
-Usage: python oracle/ref_build.py [/path/to/reference]
+Usage: python oracle/ref_build.py [/path/to/reference]   (default: $COREFL_REFERENCE, else
+DEFAULT_REFERENCE below)
 """
 import os
 import subprocess
@@ -14,12 +15,22 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
+# where the reference checkout lives in the build container; $COREFL_REFERENCE overrides it
+DEFAULT_REFERENCE = "/root/reference"
 
 
-def build(ref="/root/reference", force=False):
-    src = os.path.join(ref, "src")
-    if not os.path.isdir(src):
+def reference_dir(ref=None):
+    """The reference source tree: `ref`, else $COREFL_REFERENCE, else DEFAULT_REFERENCE; None if
+    it holds no src/ directory (as on a machine without the reference)."""
+    ref = ref or os.environ.get("COREFL_REFERENCE") or DEFAULT_REFERENCE
+    return ref if os.path.isdir(os.path.join(ref, "src")) else None
+
+
+def build(ref=None, force=False):
+    ref = reference_dir(ref)
+    if ref is None:
         return None
+    src = os.path.join(ref, "src")
     os.makedirs(OUT, exist_ok=True)
     exe = os.path.join(OUT, "dump_mech")
     mine = [os.path.join(HERE, "ref", f) for f in ("stubs.cpp", "dump_mech.cpp", "mpi.h")]
@@ -73,4 +84,4 @@ def build(ref="/root/reference", force=False):
 
 
 if __name__ == "__main__":
-    print(build(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", force=True))
+    print(build(sys.argv[1] if len(sys.argv) > 1 else None, force=True))

@@ -4,7 +4,8 @@ Reads (never at test time) the reference's own known-answer files and writes sma
 fixtures next to this script:
   sod_exact.txt  <- example/sodShockTube/exact.dat (exact Sod solution at t = 0.2:
                     x, u, rho, p on 2000 points; every 4th point is kept)
-Usage: python tests/golden/make_golden.py [/path/to/reference]
+Usage: python tests/golden/make_golden.py [/path/to/reference]  (default: oracle/ref_build.py's
+reference_dir())
 """
 import os
 import sys
@@ -35,4 +36,9 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "oracle"))
+    import ref_build
+    ref = ref_build.reference_dir(sys.argv[1] if len(sys.argv) > 1 else None)
+    if ref is None:
+        sys.exit("reference sources not found: pass the path or set COREFL_REFERENCE")
+    main(ref)

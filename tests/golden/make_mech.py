@@ -25,7 +25,8 @@ oracle/ref_build.py) on the reference's example data files and keeps its JSON ou
                    and Newton through the adaptive ROK4E sequence (RTol 1e-6, ATol 1e-12,
                    first step 1e-8): the reference's example case to 1.2 ms and 8 seeded
                    (T0, p0, phi) requests to 1 ms, each after 8 step attempts and at the end
-Usage: python tests/golden/make_mech.py [/path/to/reference]
+Usage: python tests/golden/make_mech.py [/path/to/reference]  (default: oracle/ref_build.py's
+reference_dir())
 """
 import os
 import shutil
@@ -80,4 +81,9 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "oracle"))
+    import ref_build
+    ref = ref_build.reference_dir(sys.argv[1] if len(sys.argv) > 1 else None)
+    if ref is None:
+        sys.exit("reference sources not found: pass the path or set COREFL_REFERENCE")
+    main(ref)
