@@ -308,12 +308,12 @@ bool two_temperature_step(const cb2_ctx *ctx) {
 }
 
 // The residual terms built for two-temperature contexts: the chemistry source with the control
-// temperatures and the e_ve source, the 2nd-order viscous fluxes with the e_ve terms, and the
-// characteristic WENO fluxes with rho e_ve as a scalar row.  An inviscid context has no viscous
-// term to build, so asking for it (CB2_RHS_ALL) is no refusal.
+// temperatures and the e_ve source, the 2nd- and 8th-order viscous fluxes with the e_ve terms,
+// and the characteristic WENO fluxes with rho e_ve as a scalar row.
+// An inviscid context has no viscous term to build, so asking for it (CB2_RHS_ALL) is no refusal.
 unsigned two_temperature_rhs_terms(const cb2_ctx *ctx) {
   unsigned m = CB2_RHS_CHEMISTRY;
-  if (ctx->p.viscous_order == 2 || ctx->p.viscous_order == 0) m |= CB2_RHS_VISCOUS;
+  if (ctx->p.viscous_order == 2 || ctx->p.viscous_order == 8 || ctx->p.viscous_order == 0) m |= CB2_RHS_VISCOUS;
   if (ctx->p.inviscid_scheme == CB2_INV_WENO5_CH || ctx->p.inviscid_scheme == CB2_INV_WENO7_CH) m |= CB2_RHS_INVISCID;
   return m;
 }
@@ -398,7 +398,6 @@ int cb2_init(const cb2_param_view *pv, cb2_ctx **out) {
     if (!(r == 1 || r == 2 || r == 3 || r == 5 || r == 7)) return CB2_ERR_INVALID;
   }
   if (pv->viscous_order != 0 && pv->viscous_order != 2 && pv->viscous_order != 8) return CB2_ERR_INVALID;
-  if (pv->viscous_order == 8 && ns != 0) return CB2_ERR_UNSUPPORTED;
   // the positivity limiter acts on the species rows of the characteristic-WENO fluxes
   if (pv->positive_preserving && (ns == 0 || !(sch == CB2_INV_WENO5_CH || sch == CB2_INV_WENO7_CH)))
     return CB2_ERR_UNSUPPORTED;
@@ -623,7 +622,7 @@ int cb2_bind_block(cb2_ctx *ctx, int blk, const cb2_zone_view *v, const cb2_face
     const size_t sz = (size_t)B.z.L.sz;
     auto up = [](size_t n) { return (n + 63) / 64 * 64; };  // each copy starts on a 256-byte boundary
     const size_t off = up(6 * sz), offf = off + up(10 * sz);
-    const size_t nflux = p.viscous_order == 8 ? up((size_t)p.n_var * sz) : 0;
+    const size_t nflux = p.viscous_order == 8 && visc8_f32(p) ? up((size_t)p.n_var * sz) : 0;
     e = cudaMalloc(&B.d_f32, (offf + 3 * nflux) * sizeof(float));
     if (e != cudaSuccess) return fail_cuda(e);
     B.z.bv32 = B.d_f32;

@@ -403,7 +403,7 @@ int launch_periodic_flux_exchange(const Zone &z, const Param &p, const FaceBC *f
     if (lf >= 0) {
       const long long np = face_points(faces[lf]) * (2 * z.ngg + 1);
       ProfScope prof("periodic_flux_exchange", s);
-      if (p.precision == CB2_PREC_MIXED)
+      if (visc8_f32(p))
         k_periodic_flux_pair<float><<<(unsigned)((np + 127) / 128), 128, 0, s>>>(z, p, faces[lf]);
       else
         k_periodic_flux_pair<double><<<(unsigned)((np + 127) / 128), 128, 0, s>>>(z, p, faces[lf]);
@@ -416,7 +416,7 @@ int launch_periodic_flux_exchange(const Zone &z, const Param &p, const FaceBC *f
     const unsigned blocks = (unsigned)((np + 127) / 128);
     if (!blocks) continue;
     ProfScope prof("periodic_flux_exchange", s);
-    if (p.precision == CB2_PREC_MIXED) k_periodic_flux<float><<<blocks, 128, 0, s>>>(z, p, faces[f]);
+    if (visc8_f32(p)) k_periodic_flux<float><<<blocks, 128, 0, s>>>(z, p, faces[f]);
     else k_periodic_flux<double><<<blocks, 128, 0, s>>>(z, p, faces[f]);
     ++n_launch;
     CB2_TRY(check_launch());

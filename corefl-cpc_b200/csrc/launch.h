@@ -84,6 +84,9 @@ int launch_periodic_flux_exchange(const Zone &z, const Param &p, const FaceBC *f
 // The 8th-order air viscous term writes dq instead of adding to it (assign = true) when it runs
 // first in a residual; viscous_assigns_dq tells whether the settings take that path.
 bool viscous_assigns_dq(const Param &p);
+// Whether the 8th-order node fluxes live in the block's FP32 copies (the mixed form of air); the
+// node-flux, flux-exchange and divergence kernels all follow it.
+inline bool visc8_f32(const Param &p) { return p.precision == CB2_PREC_MIXED && p.n_spec == 0; }
 int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, bool assign, cudaStream_t s,
                    int &n_launch);
 int launch_chemistry(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);

@@ -11,8 +11,11 @@
 // CB2_NOALLOC_MAX_PARTIALS doubles that every GPU loading the library keeps until the process
 // exits.  Host code must not use the array's name as a device address, so the address is
 // resolved with cudaGetSymbolAddress once per device, on the first call made with that device
-// current; that first call should therefore come before any stream capture.  All calls share
-// the array, so calls whose kernels overlap on the GPU race with each other.
+// current; that first call should therefore come before any stream capture.  The resolved
+// address is kept per device ordinal for the life of the process: it assumes the device's primary
+// context (the runtime's own) and no cudaDeviceReset in between, after which the array would live
+// at a new address.  All calls share the array, so calls whose kernels overlap on the GPU race
+// with each other.
 #include <mutex>
 #include "common.cuh"
 #include "launch.h"
@@ -24,6 +27,9 @@ constexpr int kNaThreads = 256;
 constexpr int kNaPerThread = 8;                                // elements per thread
 constexpr long long kNaPerCta = (long long)kNaThreads * kNaPerThread;
 constexpr int kNaMaxDevices = 64;
+// every n the entry point accepts must fit its partial minima in the array
+static_assert(CB2_NOALLOC_MAX_NODES <= (long long)CB2_NOALLOC_MAX_PARTIALS * kNaPerCta,
+              "CB2_NOALLOC_MAX_NODES exceeds the partial-minimum capacity");
 
 static __device__ __align__(256) double g_noalloc_partials[CB2_NOALLOC_MAX_PARTIALS];
 

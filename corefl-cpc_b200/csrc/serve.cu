@@ -172,6 +172,11 @@ extern "C" int cb2_serve_run(cb2_ctx *ctx_reactor, cb2_ctx *ctx_tube, const cb2_
   Run R;
   int rc = need_t ? R.pool.init(opt->hbm_budget_bytes) : CB2_OK;
   if (rc) return rc;
+  // a tube whose state can never fit the pool would wait for memory forever once everything
+  // else has retired: refuse the run up front
+  for (int i = 0; i < n; ++i)
+    if (reqs[i].kind == CB2_REQ_TUBE && ((line_bytes(reqs[i].n_nodes, g, nst) + 255) & ~size_t(255)) > R.pool.size)
+      return CB2_ERR_NOMEM;
   auto cuda_ok = [](cudaError_t e) { return e == cudaSuccess; };
   if (!cuda_ok(cudaMalloc(&R.d_reac, sizeof(cb2_reactor) * max_reactors)) ||
       !cuda_ok(cudaMalloc(&R.d_line, sizeof(LineCase) * max_tubes)) ||

@@ -143,6 +143,177 @@ __global__ void __launch_bounds__(kVisThreads, 4) k_visc8_node_flux_air_f32(Zone
   visc8_node_flux_air<float>(z, p);
 }
 
+// Node fluxes of a thermally perfect mixture (compute_viscous_flux_collocated<Mixture,8> followed
+// by compute_viscous_flux_collocated_scalar<8>, src/ViscousScheme.cu:470-788), FP64: the stresses
+// and the conduction kappa grad T as for air (kappa from the property kernel), in two temperatures
+// kappa_ve grad T_ve added to the energy flux, then per species the mixture-averaged diffusion flux
+// J_k = rho D_k (grad Y_k - Y_k W grad(1/W)-term [+ the pressure term]) - Y_k V_c with the
+// correction velocity V_c, its enthalpy h_k J_k (two temperatures: h_k with e_ve at T_ve) added to
+// the energy flux, and in two temperatures the e_ve flux kappa_ve grad T_ve + sum e_ve,k J_k.
+// Every flux is projected on the node's grad xi / grad eta / grad zeta, as the reference stores
+// them; additions into the energy flux follow the reference's order (the collocated kernel's
+// stresses and conduction, then species by species).
+template <int NS, bool TT>
+__global__ void __launch_bounds__(kVisThreads) k_visc8_node_flux_mix(Zone z, Param p) {
+  const int i = blockIdx.x * kVisTI + threadIdx.x, j = blockIdx.y * kVisTJ + threadIdx.y, k = blockIdx.z;
+  if (i >= z.mx || j >= z.my) return;
+  const Layout &L = z.L;
+  const idx_t sz = L.sz, g = L.at(i, j, k);
+  const BFlags b = bflags(z, i, j, k);
+  const idx_t si = 1, sj = L.disp2, sk = L.disp1;
+  const double *M = z.metric + g;
+  auto der = [&](const double *f0, double &dxi, double &deta, double &dzeta) {
+    const double *f = f0 + g;
+    dxi = d8<double>([&](int m) { return f[m * si]; }, i, z.mx, b.il, b.ir);
+    deta = d8<double>([&](int m) { return f[m * sj]; }, j, z.my, b.jl, b.jr);
+    dzeta = d8<double>([&](int m) { return f[m * sk]; }, k, z.mz, b.kl, b.kr);
+  };
+  const double xi_x = M[0], xi_y = M[sz], xi_z = M[2 * sz];
+  const double eta_x = M[3 * sz], eta_y = M[4 * sz], eta_z = M[5 * sz];
+  const double zeta_x = M[6 * sz], zeta_y = M[7 * sz], zeta_z = M[8 * sz];
+  double *FF = z.fF, *GF = z.gF, *HF = z.hF;
+  double F4, G4, H4;
+  {
+    double u_xi, u_eta, u_zeta, v_xi, v_eta, v_zeta, w_xi, w_eta, w_zeta, t_xi, t_eta, t_zeta;
+    der(z.bv + sz, u_xi, u_eta, u_zeta);
+    der(z.bv + 2 * sz, v_xi, v_eta, v_zeta);
+    der(z.bv + 3 * sz, w_xi, w_eta, w_zeta);
+    der(z.bv + 5 * sz, t_xi, t_eta, t_zeta);
+    const double u_x = u_xi * xi_x + u_eta * eta_x + u_zeta * zeta_x;
+    const double u_y = u_xi * xi_y + u_eta * eta_y + u_zeta * zeta_y;
+    const double u_z = u_xi * xi_z + u_eta * eta_z + u_zeta * zeta_z;
+    const double v_x = v_xi * xi_x + v_eta * eta_x + v_zeta * zeta_x;
+    const double v_y = v_xi * xi_y + v_eta * eta_y + v_zeta * zeta_y;
+    const double v_z = v_xi * xi_z + v_eta * eta_z + v_zeta * zeta_z;
+    const double w_x = w_xi * xi_x + w_eta * eta_x + w_zeta * zeta_x;
+    const double w_y = w_xi * xi_y + w_eta * eta_y + w_zeta * zeta_y;
+    const double w_z = w_xi * xi_z + w_eta * eta_z + w_zeta * zeta_z;
+    const double mu = z.mul[g];
+    const double txx = mu * (4 * u_x - 2 * v_y - 2 * w_z) / 3.0;
+    const double tyy = mu * (4 * v_y - 2 * u_x - 2 * w_z) / 3.0;
+    const double tzz = mu * (4 * w_z - 2 * u_x - 2 * v_y) / 3.0;
+    const double txy = mu * (u_y + v_x), txz = mu * (u_z + w_x), tyz = mu * (v_z + w_y);
+    FF[g + sz] = xi_x * txx + xi_y * txy + xi_z * txz;
+    FF[g + 2 * sz] = xi_x * txy + xi_y * tyy + xi_z * tyz;
+    FF[g + 3 * sz] = xi_x * txz + xi_y * tyz + xi_z * tzz;
+    GF[g + sz] = eta_x * txx + eta_y * txy + eta_z * txz;
+    GF[g + 2 * sz] = eta_x * txy + eta_y * tyy + eta_z * tyz;
+    GF[g + 3 * sz] = eta_x * txz + eta_y * tyz + eta_z * tzz;
+    HF[g + sz] = zeta_x * txx + zeta_y * txy + zeta_z * txz;
+    HF[g + 2 * sz] = zeta_x * txy + zeta_y * tyy + zeta_z * tyz;
+    HF[g + 3 * sz] = zeta_x * txz + zeta_y * tyz + zeta_z * tzz;
+    const double t_x = t_xi * xi_x + t_eta * eta_x + t_zeta * zeta_x;
+    const double t_y = t_xi * xi_y + t_eta * eta_y + t_zeta * zeta_y;
+    const double t_z = t_xi * xi_z + t_eta * eta_z + t_zeta * zeta_z;
+    const double kap = z.kappa[g];
+    const double u = z.bv[g + sz], v = z.bv[g + 2 * sz], w = z.bv[g + 3 * sz];
+    const double Ex = u * txx + v * txy + w * txz + kap * t_x;
+    const double Ey = u * txy + v * tyy + w * tyz + kap * t_y;
+    const double Ez = u * txz + v * tyz + w * tzz + kap * t_z;
+    F4 = xi_x * Ex + xi_y * Ey + xi_z * Ez;
+    G4 = eta_x * Ex + eta_y * Ey + eta_z * Ez;
+    H4 = zeta_x * Ex + zeta_y * Ey + zeta_z * Ez;
+  }
+  double efx = 0, efy = 0, efz = 0;
+  if constexpr (TT) {
+    double v_xi, v_eta, v_zeta;
+    der(z.tve, v_xi, v_eta, v_zeta);
+    const double v_x = v_xi * xi_x + v_eta * eta_x + v_zeta * zeta_x;
+    const double v_y = v_xi * xi_y + v_eta * eta_y + v_zeta * zeta_y;
+    const double v_z = v_xi * xi_z + v_eta * eta_z + v_zeta * zeta_z;
+    const double kve = z.kappa_ve[g];
+    efx = kve * (xi_x * v_x + xi_y * v_y + xi_z * v_z);
+    efy = kve * (eta_x * v_x + eta_y * v_y + eta_z * v_z);
+    efz = kve * (zeta_x * v_x + zeta_y * v_y + zeta_z * v_z);
+    F4 += efx;
+    G4 += efy;
+    H4 += efz;
+  }
+  // species diffusion (the scalar kernel)
+  const Mech &m = p.mech;
+  double dif[NS], yk[NS], fx[NS], fy[NS], fz[NS];
+  double swx = 0, swy = 0, swz = 0, cx = 0, cy = 0, cz = 0, mwt = 0, srdy = 0;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    yk[s] = z.sv[g + s * sz];
+    dif[s] = z.rhoD[g + s * sz];
+    double y_xi, y_eta, y_zeta;
+    der(z.sv + s * sz, y_xi, y_eta, y_zeta);
+    const double y_x = y_xi * xi_x + y_eta * eta_x + y_zeta * zeta_x;
+    const double y_y = y_xi * xi_y + y_eta * eta_y + y_zeta * zeta_y;
+    const double y_z = y_xi * xi_z + y_eta * eta_z + y_zeta * zeta_z;
+    fx[s] = xi_x * y_x + xi_y * y_y + xi_z * y_z;
+    fy[s] = eta_x * y_x + eta_y * y_y + eta_z * y_z;
+    fz[s] = zeta_x * y_x + zeta_y * y_y + zeta_z * y_z;
+    cx += dif[s] * fx[s];
+    cy += dif[s] * fy[s];
+    cz += dif[s] * fz[s];
+    const double iw = __ldg(m.imw + s);
+    swx += fx[s] * iw;
+    swy += fy[s] * iw;
+    swz += fz[s] * iw;
+    mwt += yk[s] * iw;
+    srdy += dif[s] * yk[s];
+  }
+  mwt = 1.0 / mwt;
+  cx -= mwt * srdy * swx;
+  cy -= mwt * srdy * swy;
+  cz -= mwt * srdy * swz;
+  if (p.gradP) {
+    double p_xi, p_eta, p_zeta;
+    der(z.bv + 4 * sz, p_xi, p_eta, p_zeta);
+    const double p_x = p_xi * xi_x + p_eta * eta_x + p_zeta * zeta_x;
+    const double p_y = p_xi * xi_y + p_eta * eta_y + p_zeta * zeta_y;
+    const double p_z = p_xi * xi_z + p_eta * eta_z + p_zeta * zeta_z;
+    const double pg = z.bv[g + 4 * sz];
+    const double gpx = (xi_x * p_x + xi_y * p_y + xi_z * p_z) / pg;
+    const double gpy = (eta_x * p_x + eta_y * p_y + eta_z * p_z) / pg;
+    const double gpz = (zeta_x * p_x + zeta_y * p_y + zeta_z * p_z) / pg;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const double co = (mwt * __ldg(m.imw + s) - 1) * yk[s];
+      fx[s] += co * gpx;
+      fy[s] += co * gpy;
+      fz[s] += co * gpz;
+      cx += co * gpx * dif[s];
+      cy += co * gpy * dif[s];
+      cz += co * gpz * dif[s];
+    }
+  }
+  double h[NS];
+  const double tm = z.bv[g + 5 * sz];
+  species_h<NS>(tm, m, h);
+  const double tve_m = TT ? z.tve[g] : tm;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    double hd = h[s], ev = 0;
+    if constexpr (TT) {
+      hd = h[s] - ve_energy(s, tm, m, nullptr) + ve_energy(s, tve_m, m, nullptr);
+      ev = ve_energy(s, tve_m, m, nullptr);
+    }
+    double jd = dif[s] * (fx[s] - mwt * yk[s] * swx) - yk[s] * cx;
+    FF[g + (5 + s) * sz] = jd;
+    F4 += hd * jd;
+    if constexpr (TT) efx += ev * jd;
+    jd = dif[s] * (fy[s] - mwt * yk[s] * swy) - yk[s] * cy;
+    GF[g + (5 + s) * sz] = jd;
+    G4 += hd * jd;
+    if constexpr (TT) efy += ev * jd;
+    jd = dif[s] * (fz[s] - mwt * yk[s] * swz) - yk[s] * cz;
+    HF[g + (5 + s) * sz] = jd;
+    H4 += hd * jd;
+    if constexpr (TT) efz += ev * jd;
+  }
+  FF[g + 4 * sz] = F4;
+  GF[g + 4 * sz] = G4;
+  HF[g + 4 * sz] = H4;
+  if constexpr (TT) {
+    FF[g + (5 + NS) * sz] = efx;
+    GF[g + (5 + NS) * sz] = efy;
+    HF[g + (5 + NS) * sz] = efz;
+  }
+}
+
 // The divergence reads each flux array along one direction only; rows of kVisRow i-nodes
 // measured faster than 2-D tiles for it.
 constexpr int kVisRow = 128;
@@ -381,12 +552,27 @@ int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_fac
                    int &nl) {
   if (p.viscous_order == 0) return CB2_OK;
   if (p.viscous_order == 8) {
-    if (p.n_spec != 0) return CB2_ERR_UNSUPPORTED;
     const dim3 grid((z.mx + kVisTI - 1) / kVisTI, (z.my + kVisTJ - 1) / kVisTJ, z.mz), block(kVisTI, kVisTJ);
     {
       ProfScope prof("visc8_node_flux", s);
-      if (p.precision == CB2_PREC_MIXED) k_visc8_node_flux_air_f32<<<grid, block, 0, s>>>(z, p);
-      else k_visc8_node_flux_air_f64<<<grid, block, 0, s>>>(z, p);
+      if (p.n_spec == 0) {
+        if (p.precision == CB2_PREC_MIXED) k_visc8_node_flux_air_f32<<<grid, block, 0, s>>>(z, p);
+        else k_visc8_node_flux_air_f64<<<grid, block, 0, s>>>(z, p);
+      } else {
+        // mixtures: FP64 in both forms (their mixed form keeps the viscous terms in FP64)
+        if (!z.kappa || !z.rhoD || (p.i_eve >= 0 && (!z.tve || !z.kappa_ve))) return CB2_ERR_INVALID;
+        if (p.i_eve >= 0) {
+          if (p.n_spec == 5) k_visc8_node_flux_mix<5, true><<<grid, block, 0, s>>>(z, p);
+          else if (p.n_spec == 9) k_visc8_node_flux_mix<9, true><<<grid, block, 0, s>>>(z, p);
+          else return CB2_ERR_UNSUPPORTED;
+        } else if (p.n_spec == 5) {
+          k_visc8_node_flux_mix<5, false><<<grid, block, 0, s>>>(z, p);
+        } else if (p.n_spec == 9) {
+          k_visc8_node_flux_mix<9, false><<<grid, block, 0, s>>>(z, p);
+        } else {
+          return CB2_ERR_UNSUPPORTED;
+        }
+      }
     }
     ++nl;
     CB2_TRY(check_launch());
@@ -395,7 +581,7 @@ int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_fac
       ProfScope prof("visc8_divergence", s);
       // the mixed form sums the FP32 node fluxes in FP32 and adds the result to the FP64 dq
       const dim3 grow((z.mx + kVisRow - 1) / kVisRow, z.my, z.mz);
-      if (p.precision == CB2_PREC_MIXED) {
+      if (visc8_f32(p)) {
         if (assign) k_visc8_divergence_f32<true><<<grow, kVisRow, 0, s>>>(z, p);
         else k_visc8_divergence_f32<false><<<grow, kVisRow, 0, s>>>(z, p);
       } else if (assign) {

@@ -289,8 +289,9 @@ int cb2_cfl_dt(cb2_ctx *ctx, double *dt_out, void *stream);
  * partial minima use a fixed device array of CB2_NOALLOC_MAX_PARTIALS doubles (128 KiB) that
  * every GPU loading the library holds until the process exits, so n may not exceed
  * CB2_NOALLOC_MAX_NODES (CB2_ERR_INVALID beyond).  The first call on a device resolves that
- * array's device address, so make it before any stream capture.  All calls share the array:
- * calls that overlap on the GPU race. */
+ * array's device address, so make it before any stream capture; the address is kept for the
+ * process, which assumes the runtime's primary context and no cudaDeviceReset afterwards.  All
+ * calls share the array: calls that overlap on the GPU race. */
 #define CB2_NOALLOC_MAX_PARTIALS 16384
 #define CB2_NOALLOC_MAX_NODES (16384LL * 2048LL)
 int cb2_min_dt_noalloc(const double *dt_local, long long n, double *dt_min, void *stream);

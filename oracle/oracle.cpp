@@ -961,7 +961,8 @@ double d8(F f, int n, int nx, bool bl, bool br) {
 }
 
 void viscous_8th(Zone &z, const Param &p) {
-  // collocated node fluxes (src/ViscousScheme.cu:470-585), air only
+  // collocated node fluxes (src/ViscousScheme.cu:470-585), then for mixtures the species
+  // diffusion, its enthalpy and (two temperatures) the e_ve terms (:587-788)
 #pragma omp parallel for collapse(2) schedule(static)
   for (int k = 0; k < z.mz; ++k)
     for (int j = 0; j < z.my; ++j)
@@ -1000,7 +1001,7 @@ void viscous_8th(Zone &z, const Param &p) {
         z.hF(i, j, k, 3) = zeta_x * txz + zeta_y * tyz + zeta_z * tzz;
         const double t_x = gx(5), t_y = gy(5), t_z = gz(5);
         const double cp = gamma_air * R_air / (gamma_air - 1);
-        const double cond = mul / p.Pr * cp;
+        const double cond = p.n_spec == 0 ? mul / p.Pr * cp : z.kappa(i, j, k);
         const double u = z.bv(i, j, k, 1), v = z.bv(i, j, k, 2), w = z.bv(i, j, k, 3);
         const double Ex = u * txx + v * txy + w * txz + cond * t_x;
         const double Ey = u * txy + v * tyy + w * tyz + cond * t_y;
@@ -1008,6 +1009,72 @@ void viscous_8th(Zone &z, const Param &p) {
         z.fF(i, j, k, 4) = xi_x * Ex + xi_y * Ey + xi_z * Ez;
         z.gF(i, j, k, 4) = eta_x * Ex + eta_y * Ey + eta_z * Ez;
         z.hF(i, j, k, 4) = zeta_x * Ex + zeta_y * Ey + zeta_z * Ez;
+        if (p.n_spec == 0) continue;
+        // node gradient of a field c of array f projected on grad xi, grad eta, grad zeta
+        auto proj = [&](const Arr &f, int c, double *g3) {
+          const double a0 = d8([&](int m) { return f(i + m, j, k, c); }, i, z.mx, bil, bir);
+          const double a1 = d8([&](int m) { return f(i, j + m, k, c); }, j, z.my, bjl, bjr);
+          const double a2 = d8([&](int m) { return f(i, j, k + m, c); }, k, z.mz, bkl, bkr);
+          const double fx = a0 * xi_x + a1 * eta_x + a2 * zeta_x;
+          const double fy = a0 * xi_y + a1 * eta_y + a2 * zeta_y;
+          const double fz = a0 * xi_z + a1 * eta_z + a2 * zeta_z;
+          g3[0] = xi_x * fx + xi_y * fy + xi_z * fz;
+          g3[1] = eta_x * fx + eta_y * fy + eta_z * fz;
+          g3[2] = zeta_x * fx + zeta_y * fy + zeta_z * fz;
+        };
+        const bool tt = p.i_eve >= 0;
+        double ef[3] = {0, 0, 0};
+        if (tt) {  // kappa_ve grad T_ve in the energy flux (the collocated kernel's last lines)
+          double gv3[3];
+          proj(z.tve, 0, gv3);
+          const double kve = z.kappa_ve(i, j, k);
+          for (int a = 0; a < 3; ++a) ef[a] = kve * gv3[a];
+          z.fF(i, j, k, 4) += ef[0];
+          z.gF(i, j, k, 4) += ef[1];
+          z.hF(i, j, k, 4) += ef[2];
+        }
+        const int ns = p.n_spec;
+        double dif[16], yk[16], force[16][3], sw[3] = {0, 0, 0}, corr[3] = {0, 0, 0}, mwt = 0, srdy = 0;
+        for (int l = 0; l < ns; ++l) {
+          yk[l] = z.sv(i, j, k, l);
+          dif[l] = z.rhoD(i, j, k, l);
+          proj(z.sv, l, force[l]);
+          for (int a = 0; a < 3; ++a) corr[a] += dif[l] * force[l][a];
+          for (int a = 0; a < 3; ++a) sw[a] += force[l][a] * p.mech.imw[l];
+          mwt += yk[l] * p.mech.imw[l];
+          srdy += dif[l] * yk[l];
+        }
+        mwt = 1.0 / mwt;
+        for (int a = 0; a < 3; ++a) corr[a] -= mwt * srdy * sw[a];
+        if (p.gradP) {
+          double gp[3];
+          proj(z.bv, 4, gp);
+          for (int a = 0; a < 3; ++a) gp[a] /= z.bv(i, j, k, 4);
+          for (int l = 0; l < ns; ++l) {
+            const double co = (mwt * p.mech.imw[l] - 1) * yk[l];
+            for (int a = 0; a < 3; ++a) {
+              force[l][a] += co * gp[a];
+              corr[a] += co * gp[a] * dif[l];
+            }
+          }
+        }
+        double h[16];
+        const double tm = z.bv(i, j, k, 5);
+        nasa7_h(tm, p.mech, h);
+        const double tve_m = tt ? z.tve(i, j, k) : tm;
+        Arr *F[3] = {&z.fF, &z.gF, &z.hF};
+        for (int l = 0; l < ns; ++l) {
+          const double hd = tt ? h[l] - ve_energy(p, l, tm) + ve_energy(p, l, tve_m) : h[l];
+          const double ev = tt ? ve_energy(p, l, tve_m) : 0.0;
+          for (int a = 0; a < 3; ++a) {
+            const double jd = dif[l] * (force[l][a] - mwt * yk[l] * sw[a]) - yk[l] * corr[a];
+            (*F[a])(i, j, k, 5 + l) = jd;
+            (*F[a])(i, j, k, 4) += hd * jd;
+            if (tt) ef[a] += ev * jd;
+          }
+        }
+        if (tt)
+          for (int a = 0; a < 3; ++a) (*F[a])(i, j, k, 5 + p.i_eve) = ef[a];
       }
   // periodic exchange of the node fluxes (src/DataCommunication.cu:665-712)
   for (const auto &f : z.faces) {

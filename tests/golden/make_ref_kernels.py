@@ -7,7 +7,8 @@ on a GPU:
           (setup.txt, grid, boundary files, the reference's chemistry data files, state.bin,
           task.txt) under --work.
   run   : (GPU machine) runs the runner on every case directory and copies each out.bin to --out.
-  pack  : (build container) reads the dumps and writes the fixture: for every case its definition,
+  pack  : reads the dumps and writes the fixture (cases without a new dump keep the entries the
+          fixture already has): for every case its definition,
           the digest of its initial state, the reference state the kernels read, the residual dq of
           the first stage and the conservative variables, temperature (and T_ve) after the last
           stage on the interior nodes, and for the Sod run its time-step history.
@@ -92,12 +93,18 @@ def cmd_pack(args):
         digests = json.load(f)
     arrays = {}
     meta = {}
+    if os.path.exists(FIXTURE):  # cases without a new dump keep their entries
+        old = np.load(FIXTURE)
+        meta = json.loads(bytes(old["meta"]).decode())
+        arrays = {k: old[k] for k in old.files if k != "meta"}
     for c in refcases.CASES:
         n = c["name"]
         path = os.path.join(args.out, n, "out.bin")
         if not os.path.exists(path):
-            print("missing", n)
+            print("no new dump for", n, "(kept)" if n in meta else "(missing)")
             continue
+        for k in [k for k in arrays if k.startswith(n + "/")]:
+            del arrays[k]
         d = refcases.read_dump(path)
         blk = d["blocks"][0]
         g = blk["dims"][3]

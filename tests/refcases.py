@@ -89,7 +89,7 @@ CASES = ([_air(n + "_" + bc, s, r, v, bc) for n, s, r, v in AIR_SCHEMES for bc i
           _mix("mix_ausm_muscl", 3, 2, 0, 0), _mix("mix_roe_muscl", 2, 2, 0, 0),
           _mix("mix_weno7ch_visc8", 72, 2, 8, 0)] +
          [_air5("air5_weno5ch_visc2_chem", 2, 1), _air5("air5_weno5ch_chem_pp_limit", 0, 1, pp=1, limit_flow=1),
-          _air5("air5_weno5ch_visc2_outflow", 2, 1, bc="outflow")] +
+          _air5("air5_weno5ch_visc2_outflow", 2, 1, bc="outflow"), _air5("air5_weno5ch_visc8_chem", 8, 1)] +
          [_chan("chan_hllc_muscl_visc2", 4, 2, 2), _chan("chan_weno5ch_visc2", 52, 2, 2),
           _chan("chan_roe_muscl", 2, 2, 0)] +
          [dict(family="sod", name="sod_1000x7", scheme=52, rec=2, visc=0, bc="outflow", stages=0, dt=0.0, seed=0,

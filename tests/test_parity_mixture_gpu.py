@@ -77,7 +77,8 @@ MIX = [("weno5ch", abi.INV_WENO5_CH, abi.REC_WENO5, 0, False),
        ("ausm_muscl", abi.INV_AUSMP, abi.REC_MUSCL, 0, False),
        ("roe_muscl", abi.INV_ROE, abi.REC_MUSCL, 0, False),
        ("visc2", abi.INV_HLLC, abi.REC_WENO5, 2, False),
-       ("chem", abi.INV_HLLC, abi.REC_WENO5, 0, True)]
+       ("chem", abi.INV_HLLC, abi.REC_WENO5, 0, True),
+       ("visc8", abi.INV_WENO7_CH, abi.REC_WENO5, 8, False)]
 
 
 @pytest.mark.parametrize("name,scheme,rec,visc,chem", MIX, ids=[m[0] for m in MIX])

@@ -33,7 +33,7 @@ TOL = 1e-12
 
 # cases the library refuses (combinations it does not build yet); they stay in the fixture so the
 # day the combination is built its parity is checked against the reference
-NOT_BUILT = {"mix_weno7ch_visc8": "8th-order viscous fluxes of mixtures"}
+NOT_BUILT = {}
 
 
 def _fixture():

@@ -125,3 +125,15 @@ def test_served_reactors_reach_reference_end_state(h2):
         assert abs(o.T - r["final"]["T"]) <= 1e-5 * r["final"]["T"]
         assert o.latency > 0 and o.t_done >= o.t_admit >= o.t_arrival
     ctx.close()
+
+
+def test_tube_larger_than_the_pool_is_refused(h2):
+    """A tube whose state can never fit the device pool makes the run fail at once with
+    CB2_ERR_NOMEM, also without a time limit (it used to wait for memory forever)."""
+    ctx_t = _ctx_tube(h2)
+    opt = serve.options(h2, hbm_budget=1 << 20, tube_steps=5)
+    opt.time_limit_s = 0.0
+    with pytest.raises(cb200.CB2Error) as e:
+        serve.serve(None, ctx_t, [_tube_req(50, 1e-7), _tube_req(4000, 1e-7, 0.001)], opt)
+    assert e.value.code == abi.ERR_NOMEM
+    ctx_t.close()
