@@ -1,7 +1,7 @@
 """ctypes mirror of include/cb200.h (structs and constants)."""
 import ctypes as C
 
-ABI_VERSION = 4
+ABI_VERSION = 5
 
 OK = 0
 ERR_CUDA, ERR_INVALID, ERR_NONPHYSICAL, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_NOMEM = -1, -2, -3, -4, -5, -6
@@ -31,7 +31,16 @@ class FaceBC(C.Structure):
     _fields_ = [("type", C.c_int), ("face", C.c_int), ("direction", C.c_int),
                 ("range_start", C.c_int * 3), ("range_end", C.c_int * 3),
                 ("rho", C.c_double), ("u", C.c_double), ("v", C.c_double), ("w", C.c_double),
-                ("p", C.c_double), ("T", C.c_double), ("wall_temperature", C.c_double)]
+                ("p", C.c_double), ("T", C.c_double), ("wall_temperature", C.c_double),
+                ("wall_temperature_ve", C.c_double), ("sv", C.c_void_p)]
+
+
+class InnerFace(C.Structure):
+    """cb2_inner_face: an inner face after the reference's register_boundary."""
+    _fields_ = [("range_start", C.c_int * 3), ("range_end", C.c_int * 3), ("face", C.c_int), ("direction", C.c_int),
+                ("target_start", C.c_int * 3), ("target_end", C.c_int * 3), ("target_block", C.c_int),
+                ("target_face", C.c_int), ("target_direction", C.c_int), ("src_tar", C.c_int * 3),
+                ("loop_dir", C.c_int * 3), ("target_loop_dir", C.c_int * 3), ("n_point", C.c_int * 3)]
 
 
 MECH_DOUBLE = ("mw", "low_temp_coeff", "high_temp_coeff", "t_low", "t_mid", "t_high", "geometry",

@@ -12,6 +12,7 @@ from dataclasses import dataclass, field as dfield
 import numpy as np
 
 from . import abi
+from . import mech as mechmod
 from .field import HostBlock, array_specs, box_faces
 from .mech import stoich_h2_air
 
@@ -401,3 +402,94 @@ def reactive_shock_tube(mech, n_nodes=400, ngg=3, length=0.1, scheme=abi.INV_HLL
                      reconstruction=reconstruction, cfl=0.5, rho_ref=rho_l, v_ref=c_l, mech=mech.ptr())
     par.reaction = 1 if reaction else 0
     return Case("reactive_shock_tube", par, [b], [faces], {"t_end": 50e-6, "mech": mech, "dx": dx})
+
+
+# ---- the two-temperature AIR5 square cylinder (four body-fitted blocks) --------------------
+def air5_freestream(mech, tt, mach=10.0, T=250.0, Tve=250.0, p=500.0, y=(0.767, 0.233, 0.0, 0.0, 0.0)):
+    """Freestream state of the AIR5 cylinder as the reference's Inflow builds it from
+    (mach, temperature, Tve, pressure, Y) (src/BoundCond.cpp:214-300): mw from Y, rho =
+    p mw / (R_u T), e_ve at Tve, and the speed of sound of the translational-rotational gas, so
+    the velocity is mach * c along +x."""
+    ns = mech.ns
+    yk = np.asarray(y, dtype=np.float64)
+    mw = 0.0
+    for i in range(ns):
+        mw += yk[i] / mech.mw[i]
+    mw = 1.0 / mw
+    rho = p * mw / (R_U * T)
+    # cp of the translational-rotational modes: 5/2 R (molecules) and 3/2 R (atoms) plus R
+    geom = np.asarray(mech.d["geometry"])
+    cv_tr = sum(yk[i] * (R_U / mech.mw[i]) * (1.5 if geom[i] == 0 else 2.5) for i in range(ns))
+    r_mix = R_U / mw
+    gamma = (cv_tr + r_mix) / cv_tr
+    c = math.sqrt(gamma * r_mix * T)
+    e_ve = mechmod.mixture_ve_energy(tt, mech.mw, Tve, yk)
+    sv = np.concatenate([yk, [e_ve]])
+    return dict(rho=rho, u=mach * c, v=0.0, w=0.0, p=p, T=T, Tve=Tve, y=yk, sv=sv, c=c, mw=mw)
+
+
+def square_cylinder_air5(mech, tt, n_side=256, n_normal=512, ngg=3, side=0.01, half_box=0.04, first=1e-6,
+                         mach=10.0, T_inf=250.0, p_inf=500.0, T_wall=300.0, viscous_order=2, reaction=True,
+                         scheme=abi.INV_WENO5_CH, cfl=0.3):
+    """Mach-10 two-temperature AIR5 flow over a square cylinder of side D on four body-fitted
+    blocks of n_side x n_normal nodes (grid.square_cylinder): freestream inflow on the box except
+    its downstream side (outflow), an isothermal 300 K wall (T_ve too), metrics and Jacobian from
+    the grid as the reference's Mesh computes them.  Initial state: the freestream with the
+    velocity damped and T, T_ve blended to the wall values over a 0.05 D layer at the body
+    (an impulsive start that the first steps turn into the bow shock)."""
+    from . import grid as gridmod
+    from .field import face
+    ns = mech.ns
+    g = gridmod.square_cylinder(n_side, n_normal, side=side, half_box=half_box, first=first)
+    inner = [[gridmod.register_inner_face(a, b, 2, ngg) for a, b in faces] for faces in g["inner"]]
+    padded, g1 = gridmod.extend_coordinates(g["xyz"], inner, ngg)
+    fs = air5_freestream(mech, tt, mach=mach, T=T_inf, Tve=T_inf, p=p_inf)
+    blocks, faces = [], []
+    h = 0.5 * side
+    for b in range(4):
+        X, Y, Z = padded[b]
+        met, jac = gridmod.metrics(padded[b], g1, ngg)
+        mx, my, mz = n_side, n_normal, 1
+        specs = array_specs(mx, my, mz, ngg, 6 + ns, ns + 1, viscous_order=viscous_order, reaction=reaction)
+        specs["temperature_ve"] = (1, ngg)
+        if viscous_order:
+            specs["thermal_conductivity_ve"] = (1, ngg)
+        hb = HostBlock(mx, my, mz, ngg, specs)
+        s = (slice(g1 - ngg, g1 + mz + ngg), slice(g1 - ngg, g1 + my + ngg), slice(g1 - ngg, g1 + mx + ngg))
+        x, y = X[s], Y[s]
+        d = np.sqrt(np.maximum(np.abs(x) - h, 0.0) ** 2 + np.maximum(np.abs(y) - h, 0.0) ** 2)
+        blend = np.exp(-d / (0.05 * side))
+        T = fs["T"] + (T_wall - fs["T"]) * blend
+        bv = hb.a["bv"]
+        bv[0] = fs["p"] / ((R_U / fs["mw"]) * T)
+        bv[1] = fs["u"] * (1.0 - blend)
+        bv[2] = 0.0
+        bv[3] = 0.0
+        bv[4] = fs["p"]
+        bv[5] = T
+        for i in range(ns):
+            hb.a["sv"][i] = fs["y"][i]
+        hb.a["sv"][ns] = 0.0  # e_ve from T_ve by the first cv-from-bv pass
+        hb.a["temperature_ve"][0] = T
+        hb.a["metric"][...] = met
+        hb.a["jac"][0] = jac
+        blocks.append(hb)
+        fl = []
+        for (i1, i2, j1, j2, k1, k2, lab) in g["faces"][b]:
+            if lab == abi.BC_WALL:
+                fl.append(face(abi.BC_WALL, 1, -1, (i1, j1, k1), (i2, j2, k2), wall_temperature=T_wall,
+                               wall_temperature_ve=T_wall))
+            elif lab == abi.BC_INFLOW:
+                fl.append(face(abi.BC_INFLOW, 1, 1, (i1, j1, k1), (i2, j2, k2), sv=fs["sv"], rho=fs["rho"],
+                               u=fs["u"], v=0.0, w=0.0, p=fs["p"], T=fs["T"]))
+            else:
+                fl.append(face(abi.BC_OUTFLOW, 1, 1, (i1, j1, k1), (i2, j2, k2)))
+        faces.append(fl)
+    par = make_param(n_var=6 + ns, n_spec=ns, dim=2, inviscid_scheme=scheme, reconstruction=abi.REC_WENO5,
+                     viscous_order=viscous_order, cfl=cfl, rho_ref=fs["rho"], v_ref=fs["u"], mech=mech.ptr(),
+                     two_t=tt.ptr())
+    par.reaction = 1 if reaction else 0
+    par.p_ref, par.c_ref = fs["p"], fs["c"]
+    return Case("square_cylinder_air5", par, blocks, faces,
+                {"mech": mech, "two_t": tt, "inner": inner, "grid": g, "freestream": fs, "padded": padded,
+                 "g1": g1})

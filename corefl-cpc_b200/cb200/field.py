@@ -101,13 +101,18 @@ def faces_array(faces):
     return arr
 
 
-def face(type_, face_dim, direction, start, end, **state):
+def face(type_, face_dim, direction, start, end, sv=None, **state):
+    """A cb2_face_bc; sv (sequence of the n_scalar inflow scalars) is kept with the struct."""
     f = abi.FaceBC()
     f.type, f.face, f.direction = type_, face_dim, direction
     for a in range(3):
         f.range_start[a], f.range_end[a] = start[a], end[a]
     for k, v in state.items():
         setattr(f, k, v)
+    if sv is not None:
+        keep = np.ascontiguousarray(sv, dtype=np.float64)
+        f.sv = keep.ctypes.data
+        f._sv_keep = keep
     return f
 
 

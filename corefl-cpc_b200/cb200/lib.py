@@ -91,8 +91,18 @@ class Context:
     def bind(self, blk, zone_view, faces):
         from .field import faces_array
         arr = faces_array(faces)
-        self._keep[blk] = (zone_view, arr)
+        # the faces' scalar arrays (inflow states) must stay alive until the library copies them
+        self._keep[blk] = (zone_view, arr, [getattr(f, "_sv_keep", None) for f in faces])
         check(self.lib.cb2_bind_block(self.h, blk, C.byref(zone_view), arr, len(faces)), "cb2_bind_block")
+
+    def bind_inner_faces(self, blk, faces):
+        """Inner faces (abi.InnerFace, registered form) of block blk (cb2_bind_inner_faces)."""
+        arr = (abi.InnerFace * max(1, len(faces)))(*faces)
+        self._keep[("inner", blk)] = arr
+        check(self.lib.cb2_bind_inner_faces(self.h, blk, arr, len(faces)), "cb2_bind_inner_faces")
+
+    def halo(self, stream=None):
+        check(self.lib.cb2_halo(self.h, stream), "cb2_halo")
 
     def rhs(self, blk, mask=abi.RHS_ALL, stream=None):
         check(self.lib.cb2_rhs(self.h, blk, mask, stream), "cb2_rhs")

@@ -101,3 +101,43 @@ class TwoTemperatureStruct:
 def load_two_temperature_json(path, enable_vt_relaxation=True):
     with open(path) as f:
         return TwoTemperatureStruct(json.load(f), enable_vt_relaxation)
+
+
+R_U = 8314.462618
+
+
+def species_ve_energy(tt, mw, t):
+    """e_ve [J/kg] of every species at temperature t: the harmonic-oscillator vibration
+    R theta_v / (exp(theta_v / T) - 1) plus the Boltzmann average of the electronic levels
+    (compute_ve_energy, src/Thermo.cu:635-668), with T held at >= 1 K.  Host-side, for building
+    inflow states; the kernels evaluate the same model on the device."""
+    d = tt.d
+    ns = int(d["n_spec"])
+    ml = int(d["max_level"])
+    temp = max(float(t), 1.0)
+    theta = np.asarray(d["theta_v"], dtype=np.float64)
+    nlev = np.asarray(d["n_level"], dtype=np.int64)
+    eth = np.asarray(d["elec_theta"], dtype=np.float64).reshape(ns, ml)
+    eg = np.asarray(d["elec_g"], dtype=np.float64).reshape(ns, ml)
+    e = np.zeros(ns)
+    for i in range(ns):
+        r = R_U / float(mw[i])
+        if theta[i] > 0:
+            x = theta[i] / temp
+            if x < 200:
+                e[i] += r * theta[i] / np.expm1(x)
+        if nlev[i] > 0:
+            bz = eg[i, :nlev[i]] * np.exp(-eth[i, :nlev[i]] / temp)
+            zs = bz.sum()
+            if zs > 0:
+                e[i] += r * (bz * eth[i, :nlev[i]]).sum() / zs
+    return e
+
+
+def mixture_ve_energy(tt, mw, t, y):
+    """Mixture e_ve = sum Y_k e_ve,k (compute_mixture_ve_energy, src/Thermo.cu:711-723)."""
+    e = species_ve_energy(tt, mw, t)
+    total = 0.0
+    for i in range(len(e)):
+        total += float(y[i]) * e[i]
+    return total

@@ -81,8 +81,10 @@ struct Block {
   cb2_zone_view v{};
   Zone z{};
   std::vector<FaceBC> faces;
-  int *d_btype = nullptr;  // six face flag arrays, one allocation
-  float *d_f32 = nullptr;  // mixed form: bv32 and met32, one allocation
+  std::vector<cb2_inner_face> inner;  // inner faces of a multi-block grid (cb2_bind_inner_faces)
+  int *d_btype = nullptr;     // six face flag arrays, one allocation
+  float *d_f32 = nullptr;     // mixed form: bv32 and met32, one allocation
+  double *d_face_sv = nullptr;  // inflow faces' scalars, one allocation
 };
 
 }  // namespace cb2
@@ -257,6 +259,8 @@ FaceBC register_face(const cb2_face_bc &f, int dim, int ngg, bool extend) {
   }
   if (dim == 2) { b.start[2] = -gx; b.end[2] = gx; }
   b.rho = f.rho; b.u = f.u; b.v = f.v; b.w = f.w; b.p = f.p; b.T = f.T; b.wall_T = f.wall_temperature;
+  b.wall_Tve = f.wall_temperature_ve;
+  b.sv = nullptr;  // set at bind to the device copy of f.sv
   return b;
 }
 
@@ -286,12 +290,15 @@ bool two_temperature(const cb2_ctx *ctx) { return ctx && ctx->p.i_eve >= 0; }
 
 unsigned two_temperature_rhs_terms(const cb2_ctx *ctx);
 
-// Faces whose ghost fill is built for two temperatures: periodic and outflow copy bv and every
-// scalar (e_ve included) and rebuild cv with the T_ve sync, as the reference's apply_periodic /
-// apply_outflow do (src/BoundCond.cu:2204-2350, 3390-3440).
+// Faces whose ghost fill is built for two temperatures: all of them.  Periodic, outflow and
+// symmetry copy bv, every scalar (e_ve included) and T_ve, inflow sets the given scalars, the wall
+// sets T_ve and e_ve, and each rebuilds cv with the T_ve sync, as the reference's apply_* kernels
+// do (src/BoundCond.cu:2130-3440).
 bool two_temperature_faces(const Block &B) {
   for (const FaceBC &f : B.faces)
-    if (f.type != CB2_BC_PERIODIC && f.type != CB2_BC_OUTFLOW) return false;
+    if (f.type != CB2_BC_PERIODIC && f.type != CB2_BC_OUTFLOW && f.type != CB2_BC_WALL &&
+        f.type != CB2_BC_SYMMETRY && f.type != CB2_BC_INFLOW)
+      return false;
   return true;
 }
 
@@ -482,6 +489,7 @@ void cb2_destroy(cb2_ctx *ctx) {
   for (auto &b : ctx->blocks) {
     cudaFree(b.d_btype);
     cudaFree(b.d_f32);
+    cudaFree(b.d_face_sv);
   }
   cudaFree(ctx->d_tables);
   cudaFree(ctx->d_status);
@@ -557,6 +565,8 @@ int cb2_bind_block(cb2_ctx *ctx, int blk, const cb2_zone_view *v, const cb2_face
     if (b.type != CB2_BC_OUTFLOW && b.type != CB2_BC_PERIODIC && b.type != CB2_BC_WALL &&
         b.type != CB2_BC_SYMMETRY && b.type != CB2_BC_INFLOW)
       return CB2_ERR_INVALID;
+    // an inflow of a mixture carries its scalars (Y_k, e_ve)
+    if (b.type == CB2_BC_INFLOW && p.n_scalar > 0 && !b.sv) return CB2_ERR_INVALID;
   }
   if ((int)ctx->blocks.size() <= blk) ctx->blocks.resize(blk + 1);
   Block &B = ctx->blocks[blk];
@@ -564,11 +574,32 @@ int cb2_bind_block(cb2_ctx *ctx, int blk, const cb2_zone_view *v, const cb2_face
   B.d_btype = nullptr;
   cudaFree(B.d_f32);
   B.d_f32 = nullptr;
+  cudaFree(B.d_face_sv);
+  B.d_face_sv = nullptr;
   B.v = *v;
   B.z = make_zone(*v);
   B.faces.clear();
   const bool extend = p.viscous_order == 2;
   for (int f = 0; f < n_faces; ++f) B.faces.push_back(register_face(faces[f], p.dim, v->ngg, extend));
+  {
+    // the inflow faces' scalars go to the device with the face (Inflow::sv lives in device memory)
+    std::vector<double> all_sv;
+    std::vector<int> at(n_faces, -1);
+    const int nsc = std::max(p.n_scalar, 1);
+    for (int f = 0; f < n_faces; ++f) {
+      if (faces[f].type != CB2_BC_INFLOW) continue;
+      at[f] = (int)all_sv.size();
+      for (int l = 0; l < nsc; ++l) all_sv.push_back(faces[f].sv && l < p.n_scalar ? faces[f].sv[l] : 0.0);
+    }
+    if (!all_sv.empty()) {
+      cudaError_t e = cudaMalloc(&B.d_face_sv, all_sv.size() * sizeof(double));
+      if (e != cudaSuccess) return fail_cuda(e);
+      e = cudaMemcpy(B.d_face_sv, all_sv.data(), all_sv.size() * sizeof(double), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) return fail_cuda(e);
+      for (int f = 0; f < n_faces; ++f)
+        if (at[f] >= 0) B.faces[f].sv = B.d_face_sv + at[f];
+    }
+  }
   // physical-boundary flags per face node, from the raw (unextended) ranges (src/Mesh.cpp:855-900)
   const int mx = v->mx, my = v->my, mz = v->mz;
   std::vector<int> il(my * mz, 0), ir(my * mz, 0), jl(mx * mz, 0), jr(mx * mz, 0), kl(mx * my, 0), kr(mx * my, 0);
@@ -656,6 +687,9 @@ int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream) {
   Block *B = get_block(ctx, blk);
   if (!B) return CB2_ERR_INVALID;
   if (two_temperature(ctx) && (mask & ~two_temperature_rhs_terms(ctx))) return CB2_ERR_UNSUPPORTED;
+  // the 8th-order node fluxes of a multi-block grid would need their exchange across the inner
+  // faces (exchange_value task 1, src/DataCommunication.cu:422-463), which is not built
+  if ((mask & CB2_RHS_VISCOUS) && ctx->p.viscous_order == 8 && !B->inner.empty()) return CB2_ERR_UNSUPPORTED;
   ProfGuard pg(ctx);
   cudaStream_t s = (cudaStream_t)stream;
   const Param &p = ctx->p;
@@ -793,6 +827,68 @@ int cb2_boundary(cb2_ctx *ctx, int blk, void *stream) {
   return count(ctx, nl);
 }
 
+int cb2_bind_inner_faces(cb2_ctx *ctx, int blk, const cb2_inner_face *faces, int n_faces) {
+  Block *B = get_block(ctx, blk);
+  if (!B || n_faces < 0 || (n_faces > 0 && !faces)) return CB2_ERR_INVALID;
+  for (int f = 0; f < n_faces; ++f) {
+    const cb2_inner_face &q = faces[f];
+    if (q.face < 0 || q.face > 2 || (q.direction != 1 && q.direction != -1) || q.target_block < 0) return CB2_ERR_INVALID;
+    for (int a = 0; a < 3; ++a) {
+      if (q.src_tar[a] < 0 || q.src_tar[a] > 2 || (q.loop_dir[a] != 1 && q.loop_dir[a] != -1) ||
+          (q.target_loop_dir[a] != 1 && q.target_loop_dir[a] != -1 && q.target_loop_dir[a] != 0) || q.n_point[a] < 1)
+        return CB2_ERR_INVALID;
+      if (q.range_end[a] - q.range_start[a] != q.loop_dir[a] * (q.n_point[a] - 1)) return CB2_ERR_INVALID;
+    }
+  }
+  B->inner.assign(faces, faces + n_faces);
+  ++ctx->bind_gen;
+  return CB2_OK;
+}
+
+// Whether every node an inner face reads or writes lies inside both blocks' padded arrays.
+static bool inner_face_in_range(const Zone &z, const Zone &zt, const cb2_inner_face &f) {
+  const int ext[3] = {z.mx, z.my, z.mz}, extt[3] = {zt.mx, zt.my, zt.mz};
+  for (int a = 0; a < 3; ++a) {
+    const int lo = std::min(f.range_start[a], f.range_end[a]), hi = std::max(f.range_start[a], f.range_end[a]);
+    if (lo < -z.ngg || hi > ext[a] - 1 + z.ngg) return false;
+    // the target index along a moves with the step along src_tar[a]: check both ends
+    const int b = f.src_tar[a];
+    const int d0 = 0, d1 = f.loop_dir[b] * (f.n_point[b] - 1);
+    const int t0 = f.target_start[a] + f.target_loop_dir[a] * d0, t1 = f.target_start[a] + f.target_loop_dir[a] * d1;
+    if (std::min(t0, t1) < -zt.ngg || std::max(t0, t1) > extt[a] - 1 + zt.ngg) return false;
+  }
+  return true;
+}
+
+int cb2_halo(cb2_ctx *ctx, void *stream) {
+  if (!ctx) return CB2_ERR_INVALID;
+  ProfGuard pg(ctx);
+  cudaStream_t s = (cudaStream_t)stream;
+  int nl = 0;
+  const int nb = (int)ctx->blocks.size();
+  for (int b = 0; b < nb; ++b) {
+    Block &B = ctx->blocks[b];
+    if (!B.bound) continue;
+    for (const cb2_inner_face &f : B.inner) {
+      Block *T = get_block(ctx, f.target_block);
+      if (!T || !inner_face_in_range(B.z, T->z, f)) return CB2_ERR_INVALID;
+      CB2_TRY(launch_inner_exchange(B.z, T->z, ctx->p, f, s, nl));
+    }
+  }
+  for (int b = 0; b < nb; ++b) {
+    Block &B = ctx->blocks[b];
+    if (B.bound && !B.inner.empty() && ctx->p.dim == 2 && B.z.mz == 1)
+      CB2_TRY(launch_eliminate_k_gradient(B.z, ctx->p, s, nl));
+  }
+  return count(ctx, nl);
+}
+
+static bool any_inner_faces(const cb2_ctx *ctx) {
+  for (const Block &B : ctx->blocks)
+    if (B.bound && !B.inner.empty()) return true;
+  return false;
+}
+
 int cb2_properties(cb2_ctx *ctx, int blk, void *stream) {
   Block *B = get_block(ctx, blk);
   if (!B) return CB2_ERR_INVALID;
@@ -854,6 +950,7 @@ static int enqueue_step_head(cb2_ctx *ctx, void *stream) {
 // The three stages of a step (src/RK.cuh:164-237).
 static int enqueue_stages(cb2_ctx *ctx, double dt, void *stream) {
   const int nb = (int)ctx->blocks.size();
+  const bool halo = any_inner_faces(ctx);
   for (int rk = 0; rk < 3; ++rk) {
     for (int b = 0; b < nb; ++b) {
       if (!ctx->blocks[b].bound) continue;
@@ -861,6 +958,7 @@ static int enqueue_stages(cb2_ctx *ctx, double dt, void *stream) {
       CB2_TRY(cb2_stage_update(ctx, b, dt, rk, stream));
       CB2_TRY(cb2_boundary(ctx, b, stream));
     }
+    if (halo) CB2_TRY(cb2_halo(ctx, stream));  // data_communication (src/RK.cuh:216-226)
     for (int b = 0; b < nb; ++b)
       if (ctx->blocks[b].bound) CB2_TRY(cb2_properties(ctx, b, stream));
   }
@@ -953,7 +1051,7 @@ int cb2_rk3_step(cb2_ctx *ctx, double *dt_inout, int fixed_dt, void *stream) {
 int cb2_rk3_run(cb2_ctx *ctx, double dt, int fixed_dt, long long max_steps, double t_end, double *time_inout,
                 long long *steps_out, double *dt_last_out, void *stream) {
   if (!ctx || !time_inout || !steps_out || max_steps < 0 || std::isnan(t_end)) return CB2_ERR_INVALID;
-  if (two_temperature(ctx)) return CB2_ERR_UNSUPPORTED;
+  if (two_temperature(ctx) && !two_temperature_step(ctx)) return CB2_ERR_UNSUPPORTED;
   if (fixed_dt && !(dt > 0.0 && dt < 1e300)) return CB2_ERR_INVALID;
   *steps_out = 0;
   if (max_steps == 0 || !(*time_inout < t_end)) return CB2_OK;

@@ -106,6 +106,7 @@ __global__ void k_bc_symmetry(Zone z, Param p, FaceBC f) {
     z.bv[gb + 4 * sz] = z.bv[g1 + 4 * sz];
     z.bv[gb + 5 * sz] = z.bv[g1 + 5 * sz];
     for (int l = 0; l < p.n_scalar; ++l) z.sv[gb + l * sz] = z.sv[g1 + l * sz];
+    if (p.i_eve >= 0) z.tve[gb] = z.tve[g1];
     cv_point<NS>(z, p, gb);
   }
   for (int gl = 1; gl <= z.ngg; ++gl) {
@@ -120,12 +121,16 @@ __global__ void k_bc_symmetry(Zone z, Param p, FaceBC f) {
     z.bv[gg + 4 * sz] = z.bv[gi + 4 * sz];
     z.bv[gg + 5 * sz] = z.bv[gi + 5 * sz];
     for (int l = 0; l < p.n_scalar; ++l) z.sv[gg + l * sz] = z.sv[gi + l * sz];
+    if (p.i_eve >= 0) z.tve[gg] = z.tve[gi];
     cv_point<NS>(z, p, gg);
   }
 }
 
+// Constant inflow state on the face node and every ghost layer, scalars (Y_k, then e_ve) from
+// the face's state (Inflow::sv); rebuilding cv brings T_ve into agreement with e_ve, starting
+// its inversion from the node's T_ve as the reference does.
 template <int NS>
-__global__ void k_bc_inflow(Zone z, Param p, FaceBC f, const double *y_in) {
+__global__ void k_bc_inflow(Zone z, Param p, FaceBC f) {
   int i, j, k;
   if (!face_point(f, i, j, k)) return;
   int d[3] = {0, 0, 0};
@@ -139,7 +144,7 @@ __global__ void k_bc_inflow(Zone z, Param p, FaceBC f, const double *y_in) {
     z.bv[gg + 3 * sz] = f.w;
     z.bv[gg + 4 * sz] = f.p;
     z.bv[gg + 5 * sz] = f.T;
-    for (int l = 0; l < p.n_scalar; ++l) z.sv[gg + l * sz] = y_in ? y_in[l] : 0.0;
+    for (int l = 0; l < p.n_scalar; ++l) z.sv[gg + l * sz] = f.sv[l];
     cv_point<NS>(z, p, gg);
   }
 }
@@ -167,7 +172,10 @@ __device__ __forceinline__ void project_to_interior(const Zone &z, int &i, int &
 // src/BoundCond.cu:3055-3389, without jets, blowing or wall fluctuations): the wall node takes
 // p and Y of the first interior node and T_wall; ghosts mirror the interior velocity and, for
 // an isothermal wall, T_ghost = 2 T_wall - T_inner (floored at T_wall when it drops below
-// 0.1 T_wall).
+// 0.1 T_wall; at 0.1 T_wall with two temperatures).  Two temperatures: the wall's T_ve is the
+// given wall_Tve (else T_wall) on an isothermal wall and the interior's on an adiabatic one; the
+// ghost T_ve mirrors it like T (floored at 0.1 max(T_ve,wall, 1)); e_ve of the wall node and of
+// every ghost is the mixture's at that T_ve.
 template <int NS>
 __global__ void k_bc_wall(Zone z, Param p, FaceBC f) {
   int i, j, k;
@@ -180,7 +188,13 @@ __global__ void k_bc_wall(Zone z, Param p, FaceBC f) {
   project_to_interior(z, ii, ij, ik);
   const idx_t g1 = z.L.at(ii, ij, ik);
   const bool iso = f.wall_T > 0;
+  const bool tt = NS > 0 && p.i_eve >= 0;
   const double t_wall = iso ? f.wall_T : z.bv[g1 + 5 * sz];
+  double tve_wall = t_wall;
+  if (tt) {
+    const double tve_in = z.tve[g1] > 0.0 ? z.tve[g1] : z.bv[g1 + 5 * sz];
+    tve_wall = !iso ? tve_in : (f.wall_Tve > 0.0 ? f.wall_Tve : t_wall);
+  }
   const double pw = z.bv[g1 + 4 * sz];
   double R = kRAir;
   if constexpr (NS > 0) {
@@ -196,6 +210,15 @@ __global__ void k_bc_wall(Zone z, Param p, FaceBC f) {
   z.bv[gb + 3 * sz] = 0;
   z.bv[gb + 4 * sz] = pw;
   z.bv[gb + 5 * sz] = t_wall;
+  if constexpr (NS > 0) {
+    if (tt) {
+      double y[NS];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) y[s] = z.sv[gb + s * sz];
+      z.tve[gb] = tve_wall;
+      z.sv[gb + p.i_eve * sz] = mixture_ve_energy<NS>(tve_wall, y, p.mech, nullptr);
+    }
+  }
   cv_point<NS>(z, p, gb);
   for (int gl = 1; gl <= z.ngg; ++gl) {
     int ai = i - gl * d[0], aj = j - gl * d[1], ak = k - gl * d[2];
@@ -206,7 +229,17 @@ __global__ void k_bc_wall(Zone z, Param p, FaceBC f) {
     double t_g = t_i;
     if (iso) {
       t_g = 2 * t_wall - t_i;
-      if (t_g <= 0.1 * t_wall) t_g = t_wall;
+      if (t_g <= 0.1 * t_wall) t_g = tt ? 0.1 * t_wall : t_wall;
+    }
+    double tve_g = t_g;
+    if (tt) {
+      const double tve_i = z.tve[gi] > 0.0 ? z.tve[gi] : t_i;
+      tve_g = tve_i;
+      if (iso) {
+        tve_g = 2 * tve_wall - tve_i;
+        const double floor_ve = 0.1 * fmax(tve_wall, 1.0);
+        if (tve_g <= floor_ve) tve_g = floor_ve;
+      }
     }
     if constexpr (NS > 0) {
       R = 0;
@@ -221,8 +254,95 @@ __global__ void k_bc_wall(Zone z, Param p, FaceBC f) {
     z.bv[gg + 3 * sz] = -z.bv[gi + 3 * sz];
     z.bv[gg + 4 * sz] = p_i;
     z.bv[gg + 5 * sz] = t_g;
+    if constexpr (NS > 0) {
+      if (tt) {
+        double y[NS];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) y[s] = z.sv[gg + s * sz];
+        z.tve[gg] = tve_g;
+        z.sv[gg + p.i_eve * sz] = mixture_ve_energy<NS>(tve_g, y, p.mech, nullptr);
+      }
+    }
     cv_point<NS>(z, p, gg);
   }
+}
+
+// Exchange across one inner face of a multi-block grid (inner_communication,
+// src/DataCommunication.cu:36-124), one thread per node of the registered face range (the face
+// layer and its ngg ghost layers): the node index in the target block follows the registered
+// orientation (src_tar, loop directions).  On the coincident face layer the two blocks' values
+// are averaged into both, except that a node at rest in the target block (a wall corner) is
+// copied from there when this block's node moves; ghost nodes take the target block's values.
+// cv of every written node is rebuilt (the two-temperature sync included).
+template <int NS>
+__global__ void k_inner_exchange(Zone z, Zone zt, Param p, cb2_inner_face f) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n01 = (long long)f.n_point[0] * f.n_point[1];
+  if (t >= n01 * f.n_point[2]) return;
+  int n[3];
+  n[0] = (int)(t % f.n_point[0]);
+  n[1] = (int)((t / f.n_point[0]) % f.n_point[1]);
+  n[2] = (int)(t / n01);
+  int idx[3], it[3], d_idx[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    d_idx[a] = f.loop_dir[a] * n[a];
+    idx[a] = f.range_start[a] + d_idx[a];
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) it[a] = f.target_start[a] + f.target_loop_dir[a] * d_idx[f.src_tar[a]];
+  const idx_t sz = z.L.sz, szt = zt.L.sz;
+  const idx_t g = z.L.at(idx[0], idx[1], idx[2]), gt = zt.L.at(it[0], it[1], it[2]);
+  const int face_layer = f.direction > 0 ? f.range_start[f.face] : f.range_end[f.face];
+  if (idx[f.face] == face_layer) {
+    const double u_this = norm3d(z.bv[g + sz], z.bv[g + 2 * sz], z.bv[g + 3 * sz]);
+    if (fabs(u_this) > 1e-15) {
+      const double u_that = norm3d(zt.bv[gt + szt], zt.bv[gt + 2 * szt], zt.bv[gt + 3 * szt]);
+      if (fabs(u_that) < 1e-15) {
+        for (int l = 0; l < 6; ++l) z.bv[g + l * sz] = zt.bv[gt + l * szt];
+        for (int l = 0; l < p.n_scalar; ++l) z.sv[g + l * sz] = zt.sv[gt + l * szt];
+        if (p.i_eve >= 0) z.tve[g] = zt.tve[gt];
+      } else {
+        for (int l = 0; l < 6; ++l) {
+          const double ave = 0.5 * (zt.bv[gt + l * szt] + z.bv[g + l * sz]);
+          z.bv[g + l * sz] = ave;
+          zt.bv[gt + l * szt] = ave;
+        }
+        for (int l = 0; l < p.n_scalar; ++l) {
+          const double ave = 0.5 * (zt.sv[gt + l * szt] + z.sv[g + l * sz]);
+          z.sv[g + l * sz] = ave;
+          zt.sv[gt + l * szt] = ave;
+        }
+        if (p.i_eve >= 0) {
+          const double ave = 0.5 * (zt.tve[gt] + z.tve[g]);
+          z.tve[g] = ave;
+          zt.tve[gt] = ave;
+        }
+        cv_point<NS>(zt, p, gt);
+      }
+    }
+  } else {
+    for (int l = 0; l < 6; ++l) z.bv[g + l * sz] = zt.bv[gt + l * szt];
+    for (int l = 0; l < p.n_scalar; ++l) z.sv[g + l * sz] = zt.sv[gt + l * szt];
+    if (p.i_eve >= 0) z.tve[g] = zt.tve[gt];
+  }
+  cv_point<NS>(z, p, g);
+}
+
+int launch_inner_exchange(const Zone &z, const Zone &zt, const Param &p, const cb2_inner_face &f, cudaStream_t s,
+                          int &nl) {
+  const long long np = (long long)f.n_point[0] * f.n_point[1] * f.n_point[2];
+  if (np <= 0) return CB2_OK;
+  const unsigned blocks = (unsigned)((np + 127) / 128);
+  ProfScope prof("inner_exchange", s);
+  switch (p.n_spec) {
+    case 0: k_inner_exchange<0><<<blocks, 128, 0, s>>>(z, zt, p, f); break;
+    case 5: k_inner_exchange<5><<<blocks, 128, 0, s>>>(z, zt, p, f); break;
+    case 9: k_inner_exchange<9><<<blocks, 128, 0, s>>>(z, zt, p, f); break;
+    default: return CB2_ERR_UNSUPPORTED;
+  }
+  ++nl;
+  return check_launch();
 }
 
 // 2-D blocks: copy the k = 0 plane into every k ghost plane (eliminate_k_gradient_point).
@@ -363,7 +483,7 @@ static int launch_bc_ns(const Zone &z, const Param &p, const FaceBC *faces, int 
       ProfScope prof("boundary_face", s);
       switch (t) {
         case CB2_BC_OUTFLOW: k_bc_outflow<NS><<<blocks, 128, 0, s>>>(z, p, faces[f]); break;
-        case CB2_BC_INFLOW: k_bc_inflow<NS><<<blocks, 128, 0, s>>>(z, p, faces[f], nullptr); break;
+        case CB2_BC_INFLOW: k_bc_inflow<NS><<<blocks, 128, 0, s>>>(z, p, faces[f]); break;
         case CB2_BC_SYMMETRY: k_bc_symmetry<NS><<<blocks, 128, 0, s>>>(z, p, faces[f]); break;
         case CB2_BC_WALL: k_bc_wall<NS><<<blocks, 128, 0, s>>>(z, p, faces[f]); break;
         case CB2_BC_PERIODIC: k_bc_periodic<NS><<<blocks, 128, 0, s>>>(z, p, faces[f]); break;

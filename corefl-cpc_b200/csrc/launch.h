@@ -62,7 +62,8 @@ inline int prepare_smem(K kern, size_t bytes) {
 struct FaceBC {
   int type, face, direction;
   int start[3], end[3];
-  double rho, u, v, w, p, T, wall_T;
+  double rho, u, v, w, p, T, wall_T, wall_Tve;
+  const double *sv;  // inflow scalars (device copy of cb2_face_bc::sv)
 };
 
 // ---- launchers (each returns CB2_OK or an error code; n_launch counts kernels) ----------
@@ -78,6 +79,9 @@ int launch_vt_relaxation(const Zone &z, const Param &p, double dt_stage, cudaStr
 int launch_properties(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
 int launch_boundary(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, cudaStream_t s,
                     int &n_launch);
+// one inner face of a multi-block grid: z's face nodes and ghosts from / with zt
+int launch_inner_exchange(const Zone &z, const Zone &zt, const Param &p, const cb2_inner_face &f, cudaStream_t s,
+                          int &nl);
 int launch_eliminate_k_gradient(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
 int launch_periodic_flux_exchange(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, cudaStream_t s,
                                   int &n_launch);

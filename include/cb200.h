@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define CB2_ABI_VERSION 4
+#define CB2_ABI_VERSION 5
 
 /* ---- status codes ---------------------------------------------------------------- */
 #define CB2_OK 0
@@ -111,7 +111,31 @@ typedef struct cb2_face_bc {
   /* inflow / wall data (unused for outflow and periodic) */
   double rho, u, v, w, p, T;
   double wall_temperature; /* <=0 : adiabatic wall */
+  /* two-temperature isothermal wall: the wall's T_ve (Wall::temperature_ve); <= 0: the wall
+   * temperature */
+  double wall_temperature_ve;
+  /* inflow: the n_scalar scalars of the inflow state, Y_k and then (two temperatures) e_ve
+   * (Inflow::sv, src/BoundCond.h:23-90); a HOST array copied at bind.  Required with species. */
+  const double *sv;
 } cb2_face_bc;
+
+/* One inner face of a multi-block grid, as cfd::InnerFace holds it after register_boundary
+ * (src/Mesh.h:33-60, src/Mesh.cpp:39-172): the node range of this block covering the face layer
+ * and its ngg ghost layers, the neighbour's block index and starting node, and the orientation
+ * that maps a step n along this range to the neighbour's nodes:
+ *   idx[a]     = range_start[a] + loop_dir[a] * n[a]
+ *   idx_tar[a] = target_start[a] + target_loop_dir[a] * (loop_dir[src_tar[a]] * n[src_tar[a]]).
+ * The fields have the reference's meaning and order, so a caller copies them from InnerFace. */
+typedef struct cb2_inner_face {
+  int range_start[3], range_end[3];
+  int face, direction;
+  int target_start[3], target_end[3];
+  int target_block;
+  int target_face, target_direction;
+  int src_tar[3];
+  int loop_dir[3], target_loop_dir[3];
+  int n_point[3];
+} cb2_inner_face;
 
 /* Species / reaction data (the fields of `DParameter` that come from cfd::Species and
  * cfd::Reaction, src/DParameter.cuh:82-130).  All arrays are host arrays, row-major. */
@@ -226,6 +250,12 @@ int cb2_init(const cb2_param_view *param, cb2_ctx **ctx_out);
 int cb2_bind_block(cb2_ctx *ctx, int blk, const cb2_zone_view *zone, const cb2_face_bc *faces,
                    int n_faces);
 
+/* The inner faces of block `blk` (the Block::inner_face list the reference's Mesh builds):
+ * replaces the list that inner_communication reads through DZone::innerFace
+ * (src/Field.cu:478-480).  Every target block must be bound when cb2_halo runs; the ranges are
+ * checked against both blocks' padded extents then.  Calling it again replaces the list. */
+int cb2_bind_inner_faces(cb2_ctx *ctx, int blk, const cb2_inner_face *faces, int n_faces);
+
 void cb2_destroy(cb2_ctx *ctx);
 
 /* ---- the stage pieces (each one replaces one call of RK3, src/RK.cuh) --------------- */
@@ -257,14 +287,24 @@ int cb2_stage_update(cb2_ctx *ctx, int blk, double dt, int rk, void *stream);
  * towards equilibrium at T with the Millikan-White + Park time, then T_ve and T follow.
  * CB2_ERR_UNSUPPORTED for one-temperature contexts.
  *
- * Two-temperature contexts (cb2_param_view::two_t) are built for the pointwise stage
- * operations: cb2_stage_update, cb2_vt_relaxation and cb2_cv_from_bv.  The flux, boundary,
- * property, time-step, whole-step and batched entry points return CB2_ERR_UNSUPPORTED for them. */
+ * Two-temperature contexts (cb2_param_view::two_t) run the characteristic WENO5/WENO7 fluxes,
+ * the 2nd- and 8th-order viscous terms, the chemistry, every face condition and the inner-face
+ * exchange, and so the whole step (cb2_rk3_step, cb2_rk3_run).  The primitive-variable fluxes
+ * (AUSM+, HLLC, Roe), the shock sensor, the autotuner, the batched paths and the 0-D reactors
+ * return CB2_ERR_UNSUPPORTED for them. */
 int cb2_vt_relaxation(cb2_ctx *ctx, int blk, double dt_stage, void *stream);
 
 /* Ghost fill of bv/sv/cv from the face conditions bound with the block (periodic,
  * outflow, ...): replaces DBoundCond::apply_boundary_conditions (src/BoundCond.cu:3846). */
 int cb2_boundary(cb2_ctx *ctx, int blk, void *stream);
+
+/* Device-side copies across the inner faces of every bound block, in block and face order, and
+ * for 2-D blocks the k = 0 plane into the k ghost planes afterwards: replaces the inner-face part
+ * of data_communication<mix> (src/DataCommunication.cu:6-27, inner_communication :36-124) and the
+ * eliminate_k_gradient that follows it (src/RK.cuh:218-226).  cb2_rk3_step and cb2_rk3_run call
+ * it after the boundary conditions of every stage.  Grids with inner faces take 2nd-order
+ * viscous terms only (the 8th-order node-flux exchange across blocks is not built). */
+int cb2_halo(cb2_ctx *ctx, void *stream);
 
 /* gamma, c, Mach, mu, kappa, rho*D over interior and ghosts: replaces
  * update_physical_properties<mix> (src/FieldOperation.cuh:183-247). */

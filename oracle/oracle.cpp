@@ -1725,6 +1725,8 @@ Zone make_zone(const cb2_zone_view &v, const cb2_face_bc *faces, int n_faces, co
     }
     if (p.dim == 2) { o.start[2] = -gx; o.end[2] = gx; }
     o.rho = b.rho; o.u = b.u; o.v = b.v; o.w = b.w; o.p = b.p; o.T = b.T; o.wall_T = b.wall_temperature;
+    o.wall_Tve = b.wall_temperature_ve;
+    if (b.sv) o.sv.assign(b.sv, b.sv + p.n_scalar);
     z.faces.push_back(o);
     if (b.type == CB2_BC_PERIODIC) continue;
     int lo[3], hi[3];
@@ -2014,7 +2016,7 @@ void apply_boundary_conditions(Zone &z, const Param &p) {
                 const int gi = i + g * dir[0], gj = j + g * dir[1], gk = k + g * dir[2];
                 const double st[6] = {f.rho, f.u, f.v, f.w, f.p, f.T};
                 for (int l = 0; l < 6; ++l) z.bv(gi, gj, gk, l) = st[l];
-                for (int l = 0; l < p.n_scalar; ++l) z.sv(gi, gj, gk, l) = 0.0;
+                for (int l = 0; l < p.n_scalar; ++l) z.sv(gi, gj, gk, l) = l < (int)f.sv.size() ? f.sv[l] : 0.0;
                 cv_point(z, p, gi, gj, gk);
               }
             } else if (type == CB2_BC_SYMMETRY) {  // src/BoundCond.cu:2130-2202
@@ -2033,10 +2035,12 @@ void apply_boundary_conditions(Zone &z, const Param &p) {
               z.bv(i, j, k, 4) = z.bv(in[0], in[1], in[2], 4);
               z.bv(i, j, k, 5) = z.bv(in[0], in[1], in[2], 5);
               for (int l = 0; l < p.n_scalar; ++l) z.sv(i, j, k, l) = z.sv(in[0], in[1], in[2], l);
+              if (p.i_eve >= 0) z.tve(i, j, k) = z.tve(in[0], in[1], in[2]);
               cv_point(z, p, i, j, k);
               for (int g = 1; g <= z.ngg; ++g) {
                 const int gi = i + g * dir[0], gj = j + g * dir[1], gk = k + g * dir[2];
                 const int ii = i - g * dir[0], ij = j - g * dir[1], ik = k - g * dir[2];
+                if (p.i_eve >= 0) z.tve(gi, gj, gk) = z.tve(ii, ij, ik);
                 z.bv(gi, gj, gk, 0) = z.bv(ii, ij, ik, 0);
                 const double u = z.bv(ii, ij, ik, 1), v = z.bv(ii, ij, ik, 2), w = z.bv(ii, ij, ik, 3);
                 uk = kx * u + ky * v + kz * w;
@@ -2052,7 +2056,14 @@ void apply_boundary_conditions(Zone &z, const Param &p) {
               int idx[3] = {i - dir[0], j - dir[1], k - dir[2]};
               project_to_interior(z, idx[0], idx[1], idx[2]);
               const bool iso = f.wall_T > 0;
+              const bool tt = p.i_eve >= 0;
               const double t_wall = iso ? f.wall_T : z.bv(idx[0], idx[1], idx[2], 5);
+              double tve_wall = t_wall;
+              if (tt) {  // the wall's T_ve (src/BoundCond.cu:3157-3167)
+                const double tve_in = z.tve(idx[0], idx[1], idx[2]) > 0.0 ? z.tve(idx[0], idx[1], idx[2])
+                                                                         : z.bv(idx[0], idx[1], idx[2], 5);
+                tve_wall = !iso ? tve_in : (f.wall_Tve > 0.0 ? f.wall_Tve : t_wall);
+              }
               const double pw = z.bv(idx[0], idx[1], idx[2], 4);
               for (int l = 0; l < p.n_spec; ++l) z.sv(i, j, k, l) = z.sv(idx[0], idx[1], idx[2], l);
               double R = mix_r(z, p, i, j, k);
@@ -2060,6 +2071,12 @@ void apply_boundary_conditions(Zone &z, const Param &p) {
               z.bv(i, j, k, 1) = z.bv(i, j, k, 2) = z.bv(i, j, k, 3) = 0;
               z.bv(i, j, k, 4) = pw;
               z.bv(i, j, k, 5) = t_wall;
+              if (tt) {
+                double y[16];
+                for (int l = 0; l < p.n_spec; ++l) y[l] = z.sv(i, j, k, l);
+                z.tve(i, j, k) = tve_wall;
+                z.sv(i, j, k, p.i_eve) = mixture_ve_energy(p, tve_wall, y, nullptr);
+              }
               cv_point(z, p, i, j, k);
               for (int g = 1; g <= z.ngg; ++g) {
                 int in[3] = {i - g * dir[0], j - g * dir[1], k - g * dir[2]};
@@ -2069,7 +2086,17 @@ void apply_boundary_conditions(Zone &z, const Param &p) {
                 double t_g = t_i;
                 if (iso) {
                   t_g = 2 * t_wall - t_i;
-                  if (t_g <= 0.1 * t_wall) t_g = t_wall;
+                  if (t_g <= 0.1 * t_wall) t_g = tt ? 0.1 * t_wall : t_wall;
+                }
+                double tve_g = t_g;
+                if (tt) {  // src/BoundCond.cu:3319-3330
+                  const double tve_i = z.tve(in[0], in[1], in[2]) > 0.0 ? z.tve(in[0], in[1], in[2]) : t_i;
+                  tve_g = tve_i;
+                  if (iso) {
+                    tve_g = 2 * tve_wall - tve_i;
+                    const double floor_ve = 0.1 * std::max(tve_wall, 1.0);
+                    if (tve_g <= floor_ve) tve_g = floor_ve;
+                  }
                 }
                 for (int l = 0; l < p.n_spec; ++l) z.sv(gh[0], gh[1], gh[2], l) = z.sv(in[0], in[1], in[2], l);
                 R = mix_r(z, p, in[0], in[1], in[2]);
@@ -2077,6 +2104,12 @@ void apply_boundary_conditions(Zone &z, const Param &p) {
                 for (int c = 1; c <= 3; ++c) z.bv(gh[0], gh[1], gh[2], c) = -z.bv(in[0], in[1], in[2], c);
                 z.bv(gh[0], gh[1], gh[2], 4) = p_i;
                 z.bv(gh[0], gh[1], gh[2], 5) = t_g;
+                if (tt) {
+                  double y[16];
+                  for (int l = 0; l < p.n_spec; ++l) y[l] = z.sv(gh[0], gh[1], gh[2], l);
+                  z.tve(gh[0], gh[1], gh[2]) = tve_g;
+                  z.sv(gh[0], gh[1], gh[2], p.i_eve) = mixture_ve_energy(p, tve_g, y, nullptr);
+                }
                 cv_point(z, p, gh[0], gh[1], gh[2]);
               }
             } else {  // periodic, src/BoundCond.cu:3390-3440
@@ -2232,6 +2265,74 @@ void compute_shock_sensor(Zone &z, const Param &p) {
 }
 
 // One SSP-RK3 step over all zones (src/RK.cuh:107-237, single process, no MPI)
+// inner_communication over every inner face of every zone (src/DataCommunication.cu:6-124),
+// then eliminate_k_gradient for 2-D zones (src/RK.cuh:218-226).
+void inner_exchange(std::vector<Zone> &zones, const Param &p) {
+  for (auto &z : zones) {
+    for (const auto &f : z.inner) {
+      Zone &t = zones[f.target_block];
+      const int face_layer = f.direction > 0 ? f.range_start[f.face] : f.range_end[f.face];
+      for (int n2 = 0; n2 < f.n_point[2]; ++n2)
+        for (int n1 = 0; n1 < f.n_point[1]; ++n1)
+          for (int n0 = 0; n0 < f.n_point[0]; ++n0) {
+            const int n[3] = {n0, n1, n2};
+            int idx[3], it[3], d[3];
+            for (int a = 0; a < 3; ++a) {
+              d[a] = f.loop_dir[a] * n[a];
+              idx[a] = f.range_start[a] + d[a];
+            }
+            for (int a = 0; a < 3; ++a) it[a] = f.target_start[a] + f.target_loop_dir[a] * d[f.src_tar[a]];
+            if (idx[f.face] == face_layer) {
+              const double u_this = std::sqrt(sqr(z.bv(idx[0], idx[1], idx[2], 1)) + sqr(z.bv(idx[0], idx[1], idx[2], 2)) +
+                                              sqr(z.bv(idx[0], idx[1], idx[2], 3)));
+              if (std::fabs(u_this) > 1e-15) {
+                const double u_that = std::sqrt(sqr(t.bv(it[0], it[1], it[2], 1)) + sqr(t.bv(it[0], it[1], it[2], 2)) +
+                                                sqr(t.bv(it[0], it[1], it[2], 3)));
+                if (std::fabs(u_that) < 1e-15) {
+                  for (int l = 0; l < 6; ++l) z.bv(idx[0], idx[1], idx[2], l) = t.bv(it[0], it[1], it[2], l);
+                  for (int l = 0; l < p.n_scalar; ++l) z.sv(idx[0], idx[1], idx[2], l) = t.sv(it[0], it[1], it[2], l);
+                  if (p.i_eve >= 0) z.tve(idx[0], idx[1], idx[2]) = t.tve(it[0], it[1], it[2]);
+                } else {
+                  for (int l = 0; l < 6; ++l) {
+                    const double ave = 0.5 * (t.bv(it[0], it[1], it[2], l) + z.bv(idx[0], idx[1], idx[2], l));
+                    z.bv(idx[0], idx[1], idx[2], l) = ave;
+                    t.bv(it[0], it[1], it[2], l) = ave;
+                  }
+                  for (int l = 0; l < p.n_scalar; ++l) {
+                    const double ave = 0.5 * (t.sv(it[0], it[1], it[2], l) + z.sv(idx[0], idx[1], idx[2], l));
+                    z.sv(idx[0], idx[1], idx[2], l) = ave;
+                    t.sv(it[0], it[1], it[2], l) = ave;
+                  }
+                  if (p.i_eve >= 0) {
+                    const double ave = 0.5 * (t.tve(it[0], it[1], it[2]) + z.tve(idx[0], idx[1], idx[2]));
+                    z.tve(idx[0], idx[1], idx[2]) = ave;
+                    t.tve(it[0], it[1], it[2]) = ave;
+                  }
+                  cv_point(t, p, it[0], it[1], it[2]);
+                }
+              }
+            } else {
+              for (int l = 0; l < 6; ++l) z.bv(idx[0], idx[1], idx[2], l) = t.bv(it[0], it[1], it[2], l);
+              for (int l = 0; l < p.n_scalar; ++l) z.sv(idx[0], idx[1], idx[2], l) = t.sv(it[0], it[1], it[2], l);
+              if (p.i_eve >= 0) z.tve(idx[0], idx[1], idx[2]) = t.tve(it[0], it[1], it[2]);
+            }
+            cv_point(z, p, idx[0], idx[1], idx[2]);
+          }
+    }
+  }
+  for (auto &z : zones) {
+    if (z.inner.empty() || !(p.dim == 2 && z.mz == 1)) continue;
+    const int g = z.ngg;
+    for (int j = -g; j < z.my + g; ++j)
+      for (int i = -g; i < z.mx + g; ++i)
+        for (int k = 1; k <= g; ++k) {
+          for (int l = 0; l < 6; ++l) z.bv(i, j, k, l) = z.bv(i, j, -k, l) = z.bv(i, j, 0, l);
+          for (int l = 0; l < p.n_scalar; ++l) z.sv(i, j, k, l) = z.sv(i, j, -k, l) = z.sv(i, j, 0, l);
+          for (int l = 0; l < p.n_var; ++l) z.cv(i, j, k, l) = z.cv(i, j, -k, l) = z.cv(i, j, 0, l);
+        }
+  }
+}
+
 void rk3_step(std::vector<Zone> &zones, const Param &p_in, double &dt, bool fixed_dt) {
   Param p = p_in;
   for (auto &z : zones) {
@@ -2257,6 +2358,7 @@ void rk3_step(std::vector<Zone> &zones, const Param &p_in, double &dt, bool fixe
       update_cv_and_bv_rk(z, p, dt, rk);
       apply_boundary_conditions(z, p);
     }
+    inner_exchange(zones, p);
     for (auto &z : zones) update_physical_properties(z, p);
   }
 }

@@ -87,7 +87,8 @@ struct Param {
 struct FaceBC {
   int type = 0, face = 0, direction = 1;
   int start[3] = {0, 0, 0}, end[3] = {0, 0, 0};
-  double rho = 0, u = 0, v = 0, w = 0, p = 0, T = 0, wall_T = 0;
+  double rho = 0, u = 0, v = 0, w = 0, p = 0, T = 0, wall_T = 0, wall_Tve = 0;
+  std::vector<double> sv;  // inflow scalars
 };
 
 struct Zone {
@@ -96,12 +97,14 @@ struct Zone {
       efd, tve, kappa_ve;
   std::vector<int> il, ir, jl, jr, kl, kr;  // physical-boundary flags per face node
   std::vector<FaceBC> faces;
+  std::vector<cb2_inner_face> inner;  // inner faces of a multi-block grid
 };
 
 Param make_param(const cb2_param_view &pv);
 Zone make_zone(const cb2_zone_view &v, const cb2_face_bc *faces, int n_faces, const Param &p);
 
 void update_cv_and_bv_rk(Zone &z, const Param &p, double dt, int rk);
+void inner_exchange(std::vector<Zone> &zones, const Param &p);
 void limit_flow(Zone &z, const Param &p);
 void compute_cv_from_bv(Zone &z, const Param &p);
 void compute_inviscid_flux(Zone &z, const Param &p);

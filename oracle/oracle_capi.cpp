@@ -125,6 +125,39 @@ int oracle_rk3_step(const cb2_param_view *pv, const cb2_zone_view *zvs, const cb
   return 0;
 }
 
+// The same step for a multi-block grid: the inner faces of zone b are
+// inner[ioff_b .. ioff_b + n_inner[b]) (registered form, cb2_inner_face).
+int oracle_rk3_step_inner(const cb2_param_view *pv, const cb2_zone_view *zvs, const cb2_face_bc *faces,
+                          const int *n_faces, const cb2_inner_face *inner, const int *n_inner, int n_zones,
+                          double *dt, int fixed_dt) {
+  Param p = make_param(*pv);
+  std::vector<Zone> zones;
+  int off = 0, ioff = 0;
+  for (int b = 0; b < n_zones; ++b) {
+    zones.push_back(make_zone(zvs[b], faces + off, n_faces[b], p));
+    zones.back().inner.assign(inner + ioff, inner + ioff + n_inner[b]);
+    off += n_faces[b];
+    ioff += n_inner[b];
+  }
+  rk3_step(zones, p, *dt, fixed_dt != 0);
+  return 0;
+}
+
+// The inner-face exchange alone over n_zones blocks (cb2_halo).
+int oracle_halo(const cb2_param_view *pv, const cb2_zone_view *zvs, const cb2_inner_face *inner, const int *n_inner,
+                int n_zones) {
+  Param p = make_param(*pv);
+  std::vector<Zone> zones;
+  int ioff = 0;
+  for (int b = 0; b < n_zones; ++b) {
+    zones.push_back(make_zone(zvs[b], nullptr, 0, p));
+    zones.back().inner.assign(inner + ioff, inner + ioff + n_inner[b]);
+    ioff += n_inner[b];
+  }
+  inner_exchange(zones, p);
+  return 0;
+}
+
 void oracle_nasa7_h_cp(const cb2_mechanism *m, double t, double *h, double *cp) {
   cb2_param_view pv{};
   pv.mech = m;

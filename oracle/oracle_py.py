@@ -40,6 +40,9 @@ def load():
             "oracle_cfl_dt": (C.c_int, [P(abi.ParamView), P(abi.ZoneView), P(C.c_double)]),
             "oracle_rk3_step": (C.c_int, [P(abi.ParamView), P(abi.ZoneView), P(abi.FaceBC), P(C.c_int), C.c_int,
                                           P(C.c_double), C.c_int]),
+            "oracle_rk3_step_inner": (C.c_int, [P(abi.ParamView), P(abi.ZoneView), P(abi.FaceBC), P(C.c_int),
+                                                P(abi.InnerFace), P(C.c_int), C.c_int, P(C.c_double), C.c_int]),
+            "oracle_halo": (C.c_int, [P(abi.ParamView), P(abi.ZoneView), P(abi.InnerFace), P(C.c_int), C.c_int]),
             "oracle_nasa7_h_cp": (None, [P(abi.Mechanism), C.c_double, P(C.c_double), P(C.c_double)]),
             "oracle_vt_relaxation": (C.c_int, [P(abi.ParamView), P(abi.ZoneView), C.c_double]),
             "oracle_two_temperature_state": (None, [P(abi.ParamView), C.c_double, C.c_double, C.c_double,
@@ -137,6 +140,29 @@ def rk3_step(param, blocks, faces_per_block, dt, fixed_dt=True):
     d = C.c_double(dt)
     load().oracle_rk3_step(C.byref(param), views, _faces(flat), nf, len(blocks), C.byref(d), 1 if fixed_dt else 0)
     return d.value
+
+
+def rk3_step_inner(param, blocks, faces_per_block, inner_per_block, dt, fixed_dt=True):
+    """One RK3 step of a multi-block grid with its inner faces (abi.InnerFace lists per block)."""
+    views = (abi.ZoneView * len(blocks))(*[b.view() for b in blocks])
+    flat = [f for fl in faces_per_block for f in fl]
+    nf = (C.c_int * len(blocks))(*[len(fl) for fl in faces_per_block])
+    iflat = [f for fl in inner_per_block for f in fl]
+    inner = (abi.InnerFace * max(1, len(iflat)))(*iflat)
+    ni = (C.c_int * len(blocks))(*[len(fl) for fl in inner_per_block])
+    d = C.c_double(dt)
+    load().oracle_rk3_step_inner(C.byref(param), views, _faces(flat), nf, inner, ni, len(blocks), C.byref(d),
+                                 1 if fixed_dt else 0)
+    return d.value
+
+
+def halo(param, blocks, inner_per_block):
+    """The inner-face exchange alone (cb2_halo) over the host blocks."""
+    views = (abi.ZoneView * len(blocks))(*[b.view() for b in blocks])
+    iflat = [f for fl in inner_per_block for f in fl]
+    inner = (abi.InnerFace * max(1, len(iflat)))(*iflat)
+    ni = (C.c_int * len(blocks))(*[len(fl) for fl in inner_per_block])
+    load().oracle_halo(C.byref(param), views, inner, ni, len(blocks))
 
 
 def chemistry_source(mech, rho, t, y):

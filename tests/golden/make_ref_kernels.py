@@ -38,7 +38,7 @@ FIXTURE = os.path.join(HERE, "ref_kernels.npz")
 
 
 def _runner(family):
-    return os.path.join(REPO, "oracle", "_ref", "ref_stage_runner" + ("_2t" if family == "air5" else ""))
+    return os.path.join(REPO, "oracle", "_ref", "ref_stage_runner" + ("_2t" if family in ("air5", "c5") else ""))
 
 
 def cmd_write(args):
@@ -59,7 +59,10 @@ def cmd_write(args):
         if args.only and c["name"] not in args.only.split(","):
             continue
         d = os.path.join(args.work, c["name"])
-        digests[c["name"]] = refcases.write_reference_case(c, d, ref)
+        if c["family"] == "c5":
+            digests[c["name"]] = refcases.write_reference_multi(c, d, ref)
+        else:
+            digests[c["name"]] = refcases.write_reference_case(c, d, ref)
         print("wrote", d)
     with open(dpath, "w") as f:
         json.dump(digests, f, indent=1)
@@ -85,6 +88,8 @@ def cmd_run(args):
             print("runner failed on %s (rc %d): %s" % (n, r.returncode, r.stderr[-500:]))
             continue
         os.replace(os.path.join(d, "out.bin"), os.path.join(args.out, n, "out.bin"))
+        if os.path.exists(os.path.join(d, "ref_metric.bin")):
+            os.replace(os.path.join(d, "ref_metric.bin"), os.path.join(args.out, n, "ref_metric.bin"))
         print(n, r.stdout.strip().splitlines()[-1] if r.stdout.strip() else "")
 
 
@@ -114,6 +119,20 @@ def cmd_pack(args):
             j = blk["dims"][1] // 2
             arrays[n + "/cv"] = blk["cv"][:, g, g + j, g:-g]
             arrays[n + "/dts"] = d["dts"]
+        elif c["family"] == "c5":
+            nb = len(d["blocks"])
+            for b, bk in enumerate(d["blocks"]):
+                arrays[n + "/dq0/%d" % b] = d["dq"][b]
+                arrays[n + "/cv/%d" % b] = refcases.interior(bk["cv"], g)
+                arrays[n + "/T/%d" % b] = refcases.interior(bk["bv"], g)[5]
+                arrays[n + "/Tve/%d" % b] = refcases.interior(bk["temperature_ve"], g)[0]
+            meta[n]["n_block"] = nb
+            # the reference Mesh's own metric and Jacobian of every padded node (before the runner
+            # loaded the case's), which pin the host grid module that computes them here
+            mp = os.path.join(args.out, n, "ref_metric.bin")
+            if os.path.exists(mp):
+                raw = np.fromfile(mp, dtype="<f8")
+                arrays[n + "/ref_metric"] = raw
         else:
             arrays[n + "/dq0"] = d["dq"][0]
             arrays[n + "/cv"] = refcases.interior(blk["cv"], g)

@@ -391,3 +391,103 @@ def read_dump(path):
 def interior(a, g):
     return a[(slice(None), slice(g, -g), slice(g, -g), slice(g, -g))] if a.shape[1] > 2 * g else \
         a[(slice(None), slice(g, g + 1), slice(g, -g), slice(g, -g))]
+
+
+# ---- the multi-block two-temperature square cylinder ("c5") -----------------------------------
+C5_MINI = dict(n_side=12, n_normal=10, first=2e-4, half_box=0.03)
+
+
+def _c5(name, visc=2, pp=1, limit_flow=1, stages=3, dt=1e-8):
+    return dict(family="c5", name=name, scheme=52, rec=5, visc=visc, bc="cylinder", stages=stages, dt=dt, seed=0,
+                pp=pp, limit_flow=limit_flow, reaction=1)
+
+
+CASES.append(_c5("c5_air5_cylinder_4blocks"))
+
+
+def build_multi(case):
+    """(param, blocks, faces per block, inner faces per block, extra) of a multi-block case."""
+    m, tt = _mech("air5")
+    c = cases.square_cylinder_air5(m, tt, ngg=ref_ngg(case["scheme"], case["visc"]), viscous_order=case["visc"],
+                                   reaction=bool(case["reaction"]), **C5_MINI)
+    p = c.param
+    p.positive_preserving = case["pp"]
+    p.limit_flow = case["limit_flow"]
+    p.dt = case["dt"]
+    return p, c.blocks, c.faces, c.meta["inner"], {"mech": m, "two_t": tt, "case": c}
+
+
+def multi_state_digest(blocks):
+    h = hashlib.sha256()
+    sums = []
+    for hb in blocks:
+        d = state_digest({"family": "air5"}, hb)
+        h.update(d["sha256"].encode())
+        sums += d["sums"]
+    return {"sha256": h.hexdigest(), "sums": sums}
+
+
+def write_reference_multi(case, case_dir, ref_dir):
+    """The reference's input files of a multi-block case (grid, boundary and inner-face files of
+    every block, setup, state.bin with the blocks in order)."""
+    p, blocks, faces, inner, extra = build_multi(case)
+    c = extra["case"]
+    g = c.meta["grid"]
+    fs = c.meta["freestream"]
+    nb = len(blocks)
+    for d in ("grid", "boundary_condition", "chemistry"):
+        os.makedirs(os.path.join(case_dir, "input", d), exist_ok=True)
+    os.makedirs(os.path.join(case_dir, "output", "message"), exist_ok=True)
+    with open(os.path.join(case_dir, "input", "grid", "grid%4d.grd" % 0), "w") as f:
+        f.write("%d\n" % nb)
+        for hb in blocks:
+            f.write("%d %d %d\n" % (hb.mx, hb.my, hb.mz))
+        for (x, y, z) in g["xyz"]:
+            for arr in (x, y, z):
+                f.write("\n".join("%.17g" % v for v in np.asarray(arr).ravel()) + "\n")
+    with open(os.path.join(case_dir, "input", "boundary_condition", "boundary%4d.txt" % 0), "w") as f:
+        for fl in g["faces"]:
+            f.write("%d\n" % len(fl))
+            for line in fl:
+                f.write("%d %d %d %d %d %d %d\n" % line)
+    with open(os.path.join(case_dir, "input", "boundary_condition", "inner%4d.txt" % 0), "w") as f:
+        f.write("%d\n" % sum(len(x) for x in g["inner"]))
+        f.write(" ".join("%d" % len(x) for x in g["inner"]) + "\n")
+        f.write("iMin iMax jMin jMax kMin kMax id\n")
+        for pairs in g["inner"]:
+            for a, b in pairs:
+                f.write("%d %d %d %d %d %d %d\n" % a)
+                f.write("%d %d %d %d %d %d %d\n" % b)
+    s = ["bool parallel = 0", "int gridIsBinary = 0", "int mesh_file_type = 0", "bool steady = 0",
+         "int temporal_scheme = 3", "int total_step = 1000000", "int output_screen = 1000000",
+         "int inviscid_scheme = %d" % case["scheme"], "int reconstruction = 2", "int limiter = 0",
+         "int viscous_order = %d" % case["visc"], "bool positive_preserving = %d" % case["pp"],
+         "bool limit_flow = %d" % case["limit_flow"], "real prandtl_number = 0.72", "int shock_sensor = 0",
+         "real shockSensor_threshold = 0", "real shockSensor_epsilon = -1", "bool gradPInDiffusionFlux = 0",
+         "bool fixed_time_step = 1", "real dt = %r" % case["dt"], "real cfl = 0.3",
+         "int species = 1", "int reaction = %d" % case["reaction"], "int chemSrcMethod = 0", "int therm_nasa_7_9 = 9",
+         "bool enable_vt_relaxation = 1"]
+    for key, rel in AIR5_FILES.items():
+        shutil.copy(os.path.join(ref_dir, rel), os.path.join(case_dir, "input", "chemistry", os.path.basename(rel)))
+        s.append("string %s = chemistry/%s" % (key, os.path.basename(rel)))
+    names = extra["mech"].species
+    s += ["array string boundary_conditions {", "    freestream outflow wall", "}",
+          "struct freestream {", "    string type = inflow", "    int label = 5", "    int inflow_type = 0",
+          "    real velocity = %r" % fs["u"], "    real temperature = %r" % fs["T"], "    real Tve = %r" % fs["Tve"],
+          "    real pressure = %r" % fs["p"], "    real u = 1.0", "    real v = 0.0", "    real w = 0.0"]
+    s += ["    real %s = %r" % (n, float(yv)) for n, yv in zip(names, fs["y"])]
+    s += ["}", "struct outflow {", "    string type = outflow", "    int label = 6", "}",
+          "struct wall {", "    string type = wall", "    int label = 2", "    string thermal_type = isothermal",
+          "    real temperature = 300.0", "    real Tve = 300.0", "}",
+          "string reference_state = freestream", "string default_init = freestream"]
+    with open(os.path.join(case_dir, "input", "setup.txt"), "w") as f:
+        f.write("\n".join(s) + "\n")
+    with open(os.path.join(case_dir, "state.bin"), "wb") as f:
+        for hb in blocks:
+            for a in state_arrays({"family": "air5"}, hb):
+                f.write(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+    task = {"mode": "stages", "stages": case["stages"], "dt": case["dt"], "fixed_dt": 1, "mul_constant": 0.0,
+            "load_metric": 1}
+    with open(os.path.join(case_dir, "task.txt"), "w") as f:
+        f.write("".join(("%s %s\n" if isinstance(v, str) else "%s %r\n") % (k, v) for k, v in task.items()))
+    return multi_state_digest(blocks)

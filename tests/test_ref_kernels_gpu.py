@@ -45,7 +45,8 @@ def _fixture():
 
 
 def _names(kind):
-    return [c["name"] for c in refcases.CASES if (c["family"] == "sod") == (kind == "sod")]
+    fam = {"stage": lambda f: f not in ("sod", "c5"), "sod": lambda f: f == "sod", "multi": lambda f: f == "c5"}[kind]
+    return [c["name"] for c in refcases.CASES if fam(c["family"])]
 
 
 def _rel(a, b, momentum=False):
@@ -133,3 +134,62 @@ def test_sod_matches_reference_kernels(name):
     cv = dev.to_host(["cv"])["cv"][:, g, g + j, g:-g]
     assert _rel(cv[[0, 1, 4]], z[name + "/cv"][[0, 1, 4]]) < 1e-7
     ctx.close()
+
+
+@pytest.mark.parametrize("name", _names("multi"))
+def test_multiblock_stages_match_reference_kernels(name):
+    """Four-block two-temperature AIR5 square cylinder (body-fitted 2-D grid, isothermal wall with
+    T_ve, freestream inflow, outflow, inner faces between the blocks, positivity limiter and
+    limit_flow): the reference's initialisation, then three stages with the inner-face exchange
+    (cb2_halo) after every stage's boundary conditions."""
+    z, meta = _fixture()
+    if name not in meta:
+        pytest.skip("case not in the fixture")
+    mc = meta[name]
+    case = mc["case"]
+    import torch
+    p, blocks, faces, inner, extra = refcases.build_multi(case)
+    assert refcases.same_state(refcases.multi_state_digest(blocks), mc["digest"])
+    p.rho_ref, p.v_ref = mc["rho_inf"], mc["v_inf"]
+    p.p_ref, p.c_ref = mc["p_inf"], mc["speed_of_sound"]
+    devs = [DeviceBlock(hb) for hb in blocks]
+    ctx = cb200.Context(p)
+    nb = len(blocks)
+    for b in range(nb):
+        ctx.bind(b, devs[b].view(), faces[b])
+    for b in range(nb):
+        ctx.bind_inner_faces(b, inner[b])
+    for b in range(nb):
+        ctx.properties(b)
+    for b in range(nb):
+        ctx.boundary(b)
+    ctx.halo()
+    for b in range(nb):
+        ctx.properties(b)
+    for b in range(nb):
+        ctx.cv_from_bv(b)
+        ctx.store_qn(b)
+    dq0 = []
+    for rk in range(case["stages"]):
+        for b in range(nb):
+            ctx.rhs(b)
+            if rk == 0:
+                torch.cuda.synchronize()
+                dq0.append(devs[b].to_host(["dq"])["dq"])
+            ctx.stage_update(b, case["dt"], rk)
+            ctx.boundary(b)
+        ctx.halo()
+        for b in range(nb):
+            ctx.properties(b)
+    torch.cuda.synchronize()
+    assert ctx.read_status() == 0
+    errs = {}
+    for b in range(nb):
+        g = blocks[b].ngg
+        out = devs[b].to_host(["cv", "bv", "temperature_ve"])
+        errs["dq%d" % b] = _rel(dq0[b], z[name + "/dq0/%d" % b], momentum=True)
+        errs["cv%d" % b] = _rel(refcases.interior(out["cv"], g), z[name + "/cv/%d" % b], momentum=True)
+        errs["T%d" % b] = _rel(refcases.interior(out["bv"], g)[5][None], z[name + "/T/%d" % b][None])
+        errs["Tve%d" % b] = _rel(refcases.interior(out["temperature_ve"], g)[0][None], z[name + "/Tve/%d" % b][None])
+    ctx.close()
+    assert max(errs.values()) < TOL, errs
