@@ -8,8 +8,9 @@
 // One rank, rank 0 of a world of 1.  Collectives copy the send buffer to the receive buffer (the
 // result of any reduction over one rank); point-to-point calls are never made by a serial run
 // (`parallel = 0`) and return an error if they are.  Files are plain stdio files addressed by
-// byte offsets; derived (subarray) file views are not supported and report an error, so a code
-// path that depends on them fails loudly instead of reading garbage.
+// byte offsets; of the derived datatypes only 3-D Fortran-order subarrays of doubles read with
+// MPI_File_read (the reference's binary grid reader) are supported; other uses report an error,
+// so a code path that depends on them fails loudly instead of reading garbage.
 #pragma once
 #include <cstdio>
 #include <cstdlib>
@@ -108,14 +109,29 @@ inline int MPI_Isend(const void *, int, MPI_Datatype, int, int, MPI_Comm, MPI_Re
 inline int MPI_Irecv(void *, int, MPI_Datatype, int, int, MPI_Comm, MPI_Request *) { return MPI_ERR_OTHER; }
 inline int MPI_Waitall(int, MPI_Request *, MPI_Status *) { return MPI_SUCCESS; }
 
-// ---- derived datatypes: contiguous ones only ----
+// ---- derived datatypes: contiguous ones, and 3-D Fortran-order subarrays of doubles for reads ----
 inline int MPI_Type_contiguous(int n, MPI_Datatype t, MPI_Datatype *nt) {
   *nt = n * cb2_mpi_type_size(t) * 16 + 15;
   return MPI_SUCCESS;
 }
-inline int MPI_Type_create_subarray(int, const int *, const int *, const int *, int, MPI_Datatype, MPI_Datatype *nt) {
-  *nt = 0;  // size 1: any file access through it is refused below
-  return MPI_ERR_OTHER;
+// A registered subarray: its handle is a negative index into this table.
+struct cb2_mpi_subarray { int sizes[3], subsizes[3], starts[3]; };
+inline cb2_mpi_subarray *cb2_mpi_subarrays() {
+  static cb2_mpi_subarray table[64];
+  return table;
+}
+inline int &cb2_mpi_n_subarrays() {
+  static int n = 0;
+  return n;
+}
+inline int MPI_Type_create_subarray(int ndims, const int *sizes, const int *subsizes, const int *starts, int order,
+                                    MPI_Datatype old, MPI_Datatype *nt) {
+  *nt = 0;  // size 1: any file access through an unsupported type is refused below
+  if (ndims != 3 || order != MPI_ORDER_FORTRAN || old != MPI_DOUBLE || cb2_mpi_n_subarrays() >= 64) return MPI_ERR_OTHER;
+  cb2_mpi_subarray &d = cb2_mpi_subarrays()[cb2_mpi_n_subarrays()];
+  for (int a = 0; a < 3; ++a) d.sizes[a] = sizes[a], d.subsizes[a] = subsizes[a], d.starts[a] = starts[a];
+  *nt = -1 - cb2_mpi_n_subarrays()++;
+  return MPI_SUCCESS;
 }
 inline int MPI_Type_commit(MPI_Datatype *) { return MPI_SUCCESS; }
 inline int MPI_Type_free(MPI_Datatype *) { return MPI_SUCCESS; }
@@ -140,7 +156,7 @@ inline int MPI_File_close(MPI_File *fh) {
   return MPI_SUCCESS;
 }
 inline int cb2_mpi_file_io(MPI_File fh, long long off, void *buf, int n, MPI_Datatype t, bool write) {
-  if (!fh || t == 0) return MPI_ERR_OTHER;
+  if (!fh || t <= 0) return MPI_ERR_OTHER;
   if (off >= 0 && std::fseek(fh->fp, off, SEEK_SET) != 0) return MPI_ERR_OTHER;
   const size_t bytes = static_cast<size_t>(n) * cb2_mpi_type_size(t);
   const size_t done = write ? std::fwrite(buf, 1, bytes, fh->fp) : std::fread(buf, 1, bytes, fh->fp);
@@ -153,6 +169,19 @@ inline int MPI_File_write_at(MPI_File fh, MPI_Offset off, const void *buf, int n
   return cb2_mpi_file_io(fh, off, const_cast<void *>(buf), n, t, true);
 }
 inline int MPI_File_read(MPI_File fh, void *buf, int n, MPI_Datatype t, MPI_Status *) {
+  if (t < 0 && fh && n == 1 && -1 - t < cb2_mpi_n_subarrays()) {
+    // one subarray: read its elements in file order (first index fastest) into their places in
+    // the full array at buf
+    const cb2_mpi_subarray &d = cb2_mpi_subarrays()[-1 - t];
+    double *out = static_cast<double *>(buf);
+    for (int k = 0; k < d.subsizes[2]; ++k)
+      for (int j = 0; j < d.subsizes[1]; ++j) {
+        double *row = out + d.starts[0] +
+                      (size_t)d.sizes[0] * ((d.starts[1] + j) + (size_t)d.sizes[1] * (d.starts[2] + k));
+        if (std::fread(row, sizeof(double), d.subsizes[0], fh->fp) != (size_t)d.subsizes[0]) return MPI_ERR_OTHER;
+      }
+    return MPI_SUCCESS;
+  }
   return cb2_mpi_file_io(fh, -1, buf, n, t, false);
 }
 inline int MPI_File_write(MPI_File fh, const void *buf, int n, MPI_Datatype t, MPI_Status *) {

@@ -23,8 +23,8 @@
 //
 // Usage: ref_stage_runner <case-dir>
 //   <case-dir>/input/setup.txt, input/grid/grid   0.grd, input/boundary_condition/{boundary,inner}   0.txt
-//   <case-dir>/task.txt   : "key value" lines: mode (stages|steps), stages, n_steps, dt, fixed_dt, t_end,
-//                           mul_constant, load_metric (0/1), init (file|reference)
+//   <case-dir>/task.txt   : "key value" lines: mode (stages|steps|time), stages, n_steps, warmup, dt,
+//                           fixed_dt, t_end, mul_constant, load_metric (0/1), init (file|reference)
 //   <case-dir>/state.bin  : per block, float64 padded arrays (ghost ngg): bv[6], sv[n_scalar],
 //                           T_ve (two-temperature build), then metric[9] and jac when load_metric = 1
 //   writes <case-dir>/out.bin : the layout is written out above the dump in run().
@@ -56,7 +56,10 @@
 
 namespace {
 
+bool g_checks = true;  // off while a timed run measures the step sequence alone
+
 void check(const char *where) {
+  if (!g_checks) return;
   cudaError_t e = cudaDeviceSynchronize();
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -300,6 +303,32 @@ int run(cfd::Parameter &parameter, cfd::Mesh &mesh, cfd::Species &spec, cfd::Rea
   if (mode == "stages") {
     dt = r.step<mix>(1, dt, fixed_dt, static_cast<int>(tget(task, "stages", 1)), &dq);
     steps = 1;
+  } else if (mode == "time") {
+    // warm-up steps, then n_steps steps between two CUDA events with no synchronisation of the
+    // runner's own in between (the CFL step's global minimum still copies dt to the host, as RK3
+    // does); the mean step time goes to time.txt
+    const int n_warm = static_cast<int>(tget(task, "warmup", 3)), n_time = static_cast<int>(tget(task, "n_steps", 10));
+    for (int s = 0; s < n_warm; ++s) dt = r.step<mix>(s + 1, dt, fixed_dt, 3, nullptr);
+    check("warm-up");
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    g_checks = false;
+    cudaEventRecord(e0);
+    for (int s = 0; s < n_time; ++s) dt = r.step<mix>(n_warm + s + 1, dt, fixed_dt, 3, nullptr);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    g_checks = true;
+    check("timed steps");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    std::FILE *tf = std::fopen("time.txt", "w");
+    if (tf) {
+      std::fprintf(tf, "%d %.9g %.17g\n", n_time, ms / n_time, dt);
+      std::fclose(tf);
+    }
+    std::printf("ref_stage_runner: %d timed step(s), %.6f ms per step, dt = %.17g\n", n_time, ms / n_time, dt);
+    return 0;
   } else {
     const long long n_steps = static_cast<long long>(tget(task, "n_steps", 1));
     const double t_end = tget(task, "t_end", 1e300);
