@@ -25,16 +25,24 @@ namespace cb2 {
 // 0 U_k = (rho u . grad k)/rho, 1-3 rho u_m U_k + p k_m, 4 p, 5 c |grad k|, 6 J.
 constexpr int kNF = 7;
 
+// The interface flux row v goes to out[v * os].  The scalar rows are written as soon as they are
+// known, and out[v * os] (v >= 5) holds the row's energy coefficient until then, so that no
+// per-scalar array stays in registers across the five characteristic fields.
 template <int NS, int ORDER, bool TT = false>
 __device__ __forceinline__ void char_flux(const double *__restrict__ sQ, const double *__restrict__ sF, int NN,
                                           int c, int st, double kx, double ky, double kz, double eps,
-                                          bool shock, const Mech &mech, double *fc) {
+                                          bool shock, const Mech &mech, double *out, int os) {
   constexpr int NSC = NS + (TT ? 1 : 0);  // transported scalars: species (+ e_ve)
   constexpr int NV = 5 + NSC;
   constexpr int R = ORDER / 2 + 1;  // nodes on each side of the interface
   constexpr int NW = 2 * R - 1;     // values per WENO side
 #define Qv(v, m) sQ[(v) * NN + c + (m) * st]
 #define Fv(f, m) sF[(f) * NN + c + (m) * st]
+  // reads inside the per-field loops: volatile, so that the stencil is not held in registers
+  // across the fields
+  const volatile double *vQ = sQ, *vF = sF;
+#define QvL(v, m) vQ[(v) * NN + c + (m) * st]
+#define FvL(f, m) vF[(f) * NN + c + (m) * st]
   // Roe average at the interface between node c (m = 0) and c + st (m = 1)
   const double rho_l = Qv(0, 0), rho_r = Qv(0, 1);
   double t1 = sqrt(rho_l * rho_r);
@@ -43,12 +51,14 @@ __device__ __forceinline__ void char_flux(const double *__restrict__ sQ, const d
   const double vm = rlc * Qv(2, 0) + rrc * Qv(2, 1);
   const double wm = rlc * Qv(3, 0) + rrc * Qv(3, 1);
   double cm, gm1;
-  double svm[NSC > 0 ? NSC : 1], alpha[NSC > 0 ? NSC : 1], ecoef[NSC > 0 ? NSC : 1];
+  // scalar-coupling sums sum_s alpha_s Q_s and sum_s alpha_s Q_s U_k at each stencil node
+  double sbq[NS > 0 ? 2 * R : 1], sbf[NS > 0 ? 2 * R : 1];
   if constexpr (NS == 0) {
     const double t_roe = (rlc * Fv(4, 0) + rrc * Fv(4, 1)) / kRAir;
     cm = sqrt(kGammaAir * kRAir * t_roe);
     gm1 = kGammaAir - 1;
   } else {
+    double svm[NSC], alpha[NSC], ecoef[NSC];
     double rmix = 0;
 #pragma unroll
     for (int s = 0; s < NSC; ++s) svm[s] = rlc * Qv(5 + s, 0) + rrc * Qv(5 + s, 1);
@@ -59,6 +69,19 @@ __device__ __forceinline__ void char_flux(const double *__restrict__ sQ, const d
     if constexpr (TT) characteristic_thermo_2t<NS>(t_roe, svm, mech, gamma, cm, alpha, ecoef);
     else characteristic_thermo<NS>(t_roe, svm, mech, gamma, cm, alpha, ecoef, nullptr);
     gm1 = gamma - 1;
+#pragma unroll
+    for (int s = 0; s < NSC; ++s) out[(5 + s) * os] = ecoef[s];
+#pragma unroll
+    for (int m = 0; m < 2 * R; ++m) {
+      double sp = 0, sm = 0;
+#pragma unroll
+      for (int s = 0; s < NSC; ++s) {
+        sp = fma(alpha[s], Qv(5 + s, m - R + 1), sp);
+        sm = fma(alpha[s], Qv(5 + s, m - R + 1) * Fv(0, m - R + 1), sm);
+      }
+      sbq[m] = sp;
+      sbf[m] = sm;
+    }
   }
   // orthonormal basis (k, n, q)
   t1 = rnorm3d(kx, ky, kz);
@@ -84,23 +107,7 @@ __device__ __forceinline__ void char_flux(const double *__restrict__ sQ, const d
     const double l = fabs(Fv(0, m)) + Fv(5, m);
     if (l > lam) lam = l;
   }
-  // scalar-coupling sums sum_s alpha_s Q_s and sum_s alpha_s Q_s U_k at each node
-  double sbq[2 * R], sbf[2 * R];
-  if constexpr (NS > 0) {
-#pragma unroll
-    for (int m = 0; m < 2 * R; ++m) {
-      double sp = 0, sm = 0;
-#pragma unroll
-      for (int s = 0; s < NSC; ++s) {
-        sp = fma(alpha[s], Qv(5 + s, m - R + 1), sp);
-        sm = fma(alpha[s], Qv(5 + s, m - R + 1) * Fv(0, m - R + 1), sm);
-      }
-      sbq[m] = sp;
-      sbf[m] = sm;
-    }
-  }
-
-  double fch[NV];
+  double fch[5];
   // one characteristic field at a time: keeps the stencil projections of a single field live
 #pragma unroll 1
   for (int l = 0; l < 5; ++l) {
@@ -125,55 +132,53 @@ __device__ __forceinline__ void char_flux(const double *__restrict__ sQ, const d
 #pragma unroll
     for (int m = 0; m < 2 * R; ++m) {
       const int o = m - R + 1;
-      const double uk = Fv(0, o);
-      double LF = L0 * (Qv(0, o) * uk) + L1 * Fv(1, o) + L2 * Fv(2, o) + L3 * Fv(3, o) + L4 * ((Qv(4, o) + Fv(4, o)) * uk);
-      double LQ = L0 * Qv(0, o) + L1 * Qv(1, o) + L2 * Qv(2, o) + L3 * Qv(3, o) + L4 * Qv(4, o);
+      const double uk = FvL(0, o);
+      const double q0 = QvL(0, o), q4 = QvL(4, o);
+      double LF = L0 * (q0 * uk) + L1 * FvL(1, o) + L2 * FvL(2, o) + L3 * FvL(3, o) + L4 * ((q4 + FvL(4, o)) * uk);
+      double LQ = L0 * q0 + L1 * QvL(1, o) + L2 * QvL(2, o) + L3 * QvL(3, o) + L4 * q4;
       if constexpr (NS > 0) {
         LF += tc * sbf[m];
         LQ += tc * sbq[m];
       }
-      const double hj = 0.5 * Fv(6, o);
+      const double hj = 0.5 * FvL(6, o);
       if (m < NW) vp[m] = hj * (LF + lam * LQ);
       if (m > 0) vmn[m - 1] = hj * (LF - lam * LQ);
     }
     fch[l] = weno_pm<ORDER>(vp, vmn, eps, shock);
   }
+  // back-projection with the right eigenvectors
+  const double f034 = fch[0] + fch[3] + fch[4];
+  const double f04 = fch[0] - fch[4];
+  double e = 0;
   if constexpr (NS > 0) {
 #pragma unroll 1
     for (int s = 0; s < NSC; ++s) {
+      const double svs = rlc * QvL(5 + s, 0) + rrc * QvL(5 + s, 1);
       double vp[NW], vmn[NW];
 #pragma unroll
       for (int m = 0; m < 2 * R; ++m) {
         const int o = m - R + 1;
-        const double LQ = Qv(5 + s, o) - svm[s] * Qv(0, o);
-        const double LF = Fv(0, o) * LQ;
-        const double hj = 0.5 * Fv(6, o);
+        const double LQ = QvL(5 + s, o) - svs * QvL(0, o);
+        const double LF = FvL(0, o) * LQ;
+        const double hj = 0.5 * FvL(6, o);
         if (m < NW) vp[m] = hj * (LF + lam * LQ);
         if (m > 0) vmn[m - 1] = hj * (LF - lam * LQ);
       }
-      fch[5 + s] = weno_pm<ORDER>(vp, vmn, eps, shock);
+      const double fs = weno_pm<ORDER>(vp, vmn, eps, shock);
+      e += out[(5 + s) * os] * fs;
+      out[(5 + s) * os] = svs * f034 + fs;
     }
   }
-  // back-projection with the right eigenvectors
-  const double f034 = fch[0] + fch[3] + fch[4];
-  const double f04 = fch[0] - fch[4];
-  fc[0] = f034;
-  fc[1] = um * f034 - kx * cm * f04 + nx * fch[1] + qx * fch[2];
-  fc[2] = vm * f034 - ky * cm * f04 + ny * fch[1] + qy * fch[2];
-  fc[3] = wm * f034 - kz * cm * f04 + nz * fch[1] + qz * fch[2];
+  out[0] = f034;
+  out[os] = um * f034 - kx * cm * f04 + nx * fch[1] + qx * fch[2];
+  out[2 * os] = vm * f034 - ky * cm * f04 + ny * fch[1] + qy * fch[2];
+  out[3 * os] = wm * f034 - kz * cm * f04 + nz * fch[1] + qz * fch[2];
   const double h_roe = rlc * (Qv(4, 0) + Fv(4, 0)) + rrc * (Qv(4, 1) + Fv(4, 1));
-  fc[4] = h_roe * f034 - Uk_bar * cm * f04 + Un * fch[1] + Uq * fch[2] - cm * cm / gm1 * fch[3];
-  if constexpr (NS > 0) {
-    double e = 0;
-#pragma unroll
-    for (int s = 0; s < NSC; ++s) {
-      fc[5 + s] = svm[s] * f034 + fch[5 + s];
-      e += ecoef[s] * fch[5 + s];
-    }
-    fc[4] += e;
-  }
+  out[4 * os] = h_roe * f034 - Uk_bar * cm * f04 + Un * fch[1] + Uq * fch[2] - cm * cm / gm1 * fch[3] + e;
 #undef Qv
 #undef Fv
+#undef QvL
+#undef FvL
 }
 
 // Loads node data of one slot: conservative variables, U_k, momentum fluxes, p, c|grad k|, J.
@@ -212,15 +217,16 @@ __device__ __forceinline__ void load_node(const Zone &z, idx_t g, double *sQ, do
 // temperatures, e_ve).  Slots cl / cr of the left / right node.
 template <int NS>
 __device__ __forceinline__ void positive_limit(const double *sQ, const double *sF, int NN, int cl, int cr,
-                                               const Param &p, double *fc) {
+                                               const Param &p, double *out, int os) {
+#define fc(v) out[(v) * os]
   const double dt = step_dt(p, p.dt);
   const double alpha = p.dim == 3 ? 1.0 / 3.0 : 0.5;
   const double jl = sF[6 * NN + cl], jr = sF[6 * NN + cr];
   const double alphaL = 0.5 * alpha * jl, alphaR = 0.5 * alpha * jr;
   int start = -1;
   for (int s = 0; s < NS; ++s) {
-    const double up = alphaL * sQ[(s + 5) * NN + cl] - dt * fc[s + 5];
-    const double um = alphaR * sQ[(s + 5) * NN + cr] + dt * fc[s + 5];
+    const double up = alphaL * sQ[(s + 5) * NN + cl] - dt * fc(s + 5);
+    const double um = alphaR * sQ[(s + 5) * NN + cr] + dt * fc(s + 5);
     if (up < 0 || um < 0) {
       start = s;
       break;
@@ -235,7 +241,7 @@ __device__ __forceinline__ void positive_limit(const double *sQ, const double *s
     const double yl = sQ[(s + 5) * NN + cl], yr = sQ[(s + 5) * NN + cr];
     const double fp = 0.5 * jl * (Ul + sF[5 * NN + cl]) * yl;
     const double fm = 0.5 * jr * (Ur - sF[5 * NN + cr]) * yr;
-    const double up = alphaL * yl - dt * fc[s + 5];
+    const double up = alphaL * yl - dt * fc(s + 5);
     if (up < 0) {
       f1 = 0.5 * (fp + U1 * yl) + 0.5 * (fm - U2 * yr);
       have_f1 = true;
@@ -246,7 +252,7 @@ __device__ __forceinline__ void positive_limit(const double *sQ, const double *s
         else if (theta_p < 0) theta_p = 0;
       }
     }
-    const double um = alphaR * yr + dt * fc[s + 5];
+    const double um = alphaR * yr + dt * fc(s + 5);
     if (um < 0) {
       if (!have_f1) f1 = 0.5 * (fp + U1 * yl) + 0.5 * (fm - U2 * yr);
       const double um_lf = alphaR * yr + dt * f1;
@@ -256,12 +262,13 @@ __device__ __forceinline__ void positive_limit(const double *sQ, const double *s
         else if (theta_m < 0) theta_m = 0;
       }
     }
-    fc[s + 5] = fmin(theta_p, theta_m) * (fc[s + 5] - f1) + f1;
+    fc(s + 5) = fmin(theta_p, theta_m) * (fc(s + 5) - f1) + f1;
   }
+#undef fc
 }
 
 template <int NS, int DIR, int ORDER, bool TT = false>
-__global__ void __launch_bounds__(kSweepThreads) k_weno_char(Zone z, Param p, idx_t run) {
+__global__ void __launch_bounds__(kSweepThreads, 2) k_weno_char(Zone z, Param p, idx_t run) {
   constexpr int NV = 5 + NS + (TT ? 1 : 0);
   constexpr int R = ORDER / 2 + 1;
   constexpr int NN = DIR == 0 ? (kSweepThreads + 2 * R - 1) : kTI * (kTS + 2 * R - 1);
@@ -332,13 +339,12 @@ __global__ void __launch_bounds__(kSweepThreads) k_weno_char(Zone z, Param p, id
         if (z.shock[gs] > p.sensor_threshold) { shock = true; break; }
       }
     }
-    double fc[NV];
-    char_flux<NS, ORDER, TT>(sQ, sF, NN, c, st, kx, ky, kz, kWenoEps * p.weno_eps_scale, shock, p.mech, fc);
+    char_flux<NS, ORDER, TT>(sQ, sF, NN, c, st, kx, ky, kz, kWenoEps * p.weno_eps_scale, shock, p.mech,
+                             sFl + tid, kSweepThreads);
     if constexpr (NS > 0) {
-      if (p.positive_preserving) positive_limit<NS + (TT ? 1 : 0)>(sQ, sF, NN, c, c + st, p, fc);
+      if (p.positive_preserving)
+        positive_limit<NS + (TT ? 1 : 0)>(sQ, sF, NN, c, c + st, p, sFl + tid, kSweepThreads);
     }
-#pragma unroll
-    for (int v = 0; v < NV; ++v) sFl[v * kSweepThreads + tid] = fc[v];
   }
   __syncthreads();
 

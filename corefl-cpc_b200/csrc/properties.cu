@@ -19,18 +19,73 @@ __global__ void __launch_bounds__(kPropThreads) k_properties(Zone z, Param p) {
   properties_point<NS>(z, p, i, j, k);
 }
 
+// A 2-D block (mz = 1) carries ngg ghost planes on each side of its one k plane.  The reference
+// evaluates the properties on every one of them (src/RK.cuh:230-235); after eliminate_k_gradient
+// their basic and scalar variables are copies of plane 0, so their properties are copies of
+// plane 0's, which is how they are filled here: the transport evaluation runs once per (i, j)
+// instead of 2 ngg + 1 times.  Only kappa_ve, which also depends on the plane's own T_ve (not
+// copied by eliminate_k_gradient), is re-evaluated where that differs.
+template <int NS>
+__global__ void __launch_bounds__(kPropThreads) k_properties_planar(Zone z, Param p) {
+  const int g_ = z.ngg;
+  const int i = blockIdx.x * kPropThreads + threadIdx.x - g_;
+  const int j = blockIdx.y - g_;
+  if (i >= z.mx + g_) return;
+  properties_point<NS>(z, p, i, j, 0);
+  const idx_t sz = z.L.sz, g0 = z.L.at(i, j, 0);
+  for (int kk = -g_; kk <= g_; ++kk) {
+    if (kk == 0) continue;
+    const idx_t gk = z.L.at(i, j, kk);
+    z.mul[gk] = z.mul[g0];
+    if (z.mach) z.mach[gk] = z.mach[g0];
+    if constexpr (NS > 0) {
+      z.gamma[gk] = z.gamma[g0];
+      z.acoustic[gk] = z.acoustic[g0];
+      z.kappa[gk] = z.kappa[g0];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) z.rhoD[gk + s * sz] = z.rhoD[g0 + s * sz];
+      if (p.i_eve >= 0) {
+        if (z.tve[gk] <= 0) z.tve[gk] = z.bv[gk + 5 * sz];
+        if (z.kappa_ve) {
+          const double tk = z.tve[gk];
+          if (tk == z.tve[g0]) {
+            z.kappa_ve[gk] = z.kappa_ve[g0];
+          } else {
+            double y[NS], cp[NS], cv_ve, cpt = 0;
+#pragma unroll
+            for (int s = 0; s < NS; ++s) y[s] = z.sv[gk + s * sz];
+            species_cp<NS>(z.bv[gk + 5 * sz], p.mech, cp);
+#pragma unroll
+            for (int s = 0; s < NS; ++s) cpt = fma(y[s], cp[s], cpt);
+            mixture_ve_energy<NS>(tk, y, p.mech, &cv_ve);
+            z.kappa_ve[gk] = z.kappa[g0] * cv_ve / fmax(cpt, 1e-8);
+          }
+        }
+      }
+    }
+  }
+}
+
 int launch_properties(const Zone &z, const Param &p, cudaStream_t s, int &n_launch) {
   const int g = z.ngg;
-  dim3 grid((z.mx + 2 * g + kPropThreads - 1) / kPropThreads, z.my + 2 * g, z.mz + 2 * g);
+  const bool planar = z.mz == 1 && p.dim == 2;
+  dim3 grid((z.mx + 2 * g + kPropThreads - 1) / kPropThreads, z.my + 2 * g, planar ? 1 : z.mz + 2 * g);
   ++n_launch;
   ProfScope prof("properties", s);
   switch (p.n_spec) {
     case 0:
       if (p.mu_constant > 0 && !z.mach) { --n_launch; return CB2_OK; }  // nothing changes
-      k_properties<0><<<grid, kPropThreads, 0, s>>>(z, p);
+      if (planar) k_properties_planar<0><<<grid, kPropThreads, 0, s>>>(z, p);
+      else k_properties<0><<<grid, kPropThreads, 0, s>>>(z, p);
       break;
-    case 5: k_properties<5><<<grid, kPropThreads, 0, s>>>(z, p); break;
-    case 9: k_properties<9><<<grid, kPropThreads, 0, s>>>(z, p); break;
+    case 5:
+      if (planar) k_properties_planar<5><<<grid, kPropThreads, 0, s>>>(z, p);
+      else k_properties<5><<<grid, kPropThreads, 0, s>>>(z, p);
+      break;
+    case 9:
+      if (planar) k_properties_planar<9><<<grid, kPropThreads, 0, s>>>(z, p);
+      else k_properties<9><<<grid, kPropThreads, 0, s>>>(z, p);
+      break;
     default: return CB2_ERR_UNSUPPORTED;
   }
   return check_launch();
