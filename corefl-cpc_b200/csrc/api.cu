@@ -221,6 +221,27 @@ int upload_mechanism(const cb2_mechanism &m, const cb2_two_temperature *tt, cb2_
     addd(&d.lt_b, tt->lt_b, (size_t)ns * ns);
     addd(&d.park_sigma, tt->park_sigma, ns);
     addi(&d.n_level, tt->n_level, ns);
+    // Electronic levels past which the partition sums stop changing (see ve_energy): for
+    // ascending level temperatures theta_1 < theta_2 < ..., a level l >= 2 with
+    // theta_l - theta_1 > A T contributes g_l theta_l^k exp(-theta_l / T) (k = 0, 1, 2) below
+    // 2^-54 of the first excited level's term, i.e. below half an ulp of every running sum, when
+    // A = ln(max_l (g_l / g_1) max(1, (theta_l / theta_1)^2)) + 54 ln 2 (+ 1 of margin).
+    // Unsorted or degenerate level tables get A = inf (every level is summed).
+    std::vector<double> cut((size_t)ns, INFINITY);
+    for (int sp = 0; sp < ns; ++sp) {
+      const int nl = tt->n_level[sp];
+      const double *th = tt->elec_theta + (size_t)sp * ml, *gg = tt->elec_g + (size_t)sp * ml;
+      if (nl < 3 || !(th[1] > 0) || !(gg[1] > 0) || th[0] > th[1]) continue;
+      bool ok = true;
+      double worst = 1.0;
+      for (int l = 2; l < nl && ok; ++l) {
+        if (!(th[l] >= th[l - 1]) || gg[l] < 0) ok = false;
+        const double r = th[l] / th[1];
+        worst = std::max(worst, gg[l] / gg[1] * std::max(1.0, r * r));
+      }
+      if (ok) cut[(size_t)sp] = std::log(worst) + 54.0 * std::log(2.0) + 1.0;
+    }
+    addd(&d.elec_cut, cut.data(), ns);
   }
   const size_t bd = buf.size() * sizeof(double), bi = ibuf.size() * sizeof(int);
   char *dev = nullptr;

@@ -20,9 +20,8 @@
 
 namespace cb2 {
 
-__device__ __forceinline__ bool face_point(const FaceBC &f, int &i, int &j, int &k) {
+__device__ __forceinline__ bool face_point_at(const FaceBC &f, long long t, int &i, int &j, int &k) {
   const int n0 = f.end[0] - f.start[0] + 1, n1 = f.end[1] - f.start[1] + 1, n2 = f.end[2] - f.start[2] + 1;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)n0 * n1 * n2) return false;
   i = f.start[0] + (int)(t % n0);
   j = f.start[1] + (int)((t / n0) % n1);
@@ -30,15 +29,32 @@ __device__ __forceinline__ bool face_point(const FaceBC &f, int &i, int &j, int 
   return true;
 }
 
+__device__ __forceinline__ bool face_point(const FaceBC &f, int &i, int &j, int &k) {
+  return face_point_at(f, (long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k);
+}
+
+// One thread per (face node, layer): consecutive threads take consecutive nodes of one layer.
+// The layers of a face node are independent of one another in the outflow, inflow, symmetry and
+// wall fills (each reads only interior nodes or the face's own constants), so every layer's cv
+// rebuild -- the costly part with two temperatures -- runs in its own thread.
+__device__ __forceinline__ bool face_layer_point(const FaceBC &f, int n_layer, int &i, int &j, int &k, int &l) {
+  const long long n = (long long)(f.end[0] - f.start[0] + 1) * (f.end[1] - f.start[1] + 1) * (f.end[2] - f.start[2] + 1);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * n_layer) return false;
+  l = (int)(t / n);
+  return face_point_at(f, t - l * n, i, j, k);
+}
+
 template <int NS>
 __global__ void k_bc_outflow(Zone z, Param p, FaceBC f) {
-  int i, j, k;
-  if (!face_point(f, i, j, k)) return;
+  int i, j, k, gl;
+  if (!face_layer_point(f, z.ngg, i, j, k, gl)) return;
+  ++gl;  // ghost layers 1..ngg
   int d[3] = {0, 0, 0};
   d[f.face] = f.direction;
   const idx_t sz = z.L.sz;
   const idx_t gb = z.L.at(i, j, k);
-  for (int gl = 1; gl <= z.ngg; ++gl) {
+  {
     const idx_t gg = z.L.at(i + gl * d[0], j + gl * d[1], k + gl * d[2]);
     for (int l = 0; l < 6; ++l) z.bv[gg + l * sz] = z.bv[gb + l * sz];
     for (int l = 0; l < p.n_scalar; ++l) z.sv[gg + l * sz] = z.sv[gb + l * sz];
@@ -85,8 +101,8 @@ __global__ void k_bc_periodic(Zone z, Param p, FaceBC f) {
 // normal velocity reflected.
 template <int NS>
 __global__ void k_bc_symmetry(Zone z, Param p, FaceBC f) {
-  int i, j, k;
-  if (!face_point(f, i, j, k)) return;
+  int i, j, k, gl;
+  if (!face_layer_point(f, z.ngg + 1, i, j, k, gl)) return;
   int d[3] = {0, 0, 0};
   d[f.face] = f.direction;
   const idx_t sz = z.L.sz;
@@ -96,7 +112,7 @@ __global__ void k_bc_symmetry(Zone z, Param p, FaceBC f) {
   double kx = M[gb], ky = M[gb + sz], kz = M[gb + 2 * sz];
   const double km = sqrt(kx * kx + ky * ky + kz * kz);
   kx /= km; ky /= km; kz /= km;
-  {
+  if (gl == 0) {
     const double u1 = z.bv[g1 + sz], v1 = z.bv[g1 + 2 * sz], w1 = z.bv[g1 + 3 * sz];
     const double uk = kx * u1 + ky * v1 + kz * w1;
     z.bv[gb + sz] = u1 - kx * uk;
@@ -108,8 +124,7 @@ __global__ void k_bc_symmetry(Zone z, Param p, FaceBC f) {
     for (int l = 0; l < p.n_scalar; ++l) z.sv[gb + l * sz] = z.sv[g1 + l * sz];
     if (p.i_eve >= 0) z.tve[gb] = z.tve[g1];
     cv_point<NS>(z, p, gb);
-  }
-  for (int gl = 1; gl <= z.ngg; ++gl) {
+  } else {
     const idx_t gg = z.L.at(i + gl * d[0], j + gl * d[1], k + gl * d[2]);
     const idx_t gi = z.L.at(i - gl * d[0], j - gl * d[1], k - gl * d[2]);
     z.bv[gg] = z.bv[gi];
@@ -131,12 +146,12 @@ __global__ void k_bc_symmetry(Zone z, Param p, FaceBC f) {
 // its inversion from the node's T_ve as the reference does.
 template <int NS>
 __global__ void k_bc_inflow(Zone z, Param p, FaceBC f) {
-  int i, j, k;
-  if (!face_point(f, i, j, k)) return;
+  int i, j, k, gl;
+  if (!face_layer_point(f, z.ngg + 1, i, j, k, gl)) return;
   int d[3] = {0, 0, 0};
   d[f.face] = f.direction;
   const idx_t sz = z.L.sz;
-  for (int gl = 0; gl <= z.ngg; ++gl) {
+  {
     const idx_t gg = z.L.at(i + gl * d[0], j + gl * d[1], k + gl * d[2]);
     z.bv[gg] = f.rho;
     z.bv[gg + sz] = f.u;
@@ -178,8 +193,8 @@ __device__ __forceinline__ void project_to_interior(const Zone &z, int &i, int &
 // every ghost is the mixture's at that T_ve.
 template <int NS>
 __global__ void k_bc_wall(Zone z, Param p, FaceBC f) {
-  int i, j, k;
-  if (!face_point(f, i, j, k)) return;
+  int i, j, k, gl;
+  if (!face_layer_point(f, z.ngg + 1, i, j, k, gl)) return;
   int d[3] = {0, 0, 0};
   d[f.face] = f.direction;
   const idx_t sz = z.L.sz;
@@ -195,32 +210,33 @@ __global__ void k_bc_wall(Zone z, Param p, FaceBC f) {
     const double tve_in = z.tve[g1] > 0.0 ? z.tve[g1] : z.bv[g1 + 5 * sz];
     tve_wall = !iso ? tve_in : (f.wall_Tve > 0.0 ? f.wall_Tve : t_wall);
   }
-  const double pw = z.bv[g1 + 4 * sz];
   double R = kRAir;
-  if constexpr (NS > 0) {
-    R = 0;
-    for (int s = 0; s < NS; ++s) {
-      z.sv[gb + s * sz] = z.sv[g1 + s * sz];
-      R += z.sv[gb + s * sz] * __ldg(p.mech.gas_const + s);
+  if (gl == 0) {
+    const double pw = z.bv[g1 + 4 * sz];
+    if constexpr (NS > 0) {
+      R = 0;
+      for (int s = 0; s < NS; ++s) {
+        z.sv[gb + s * sz] = z.sv[g1 + s * sz];
+        R += z.sv[gb + s * sz] * __ldg(p.mech.gas_const + s);
+      }
     }
-  }
-  z.bv[gb] = pw / (t_wall * R);
-  z.bv[gb + sz] = 0;
-  z.bv[gb + 2 * sz] = 0;
-  z.bv[gb + 3 * sz] = 0;
-  z.bv[gb + 4 * sz] = pw;
-  z.bv[gb + 5 * sz] = t_wall;
-  if constexpr (NS > 0) {
-    if (tt) {
-      double y[NS];
+    z.bv[gb] = pw / (t_wall * R);
+    z.bv[gb + sz] = 0;
+    z.bv[gb + 2 * sz] = 0;
+    z.bv[gb + 3 * sz] = 0;
+    z.bv[gb + 4 * sz] = pw;
+    z.bv[gb + 5 * sz] = t_wall;
+    if constexpr (NS > 0) {
+      if (tt) {
+        double y[NS];
 #pragma unroll
-      for (int s = 0; s < NS; ++s) y[s] = z.sv[gb + s * sz];
-      z.tve[gb] = tve_wall;
-      z.sv[gb + p.i_eve * sz] = mixture_ve_energy<NS>(tve_wall, y, p.mech, nullptr);
+        for (int s = 0; s < NS; ++s) y[s] = z.sv[gb + s * sz];
+        z.tve[gb] = tve_wall;
+        z.sv[gb + p.i_eve * sz] = mixture_ve_energy<NS>(tve_wall, y, p.mech, nullptr);
+      }
     }
-  }
-  cv_point<NS>(z, p, gb);
-  for (int gl = 1; gl <= z.ngg; ++gl) {
+    cv_point<NS>(z, p, gb);
+  } else {
     int ai = i - gl * d[0], aj = j - gl * d[1], ak = k - gl * d[2];
     project_to_interior(z, ai, aj, ak);
     const idx_t gi = z.L.at(ai, aj, ak);
@@ -453,6 +469,9 @@ static int periodic_pair(const Zone &z, const FaceBC *faces, int n, int f, int *
   return a.direction < 0 ? f : q;
 }
 
+// Small CTAs: a face has few nodes, and spreading them over more SMs shortens the launch.
+constexpr int kFaceThreads = 64;
+
 template <int NS>
 static int launch_bc_ns(const Zone &z, const Param &p, const FaceBC *faces, int n, cudaStream_t s, int &nl) {
   // priority order of the reference
@@ -478,15 +497,18 @@ static int launch_bc_ns(const Zone &z, const Param &p, const FaceBC *faces, int 
         }
       }
       const long long np = face_points(faces[f]);
-      const unsigned blocks = (unsigned)((np + 127) / 128);
-      if (blocks == 0) continue;
+      if (np == 0) continue;
+      // threads per face node: one per ghost layer (outflow), one per layer including the face
+      // node (inflow, symmetry, wall), one per line (periodic)
+      const int layers = t == CB2_BC_OUTFLOW ? z.ngg : (t == CB2_BC_PERIODIC ? 1 : z.ngg + 1);
+      const unsigned blocks = (unsigned)((np * layers + kFaceThreads - 1) / kFaceThreads);
       ProfScope prof("boundary_face", s);
       switch (t) {
-        case CB2_BC_OUTFLOW: k_bc_outflow<NS><<<blocks, 128, 0, s>>>(z, p, faces[f]); break;
-        case CB2_BC_INFLOW: k_bc_inflow<NS><<<blocks, 128, 0, s>>>(z, p, faces[f]); break;
-        case CB2_BC_SYMMETRY: k_bc_symmetry<NS><<<blocks, 128, 0, s>>>(z, p, faces[f]); break;
-        case CB2_BC_WALL: k_bc_wall<NS><<<blocks, 128, 0, s>>>(z, p, faces[f]); break;
-        case CB2_BC_PERIODIC: k_bc_periodic<NS><<<blocks, 128, 0, s>>>(z, p, faces[f]); break;
+        case CB2_BC_OUTFLOW: k_bc_outflow<NS><<<blocks, kFaceThreads, 0, s>>>(z, p, faces[f]); break;
+        case CB2_BC_INFLOW: k_bc_inflow<NS><<<blocks, kFaceThreads, 0, s>>>(z, p, faces[f]); break;
+        case CB2_BC_SYMMETRY: k_bc_symmetry<NS><<<blocks, kFaceThreads, 0, s>>>(z, p, faces[f]); break;
+        case CB2_BC_WALL: k_bc_wall<NS><<<blocks, kFaceThreads, 0, s>>>(z, p, faces[f]); break;
+        case CB2_BC_PERIODIC: k_bc_periodic<NS><<<blocks, kFaceThreads, 0, s>>>(z, p, faces[f]); break;
       }
       ++nl;
       CB2_TRY(check_launch());

@@ -104,6 +104,7 @@ struct Mech {
   int max_level, enable_vt;
   const double *theta_v, *elec_theta, *elec_g, *lt_a, *lt_b, *park_sigma;
   const int *n_level;
+  const double *elec_cut;  // [n_spec] truncation constant A of the electronic sums (ve_energy)
 };
 
 // Scalar settings passed by value to kernels.

@@ -42,6 +42,11 @@ __device__ __forceinline__ double vib_cv(int i, double t, const Mech &m) {
 
 // e_ve of species i: vibration plus the electronic levels' Boltzmann average (compute_ve_energy,
 // src/Thermo.cu:635-654); with cv: its heat capacity too (compute_ve_cv, :670-693).
+// The level sums run in the reference's order and stop at the first level l >= 2 with
+// theta_l - theta_1 > A_i T (A_i = m.elec_cut[i], set at mechanism upload): every remaining
+// term is then below half an ulp of each running sum, so adding it would leave the sums -- and
+// the result -- unchanged.  At the cold freestream of a hypersonic case this skips most of the
+// 46 exponentials of AIR5.
 __device__ __forceinline__ double ve_energy(int i, double t, const Mech &m, double *cv) {
   const double temp = fmax(t, 1.0);
   const double r = __ldg(m.gas_const + i);
@@ -50,8 +55,12 @@ __device__ __forceinline__ double ve_energy(int i, double t, const Mech &m, doub
   const int nl = __ldg(m.n_level + i);
   if (nl > 0) {
     double zs = 0.0, b = 0.0, cc = 0.0;
+    const double cut_t = __ldg(m.elec_cut + i) * temp;
+    double th1 = 0.0;
     for (int l = 0; l < nl; ++l) {
       const double th = __ldg(m.elec_theta + i * m.max_level + l);
+      if (l == 1) th1 = th;
+      else if (l > 1 && th - th1 > cut_t) break;
       const double bz = __ldg(m.elec_g + i * m.max_level + l) * exp(-th / temp);
       zs += bz;
       b += bz * th;
