@@ -23,6 +23,14 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", 
          "--expt-relaxed-constexpr", "-I", os.path.join(REPO, "include"), "-I", CSRC]
 
 
+# The mixed form's FP32 reconstruction, fluxes and viscous stencils: FP32 division and square
+# root use the hardware approximations (about 2 ulp) instead of the IEEE-rounded instruction
+# sequences.  These flags change single-precision arithmetic only; every FP64 operation in these
+# files (the plain form, the mixture thermodynamics, the state) is compiled as before.
+FAST_F32_FILES = {"inviscid_pv_f32.cu": ["-prec-div=false", "-prec-sqrt=false"],
+                  "viscous.cu": ["-prec-div=false", "-prec-sqrt=false"]}
+
+
 def _newest_header():
     t = 0.0
     for d in (CSRC, os.path.join(REPO, "include")):
@@ -37,7 +45,7 @@ def _compile(src, force, verbose):
     if (not force and os.path.exists(obj)
             and os.path.getmtime(obj) >= max(os.path.getmtime(src), _newest_header())):
         return obj, None
-    cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj]
+    cmd = [NVCC, *ARCH, *FLAGS, *FAST_F32_FILES.get(os.path.basename(src), []), "-c", src, "-o", obj]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)

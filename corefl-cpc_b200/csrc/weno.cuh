@@ -129,7 +129,9 @@ __device__ __forceinline__ T weno7_minus(const T *v, T eps, bool shock) {
 // the same weights up to a common factor, every term bounded by c_s.  (The square of a small A_s,
 // e.g. eps + 0 for a uniform density of 0.3, is below the smallest normal FP32 number, and the
 // paired FP32 instructions flush such results to zero.)
-__device__ __forceinline__ float rcp32(float x) { return __frcp_rn(x); }
+// The reciprocal is the hardware approximation (rcp.approx, within 1 ulp): 1/0 = inf and
+// 1/inf = 0 as the formulas above require.
+__device__ __forceinline__ float rcp32(float x) { return __fdividef(1.0f, x); }
 
 // ---- node-centred pair ---------------------------------------------------------------
 // Both one-sided values that the stencil centred on node n produces: the left-biased value at
