@@ -720,12 +720,24 @@ int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream) {
     CB2_TRY(launch_to_f32(B->z.bv, B->z.bv32, 6 * (size_t)B->z.L.sz, s, nl));
   }
   const bool visc = (mask & CB2_RHS_VISCOUS) && p.viscous_order > 0;
-  const bool assign = visc && viscous_assigns_dq(p);  // the viscous term writes dq: no zeroing
+  const bool pv = p.inviscid_scheme != CB2_INV_WENO5_CH && p.inviscid_scheme != CB2_INV_WENO7_CH &&
+                  p.inviscid_scheme != CB2_INV_WENO5_CP && p.inviscid_scheme != CB2_INV_WENO7_CP;
+  // mixed form of air with 8th-order viscous terms and WENO7 primitive sweeps over all three
+  // directions: the sweeps take the viscous divergence along their direction (the tile already
+  // holds the +-4 stencil), and the x sweep, the first term of the residual, assigns dq.  The FP64
+  // form keeps the separate divergence kernel: its tile with the node fluxes (55 KB, more
+  // registers) runs fewer CTAs per SM, which cost more than the divergence pass it saves.
+  Param pf = p;
+  pf.visc8_fused = visc && p.viscous_order == 8 && p.n_spec == 0 && (mask & CB2_RHS_INVISCID) && pv &&
+                           p.reconstruction == CB2_REC_WENO7 && !B->z.sweep_mask && p.precision == CB2_PREC_MIXED
+                       ? 2
+                       : 0;
+  const bool assign = pf.visc8_fused || (visc && viscous_assigns_dq(p));  // no zeroing of dq
   if (!assign) {
     ProfScope prof("zero_dq", s);
     CB2_TRY(check_cuda(cudaMemsetAsync(B->z.dq, 0, (size_t)B->z.L0.sz * p.n_var * sizeof(double), s)));
   }
-  if (visc) CB2_TRY(launch_viscous(B->z, p, B->faces.data(), (int)B->faces.size(), assign, s, nl));
+  if (visc) CB2_TRY(launch_viscous(B->z, pf, B->faces.data(), (int)B->faces.size(), assign, s, nl));
   if ((mask & CB2_RHS_CHEMISTRY) && p.reaction) CB2_TRY(launch_chemistry(B->z, p, s, nl));
   if (mask & CB2_RHS_INVISCID) {
     if (p.inviscid_scheme == CB2_INV_WENO5_CH || p.inviscid_scheme == CB2_INV_WENO7_CH)
@@ -733,7 +745,7 @@ int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream) {
     else if (p.inviscid_scheme == CB2_INV_WENO5_CP || p.inviscid_scheme == CB2_INV_WENO7_CP)
       CB2_TRY(launch_inviscid_comp(B->z, p, s, nl));
     else
-      CB2_TRY(launch_inviscid_pv(B->z, p, s, nl));
+      CB2_TRY(launch_inviscid_pv(B->z, pf, s, nl));
   }
   return count(ctx, nl);
 }

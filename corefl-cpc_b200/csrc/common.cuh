@@ -116,6 +116,10 @@ struct Param {
   double sensor_eps, sensor_threshold, entropy_fix_factor, Pr, cfl;
   double rho_ref, v_ref, weno_eps_scale, mu_constant;
   int precision;
+  // air with 8th-order viscous terms and WENO7 primitive sweeps: each sweep also adds
+  // J d(node flux)/d(its direction) (the viscous divergence), and the x sweep, the first writer
+  // of the residual, assigns dq instead of adding to it
+  int visc8_fused;
   int limit_flow;
   double lf_ll[5], lf_ul[5];  // limit_flow bounds of rho, u, v, w, p
   double dt;                  // the current step's time step (positivity limiter)

@@ -21,6 +21,7 @@
 #include "thermo.cuh"
 #include "weno.cuh"
 #include "sweep.cuh"
+#include "stencil8.cuh"
 #include "launch.h"
 
 namespace cb2 {
@@ -393,9 +394,10 @@ template <int REC>
 __host__ __device__ constexpr int pv_half_width() { return REC == 1 ? 0 : (REC <= 3 ? 1 : REC / 2); }
 
 // Shared-memory bytes of one sweep tile.
-template <typename T, int NS, int REC, int SOLVER>
+// VF: the tile also holds the node flux comps 1-4 of the 8th-order viscous terms along the sweep.
+template <typename T, int NS, int REC, int SOLVER, bool VF = false>
 __host__ __device__ constexpr size_t pv_tile_smem(int dir, int ni = kNI) {
-  return sizeof(T) * ((size_t)(5 + NS + 4 + (SOLVER == CB2_INV_ROE ? 1 : 0)) *
+  return sizeof(T) * ((size_t)(5 + NS + 4 + (SOLVER == CB2_INV_ROE ? 1 : 0) + (VF ? 4 : 0)) *
                           (dir == 0 ? (kSweepThreads + 2 * pv_half_width<REC>())
                                     : ni * (kSweepThreads / ni + 2 * pv_half_width<REC>())) +
                       (size_t)(2 * (5 + NS) + 2) * kSweepThreads);
@@ -405,9 +407,17 @@ __host__ __device__ constexpr size_t pv_tile_smem(int dir, int ni = kNI) {
 // CTA of kSweepThreads threads; sN holds the node data [NSLOT][NN], sR the right states
 // [NV+2][kSweepThreads], sF the interface fluxes [NV][kSweepThreads].  The tile ends with the
 // whole CTA in step, so a CTA may run several tiles back to back.
-template <typename T, int NS, int DIR, int REC, int SOLVER, int NI = kNI>
+// VF (air, WENO7): the 8th-order viscous divergence along this direction is taken here too
+// (compute_viscous_flux_derivative<8>, src/ViscousScheme.cu:790-834, one direction of it): the
+// tile also stages comps 1-4 of this direction's node flux (fFlux / gFlux / hFlux after their
+// periodic exchange), and every updated node adds J d8(F) before subtracting its inviscid flux
+// difference.  The WENO7 tile's halo of 3 nodes plus the neighbour node covers the +-4 stencil
+// of every updated node.
+template <typename T, int NS, int DIR, int REC, int SOLVER, int NI = kNI, bool VF = false>
 __device__ __forceinline__ void pv_tile_body(const Zone &z, const Param &p, idx_t run, int bx, int by, int bz,
                                              T *sN, T *sR, T *sF) {
+  static_assert(!VF || (REC == 7 && NS == 0 && sizeof(T) == 4),
+                "the fused viscous divergence is built for the mixed form's WENO7 air tile");
   constexpr int NV = 5 + NS;
   constexpr int RH = pv_half_width<REC>();
   constexpr int NSW = kSweepThreads / NI;  // y/z tile: nodes along the sweep
@@ -417,8 +427,20 @@ __device__ __forceinline__ void pv_tile_body(const Zone &z, const Param &p, idx_
   const Layout &L = z.L;
   const idx_t sz = L.sz;
 
+  constexpr int NSB = NV + 4 + (SOLVER == CB2_INV_ROE ? 1 : 0);  // first node-flux slot (VF)
   auto put = [&](int idx, const double *src) { sN[idx] = T(*src); };
   auto load = [&](idx_t gi, int slot, int i, int j, int k) {
+    if constexpr (VF) {
+      if constexpr (sizeof(T) == 4) {
+        const float *FL = DIR == 0 ? z.fF32 : (DIR == 1 ? z.gF32 : z.hF32);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) sN[(NSB + c) * NN + slot] = FL[gi + (c + 1) * sz];
+      } else {
+        const double *FL = DIR == 0 ? z.fF : (DIR == 1 ? z.gF : z.hF);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) sN[(NSB + c) * NN + slot] = FL[gi + (c + 1) * sz];
+      }
+    }
     if constexpr (sizeof(T) == 4) {
       // mixed form: the FP32 copies of bv, the metric and J
 #pragma unroll
@@ -534,31 +556,60 @@ __device__ __forceinline__ void pv_tile_body(const Zone &z, const Param &p, idx_
     const int tprev = tid - st;
     const idx_t gd = z.L0.at(i, j, k);
     const idx_t sz0 = z.L0.sz;
+    if constexpr (VF) {
+      // physical-boundary closures of the stencil along this direction
+      bool bl, br;
+      if (DIR == 0) {
+        bl = z.bt.il[j + k * z.my] != 0;
+        br = z.bt.ir[j + k * z.my] != 0;
+      } else if (DIR == 1) {
+        bl = z.bt.jl[i + k * z.mx] != 0;
+        br = z.bt.jr[i + k * z.mx] != 0;
+      } else {
+        bl = z.bt.kl[i + j * z.mx] != 0;
+        br = z.bt.kr[i + j * z.mx] != 0;
+      }
+      const T jac = sN[(NV + 3) * NN + c];
+      const bool first = DIR == 0 && p.visc8_fused == 2;
+      const double d0 = double(sF[tid] - sF[tprev]);
+      if (first) z.dq[gd] = -d0;
+      else z.dq[gd] -= d0;
 #pragma unroll
-    for (int v = 0; v < NV; ++v)
-      z.dq[gd + v * sz0] -= double(sF[v * kSweepThreads + tid] - sF[v * kSweepThreads + tprev]);
+      for (int v = 1; v < 5; ++v) {
+        const T *Fv = sN + (NSB + v - 1) * NN + c;
+        const T dv = d8<T>([&](int m) { return Fv[m * st]; }, n, ms, bl, br);
+        const double inv = double(sF[v * kSweepThreads + tid] - sF[v * kSweepThreads + tprev]);
+        const double vis = double(dv * jac);
+        if (first) z.dq[gd + v * sz0] = vis - inv;
+        else z.dq[gd + v * sz0] = (z.dq[gd + v * sz0] + vis) - inv;
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < NV; ++v)
+        z.dq[gd + v * sz0] -= double(sF[v * kSweepThreads + tid] - sF[v * kSweepThreads + tprev]);
+    }
   }
   __syncthreads();
 }
 
 // One whole tile with pv_tile_smem bytes at pv_smem.
-template <typename T, int NS, int DIR, int REC, int SOLVER, int NI = kNI>
+template <typename T, int NS, int DIR, int REC, int SOLVER, int NI = kNI, bool VF = false>
 __device__ __forceinline__ void pv_tile(const Zone &z, const Param &p, idx_t run, int bx, int by, int bz,
                                         unsigned char *pv_smem) {
   constexpr int NV = 5 + NS;
   constexpr int RH = pv_half_width<REC>();
   constexpr int NN = DIR == 0 ? (kSweepThreads + 2 * RH) : NI * (kSweepThreads / NI + 2 * RH);
-  constexpr int NSLOT = NV + 4 + (SOLVER == CB2_INV_ROE ? 1 : 0);
+  constexpr int NSLOT = NV + 4 + (SOLVER == CB2_INV_ROE ? 1 : 0) + (VF ? 4 : 0);
   T *sN = reinterpret_cast<T *>(pv_smem);
   T *sR = sN + NSLOT * NN;
   T *sF = sR + (NV + 2) * kSweepThreads;
-  pv_tile_body<T, NS, DIR, REC, SOLVER, NI>(z, p, run, bx, by, bz, sN, sR, sF);
+  pv_tile_body<T, NS, DIR, REC, SOLVER, NI, VF>(z, p, run, bx, by, bz, sN, sR, sF);
 }
 
-template <typename T, int NS, int DIR, int REC, int SOLVER, int NI = kNI>
+template <typename T, int NS, int DIR, int REC, int SOLVER, int NI = kNI, bool VF = false>
 __global__ void __launch_bounds__(kSweepThreads) k_inviscid_pv(Zone z, Param p, idx_t run) {
   extern __shared__ __align__(16) unsigned char pv_smem[];
-  pv_tile<T, NS, DIR, REC, SOLVER, NI>(z, p, run, blockIdx.x, blockIdx.y, blockIdx.z, pv_smem);
+  pv_tile<T, NS, DIR, REC, SOLVER, NI, VF>(z, p, run, blockIdx.x, blockIdx.y, blockIdx.z, pv_smem);
 }
 
 // Entropy-fix delta of the Roe scheme on [-1, m] in every direction (ghost width 1), FP64.
@@ -584,12 +635,12 @@ __global__ void k_entropy_fix_delta(Zone z, Param p) {
   z.efd[z.L1.at(i, j, k)] = d;
 }
 
-template <typename T, int NS, int DIR, int REC, int SOLVER, int NI>
+template <typename T, int NS, int DIR, int REC, int SOLVER, int NI, bool VF = false>
 static int launch_pv_yz(const Zone &z, const Param &p, cudaStream_t s) {
   SweepGeom geo;
   const dim3 grid = node_sweep_grid(DIR, z.L, geo, NI);
-  const size_t smem = pv_tile_smem<T, NS, REC, SOLVER>(DIR, NI);
-  auto kern = k_inviscid_pv<T, NS, DIR, REC, SOLVER, NI>;
+  const size_t smem = pv_tile_smem<T, NS, REC, SOLVER, VF>(DIR, NI);
+  auto kern = k_inviscid_pv<T, NS, DIR, REC, SOLVER, NI, VF>;
   CB2_TRY(prepare_smem(kern, smem));
   kern<<<grid, kSweepThreads, smem, s>>>(z, p, 0);
   return check_launch();
@@ -597,14 +648,29 @@ static int launch_pv_yz(const Zone &z, const Param &p, cudaStream_t s) {
 
 // y/z sweep with the block's tile width: the autotuned widths exist for the WENO5/7 air sweeps
 // (the bench's kernels); every other combination uses kNI.
-template <typename T, int NS, int DIR, int REC, int SOLVER>
+template <typename T, int NS, int DIR, int REC, int SOLVER, bool VF = false>
 static int launch_pv_yz_ni(const Zone &z, const Param &p, cudaStream_t s) {
   if constexpr ((REC == 5 || REC == 7) && NS == 0) {
     const int ni = z.tile_ni[DIR];
-    if (ni == 4) return launch_pv_yz<T, NS, DIR, REC, SOLVER, 4>(z, p, s);
-    if (ni == 16) return launch_pv_yz<T, NS, DIR, REC, SOLVER, 16>(z, p, s);
+    if (ni == 4) return launch_pv_yz<T, NS, DIR, REC, SOLVER, 4, VF>(z, p, s);
+    if (ni == 16) return launch_pv_yz<T, NS, DIR, REC, SOLVER, 16, VF>(z, p, s);
   }
-  return launch_pv_yz<T, NS, DIR, REC, SOLVER, kNI>(z, p, s);
+  return launch_pv_yz<T, NS, DIR, REC, SOLVER, kNI, VF>(z, p, s);
+}
+
+template <typename T, int NS, int REC, int SOLVER, bool VF>
+static int launch_pv_dir(int d, const Zone &z, const Param &p, cudaStream_t s) {
+  if (d == 0) {
+    SweepGeom geo;
+    const dim3 grid = node_sweep_grid(0, z.L, geo);
+    const size_t smem = pv_tile_smem<T, NS, REC, SOLVER, VF>(0);
+    auto kern = k_inviscid_pv<T, NS, 0, REC, SOLVER, kNI, VF>;
+    CB2_TRY(prepare_smem(kern, smem));
+    kern<<<grid, kSweepThreads, smem, s>>>(z, p, geo.run);
+    return check_launch();
+  }
+  if (d == 1) return launch_pv_yz_ni<T, NS, 1, REC, SOLVER, VF>(z, p, s);
+  return launch_pv_yz_ni<T, NS, 2, REC, SOLVER, VF>(z, p, s);
 }
 
 template <typename T, int NS, int REC, int SOLVER>
@@ -621,18 +687,12 @@ static int launch_pv_dirs(const Zone &z, const Param &p, cudaStream_t s, int &nl
     if (z.sweep_mask && !(z.sweep_mask & (1u << d))) continue;
     static const char *names[3] = {"pv_flux_x", "pv_flux_y", "pv_flux_z"};
     ProfScope prof(names[d], s);
-    if (d == 0) {
-      SweepGeom geo;
-      const dim3 grid = node_sweep_grid(0, z.L, geo);
-      const size_t smem = pv_tile_smem<T, NS, REC, SOLVER>(0);
-      auto kern = k_inviscid_pv<T, NS, 0, REC, SOLVER>;
-      CB2_TRY(prepare_smem(kern, smem));
-      kern<<<grid, kSweepThreads, smem, s>>>(z, p, geo.run);
-      CB2_TRY(check_launch());
-    } else if (d == 1) {
-      CB2_TRY((launch_pv_yz_ni<T, NS, 1, REC, SOLVER>(z, p, s)));
+    if constexpr (REC == 7 && NS == 0 && sizeof(T) == 4) {
+      if (p.visc8_fused) CB2_TRY((launch_pv_dir<T, NS, REC, SOLVER, true>(d, z, p, s)));
+      else CB2_TRY((launch_pv_dir<T, NS, REC, SOLVER, false>(d, z, p, s)));
     } else {
-      CB2_TRY((launch_pv_yz_ni<T, NS, 2, REC, SOLVER>(z, p, s)));
+      if (p.visc8_fused) return CB2_ERR_UNSUPPORTED;
+      CB2_TRY((launch_pv_dir<T, NS, REC, SOLVER, false>(d, z, p, s)));
     }
     ++nl;
   }

@@ -91,6 +91,8 @@ bool viscous_assigns_dq(const Param &p);
 // Whether the 8th-order node fluxes live in the block's FP32 copies (the mixed form of air); the
 // node-flux, flux-exchange and divergence kernels all follow it.
 inline bool visc8_f32(const Param &p) { return p.precision == CB2_PREC_MIXED && p.n_spec == 0; }
+// With p.visc8_fused the 8th-order path stops after the node fluxes and their periodic
+// exchange: the WENO7 primitive sweeps take the divergence.
 int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, bool assign, cudaStream_t s,
                    int &n_launch);
 int launch_chemistry(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
