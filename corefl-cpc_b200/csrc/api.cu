@@ -182,6 +182,21 @@ int upload_mechanism(const cb2_mechanism &m, const cb2_two_temperature *tt, cb2_
   addd(&d.bdc, m.binary_diffusivity_coeff, (size_t)ns * ns);
   addd(&d.kbe, m.kb_over_eps_jk, (size_t)ns * ns);
   addd(&d.zrot, m.ZRotF298, ns);
+  // natural logs of the reduced-temperature factors: the transport kernel forms the powers
+  // (T k)^a as exp(a (ln T + ln k)) with one ln T per node (usable when every factor is > 0)
+  {
+    std::vector<double> lk((size_t)ns * ns, 0.0), ll(ns, 0.0);
+    bool ok = m.kb_over_eps_jk && m.LJ_potent_inv;
+    for (size_t a = 0; ok && a < (size_t)ns * ns; ++a) ok = m.kb_over_eps_jk[a] > 0;
+    for (int a = 0; ok && a < ns; ++a) ok = m.LJ_potent_inv[a] > 0;
+    if (ok) {
+      for (size_t a = 0; a < (size_t)ns * ns; ++a) lk[a] = std::log(m.kb_over_eps_jk[a]);
+      for (int a = 0; a < ns; ++a) ll[a] = std::log(m.LJ_potent_inv[a]);
+    }
+    addd(&d.ln_kbe, lk.data(), (size_t)ns * ns);
+    addd(&d.ln_lj_inv, ll.data(), ns);
+    d.transport_ln = ok ? 1 : 0;
+  }
   addd(&d.A, m.A, nr);
   addd(&d.b, m.b, nr);
   addd(&d.Ea, m.Ea, nr);

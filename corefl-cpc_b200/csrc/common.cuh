@@ -89,6 +89,8 @@ struct Mech {
   const double *t_low, *t_mid, *t_high;
   const double *geometry, *lj_inv, *vis_coeff;
   const double *wjwi14, *sqwiwj8, *bdc, *kbe;  // [n_spec*n_spec]
+  const double *ln_kbe, *ln_lj_inv;            // ln of kbe and lj_inv (transport_ln = 1)
+  int transport_ln;
   const double *zrot;
   const int *reac_type, *rev_type, *stoi_f, *stoi_b, *reac_order;
   const double *A, *b, *Ea, *A2, *b2, *Ea2, *tbc, *troe_alpha, *troe_t3, *troe_t1, *troe_t2;

@@ -107,7 +107,8 @@ __device__ __forceinline__ void stage_update_point(const Zone &z, const Param &p
 // Physical properties of one node (update_physical_properties<mix>,
 // src/FieldOperation.cuh:183-247).  transport = false skips mu, kappa and rho*D of a mixture
 // (used by callers that take no viscous or diffusive term).
-template <int NS>
+// F32T: the transport coefficients in FP32 (the mixed form).
+template <int NS, bool F32T = false>
 __device__ __forceinline__ void properties_point(const Zone &z, const Param &p, int i, int j, int k,
                                                  bool transport = true) {
   const idx_t g = z.L.at(i, j, k), sz = z.L.sz;
@@ -149,7 +150,8 @@ __device__ __forceinline__ void properties_point(const Zone &z, const Param &p, 
     }
     if (!transport) return;
     double mu, kappa, rhoD[NS];
-    transport_properties<NS>(t, z.bv[g + 4 * sz], mw, y, cp, p.mech, mu, kappa, rhoD);
+    if constexpr (F32T) transport_properties_f32<NS>(t, mw, y, cp, p.mech, mu, kappa, rhoD);
+    else transport_properties<NS>(t, z.bv[g + 4 * sz], mw, y, cp, p.mech, mu, kappa, rhoD);
     z.mul[g] = mu;
     z.kappa[g] = kappa;
 #pragma unroll

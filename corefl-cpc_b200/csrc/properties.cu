@@ -10,13 +10,13 @@ namespace cb2 {
 
 constexpr int kPropThreads = 128;
 
-template <int NS>
+template <int NS, bool F32T = false>
 __global__ void __launch_bounds__(kPropThreads) k_properties(Zone z, Param p) {
   const int g_ = z.ngg;
   const int i = blockIdx.x * kPropThreads + threadIdx.x - g_;
   const int j = blockIdx.y - g_, k = blockIdx.z - g_;
   if (i >= z.mx + g_) return;
-  properties_point<NS>(z, p, i, j, k);
+  properties_point<NS, F32T>(z, p, i, j, k);
 }
 
 // A 2-D block (mz = 1) carries ngg ghost planes on each side of its one k plane.  The reference
@@ -25,13 +25,13 @@ __global__ void __launch_bounds__(kPropThreads) k_properties(Zone z, Param p) {
 // plane 0's, which is how they are filled here: the transport evaluation runs once per (i, j)
 // instead of 2 ngg + 1 times.  Only kappa_ve, which also depends on the plane's own T_ve (not
 // copied by eliminate_k_gradient), is re-evaluated where that differs.
-template <int NS>
+template <int NS, bool F32T = false>
 __global__ void __launch_bounds__(kPropThreads) k_properties_planar(Zone z, Param p) {
   const int g_ = z.ngg;
   const int i = blockIdx.x * kPropThreads + threadIdx.x - g_;
   const int j = blockIdx.y - g_;
   if (i >= z.mx + g_) return;
-  properties_point<NS>(z, p, i, j, 0);
+  properties_point<NS, F32T>(z, p, i, j, 0);
   const idx_t sz = z.L.sz, g0 = z.L.at(i, j, 0);
   for (int kk = -g_; kk <= g_; ++kk) {
     if (kk == 0) continue;
@@ -69,6 +69,7 @@ __global__ void __launch_bounds__(kPropThreads) k_properties_planar(Zone z, Para
 int launch_properties(const Zone &z, const Param &p, cudaStream_t s, int &n_launch) {
   const int g = z.ngg;
   const bool planar = z.mz == 1 && p.dim == 2;
+  const bool mixed = p.precision == CB2_PREC_MIXED;  // transport in FP32
   dim3 grid((z.mx + 2 * g + kPropThreads - 1) / kPropThreads, z.my + 2 * g, planar ? 1 : z.mz + 2 * g);
   ++n_launch;
   ProfScope prof("properties", s);
@@ -79,12 +80,24 @@ int launch_properties(const Zone &z, const Param &p, cudaStream_t s, int &n_laun
       else k_properties<0><<<grid, kPropThreads, 0, s>>>(z, p);
       break;
     case 5:
-      if (planar) k_properties_planar<5><<<grid, kPropThreads, 0, s>>>(z, p);
-      else k_properties<5><<<grid, kPropThreads, 0, s>>>(z, p);
+      if (mixed) {
+        if (planar) k_properties_planar<5, true><<<grid, kPropThreads, 0, s>>>(z, p);
+        else k_properties<5, true><<<grid, kPropThreads, 0, s>>>(z, p);
+      } else if (planar) {
+        k_properties_planar<5><<<grid, kPropThreads, 0, s>>>(z, p);
+      } else {
+        k_properties<5><<<grid, kPropThreads, 0, s>>>(z, p);
+      }
       break;
     case 9:
-      if (planar) k_properties_planar<9><<<grid, kPropThreads, 0, s>>>(z, p);
-      else k_properties<9><<<grid, kPropThreads, 0, s>>>(z, p);
+      if (mixed) {
+        if (planar) k_properties_planar<9, true><<<grid, kPropThreads, 0, s>>>(z, p);
+        else k_properties<9, true><<<grid, kPropThreads, 0, s>>>(z, p);
+      } else if (planar) {
+        k_properties_planar<9><<<grid, kPropThreads, 0, s>>>(z, p);
+      } else {
+        k_properties<9><<<grid, kPropThreads, 0, s>>>(z, p);
+      }
       break;
     default: return CB2_ERR_UNSUPPORTED;
   }

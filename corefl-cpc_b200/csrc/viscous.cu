@@ -462,13 +462,16 @@ __device__ __forceinline__ void visc2_face(const Zone &z, const Param &p, int i,
 constexpr int kV2TI = 16, kV2TS = 16;  // tile of 16 transverse x 16 faces along the direction
 
 // Face fluxes of a tile and their difference: a CTA owns kV2TS faces along DIR (the first
-// one is the left face of the first node) for kV2TI positions of the transverse index.
+// one is the left face of the first node) for kV2TI positions of the transverse index.  The
+// thread index runs fastest along i in every direction (along the faces for x, along the
+// transverse index for y/z), so a warp's loads are contiguous.
 template <int NS, int DIR, bool TT = false>
 __global__ void __launch_bounds__(kV2TI *kV2TS) k_visc2(Zone z, Param p) {
   constexpr int NF = 4 + NS + (TT ? 1 : 0);
+  constexpr int kPrev = DIR == 0 ? 1 : kV2TI;  // thread of the previous face along DIR
   __shared__ double sfv[NF][kV2TI * kV2TS];
   const int tid = threadIdx.x;
-  const int tt = tid % kV2TI, ts = tid / kV2TI;
+  const int tt = DIR == 0 ? tid / kV2TS : tid % kV2TI, ts = DIR == 0 ? tid % kV2TS : tid / kV2TI;
   int i, j, k, n;
   const int s0 = blockIdx.y * (kV2TS - 1);
   n = s0 - 1 + ts;  // face n + 1/2 along DIR
@@ -489,7 +492,7 @@ __global__ void __launch_bounds__(kV2TI *kV2TS) k_visc2(Zone z, Param p) {
   if (valid && ts >= 1 && n >= 0) {
     const idx_t g0 = z.L0.at(i, j, k), sz0 = z.L0.sz;
 #pragma unroll
-    for (int c = 0; c < NF; ++c) z.dq[g0 + (c + 1) * sz0] += sfv[c][tid] - sfv[c][tid - kV2TI];
+    for (int c = 0; c < NF; ++c) z.dq[g0 + (c + 1) * sz0] += sfv[c][tid] - sfv[c][tid - kPrev];
   }
 }
 

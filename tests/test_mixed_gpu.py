@@ -162,3 +162,29 @@ def test_mixed_reacting_box_steps_stay_physical():
     for c in (0, 5):
         a, b = res["mixed"][c, g:-g, g:-g, g:-g], res["fp64"][c, g:-g, g:-g, g:-g]
         assert np.abs(a - b).mean() / np.abs(b).mean() < 1e-6, c
+
+
+def test_mixed_transport_close_to_fp64_oracle(oracle_lib):
+    """The mixed form evaluates the mixture-averaged transport (mu, kappa, rho D_k) in FP32: on the
+    H2/air box with its hot spots (1200-1500 K) every node agrees with the FP64 oracle to 1e-5
+    relative, and gamma and the acoustic speed, which stay FP64, to 1e-13."""
+    h2 = _h2()
+    case = cases.h2_air_box(h2, n_nodes=14, scheme=abi.INV_HLLC, reconstruction=abi.REC_WENO5, viscous_order=2,
+                            reaction=False)
+    p, hb, faces = case.param, case.blocks[0], case.faces[0]
+    dev = DeviceBlock(hb)
+    pm = abi.ParamView.from_buffer_copy(p)
+    pm.precision = abi.PREC_MIXED
+    ctx = cb200.Context(pm)
+    ctx.bind(0, dev.view(), faces)
+    ctx.properties(0)
+    _sync()
+    oracle_lib.properties(p, hb)
+    names = ["mul", "thermal_conductivity", "rho_D", "gamma", "acoustic_speed"]
+    got = dev.to_host(names)
+    for n in names:
+        a, b = got[n], hb.a[n]
+        rel = float(np.abs(a - b).max() / np.abs(b).max())
+        assert np.isfinite(a).all(), n
+        assert rel < (1e-13 if n in ("gamma", "acoustic_speed") else 1e-5), (n, rel)
+    ctx.close()
