@@ -197,6 +197,7 @@ int upload_mechanism(const cb2_mechanism &m, const cb2_two_temperature *tt, cb2_
     addd(&d.ln_lj_inv, ll.data(), ns);
     d.transport_ln = ok ? 1 : 0;
   }
+  d.ln_temp_p = std::log(kPatm / kRu * 1e-3);
   addd(&d.A, m.A, nr);
   addd(&d.b, m.b, nr);
   addd(&d.Ea, m.Ea, nr);

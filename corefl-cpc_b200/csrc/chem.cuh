@@ -21,6 +21,16 @@ __device__ __forceinline__ double arrhenius(double t, double A, double b, double
   return A * pow(t, b) * exp(-Ea / t);
 }
 
+// A T^b exp(-Ea/T) as one exponential, with ln T and 1/T formed once per temperature: the same
+// value as the form above to a few ulp (the exponent's rounding), for a third of its cost.
+struct LnT {
+  double lnt, it;
+  __device__ __forceinline__ explicit LnT(double t) : lnt(log(t)), it(1.0 / t) {}
+};
+__device__ __forceinline__ double arrhenius(const LnT &l, double A, double b, double Ea) {
+  return A * exp(fma(b, l.lnt, -Ea * l.it));
+}
+
 // c^n for the small non-negative integer stoichiometric coefficients of a mechanism.
 __device__ __forceinline__ double ipow(double c, int n) {
   double r = 1.0;
@@ -47,6 +57,7 @@ __device__ __forceinline__ double reaction_temperature(double t, double tve, dou
 template <int NS>
 struct ParkCache {
   double fa, fb, tf, ba, bb, tb;
+  LnT lf{1.0}, lb{1.0};
   bool have_g;
   double g[NS];
   __device__ __forceinline__ ParkCache() {
@@ -60,32 +71,36 @@ struct ParkCache {
 template <int NS>
 __device__ __forceinline__ void reaction_progress(int r, double t0, double tve, const double *c,
                                                   const double *gibbs, double temp_t, const Mech &m,
-                                                  double &q1_out, double &q2_out, ParkCache<NS> *pc = nullptr) {
+                                                  double &q1_out, double &q2_out, ParkCache<NS> *pc = nullptr,
+                                                  const LnT *lt0 = nullptr) {
   const int ty = __ldg(m.reac_type + r);
   const int *sf = m.stoi_f + r * NS, *sb = m.stoi_b + r * NS;
   double t = t0;
+  LnT lt = m.park ? LnT(1.0) : (lt0 ? *lt0 : LnT(t0));
   if (m.park) {
     const double a = __ldg(m.tcf_a + r), b = __ldg(m.tcf_b + r);
     if (pc && pc->fa == a && pc->fb == b) {
       t = pc->tf;
+      lt = pc->lf;
     } else {
       t = reaction_temperature(t0, tve, a, b);
-      if (pc) { pc->fa = a; pc->fb = b; pc->tf = t; }
+      lt = LnT(t);
+      if (pc) { pc->fa = a; pc->fb = b; pc->tf = t; pc->lf = lt; }
     }
   }
   // forward rate
-  double kf = arrhenius(t, __ldg(m.A + r), __ldg(m.b + r), __ldg(m.Ea + r));
+  double kf = arrhenius(lt, __ldg(m.A + r), __ldg(m.b + r), __ldg(m.Ea + r));
   double cc = 0;
   if (ty > 3 || (ty != 0 && __ldg(m.rev_type + r) == 1 && ty == 4)) {
 #pragma unroll
     for (int s = 0; s < NS; ++s) cc += c[s] * __ldg(m.tbc + r * NS + s);
   }
   if (ty == 3) {
-    kf += arrhenius(t, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
+    kf += arrhenius(lt, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
   } else if (ty == 4) {
     kf *= cc;
   } else if (ty > 4) {
-    const double kf_low = arrhenius(t, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
+    const double kf_low = arrhenius(lt, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
     const double kf_high = kf;
     if (kf_high < 1e-25 && kf_low < 1e-25) {
       kf = 0;
@@ -112,14 +127,17 @@ __device__ __forceinline__ void reaction_progress(int r, double t0, double tve, 
     if (ty != 0) {
       const double a = __ldg(m.tcb_a + r), b = __ldg(m.tcb_b + r);
       double thb;
+      LnT lb(1.0);
       if (pc && pc->ba == a && pc->bb == b) {
         thb = pc->tb;
+        lb = pc->lb;
       } else {
         thb = reaction_temperature(t0, tve, a, b);
-        if (pc) { pc->ba = a; pc->bb = b; pc->tb = thb; pc->have_g = false; }
+        lb = LnT(thb);
+        if (pc) { pc->ba = a; pc->bb = b; pc->tb = thb; pc->lb = lb; pc->have_g = false; }
       }
       if (__ldg(m.rev_type + r) == 1) {
-        kb = arrhenius(thb, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
+        kb = arrhenius(lb, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
         if (ty == 4) kb *= cc;
       } else {
         double gl[NS];
@@ -136,20 +154,21 @@ __device__ __forceinline__ void reaction_progress(int r, double t0, double tve, 
         double dg = 0;
 #pragma unroll
         for (int s = 0; s < NS; ++s) dg += g[s] * (__ldg(sb + s) - __ldg(sf + s));
-        constexpr double temp_p = kPatm / kRu * 1e-3;
-        const double kc = pow(temp_p / thb, __ldg(m.reac_order + r)) * exp(-dg);
+        // (p_atm / (R_u T_b) 1e-3)^order exp(-dg) as one exponential
+        const double kc = exp(fma(__ldg(m.reac_order + r), m.ln_temp_p - lb.lnt, -dg));
         kb = kf / kc;
       }
     }
   } else if (ty != 0) {
     if (__ldg(m.rev_type + r) == 1) {
-      kb = arrhenius(t, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
+      kb = arrhenius(lt, __ldg(m.A2 + r), __ldg(m.b2 + r), __ldg(m.Ea2 + r));
       if (ty == 4) kb *= cc;
     } else if (ty != 2) {
       double dg = 0;
 #pragma unroll
       for (int s = 0; s < NS; ++s) dg += gibbs[s] * (__ldg(sb + s) - __ldg(sf + s));
-      const double kc = pow(temp_t, __ldg(m.reac_order + r)) * exp(-dg);
+      // temp_t^order exp(-dg), temp_t = p_atm / (R_u T) 1e-3, as one exponential
+      const double kc = exp(fma(__ldg(m.reac_order + r), m.ln_temp_p - lt.lnt, -dg));
       kb = kf / kc;
     }
   }
@@ -185,6 +204,7 @@ __device__ __forceinline__ void chem_rates(double t, double tve, const double *c
   if (!m.park && mech_needs_gibbs(m)) species_gibbs_rt<NS>(t, m, gibbs);
   constexpr double temp_p = kPatm / kRu * 1e-3;
   const double temp_t = temp_p / t;
+  const LnT lt(t);
 #pragma unroll
   for (int s = 0; s < NS; ++s) creation[s] = destruction[s] = 0;
 
@@ -208,7 +228,7 @@ __device__ __forceinline__ void chem_rates(double t, double tve, const double *c
   } else {
     for (int r = 0; r < m.n_reac; ++r) {
       double q1, q2;
-      reaction_progress<NS>(r, t, tve, c, gibbs, temp_t, m, q1, q2);
+      reaction_progress<NS>(r, t, tve, c, gibbs, temp_t, m, q1, q2, nullptr, &lt);
       if (q1r) {
         q1r[r] = q1;
         q2r[r] = q2;

@@ -91,6 +91,7 @@ struct Mech {
   const double *wjwi14, *sqwiwj8, *bdc, *kbe;  // [n_spec*n_spec]
   const double *ln_kbe, *ln_lj_inv;            // ln of kbe and lj_inv (transport_ln = 1)
   int transport_ln;
+  double ln_temp_p;  // ln(p_atm / R_u * 1e-3): the equilibrium constant's (p_atm / (R_u T))^order
   const double *zrot;
   const int *reac_type, *rev_type, *stoi_f, *stoi_b, *reac_order;
   const double *A, *b, *Ea, *A2, *b2, *Ea2, *tbc, *troe_alpha, *troe_t3, *troe_t1, *troe_t2;
