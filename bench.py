@@ -684,7 +684,7 @@ def reacting_box(args, local_rank):
 
 
 def square_cylinder(args, local_rank):
-    """The two-temperature AIR5 Mach-10 square cylinder (config C5): four body-fitted blocks of
+    """The two-temperature AIR5 Mach-10 square cylinder: four body-fitted blocks of
     --c5-side x --c5-normal nodes (1024 x 512 in all by default; tanh wall clustering, first cell
     1e-6 m; cb200.grid), freestream T = T_ve = 250 K, p = 500 Pa, Y_N2 = 0.767, Y_O2 = 0.233 on
     the box except its downstream side (outflow), isothermal 300 K wall; characteristic WENO5 with

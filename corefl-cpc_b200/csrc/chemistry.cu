@@ -9,7 +9,7 @@ constexpr int kChemThreads = 128;
 
 // Bounded to 128 registers (4 CTAs of 128 threads per SM): the 9-species kernel otherwise takes
 // 168 and runs 3 CTAs; its latency-bound exponentials gain more from the extra warps than the
-// few spills cost (C3 27.0 -> 22.7 ms per step).
+// few spills cost (192^3 H2/air box: 27.0 -> 22.7 ms per step).
 template <int NS>
 __global__ void __launch_bounds__(kChemThreads, 4) k_chemistry(Zone z, Param p) {
   const int i = blockIdx.x * kChemThreads + threadIdx.x, j = blockIdx.y, k = blockIdx.z;

@@ -11,7 +11,8 @@ namespace cb2 {
 constexpr int kPropThreads = 128;
 
 // Bounded to 80 registers (6 CTAs of 128 threads per SM; the FP64 9-species transport otherwise
-// takes 163): the exponential and logarithm chains are latency-bound (C3 29.9 -> 20.7 ms per step).
+// takes 163): the exponential and logarithm chains are latency-bound (192^3 H2/air box: 29.9 -> 20.7
+// ms per step).
 template <int NS, bool F32T = false>
 __global__ void __launch_bounds__(kPropThreads, 6) k_properties(Zone z, Param p) {
   const int g_ = z.ngg;
