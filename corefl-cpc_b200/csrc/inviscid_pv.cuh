@@ -109,6 +109,19 @@ __device__ __forceinline__ void state_energy(T *pv, const Mech &m) {
   if constexpr (NS == 0) {
     pv[NV] = ek * pv[0] + mul_rn(pv[4], T(1.0 / (kGammaAir - 1)));
     pv[NV + 1] = T(kGammaAir);
+  } else if (sizeof(T) == 4 && !m.nasa9) {
+    // mixed form: the state's thermodynamics in FP32 (NASA7)
+    float y[NS], r = 0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      y[s] = float(pv[5 + s]);
+      r += y[s] * float(__ldg(m.gas_const + s));
+    }
+    const float t = float(pv[4]) / fmaxf(float(pv[0]) * r, 1e-12f);
+    float gam, c, etr;
+    characteristic_thermo_f32<NS>(t, y, m, gam, c, nullptr, nullptr, &etr);
+    pv[NV] = T(float(pv[0]) * (float(ek) + etr));
+    pv[NV + 1] = T(gam);
   } else {
     double y[NS], r = 0;
 #pragma unroll
@@ -187,6 +200,18 @@ __device__ __forceinline__ void hllc(const T *pl, const T *pr, const T *ml, cons
     const T ht = hl * rlc + hr * rrc;
     const T ekt = half * (ut * ut + vt * vt + wt * wt);
     ct = sqrt(T(kGammaAir - 1) * (ht - ekt));
+  } else if (sizeof(T) == 4 && !mech.nasa9) {
+    // mixed form: the Roe state's sound speed in FP32 (NASA7)
+    float svm[NS], r = 0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      svm[s] = float(rlc * pl[5 + s] + rrc * pr[5 + s]);
+      r += svm[s] * float(__ldg(mech.gas_const + s));
+    }
+    const float t = float(rlc * (pl[4] / pl[0]) + rrc * (pr[4] / pr[0])) / fmaxf(r, 1e-12f);
+    float gam, c32;
+    characteristic_thermo_f32<NS>(t, svm, mech, gam, c32, nullptr, nullptr, nullptr);
+    ct = T(c32);
   } else {
     double svm[NS], r = 0;
 #pragma unroll
@@ -612,6 +637,20 @@ __global__ void __launch_bounds__(kSweepThreads) k_inviscid_pv(Zone z, Param p, 
   pv_tile<T, NS, DIR, REC, SOLVER, NI, VF>(z, p, run, blockIdx.x, blockIdx.y, blockIdx.z, pv_smem);
 }
 
+// The mixed form's mixture sweeps, held to 128 registers (two CTAs per SM): with the FP32 state
+// thermodynamics the y/z tiles would otherwise take 170 and run one CTA per SM.
+template <typename T, int NS, int DIR, int REC, int SOLVER, int NI = kNI, bool VF = false>
+__global__ void __launch_bounds__(kSweepThreads, 2) k_inviscid_pv_mb2(Zone z, Param p, idx_t run) {
+  extern __shared__ __align__(16) unsigned char pv_smem[];
+  pv_tile<T, NS, DIR, REC, SOLVER, NI, VF>(z, p, run, blockIdx.x, blockIdx.y, blockIdx.z, pv_smem);
+}
+
+template <typename T, int NS, int DIR, int REC, int SOLVER, int NI, bool VF>
+constexpr auto pv_kernel() {
+  if constexpr (sizeof(T) == 4 && NS > 0) return k_inviscid_pv_mb2<T, NS, DIR, REC, SOLVER, NI, VF>;
+  else return k_inviscid_pv<T, NS, DIR, REC, SOLVER, NI, VF>;
+}
+
 // Entropy-fix delta of the Roe scheme on [-1, m] in every direction (ghost width 1), FP64.
 template <int NS>
 __global__ void k_entropy_fix_delta(Zone z, Param p) {
@@ -640,7 +679,7 @@ static int launch_pv_yz(const Zone &z, const Param &p, cudaStream_t s) {
   SweepGeom geo;
   const dim3 grid = node_sweep_grid(DIR, z.L, geo, NI);
   const size_t smem = pv_tile_smem<T, NS, REC, SOLVER, VF>(DIR, NI);
-  auto kern = k_inviscid_pv<T, NS, DIR, REC, SOLVER, NI, VF>;
+  auto kern = pv_kernel<T, NS, DIR, REC, SOLVER, NI, VF>();
   CB2_TRY(prepare_smem(kern, smem));
   kern<<<grid, kSweepThreads, smem, s>>>(z, p, 0);
   return check_launch();
@@ -664,7 +703,7 @@ static int launch_pv_dir(int d, const Zone &z, const Param &p, cudaStream_t s) {
     SweepGeom geo;
     const dim3 grid = node_sweep_grid(0, z.L, geo);
     const size_t smem = pv_tile_smem<T, NS, REC, SOLVER, VF>(0);
-    auto kern = k_inviscid_pv<T, NS, 0, REC, SOLVER, kNI, VF>;
+    auto kern = pv_kernel<T, NS, 0, REC, SOLVER, kNI, VF>();
     CB2_TRY(prepare_smem(kern, smem));
     kern<<<grid, kSweepThreads, smem, s>>>(z, p, geo.run);
     return check_launch();

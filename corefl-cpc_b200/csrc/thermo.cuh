@@ -233,4 +233,58 @@ __device__ __forceinline__ void characteristic_thermo(double t, const double *y,
   }
 }
 
+// FP32 twins of species_h_cp and characteristic_thermo for the NASA7 tables (the mixed form's
+// reconstructed and Roe states; its temperature inversions stay FP64).  Same formulas and branch
+// structure, coefficients rounded to FP32.
+template <int NS>
+__device__ __forceinline__ void species_h_cp_f32(float t, const Mech &m, float *h, float *cp) {
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const float tl = float(__ldg(m.t_low + s)), th = float(__ldg(m.t_high + s));
+    const bool out = t < tl || t > th;
+    const float tt = out ? (t < tl ? tl : th) : t;
+    const double *c = (out ? (t < tl) : (t < float(__ldg(m.t_mid + s)))) ? m.lo + s * 7 : m.hi + s * 7;
+    const float c0 = float(__ldg(c + 0)), c1 = float(__ldg(c + 1)), c2 = float(__ldg(c + 2)), c3 = float(__ldg(c + 3));
+    const float c4 = float(__ldg(c + 4)), c5 = float(__ldg(c + 5));
+    // Horner forms of h/R = a0 T + a1 T^2/2 + a2 T^3/3 + a3 T^4/4 + a4 T^5/5 + a5 and cp/R
+    float hs = tt * (c0 + tt * (0.5f * c1 + tt * (c2 * (1.0f / 3) + tt * (0.25f * c3 + tt * (0.2f * c4))))) + c5;
+    const float cps = c0 + tt * (c1 + tt * (c2 + tt * (c3 + tt * c4)));
+    if (out) hs += cps * (t - tt);
+    const float r = float(__ldg(m.gas_const + s));
+    h[s] = hs * r;
+    cp[s] = cps * r;
+  }
+}
+
+template <int NS>
+__device__ __forceinline__ void characteristic_thermo_f32(float t, const float *y, const Mech &m, float &gamma,
+                                                          float &c, float *alpha, float *ecoef, float *e_tr_out) {
+  const float te = fmaxf(t, 1.0f);
+  float h[NS], cp[NS];
+  species_h_cp_f32<NS>(te, m, h, cp);
+  float e_tr = 0, r = 0, cpm = 0, cvm = 0;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const float rs = float(__ldg(m.gas_const + s));
+    e_tr += y[s] * (h[s] - rs * te);
+    r += y[s] * rs;
+    cpm += y[s] * cp[s];
+    cvm += y[s] * (cp[s] - rs);
+  }
+  gamma = cpm / fmaxf(cvm, 1e-8f);
+  c = sqrtf(fmaxf(gamma * r * te, 1e-12f));
+  if (e_tr_out) *e_tr_out = e_tr;
+  if (alpha) {
+    const float gm1 = gamma - 1.0f;
+    const float c2 = fmaxf(c * c, 1e-30f);
+    const float inv_gm1 = 1.0f / fmaxf(gm1, 1e-12f);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const float a = (gamma * float(__ldg(m.gas_const + s)) * te - gm1 * h[s]) / c2;
+      alpha[s] = a;
+      ecoef[s] = -a * c2 * inv_gm1;
+    }
+  }
+}
+
 }  // namespace cb2
