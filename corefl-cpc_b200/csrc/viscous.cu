@@ -466,7 +466,7 @@ constexpr int kV2TI = 16, kV2TS = 16;  // tile of 16 transverse x 16 faces along
 // thread index runs fastest along i in every direction (along the faces for x, along the
 // transverse index for y/z), so a warp's loads are contiguous.
 template <int NS, int DIR, bool TT = false>
-__global__ void __launch_bounds__(kV2TI *kV2TS) k_visc2(Zone z, Param p) {
+__device__ __forceinline__ void visc2_tile(const Zone &z, const Param &p) {
   constexpr int NF = 4 + NS + (TT ? 1 : 0);
   constexpr int kPrev = DIR == 0 ? 1 : kV2TI;  // thread of the previous face along DIR
   __shared__ double sfv[NF][kV2TI * kV2TS];
@@ -496,6 +496,17 @@ __global__ void __launch_bounds__(kV2TI *kV2TS) k_visc2(Zone z, Param p) {
   }
 }
 
+template <int NS, int DIR>
+__global__ void __launch_bounds__(kV2TI *kV2TS) k_visc2(Zone z, Param p) {
+  visc2_tile<NS, DIR, false>(z, p);
+}
+
+// Two temperatures: held to 128 registers (two CTAs per SM; 170-180 unbounded).
+template <int NS, int DIR>
+__global__ void __launch_bounds__(kV2TI *kV2TS, 2) k_visc2_2t(Zone z, Param p) {
+  visc2_tile<NS, DIR, true>(z, p);
+}
+
 template <int NS, bool TT = false>
 static int launch_visc2_ns(const Zone &z, const Param &p, cudaStream_t s, int &nl) {
   const int ndir = z.mz > 1 ? 3 : 2;
@@ -506,9 +517,15 @@ static int launch_visc2_ns(const Zone &z, const Param &p, cudaStream_t s, int &n
     dim3 grid((tr + kV2TI - 1) / kV2TI, (ext[d] + kV2TS - 2) / (kV2TS - 1), other);
     static const char *names[3] = {"visc2_x", "visc2_y", "visc2_z"};
     ProfScope prof(names[d], s);
-    if (d == 0) k_visc2<NS, 0, TT><<<grid, kV2TI * kV2TS, 0, s>>>(z, p);
-    else if (d == 1) k_visc2<NS, 1, TT><<<grid, kV2TI * kV2TS, 0, s>>>(z, p);
-    else k_visc2<NS, 2, TT><<<grid, kV2TI * kV2TS, 0, s>>>(z, p);
+    if constexpr (TT) {
+      if (d == 0) k_visc2_2t<NS, 0><<<grid, kV2TI * kV2TS, 0, s>>>(z, p);
+      else if (d == 1) k_visc2_2t<NS, 1><<<grid, kV2TI * kV2TS, 0, s>>>(z, p);
+      else k_visc2_2t<NS, 2><<<grid, kV2TI * kV2TS, 0, s>>>(z, p);
+    } else {
+      if (d == 0) k_visc2<NS, 0><<<grid, kV2TI * kV2TS, 0, s>>>(z, p);
+      else if (d == 1) k_visc2<NS, 1><<<grid, kV2TI * kV2TS, 0, s>>>(z, p);
+      else k_visc2<NS, 2><<<grid, kV2TI * kV2TS, 0, s>>>(z, p);
+    }
     ++nl;
     CB2_TRY(check_launch());
   }
