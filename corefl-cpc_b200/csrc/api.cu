@@ -119,6 +119,11 @@ struct cb2_ctx {
   int *d_queue = nullptr;     // work counter of the persistent batch grid
   int batch_ni = kNI;         // y/z tile width of the batch kernel (cb2_block_batch_autotune)
   int batch_cs = 8;           // CTAs per thread-block cluster sharing one batched block
+  // multi-block steps: the per-block work of a stage runs on these streams concurrently, forked
+  // from the caller's stream and joined back before anything that reads another block
+  std::vector<cudaStream_t> branch;
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_join;
 };
 
 namespace cb2 {
@@ -517,6 +522,9 @@ int cb2_init(const cb2_param_view *pv, cb2_ctx **out) {
 
 void cb2_destroy(cb2_ctx *ctx) {
   if (!ctx) return;
+  for (cudaStream_t b : ctx->branch) cudaStreamDestroy(b);
+  for (cudaEvent_t e : ctx->ev_join) cudaEventDestroy(e);
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->sg.exec) cudaGraphExecDestroy(ctx->sg.exec);
   if (ctx->sg.graph) cudaGraphDestroy(ctx->sg.graph);
   if (ctx->sg.capture) cudaStreamDestroy(ctx->sg.capture);
@@ -996,20 +1004,68 @@ static int enqueue_step_head(cb2_ctx *ctx, void *stream) {
   return CB2_OK;
 }
 
-// The three stages of a step (src/RK.cuh:164-237).
+// Branch streams and events for concurrent per-block work (created on first use).
+constexpr int kMaxBranches = 8;
+
+static int ensure_branches(cb2_ctx *ctx, int n) {
+  if (!ctx->ev_fork) CB2_TRY(check_cuda(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming)));
+  while ((int)ctx->branch.size() < n) {
+    cudaStream_t st = nullptr;
+    CB2_TRY(check_cuda(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)));
+    ctx->branch.push_back(st);
+    cudaEvent_t e = nullptr;
+    CB2_TRY(check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming)));
+    ctx->ev_join.push_back(e);
+  }
+  return CB2_OK;
+}
+
+// Branches 0..n-1 start after everything enqueued on s so far.
+static int fork_branches(cb2_ctx *ctx, cudaStream_t s, int n) {
+  CB2_TRY(check_cuda(cudaEventRecord(ctx->ev_fork, s)));
+  for (int i = 0; i < n; ++i) CB2_TRY(check_cuda(cudaStreamWaitEvent(ctx->branch[i], ctx->ev_fork, 0)));
+  return CB2_OK;
+}
+
+// s continues after everything enqueued on branches 0..n-1.
+static int join_branches(cb2_ctx *ctx, cudaStream_t s, int n) {
+  for (int i = 0; i < n; ++i) {
+    CB2_TRY(check_cuda(cudaEventRecord(ctx->ev_join[i], ctx->branch[i])));
+    CB2_TRY(check_cuda(cudaStreamWaitEvent(s, ctx->ev_join[i], 0)));
+  }
+  return CB2_OK;
+}
+
+// The three stages of a step (src/RK.cuh:164-237).  With several blocks, each block's residual,
+// stage update and boundary conditions -- and later its properties -- touch only that block's
+// arrays, so they run on branch streams concurrently (the latency-bound face kernels and the
+// sweeps of one block fill the SMs the others leave idle); the inner-face exchange, which reads
+// other blocks, runs on the caller's stream after the join.  Under graph capture the branches
+// become parallel paths of the graph.
 static int enqueue_stages(cb2_ctx *ctx, double dt, void *stream) {
   const int nb = (int)ctx->blocks.size();
   const bool halo = any_inner_faces(ctx);
+  cudaStream_t s = (cudaStream_t)stream;
+  int nbound = 0;
+  for (auto &B : ctx->blocks) nbound += B.bound ? 1 : 0;
+  const int nbr = nbound > 1 ? std::min(nbound, kMaxBranches) : 0;
+  if (nbr) CB2_TRY(ensure_branches(ctx, nbr));
+  auto on = [&](int slot) { return nbr ? (void *)ctx->branch[slot % nbr] : stream; };
   for (int rk = 0; rk < 3; ++rk) {
-    for (int b = 0; b < nb; ++b) {
+    if (nbr) CB2_TRY(fork_branches(ctx, s, nbr));
+    for (int b = 0, slot = 0; b < nb; ++b) {
       if (!ctx->blocks[b].bound) continue;
-      CB2_TRY(cb2_rhs(ctx, b, CB2_RHS_ALL, stream));
-      CB2_TRY(cb2_stage_update(ctx, b, dt, rk, stream));
-      CB2_TRY(cb2_boundary(ctx, b, stream));
+      void *sb = on(slot++);
+      CB2_TRY(cb2_rhs(ctx, b, CB2_RHS_ALL, sb));
+      CB2_TRY(cb2_stage_update(ctx, b, dt, rk, sb));
+      CB2_TRY(cb2_boundary(ctx, b, sb));
     }
+    if (nbr) CB2_TRY(join_branches(ctx, s, nbr));
     if (halo) CB2_TRY(cb2_halo(ctx, stream));  // data_communication (src/RK.cuh:216-226)
-    for (int b = 0; b < nb; ++b)
-      if (ctx->blocks[b].bound) CB2_TRY(cb2_properties(ctx, b, stream));
+    if (nbr) CB2_TRY(fork_branches(ctx, s, nbr));
+    for (int b = 0, slot = 0; b < nb; ++b)
+      if (ctx->blocks[b].bound) CB2_TRY(cb2_properties(ctx, b, on(slot++)));
+    if (nbr) CB2_TRY(join_branches(ctx, s, nbr));
   }
   return CB2_OK;
 }
