@@ -93,6 +93,9 @@ def parse():
     ap.add_argument("--c5-normal", type=int, default=512, help="wall-normal nodes of each cylinder block")
     ap.add_argument("--c5-steps", type=int, default=100, help="timed steps of the square cylinder")
     ap.add_argument("--c5-warmup", type=int, default=20, help="warm-up steps of the square cylinder")
+    ap.add_argument("--c5-variants", type=int, default=16,
+                    help="freestream-Mach variants of the cylinder batched in one context (0: skip)")
+    ap.add_argument("--c5-variant-steps", type=int, default=20, help="timed steps of the batched variants")
     ap.add_argument("--reacting-steps", type=int, default=5, help="timed steps of the reacting H2/air box")
     ap.add_argument("--serve-seconds", type=float, default=0.05,
                     help="length of the seeded Poisson arrival window of the served workload")
@@ -490,6 +493,9 @@ def gpu_arm(args, rank, world, local_rank):
     reacting = None if args.no_reacting else reacting_box(args, local_rank)
     batched = None if args.no_batch else batched_blocks(args, local_rank)
     c5 = None if args.no_c5 else square_cylinder(args, local_rank)
+    c5v = None
+    if not args.no_c5 and args.c5_variants > 0:
+        c5v = square_cylinder_variants(args, local_rank, c5 and c5.get("value"))
     served = None if args.no_serve else serve_workload(args)
     samples = accuracy_samples(args, local_rank) if (rank == 0 and not args.no_cpu_baseline) else None
     if dist:
@@ -532,11 +538,14 @@ def gpu_arm(args, rank, world, local_rank):
                                           "mixed_l1_Y_vs_oracle": racc.get("l1_Y_mixed")},
             "square_cylinder_air5": c5 and {k: c5.get(k) for k in ("value", "ms_per_step", "steps", "nodes",
                                                                      "status_flags", "error") if k in c5},
+            "square_cylinder_air5_variants": c5v and {k: c5v.get(k) for k in (
+                "variants", "value", "ms_per_step", "steps", "nodes", "speedup_vs_one_case", "status_flags", "error")
+                if k in c5v},
             "batched_blocks": batched and {"speedup_batched": batched["speedup_batched"],
                                            "batched_value": batched["batched"]["value"]},
             "details": "second JSON object on stderr"}
     details = {"mixed": mixed, "serve": served, "reacting_box": reacting, "batched_blocks": batched,
-               "square_cylinder_air5": c5, "cpu_baseline": base, "e2e": e2e,
+               "square_cylinder_air5": c5, "square_cylinder_air5_variants": c5v, "cpu_baseline": base, "e2e": e2e,
                "kernel_ms_per_step": {k: v[1] for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
                "kernel_rooflines": kernel_roofs}
     print(json.dumps(details, default=float), file=sys.stderr, flush=True)
@@ -747,6 +756,85 @@ def square_cylinder(args, local_rank):
         out.update({"steps": n_s, "warmup": n_w, "value": nodes / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
                     "dt_last": dt_last, "physical_time": t1, "status_flags": ctx.read_status(sh),
                     "kernel_ms_per_step": {k: v[1] for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])[:10]}})
+    except cb200.CB2Error as e:
+        out["error"] = str(e)
+    ctx.close()
+    del devs
+    torch.cuda.empty_cache()
+    return out
+
+
+def square_cylinder_variants(args, local_rank, one_case_value=None):
+    """The AIR5 cylinder's freestream-Mach variants batched in one context: --c5-variants copies of
+    the four-block grid (64 blocks for 16 variants), Mach linspace(6, 14), each with its own inflow
+    faces and inner faces, advanced together inside one device-driven graph launch per call
+    (cb2_rk3_run), the blocks' work of every stage on concurrent branch streams.  All variants
+    take the common CFL step (the minimum over the 64 blocks, set by the fastest freestream).
+    Every variant starts from the Mach-10 impulsive start with its velocity scaled to its Mach
+    number.  Timed with CUDA events after --c5-warmup steps."""
+    import numpy as np
+    import torch
+    import cb200
+    from cb200 import abi, cases
+    from cb200 import mech as mechmod
+    from cb200.field import DeviceBlock
+    gold = os.path.join(REPO, "tests", "golden", "air5_park.json")
+    air5 = mechmod.load_json(gold)
+    tt = mechmod.load_two_temperature_json(gold)
+    base = cases.square_cylinder_air5(air5, tt, n_side=args.c5_side, n_normal=args.c5_normal)
+    p = base.param
+    p.positive_preserving = 1
+    p.limit_flow = 1
+    fs = base.meta["freestream"]
+    machs = np.linspace(6.0, 14.0, args.c5_variants)
+    ctx = cb200.Context(p)
+    devs = []
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    out = {"variants": len(machs), "machs": [float(m) for m in machs]}
+    try:
+        for v, mach in enumerate(machs):
+            for b in range(4):
+                dev = DeviceBlock(base.blocks[b], device=f"cuda:{local_rank}")
+                dev.t["bv"][1] *= mach / 10.0
+                devs.append(dev)
+                fl = []
+                for f in base.faces[b]:
+                    f2 = abi.FaceBC.from_buffer_copy(f)
+                    if f2.type == abi.BC_INFLOW:
+                        f2.u = mach * fs["c"]
+                    fl.append(f2)
+                ctx.bind(4 * v + b, dev.view(), fl)
+        for v in range(len(machs)):
+            for b in range(4):
+                inner = []
+                for f in base.meta["inner"][b]:
+                    f2 = abi.InnerFace.from_buffer_copy(f)
+                    f2.target_block += 4 * v
+                    inner.append(f2)
+                ctx.bind_inner_faces(4 * v + b, inner)
+        nb = 4 * len(machs)
+        for fn in (ctx.properties, ctx.boundary):
+            for b in range(nb):
+                fn(b, sh)
+        ctx.halo(sh)
+        for fn in (ctx.properties, ctx.cv_from_bv):
+            for b in range(nb):
+                fn(b, sh)
+        t, n_w, _ = ctx.rk3_run(args.c5_warmup, fixed_dt=False, stream=sh)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        t1, n_s, dt_last = ctx.rk3_run(args.c5_variant_steps, time=t, fixed_dt=False, stream=sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / max(n_s, 1)
+        nodes = nb * args.c5_side * args.c5_normal
+        out.update({"blocks": nb, "nodes": nodes, "steps": n_s, "warmup": n_w, "ms_per_step": ms,
+                    "value": nodes / (ms * 1e-3), "unit": UNIT, "dt_last": dt_last,
+                    "status_flags": ctx.read_status(sh)})
+        if one_case_value:
+            out["speedup_vs_one_case"] = out["value"] / one_case_value
     except cb200.CB2Error as e:
         out["error"] = str(e)
     ctx.close()
