@@ -63,6 +63,7 @@ def load():
         "cb2_profile_entry": (C.c_int, [vp, C.c_int, C.c_char_p, C.c_int, P(C.c_ulonglong), P(C.c_double)]),
         "cb2_reactor_setup": (C.c_int, [vp, vp, C.c_int, vp, vp, vp, vp, C.c_double, vp]),
         "cb2_reactor_advance": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_double, C.c_double, vp]),
+        "cb2_metrics": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -70,6 +71,14 @@ def load():
         fn.argtypes = args
     _lib = lib
     return lib
+
+
+def metrics(x, y, z, mx, my, mz, g_coord, ngg, metric, jac, stream=None):
+    """cb2_metrics on device tensors: x, y, z on the ghost-g_coord lattice, metric [9, ...] and jac
+    on the ghost-ngg lattice (written)."""
+    lib = load()
+    check(lib.cb2_metrics(x.data_ptr(), y.data_ptr(), z.data_ptr(), mx, my, mz, g_coord, ngg, metric.data_ptr(),
+                          jac.data_ptr(), stream), "cb2_metrics")
 
 
 def check(rc, what):

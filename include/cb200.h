@@ -315,6 +315,16 @@ int cb2_properties(cb2_ctx *ctx, int blk, void *stream);
  * agreement (sync_two_temperature_state_from_sv, :28-58). */
 int cb2_cv_from_bv(cb2_ctx *ctx, int blk, void *stream);
 
+/* Metrics and Jacobian of one block from its node coordinates: replaces
+ * Block::compute_jac_metric (src/Mesh.cpp:244-528, its 2nd-order branch), which the reference
+ * runs on the host.  x, y, z are device arrays on the padded lattice of ghost width g_coord
+ * (>= ngg + 1: the ghost coordinates the reference's init_ghost_grid builds, src/Mesh.cpp:1013-1163,
+ * filled by the caller); metric (9 comps) and jac receive the values on the ghost-ngg lattice of
+ * cb2_zone_view.  Allocates a 4-byte flag, synchronizes the stream, and returns
+ * CB2_ERR_NONPHYSICAL if any node's Jacobian is not positive (where the reference aborts). */
+int cb2_metrics(const double *x, const double *y, const double *z, int mx, int my, int mz, int g_coord, int ngg,
+                double *metric, double *jac, void *stream);
+
 /* Local CFL time step of every node and the min over all bound blocks, returned to the
  * host: replaces local_time_step<mix> + global_time_step (src/TimeAdvanceFunc.cuh:28-127,
  * src/TimeAdvanceFunc.cu:114-139).  Synchronises `stream`. */
