@@ -339,7 +339,7 @@ unsigned two_temperature_rhs_terms(const cb2_ctx *ctx);
 bool two_temperature_faces(const Block &B) {
   for (const FaceBC &f : B.faces)
     if (f.type != CB2_BC_PERIODIC && f.type != CB2_BC_OUTFLOW && f.type != CB2_BC_WALL &&
-        f.type != CB2_BC_SYMMETRY && f.type != CB2_BC_INFLOW)
+        f.type != CB2_BC_SYMMETRY && f.type != CB2_BC_INFLOW && f.type != CB2_BC_FARFIELD)
       return false;
   return true;
 }
@@ -608,10 +608,11 @@ int cb2_bind_block(cb2_ctx *ctx, int blk, const cb2_zone_view *v, const cb2_face
     const auto &b = faces[f];
     if (b.face < 0 || b.face > 2 || (b.direction != 1 && b.direction != -1)) return CB2_ERR_INVALID;
     if (b.type != CB2_BC_OUTFLOW && b.type != CB2_BC_PERIODIC && b.type != CB2_BC_WALL &&
-        b.type != CB2_BC_SYMMETRY && b.type != CB2_BC_INFLOW)
+        b.type != CB2_BC_SYMMETRY && b.type != CB2_BC_INFLOW && b.type != CB2_BC_FARFIELD)
       return CB2_ERR_INVALID;
-    // an inflow of a mixture carries its scalars (Y_k, e_ve)
-    if (b.type == CB2_BC_INFLOW && p.n_scalar > 0 && !b.sv) return CB2_ERR_INVALID;
+    // an inflow or farfield state of a mixture carries its scalars (Y_k, e_ve)
+    if ((b.type == CB2_BC_INFLOW || b.type == CB2_BC_FARFIELD) && p.n_scalar > 0 && !b.sv) return CB2_ERR_INVALID;
+    if (b.type == CB2_BC_FARFIELD && !(b.rho > 0 && b.p > 0 && b.T > 0)) return CB2_ERR_INVALID;
   }
   if ((int)ctx->blocks.size() <= blk) ctx->blocks.resize(blk + 1);
   Block &B = ctx->blocks[blk];
@@ -632,7 +633,7 @@ int cb2_bind_block(cb2_ctx *ctx, int blk, const cb2_zone_view *v, const cb2_face
     std::vector<int> at(n_faces, -1);
     const int nsc = std::max(p.n_scalar, 1);
     for (int f = 0; f < n_faces; ++f) {
-      if (faces[f].type != CB2_BC_INFLOW) continue;
+      if (faces[f].type != CB2_BC_INFLOW && faces[f].type != CB2_BC_FARFIELD) continue;
       at[f] = (int)all_sv.size();
       for (int l = 0; l < nsc; ++l) all_sv.push_back(faces[f].sv && l < p.n_scalar ? faces[f].sv[l] : 0.0);
     }

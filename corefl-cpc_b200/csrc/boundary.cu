@@ -45,6 +45,25 @@ __device__ __forceinline__ bool face_layer_point(const FaceBC &f, int n_layer, i
   return face_point_at(f, t - l * n, i, j, k);
 }
 
+// gamma = cp / (cp - R) of the node's mixture at its T (the back-pressure outflow's sound speed).
+template <int NS>
+__device__ __forceinline__ double node_gamma(const Zone &z, const Param &p, idx_t g) {
+  if constexpr (NS == 0) {
+    return kGammaAir;
+  } else {
+    const idx_t sz = z.L.sz;
+    double cp[NS];
+    species_cp<NS>(z.bv[g + 5 * sz], p.mech, cp);
+    double cpm = 0, r = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      cpm += z.sv[g + l * sz] * cp[l];
+      r += z.sv[g + l * sz] * __ldg(p.mech.gas_const + l);
+    }
+    return cpm / (cpm - r);
+  }
+}
+
 template <int NS>
 __global__ void k_bc_outflow(Zone z, Param p, FaceBC f) {
   int i, j, k, gl;
@@ -54,6 +73,63 @@ __global__ void k_bc_outflow(Zone z, Param p, FaceBC f) {
   d[f.face] = f.direction;
   const idx_t sz = z.L.sz;
   const idx_t gb = z.L.at(i, j, k);
+  if (f.p > 0) {
+    // back pressure (Outflow::if_backPressure, src/BoundCond.cu:2219-2320): where the face node's
+    // normal Mach number is below 1 the face state takes the back pressure along the acoustic
+    // invariant of the node inside, and the ghosts are reflected about it; the face node itself
+    // keeps its values
+    const double *M = z.metric + (idx_t)(3 * f.face) * sz;
+    double nx = M[gb], ny = M[gb + sz], nz = M[gb + 2 * sz];
+    const double gni = f.direction / sqrt(nx * nx + ny * ny + nz * nz);
+    nx *= gni; ny *= gni; nz *= gni;
+    double u_b = z.bv[gb + sz], v_b = z.bv[gb + 2 * sz], w_b = z.bv[gb + 3 * sz];
+    const double u_face = nx * u_b + ny * v_b + nz * w_b;
+    double p_b = z.bv[gb + 4 * sz], rho_b = z.bv[gb];
+    const double a_b = sqrt(node_gamma<NS>(z, p, gb) * p_b / rho_b);
+    const idx_t gg = z.L.at(i + gl * d[0], j + gl * d[1], k + gl * d[2]);
+    const idx_t gi = z.L.at(i - gl * d[0], j - gl * d[1], k - gl * d[2]);
+    if (fabs(u_face / a_b) < 1) {
+      p_b = f.p;
+      const idx_t g1 = z.L.at(i - d[0], j - d[1], k - d[2]);
+      const double d1 = z.bv[g1], u1 = z.bv[g1 + sz], v1 = z.bv[g1 + 2 * sz], w1 = z.bv[g1 + 3 * sz],
+                   p1 = z.bv[g1 + 4 * sz];
+      const double c1 = sqrt(node_gamma<NS>(z, p, g1) * p1 / d1);
+      const double temp = (p_b - p1) / c1;
+      rho_b = d1 + temp / c1;
+      u_b = u1 - nx * temp / d1;
+      v_b = v1 - ny * temp / d1;
+      w_b = w1 - nz * temp / d1;
+      const double p_g = 2 * p_b - z.bv[gi + 4 * sz], rho_g = 2 * rho_b - z.bv[gi];
+      z.bv[gg] = rho_g;
+      z.bv[gg + sz] = 2 * u_b - z.bv[gi + sz];
+      z.bv[gg + 2 * sz] = 2 * v_b - z.bv[gi + 2 * sz];
+      z.bv[gg + 3 * sz] = 2 * w_b - z.bv[gi + 3 * sz];
+      z.bv[gg + 4 * sz] = p_g;
+      for (int l = 0; l < p.n_scalar; ++l) z.sv[gg + l * sz] = 2 * z.sv[gb + l * sz] - z.sv[gi + l * sz];
+      double R = kRAir;
+      if constexpr (NS > 0) {
+        R = 0;
+        for (int l = 0; l < NS; ++l) R += z.sv[gg + l * sz] * __ldg(p.mech.gas_const + l);
+      }
+      z.bv[gg + 5 * sz] = p_g / (rho_g * R);
+      if (NS > 0 && p.i_eve >= 0) {
+        const double tve_b = z.tve[gb] > 0.0 ? z.tve[gb] : z.bv[gb + 5 * sz];
+        const double tve_i = z.tve[gi] > 0.0 ? z.tve[gi] : z.bv[gi + 5 * sz];
+        z.tve[gg] = fmax(2 * tve_b - tve_i, 1.0);
+      }
+    } else {
+      z.bv[gg] = rho_b;
+      z.bv[gg + sz] = u_b;
+      z.bv[gg + 2 * sz] = v_b;
+      z.bv[gg + 3 * sz] = w_b;
+      z.bv[gg + 4 * sz] = p_b;
+      z.bv[gg + 5 * sz] = z.bv[gb + 5 * sz];
+      for (int l = 0; l < p.n_scalar; ++l) z.sv[gg + l * sz] = z.sv[gb + l * sz];
+      if (p.i_eve >= 0) z.tve[gg] = z.tve[gb] > 0.0 ? z.tve[gb] : z.bv[gb + 5 * sz];
+    }
+    cv_point<NS>(z, p, gg);
+    return;
+  }
   {
     const idx_t gg = z.L.at(i + gl * d[0], j + gl * d[1], k + gl * d[2]);
     for (int l = 0; l < 6; ++l) z.bv[gg + l * sz] = z.bv[gb + l * sz];
@@ -181,6 +257,107 @@ __device__ __forceinline__ void project_to_interior(const Zone &z, int &i, int &
     if (k <= 0 && flag_at(z.bt.kl, i, z.mx, j, z.my)) k = 1;
     else if (k >= z.mz - 1 && flag_at(z.bt.kr, i, z.mx, j, z.my)) k = z.mz - 2;
   }
+}
+
+// Farfield (apply_farfield, src/BoundCond.cu:2351-2482): from the normal Mach number of the node
+// inside, a supersonic inflow takes the farfield state, a subsonic inflow blends it with the
+// interior along the acoustic invariant (the pressure averaged, density and velocity shifted by
+// the pressure jump), a subsonic outflow imposes the farfield pressure the same way, and a
+// supersonic outflow keeps the interior state; the scalars come from the farfield on inflow and
+// from the interior on outflow.  Subsonic ghosts are reflected about the face state, supersonic
+// ones equal it.  One thread per (face node, layer): every layer reads interior nodes only.
+template <int NS>
+__global__ void k_bc_farfield(Zone z, Param p, FaceBC f) {
+  int i, j, k, gl;
+  if (!face_layer_point(f, z.ngg + 1, i, j, k, gl)) return;
+  int d[3] = {0, 0, 0};
+  d[f.face] = f.direction;
+  const idx_t sz = z.L.sz;
+  int ii = i - d[0], ij = j - d[1], ik = k - d[2];
+  project_to_interior(z, ii, ij, ik);
+  const idx_t gin = z.L.at(ii, ij, ik), gf = z.L.at(i, j, k);
+  const double *M = z.metric + (idx_t)(3 * f.face) * sz;
+  double nx = M[gf], ny = M[gf + sz], nz = M[gf + 2 * sz];
+  const double gni = f.direction / sqrt(nx * nx + ny * ny + nz * nz);
+  nx *= gni; ny *= gni; nz *= gni;
+  const double rho_in = z.bv[gin], u_in = z.bv[gin + sz], v_in = z.bv[gin + 2 * sz], w_in = z.bv[gin + 3 * sz];
+  const double p_in = z.bv[gin + 4 * sz], t_in = z.bv[gin + 5 * sz];
+  double c_in;
+  if constexpr (NS == 0) c_in = sqrt(fmax(kGammaAir * kRAir * t_in, 1e-12));
+  else c_in = fmax(z.acoustic[gin], 1e-12);
+  const double rho_c_in = fmax(rho_in * c_in, 1e-12);
+  const double mn_in = (u_in * nx + v_in * ny + w_in * nz) / c_in;
+  const bool tt = NS > 0 && p.i_eve >= 0;
+  constexpr int NSC = NS + 1;  // species and, with two temperatures, e_ve
+  double sv_b[NSC];
+  auto r_mix = [&]() {
+    if constexpr (NS == 0) {
+      return kRAir;
+    } else {
+      double r = 0;
+#pragma unroll
+      for (int l = 0; l < NS; ++l) r += sv_b[l] * __ldg(p.mech.gas_const + l);
+      return fmax(r, 1e-12);
+    }
+  };
+  double rho_b = rho_in, u_b = u_in, v_b = v_in, w_b = w_in, p_b = p_in, t_b = t_in;
+  double tve_b = t_in;
+  if (tt) tve_b = z.tve[gin] > 0.0 ? z.tve[gin] : t_in;
+  if (mn_in < 0.0) {
+    for (int l = 0; l < p.n_scalar; ++l) sv_b[l] = f.sv[l];
+    if (mn_in <= -1.0) {
+      rho_b = f.rho; u_b = f.u; v_b = f.v; w_b = f.w; p_b = f.p; t_b = f.T;
+    } else {
+      const double du_n = (f.u - u_in) * nx + (f.v - v_in) * ny + (f.w - w_in) * nz;
+      p_b = 0.5 * (p_in + f.p - rho_in * c_in * du_n);
+      p_b = fmax(p_b, 0.1 * fmax(f.p, 1.0));
+      rho_b = f.rho + (p_b - f.p) / (c_in * c_in);
+      rho_b = fmax(rho_b, 0.1 * fmax(f.rho, 1e-12));
+      u_b = f.u - (p_b - f.p) * nx / rho_c_in;
+      v_b = f.v - (p_b - f.p) * ny / rho_c_in;
+      w_b = f.w - (p_b - f.p) * nz / rho_c_in;
+      t_b = p_b / fmax(rho_b * r_mix(), 1e-12);
+    }
+    if (tt) tve_b = f.wall_Tve > 0.0 ? f.wall_Tve : t_b;
+  } else {
+    for (int l = 0; l < p.n_scalar; ++l) sv_b[l] = z.sv[gin + l * sz];
+    if (mn_in < 1.0) {
+      p_b = f.p;
+      const double dp = p_b - p_in;
+      rho_b = rho_in + dp / (c_in * c_in);
+      rho_b = fmax(rho_b, 0.1 * fmax(rho_in, 1e-12));
+      u_b = u_in - dp * nx / rho_c_in;
+      v_b = v_in - dp * ny / rho_c_in;
+      w_b = w_in - dp * nz / rho_c_in;
+      t_b = p_b / fmax(rho_b * r_mix(), 1e-12);
+    }
+  }
+  double st[6] = {rho_b, u_b, v_b, w_b, p_b, t_b};
+  double tve_s = tve_b;
+  idx_t gw = gf;
+  if (gl > 0) {
+    int ai = i - gl * d[0], aj = j - gl * d[1], ak = k - gl * d[2];
+    project_to_interior(z, ai, aj, ak);
+    const idx_t gi = z.L.at(ai, aj, ak);
+    gw = z.L.at(i + gl * d[0], j + gl * d[1], k + gl * d[2]);
+    if (mn_in > -1.0 && mn_in < 1.0) {
+      double rho_g = 2 * rho_b - z.bv[gi], p_g = 2 * p_b - z.bv[gi + 4 * sz];
+      rho_g = fmax(rho_g, 0.1 * fmax(rho_b, 1e-12));
+      p_g = fmax(p_g, 0.1 * fmax(p_b, 1.0));
+      st[0] = rho_g;
+      st[1] = 2 * u_b - z.bv[gi + sz];
+      st[2] = 2 * v_b - z.bv[gi + 2 * sz];
+      st[3] = 2 * w_b - z.bv[gi + 3 * sz];
+      st[4] = p_g;
+      st[5] = p_g / fmax(rho_g * r_mix(), 1e-12);
+    }
+  }
+  // set_boundary_state (src/BoundCond.cu:55-76)
+#pragma unroll
+  for (int l = 0; l < 6; ++l) z.bv[gw + l * sz] = st[l];
+  for (int l = 0; l < p.n_scalar; ++l) z.sv[gw + l * sz] = sv_b[l];
+  if (tt) z.tve[gw] = fmax(tve_s, 1.0);
+  cv_point<NS>(z, p, gw);
 }
 
 // No-slip, non-catalytic wall, isothermal (wall_T > 0) or adiabatic (apply_wall,
@@ -475,7 +652,8 @@ constexpr int kFaceThreads = 64;
 template <int NS>
 static int launch_bc_ns(const Zone &z, const Param &p, const FaceBC *faces, int n, cudaStream_t s, int &nl) {
   // priority order of the reference
-  const int order[5] = {CB2_BC_OUTFLOW, CB2_BC_INFLOW, CB2_BC_SYMMETRY, CB2_BC_WALL, CB2_BC_PERIODIC};
+  const int order[6] = {CB2_BC_FARFIELD, CB2_BC_OUTFLOW, CB2_BC_INFLOW, CB2_BC_SYMMETRY, CB2_BC_WALL,
+                        CB2_BC_PERIODIC};
   for (int t : order) {
     for (int f = 0; f < n; ++f) {
       if (faces[f].type != t) continue;
@@ -504,6 +682,7 @@ static int launch_bc_ns(const Zone &z, const Param &p, const FaceBC *faces, int 
       const unsigned blocks = (unsigned)((np * layers + kFaceThreads - 1) / kFaceThreads);
       ProfScope prof("boundary_face", s);
       switch (t) {
+        case CB2_BC_FARFIELD: k_bc_farfield<NS><<<blocks, kFaceThreads, 0, s>>>(z, p, faces[f]); break;
         case CB2_BC_OUTFLOW: k_bc_outflow<NS><<<blocks, kFaceThreads, 0, s>>>(z, p, faces[f]); break;
         case CB2_BC_INFLOW: k_bc_inflow<NS><<<blocks, kFaceThreads, 0, s>>>(z, p, faces[f]); break;
         case CB2_BC_SYMMETRY: k_bc_symmetry<NS><<<blocks, kFaceThreads, 0, s>>>(z, p, faces[f]); break;

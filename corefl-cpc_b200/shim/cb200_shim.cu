@@ -188,8 +188,9 @@ inline void fill_mechanism(const cfd::Species &sp, const cfd::Reaction &re, bool
 }
 
 // The face conditions the library applies, by label: the setup's boundary_conditions structs
-// (src/BoundCond.cu:80-200 reads the same ones).  Other types (farfield, back pressure,
-// subsonic inflow, ...) are left to the reference: their label maps to -1.
+// (src/BoundCond.cu:80-200 reads the same ones).  An outflow with if_backPressure is the library's
+// back-pressure outflow.  Other types (subsonic inflow, the separate back_pressure type, ...) are
+// left to the reference: their label maps to -1.
 struct FaceKinds {
   std::map<int, int> type;          // label -> CB2_BC_*
   std::map<int, std::string> name;  // label -> struct name (inflow and wall data)
@@ -207,6 +208,7 @@ inline FaceKinds face_kinds(const cfd::Parameter &par) {
     else if (type == "inflow") t = CB2_BC_INFLOW;
     else if (type == "outflow") t = CB2_BC_OUTFLOW;
     else if (type == "periodic") t = CB2_BC_PERIODIC;
+    else if (type == "farfield") t = CB2_BC_FARFIELD;
     k.type[label] = t;
     k.name[label] = bc;
   }
@@ -237,7 +239,8 @@ inline cb2_face_bc face(const cfd::Boundary &b, int dim, int ngg, bool extended)
 struct Shim {
   cb2_ctx *ctx = nullptr;
   MechTables tables;
-  std::vector<cfd::Inflow> inflows;  // keeps every inflow's sv alive until bind has copied it
+  std::vector<cfd::Inflow> inflows;      // keep every inflow's and farfield's sv alive until bind
+  std::vector<cfd::FarField> farfields;  // has copied it
 
   ~Shim() {
     if (ctx) cb2_destroy(ctx);
@@ -305,6 +308,20 @@ struct Shim {
           c.p = in.pressure;
           c.T = in.temperature;
           c.sv = in.sv;
+        } else if (c.type == CB2_BC_FARFIELD) {
+          farfields.emplace_back(name, const_cast<cfd::Species &>(sp), par);
+          const cfd::FarField &ff = farfields.back();
+          c.rho = ff.density;
+          c.u = ff.u;
+          c.v = ff.v;
+          c.w = ff.w;
+          c.p = ff.pressure;
+          c.T = ff.temperature;
+          c.wall_temperature_ve = ff.temperature_ve > 0 ? ff.temperature_ve : 0.0;
+          c.sv = ff.sv;
+        } else if (c.type == CB2_BC_OUTFLOW) {
+          cfd::Outflow out(name, par);  // back pressure (if_backPressure) as p > 0
+          if (out.if_backPressure == 1) c.p = out.backPressure;
         } else if (c.type == CB2_BC_WALL) {
           cfd::Wall wall(par.get_struct(name), par, sp);
           c.wall_temperature = wall.thermal_type == cfd::Wall::ThermalType::isothermal ? wall.temperature : 0.0;

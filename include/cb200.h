@@ -56,6 +56,7 @@ extern "C" {
 
 /* boundary types: the reference's BC kinds (src/BoundCond.cu:3846-3998 comments) */
 #define CB2_BC_WALL 2
+#define CB2_BC_FARFIELD 4
 #define CB2_BC_SYMMETRY 3
 #define CB2_BC_INFLOW 5
 #define CB2_BC_OUTFLOW 6
@@ -108,14 +109,16 @@ typedef struct cb2_face_bc {
   int type;          /* CB2_BC_* */
   int face, direction;
   int range_start[3], range_end[3];
-  /* inflow / wall data (unused for outflow and periodic) */
+  /* inflow / farfield state and wall data; an outflow with p > 0 is the back-pressure outflow
+   * (Outflow::if_backPressure, src/BoundCond.cu:2219-2320) with p its back pressure */
   double rho, u, v, w, p, T;
   double wall_temperature; /* <=0 : adiabatic wall */
-  /* two-temperature isothermal wall: the wall's T_ve (Wall::temperature_ve); <= 0: the wall
-   * temperature */
+  /* two temperatures: the T_ve of an isothermal wall (Wall::temperature_ve; <= 0: the wall
+   * temperature) or of a farfield state (FarField::temperature_ve; <= 0: its boundary T) */
   double wall_temperature_ve;
-  /* inflow: the n_scalar scalars of the inflow state, Y_k and then (two temperatures) e_ve
-   * (Inflow::sv, src/BoundCond.h:23-90); a HOST array copied at bind.  Required with species. */
+  /* inflow and farfield: the n_scalar scalars of the state, Y_k and then (two temperatures) e_ve
+   * (Inflow::sv / FarField::sv, src/BoundCond.h:23-169); a HOST array copied at bind.  Required
+   * with species. */
   const double *sv;
 } cb2_face_bc;
 

@@ -1992,9 +1992,151 @@ double mix_r(const Zone &z, const Param &p, int i, int j, int k) {
   return R;
 }
 
+// gamma = cp / (cp - R) of a node's mixture at its temperature (apply_outflow's back-pressure
+// branch, src/BoundCond.cu:2232-2243)
+double node_gamma(const Zone &z, const Param &p, int i, int j, int k) {
+  if (p.n_spec == 0) return gamma_air;
+  std::vector<double> cp(p.n_spec);
+  nasa7_cp(z.bv(i, j, k, 5), p.mech, cp.data());  // compute_cp (NASA9 tables when loaded)
+  double cpm = 0, r = 0;
+  for (int l = 0; l < p.n_spec; ++l) {
+    cpm += z.sv(i, j, k, l) * cp[l];
+    r += z.sv(i, j, k, l) * p.mech.gas_const[l];
+  }
+  return cpm / (cpm - r);
+}
+
+// set_boundary_state (src/BoundCond.cu:55-76)
+void set_boundary_state(Zone &z, const Param &p, int i, int j, int k, const double *st, const double *sv,
+                        double tve) {
+  for (int l = 0; l < 6; ++l) z.bv(i, j, k, l) = st[l];
+  for (int l = 0; l < p.n_scalar; ++l) z.sv(i, j, k, l) = sv[l];
+  if (p.i_eve >= 0) z.tve(i, j, k) = std::max(tve, 1.0);
+  cv_point(z, p, i, j, k);
+}
+
+// apply_farfield (src/BoundCond.cu:2351-2482) at face node (i, j, k)
+void farfield_point(Zone &z, const Param &p, const FaceBC &f, const int *dir, int i, int j, int k) {
+  int in[3] = {i - dir[0], j - dir[1], k - dir[2]};
+  project_to_interior(z, in[0], in[1], in[2]);
+  double nx = z.metric(i, j, k, f.face * 3), ny = z.metric(i, j, k, f.face * 3 + 1),
+         nz = z.metric(i, j, k, f.face * 3 + 2);
+  const double gni = f.direction / std::sqrt(nx * nx + ny * ny + nz * nz);
+  nx *= gni; ny *= gni; nz *= gni;
+  const double rho_in = z.bv(in[0], in[1], in[2], 0), u_in = z.bv(in[0], in[1], in[2], 1),
+               v_in = z.bv(in[0], in[1], in[2], 2), w_in = z.bv(in[0], in[1], in[2], 3),
+               p_in = z.bv(in[0], in[1], in[2], 4), t_in = z.bv(in[0], in[1], in[2], 5);
+  const double c_in = p.n_spec == 0 ? std::sqrt(std::max(gamma_air * R_air * t_in, 1e-12))
+                                    : std::max(z.acoustic(in[0], in[1], in[2]), 1e-12);
+  const double rho_c_in = std::max(rho_in * c_in, 1e-12);
+  const double mn_in = (u_in * nx + v_in * ny + w_in * nz) / c_in;
+  std::vector<double> sv_b(std::max(p.n_scalar, 1), 0.0);
+  auto r_mix = [&]() {
+    if (p.n_spec == 0) return R_air;
+    double r = 0;
+    for (int l = 0; l < p.n_spec; ++l) r += sv_b[l] * p.mech.gas_const[l];
+    return std::max(r, 1e-12);
+  };
+  double rho_b = rho_in, u_b = u_in, v_b = v_in, w_b = w_in, p_b = p_in, t_b = t_in, tve_b = t_in;
+  if (p.i_eve >= 0) tve_b = z.tve(in[0], in[1], in[2]) > 0.0 ? z.tve(in[0], in[1], in[2]) : t_in;
+  if (mn_in < 0.0) {  // supersonic or subsonic inflow
+    for (int l = 0; l < p.n_scalar; ++l) sv_b[l] = f.sv[l];
+    if (mn_in <= -1.0) {
+      rho_b = f.rho; u_b = f.u; v_b = f.v; w_b = f.w; p_b = f.p; t_b = f.T;
+    } else {
+      const double du_n = (f.u - u_in) * nx + (f.v - v_in) * ny + (f.w - w_in) * nz;
+      p_b = std::max(0.5 * (p_in + f.p - rho_in * c_in * du_n), 0.1 * std::max(f.p, 1.0));
+      rho_b = std::max(f.rho + (p_b - f.p) / (c_in * c_in), 0.1 * std::max(f.rho, 1e-12));
+      u_b = f.u - (p_b - f.p) * nx / rho_c_in;
+      v_b = f.v - (p_b - f.p) * ny / rho_c_in;
+      w_b = f.w - (p_b - f.p) * nz / rho_c_in;
+      t_b = p_b / std::max(rho_b * r_mix(), 1e-12);
+    }
+    if (p.i_eve >= 0) tve_b = f.wall_Tve > 0.0 ? f.wall_Tve : t_b;
+  } else {  // subsonic or supersonic outflow
+    for (int l = 0; l < p.n_scalar; ++l) sv_b[l] = z.sv(in[0], in[1], in[2], l);
+    if (mn_in < 1.0) {
+      p_b = f.p;
+      const double dp = p_b - p_in;
+      rho_b = std::max(rho_in + dp / (c_in * c_in), 0.1 * std::max(rho_in, 1e-12));
+      u_b = u_in - dp * nx / rho_c_in;
+      v_b = v_in - dp * ny / rho_c_in;
+      w_b = w_in - dp * nz / rho_c_in;
+      t_b = p_b / std::max(rho_b * r_mix(), 1e-12);
+    }
+  }
+  const double st[6] = {rho_b, u_b, v_b, w_b, p_b, t_b};
+  set_boundary_state(z, p, i, j, k, st, sv_b.data(), tve_b);
+  for (int g = 1; g <= z.ngg; ++g) {
+    int ii[3] = {i - g * dir[0], j - g * dir[1], k - g * dir[2]};
+    project_to_interior(z, ii[0], ii[1], ii[2]);
+    double sg[6] = {rho_b, u_b, v_b, w_b, p_b, t_b};
+    if (mn_in > -1.0 && mn_in < 1.0) {
+      sg[0] = std::max(2 * rho_b - z.bv(ii[0], ii[1], ii[2], 0), 0.1 * std::max(rho_b, 1e-12));
+      sg[4] = std::max(2 * p_b - z.bv(ii[0], ii[1], ii[2], 4), 0.1 * std::max(p_b, 1.0));
+      sg[1] = 2 * u_b - z.bv(ii[0], ii[1], ii[2], 1);
+      sg[2] = 2 * v_b - z.bv(ii[0], ii[1], ii[2], 2);
+      sg[3] = 2 * w_b - z.bv(ii[0], ii[1], ii[2], 3);
+      sg[5] = sg[4] / std::max(sg[0] * r_mix(), 1e-12);
+    }
+    set_boundary_state(z, p, i + g * dir[0], j + g * dir[1], k + g * dir[2], sg, sv_b.data(), tve_b);
+  }
+}
+
+// the back-pressure branch of apply_outflow (src/BoundCond.cu:2219-2320) at face node (i, j, k)
+void back_pressure_point(Zone &z, const Param &p, const FaceBC &f, const int *dir, int i, int j, int k) {
+  double nx = z.metric(i, j, k, f.face * 3), ny = z.metric(i, j, k, f.face * 3 + 1),
+         nz = z.metric(i, j, k, f.face * 3 + 2);
+  const double gni = f.direction / std::sqrt(nx * nx + ny * ny + nz * nz);
+  nx *= gni; ny *= gni; nz *= gni;
+  double u_b = z.bv(i, j, k, 1), v_b = z.bv(i, j, k, 2), w_b = z.bv(i, j, k, 3);
+  const double u_face = nx * u_b + ny * v_b + nz * w_b;
+  double p_b = z.bv(i, j, k, 4), rho_b = z.bv(i, j, k, 0);
+  const double a_b = std::sqrt(node_gamma(z, p, i, j, k) * p_b / rho_b);
+  if (std::fabs(u_face / a_b) < 1) {
+    p_b = f.p;
+    const int i1 = i - dir[0], j1 = j - dir[1], k1 = k - dir[2];
+    const double d1 = z.bv(i1, j1, k1, 0), u1 = z.bv(i1, j1, k1, 1), v1 = z.bv(i1, j1, k1, 2),
+                 w1 = z.bv(i1, j1, k1, 3), p1 = z.bv(i1, j1, k1, 4);
+    const double c1 = std::sqrt(node_gamma(z, p, i1, j1, k1) * p1 / d1);
+    const double temp = (p_b - p1) / c1;
+    rho_b = d1 + temp / c1;
+    u_b = u1 - nx * temp / d1;
+    v_b = v1 - ny * temp / d1;
+    w_b = w1 - nz * temp / d1;
+    for (int g = 1; g <= z.ngg; ++g) {
+      const int gi = i + g * dir[0], gj = j + g * dir[1], gk = k + g * dir[2];
+      const int ii = i - g * dir[0], ij = j - g * dir[1], ik = k - g * dir[2];
+      const double p_g = 2 * p_b - z.bv(ii, ij, ik, 4), rho_g = 2 * rho_b - z.bv(ii, ij, ik, 0);
+      z.bv(gi, gj, gk, 0) = rho_g;
+      z.bv(gi, gj, gk, 1) = 2 * u_b - z.bv(ii, ij, ik, 1);
+      z.bv(gi, gj, gk, 2) = 2 * v_b - z.bv(ii, ij, ik, 2);
+      z.bv(gi, gj, gk, 3) = 2 * w_b - z.bv(ii, ij, ik, 3);
+      z.bv(gi, gj, gk, 4) = p_g;
+      for (int l = 0; l < p.n_scalar; ++l) z.sv(gi, gj, gk, l) = 2 * z.sv(i, j, k, l) - z.sv(ii, ij, ik, l);
+      z.bv(gi, gj, gk, 5) = p_g / (rho_g * mix_r(z, p, gi, gj, gk));
+      if (p.i_eve >= 0) {
+        const double tve_b = z.tve(i, j, k) > 0.0 ? z.tve(i, j, k) : z.bv(i, j, k, 5);
+        const double tve_i = z.tve(ii, ij, ik) > 0.0 ? z.tve(ii, ij, ik) : z.bv(ii, ij, ik, 5);
+        z.tve(gi, gj, gk) = std::max(2 * tve_b - tve_i, 1.0);
+      }
+      cv_point(z, p, gi, gj, gk);
+    }
+  } else {
+    for (int g = 1; g <= z.ngg; ++g) {
+      const int gi = i + g * dir[0], gj = j + g * dir[1], gk = k + g * dir[2];
+      const double st[6] = {rho_b, u_b, v_b, w_b, p_b, z.bv(i, j, k, 5)};
+      for (int l = 0; l < 6; ++l) z.bv(gi, gj, gk, l) = st[l];
+      for (int l = 0; l < p.n_scalar; ++l) z.sv(gi, gj, gk, l) = z.sv(i, j, k, l);
+      if (p.i_eve >= 0) z.tve(gi, gj, gk) = z.tve(i, j, k) > 0.0 ? z.tve(i, j, k) : z.bv(i, j, k, 5);
+      cv_point(z, p, gi, gj, gk);
+    }
+  }
+}
+
 // apply_boundary_conditions (src/BoundCond.cu:3846-3998) in its priority order
 void apply_boundary_conditions(Zone &z, const Param &p) {
-  for (int type : {CB2_BC_OUTFLOW, CB2_BC_INFLOW, CB2_BC_SYMMETRY, CB2_BC_WALL, CB2_BC_PERIODIC}) {
+  for (int type : {CB2_BC_FARFIELD, CB2_BC_OUTFLOW, CB2_BC_INFLOW, CB2_BC_SYMMETRY, CB2_BC_WALL, CB2_BC_PERIODIC}) {
     for (const auto &f : z.faces) {
       if (f.type != type) continue;
       int dir[3] = {0, 0, 0};
@@ -2002,7 +2144,11 @@ void apply_boundary_conditions(Zone &z, const Param &p) {
       for (int k = f.start[2]; k <= f.end[2]; ++k)
         for (int j = f.start[1]; j <= f.end[1]; ++j)
           for (int i = f.start[0]; i <= f.end[0]; ++i) {
-            if (type == CB2_BC_OUTFLOW) {  // src/BoundCond.cu:2328-2347
+            if (type == CB2_BC_FARFIELD) {
+              farfield_point(z, p, f, dir, i, j, k);
+            } else if (type == CB2_BC_OUTFLOW && f.p > 0) {
+              back_pressure_point(z, p, f, dir, i, j, k);
+            } else if (type == CB2_BC_OUTFLOW) {  // src/BoundCond.cu:2328-2347
               for (int g = 1; g <= z.ngg; ++g) {
                 const int gi = i + g * dir[0], gj = j + g * dir[1], gk = k + g * dir[2];
                 for (int l = 0; l < 6; ++l) z.bv(gi, gj, gk, l) = z.bv(i, j, k, l);

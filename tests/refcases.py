@@ -43,6 +43,9 @@ CHAN_DIMS = (24, 16, 1)
 # the channel's faces: supersonic inflow (i-), outflow (i+), isothermal wall (j-), symmetry (j+)
 CHAN_INFLOW = dict(rho=1.1, u=2.5, p=1.0)
 CHAN_WALL_T = 0.004
+# the farfield channel: farfield (i- and j+), back-pressure outflow (i+), isothermal wall (j-)
+CHAN_FARFIELD = dict(rho=1.1, u=0.6, p=1.0)
+CHAN_BACK_PRESSURE = 1.05
 
 
 def ref_ngg(scheme, visc):
@@ -73,8 +76,8 @@ def _air5(name, visc, reaction, pp=0, limit_flow=0, stages=3, dt=2e-9, bc="perio
                 seed=91, pp=pp, limit_flow=limit_flow, reaction=reaction)
 
 
-def _chan(name, scheme, rec, visc, stages=3, dt=2e-3):
-    return dict(family="chan", name=name, scheme=scheme, rec=rec, visc=visc, bc="channel", stages=stages, dt=dt,
+def _chan(name, scheme, rec, visc, stages=3, dt=2e-3, bc="channel"):
+    return dict(family="chan", name=name, scheme=scheme, rec=rec, visc=visc, bc=bc, stages=stages, dt=dt,
                 seed=9, pp=0, limit_flow=0, reaction=0)
 
 
@@ -91,7 +94,8 @@ CASES = ([_air(n + "_" + bc, s, r, v, bc) for n, s, r, v in AIR_SCHEMES for bc i
          [_air5("air5_weno5ch_visc2_chem", 2, 1), _air5("air5_weno5ch_chem_pp_limit", 0, 1, pp=1, limit_flow=1),
           _air5("air5_weno5ch_visc2_outflow", 2, 1, bc="outflow"), _air5("air5_weno5ch_visc8_chem", 8, 1)] +
          [_chan("chan_hllc_muscl_visc2", 4, 2, 2), _chan("chan_weno5ch_visc2", 52, 2, 2),
-          _chan("chan_roe_muscl", 2, 2, 0)] +
+          _chan("chan_roe_muscl", 2, 2, 0), _chan("chan_farfield_weno5ch", 52, 2, 0, bc="farfield"),
+          _chan("chan_farfield_hllc_visc2", 4, 2, 2, bc="farfield")] +
          [dict(family="sod", name="sod_1000x7", scheme=52, rec=2, visc=0, bc="outflow", stages=0, dt=0.0, seed=0,
                pp=0, limit_flow=0, reaction=0, mx=1000, my=7, cfl=0.5, t_end=0.2)])
 
@@ -144,11 +148,20 @@ def build(case):
         ci = CHAN_INFLOW
         # T from (p, rho) as the reference's Inflow takes it: pressure * mw / (density * R_u)
         t_in = ci["p"] * cases.MW_AIR / (ci["rho"] * cases.R_U)
-        faces = [face(abi.BC_INFLOW, 0, -1, (0, 0, 0), (0, my - 1, 0), rho=ci["rho"], u=ci["u"], v=0.0, w=0.0,
-                      p=ci["p"], T=t_in),
-                 face(abi.BC_OUTFLOW, 0, 1, (mx - 1, 0, 0), (mx - 1, my - 1, 0)),
-                 face(abi.BC_WALL, 1, -1, (0, 0, 0), (mx - 1, 0, 0), wall_temperature=CHAN_WALL_T),
-                 face(abi.BC_SYMMETRY, 1, 1, (0, my - 1, 0), (mx - 1, my - 1, 0))]
+        if case["bc"] == "farfield":
+            ff = CHAN_FARFIELD
+            t_ff = ff["p"] * cases.MW_AIR / (ff["rho"] * cases.R_U)
+            st = dict(rho=ff["rho"], u=ff["u"], v=0.0, w=0.0, p=ff["p"], T=t_ff)
+            faces = [face(abi.BC_FARFIELD, 0, -1, (0, 0, 0), (0, my - 1, 0), **st),
+                     face(abi.BC_OUTFLOW, 0, 1, (mx - 1, 0, 0), (mx - 1, my - 1, 0), p=CHAN_BACK_PRESSURE),
+                     face(abi.BC_WALL, 1, -1, (0, 0, 0), (mx - 1, 0, 0), wall_temperature=CHAN_WALL_T),
+                     face(abi.BC_FARFIELD, 1, 1, (0, my - 1, 0), (mx - 1, my - 1, 0), **st)]
+        else:
+            faces = [face(abi.BC_INFLOW, 0, -1, (0, 0, 0), (0, my - 1, 0), rho=ci["rho"], u=ci["u"], v=0.0,
+                          w=0.0, p=ci["p"], T=t_in),
+                     face(abi.BC_OUTFLOW, 0, 1, (mx - 1, 0, 0), (mx - 1, my - 1, 0)),
+                     face(abi.BC_WALL, 1, -1, (0, 0, 0), (mx - 1, 0, 0), wall_temperature=CHAN_WALL_T),
+                     face(abi.BC_SYMMETRY, 1, 1, (0, my - 1, 0), (mx - 1, my - 1, 0))]
         extra = {}
     elif fam == "sod":
         c = cases.sod(mx=case["mx"], my=case["my"], ngg=g, scheme=case["scheme"], reconstruction=case["rec"],
@@ -223,7 +236,7 @@ def _face_lines(faces, dim):
 
 
 BC_NAMES = {abi.BC_OUTFLOW: "outflow", abi.BC_PERIODIC: "periodic", abi.BC_SYMMETRY: "symmetry",
-            abi.BC_WALL: "wall", abi.BC_INFLOW: "inflow"}
+            abi.BC_WALL: "wall", abi.BC_INFLOW: "inflow", abi.BC_FARFIELD: "farfield"}
 
 
 def _coords(case, hb):
@@ -308,6 +321,12 @@ def write_reference_case(case, case_dir, ref_dir):
                   "    real v = 0.0", "    real w = 0.0", "    real pressure = %r" % ci["p"]]
         if t == abi.BC_WALL:
             s += ["    string thermal_type = isothermal", "    real temperature = %r" % CHAN_WALL_T]
+        if t == abi.BC_FARFIELD:
+            ff = CHAN_FARFIELD
+            s += ["    real density = %r" % ff["rho"], "    real velocity = %r" % ff["u"], "    real u = 1.0",
+                  "    real v = 0.0", "    real w = 0.0", "    real pressure = %r" % ff["p"]]
+        if t == abi.BC_OUTFLOW and case.get("bc") == "farfield":
+            s += ["    int if_backPressure = 1", "    real backPressure = %r" % CHAN_BACK_PRESSURE]
         s.append("}")
     # reference state: (density, velocity, pressure) of the case's reference values; the runner
     # builds the reference's Inflow from it (rho_inf, v_inf, p_inf, speed_of_sound)
