@@ -11,6 +11,7 @@ INV_WENO5_CP, INV_WENO5_CH, INV_WENO7_CP, INV_WENO7_CH = 51, 52, 71, 72
 REC_FIRST, REC_MUSCL, REC_NND2, REC_WENO5, REC_WENO7 = 1, 2, 3, 5, 7
 BC_WALL, BC_SYMMETRY, BC_INFLOW, BC_OUTFLOW, BC_PERIODIC = 2, 3, 5, 6, 8
 BC_FARFIELD = 4
+BC_NONREFLECTING = 0x100  # OR'd into BC_OUTFLOW: non-reflecting outflow
 PREC_FP64, PREC_MIXED = 0, 1
 RHS_VISCOUS, RHS_CHEMISTRY, RHS_INVISCID, RHS_ALL = 1, 2, 4, 7
 

@@ -288,7 +288,8 @@ int upload_mechanism(const cb2_mechanism &m, const cb2_two_temperature *tt, cb2_
 // and for 2-D blocks the k range becomes [-ngg, ngg] (or [0, 0] without extension).
 FaceBC register_face(const cb2_face_bc &f, int dim, int ngg, bool extend) {
   FaceBC b{};
-  b.type = f.type;
+  b.type = f.type & ~CB2_BC_NONREFLECTING;
+  b.nonreflecting = (f.type & CB2_BC_NONREFLECTING) != 0;
   for (int a = 0; a < 3; ++a) { b.start[a] = f.range_start[a]; b.end[a] = f.range_end[a]; }
   b.face = f.face;
   b.direction = f.direction;
@@ -607,9 +608,12 @@ int cb2_bind_block(cb2_ctx *ctx, int blk, const cb2_zone_view *v, const cb2_face
   for (int f = 0; f < n_faces; ++f) {
     const auto &b = faces[f];
     if (b.face < 0 || b.face > 2 || (b.direction != 1 && b.direction != -1)) return CB2_ERR_INVALID;
-    if (b.type != CB2_BC_OUTFLOW && b.type != CB2_BC_PERIODIC && b.type != CB2_BC_WALL &&
-        b.type != CB2_BC_SYMMETRY && b.type != CB2_BC_INFLOW && b.type != CB2_BC_FARFIELD)
+    const int t = b.type & ~CB2_BC_NONREFLECTING;
+    if (t != CB2_BC_OUTFLOW && t != CB2_BC_PERIODIC && t != CB2_BC_WALL && t != CB2_BC_SYMMETRY &&
+        t != CB2_BC_INFLOW && t != CB2_BC_FARFIELD)
       return CB2_ERR_INVALID;
+    // only an outflow face can be non-reflecting (Outflow::nonReflecting)
+    if ((b.type & CB2_BC_NONREFLECTING) && t != CB2_BC_OUTFLOW) return CB2_ERR_INVALID;
     // an inflow or farfield state of a mixture carries its scalars (Y_k, e_ve)
     if ((b.type == CB2_BC_INFLOW || b.type == CB2_BC_FARFIELD) && p.n_scalar > 0 && !b.sv) return CB2_ERR_INVALID;
     if (b.type == CB2_BC_FARFIELD && !(b.rho > 0 && b.p > 0 && b.T > 0)) return CB2_ERR_INVALID;
@@ -633,9 +637,12 @@ int cb2_bind_block(cb2_ctx *ctx, int blk, const cb2_zone_view *v, const cb2_face
     std::vector<int> at(n_faces, -1);
     const int nsc = std::max(p.n_scalar, 1);
     for (int f = 0; f < n_faces; ++f) {
-      if (faces[f].type != CB2_BC_INFLOW && faces[f].type != CB2_BC_FARFIELD) continue;
+      const bool wall = faces[f].type == CB2_BC_WALL;
+      if (!(faces[f].type == CB2_BC_INFLOW || faces[f].type == CB2_BC_FARFIELD || (wall && faces[f].sv))) continue;
+      // a catalytic wall's sv holds the n_spec wall mass fractions (Wall::yk)
+      const int nin = wall ? p.n_spec : p.n_scalar;
       at[f] = (int)all_sv.size();
-      for (int l = 0; l < nsc; ++l) all_sv.push_back(faces[f].sv && l < p.n_scalar ? faces[f].sv[l] : 0.0);
+      for (int l = 0; l < nsc; ++l) all_sv.push_back(faces[f].sv && l < nin ? faces[f].sv[l] : 0.0);
     }
     if (!all_sv.empty()) {
       cudaError_t e = cudaMalloc(&B.d_face_sv, all_sv.size() * sizeof(double));
@@ -664,9 +671,10 @@ int cb2_bind_block(cb2_ctx *ctx, int blk, const cb2_zone_view *v, const cb2_face
     for (int k = lo[2]; k <= hi[2]; ++k)
       for (int j = lo[1]; j <= hi[1]; ++j)
         for (int i = lo[0]; i <= hi[0]; ++i) {
-          if (b.face == 0) (b.direction < 0 ? il : ir)[j + k * my] = b.type;
-          else if (b.face == 1) (b.direction < 0 ? jl : jr)[i + k * mx] = b.type;
-          else (b.direction < 0 ? kl : kr)[i + j * mx] = b.type;
+          const int t = b.type & ~CB2_BC_NONREFLECTING;
+          if (b.face == 0) (b.direction < 0 ? il : ir)[j + k * my] = t;
+          else if (b.face == 1) (b.direction < 0 ? jl : jr)[i + k * mx] = t;
+          else (b.direction < 0 ? kl : kr)[i + j * mx] = t;
         }
   }
   const size_t n_all = il.size() + ir.size() + jl.size() + jr.size() + kl.size() + kr.size();
@@ -771,6 +779,8 @@ int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream) {
       CB2_TRY(launch_inviscid_comp(B->z, p, s, nl));
     else
       CB2_TRY(launch_inviscid_pv(B->z, pf, s, nl));
+    // the non-reflecting outflow faces correct dq after the inviscid flux (src/RK.cuh:190-193)
+    CB2_TRY(launch_nonreflecting(B->z, p, B->faces.data(), (int)B->faces.size(), s, nl));
   }
   return count(ctx, nl);
 }

@@ -387,13 +387,16 @@ __global__ void k_bc_wall(Zone z, Param p, FaceBC f) {
     const double tve_in = z.tve[g1] > 0.0 ? z.tve[g1] : z.bv[g1 + 5 * sz];
     tve_wall = !iso ? tve_in : (f.wall_Tve > 0.0 ? f.wall_Tve : t_wall);
   }
+  // a fully catalytic wall (Wall::catalytic_type 1) gives its face node and ghosts the wall's
+  // mass fractions f.sv (Wall::yk); a non-catalytic one copies them from the interior
+  const bool cat = NS > 0 && f.sv != nullptr;
   double R = kRAir;
   if (gl == 0) {
     const double pw = z.bv[g1 + 4 * sz];
     if constexpr (NS > 0) {
       R = 0;
       for (int s = 0; s < NS; ++s) {
-        z.sv[gb + s * sz] = z.sv[g1 + s * sz];
+        z.sv[gb + s * sz] = cat ? f.sv[s] : z.sv[g1 + s * sz];
         R += z.sv[gb + s * sz] * __ldg(p.mech.gas_const + s);
       }
     }
@@ -437,8 +440,10 @@ __global__ void k_bc_wall(Zone z, Param p, FaceBC f) {
     if constexpr (NS > 0) {
       R = 0;
       for (int s = 0; s < NS; ++s) {
-        z.sv[gg + s * sz] = z.sv[gi + s * sz];
-        R += z.sv[gi + s * sz] * __ldg(p.mech.gas_const + s);
+        // catalytic: R of the face node, which holds the wall's mass fractions
+        const double y = cat ? f.sv[s] : z.sv[gi + s * sz];
+        z.sv[gg + s * sz] = y;
+        R += y * __ldg(p.mech.gas_const + s);
       }
     }
     z.bv[gg] = p_i / (t_g * R);
@@ -694,6 +699,158 @@ static int launch_bc_ns(const Zone &z, const Param &p, const FaceBC *faces, int 
     }
   }
   return CB2_OK;
+}
+
+// Non-reflecting outflow (DBoundCond::nonReflectingBoundary -> apply_outflow_nr_conserv,
+// src/BoundCond.cu:3580-3845; called after the inviscid flux, src/RK.cuh:190-193): at every node
+// of the face, the conservative variables' normal derivative (one-sided, second order, into the
+// block) is split into the acoustic, entropy/vorticity and species waves along the unit face
+// normal; the waves that travel into the block are dropped (their speeds clipped at zero), and
+// the outgoing ones are added back to dq as -J (R Lambda L) dQ/dn.  The wave speeds are
+// u.n - c|grad k|, u.n, u.n + c|grad k| with n the unit normal, as the reference takes them.  The
+// mixture's gamma = cp / (cp - R) at the node's T; the species rows carry Y_k, and in two
+// temperatures the e_ve row takes no correction.  One thread per face node; the face's nodes
+// only (the reference also visits the tangential ghost nodes of an extended face, whose writes
+// land on other nodes of the ghost-free dq array).
+template <int NS>
+__global__ void k_outflow_nonreflecting(Zone z, Param p, FaceBC f) {
+  const int n0 = f.end[0] - f.start[0] + 1, n1 = f.end[1] - f.start[1] + 1;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n0 * n1 * (f.end[2] - f.start[2] + 1)) return;
+  const int i = f.start[0] + (int)(t % n0), j = f.start[1] + (int)((t / n0) % n1),
+            k = f.start[2] + (int)(t / ((long long)n0 * n1));
+  const idx_t sz = z.L.sz;
+  const int sgn = f.direction == -1 ? 1 : -1;  // into the block
+  idx_t step;
+  if (f.face == 0) step = 1;
+  else if (f.face == 1) step = z.L.disp2;
+  else step = z.L.disp1;
+  step *= sgn;
+  const idx_t g = z.L.at(i, j, k);
+  // dQ/dn: sgn * (-3/2 Q0 + 2 Q1 - 1/2 Q2), summed in the reference's order
+  const double cc[3] = {-1.5, 2.0, -0.5};
+  double dQ[5 + NS];
+#pragma unroll
+  for (int v = 0; v < 5 + NS; ++v) dQ[v] = 0;
+#pragma unroll
+  for (int l = 0; l <= 2; ++l) {
+    const double c = sgn * cc[l];
+    const idx_t gl = g + l * step;
+#pragma unroll
+    for (int v = 0; v < 5 + NS; ++v) dQ[v] += c * z.cv[gl + v * sz];
+  }
+  const double r = z.bv[g], u = z.bv[g + sz], v = z.bv[g + 2 * sz], w = z.bv[g + 3 * sz], pr = z.bv[g + 4 * sz];
+  const double *M = z.metric + (idx_t)(3 * f.face) * sz;
+  double kx = M[g], ky = M[g + sz], kz = M[g + 2 * sz];
+  const double gki = 1 / norm3d(kx, ky, kz);
+  kx *= gki; ky *= gki; kz *= gki;
+  const double Uk = u * kx + v * ky + w * kz;
+  double gam = kGammaAir;
+  double h[NS > 0 ? NS : 1], Y[NS > 0 ? NS : 1];
+  const double T = z.bv[g + 5 * sz];
+  if constexpr (NS > 0) {
+    double cp[NS];
+    species_h_cp<NS>(T, p.mech, h, cp);
+    double cpm = 0, cvm = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      Y[l] = z.sv[g + l * sz];
+      cpm += Y[l] * cp[l];
+      cvm += Y[l] * (cp[l] - __ldg(p.mech.gas_const + l));
+    }
+    gam = cpm / cvm;
+  }
+  const double c2 = gam * pr / r, c = sqrt(c2), ic2 = 1 / c2, cgk = c / gki;
+  double lam0 = Uk - cgk, lam1 = Uk, lam2 = Uk + cgk;
+  if (f.direction == -1) {
+    lam0 = fmin(lam0, 0.0); lam1 = fmin(lam1, 0.0); lam2 = fmin(lam2, 0.0);
+  } else {
+    lam0 = fmax(lam0, 0.0); lam1 = fmax(lam1, 0.0); lam2 = fmax(lam2, 0.0);
+  }
+  const double ek = 0.5 * (u * u + v * v + w * w), gm1 = gam - 1, alpha = gm1 * ek;
+  double aY = 0, al[NS > 0 ? NS : 1];
+  if constexpr (NS > 0) {
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      al[l] = gam * __ldg(p.mech.gas_const + l) * T - gm1 * h[l];
+      aY += al[l] * dQ[5 + l];
+    }
+  }
+  // wave amplitudes
+  const double L0 = lam0 * 0.5 * ic2 *
+                    ((alpha + Uk * c) * dQ[0] - (gm1 * u + kx * c) * dQ[1] - (gm1 * v + ky * c) * dQ[2] -
+                     (gm1 * w + kz * c) * dQ[3] + gm1 * dQ[4] + aY);
+  double tk = gm1 * kx;
+  const double L1 = lam1 * ic2 *
+                    ((kx * (c2 - alpha) - c * (kz * v - ky * w)) * dQ[0] + (tk * u) * dQ[1] + (tk * v + kz * c) * dQ[2] +
+                     (tk * w - ky * c) * dQ[3] - tk * dQ[4] - kx * aY);
+  tk = gm1 * ky;
+  const double L2 = lam1 * ic2 *
+                    ((ky * (c2 - alpha) - c * (kx * w - kz * u)) * dQ[0] + (tk * u - kz * c) * dQ[1] + (tk * v) * dQ[2] +
+                     (tk * w + kx * c) * dQ[3] - tk * dQ[4] - ky * aY);
+  tk = gm1 * kz;
+  const double L3 = lam1 * ic2 *
+                    ((kz * (c2 - alpha) - c * (ky * u - kx * v)) * dQ[0] + (tk * u + ky * c) * dQ[1] +
+                     (tk * v - kx * c) * dQ[2] + (tk * w) * dQ[3] - tk * dQ[4] - kz * aY);
+  const double L4 = lam2 * 0.5 * ic2 *
+                    ((alpha - Uk * c) * dQ[0] - (gm1 * u - kx * c) * dQ[1] - (gm1 * v - ky * c) * dQ[2] -
+                     (gm1 * w - kz * c) * dQ[3] + gm1 * dQ[4] + aY);
+  // back to conservative increments
+  const double hh = (z.cv[g + 4 * sz] + pr) / r, igm1 = 1 / gm1;
+  const double sum = L0 + kx * L1 + ky * L2 + kz * L3 + L4;
+  double d[5];
+  d[0] = sum;
+  d[1] = u * sum + c * (kx * (L4 - L0) - kz * L2 + ky * L3);
+  d[2] = v * sum + c * (ky * (L4 - L0) + kz * L1 - kx * L3);
+  d[3] = w * sum + c * (kz * (L4 - L0) - ky * L1 + kx * L2);
+  d[4] = hh * sum + c * (Uk * (L4 - L0) + (kz * v - ky * w - kx * c * igm1) * L1 +
+                         (kx * w - kz * u - ky * c * igm1) * L2 + (ky * u - kx * v - kz * c * igm1) * L3);
+  const double mj = -z.jac[g];
+  const idx_t g0 = z.L0.at(i, j, k), sz0 = z.L0.sz;
+  if constexpr (NS > 0) {
+    double add = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      const double Ls = lam1 * (dQ[5 + l] - Y[l] * dQ[0]);
+      z.dq[g0 + (5 + l) * sz0] += mj * (Ls + Y[l] * sum);
+      add += al[l] * Ls;
+    }
+    d[4] -= add * igm1;
+  }
+#pragma unroll
+  for (int l = 0; l < 5; ++l) z.dq[g0 + l * sz0] += mj * d[l];
+}
+
+template <int NS>
+static int launch_nr_ns(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, cudaStream_t s, int &nl) {
+  const int ext[3] = {z.mx, z.my, z.mz};
+  for (int fi = 0; fi < n_faces; ++fi) {
+    if (!faces[fi].nonreflecting) continue;
+    FaceBC f = faces[fi];
+    for (int a = 0; a < 3; ++a) {  // the face's own nodes
+      if (a == f.face) continue;
+      f.start[a] = max(f.start[a], 0);
+      f.end[a] = min(f.end[a], ext[a] - 1);
+    }
+    const long long n = (long long)max(f.end[0] - f.start[0] + 1, 0) * max(f.end[1] - f.start[1] + 1, 0) *
+                        max(f.end[2] - f.start[2] + 1, 0);
+    if (n == 0) continue;
+    ProfScope prof("outflow_nonreflecting", s);
+    k_outflow_nonreflecting<NS><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(z, p, f);
+    ++nl;
+    CB2_TRY(check_launch());
+  }
+  return CB2_OK;
+}
+
+int launch_nonreflecting(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, cudaStream_t s,
+                         int &n_launch) {
+  switch (p.n_spec) {
+    case 0: return launch_nr_ns<0>(z, p, faces, n_faces, s, n_launch);
+    case 5: return launch_nr_ns<5>(z, p, faces, n_faces, s, n_launch);
+    case 9: return launch_nr_ns<9>(z, p, faces, n_faces, s, n_launch);
+    default: return CB2_ERR_UNSUPPORTED;
+  }
 }
 
 int launch_eliminate_k_gradient(const Zone &z, const Param &p, cudaStream_t s, int &nl) {

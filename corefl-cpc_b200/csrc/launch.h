@@ -61,6 +61,7 @@ inline int prepare_smem(K kern, size_t bytes) {
 // Face boundary condition in device-usable form (after the reference's register_boundary).
 struct FaceBC {
   int type, face, direction;
+  int nonreflecting;  // outflow with the non-reflecting correction of dq (CB2_BC_NONREFLECTING)
   int start[3], end[3];
   double rho, u, v, w, p, T, wall_T, wall_Tve;
   const double *sv;  // inflow scalars (device copy of cb2_face_bc::sv)
@@ -83,6 +84,9 @@ int launch_boundary(const Zone &z, const Param &p, const FaceBC *faces, int n_fa
 int launch_inner_exchange(const Zone &z, const Zone &zt, const Param &p, const cb2_inner_face &f, cudaStream_t s,
                           int &nl);
 int launch_eliminate_k_gradient(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
+// the non-reflecting correction of dq at the nodes of every outflow face that asks for it
+int launch_nonreflecting(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, cudaStream_t s,
+                         int &n_launch);
 int launch_periodic_flux_exchange(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, cudaStream_t s,
                                   int &n_launch);
 // The 8th-order air viscous term writes dq instead of adding to it (assign = true) when it runs

@@ -189,7 +189,7 @@ inline void fill_mechanism(const cfd::Species &sp, const cfd::Reaction &re, bool
 
 // The face conditions the library applies, by label: the setup's boundary_conditions structs
 // (src/BoundCond.cu:80-200 reads the same ones).  An outflow with if_backPressure is the library's
-// back-pressure outflow.  Other types (subsonic inflow, the separate back_pressure type, ...) are
+// back-pressure outflow, one with nonReflecting its non-reflecting outflow.  Other types (subsonic inflow, the separate back_pressure type, ...) are
 // left to the reference: their label maps to -1.
 struct FaceKinds {
   std::map<int, int> type;          // label -> CB2_BC_*
@@ -241,6 +241,7 @@ struct Shim {
   MechTables tables;
   std::vector<cfd::Inflow> inflows;      // keep every inflow's and farfield's sv alive until bind
   std::vector<cfd::FarField> farfields;  // has copied it
+  std::vector<cfd::Wall> walls;          // and every catalytic wall's yk
 
   ~Shim() {
     if (ctx) cb2_destroy(ctx);
@@ -322,10 +323,13 @@ struct Shim {
         } else if (c.type == CB2_BC_OUTFLOW) {
           cfd::Outflow out(name, par);  // back pressure (if_backPressure) as p > 0
           if (out.if_backPressure == 1) c.p = out.backPressure;
+          if (out.nonReflecting > 0) c.type |= CB2_BC_NONREFLECTING;  // nonReflectingBoundary's faces
         } else if (c.type == CB2_BC_WALL) {
-          cfd::Wall wall(par.get_struct(name), par, sp);
+          walls.emplace_back(par.get_struct(name), par, sp);
+          const cfd::Wall &wall = walls.back();
           c.wall_temperature = wall.thermal_type == cfd::Wall::ThermalType::isothermal ? wall.temperature : 0.0;
           c.wall_temperature_ve = wall.temperature_ve > 0 ? wall.temperature_ve : 0.0;
+          if (wall.catalytic_type == 1) c.sv = wall.yk;  // fully catalytic: the wall mass fractions
         }
         faces.push_back(c);
       }

@@ -61,6 +61,11 @@ extern "C" {
 #define CB2_BC_INFLOW 5
 #define CB2_BC_OUTFLOW 6
 #define CB2_BC_PERIODIC 8
+/* OR'd into CB2_BC_OUTFLOW: the face is also a non-reflecting outflow (an Outflow with
+ * nonReflecting = 1): after the inviscid flux, cb2_rhs adds the characteristic correction of
+ * DBoundCond::nonReflectingBoundary (apply_outflow_nr_conserv, src/BoundCond.cu:3580-3845; called
+ * at src/RK.cuh:190-193) to dq at the face's nodes.  The ghost fill is the outflow's. */
+#define CB2_BC_NONREFLECTING 0x100
 
 /* precision forms */
 #define CB2_PREC_FP64 0  /* plain form: FP64 throughout                                    */
@@ -117,8 +122,10 @@ typedef struct cb2_face_bc {
    * temperature) or of a farfield state (FarField::temperature_ve; <= 0: its boundary T) */
   double wall_temperature_ve;
   /* inflow and farfield: the n_scalar scalars of the state, Y_k and then (two temperatures) e_ve
-   * (Inflow::sv / FarField::sv, src/BoundCond.h:23-169); a HOST array copied at bind.  Required
-   * with species. */
+   * (Inflow::sv / FarField::sv, src/BoundCond.h:23-169); required with species.  A wall of a
+   * mixture: NULL for a non-catalytic wall (the ghosts copy the interior's Y_k), else the n_spec
+   * mass fractions of a fully catalytic wall (Wall::yk with catalytic_type 1, src/BoundCond.h:105-107),
+   * which its face node and ghosts take.  A HOST array copied at bind. */
   const double *sv;
 } cb2_face_bc;
 

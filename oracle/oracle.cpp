@@ -1713,7 +1713,9 @@ Zone make_zone(const cb2_zone_view &v, const cb2_face_bc *faces, int n_faces, co
   for (int f = 0; f < n_faces; ++f) {
     const cb2_face_bc &b = faces[f];
     FaceBC o;
-    o.type = b.type; o.face = b.face; o.direction = b.direction;
+    o.type = b.type & ~CB2_BC_NONREFLECTING;
+    o.nonreflecting = (b.type & CB2_BC_NONREFLECTING) != 0;
+    o.face = b.face; o.direction = b.direction;
     for (int a = 0; a < 3; ++a) { o.start[a] = b.range_start[a]; o.end[a] = b.range_end[a]; }
     // register_boundary (src/Mesh.cpp:14-32)
     const int gx = extend ? g : 0;
@@ -1726,7 +1728,8 @@ Zone make_zone(const cb2_zone_view &v, const cb2_face_bc *faces, int n_faces, co
     if (p.dim == 2) { o.start[2] = -gx; o.end[2] = gx; }
     o.rho = b.rho; o.u = b.u; o.v = b.v; o.w = b.w; o.p = b.p; o.T = b.T; o.wall_T = b.wall_temperature;
     o.wall_Tve = b.wall_temperature_ve;
-    if (b.sv) o.sv.assign(b.sv, b.sv + p.n_scalar);
+    // a wall's sv: its mass fractions when fully catalytic (Wall::yk, n_spec values)
+    if (b.sv) o.sv.assign(b.sv, b.sv + (o.type == CB2_BC_WALL ? p.n_spec : p.n_scalar));
     z.faces.push_back(o);
     if (b.type == CB2_BC_PERIODIC) continue;
     int lo[3], hi[3];
@@ -1738,9 +1741,9 @@ Zone make_zone(const cb2_zone_view &v, const cb2_face_bc *faces, int n_faces, co
     for (int k = lo[2]; k <= hi[2]; ++k)
       for (int j = lo[1]; j <= hi[1]; ++j)
         for (int i = lo[0]; i <= hi[0]; ++i) {
-          if (b.face == 0) (b.direction < 0 ? z.il : z.ir)[j + k * my] = b.type;
-          else if (b.face == 1) (b.direction < 0 ? z.jl : z.jr)[i + k * mx] = b.type;
-          else (b.direction < 0 ? z.kl : z.kr)[i + j * mx] = b.type;
+          if (b.face == 0) (b.direction < 0 ? z.il : z.ir)[j + k * my] = o.type;
+          else if (b.face == 1) (b.direction < 0 ? z.jl : z.jr)[i + k * mx] = o.type;
+          else (b.direction < 0 ? z.kl : z.kr)[i + j * mx] = o.type;
         }
   }
   return z;
@@ -2135,6 +2138,111 @@ void back_pressure_point(Zone &z, const Param &p, const FaceBC &f, const int *di
 }
 
 // apply_boundary_conditions (src/BoundCond.cu:3846-3998) in its priority order
+// apply_outflow_nr_conserv (src/BoundCond.cu:3580-3817), run by nonReflectingBoundary
+// (:3818-3845) over the outflow faces flagged nonReflecting, after the inviscid flux
+// (src/RK.cuh:190-193).  Restricted to the face's own nodes: the reference's launch also covers
+// the tangential ghost nodes of an extended face (viscous_order 2), whose dq writes fall on
+// other nodes of the ghost-free dq array.
+void outflow_nonreflecting(Zone &z, const Param &p) {
+  const int ext[3] = {z.mx, z.my, z.mz};
+  for (const FaceBC &f : z.faces) {
+    if (!f.nonreflecting) continue;
+    int lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = f.start[a]; hi[a] = f.end[a];
+      if (a == f.face) continue;
+      lo[a] = std::max(lo[a], 0); hi[a] = std::min(hi[a], ext[a] - 1);
+    }
+    const int face = f.face;
+    const double cc[3] = {-1.5, 2, -0.5};
+    const bool start_face = f.direction == -1;
+    const int sgn = start_face ? 1 : -1;
+    for (int k = lo[2]; k <= hi[2]; ++k)
+      for (int j = lo[1]; j <= hi[1]; ++j)
+        for (int i = lo[0]; i <= hi[0]; ++i) {
+          double dR = 0, dRU = 0, dRV = 0, dRW = 0, dRE = 0;
+          std::vector<double> dRY(std::max(p.n_scalar, 1), 0.0);
+          for (int l = 0; l <= 2; ++l) {
+            const double c = sgn * cc[l];
+            const int ii = i + (face == 0 ? sgn * l : 0), jj = j + (face == 1 ? sgn * l : 0),
+                      kk = k + (face == 2 ? sgn * l : 0);
+            dR += c * z.cv(ii, jj, kk, 0);
+            dRU += c * z.cv(ii, jj, kk, 1);
+            dRV += c * z.cv(ii, jj, kk, 2);
+            dRW += c * z.cv(ii, jj, kk, 3);
+            dRE += c * z.cv(ii, jj, kk, 4);
+            for (int ls = 0; ls < p.n_scalar; ++ls) dRY[ls] += c * z.cv(ii, jj, kk, 5 + ls);
+          }
+          const double r = z.bv(i, j, k, 0), u = z.bv(i, j, k, 1), v = z.bv(i, j, k, 2), w = z.bv(i, j, k, 3),
+                       pr = z.bv(i, j, k, 4);
+          double kx = z.metric(i, j, k, face * 3), ky = z.metric(i, j, k, face * 3 + 1),
+                 kz = z.metric(i, j, k, face * 3 + 2);
+          const double gki = 1 / std::sqrt(kx * kx + ky * ky + kz * kz);
+          kx *= gki; ky *= gki; kz *= gki;
+          const double Uk = u * kx + v * ky + w * kz;
+          double gam = gamma_air;
+          const double T = z.bv(i, j, k, 5);
+          std::vector<double> h(std::max(p.n_spec, 1)), cp(std::max(p.n_spec, 1));
+          if (p.n_spec > 0) {
+            nasa7_h_cp(T, p.mech, h.data(), cp.data());
+            double cpm = 0, cvm = 0;
+            for (int l = 0; l < p.n_spec; ++l) {
+              cpm += z.sv(i, j, k, l) * cp[l];
+              cvm += z.sv(i, j, k, l) * (cp[l] - p.mech.gas_const[l]);
+            }
+            gam = cpm / cvm;
+          }
+          const double c2 = gam * pr / r, c = std::sqrt(c2), ic2 = 1 / c2, cgk = c / gki;
+          double lam[3] = {Uk - cgk, Uk, Uk + cgk};
+          for (double &x : lam) x = start_face ? std::min(x, 0.0) : std::max(x, 0.0);
+          const double ek = 0.5 * (u * u + v * v + w * w), gm1 = gam - 1, alpha = gm1 * ek;
+          double aY = 0;
+          std::vector<double> al(std::max(p.n_spec, 1), 0.0);
+          for (int l = 0; l < p.n_spec; ++l) {
+            al[l] = gam * p.mech.gas_const[l] * T - gm1 * h[l];
+            aY += al[l] * dRY[l];
+          }
+          double L[5];
+          L[0] = lam[0] * 0.5 * ic2 *
+                 ((alpha + Uk * c) * dR - (gm1 * u + kx * c) * dRU - (gm1 * v + ky * c) * dRV -
+                  (gm1 * w + kz * c) * dRW + gm1 * dRE + aY);
+          double tk = gm1 * kx;
+          L[1] = lam[1] * ic2 *
+                 ((kx * (c2 - alpha) - c * (kz * v - ky * w)) * dR + (tk * u) * dRU + (tk * v + kz * c) * dRV +
+                  (tk * w - ky * c) * dRW - tk * dRE - kx * aY);
+          tk = gm1 * ky;
+          L[2] = lam[1] * ic2 *
+                 ((ky * (c2 - alpha) - c * (kx * w - kz * u)) * dR + (tk * u - kz * c) * dRU + (tk * v) * dRV +
+                  (tk * w + kx * c) * dRW - tk * dRE - ky * aY);
+          tk = gm1 * kz;
+          L[3] = lam[1] * ic2 *
+                 ((kz * (c2 - alpha) - c * (ky * u - kx * v)) * dR + (tk * u + ky * c) * dRU +
+                  (tk * v - kx * c) * dRV + (tk * w) * dRW - tk * dRE - kz * aY);
+          L[4] = lam[2] * 0.5 * ic2 *
+                 ((alpha - Uk * c) * dR - (gm1 * u - kx * c) * dRU - (gm1 * v - ky * c) * dRV -
+                  (gm1 * w - kz * c) * dRW + gm1 * dRE + aY);
+          const double hh = (z.cv(i, j, k, 4) + pr) / r, igm1 = 1 / gm1;
+          const double sum = L[0] + kx * L[1] + ky * L[2] + kz * L[3] + L[4];
+          double d[5];
+          d[0] = sum;
+          d[1] = u * sum + c * (kx * (L[4] - L[0]) - kz * L[2] + ky * L[3]);
+          d[2] = v * sum + c * (ky * (L[4] - L[0]) + kz * L[1] - kx * L[3]);
+          d[3] = w * sum + c * (kz * (L[4] - L[0]) - ky * L[1] + kx * L[2]);
+          d[4] = hh * sum + c * (Uk * (L[4] - L[0]) + (kz * v - ky * w - kx * c * igm1) * L[1] +
+                                 (kx * w - kz * u - ky * c * igm1) * L[2] + (ky * u - kx * v - kz * c * igm1) * L[3]);
+          const double mj = -z.jac(i, j, k);
+          double add = 0;
+          for (int l = 0; l < p.n_spec; ++l) {
+            const double Ls = lam[1] * (dRY[l] - z.sv(i, j, k, l) * dR);
+            z.dq(i, j, k, 5 + l) += mj * (Ls + z.sv(i, j, k, l) * sum);
+            add += al[l] * Ls;
+          }
+          d[4] -= add * igm1;
+          for (int l = 0; l < 5; ++l) z.dq(i, j, k, l) += mj * d[l];
+        }
+  }
+}
+
 void apply_boundary_conditions(Zone &z, const Param &p) {
   for (int type : {CB2_BC_FARFIELD, CB2_BC_OUTFLOW, CB2_BC_INFLOW, CB2_BC_SYMMETRY, CB2_BC_WALL, CB2_BC_PERIODIC}) {
     for (const auto &f : z.faces) {
@@ -2198,7 +2306,10 @@ void apply_boundary_conditions(Zone &z, const Param &p) {
                 for (int l = 0; l < p.n_scalar; ++l) z.sv(gi, gj, gk, l) = z.sv(ii, ij, ik, l);
                 cv_point(z, p, gi, gj, gk);
               }
-            } else if (type == CB2_BC_WALL) {  // src/BoundCond.cu:3055-3389, non-catalytic
+            } else if (type == CB2_BC_WALL) {  // src/BoundCond.cu:3055-3389
+              // a fully catalytic wall (catalytic_type 1) sets the face node and its ghosts to the
+              // wall's mass fractions (Wall::yk, :3197-3203 and :3344-3357)
+              const bool cat = p.n_spec > 0 && !f.sv.empty();
               int idx[3] = {i - dir[0], j - dir[1], k - dir[2]};
               project_to_interior(z, idx[0], idx[1], idx[2]);
               const bool iso = f.wall_T > 0;
@@ -2211,7 +2322,7 @@ void apply_boundary_conditions(Zone &z, const Param &p) {
                 tve_wall = !iso ? tve_in : (f.wall_Tve > 0.0 ? f.wall_Tve : t_wall);
               }
               const double pw = z.bv(idx[0], idx[1], idx[2], 4);
-              for (int l = 0; l < p.n_spec; ++l) z.sv(i, j, k, l) = z.sv(idx[0], idx[1], idx[2], l);
+              for (int l = 0; l < p.n_spec; ++l) z.sv(i, j, k, l) = cat ? f.sv[l] : z.sv(idx[0], idx[1], idx[2], l);
               double R = mix_r(z, p, i, j, k);
               z.bv(i, j, k, 0) = pw / (t_wall * R);
               z.bv(i, j, k, 1) = z.bv(i, j, k, 2) = z.bv(i, j, k, 3) = 0;
@@ -2244,8 +2355,9 @@ void apply_boundary_conditions(Zone &z, const Param &p) {
                     if (tve_g <= floor_ve) tve_g = floor_ve;
                   }
                 }
-                for (int l = 0; l < p.n_spec; ++l) z.sv(gh[0], gh[1], gh[2], l) = z.sv(in[0], in[1], in[2], l);
-                R = mix_r(z, p, in[0], in[1], in[2]);
+                for (int l = 0; l < p.n_spec; ++l)
+                  z.sv(gh[0], gh[1], gh[2], l) = cat ? f.sv[l] : z.sv(in[0], in[1], in[2], l);
+                R = cat ? mix_r(z, p, i, j, k) : mix_r(z, p, in[0], in[1], in[2]);
                 z.bv(gh[0], gh[1], gh[2], 0) = p_i / (t_g * R);
                 for (int c = 1; c <= 3; ++c) z.bv(gh[0], gh[1], gh[2], c) = -z.bv(in[0], in[1], in[2], c);
                 z.bv(gh[0], gh[1], gh[2], 4) = p_i;
@@ -2501,6 +2613,7 @@ void rk3_step(std::vector<Zone> &zones, const Param &p_in, double &dt, bool fixe
     for (auto &z : zones) {
       if (p.reaction) finite_rate_chemistry(z, p);
       compute_inviscid_flux(z, p);
+      outflow_nonreflecting(z, p);
       update_cv_and_bv_rk(z, p, dt, rk);
       apply_boundary_conditions(z, p);
     }

@@ -86,6 +86,7 @@ struct Param {
 
 struct FaceBC {
   int type = 0, face = 0, direction = 1;
+  bool nonreflecting = false;  // outflow with the non-reflecting dq correction
   int start[3] = {0, 0, 0}, end[3] = {0, 0, 0};
   double rho = 0, u = 0, v = 0, w = 0, p = 0, T = 0, wall_T = 0, wall_Tve = 0;
   std::vector<double> sv;  // inflow scalars
@@ -108,6 +109,7 @@ void inner_exchange(std::vector<Zone> &zones, const Param &p);
 void limit_flow(Zone &z, const Param &p);
 void compute_cv_from_bv(Zone &z, const Param &p);
 void compute_inviscid_flux(Zone &z, const Param &p);
+void outflow_nonreflecting(Zone &z, const Param &p);
 void compute_viscous_flux(Zone &z, const Param &p);
 void compute_chemistry(Zone &z, const Param &p);
 void chemistry_source(const Mechanism &m, double rho, double t, const double *y, double *omega, double *omega_d);

@@ -79,7 +79,10 @@ int oracle_rhs(const cb2_param_view *pv, const cb2_zone_view *zv, const cb2_face
   std::memset(z.dq.p, 0, (size_t)z.dq.sz * p.n_var * sizeof(double));
   if (mask & CB2_RHS_VISCOUS) compute_viscous_flux(z, p);
   if ((mask & CB2_RHS_CHEMISTRY) && p.reaction) compute_chemistry(z, p);
-  if (mask & CB2_RHS_INVISCID) compute_inviscid_flux(z, p);
+  if (mask & CB2_RHS_INVISCID) {
+    compute_inviscid_flux(z, p);
+    outflow_nonreflecting(z, p);
+  }
   return 0;
 }
 

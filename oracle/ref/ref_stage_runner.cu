@@ -181,6 +181,8 @@ struct Runner {
       for (int b = 0; b < mesh.n_block; ++b) {
         if (parameter.get_int("reaction") == 1) cfd::finite_rate_chemistry<<<bpg[b], tpb>>>(field[b].d_ptr, param);
         cfd::compute_inviscid_flux<mix>(mesh[b], field[b].d_ptr, param, n_var, parameter);
+        // the non-reflecting outflows' correction of dq, before the dump (RK.cuh:190-193)
+        bc.nonReflectingBoundary<mix>(mesh[b], field[b], param);
       }
       check("residual");
       if (dq_out) {
@@ -191,7 +193,6 @@ struct Runner {
         }
       }
       for (int b = 0; b < mesh.n_block; ++b) {
-        bc.nonReflectingBoundary<mix>(mesh[b], field[b], param);
         cfd::update_cv_and_bv_rk<mix><<<bpg[b], tpb>>>(field[b].d_ptr, param, dt, rk);
         if constexpr (cfd::kTwoTemperature) {
           cfd::apply_vt_relaxation_rk<<<bpg[b], tpb>>>(field[b].d_ptr, param, rk_stage_dt_scale[rk] * dt);

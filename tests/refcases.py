@@ -46,6 +46,11 @@ CHAN_WALL_T = 0.004
 # the farfield channel: farfield (i- and j+), back-pressure outflow (i+), isothermal wall (j-)
 CHAN_FARFIELD = dict(rho=1.1, u=0.6, p=1.0)
 CHAN_BACK_PRESSURE = 1.05
+# fully catalytic isothermal walls of the mixture boxes (low x face): wall temperature and the
+# wall's mass fractions (Wall::yk), by species name
+CAT_WALL = {"mix": (1000.0, {"H2O": 0.25, "N2": 0.75}), "air5": (2000.0, {"N2": 0.767, "O2": 0.233})}
+# a non-reflecting outflow face: its type (and the label of its struct in the reference's setup)
+BC_OUTFLOW_NR = abi.BC_OUTFLOW | abi.BC_NONREFLECTING
 
 
 def ref_ngg(scheme, visc):
@@ -66,8 +71,8 @@ def _air(name, scheme, rec, visc, bc, stages=3, dt=2e-3, seed=11):
                 seed=seed, pp=0, limit_flow=0, reaction=0)
 
 
-def _mix(name, scheme, rec, visc, reaction, pp=0, stages=3, dt=2e-9):
-    return dict(family="mix", name=name, scheme=scheme, rec=rec, visc=visc, bc="periodic", stages=stages, dt=dt,
+def _mix(name, scheme, rec, visc, reaction, pp=0, stages=3, dt=2e-9, bc="periodic"):
+    return dict(family="mix", name=name, scheme=scheme, rec=rec, visc=visc, bc=bc, stages=stages, dt=dt,
                 seed=2024, pp=pp, limit_flow=0, reaction=reaction)
 
 
@@ -95,7 +100,10 @@ CASES = ([_air(n + "_" + bc, s, r, v, bc) for n, s, r, v in AIR_SCHEMES for bc i
           _air5("air5_weno5ch_visc2_outflow", 2, 1, bc="outflow"), _air5("air5_weno5ch_visc8_chem", 8, 1)] +
          [_chan("chan_hllc_muscl_visc2", 4, 2, 2), _chan("chan_weno5ch_visc2", 52, 2, 2),
           _chan("chan_roe_muscl", 2, 2, 0), _chan("chan_farfield_weno5ch", 52, 2, 0, bc="farfield"),
-          _chan("chan_farfield_hllc_visc2", 4, 2, 2, bc="farfield")] +
+          _chan("chan_farfield_hllc_visc2", 4, 2, 2, bc="farfield"), _chan("chan_nr_weno5ch", 52, 2, 0, bc="nr"),
+          _chan("chan_nr_ausm_muscl", 3, 2, 0, bc="nr"), _mix("mix_nr_weno5ch", 52, 2, 0, 0, bc="nr"),
+          _mix("mix_catwall_weno5ch", 52, 2, 0, 0, bc="catwall"),
+          _air5("air5_catwall_weno5ch", 0, 1, bc="catwall")] +
          [dict(family="sod", name="sod_1000x7", scheme=52, rec=2, visc=0, bc="outflow", stages=0, dt=0.0, seed=0,
                pp=0, limit_flow=0, reaction=0, mx=1000, my=7, cfl=0.5, t_end=0.2)])
 
@@ -148,12 +156,15 @@ def build(case):
         ci = CHAN_INFLOW
         # T from (p, rho) as the reference's Inflow takes it: pressure * mw / (density * R_u)
         t_in = ci["p"] * cases.MW_AIR / (ci["rho"] * cases.R_U)
-        if case["bc"] == "farfield":
+        if case["bc"] in ("farfield", "nr"):
             ff = CHAN_FARFIELD
             t_ff = ff["p"] * cases.MW_AIR / (ff["rho"] * cases.R_U)
             st = dict(rho=ff["rho"], u=ff["u"], v=0.0, w=0.0, p=ff["p"], T=t_ff)
-            faces = [face(abi.BC_FARFIELD, 0, -1, (0, 0, 0), (0, my - 1, 0), **st),
-                     face(abi.BC_OUTFLOW, 0, 1, (mx - 1, 0, 0), (mx - 1, my - 1, 0), p=CHAN_BACK_PRESSURE),
+            # the subsonic channel's exit: back pressure, or non-reflecting (its upstream wave clipped)
+            exit_face = (face(abi.BC_OUTFLOW, 0, 1, (mx - 1, 0, 0), (mx - 1, my - 1, 0), p=CHAN_BACK_PRESSURE)
+                         if case["bc"] == "farfield" else
+                         face(BC_OUTFLOW_NR, 0, 1, (mx - 1, 0, 0), (mx - 1, my - 1, 0)))
+            faces = [face(abi.BC_FARFIELD, 0, -1, (0, 0, 0), (0, my - 1, 0), **st), exit_face,
                      face(abi.BC_WALL, 1, -1, (0, 0, 0), (mx - 1, 0, 0), wall_temperature=CHAN_WALL_T),
                      face(abi.BC_FARFIELD, 1, 1, (0, my - 1, 0), (mx - 1, my - 1, 0), **st)]
         else:
@@ -173,6 +184,12 @@ def build(case):
         c = cases.h2_air_box(m, n_nodes=MIX_NODES, ngg=g, seed=case["seed"], scheme=case["scheme"],
                              reconstruction=case["rec"], viscous_order=case["visc"], reaction=bool(case["reaction"]))
         p, hb, faces = c.param, c.blocks[0], c.faces[0]
+        if case["bc"] == "catwall":
+            faces = catalytic_wall_faces(fam, m, hb)
+        if case["bc"] == "nr":  # x faces non-reflecting outflows, the others plain outflows
+            faces = box_faces(hb.mx, hb.my, hb.mz,
+                              {(d, s_): (BC_OUTFLOW_NR if d == 0 else abi.BC_OUTFLOW) for d in range(3)
+                               for s_ in (-1, 1)})
         extra = {"mech": m}
     elif fam == "air5":
         m, tt = _mech(fam)
@@ -181,6 +198,8 @@ def build(case):
         p, hb, faces = c.param, c.blocks[0], c.faces[0]
         if case["bc"] == "outflow":
             faces = box_faces(hb.mx, hb.my, hb.mz, {(d, s_): abi.BC_OUTFLOW for d in range(3) for s_ in (-1, 1)})
+        if case["bc"] == "catwall":
+            faces = catalytic_wall_faces(fam, m, hb)
         extra = {"mech": m, "two_t": tt}
     else:
         raise ValueError(fam)
@@ -188,6 +207,21 @@ def build(case):
     p.limit_flow = case["limit_flow"]
     p.dt = case["dt"]
     return p, hb, faces, extra
+
+
+def catalytic_wall_faces(fam, m, hb):
+    """A fully catalytic isothermal wall on the low x face, an outflow on the high one, periodic in
+    y and z."""
+    from cb200.field import face
+    t_wall, yw = CAT_WALL[fam]
+    y = np.zeros(m.ns)
+    for name, v in yw.items():
+        y[m.index(name)] = v
+    mx, my, mz = hb.mx, hb.my, hb.mz
+    faces = [face(abi.BC_WALL, 0, -1, (0, 0, 0), (0, my - 1, mz - 1), sv=y, wall_temperature=t_wall),
+             face(abi.BC_OUTFLOW, 0, 1, (mx - 1, 0, 0), (mx - 1, my - 1, mz - 1))]
+    faces += box_faces(mx, my, mz, {(d, s_): abi.BC_PERIODIC for d in (1, 2) for s_ in (-1, 1)})
+    return faces
 
 
 def state_arrays(case, hb):
@@ -236,7 +270,10 @@ def _face_lines(faces, dim):
 
 
 BC_NAMES = {abi.BC_OUTFLOW: "outflow", abi.BC_PERIODIC: "periodic", abi.BC_SYMMETRY: "symmetry",
-            abi.BC_WALL: "wall", abi.BC_INFLOW: "inflow", abi.BC_FARFIELD: "farfield"}
+            abi.BC_WALL: "wall", abi.BC_INFLOW: "inflow", abi.BC_FARFIELD: "farfield",
+            BC_OUTFLOW_NR: "outflow_nr"}
+# the reference's type of each struct (a non-reflecting outflow is an outflow with its own label)
+BC_TYPES = {**BC_NAMES, BC_OUTFLOW_NR: "outflow"}
 
 
 def _coords(case, hb):
@@ -314,12 +351,18 @@ def write_reference_case(case, case_dir, ref_dir):
     s += ["    %s" % BC_NAMES[t] for t in labels]
     s.append("}")
     for t in labels:
-        s += ["struct %s {" % BC_NAMES[t], "    string type = %s" % BC_NAMES[t], "    int label = %d" % t]
+        s += ["struct %s {" % BC_NAMES[t], "    string type = %s" % BC_TYPES[t], "    int label = %d" % t]
+        if t == BC_OUTFLOW_NR:
+            s.append("    int nonReflecting = 1")
         if t == abi.BC_INFLOW:
             ci = CHAN_INFLOW
             s += ["    real density = %r" % ci["rho"], "    real velocity = %r" % ci["u"], "    real u = 1.0",
                   "    real v = 0.0", "    real w = 0.0", "    real pressure = %r" % ci["p"]]
-        if t == abi.BC_WALL:
+        if t == abi.BC_WALL and case.get("bc") == "catwall":
+            t_wall, yw = CAT_WALL[fam]
+            s += ["    string thermal_type = isothermal", "    real temperature = %r" % t_wall,
+                  "    int catalytic_type = 1"] + ["    real %s = %r" % (n, v) for n, v in yw.items()]
+        elif t == abi.BC_WALL:
             s += ["    string thermal_type = isothermal", "    real temperature = %r" % CHAN_WALL_T]
         if t == abi.BC_FARFIELD:
             ff = CHAN_FARFIELD
