@@ -64,6 +64,8 @@ def load():
         "cb2_reactor_setup": (C.c_int, [vp, vp, C.c_int, vp, vp, vp, vp, C.c_double, vp]),
         "cb2_reactor_advance": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_double, C.c_double, vp]),
         "cb2_metrics": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp]),
+        "cb2_write_flowfield": (C.c_int, [vp, C.c_char_p, P(vp), P(C.c_char_p), C.c_int, C.c_double, vp]),
+        "cb2_read_flowfield": (C.c_int, [vp, C.c_char_p, P(C.c_char_p), P(C.c_double), vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -158,6 +160,23 @@ class Context:
 
     def cv_from_bv(self, blk, stream=None):
         check(self.lib.cb2_cv_from_bv(self.h, blk, stream), "cb2_cv_from_bv")
+
+    def write_flowfield(self, path, xyz, species_names=(), ngg_out=0, solution_time=0.0, stream=None):
+        """cb2_write_flowfield: xyz = per block (x, y, z) float64 host arrays padded like the fields."""
+        import numpy as np
+        keep = [np.ascontiguousarray(a, dtype=np.float64) for blk in xyz for a in blk]
+        ptrs = (C.c_void_p * len(keep))(*[a.ctypes.data for a in keep])
+        names = (C.c_char_p * max(1, len(species_names)))(*[n.encode() for n in species_names])
+        check(self.lib.cb2_write_flowfield(self.h, str(path).encode(), ptrs, names, ngg_out, solution_time, stream),
+              "cb2_write_flowfield")
+
+    def read_flowfield(self, path, species_names=(), stream=None):
+        """cb2_read_flowfield; returns the file's solution time."""
+        names = (C.c_char_p * max(1, len(species_names)))(*[n.encode() for n in species_names])
+        t = C.c_double(0.0)
+        check(self.lib.cb2_read_flowfield(self.h, str(path).encode(), names, C.byref(t), stream),
+              "cb2_read_flowfield")
+        return t.value
 
     def store_qn(self, blk, stream=None):
         check(self.lib.cb2_store_qn(self.h, blk, stream), "cb2_store_qn")

@@ -128,6 +128,16 @@ struct cb2_ctx {
 
 namespace cb2 {
 const Param *ctx_param(const cb2_ctx *ctx) { return ctx ? &ctx->p : nullptr; }
+// The zones of the context's blocks 0 .. n-1, all of which must be bound.
+int ctx_zones(const cb2_ctx *ctx, std::vector<Zone> &zones) {
+  zones.clear();
+  if (!ctx || ctx->blocks.empty()) return CB2_ERR_INVALID;
+  for (const Block &B : ctx->blocks) {
+    if (!B.bound) return CB2_ERR_INVALID;
+    zones.push_back(B.z);
+  }
+  return CB2_OK;
+}
 }  // namespace cb2
 
 namespace {

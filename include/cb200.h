@@ -335,6 +335,30 @@ int cb2_cv_from_bv(cb2_ctx *ctx, int blk, void *stream);
 int cb2_metrics(const double *x, const double *y, const double *z, int mx, int my, int mz, int g_coord, int ngg,
                 double *metric, double *jac, void *stream);
 
+/* Flowfield file of every bound block (blocks 0 .. n-1, all bound): the reference's
+ * output/flowfield.plt (FieldIO::initialize / print_field, src/FieldIO.h:77-470), a Tecplot binary
+ * file (version 112, one ordered zone "zone <b>" per block, double data at the nodes) holding x, y,
+ * z, density, u, v, w, pressure, temperature, the n_spec species (`species_names`, the mechanism's
+ * order), Eve (two temperatures), mach and Tve (two temperatures), over the block's nodes and
+ * `ngg_out` ghost layers (the reference writes 0).  xyz[3 b + c] are HOST arrays of block b's
+ * coordinates x, y, z, padded like its field arrays (ghost ngg).  The blocks' bv, sv, mach and
+ * T_ve are copied to the host over `stream`, which is synchronised.  Error: CB2_ERR_INVALID
+ * (bad arguments, no mach array, the file cannot be written). */
+int cb2_write_flowfield(cb2_ctx *ctx, const char *path, const double *const *xyz, const char *const *species_names,
+                        int ngg_out, double solution_time, void *stream);
+
+/* Restart from a flowfield file (read_flowfield with the same blocks, src/Initialize.cu:167-411): the
+ * file's zones must be the bound blocks in order, each with the same number g <= ngg of ghost layers
+ * on every side.  Variables are matched by name, ignoring case, as the reference does: density (or
+ * rho), u, v, w, pressure (or p), temperature (or t) into bv, the species names into sv, Eve into
+ * e_ve's sv slot and Tve into T_ve (two temperatures; without Tve, T_ve is set to 0 so that the next
+ * cv-from-bv pass finds it from e_ve); other variables are skipped.  The file's nodes (with its g
+ * ghost layers) are overwritten; the rest keeps its values.  The caller then rebuilds cv and the
+ * properties (cb2_cv_from_bv, cb2_properties) as after any change of bv.  *solution_time (if not
+ * NULL) receives the zones' solution time.  Synchronises `stream`. */
+int cb2_read_flowfield(cb2_ctx *ctx, const char *path, const char *const *species_names, double *solution_time,
+                       void *stream);
+
 /* Local CFL time step of every node and the min over all bound blocks, returned to the
  * host: replaces local_time_step<mix> + global_time_step (src/TimeAdvanceFunc.cuh:28-127,
  * src/TimeAdvanceFunc.cu:114-139).  Synchronises `stream`. */

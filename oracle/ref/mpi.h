@@ -8,8 +8,9 @@
 // One rank, rank 0 of a world of 1.  Collectives copy the send buffer to the receive buffer (the
 // result of any reduction over one rank); point-to-point calls are never made by a serial run
 // (`parallel = 0`) and return an error if they are.  Files are plain stdio files addressed by
-// byte offsets; of the derived datatypes only 3-D Fortran-order subarrays of doubles read with
-// MPI_File_read (the reference's binary grid reader) are supported; other uses report an error,
+// byte offsets; of the derived datatypes only 3-D Fortran-order subarrays of doubles are supported
+// (MPI_File_read of the binary grid reader, MPI_File_read_at / write_at of the flowfield reader and
+// writer); other uses report an error,
 // so a code path that depends on them fails loudly instead of reading garbage.
 #pragma once
 #include <cstdio>
@@ -138,8 +139,12 @@ inline int MPI_Type_free(MPI_Datatype *) { return MPI_SUCCESS; }
 
 // ---- files ----
 inline int MPI_File_open(MPI_Comm, const char *name, int mode, MPI_Info, MPI_File *fh) {
+  // a write without MPI_MODE_CREATE updates the existing file in place (the flowfield writer opens
+  // its file again to write the data section after the header)
   const char *m = (mode & MPI_MODE_RDONLY) ? "rb" : ((mode & MPI_MODE_APPEND) ? "ab" : "w+b");
-  std::FILE *fp = std::fopen(name, m);
+  std::FILE *fp = nullptr;
+  if (!(mode & (MPI_MODE_RDONLY | MPI_MODE_APPEND | MPI_MODE_CREATE))) fp = std::fopen(name, "r+b");
+  if (!fp) fp = std::fopen(name, m);
   if (!fp) {
     *fh = MPI_FILE_NULL;
     return MPI_ERR_OTHER;
@@ -162,10 +167,28 @@ inline int cb2_mpi_file_io(MPI_File fh, long long off, void *buf, int n, MPI_Dat
   const size_t done = write ? std::fwrite(buf, 1, bytes, fh->fp) : std::fread(buf, 1, bytes, fh->fp);
   return done == bytes ? MPI_SUCCESS : MPI_ERR_OTHER;
 }
+// one 3-D Fortran-order subarray of doubles at byte offset off: its elements in file order (first
+// index fastest) to or from their places in the full array at buf (the flowfield writer and the
+// restart reader, src/FieldIO.h, src/Initialize.cu)
+inline int cb2_mpi_subarray_io(MPI_File fh, long long off, double *buf, MPI_Datatype t, bool write) {
+  if (!fh || -1 - t >= cb2_mpi_n_subarrays()) return MPI_ERR_OTHER;
+  if (std::fseek(fh->fp, off, SEEK_SET) != 0) return MPI_ERR_OTHER;
+  const cb2_mpi_subarray &d = cb2_mpi_subarrays()[-1 - t];
+  for (int k = 0; k < d.subsizes[2]; ++k)
+    for (int j = 0; j < d.subsizes[1]; ++j) {
+      double *row = buf + d.starts[0] + (size_t)d.sizes[0] * ((d.starts[1] + j) + (size_t)d.sizes[1] * (d.starts[2] + k));
+      const size_t done = write ? std::fwrite(row, sizeof(double), d.subsizes[0], fh->fp)
+                                : std::fread(row, sizeof(double), d.subsizes[0], fh->fp);
+      if (done != (size_t)d.subsizes[0]) return MPI_ERR_OTHER;
+    }
+  return MPI_SUCCESS;
+}
 inline int MPI_File_read_at(MPI_File fh, MPI_Offset off, void *buf, int n, MPI_Datatype t, MPI_Status *) {
+  if (t < 0 && n == 1) return cb2_mpi_subarray_io(fh, off, static_cast<double *>(buf), t, false);
   return cb2_mpi_file_io(fh, off, buf, n, t, false);
 }
 inline int MPI_File_write_at(MPI_File fh, MPI_Offset off, const void *buf, int n, MPI_Datatype t, MPI_Status *) {
+  if (t < 0 && n == 1) return cb2_mpi_subarray_io(fh, off, static_cast<double *>(const_cast<void *>(buf)), t, true);
   return cb2_mpi_file_io(fh, off, const_cast<void *>(buf), n, t, true);
 }
 inline int MPI_File_read(MPI_File fh, void *buf, int n, MPI_Datatype t, MPI_Status *) {

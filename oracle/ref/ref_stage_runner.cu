@@ -24,7 +24,8 @@
 // Usage: ref_stage_runner <case-dir>
 //   <case-dir>/input/setup.txt, input/grid/grid   0.grd, input/boundary_condition/{boundary,inner}   0.txt
 //   <case-dir>/task.txt   : "key value" lines: mode (stages|steps|time), stages, n_steps, warmup, dt,
-//                           fixed_dt, t_end, mul_constant, load_metric (0/1), init (file|reference)
+//                           fixed_dt, t_end, mul_constant, load_metric (0/1), init (file|reference),
+//                           write_plt (0/1: the reference's output/flowfield.plt of the final state)
 //   <case-dir>/state.bin  : per block, float64 padded arrays (ghost ngg): bv[6], sv[n_scalar],
 //                           T_ve (two-temperature build), then metric[9] and jac when load_metric = 1
 //   writes <case-dir>/out.bin : the layout is written out above the dump in run().
@@ -53,6 +54,7 @@
 #include "Initialize.cuh"
 #include "SinglePointStat.cuh"
 #include "RK.cuh"
+#include "FieldIO.h"
 
 namespace {
 
@@ -376,6 +378,15 @@ int run(cfd::Parameter &parameter, cfd::Mesh &mesh, cfd::Species &spec, cfd::Rea
   for (auto &d : dq) std::fwrite(d.data(), sizeof(double), d.size(), o);
   std::fclose(o);
   check("dump");
+  if (tget(task, "write_plt", 0) != 0) {
+    // the reference's own flowfield file of the final state (output/flowfield.plt, no ghost layers
+    // as its drivers write it): FieldIO::initialize after copying the fields to the host
+    for (int b = 0; b < mesh.n_block; ++b) field[b].copy_data_from_device(parameter);
+    parameter.update_parameter("solution_time", time);
+    cfd::FieldIO<mix> io(0, mesh, field, parameter, spec, 0);
+    io.initialize();
+    check("flowfield");
+  }
   std::printf("ref_stage_runner: %d step(s), t = %.17g, dt = %.17g\n", steps, time, dt);
   return 0;
 }

@@ -11,7 +11,9 @@ on a GPU:
           fixture already has): for every case its definition,
           the digest of its initial state, the reference state the kernels read, the residual dq of
           the first stage and the conservative variables, temperature (and T_ve) after the last
-          stage on the interior nodes, and for the Sod run its time-step history.
+          stage on the interior nodes, and for the Sod run its time-step history.  Cases flagged
+          `plt` also leave the reference's own flowfield file of their final state
+          (tests/golden/plt/<case>.plt, written by its FieldIO).
 Usage:
   python tests/golden/make_ref_kernels.py write --work DIR [--ref REFDIR]
   python tests/golden/make_ref_kernels.py run --work DIR --out OUTDIR
@@ -22,6 +24,7 @@ import argparse
 import importlib.util
 import json
 import os
+import shutil
 import subprocess
 import sys
 
@@ -35,6 +38,7 @@ import numpy as np  # noqa: E402
 import refcases  # noqa: E402
 
 FIXTURE = os.path.join(HERE, "ref_kernels.npz")
+PLT_DIR = os.path.join(HERE, "plt")
 
 
 def _runner(family):
@@ -88,6 +92,9 @@ def cmd_run(args):
             print("runner failed on %s (rc %d): %s" % (n, r.returncode, r.stderr[-500:]))
             continue
         os.replace(os.path.join(d, "out.bin"), os.path.join(args.out, n, "out.bin"))
+        plt = os.path.join(d, "output", "flowfield.plt")
+        if os.path.exists(plt):
+            os.replace(plt, os.path.join(args.out, n, "flowfield.plt"))
         if os.path.exists(os.path.join(d, "ref_metric.bin")):
             os.replace(os.path.join(d, "ref_metric.bin"), os.path.join(args.out, n, "ref_metric.bin"))
         print(n, r.stdout.strip().splitlines()[-1] if r.stdout.strip() else "")
@@ -110,6 +117,10 @@ def cmd_pack(args):
             continue
         for k in [k for k in arrays if k.startswith(n + "/")]:
             del arrays[k]
+        plt = os.path.join(args.out, n, "flowfield.plt")
+        if os.path.exists(plt):  # the reference's flowfield file: tests/golden/plt/<case>.plt
+            os.makedirs(PLT_DIR, exist_ok=True)
+            shutil.copy(plt, os.path.join(PLT_DIR, n + ".plt"))
         d = refcases.read_dump(path)
         blk = d["blocks"][0]
         g = blk["dims"][3]

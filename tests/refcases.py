@@ -71,19 +71,19 @@ def _air(name, scheme, rec, visc, bc, stages=3, dt=2e-3, seed=11):
                 seed=seed, pp=0, limit_flow=0, reaction=0)
 
 
-def _mix(name, scheme, rec, visc, reaction, pp=0, stages=3, dt=2e-9, bc="periodic"):
+def _mix(name, scheme, rec, visc, reaction, pp=0, stages=3, dt=2e-9, bc="periodic", plt=0):
     return dict(family="mix", name=name, scheme=scheme, rec=rec, visc=visc, bc=bc, stages=stages, dt=dt,
-                seed=2024, pp=pp, limit_flow=0, reaction=reaction)
+                seed=2024, pp=pp, limit_flow=0, reaction=reaction, plt=plt)
 
 
-def _air5(name, visc, reaction, pp=0, limit_flow=0, stages=3, dt=2e-9, bc="periodic"):
+def _air5(name, visc, reaction, pp=0, limit_flow=0, stages=3, dt=2e-9, bc="periodic", plt=0):
     return dict(family="air5", name=name, scheme=52, rec=2, visc=visc, bc=bc, stages=stages, dt=dt,
-                seed=91, pp=pp, limit_flow=limit_flow, reaction=reaction)
+                seed=91, pp=pp, limit_flow=limit_flow, reaction=reaction, plt=plt)
 
 
-def _chan(name, scheme, rec, visc, stages=3, dt=2e-3, bc="channel"):
+def _chan(name, scheme, rec, visc, stages=3, dt=2e-3, bc="channel", plt=0):
     return dict(family="chan", name=name, scheme=scheme, rec=rec, visc=visc, bc=bc, stages=stages, dt=dt,
-                seed=9, pp=0, limit_flow=0, reaction=0)
+                seed=9, pp=0, limit_flow=0, reaction=0, plt=plt)
 
 
 AIR_SCHEMES = [("weno5ch", 52, 2, 0), ("weno7ch", 72, 2, 0), ("weno5cp", 51, 2, 0), ("weno7cp", 71, 2, 0),
@@ -100,10 +100,10 @@ CASES = ([_air(n + "_" + bc, s, r, v, bc) for n, s, r, v in AIR_SCHEMES for bc i
           _air5("air5_weno5ch_visc2_outflow", 2, 1, bc="outflow"), _air5("air5_weno5ch_visc8_chem", 8, 1)] +
          [_chan("chan_hllc_muscl_visc2", 4, 2, 2), _chan("chan_weno5ch_visc2", 52, 2, 2),
           _chan("chan_roe_muscl", 2, 2, 0), _chan("chan_farfield_weno5ch", 52, 2, 0, bc="farfield"),
-          _chan("chan_farfield_hllc_visc2", 4, 2, 2, bc="farfield"), _chan("chan_nr_weno5ch", 52, 2, 0, bc="nr"),
+          _chan("chan_farfield_hllc_visc2", 4, 2, 2, bc="farfield"), _chan("chan_nr_weno5ch", 52, 2, 0, bc="nr", plt=1),
           _chan("chan_nr_ausm_muscl", 3, 2, 0, bc="nr"), _mix("mix_nr_weno5ch", 52, 2, 0, 0, bc="nr"),
-          _mix("mix_catwall_weno5ch", 52, 2, 0, 0, bc="catwall"),
-          _air5("air5_catwall_weno5ch", 0, 1, bc="catwall")] +
+          _mix("mix_catwall_weno5ch", 52, 2, 0, 0, bc="catwall", plt=1),
+          _air5("air5_catwall_weno5ch", 0, 1, bc="catwall", plt=1)] +
          [dict(family="sod", name="sod_1000x7", scheme=52, rec=2, visc=0, bc="outflow", stages=0, dt=0.0, seed=0,
                pp=0, limit_flow=0, reaction=0, mx=1000, my=7, cfl=0.5, t_end=0.2)])
 
@@ -398,6 +398,8 @@ def write_reference_case(case, case_dir, ref_dir):
     task = {"mode": "steps" if fam == "sod" else "stages", "stages": case["stages"], "dt": case["dt"],
             "fixed_dt": 0 if fam == "sod" else 1, "mul_constant": 1e-3 if fam in ("air", "chan") else 0.0,
             "load_metric": 1}
+    if case.get("plt"):
+        task["write_plt"] = 1  # the reference's own flowfield file of the final state
     if fam == "sod":
         task.update(n_steps=100000, t_end=case["t_end"])
     with open(os.path.join(case_dir, "task.txt"), "w") as f:
@@ -550,6 +552,8 @@ def write_reference_multi(case, case_dir, ref_dir):
                 f.write(np.ascontiguousarray(a, dtype=np.float64).tobytes())
     task = {"mode": "stages", "stages": case["stages"], "dt": case["dt"], "fixed_dt": 1, "mul_constant": 0.0,
             "load_metric": 1}
+    if case.get("plt"):
+        task["write_plt"] = 1  # the reference's own flowfield file of the final state
     with open(os.path.join(case_dir, "task.txt"), "w") as f:
         f.write("".join(("%s %s\n" if isinstance(v, str) else "%s %r\n") % (k, v) for k, v in task.items()))
     return multi_state_digest(blocks)
