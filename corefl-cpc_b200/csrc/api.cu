@@ -374,7 +374,9 @@ bool two_temperature_step(const cb2_ctx *ctx) {
 unsigned two_temperature_rhs_terms(const cb2_ctx *ctx) {
   unsigned m = CB2_RHS_CHEMISTRY;
   if (ctx->p.viscous_order == 2 || ctx->p.viscous_order == 8 || ctx->p.viscous_order == 0) m |= CB2_RHS_VISCOUS;
-  if (ctx->p.inviscid_scheme == CB2_INV_WENO5_CH || ctx->p.inviscid_scheme == CB2_INV_WENO7_CH) m |= CB2_RHS_INVISCID;
+  if (ctx->p.inviscid_scheme == CB2_INV_WENO5_CH || ctx->p.inviscid_scheme == CB2_INV_WENO7_CH ||
+      ctx->p.inviscid_scheme == CB2_INV_AUSMP || ctx->p.inviscid_scheme == CB2_INV_HLLC)
+    m |= CB2_RHS_INVISCID;
   return m;
 }
 
@@ -453,6 +455,9 @@ int cb2_init(const cb2_param_view *pv, cb2_ctx **out) {
                        sch == CB2_INV_WENO7_CP;
   const bool pvpath = sch == CB2_INV_AUSMP || sch == CB2_INV_HLLC || sch == CB2_INV_ROE || (sch == 1 && ns == 0);
   if (!weno_ch && !pvpath) return CB2_ERR_UNSUPPORTED;
+  // two temperatures: AUSM+ and HLLC are the primitive-variable fluxes of the reference's
+  // two-temperature build
+  if (tt && pvpath && sch != CB2_INV_AUSMP && sch != CB2_INV_HLLC) return CB2_ERR_UNSUPPORTED;
   if (pvpath) {
     const int r = pv->reconstruction;
     if (!(r == 1 || r == 2 || r == 3 || r == 5 || r == 7)) return CB2_ERR_INVALID;

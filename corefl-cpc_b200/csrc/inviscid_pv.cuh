@@ -19,6 +19,7 @@
 #include <algorithm>
 #include "common.cuh"
 #include "thermo.cuh"
+#include "thermo_2t.cuh"
 #include "weno.cuh"
 #include "sweep.cuh"
 #include "stencil8.cuh"
@@ -101,12 +102,29 @@ __device__ __forceinline__ void reconstruct_node(const T *sN, int NN, int c, int
 #undef PV
 }
 
-// Total energy (index NV) and gamma (index NV+1) of a reconstructed state.
-template <int NS, typename T>
+// Total energy (index NV) and gamma (index NV+1) of a reconstructed state.  NS counts the
+// scalars; with TT (two temperatures) the last one is e_ve: the energy is
+// rho (e_k + e_tr(T) + max(e_ve, 0)) and gamma the translational-rotational one
+// (src/InviscidScheme.cu:184-211).
+template <int NS, typename T, bool TT = false>
 __device__ __forceinline__ void state_energy(T *pv, const Mech &m) {
   constexpr int NV = 5 + NS;
   const T ek = T(0.5) * (pv[1] * pv[1] + pv[2] * pv[2] + pv[3] * pv[3]);
-  if constexpr (NS == 0) {
+  if constexpr (TT) {
+    constexpr int NSP = NS - 1;  // species
+    double y[NSP], r = 0;
+#pragma unroll
+    for (int s = 0; s < NSP; ++s) {
+      y[s] = double(pv[5 + s]);
+      r += y[s] * __ldg(m.gas_const + s);
+    }
+    const double t = double(pv[4]) / fmax(double(pv[0]) * r, 1e-12);
+    double gam, c, etr;
+    characteristic_thermo_2t<NSP>(t, y, m, gam, c, nullptr, nullptr, &etr);
+    const double eve = fmax(double(pv[5 + NSP]), 0.0);
+    pv[NV] = T(double(pv[0]) * (double(ek) + etr + eve));
+    pv[NV + 1] = T(gam);
+  } else if constexpr (NS == 0) {
     pv[NV] = ek * pv[0] + mul_rn(pv[4], T(1.0 / (kGammaAir - 1)));
     pv[NV + 1] = T(kGammaAir);
   } else if (sizeof(T) == 4 && !m.nasa9) {
@@ -185,7 +203,7 @@ __device__ __forceinline__ void ausm_plus(const T *pl, const T *pr, const T *ml,
   for (int l = 5; l < NV; ++l) fc[l] = coeff * pu[l];
 }
 
-template <int NS, typename T>
+template <int NS, typename T, bool TT = false>
 __device__ __forceinline__ void hllc(const T *pl, const T *pr, const T *ml, const T *mr, T jl, T jr,
                                      const Mech &mech, T *fc) {
   constexpr int NV = 5 + NS;
@@ -200,6 +218,19 @@ __device__ __forceinline__ void hllc(const T *pl, const T *pr, const T *ml, cons
     const T ht = hl * rlc + hr * rrc;
     const T ekt = half * (ut * ut + vt * vt + wt * wt);
     ct = sqrt(T(kGammaAir - 1) * (ht - ekt));
+  } else if constexpr (TT) {
+    // two temperatures: the Roe state's translational-rotational sound speed
+    constexpr int NSP = NS - 1;
+    double svm[NSP], r = 0;
+#pragma unroll
+    for (int s = 0; s < NSP; ++s) {
+      svm[s] = double(rlc * pl[5 + s] + rrc * pr[5 + s]);
+      r += svm[s] * __ldg(mech.gas_const + s);
+    }
+    const double t = double(rlc * (pl[4] / pl[0]) + rrc * (pr[4] / pr[0])) / fmax(r, 1e-12);
+    double gam, c64;
+    characteristic_thermo_2t<NSP>(t, svm, mech, gam, c64, nullptr, nullptr);
+    ct = T(c64);
   } else if (sizeof(T) == 4 && !mech.nasa9) {
     // mixed form: the Roe state's sound speed in FP32 (NASA7)
     float svm[NS], r = 0;
@@ -438,7 +469,7 @@ __host__ __device__ constexpr size_t pv_tile_smem(int dir, int ni = kNI) {
 // periodic exchange), and every updated node adds J d8(F) before subtracting its inviscid flux
 // difference.  The WENO7 tile's halo of 3 nodes plus the neighbour node covers the +-4 stencil
 // of every updated node.
-template <typename T, int NS, int DIR, int REC, int SOLVER, int NI = kNI, bool VF = false>
+template <typename T, int NS, int DIR, int REC, int SOLVER, int NI = kNI, bool VF = false, bool TT = false>
 __device__ __forceinline__ void pv_tile_body(const Zone &z, const Param &p, idx_t run, int bx, int by, int bz,
                                              T *sN, T *sR, T *sF) {
   static_assert(!VF || (REC == 7 && NS == 0 && sizeof(T) == 4),
@@ -551,8 +582,8 @@ __device__ __forceinline__ void pv_tile_body(const Zone &z, const Param &p, idx_
   if (rec) {
     T pr[NV + 2];
     reconstruct_node<NS, REC>(sN, NN, c, st, p, pl, pr);
-    state_energy<NS>(pl, p.mech);
-    state_energy<NS>(pr, p.mech);
+    state_energy<NS, T, TT>(pl, p.mech);
+    state_energy<NS, T, TT>(pr, p.mech);
 #pragma unroll
     for (int v = 0; v < NV + 2; ++v) sR[v * kSweepThreads + tid] = pr[v];
   }
@@ -568,7 +599,7 @@ __device__ __forceinline__ void pv_tile_body(const Zone &z, const Param &p, idx_
     const T jl = sN[(NV + 3) * NN + c], jr = sN[(NV + 3) * NN + c + st];
     T fc[NV];
     if constexpr (SOLVER == CB2_INV_AUSMP) ausm_plus<NS>(pl, pr, ml, mr, jl, jr, fc);
-    else if constexpr (SOLVER == CB2_INV_HLLC) hllc<NS>(pl, pr, ml, mr, jl, jr, p.mech, fc);
+    else if constexpr (SOLVER == CB2_INV_HLLC) hllc<NS, T, TT>(pl, pr, ml, mr, jl, jr, p.mech, fc);
     else if constexpr (SOLVER == CB2_INV_ROE)
       roe_flux<NS>(pl, pr, ml, mr, jl, jr, sN[(NV + 4) * NN + c], sN[(NV + 4) * NN + c + st], p, fc);
     else lax_friedrichs_air(pl, pr, ml, mr, jl, jr, fc);
@@ -618,7 +649,7 @@ __device__ __forceinline__ void pv_tile_body(const Zone &z, const Param &p, idx_
 }
 
 // One whole tile with pv_tile_smem bytes at pv_smem.
-template <typename T, int NS, int DIR, int REC, int SOLVER, int NI = kNI, bool VF = false>
+template <typename T, int NS, int DIR, int REC, int SOLVER, int NI = kNI, bool VF = false, bool TT = false>
 __device__ __forceinline__ void pv_tile(const Zone &z, const Param &p, idx_t run, int bx, int by, int bz,
                                         unsigned char *pv_smem) {
   constexpr int NV = 5 + NS;
@@ -628,13 +659,13 @@ __device__ __forceinline__ void pv_tile(const Zone &z, const Param &p, idx_t run
   T *sN = reinterpret_cast<T *>(pv_smem);
   T *sR = sN + NSLOT * NN;
   T *sF = sR + (NV + 2) * kSweepThreads;
-  pv_tile_body<T, NS, DIR, REC, SOLVER, NI, VF>(z, p, run, bx, by, bz, sN, sR, sF);
+  pv_tile_body<T, NS, DIR, REC, SOLVER, NI, VF, TT>(z, p, run, bx, by, bz, sN, sR, sF);
 }
 
-template <typename T, int NS, int DIR, int REC, int SOLVER, int NI = kNI, bool VF = false>
+template <typename T, int NS, int DIR, int REC, int SOLVER, int NI = kNI, bool VF = false, bool TT = false>
 __global__ void __launch_bounds__(kSweepThreads) k_inviscid_pv(Zone z, Param p, idx_t run) {
   extern __shared__ __align__(16) unsigned char pv_smem[];
-  pv_tile<T, NS, DIR, REC, SOLVER, NI, VF>(z, p, run, blockIdx.x, blockIdx.y, blockIdx.z, pv_smem);
+  pv_tile<T, NS, DIR, REC, SOLVER, NI, VF, TT>(z, p, run, blockIdx.x, blockIdx.y, blockIdx.z, pv_smem);
 }
 
 // The mixed form's mixture sweeps, held to 128 registers (two CTAs per SM): with the FP32 state
@@ -645,10 +676,10 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_inviscid_pv_mb2(Zone z, Pa
   pv_tile<T, NS, DIR, REC, SOLVER, NI, VF>(z, p, run, blockIdx.x, blockIdx.y, blockIdx.z, pv_smem);
 }
 
-template <typename T, int NS, int DIR, int REC, int SOLVER, int NI, bool VF>
+template <typename T, int NS, int DIR, int REC, int SOLVER, int NI, bool VF, bool TT = false>
 constexpr auto pv_kernel() {
   if constexpr (sizeof(T) == 4 && NS > 0) return k_inviscid_pv_mb2<T, NS, DIR, REC, SOLVER, NI, VF>;
-  else return k_inviscid_pv<T, NS, DIR, REC, SOLVER, NI, VF>;
+  else return k_inviscid_pv<T, NS, DIR, REC, SOLVER, NI, VF, TT>;
 }
 
 // Entropy-fix delta of the Roe scheme on [-1, m] in every direction (ghost width 1), FP64.
@@ -674,12 +705,12 @@ __global__ void k_entropy_fix_delta(Zone z, Param p) {
   z.efd[z.L1.at(i, j, k)] = d;
 }
 
-template <typename T, int NS, int DIR, int REC, int SOLVER, int NI, bool VF = false>
+template <typename T, int NS, int DIR, int REC, int SOLVER, int NI, bool VF = false, bool TT = false>
 static int launch_pv_yz(const Zone &z, const Param &p, cudaStream_t s) {
   SweepGeom geo;
   const dim3 grid = node_sweep_grid(DIR, z.L, geo, NI);
   const size_t smem = pv_tile_smem<T, NS, REC, SOLVER, VF>(DIR, NI);
-  auto kern = pv_kernel<T, NS, DIR, REC, SOLVER, NI, VF>();
+  auto kern = pv_kernel<T, NS, DIR, REC, SOLVER, NI, VF, TT>();
   CB2_TRY(prepare_smem(kern, smem));
   kern<<<grid, kSweepThreads, smem, s>>>(z, p, 0);
   return check_launch();
@@ -687,32 +718,33 @@ static int launch_pv_yz(const Zone &z, const Param &p, cudaStream_t s) {
 
 // y/z sweep with the block's tile width: the autotuned widths exist for the WENO5/7 air sweeps
 // (the bench's kernels); every other combination uses kNI.
-template <typename T, int NS, int DIR, int REC, int SOLVER, bool VF = false>
+template <typename T, int NS, int DIR, int REC, int SOLVER, bool VF = false, bool TT = false>
 static int launch_pv_yz_ni(const Zone &z, const Param &p, cudaStream_t s) {
   if constexpr ((REC == 5 || REC == 7) && NS == 0) {
     const int ni = z.tile_ni[DIR];
     if (ni == 4) return launch_pv_yz<T, NS, DIR, REC, SOLVER, 4, VF>(z, p, s);
     if (ni == 16) return launch_pv_yz<T, NS, DIR, REC, SOLVER, 16, VF>(z, p, s);
   }
-  return launch_pv_yz<T, NS, DIR, REC, SOLVER, kNI, VF>(z, p, s);
+  return launch_pv_yz<T, NS, DIR, REC, SOLVER, kNI, VF, TT>(z, p, s);
 }
 
-template <typename T, int NS, int REC, int SOLVER, bool VF>
+template <typename T, int NS, int REC, int SOLVER, bool VF, bool TT = false>
 static int launch_pv_dir(int d, const Zone &z, const Param &p, cudaStream_t s) {
   if (d == 0) {
     SweepGeom geo;
     const dim3 grid = node_sweep_grid(0, z.L, geo);
     const size_t smem = pv_tile_smem<T, NS, REC, SOLVER, VF>(0);
-    auto kern = pv_kernel<T, NS, 0, REC, SOLVER, kNI, VF>();
+    auto kern = pv_kernel<T, NS, 0, REC, SOLVER, kNI, VF, TT>();
     CB2_TRY(prepare_smem(kern, smem));
     kern<<<grid, kSweepThreads, smem, s>>>(z, p, geo.run);
     return check_launch();
   }
-  if (d == 1) return launch_pv_yz_ni<T, NS, 1, REC, SOLVER, VF>(z, p, s);
-  return launch_pv_yz_ni<T, NS, 2, REC, SOLVER, VF>(z, p, s);
+  if (d == 1) return launch_pv_yz_ni<T, NS, 1, REC, SOLVER, VF, TT>(z, p, s);
+  return launch_pv_yz_ni<T, NS, 2, REC, SOLVER, VF, TT>(z, p, s);
 }
 
-template <typename T, int NS, int REC, int SOLVER>
+// NS counts the scalars of sv; TT: two temperatures (the last scalar is e_ve)
+template <typename T, int NS, int REC, int SOLVER, bool TT = false>
 static int launch_pv_dirs(const Zone &z, const Param &p, cudaStream_t s, int &nl) {
   if (SOLVER == CB2_INV_ROE) {
     dim3 grid((z.mx + 2 + 127) / 128, z.my + 2, z.mz + 2);
@@ -731,7 +763,7 @@ static int launch_pv_dirs(const Zone &z, const Param &p, cudaStream_t s, int &nl
       else CB2_TRY((launch_pv_dir<T, NS, REC, SOLVER, false>(d, z, p, s)));
     } else {
       if (p.visc8_fused) return CB2_ERR_UNSUPPORTED;
-      CB2_TRY((launch_pv_dir<T, NS, REC, SOLVER, false>(d, z, p, s)));
+      CB2_TRY((launch_pv_dir<T, NS, REC, SOLVER, false, TT>(d, z, p, s)));
     }
     ++nl;
   }

@@ -356,15 +356,18 @@ __device__ __forceinline__ void vt_relax_point(const Zone &z, const Param &p, id
 
 // Roe-state characteristic thermo of the two-temperature model (src/Thermo.cuh:49-110 with
 // two_temperature on): gamma and c of the translational-rotational mode, h_tr = h - e_ve(T),
-// cp_tr = cp - cv_ve(T); the species rows alpha_s and energy coefficients as in one temperature,
-// and the e_ve scalar's row alpha = -(gamma - 1)/c^2 with energy coefficient 1.
+// cp_tr = cp - cv_ve(T), and (etr not null) the mixture's translational-rotational energy
+// e_tr = sum Y (h_tr - R T); with alpha and ecoef not null, the species rows alpha_s and energy
+// coefficients as in one temperature, and the e_ve scalar's row alpha = -(gamma - 1)/c^2 with
+// energy coefficient 1.
 template <int NS>
 __device__ __forceinline__ void characteristic_thermo_2t(double t, const double *y, const Mech &m, double &gamma,
-                                                         double &c, double *alpha, double *ecoef) {
+                                                         double &c, double *alpha, double *ecoef,
+                                                         double *etr = nullptr) {
   const double te = fmax(t, 1.0);
   double h[NS], cp[NS], htr[NS];
   species_h_cp<NS>(te, m, h, cp);
-  double r = 0, cpm = 0, cvm = 0;
+  double r = 0, cpm = 0, cvm = 0, e_tr = 0;
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
     double cv_ve;
@@ -372,12 +375,15 @@ __device__ __forceinline__ void characteristic_thermo_2t(double t, const double 
     const double rs = __ldg(m.gas_const + s);
     htr[s] = h[s] - e_ve;
     const double cp_tr = cp[s] - cv_ve;
+    e_tr += y[s] * (htr[s] - rs * te);
     r += y[s] * rs;
     cpm += y[s] * cp_tr;
     cvm += y[s] * (cp_tr - rs);
   }
   gamma = cpm / fmax(cvm, 1e-8);
   c = sqrt(fmax(gamma * r * te, 1e-12));
+  if (etr) *etr = e_tr;
+  if (!alpha || !ecoef) return;
   const double gm1 = gamma - 1.0;
   const double c2 = fmax(c * c, 1e-30);
   const double inv_gm1 = 1.0 / fmax(gm1, 1e-12);

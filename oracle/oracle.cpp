@@ -641,8 +641,14 @@ void reconstruct(const Param &p, double pv[][8], int r, double *pl, double *pr) 
       for (int l = 0; l < p.n_spec; ++l) rg += s[5 + l] * p.mech.gas_const[l];
       const double t = s[4] / std::max(s[0] * rg, 1e-12);
       double g, c, etr;
-      characteristic_thermo(t, s + 5, p.mech, &g, &c, nullptr, nullptr, &etr);
-      s[nv] = s[0] * (ek + etr);
+      if (p.i_eve >= 0) {
+        // two temperatures: translational-rotational energy and gamma, plus e_ve (:197-211)
+        characteristic_thermo_2t(p, t, s + 5, &g, &c, nullptr, nullptr, &etr);
+        s[nv] = s[0] * (ek + etr + std::max(s[5 + p.i_eve], 0.0));
+      } else {
+        characteristic_thermo(t, s + 5, p.mech, &g, &c, nullptr, nullptr, &etr);
+        s[nv] = s[0] * (ek + etr);
+      }
       s[nv + 1] = g;
     }
   }
@@ -708,7 +714,8 @@ void hllc(const Param &p, const double *pl, const double *pr, const double *ml, 
     for (int l = 0; l < p.n_spec; ++l) rg += svm[l] * p.mech.gas_const[l];
     const double t = (rl_c * (pl[4] / pl[0]) + rr_c * (pr[4] / pr[0])) / std::max(rg, 1e-12);
     double g;
-    characteristic_thermo(t, svm, p.mech, &g, &c_tilde, nullptr, nullptr, nullptr);
+    if (p.i_eve >= 0) characteristic_thermo_2t(p, t, svm, &g, &c_tilde, nullptr, nullptr);
+    else characteristic_thermo(t, svm, p.mech, &g, &c_tilde, nullptr, nullptr, nullptr);
   }
   const double kx = 0.5 * (ml[0] + mr[0]), ky = 0.5 * (ml[1] + mr[1]), kz = 0.5 * (ml[2] + mr[2]);
   const double gK = std::sqrt(kx * kx + ky * ky + kz * kz);

@@ -135,7 +135,7 @@ double ve_energy(const Param &p, int i, double t);
 double ve_cv(const Param &p, int i, double t);
 double mixture_ve_energy(const Param &p, double t, const double *y, double *cv_ve);
 void characteristic_thermo_2t(const Param &p, double t, const double *y, double *gamma, double *c, double *alpha,
-                              double *ecoef);
+                              double *ecoef, double *e_tr_out = nullptr);
 // cv_tr, cp_tr and R of the mixture at t (compute_mixture_tr_energy's heat capacities)
 void tr_heat_capacities(const Param &p, double t, const double *y, double &cv_tr, double &cp_tr, double &r_mix);
 double invert_tve_from_eve(const Param &p, double eve_target, const double *y, double t_init);

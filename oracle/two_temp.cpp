@@ -346,14 +346,15 @@ void tr_heat_capacities(const Param &p, double t, const double *y, double &cv_tr
 // two_temperature on): h_tr = h - e_ve(T), cp_tr = cp - cv_ve(T); the e_ve row
 // alpha = -(gamma - 1)/c^2 with energy coefficient 1.
 void characteristic_thermo_2t(const Param &p, double t, const double *y, double *gamma, double *c, double *alpha,
-                              double *ecoef) {
+                              double *ecoef, double *e_tr_out) {
   const double te = std::max(t, 1.0);
   double h[16], cp[16], htr[16];
   nasa7_h_cp(te, p.mech, h, cp);
-  double r = 0, cpm = 0, cvm = 0;
+  double r = 0, cpm = 0, cvm = 0, e_tr = 0;
   for (int l = 0; l < p.n_spec; ++l) {
     htr[l] = h[l] - ve_energy(p, l, te);
     const double cp_tr = cp[l] - ve_cv(p, l, te);
+    e_tr += y[l] * (htr[l] - p.mech.gas_const[l] * te);
     r += y[l] * p.mech.gas_const[l];
     cpm += y[l] * cp_tr;
     cvm += y[l] * (cp_tr - p.mech.gas_const[l]);
@@ -362,6 +363,8 @@ void characteristic_thermo_2t(const Param &p, double t, const double *y, double 
   const double cc = std::sqrt(std::max(g * r * te, 1e-12));
   *gamma = g;
   *c = cc;
+  if (e_tr_out) *e_tr_out = e_tr;
+  if (!alpha || !ecoef) return;
   const double gm1 = g - 1.0;
   const double c2 = std::max(cc * cc, 1e-30);
   const double inv_gm1 = 1.0 / std::max(gm1, 1e-12);

@@ -76,8 +76,8 @@ def _mix(name, scheme, rec, visc, reaction, pp=0, stages=3, dt=2e-9, bc="periodi
                 seed=2024, pp=pp, limit_flow=0, reaction=reaction, plt=plt)
 
 
-def _air5(name, visc, reaction, pp=0, limit_flow=0, stages=3, dt=2e-9, bc="periodic", plt=0):
-    return dict(family="air5", name=name, scheme=52, rec=2, visc=visc, bc=bc, stages=stages, dt=dt,
+def _air5(name, visc, reaction, pp=0, limit_flow=0, stages=3, dt=2e-9, bc="periodic", plt=0, scheme=52, rec=2):
+    return dict(family="air5", name=name, scheme=scheme, rec=rec, visc=visc, bc=bc, stages=stages, dt=dt,
                 seed=91, pp=pp, limit_flow=limit_flow, reaction=reaction, plt=plt)
 
 
@@ -103,7 +103,8 @@ CASES = ([_air(n + "_" + bc, s, r, v, bc) for n, s, r, v in AIR_SCHEMES for bc i
           _chan("chan_farfield_hllc_visc2", 4, 2, 2, bc="farfield"), _chan("chan_nr_weno5ch", 52, 2, 0, bc="nr", plt=1),
           _chan("chan_nr_ausm_muscl", 3, 2, 0, bc="nr"), _mix("mix_nr_weno5ch", 52, 2, 0, 0, bc="nr"),
           _mix("mix_catwall_weno5ch", 52, 2, 0, 0, bc="catwall", plt=1),
-          _air5("air5_catwall_weno5ch", 0, 1, bc="catwall", plt=1)] +
+          _air5("air5_catwall_weno5ch", 0, 1, bc="catwall", plt=1),
+          _air5("air5_hllc_muscl_visc2_chem", 2, 1, scheme=4), _air5("air5_ausm_muscl_chem", 0, 1, scheme=3)] +
          [dict(family="sod", name="sod_1000x7", scheme=52, rec=2, visc=0, bc="outflow", stages=0, dt=0.0, seed=0,
                pp=0, limit_flow=0, reaction=0, mx=1000, my=7, cfl=0.5, t_end=0.2)])
 

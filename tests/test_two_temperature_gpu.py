@@ -93,14 +93,21 @@ def test_vt_relaxation_parity(oracle_lib, h2, tt):
     assert np.abs(_inner(b.a["temperature_ve"], g) - _inner(before, g)).max() > 1.0
 
 
-def test_two_temperature_context_refuses_unbuilt_paths(oracle_lib, h2, tt):
-    """The two-temperature primitive-variable (HLLC) flux is not built: the residual with it and the
-    whole step refuse the context; the chemistry-only residual and the periodic ghost fill run."""
+def test_two_temperature_box_hllc_residual_and_roe_refused(oracle_lib, h2, tt):
+    """The H2/air box's two-temperature residual with its WENO5 + HLLC primitive-variable flux
+    (e_ve carried as a scalar, the translational-rotational energy and gamma of the states) matches
+    the oracle; the Roe flux, which the reference's two-temperature build does not have, is
+    refused."""
     p, b, faces, dev, ctx = _setup(oracle_lib, h2, tt)
-    ctx.boundary(0)
-    for call in (lambda: ctx.rhs(0), lambda: ctx.rhs(0, abi.RHS_INVISCID),
-                 lambda: ctx.rk3_step(1e-9, fixed_dt=True)):
-        with pytest.raises(cb200.CB2Error) as e:
-            call()
-        assert e.value.code == abi.ERR_UNSUPPORTED
-    ctx.rhs(0, abi.RHS_CHEMISTRY)
+    oracle_lib.properties(p, b)
+    dev.load(b)
+    ctx.rhs(0, abi.RHS_INVISCID)
+    _sync()
+    dq = dev.to_host(["dq"])["dq"]
+    oracle_lib.rhs(p, b, faces, abi.RHS_INVISCID)
+    assert helpers.rel_err(dq, b.a["dq"]) < TOL
+    ctx.close()
+    p.inviscid_scheme = abi.INV_ROE
+    with pytest.raises(cb200.CB2Error) as e:
+        cb200.Context(p)
+    assert e.value.code == abi.ERR_UNSUPPORTED
