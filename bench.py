@@ -50,6 +50,13 @@ KERNEL_BYTES_PER_NODE_MIXED = dict(KERNEL_BYTES_PER_NODE, **{
     "pv_flux_z": 4 * (5 + 3 + 1) + 8 * 10,
     "visc8_node_flux": 4 * (4 + 9 + 12) + 8, "visc8_divergence": 4 * (12 + 1) + 8 * 5,
 })
+# Executed FP64 operations per interior node (an FMA counted as 2) of the FP64 sweeps, from ncu's
+# sm__sass_thread_inst_executed_op_d{fma,mul,add}_pred_on on the 129^3 sine wave, per node of one
+# launch; these kernels are bound by the FP64 pipe, not by HBM.  The FP64 peak is the B200's
+# nominal (no measured FP64 figure is available).
+KERNEL_FP64_FLOPS_PER_NODE = {"pv_flux_x": 1500, "pv_flux_y": 1500, "pv_flux_z": 1500}
+FP64_NOMINAL_TFLOPS = 37.0
+FLOPS_PER_CELL_UPDATE = 15000  # 3 stages x (3 sweeps x 1,500 + node fluxes 406 + divergence 144)
 # per padded node (kernels that sweep the ghost layers too)
 KERNEL_BYTES_PER_PADDED_NODE = {"bv_to_f32": 6 * (8 + 4), "store_qn": 5 * 16, "properties": 8 * (4 + 2)}
 
@@ -418,6 +425,13 @@ def gpu_arm(args, rank, world, local_rank):
                 "traffic": (traffic * nodes if traffic else None),
                 "algorithmic_bytes": bpn * nodes, "avg_launch_ms": avg_ms,
                 "share": kms / total}
+        fpn = KERNEL_FP64_FLOPS_PER_NODE.get(kname)
+        if fpn:
+            # the roof that binds this kernel: the FP64 pipe
+            tf = fpn * nodes / (avg_ms * 1e-3) / 1e12
+            roof["compute"] = {"pipe": "fp64", "achieved": tf, "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+                               "frac": tf / FP64_NOMINAL_TFLOPS, "peak_source": "nominal",
+                               "flops_per_node": fpn, "flops_per_cell_update": FLOPS_PER_CELL_UPDATE}
     padded = (args.n + 1 + 8) ** 3
     kernel_roofs = kernel_rooflines(prof, nodes, padded, KERNEL_BYTES_PER_NODE, peak)
 
