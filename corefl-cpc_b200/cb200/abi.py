@@ -14,6 +14,7 @@ BC_FARFIELD = 4
 BC_NONREFLECTING = 0x100  # OR'd into BC_OUTFLOW: non-reflecting outflow
 PREC_FP64, PREC_MIXED = 0, 1
 RHS_VISCOUS, RHS_CHEMISTRY, RHS_INVISCID, RHS_ALL = 1, 2, 4, 7
+RHS_ACCUMULATE = 8  # add to the caller's dq
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)

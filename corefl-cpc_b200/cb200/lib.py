@@ -38,6 +38,7 @@ def load():
         "cb2_destroy": (None, [vp]),
         "cb2_store_qn": (C.c_int, [vp, C.c_int, vp]),
         "cb2_rhs": (C.c_int, [vp, C.c_int, C.c_uint, vp]),
+        "cb2_viscous": (C.c_int, [vp, vp]),
         "cb2_shock_sensor": (C.c_int, [vp, C.c_int, vp]),
         "cb2_stage_update": (C.c_int, [vp, C.c_int, C.c_double, C.c_int, vp]),
         "cb2_boundary": (C.c_int, [vp, C.c_int, vp]),
@@ -117,6 +118,10 @@ class Context:
 
     def rhs(self, blk, mask=abi.RHS_ALL, stream=None):
         check(self.lib.cb2_rhs(self.h, blk, mask, stream), "cb2_rhs")
+
+    def viscous(self, stream=None):
+        """cb2_viscous: the viscous term of every bound block (node fluxes exchanged across inner faces)."""
+        check(self.lib.cb2_viscous(self.h, stream), "cb2_viscous")
 
     def shock_sensor(self, blk, stream=None):
         check(self.lib.cb2_shock_sensor(self.h, blk, stream), "cb2_shock_sensor")

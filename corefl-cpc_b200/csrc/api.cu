@@ -755,10 +755,11 @@ int cb2_store_qn(cb2_ctx *ctx, int blk, void *stream) {
 int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream) {
   Block *B = get_block(ctx, blk);
   if (!B) return CB2_ERR_INVALID;
-  if (two_temperature(ctx) && (mask & ~two_temperature_rhs_terms(ctx))) return CB2_ERR_UNSUPPORTED;
-  // the 8th-order node fluxes of a multi-block grid would need their exchange across the inner
-  // faces (exchange_value task 1, src/DataCommunication.cu:422-463), which is not built
+  if (two_temperature(ctx) && (mask & CB2_RHS_ALL & ~two_temperature_rhs_terms(ctx))) return CB2_ERR_UNSUPPORTED;
+  // the 8th-order node fluxes of a multi-block grid are exchanged across the inner faces between
+  // all blocks' node fluxes and any block's divergence: cb2_viscous does that for every block
   if ((mask & CB2_RHS_VISCOUS) && ctx->p.viscous_order == 8 && !B->inner.empty()) return CB2_ERR_UNSUPPORTED;
+  const bool accumulate = (mask & CB2_RHS_ACCUMULATE) != 0;
   ProfGuard pg(ctx);
   cudaStream_t s = (cudaStream_t)stream;
   const Param &p = ctx->p;
@@ -777,11 +778,13 @@ int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream) {
   // registers) runs fewer CTAs per SM, which cost more than the divergence pass it saves.
   Param pf = p;
   pf.visc8_fused = visc && p.viscous_order == 8 && p.n_spec == 0 && (mask & CB2_RHS_INVISCID) && pv &&
-                           p.reconstruction == CB2_REC_WENO7 && !B->z.sweep_mask && p.precision == CB2_PREC_MIXED
+                           p.reconstruction == CB2_REC_WENO7 && !B->z.sweep_mask && p.precision == CB2_PREC_MIXED &&
+                           !accumulate
                        ? 2
                        : 0;
-  const bool assign = pf.visc8_fused || (visc && viscous_assigns_dq(p));  // no zeroing of dq
-  if (!assign) {
+  // no zeroing of dq when the first term assigns it, or when the caller's dq is added to
+  const bool assign = !accumulate && (pf.visc8_fused || (visc && viscous_assigns_dq(p)));
+  if (!assign && !accumulate) {
     ProfScope prof("zero_dq", s);
     CB2_TRY(check_cuda(cudaMemsetAsync(B->z.dq, 0, (size_t)B->z.L0.sz * p.n_var * sizeof(double), s)));
   }
@@ -796,6 +799,54 @@ int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream) {
       CB2_TRY(launch_inviscid_pv(B->z, pf, s, nl));
     // the non-reflecting outflow faces correct dq after the inviscid flux (src/RK.cuh:190-193)
     CB2_TRY(launch_nonreflecting(B->z, p, B->faces.data(), (int)B->faces.size(), s, nl));
+  }
+  return count(ctx, nl);
+}
+
+static bool inner_face_in_range(const Zone &z, const Zone &zt, const cb2_inner_face &f);
+
+int cb2_viscous(cb2_ctx *ctx, void *stream) {
+  if (!ctx || ctx->blocks.empty()) return CB2_ERR_INVALID;
+  if (two_temperature(ctx) && !(two_temperature_rhs_terms(ctx) & CB2_RHS_VISCOUS)) return CB2_ERR_UNSUPPORTED;
+  ProfGuard pg(ctx);
+  cudaStream_t s = (cudaStream_t)stream;
+  const Param &p = ctx->p;
+  Param pf = p;
+  pf.visc8_fused = 0;
+  const bool assign = p.viscous_order > 0 && viscous_assigns_dq(p);
+  const int nb = (int)ctx->blocks.size();
+  int nl = 0;
+  // every block's dq and (order 8) node fluxes
+  for (int b = 0; b < nb; ++b) {
+    Block &B = ctx->blocks[b];
+    if (!B.bound) continue;
+    if (p.precision == CB2_PREC_MIXED) {
+      ProfScope prof("bv_to_f32", s);
+      CB2_TRY(launch_to_f32(B.z.bv, B.z.bv32, 6 * (size_t)B.z.L.sz, s, nl));
+    }
+    if (!assign) {
+      ProfScope prof("zero_dq", s);
+      CB2_TRY(check_cuda(cudaMemsetAsync(B.z.dq, 0, (size_t)B.z.L0.sz * p.n_var * sizeof(double), s)));
+    }
+    if (p.viscous_order > 0)
+      CB2_TRY(launch_viscous(B.z, pf, B.faces.data(), (int)B.faces.size(), assign, s, nl, p.viscous_order == 8 ? 1 : 0));
+  }
+  if (p.viscous_order == 8) {
+    // the node fluxes across the inner faces, then each block's periodic exchange and divergence
+    // (exchange_value: inner faces before periodic ones, src/DataCommunication.cu:437-485)
+    for (int b = 0; b < nb; ++b) {
+      Block &B = ctx->blocks[b];
+      if (!B.bound) continue;
+      for (const cb2_inner_face &f : B.inner) {
+        Block *T = get_block(ctx, f.target_block);
+        if (!T || !inner_face_in_range(B.z, T->z, f)) return CB2_ERR_INVALID;
+        CB2_TRY(launch_inner_flux_exchange(B.z, T->z, p, f, s, nl));
+      }
+    }
+    for (int b = 0; b < nb; ++b) {
+      Block &B = ctx->blocks[b];
+      if (B.bound) CB2_TRY(launch_viscous(B.z, pf, B.faces.data(), (int)B.faces.size(), assign, s, nl, 2));
+    }
   }
   return count(ctx, nl);
 }
@@ -1077,12 +1128,18 @@ static int enqueue_stages(cb2_ctx *ctx, double dt, void *stream) {
   const int nbr = nbound > 1 ? std::min(nbound, kMaxBranches) : 0;
   if (nbr) CB2_TRY(ensure_branches(ctx, nbr));
   auto on = [&](int slot) { return nbr ? (void *)ctx->branch[slot % nbr] : stream; };
+  // 8th-order viscous terms across inner faces: every block's viscous term first (cb2_viscous,
+  // as the reference's compute_viscous_flux runs over the whole mesh), then the rest of each
+  // block's residual added to it
+  const bool visc_all = halo && ctx->p.viscous_order == 8;
+  const unsigned mask = visc_all ? (CB2_RHS_CHEMISTRY | CB2_RHS_INVISCID | CB2_RHS_ACCUMULATE) : CB2_RHS_ALL;
   for (int rk = 0; rk < 3; ++rk) {
+    if (visc_all) CB2_TRY(cb2_viscous(ctx, stream));
     if (nbr) CB2_TRY(fork_branches(ctx, s, nbr));
     for (int b = 0, slot = 0; b < nb; ++b) {
       if (!ctx->blocks[b].bound) continue;
       void *sb = on(slot++);
-      CB2_TRY(cb2_rhs(ctx, b, CB2_RHS_ALL, sb));
+      CB2_TRY(cb2_rhs(ctx, b, mask, sb));
       CB2_TRY(cb2_stage_update(ctx, b, dt, rk, sb));
       CB2_TRY(cb2_boundary(ctx, b, sb));
     }

@@ -543,6 +543,65 @@ int launch_inner_exchange(const Zone &z, const Zone &zt, const Param &p, const c
   return check_launch();
 }
 
+// The 8th-order node fluxes across one inner face (exchange_value task 1 -> inner_exchange,
+// src/DataCommunication.cu:437-527): on the coincident face layer the two blocks' fluxes are
+// averaged into both, every component of fFlux, gFlux and hFlux; on the ghost layers this block
+// takes the neighbour's.  E: double, or float for the mixed form's FP32 node fluxes.
+template <typename E>
+__global__ void k_inner_flux_exchange(Zone z, Zone zt, int n_var, cb2_inner_face f) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n01 = (long long)f.n_point[0] * f.n_point[1];
+  if (t >= n01 * f.n_point[2]) return;
+  int n[3];
+  n[0] = (int)(t % f.n_point[0]);
+  n[1] = (int)((t / f.n_point[0]) % f.n_point[1]);
+  n[2] = (int)(t / n01);
+  int idx[3], it[3], d_idx[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    d_idx[a] = f.loop_dir[a] * n[a];
+    idx[a] = f.range_start[a] + d_idx[a];
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) it[a] = f.target_start[a] + f.target_loop_dir[a] * d_idx[f.src_tar[a]];
+  const idx_t sz = z.L.sz, szt = zt.L.sz;
+  const idx_t g = z.L.at(idx[0], idx[1], idx[2]), gt = zt.L.at(it[0], it[1], it[2]);
+  E *F[3], *Ft[3];
+  if constexpr (sizeof(E) == 4) {
+    F[0] = z.fF32; F[1] = z.gF32; F[2] = z.hF32;
+    Ft[0] = zt.fF32; Ft[1] = zt.gF32; Ft[2] = zt.hF32;
+  } else {
+    F[0] = z.fF; F[1] = z.gF; F[2] = z.hF;
+    Ft[0] = zt.fF; Ft[1] = zt.gF; Ft[2] = zt.hF;
+  }
+  const int face_layer = f.direction > 0 ? f.range_start[f.face] : f.range_end[f.face];
+  const bool coincident = idx[f.face] == face_layer;
+  for (int l = 0; l < n_var; ++l)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const E that = Ft[a][gt + l * szt];
+      if (coincident) {
+        const E ave = E(0.5) * (F[a][g + l * sz] + that);
+        F[a][g + l * sz] = ave;
+        Ft[a][gt + l * szt] = ave;
+      } else {
+        F[a][g + l * sz] = that;
+      }
+    }
+}
+
+int launch_inner_flux_exchange(const Zone &z, const Zone &zt, const Param &p, const cb2_inner_face &f,
+                               cudaStream_t s, int &nl) {
+  const long long np = (long long)f.n_point[0] * f.n_point[1] * f.n_point[2];
+  if (np <= 0) return CB2_OK;
+  const unsigned blocks = (unsigned)((np + 127) / 128);
+  ProfScope prof("inner_flux_exchange", s);
+  if (visc8_f32(p)) k_inner_flux_exchange<float><<<blocks, 128, 0, s>>>(z, zt, p.n_var, f);
+  else k_inner_flux_exchange<double><<<blocks, 128, 0, s>>>(z, zt, p.n_var, f);
+  ++nl;
+  return check_launch();
+}
+
 // 2-D blocks: copy the k = 0 plane into every k ghost plane (eliminate_k_gradient_point).
 __global__ void k_eliminate_k_gradient(Zone z, Param p) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x - z.ngg;

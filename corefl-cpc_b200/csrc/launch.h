@@ -96,9 +96,14 @@ bool viscous_assigns_dq(const Param &p);
 // node-flux, flux-exchange and divergence kernels all follow it.
 inline bool visc8_f32(const Param &p) { return p.precision == CB2_PREC_MIXED && p.n_spec == 0; }
 // With p.visc8_fused the 8th-order path stops after the node fluxes and their periodic
-// exchange: the WENO7 primitive sweeps take the divergence.
+// exchange: the WENO7 primitive sweeps take the divergence.  phase (order 8 only): 0 the whole
+// viscous term; 1 the node fluxes only; 2 the periodic node-flux exchange and the divergence
+// (between the two, a multi-block step exchanges the node fluxes across inner faces).
 int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, bool assign, cudaStream_t s,
-                   int &n_launch);
+                   int &n_launch, int phase = 0);
+// the 8th-order node fluxes across one inner face of a multi-block grid (exchange_value task 1)
+int launch_inner_flux_exchange(const Zone &z, const Zone &zt, const Param &p, const cb2_inner_face &f,
+                               cudaStream_t s, int &n_launch);
 int launch_chemistry(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
 int launch_shock_sensor(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);
 int launch_local_dt(const Zone &z, const Param &p, cudaStream_t s, int &n_launch);

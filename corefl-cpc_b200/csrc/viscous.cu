@@ -535,9 +535,9 @@ static int launch_visc2_ns(const Zone &z, const Param &p, cudaStream_t s, int &n
 bool viscous_assigns_dq(const Param &p) { return p.viscous_order == 8 && p.n_spec == 0; }
 
 int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_faces, bool assign, cudaStream_t s,
-                   int &nl) {
+                   int &nl, int phase) {
   if (p.viscous_order == 0) return CB2_OK;
-  if (p.viscous_order == 8) {
+  if (p.viscous_order == 8 && phase != 2) {
     const dim3 grid((z.mx + kVisTI - 1) / kVisTI, (z.my + kVisTJ - 1) / kVisTJ, z.mz), block(kVisTI, kVisTJ);
     {
       ProfScope prof("visc8_node_flux", s);
@@ -562,6 +562,9 @@ int launch_viscous(const Zone &z, const Param &p, const FaceBC *faces, int n_fac
     }
     ++nl;
     CB2_TRY(check_launch());
+    if (phase == 1) return CB2_OK;
+  }
+  if (p.viscous_order == 8) {
     CB2_TRY(launch_periodic_flux_exchange(z, p, faces, n_faces, s, nl));
     if (p.visc8_fused) return CB2_OK;  // the sweeps take the divergence
     {

@@ -76,6 +76,9 @@ extern "C" {
 #define CB2_RHS_CHEMISTRY 2u
 #define CB2_RHS_INVISCID 4u
 #define CB2_RHS_ALL 7u
+/* with the terms above: add them to the caller's dq instead of starting from zero (after
+ * cb2_viscous, whose viscous residual the rest of the stage adds to) */
+#define CB2_RHS_ACCUMULATE 8u
 
 /* ---- views ------------------------------------------------------------------------- */
 
@@ -282,6 +285,16 @@ int cb2_rhs(cb2_ctx *ctx, int blk, unsigned mask, void *stream);
  * nodes: replaces compute_shock_sensor (src/FieldOperation.cu:207-228, src/RK.cuh:139-143).
  * With sensor_threshold > 1e-10 the WENO kernels use nonlinear weights only where the
  * sensor exceeds the threshold within the stencil window, and linear weights elsewhere. */
+/* The viscous term of every bound block at once, as the reference's compute_viscous_flux runs over
+ * the whole mesh (src/ViscousScheme.cu:14-100): each block's dq becomes its viscous residual (with
+ * 8th-order terms: every block's node fluxes, then their exchange across the inner faces
+ * (exchange_value task 1, src/DataCommunication.cu:437-527), then each block's periodic node-flux
+ * exchange and divergence).  Then, per block, cb2_rhs with CB2_RHS_CHEMISTRY | CB2_RHS_INVISCID |
+ * CB2_RHS_ACCUMULATE completes the residual.  Needed for 8th-order viscous terms on grids with
+ * inner faces, where cb2_rhs of one block refuses them; cb2_rk3_step and cb2_rk3_run call it
+ * themselves. */
+int cb2_viscous(cb2_ctx *ctx, void *stream);
+
 int cb2_shock_sensor(cb2_ctx *ctx, int blk, void *stream);
 
 /* Shu-Osher stage `rk` (0,1,2) with time step dt, species clipping and primitive recovery:

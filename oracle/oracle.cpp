@@ -967,7 +967,16 @@ double d8(F f, int n, int nx, bool bl, bool br) {
   return df;
 }
 
-void viscous_8th(Zone &z, const Param &p) {
+// phase 0: the whole term; 1: the node fluxes only; 2: their periodic exchange and the divergence
+// (a multi-block grid exchanges the node fluxes across its inner faces in between)
+void viscous_8th_nodes(Zone &z, const Param &p);
+void viscous_8th_divergence(Zone &z, const Param &p);
+void viscous_8th(Zone &z, const Param &p, int phase) {
+  if (phase != 2) viscous_8th_nodes(z, p);
+  if (phase != 1) viscous_8th_divergence(z, p);
+}
+
+void viscous_8th_nodes(Zone &z, const Param &p) {
   // collocated node fluxes (src/ViscousScheme.cu:470-585), then for mixtures the species
   // diffusion, its enthalpy and (two temperatures) the e_ve terms (:587-788)
 #pragma omp parallel for collapse(2) schedule(static)
@@ -1083,6 +1092,9 @@ void viscous_8th(Zone &z, const Param &p) {
         if (tt)
           for (int a = 0; a < 3; ++a) (*F[a])(i, j, k, 5 + p.i_eve) = ef[a];
       }
+}
+
+void viscous_8th_divergence(Zone &z, const Param &p) {
   // periodic exchange of the node fluxes (src/DataCommunication.cu:665-712)
   for (const auto &f : z.faces) {
     if (f.type != CB2_BC_PERIODIC) continue;
@@ -1919,9 +1931,59 @@ void chemistry_source_2t(const Mechanism &m, double rho, double t, double tve, c
   chemistry_point(m, rho, t, tve, y, omega, omega_d);
 }
 
-void compute_viscous_flux(Zone &z, const Param &p) {
-  if (p.viscous_order == 8) viscous_8th(z, p);
-  else if (p.viscous_order == 2) viscous_2nd(z, p);
+void compute_viscous_flux(Zone &z, const Param &p, int phase) {
+  if (p.viscous_order == 8) viscous_8th(z, p, phase);
+  else if (p.viscous_order == 2 && phase != 2) viscous_2nd(z, p);
+}
+
+// exchange_value task 1 over the inner faces (inner_exchange, src/DataCommunication.cu:437-527):
+// the node fluxes averaged on each coincident face layer, copied into the ghost layers
+void inner_flux_exchange(std::vector<Zone> &zones, const Param &p) {
+  for (auto &z : zones)
+    for (const auto &f : z.inner) {
+      Zone &t = zones[f.target_block];
+      const int face_layer = f.direction > 0 ? f.range_start[f.face] : f.range_end[f.face];
+      for (int n2 = 0; n2 < f.n_point[2]; ++n2)
+        for (int n1 = 0; n1 < f.n_point[1]; ++n1)
+          for (int n0 = 0; n0 < f.n_point[0]; ++n0) {
+            const int n[3] = {n0, n1, n2};
+            int idx[3], it[3], d[3];
+            for (int a = 0; a < 3; ++a) {
+              d[a] = f.loop_dir[a] * n[a];
+              idx[a] = f.range_start[a] + d[a];
+            }
+            for (int a = 0; a < 3; ++a) it[a] = f.target_start[a] + f.target_loop_dir[a] * d[f.src_tar[a]];
+            const bool coincident = idx[f.face] == face_layer;
+            for (int l = 0; l < p.n_var; ++l) {
+              const Arr *mine[3] = {&z.fF, &z.gF, &z.hF}, *theirs[3] = {&t.fF, &t.gF, &t.hF};
+              for (int a = 0; a < 3; ++a) {
+                double &x = (*mine[a])(idx[0], idx[1], idx[2], l);
+                double &y = (*theirs[a])(it[0], it[1], it[2], l);
+                if (coincident) {
+                  const double ave = 0.5 * (x + y);
+                  x = ave;
+                  y = ave;
+                } else {
+                  x = y;
+                }
+              }
+            }
+          }
+    }
+}
+
+// compute_viscous_flux over the whole mesh (src/ViscousScheme.cu:14-100): every zone's dq starts
+// from zero and takes its viscous term; 8th-order node fluxes are exchanged across inner faces
+// between the node fluxes and the divergences
+void viscous_all(std::vector<Zone> &zones, const Param &p) {
+  for (auto &z : zones) {
+    std::memset(z.dq.p, 0, (size_t)z.dq.sz * p.n_var * sizeof(double));
+    compute_viscous_flux(z, p, p.viscous_order == 8 ? 1 : 0);
+  }
+  if (p.viscous_order == 8) {
+    inner_flux_exchange(zones, p);
+    for (auto &z : zones) compute_viscous_flux(z, p, 2);
+  }
 }
 
 // update_physical_properties (src/FieldOperation.cuh:183-247)
@@ -2613,10 +2675,7 @@ void rk3_step(std::vector<Zone> &zones, const Param &p_in, double &dt, bool fixe
   }
   p.dt = dt;
   for (int rk = 0; rk < 3; ++rk) {
-    for (auto &z : zones) {
-      std::memset(z.dq.p, 0, (size_t)z.dq.sz * p.n_var * sizeof(double));
-      compute_viscous_flux(z, p);
-    }
+    viscous_all(zones, p);
     for (auto &z : zones) {
       if (p.reaction) finite_rate_chemistry(z, p);
       compute_inviscid_flux(z, p);

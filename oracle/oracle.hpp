@@ -110,7 +110,9 @@ void limit_flow(Zone &z, const Param &p);
 void compute_cv_from_bv(Zone &z, const Param &p);
 void compute_inviscid_flux(Zone &z, const Param &p);
 void outflow_nonreflecting(Zone &z, const Param &p);
-void compute_viscous_flux(Zone &z, const Param &p);
+void compute_viscous_flux(Zone &z, const Param &p, int phase = 0);
+void inner_flux_exchange(std::vector<Zone> &zones, const Param &p);
+void viscous_all(std::vector<Zone> &zones, const Param &p);
 void compute_chemistry(Zone &z, const Param &p);
 void chemistry_source(const Mechanism &m, double rho, double t, const double *y, double *omega, double *omega_d);
 // g_k/(R_k T) of every species (compute_gibbs_div_rt)

@@ -468,6 +468,8 @@ def _c5(name, visc=2, pp=1, limit_flow=1, stages=3, dt=1e-8):
 
 
 CASES.append(_c5("c5_air5_cylinder_4blocks"))
+# the same grid with 8th-order viscous terms: node fluxes exchanged across the inner faces
+CASES.append(_c5("c5_air5_cylinder_4blocks_visc8", visc=8))
 
 
 def build_multi(case):

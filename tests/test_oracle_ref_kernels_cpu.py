@@ -65,3 +65,35 @@ def test_oracle_matches_reference_kernels(oracle_lib, name):
     # amplified by the stiff rates, so those cases take 3e-12
     tol = 3 * TOL if case["reaction"] else TOL
     assert max(errs.values()) < tol, errs
+
+
+@pytest.mark.parametrize("name", ["c5_air5_cylinder_4blocks", "c5_air5_cylinder_4blocks_visc8"])
+def test_oracle_multiblock_matches_reference_kernels(oracle_lib, name):
+    """The four-block two-temperature AIR5 cylinder, with 2nd- and with 8th-order viscous terms (the
+    node fluxes exchanged across the inner faces): the runner's initialisation, then one step of
+    the oracle (its three stages) against the reference's state after the same three stages."""
+    z = np.load(FIXTURE)
+    meta = json.loads(bytes(z["meta"]).decode())
+    if name not in meta:
+        pytest.skip("case not in the fixture")
+    m = meta[name]
+    case = m["case"]
+    p, blocks, faces, inner, extra = refcases.build_multi(case)
+    assert refcases.same_state(refcases.multi_state_digest(blocks), m["digest"])
+    p.rho_ref, p.v_ref, p.p_ref, p.c_ref = m["rho_inf"], m["v_inf"], m["p_inf"], m["speed_of_sound"]
+    for hb in blocks:
+        oracle_lib.properties(p, hb)
+    for hb, fl in zip(blocks, faces):
+        oracle_lib.boundary(p, hb, fl)
+    oracle_lib.halo(p, blocks, inner)
+    for hb in blocks:
+        oracle_lib.properties(p, hb)
+        oracle_lib.cv_from_bv(p, hb)
+    oracle_lib.rk3_step_inner(p, blocks, faces, inner, case["dt"], fixed_dt=True)
+    errs = {}
+    for b, hb in enumerate(blocks):
+        g = hb.ngg
+        errs["cv%d" % b] = _rel(refcases.interior(hb.a["cv"], g), z[name + "/cv/%d" % b])
+        errs["T%d" % b] = _rel(refcases.interior(hb.a["bv"], g)[5][None], z[name + "/T/%d" % b][None])
+        errs["Tve%d" % b] = _rel(refcases.interior(hb.a["temperature_ve"], g)[0][None], z[name + "/Tve/%d" % b][None])
+    assert max(errs.values()) < 3 * TOL, errs

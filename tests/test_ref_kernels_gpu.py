@@ -23,6 +23,7 @@ import numpy as np
 import pytest
 
 import cb200
+from cb200 import abi
 from cb200.field import DeviceBlock
 
 import refcases
@@ -140,8 +141,10 @@ def test_sod_matches_reference_kernels(name):
 def test_multiblock_stages_match_reference_kernels(name):
     """Four-block two-temperature AIR5 square cylinder (body-fitted 2-D grid, isothermal wall with
     T_ve, freestream inflow, outflow, inner faces between the blocks, positivity limiter and
-    limit_flow): the reference's initialisation, then three stages with the inner-face exchange
-    (cb2_halo) after every stage's boundary conditions."""
+    limit_flow), with 2nd- and with 8th-order viscous terms: the reference's initialisation, then
+    three stages with the inner-face exchange (cb2_halo) after every stage's boundary conditions;
+    with 8th-order terms every stage starts with cb2_viscous (the node fluxes exchanged across the
+    inner faces) and each block's residual adds the rest to it."""
     z, meta = _fixture()
     if name not in meta:
         pytest.skip("case not in the fixture")
@@ -170,9 +173,12 @@ def test_multiblock_stages_match_reference_kernels(name):
         ctx.cv_from_bv(b)
         ctx.store_qn(b)
     dq0 = []
+    visc_all = case["visc"] == 8  # node fluxes exchanged across the inner faces: cb2_viscous first
     for rk in range(case["stages"]):
+        if visc_all:
+            ctx.viscous()
         for b in range(nb):
-            ctx.rhs(b)
+            ctx.rhs(b, abi.RHS_CHEMISTRY | abi.RHS_INVISCID | abi.RHS_ACCUMULATE if visc_all else abi.RHS_ALL)
             if rk == 0:
                 torch.cuda.synchronize()
                 dq0.append(devs[b].to_host(["dq"])["dq"])
