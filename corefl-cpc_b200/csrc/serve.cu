@@ -5,9 +5,10 @@
 // device and stays resident until it finishes.  Every iteration of the loop launches one batched
 // kernel per kind over all admitted cases (reactors: a bounded number of ROK4E attempts each;
 // tubes: a bounded number of RK3 steps each, one CTA per tube) on two streams, so the kinds
-// overlap on the device; the host then reads the per-case progress words, retires finished
-// cases (their slots and memory return to the pool, their results are copied out) and admits
-// new arrivals.  A request's latency is its completion time minus its arrival time on the host
+// overlap on the device.  The kinds are independent: whenever one kind's launch comes back, the
+// host reads its per-case progress words, retires its finished cases (their slots and memory
+// return to the pool, their results are copied out), admits its new arrivals and launches it
+// again, while the other kind's launch may still run.  A request's latency is its completion time minus its arrival time on the host
 // clock.
 #include <algorithm>
 #include <chrono>
@@ -126,9 +127,12 @@ struct Run {
   double *d_in = nullptr;  // per reactor slot: T0, p0, t_end, Y[]; then the tube composition
   double *h_in = nullptr;
   cudaStream_t s_r = nullptr, s_t = nullptr;
+  cudaEvent_t ev_r = nullptr, ev_t = nullptr;  // end of the last launch of each kind
   ~Run() {
     if (s_r) cudaStreamSynchronize(s_r);
     if (s_t) cudaStreamSynchronize(s_t);
+    if (ev_r) cudaEventDestroy(ev_r);
+    if (ev_t) cudaEventDestroy(ev_t);
     if (s_r) cudaStreamDestroy(s_r);
     if (s_t) cudaStreamDestroy(s_t);
     cudaFree(d_reac);
@@ -186,7 +190,9 @@ extern "C" int cb2_serve_run(cb2_ctx *ctx_reactor, cb2_ctx *ctx_tube, const cb2_
       !cuda_ok(cudaMallocHost(&R.h_in, sizeof(double) * kInPer * max_reactors)))
     return CB2_ERR_NOMEM;
   if (!cuda_ok(cudaStreamCreateWithFlags(&R.s_r, cudaStreamNonBlocking)) ||
-      !cuda_ok(cudaStreamCreateWithFlags(&R.s_t, cudaStreamNonBlocking)))
+      !cuda_ok(cudaStreamCreateWithFlags(&R.s_t, cudaStreamNonBlocking)) ||
+      !cuda_ok(cudaEventCreateWithFlags(&R.ev_r, cudaEventDisableTiming)) ||
+      !cuda_ok(cudaEventCreateWithFlags(&R.ev_t, cudaEventDisableTiming)))
     return CB2_ERR_CUDA;
   std::memset(R.h_line, 0, sizeof(LineCase) * max_tubes);
   std::memset(R.h_reac, 0, sizeof(cb2_reactor) * max_reactors);
@@ -207,6 +213,7 @@ extern "C" int cb2_serve_run(cb2_ctx *ctx_reactor, cb2_ctx *ctx_tube, const cb2_
   int next = 0, done = 0, n_r = 0, n_t = 0, hi_r = 0, hi_t = 0;
   long long iterations = 0;
   size_t peak_pool = 0;
+  bool busy_r = false, busy_t = false;  // a batched launch of the kind is in flight
   const auto t0 = std::chrono::steady_clock::now();
 
   while (done < n) {
@@ -214,7 +221,9 @@ extern "C" int cb2_serve_run(cb2_ctx *ctx_reactor, cb2_ctx *ctx_tube, const cb2_
     // admission, in arrival order; a request that finds no slot or memory waits, and the ones
     // behind it of the other kind may still go
     const double t_now = now_s(t0);
-    bool full_r = false, full_t = false;
+    // a kind whose launch is in flight admits nothing until it comes back (its slots, inputs
+    // and pinned buffers are in use)
+    bool full_r = busy_r, full_t = busy_t;
     for (int q = next; q < n; ++q) {
       const int id = order[q];
       if (admitted[id]) continue;
@@ -266,29 +275,68 @@ extern "C" int cb2_serve_run(cb2_ctx *ctx_reactor, cb2_ctx *ctx_tube, const cb2_
     while (next < n && admitted[order[next]]) ++next;
     peak_pool = std::max(peak_pool, R.pool.used);
 
-    if (n_r == 0 && n_t == 0) {  // idle until the next arrival
+    // one batched launch per idle kind with cases, each on its own stream, its progress words
+    // copied back behind it; the kinds run independently, so a short tube launch never waits for
+    // a long reactor launch
+    if (n_r && !busy_r) {
+      rc = launch_reactor_advance(*pr, R.d_reac, hi_r, attempts_per, opt->rtol, opt->atol, R.s_r);
+      if (rc) return rc;
+      if (!cuda_ok(cudaMemcpyAsync(R.h_reac, R.d_reac, sizeof(cb2_reactor) * hi_r, cudaMemcpyDeviceToHost, R.s_r)) ||
+          !cuda_ok(cudaEventRecord(R.ev_r, R.s_r)))
+        return CB2_ERR_CUDA;
+      busy_r = true;
+      ++iterations;
+    }
+    if (n_t && !busy_t) {
+      rc = launch_line_batch(R.d_line, hi_t, *pt, steps_per, R.s_t);
+      if (rc) return rc;
+      if (!cuda_ok(cudaMemcpyAsync(R.h_line, R.d_line, sizeof(LineCase) * hi_t, cudaMemcpyDeviceToHost, R.s_t)) ||
+          !cuda_ok(cudaEventRecord(R.ev_t, R.s_t)))
+        return CB2_ERR_CUDA;
+      busy_t = true;
+      ++iterations;
+    }
+    if (!busy_r && !busy_t) {  // idle until the next arrival
       if (next < n) {
         const double wait = reqs[order[next]].arrival - now_s(t0);
         if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 0.01)));
       }
       continue;
     }
-    // one batched launch per kind, each on its own stream, then the progress words come back
-    if (n_r) {
-      rc = launch_reactor_advance(*pr, R.d_reac, hi_r, attempts_per, opt->rtol, opt->atol, R.s_r);
-      if (rc) return rc;
-      cudaMemcpyAsync(R.h_reac, R.d_reac, sizeof(cb2_reactor) * hi_r, cudaMemcpyDeviceToHost, R.s_r);
+    // wait for a launch to come back, or for the arrival of a request of an idle kind
+    double t_idle_arrival = 1e300;
+    for (int q = next; q < n; ++q) {
+      const int id = order[q];
+      if (admitted[id]) continue;
+      const bool is_r = reqs[id].kind == CB2_REQ_REACTOR;
+      if ((is_r && !busy_r) || (!is_r && !busy_t)) {
+        t_idle_arrival = reqs[id].arrival;
+        break;
+      }
     }
-    if (n_t) {
-      rc = launch_line_batch(R.d_line, hi_t, *pt, steps_per, R.s_t);
-      if (rc) return rc;
-      cudaMemcpyAsync(R.h_line, R.d_line, sizeof(LineCase) * hi_t, cudaMemcpyDeviceToHost, R.s_t);
+    bool fin_r = false, fin_t = false;
+    for (;;) {
+      if (busy_r) {
+        const cudaError_t e = cudaEventQuery(R.ev_r);
+        if (e == cudaSuccess) fin_r = true;
+        else if (e != cudaErrorNotReady) return CB2_ERR_CUDA;
+      }
+      if (busy_t) {
+        const cudaError_t e = cudaEventQuery(R.ev_t);
+        if (e == cudaSuccess) fin_t = true;
+        else if (e != cudaErrorNotReady) return CB2_ERR_CUDA;
+      }
+      if (fin_r || fin_t) break;
+      const double t = now_s(t0);
+      if (t >= t_idle_arrival) break;
+      if (t > time_limit) return CB2_ERR_TIMEOUT;
+      std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
-    if (!cuda_ok(cudaStreamSynchronize(R.s_r)) || !cuda_ok(cudaStreamSynchronize(R.s_t))) return CB2_ERR_CUDA;
-    ++iterations;
+    if (fin_r) busy_r = false;
+    if (fin_t) busy_t = false;
     const double t_done = now_s(t0);
     // retire the finished reactors (a finished slot is skipped by the kernel until reused)
-    for (int k = 0; k < hi_r; ++k) {
+    for (int k = 0; fin_r && k < hi_r; ++k) {
       const int id = slot_r[k];
       const cb2_reactor &st = R.h_reac[k];
       if (id < 0 || !(st.status & (CB2_REACTOR_DONE | CB2_REACTOR_NONPHYSICAL))) continue;
@@ -306,7 +354,7 @@ extern "C" int cb2_serve_run(cb2_ctx *ctx_reactor, cb2_ctx *ctx_tube, const cb2_
       ++done;
     }
     // retire the finished tubes: results out, slot deactivated, memory back to the pool
-    for (int k = 0; k < hi_t; ++k) {
+    for (int k = 0; fin_t && k < hi_t; ++k) {
       const int id = slot_t[k];
       const LineCase &lc = R.h_line[k];
       if (id < 0 || !(lc.status & (kLineDone | kLineFailed))) continue;
@@ -339,8 +387,10 @@ extern "C" int cb2_serve_run(cb2_ctx *ctx_reactor, cb2_ctx *ctx_tube, const cb2_
       --n_t;
       ++done;
     }
-    while (hi_r > 0 && slot_r[hi_r - 1] < 0) --hi_r;
-    while (hi_t > 0 && slot_t[hi_t - 1] < 0) --hi_t;
+    if (!busy_r)
+      while (hi_r > 0 && slot_r[hi_r - 1] < 0) --hi_r;
+    if (!busy_t)
+      while (hi_t > 0 && slot_t[hi_t - 1] < 0) --hi_t;
   }
   if (opt->stats) {
     opt->stats->iterations = iterations;
