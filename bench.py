@@ -111,6 +111,8 @@ def parse():
     ap.add_argument("--serve-reactor-t-end", type=float, default=1e-3,
                     help="physical end time of the served 0-D reactors")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="mean arrivals per second")
+    ap.add_argument("--reactor-sweep", action="store_true",
+                    help="time one ROK4E attempt of the batched H2/air reactors at several batch sizes")
     ap.add_argument("--schedule", default=None,
                     help="use these tile widths instead of timing them: 'NI' for the y/z sweeps and the "
                          "batch, or 'NI,CS' to also fix the batch's cluster size (e.g. from an earlier run)")
@@ -511,6 +513,7 @@ def gpu_arm(args, rank, world, local_rank):
     if not args.no_c5 and args.c5_variants > 0:
         c5v = square_cylinder_variants(args, local_rank, c5 and c5.get("value"))
     served = None if args.no_serve else serve_workload(args)
+    reactors = reactor_sweep(args) if args.reactor_sweep else None
     samples = accuracy_samples(args, local_rank) if (rank == 0 and not args.no_cpu_baseline) else None
     if dist:
         dist.barrier()
@@ -560,6 +563,7 @@ def gpu_arm(args, rank, world, local_rank):
             "details": "second JSON object on stderr"}
     details = {"mixed": mixed, "serve": served, "reacting_box": reacting, "batched_blocks": batched,
                "square_cylinder_air5": c5, "square_cylinder_air5_variants": c5v, "cpu_baseline": base, "e2e": e2e,
+               "reactor_sweep": reactors,
                "kernel_ms_per_step": {k: v[1] for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
                "kernel_rooflines": kernel_roofs}
     print(json.dumps(details, default=float), file=sys.stderr, flush=True)
@@ -924,6 +928,42 @@ def batched_blocks(args, local_rank):
     out["speedup_batched"] = t_seq / t_batch
     del devs
     torch.cuda.empty_cache()
+    return out
+
+
+def reactor_sweep(args):
+    """us per ROK4E attempt of the batched 0-D H2/air reactors (one warp each) at batch sizes from a
+    few warps to past the GPU's concurrency: latency where the batch is small, throughput where it
+    saturates.  The reactors start from the reference's reactor runs (tests/golden) with their end
+    times moved out of reach, so every reactor takes every attempt."""
+    import ctypes as C
+    import torch
+    import cb200
+    from cb200 import abi, cases, mech as mechmod
+    runs = json.load(open(os.path.join(REPO, "tests", "golden", "h2_reactor_runs.json")))
+    h2 = mechmod.load_json(os.path.join(REPO, "tests", "golden", "h2_li2004.json"))
+    p = cases.make_param(n_var=5 + h2.ns, n_spec=h2.ns, dim=1, inviscid_scheme=abi.INV_HLLC,
+                         reconstruction=abi.REC_WENO5, mech=h2.ptr())
+    ctx = cb200.Context(p)
+    out = {}
+    attempts = 200
+    for n in (32, 592, 4096, 16384):
+        rr = [runs["runs"][i % len(runs["runs"])] for i in range(n)]
+        dev = lambda a: torch.tensor(a, dtype=torch.float64, device="cuda")
+        T0, p0 = dev([r["T0"] for r in rr]), dev([r["p0"] for r in rr])
+        Y, t_end = dev([r["Y"] for r in rr]), dev([r["t_end"] * 1e3 for r in rr])
+        st = torch.zeros(n * C.sizeof(abi.Reactor), dtype=torch.uint8, device="cuda")
+        ctx.reactor_setup(st.data_ptr(), n, T0.data_ptr(), p0.data_ptr(), Y.data_ptr(), t_end.data_ptr(), runs["h0"])
+        ctx.reactor_advance(st.data_ptr(), n, 20, runs["rtol"], runs["atol"])
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ctx.reactor_advance(st.data_ptr(), n, attempts, runs["rtol"], runs["atol"])
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[str(n)] = {"us_per_attempt": ms * 1e3 / attempts, "attempts_per_s": n * attempts / (ms * 1e-3)}
+    ctx.close()
     return out
 
 
