@@ -1,7 +1,7 @@
 """ctypes mirror of include/cb200.h (structs and constants)."""
 import ctypes as C
 
-ABI_VERSION = 5
+ABI_VERSION = 6
 
 OK = 0
 ERR_CUDA, ERR_INVALID, ERR_NONPHYSICAL, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_NOMEM = -1, -2, -3, -4, -5, -6
@@ -35,7 +35,9 @@ class FaceBC(C.Structure):
                 ("range_start", C.c_int * 3), ("range_end", C.c_int * 3),
                 ("rho", C.c_double), ("u", C.c_double), ("v", C.c_double), ("w", C.c_double),
                 ("p", C.c_double), ("T", C.c_double), ("wall_temperature", C.c_double),
-                ("wall_temperature_ve", C.c_double), ("sv", C.c_void_p)]
+                ("wall_temperature_ve", C.c_double), ("sv", C.c_void_p),
+                ("blow_shock_wave", C.c_int), ("blow_start_step", C.c_int), ("blow_end_step", C.c_int),
+                ("blow_coefficient", C.c_double)]
 
 
 class InnerFace(C.Structure):

@@ -39,6 +39,7 @@ def load():
         "cb2_store_qn": (C.c_int, [vp, C.c_int, vp]),
         "cb2_rhs": (C.c_int, [vp, C.c_int, C.c_uint, vp]),
         "cb2_viscous": (C.c_int, [vp, vp]),
+        "cb2_set_step": (C.c_int, [vp, C.c_longlong]),
         "cb2_shock_sensor": (C.c_int, [vp, C.c_int, vp]),
         "cb2_stage_update": (C.c_int, [vp, C.c_int, C.c_double, C.c_int, vp]),
         "cb2_boundary": (C.c_int, [vp, C.c_int, vp]),
@@ -118,6 +119,10 @@ class Context:
 
     def rhs(self, blk, mask=abi.RHS_ALL, stream=None):
         check(self.lib.cb2_rhs(self.h, blk, mask, stream), "cb2_rhs")
+
+    def set_step(self, step):
+        """cb2_set_step: the step number the face conditions see."""
+        check(self.lib.cb2_set_step(self.h, step), "cb2_set_step")
 
     def viscous(self, stream=None):
         """cb2_viscous: the viscous term of every bound block (node fluxes exchanged across inner faces)."""

@@ -314,6 +314,10 @@ FaceBC register_face(const cb2_face_bc &f, int dim, int ngg, bool extend) {
   b.rho = f.rho; b.u = f.u; b.v = f.v; b.w = f.w; b.p = f.p; b.T = f.T; b.wall_T = f.wall_temperature;
   b.wall_Tve = f.wall_temperature_ve;
   b.sv = nullptr;  // set at bind to the device copy of f.sv
+  b.blow = b.type == CB2_BC_WALL && f.blow_shock_wave != 0;
+  b.blow_start = f.blow_start_step;
+  b.blow_end = f.blow_end_step;
+  b.blow_coef = f.blow_coefficient;
   return b;
 }
 
@@ -1233,7 +1237,14 @@ int cb2_rk3_step(cb2_ctx *ctx, double *dt_inout, int fixed_dt, void *stream) {
     *dt_inout = dt;
   }
   ctx->p.dt = dt;
+  ++ctx->p.step;  // the step this call takes (RK3 counts it before its stages)
   return enqueue_stages(ctx, dt, stream);
+}
+
+int cb2_set_step(cb2_ctx *ctx, long long step) {
+  if (!ctx) return CB2_ERR_INVALID;
+  ctx->p.step = step;
+  return CB2_OK;
 }
 
 int cb2_rk3_run(cb2_ctx *ctx, double dt, int fixed_dt, long long max_steps, double t_end, double *time_inout,
@@ -1247,6 +1258,10 @@ int cb2_rk3_run(cb2_ctx *ctx, double dt, int fixed_dt, long long max_steps, doub
   for (auto &B : ctx->blocks) {
     any = any || B.bound;
     if (B.bound && !fixed_dt && !B.z.dtl) return CB2_ERR_INVALID;
+    // a blowing wall reads the step number, which the device-driven loop does not pass on
+    if (B.bound)
+      for (const FaceBC &f : B.faces)
+        if (f.blow) return CB2_ERR_UNSUPPORTED;
   }
   if (!any) return CB2_ERR_INVALID;
   fixed_dt = fixed_dt ? 1 : 0;

@@ -390,6 +390,23 @@ __global__ void k_bc_wall(Zone z, Param p, FaceBC f) {
   // a fully catalytic wall (Wall::catalytic_type 1) gives its face node and ghosts the wall's
   // mass fractions f.sv (Wall::yk); a non-catalytic one copies them from the interior
   const bool cat = NS > 0 && f.sv != nullptr;
+  // the wall's velocity: at rest, or blowing along its inward normal while the step lies in the
+  // blowing window (src/BoundCond.cu:3226-3245): blow_coefficient x max(the inner node's normal
+  // velocity towards the wall, and for steps <= 50 the freestream's (f.u, f.v, f.w))
+  double wu = 0, wv = 0, ww = 0;
+  if (f.blow && p.step >= f.blow_start && p.step <= f.blow_end) {
+    const double *Mf = z.metric + (idx_t)(3 * f.face) * sz;
+    double nx = Mf[gb], ny = Mf[gb + sz], nz = Mf[gb + 2 * sz];
+    const double ninv = f.direction / fmax(sqrt(nx * nx + ny * ny + nz * nz), 1e-30);
+    nx *= ninv; ny *= ninv; nz *= ninv;
+    const double vn_local = nx * z.bv[g1 + sz] + ny * z.bv[g1 + 2 * sz] + nz * z.bv[g1 + 3 * sz];
+    const double vn_inf = nx * f.u + ny * f.v + nz * f.w;
+    const double seed = p.step <= 50 ? fmax(vn_inf, 0.0) : 0.0;
+    const double blow = fmax(f.blow_coef, 0.0) * fmax(fmax(vn_local, 0.0), seed);
+    wu = -blow * nx;
+    wv = -blow * ny;
+    ww = -blow * nz;
+  }
   double R = kRAir;
   if (gl == 0) {
     const double pw = z.bv[g1 + 4 * sz];
@@ -401,9 +418,9 @@ __global__ void k_bc_wall(Zone z, Param p, FaceBC f) {
       }
     }
     z.bv[gb] = pw / (t_wall * R);
-    z.bv[gb + sz] = 0;
-    z.bv[gb + 2 * sz] = 0;
-    z.bv[gb + 3 * sz] = 0;
+    z.bv[gb + sz] = wu;
+    z.bv[gb + 2 * sz] = wv;
+    z.bv[gb + 3 * sz] = ww;
     z.bv[gb + 4 * sz] = pw;
     z.bv[gb + 5 * sz] = t_wall;
     if constexpr (NS > 0) {
@@ -447,9 +464,9 @@ __global__ void k_bc_wall(Zone z, Param p, FaceBC f) {
       }
     }
     z.bv[gg] = p_i / (t_g * R);
-    z.bv[gg + sz] = -z.bv[gi + sz];
-    z.bv[gg + 2 * sz] = -z.bv[gi + 2 * sz];
-    z.bv[gg + 3 * sz] = -z.bv[gi + 3 * sz];
+    z.bv[gg + sz] = 2 * wu - z.bv[gi + sz];
+    z.bv[gg + 2 * sz] = 2 * wv - z.bv[gi + 2 * sz];
+    z.bv[gg + 3 * sz] = 2 * ww - z.bv[gi + 3 * sz];
     z.bv[gg + 4 * sz] = p_i;
     z.bv[gg + 5 * sz] = t_g;
     if constexpr (NS > 0) {

@@ -127,6 +127,7 @@ struct Param {
   double lf_ll[5], lf_ul[5];  // limit_flow bounds of rho, u, v, w, p
   double dt;                  // the current step's time step (positivity limiter)
   const double *dt_dev;       // non-null: the step's time step lives on the device (graph runs)
+  long long step;             // the step number the face conditions see (the blowing wall)
   unsigned *status;  // device status word
   Mech mech;
 };

@@ -65,6 +65,8 @@ struct FaceBC {
   int start[3], end[3];
   double rho, u, v, w, p, T, wall_T, wall_Tve;
   const double *sv;  // inflow scalars (device copy of cb2_face_bc::sv)
+  int blow, blow_start, blow_end;  // blowing wall (cb2_face_bc::blow_*)
+  double blow_coef;
 };
 
 // ---- launchers (each returns CB2_OK or an error code; n_launch counts kernels) ----------

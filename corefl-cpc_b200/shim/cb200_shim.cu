@@ -329,6 +329,15 @@ struct Shim {
           const cfd::Wall &wall = walls.back();
           c.wall_temperature = wall.thermal_type == cfd::Wall::ThermalType::isothermal ? wall.temperature : 0.0;
           c.wall_temperature_ve = wall.temperature_ve > 0 ? wall.temperature_ve : 0.0;
+          if (wall.if_blow_shock_wave) {  // blowing wall: its window and the freestream velocity
+            c.blow_shock_wave = 1;
+            c.blow_coefficient = wall.blow_shock_wave_coefficient;
+            c.blow_start_step = wall.blow_shock_wave_start_step;
+            c.blow_end_step = wall.blow_shock_wave_end_step;
+            c.u = par.get_real("ux_inf");
+            c.v = par.get_real("uy_inf");
+            c.w = par.get_real("uz_inf");
+          }
           if (wall.catalytic_type == 1) c.sv = wall.yk;  // fully catalytic: the wall mass fractions
         }
         faces.push_back(c);

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define CB2_ABI_VERSION 5
+#define CB2_ABI_VERSION 6
 
 /* ---- status codes ---------------------------------------------------------------- */
 #define CB2_OK 0
@@ -130,6 +130,13 @@ typedef struct cb2_face_bc {
    * mass fractions of a fully catalytic wall (Wall::yk with catalytic_type 1, src/BoundCond.h:105-107),
    * which its face node and ghosts take.  A HOST array copied at bind. */
   const double *sv;
+  /* a wall that blows (Wall::if_blow_shock_wave, src/BoundCond.cu:3226-3245): while the context's
+   * step (cb2_set_step) lies in [blow_start_step, blow_end_step], the wall moves along its inward
+   * normal at blow_coefficient x max(normal velocity of the node inside towards the wall, seed),
+   * the seed being the freestream's normal velocity (u, v, w of this face: ux_inf, uy_inf, uz_inf)
+   * for steps <= 50.  blow_shock_wave = 0: a wall at rest.  (ABI version 6) */
+  int blow_shock_wave, blow_start_step, blow_end_step;
+  double blow_coefficient;
 } cb2_face_bc;
 
 /* One inner face of a multi-block grid, as cfd::InnerFace holds it after register_boundary
@@ -347,6 +354,12 @@ int cb2_cv_from_bv(cb2_ctx *ctx, int blk, void *stream);
  * CB2_ERR_NONPHYSICAL if any node's Jacobian is not positive (where the reference aborts). */
 int cb2_metrics(const double *x, const double *y, const double *z, int mx, int my, int mz, int g_coord, int ngg,
                 double *metric, double *jac, void *stream);
+
+/* The step number the face conditions see (the reference's `step`, src/RK.cuh:69-108: a new run
+ * starts from 0, a restart from its step file, and each step counts one before its stages).
+ * cb2_rk3_step adds one at its start; cb2_boundary uses the value as it is.  Only the blowing wall
+ * reads it; cb2_rk3_run refuses contexts with one.  (ABI version 6) */
+int cb2_set_step(cb2_ctx *ctx, long long step);
 
 /* Flowfield file of every bound block (blocks 0 .. n-1, all bound): the reference's
  * output/flowfield.plt (FieldIO::initialize / print_field, src/FieldIO.h:77-470), a Tecplot binary

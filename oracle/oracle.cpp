@@ -1592,6 +1592,9 @@ void nasa7_h_cp(double t, const Mechanism &m, double *h, double *cp) {
   }
 }
 
+static long long g_step = 0;
+void set_step(long long step) { g_step = step; }
+
 Param make_param(const cb2_param_view &pv) {
   Param p;
   p.dim = pv.dim;
@@ -1709,6 +1712,7 @@ Param make_param(const cb2_param_view &pv) {
     o.park_sigma.assign(t.park_sigma, t.park_sigma + ns);
     p.i_eve = p.n_spec;
   }
+  p.step = g_step;
   return p;
 }
 
@@ -1749,6 +1753,10 @@ Zone make_zone(const cb2_zone_view &v, const cb2_face_bc *faces, int n_faces, co
     o.wall_Tve = b.wall_temperature_ve;
     // a wall's sv: its mass fractions when fully catalytic (Wall::yk, n_spec values)
     if (b.sv) o.sv.assign(b.sv, b.sv + (o.type == CB2_BC_WALL ? p.n_spec : p.n_scalar));
+    o.blow = o.type == CB2_BC_WALL && b.blow_shock_wave != 0;
+    o.blow_start = b.blow_start_step;
+    o.blow_end = b.blow_end_step;
+    o.blow_coef = b.blow_coefficient;
     z.faces.push_back(o);
     if (b.type == CB2_BC_PERIODIC) continue;
     int lo[3], hi[3];
@@ -2394,7 +2402,21 @@ void apply_boundary_conditions(Zone &z, const Param &p) {
               for (int l = 0; l < p.n_spec; ++l) z.sv(i, j, k, l) = cat ? f.sv[l] : z.sv(idx[0], idx[1], idx[2], l);
               double R = mix_r(z, p, i, j, k);
               z.bv(i, j, k, 0) = pw / (t_wall * R);
-              z.bv(i, j, k, 1) = z.bv(i, j, k, 2) = z.bv(i, j, k, 3) = 0;
+              // the wall's velocity: at rest, or blowing (if_blow_shock_wave, :3226-3245)
+              double wall_u[3] = {0, 0, 0};
+              if (f.blow && p.step >= f.blow_start && p.step <= f.blow_end) {
+                double n[3] = {z.metric(i, j, k, f.face * 3), z.metric(i, j, k, f.face * 3 + 1),
+                               z.metric(i, j, k, f.face * 3 + 2)};
+                const double ninv = f.direction / std::max(std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]), 1e-30);
+                for (double &c : n) c *= ninv;
+                const double vn_local = n[0] * z.bv(idx[0], idx[1], idx[2], 1) + n[1] * z.bv(idx[0], idx[1], idx[2], 2) +
+                                        n[2] * z.bv(idx[0], idx[1], idx[2], 3);
+                const double vn_inf = n[0] * f.u + n[1] * f.v + n[2] * f.w;  // the freestream (ux_inf, ...)
+                const double seed = p.step <= 50 ? std::max(vn_inf, 0.0) : 0.0;
+                const double blow = std::max(f.blow_coef, 0.0) * std::max(std::max(vn_local, 0.0), seed);
+                for (int c = 0; c < 3; ++c) wall_u[c] = -blow * n[c];
+              }
+              for (int c = 0; c < 3; ++c) z.bv(i, j, k, 1 + c) = wall_u[c];
               z.bv(i, j, k, 4) = pw;
               z.bv(i, j, k, 5) = t_wall;
               if (tt) {
@@ -2428,7 +2450,7 @@ void apply_boundary_conditions(Zone &z, const Param &p) {
                   z.sv(gh[0], gh[1], gh[2], l) = cat ? f.sv[l] : z.sv(in[0], in[1], in[2], l);
                 R = cat ? mix_r(z, p, i, j, k) : mix_r(z, p, in[0], in[1], in[2]);
                 z.bv(gh[0], gh[1], gh[2], 0) = p_i / (t_g * R);
-                for (int c = 1; c <= 3; ++c) z.bv(gh[0], gh[1], gh[2], c) = -z.bv(in[0], in[1], in[2], c);
+                for (int c = 1; c <= 3; ++c) z.bv(gh[0], gh[1], gh[2], c) = 2 * wall_u[c - 1] - z.bv(in[0], in[1], in[2], c);
                 z.bv(gh[0], gh[1], gh[2], 4) = p_i;
                 z.bv(gh[0], gh[1], gh[2], 5) = t_g;
                 if (tt) {
@@ -2662,6 +2684,7 @@ void inner_exchange(std::vector<Zone> &zones, const Param &p) {
 
 void rk3_step(std::vector<Zone> &zones, const Param &p_in, double &dt, bool fixed_dt) {
   Param p = p_in;
+  g_step = ++p.step;  // the step this call takes, counted before its stages (src/RK.cuh:108)
   for (auto &z : zones) {
     const size_t n = (size_t)z.cv.sz * p.n_var;
     std::memcpy(z.qn.p, z.cv.p, n * sizeof(double));

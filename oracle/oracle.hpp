@@ -79,6 +79,7 @@ struct Param {
   double rho_ref = 1, v_ref = 1, weno_eps_scale = 1, mu_constant = 0;
   int limit_flow = 0;
   double dt = 0;  // the step's time step (positivity limiter)
+  long long step = 0;  // the step number the face conditions see (the blowing wall)
   double lf_ll[5] = {0, 0, 0, 0, 0}, lf_ul[5] = {0, 0, 0, 0, 0};
   Mechanism mech;
   TwoTemperature tt;
@@ -90,6 +91,9 @@ struct FaceBC {
   int start[3] = {0, 0, 0}, end[3] = {0, 0, 0};
   double rho = 0, u = 0, v = 0, w = 0, p = 0, T = 0, wall_T = 0, wall_Tve = 0;
   std::vector<double> sv;  // inflow scalars
+  bool blow = false;        // blowing wall (cb2_face_bc::blow_*)
+  int blow_start = 0, blow_end = 0;
+  double blow_coef = 0;
 };
 
 struct Zone {
@@ -102,6 +106,9 @@ struct Zone {
 };
 
 Param make_param(const cb2_param_view &pv);
+// the step number make_param gives the face conditions (the library's cb2_set_step); rk3_step
+// counts one before its stages and leaves it there
+void set_step(long long step);
 Zone make_zone(const cb2_zone_view &v, const cb2_face_bc *faces, int n_faces, const Param &p);
 
 void update_cv_and_bv_rk(Zone &z, const Param &p, double dt, int rk);

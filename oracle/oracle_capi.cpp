@@ -72,6 +72,8 @@ int oracle_cv_from_bv(const cb2_param_view *pv, const cb2_zone_view *zv) {
   return 0;
 }
 
+void oracle_set_step(long long step) { set_step(step); }
+
 int oracle_rhs(const cb2_param_view *pv, const cb2_zone_view *zv, const cb2_face_bc *faces, int n_faces,
                unsigned mask) {
   Param p = make_param(*pv);

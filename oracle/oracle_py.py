@@ -30,6 +30,7 @@ def load():
         P = C.POINTER
         sig = {
             "oracle_set_threads": (None, [C.c_int]),
+            "oracle_set_step": (None, [C.c_longlong]),
             "oracle_max_threads": (C.c_int, []),
             "oracle_stage_update": (C.c_int, [P(abi.ParamView), P(abi.ZoneView), C.c_double, C.c_int]),
             "oracle_cv_from_bv": (C.c_int, [P(abi.ParamView), P(abi.ZoneView)]),
@@ -63,6 +64,11 @@ def _faces(faces):
     for a, f in enumerate(faces):
         arr[a] = f
     return arr
+
+
+def set_step(step):
+    """The step number the face conditions see (the library's cb2_set_step)."""
+    load().oracle_set_step(step)
 
 
 def set_threads(n):

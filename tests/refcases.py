@@ -46,6 +46,8 @@ CHAN_WALL_T = 0.004
 # the farfield channel: farfield (i- and j+), back-pressure outflow (i+), isothermal wall (j-)
 CHAN_FARFIELD = dict(rho=1.1, u=0.6, p=1.0)
 CHAN_BACK_PRESSURE = 1.05
+# the blowing wall of the channel (Wall::if_blow_shock_wave): coefficient and step window
+CHAN_BLOW = {"coefficient": 0.5, "start": 0, "end": 10}
 # fully catalytic isothermal walls of the mixture boxes (low x face): wall temperature and the
 # wall's mass fractions (Wall::yk), by species name
 CAT_WALL = {"mix": (1000.0, {"H2O": 0.25, "N2": 0.75}), "air5": (2000.0, {"N2": 0.767, "O2": 0.233})}
@@ -101,7 +103,7 @@ CASES = ([_air(n + "_" + bc, s, r, v, bc) for n, s, r, v in AIR_SCHEMES for bc i
          [_chan("chan_hllc_muscl_visc2", 4, 2, 2), _chan("chan_weno5ch_visc2", 52, 2, 2),
           _chan("chan_roe_muscl", 2, 2, 0), _chan("chan_farfield_weno5ch", 52, 2, 0, bc="farfield"),
           _chan("chan_farfield_hllc_visc2", 4, 2, 2, bc="farfield"), _chan("chan_nr_weno5ch", 52, 2, 0, bc="nr", plt=1),
-          _chan("chan_nr_ausm_muscl", 3, 2, 0, bc="nr"), _mix("mix_nr_weno5ch", 52, 2, 0, 0, bc="nr"),
+          _chan("chan_nr_ausm_muscl", 3, 2, 0, bc="nr"), _chan("chan_blow_weno5ch", 52, 2, 0, bc="blow"), _mix("mix_nr_weno5ch", 52, 2, 0, 0, bc="nr"),
           _mix("mix_catwall_weno5ch", 52, 2, 0, 0, bc="catwall", plt=1),
           _air5("air5_catwall_weno5ch", 0, 1, bc="catwall", plt=1),
           _air5("air5_hllc_muscl_visc2_chem", 2, 1, scheme=4), _air5("air5_ausm_muscl_chem", 0, 1, scheme=3)] +
@@ -169,10 +171,17 @@ def build(case):
                      face(abi.BC_WALL, 1, -1, (0, 0, 0), (mx - 1, 0, 0), wall_temperature=CHAN_WALL_T),
                      face(abi.BC_FARFIELD, 1, 1, (0, my - 1, 0), (mx - 1, my - 1, 0), **st)]
         else:
+            wall = face(abi.BC_WALL, 1, -1, (0, 0, 0), (mx - 1, 0, 0), wall_temperature=CHAN_WALL_T)
+            if case["bc"] == "blow":
+                # a blowing wall: the freestream velocity (ux_inf, uy_inf, uz_inf) of the reference
+                # state and the blowing window
+                wall.u, wall.v, wall.w = p.v_ref, 0.0, 0.0
+                wall.blow_shock_wave = 1
+                wall.blow_coefficient = CHAN_BLOW["coefficient"]
+                wall.blow_start_step, wall.blow_end_step = CHAN_BLOW["start"], CHAN_BLOW["end"]
             faces = [face(abi.BC_INFLOW, 0, -1, (0, 0, 0), (0, my - 1, 0), rho=ci["rho"], u=ci["u"], v=0.0,
                           w=0.0, p=ci["p"], T=t_in),
-                     face(abi.BC_OUTFLOW, 0, 1, (mx - 1, 0, 0), (mx - 1, my - 1, 0)),
-                     face(abi.BC_WALL, 1, -1, (0, 0, 0), (mx - 1, 0, 0), wall_temperature=CHAN_WALL_T),
+                     face(abi.BC_OUTFLOW, 0, 1, (mx - 1, 0, 0), (mx - 1, my - 1, 0)), wall,
                      face(abi.BC_SYMMETRY, 1, 1, (0, my - 1, 0), (mx - 1, my - 1, 0))]
         extra = {}
     elif fam == "sod":
@@ -365,6 +374,11 @@ def write_reference_case(case, case_dir, ref_dir):
                   "    int catalytic_type = 1"] + ["    real %s = %r" % (n, v) for n, v in yw.items()]
         elif t == abi.BC_WALL:
             s += ["    string thermal_type = isothermal", "    real temperature = %r" % CHAN_WALL_T]
+            if case.get("bc") == "blow":
+                s += ["    int if_blow_shock_wave = 1",
+                      "    real blow_shock_wave_coefficient = %r" % CHAN_BLOW["coefficient"],
+                      "    int blow_shock_wave_start_step = %d" % CHAN_BLOW["start"],
+                      "    int blow_shock_wave_end_step = %d" % CHAN_BLOW["end"]]
         if t == abi.BC_FARFIELD:
             ff = CHAN_FARFIELD
             s += ["    real density = %r" % ff["rho"], "    real velocity = %r" % ff["u"], "    real u = 1.0",

@@ -38,7 +38,8 @@ def test_struct_sizes_match_header():
     assert C.sizeof(abi.Mechanism) == 2 * 4 + n_tab * 8 + 2 * 4 + 3 * 8 + 8 + 4 * 8
     # 2 ints, 7 pointers, 1 int (padded to 8)
     assert C.sizeof(abi.TwoTemperature) == 2 * 4 + 7 * 8 + 8
-    assert C.sizeof(abi.FaceBC) == 4 * 9 + 4 + 8 * 8 + 8  # 36 bytes of ints padded to 8, 8 doubles, a pointer
+    # 36 bytes of ints padded to 8, 8 doubles, a pointer, then the blowing wall's 3 ints padded to 8 and a double
+    assert C.sizeof(abi.FaceBC) == 4 * 9 + 4 + 8 * 8 + 8 + 3 * 4 + 4 + 8
     assert C.sizeof(abi.InnerFace) == 4 * 29
     assert abi.ParamView.abi_version.offset == 0
 

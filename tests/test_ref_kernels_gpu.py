@@ -72,7 +72,9 @@ def _prepare(meta_case):
     dev = DeviceBlock(hb)
     ctx = cb200.Context(p)
     ctx.bind(0, dev.view(), faces)
-    # Driver::initialize_computation as the runner performs it, then cv from bv at the start of RK3
+    # Driver::initialize_computation as the runner performs it (the runner passes step 0 to its face conditions),
+    # then cv from bv at the start of RK3
+    ctx.set_step(0)
     ctx.properties(0)
     ctx.boundary(0)
     ctx.properties(0)
@@ -91,6 +93,7 @@ def test_stages_match_reference_kernels(name):
     import torch
     g = hb.ngg
     ctx.store_qn(0)
+    ctx.set_step(1)  # the runner's one step
     dq0 = None
     for rk in range(case["stages"]):
         ctx.rhs(0)
