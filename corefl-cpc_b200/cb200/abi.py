@@ -88,6 +88,7 @@ class ParamView(C.Structure):
 # ---- batched solves (include/cb200_serve.h) ---------------------------------------------------
 REACTOR_MAX_SPEC = 9
 REACTOR_DONE, REACTOR_NONPHYSICAL = 1, 2
+REACTOR_EXPLICIT, REACTOR_EPI, REACTOR_DA, REACTOR_RK3, REACTOR_CONSERVE_MASS = 0, 1, 2, 3, 0x10
 
 
 class Reactor(C.Structure):

@@ -65,6 +65,7 @@ def load():
         "cb2_profile_entry": (C.c_int, [vp, C.c_int, C.c_char_p, C.c_int, P(C.c_ulonglong), P(C.c_double)]),
         "cb2_reactor_setup": (C.c_int, [vp, vp, C.c_int, vp, vp, vp, vp, C.c_double, vp]),
         "cb2_reactor_advance": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_double, C.c_double, vp]),
+        "cb2_reactor_advance_fixed": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, vp]),
         "cb2_metrics": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp]),
         "cb2_write_flowfield": (C.c_int, [vp, C.c_char_p, P(vp), P(C.c_char_p), C.c_int, C.c_double, vp]),
         "cb2_read_flowfield": (C.c_int, [vp, C.c_char_p, P(C.c_char_p), P(C.c_double), vp]),
@@ -219,6 +220,12 @@ class Context:
     def reactor_advance(self, reactors, n, max_attempts, rtol=1e-6, atol=1e-12, stream=None):
         check(self.lib.cb2_reactor_advance(self.h, reactors, n, max_attempts, rtol, atol, stream),
               "cb2_reactor_advance")
+
+    def reactor_advance_fixed(self, reactors, n, max_steps, scheme, stream=None):
+        """At most max_steps fixed steps (dt = each reactor's h) of the form `scheme`
+        (abi.REACTOR_EXPLICIT .. abi.REACTOR_RK3, optionally | abi.REACTOR_CONSERVE_MASS)."""
+        check(self.lib.cb2_reactor_advance_fixed(self.h, reactors, n, max_steps, scheme, stream),
+              "cb2_reactor_advance_fixed")
 
     def read_status(self, stream=None):
         f = C.c_uint()

@@ -129,6 +129,7 @@ int launch_run_advance(RunState *r, const double *dt, const unsigned *status, cu
 // batched 0-D reactors (reactor.cu); the state type is cb2_reactor of cb200_serve.h
 int launch_reactor_setup(const Param &p, cb2_reactor *r, int n, const double *T0, const double *p0,
                          const double *Y, const double *t_end, double h0, cudaStream_t s);
+int launch_reactor_fixed(const Param &p, cb2_reactor *r, int n, int max_steps, int scheme, cudaStream_t s);
 int launch_reactor_advance(const Param &p, cb2_reactor *r, int n, int max_attempts, double rtol, double atol,
                            cudaStream_t s);
 

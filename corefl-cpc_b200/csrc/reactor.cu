@@ -14,7 +14,8 @@
 //                <= 1; next step h * min(5, max(0.2, 0.8 err_last^0.1 err^-0.175)) after the
 //                first accepted step, h * 0.2 on a rejected first step (:664-700)
 // The Rosenbrock coefficients are the published ROK4E table (Tranquilli and Sandu), the same
-// numbers src/Define.h:33-48 lists.
+// numbers src/Define.h:33-48 lists.  k_reactor_fixed runs the fixed-step forms (explicit, EPI, DA,
+// explicit RK3) of the same function.
 #include "chem.cuh"
 #include "launch.h"
 #include "cb200_serve.h"
@@ -239,6 +240,22 @@ __device__ __forceinline__ void warp_solve(SH &S, double *b, int lane) {
   __syncwarp();
 }
 
+// d omega_r / d (rho Y)_c from the rates of progress in S.q1/S.q2 (compute_chem_src_jacobian,
+// src/ConstVolumeReactor.cpp:1739-1758; its diagonal is compute_chem_src_jacobian_diagonal).
+template <int NS>
+__device__ __forceinline__ double jacobian_entry(int r, int c, const ReactorShared<NS> &S, const Mech &m) {
+  double zz = 0;
+  if (S.rhoY[c] > 1e-30) {
+    for (int q = 0; q < m.n_reac; ++q) {
+      const int fr = __ldg(m.stoi_f + q * NS + r), br = __ldg(m.stoi_b + q * NS + r);
+      const int fc = __ldg(m.stoi_f + q * NS + c), bc = __ldg(m.stoi_b + q * NS + c);
+      zz += (br - fr) * (fc * S.q1[q] - bc * S.q2[q]);
+    }
+    zz /= S.rhoY[c];
+  }
+  return zz * 1e+3 * __ldg(m.mw + r);
+}
+
 template <int NS>
 __global__ void __launch_bounds__(32 * kReactorWarps) k_reactor_advance(cb2_reactor *R, int n, Mech m,
                                                                         int max_attempts, double rtol, double atol) {
@@ -266,16 +283,7 @@ __global__ void __launch_bounds__(32 * kReactorWarps) k_reactor_advance(cb2_reac
     // lhs = I - h gamma J
     for (int e = lane; e < NS * NS; e += 32) {
       const int r = e / NS, c = e % NS;
-      double zz = 0;
-      if (S.rhoY[c] > 1e-30) {
-        for (int q = 0; q < m.n_reac; ++q) {
-          const int fr = __ldg(m.stoi_f + q * NS + r), br = __ldg(m.stoi_b + q * NS + r);
-          const int fc = __ldg(m.stoi_f + q * NS + c), bc = __ldg(m.stoi_b + q * NS + c);
-          zz += (br - fr) * (fc * S.q1[q] - bc * S.q2[q]);
-        }
-        zz /= S.rhoY[c];
-      }
-      const double j = zz * 1e+3 * __ldg(m.mw + r);
+      const double j = jacobian_entry<NS>(r, c, S, m);
       S.lhs[e] = r == c ? 1.0 - h * gamma * j : -h * gamma * j;
     }
     __syncwarp();
@@ -361,6 +369,120 @@ __global__ void __launch_bounds__(32 * kReactorWarps) k_reactor_advance(cb2_reac
     R[id].n_reject = n_reject;
     R[id].status = status;
   }
+}
+
+// ---- fixed-step forms, one warp per reactor -------------------------------------------------
+// const_volume_reactor with advance_scheme = 0 (src/ConstVolumeReactor.cpp:403-441: the source,
+// then for implicit_method 1 (EPI, :1779-1793) omega <- (I - dt J)^-1 omega by the same LU, for
+// implicit_method 2 (DA, :1795-1800) omega_l <- omega_l / (1 - dt J_ll); rhoY += omega dt clipped
+// at 0, renormalised to rho when conserve_mass_corefl is set) or advance_scheme = 3 (:708-745, the
+// explicit three-stage Runge-Kutta, two more source evaluations at the stage temperatures); then
+// T by update_t, p, time += dt (:747-763).  dt is the reactor's h, left unchanged.
+template <int NS>
+__global__ void __launch_bounds__(32 * kReactorWarps) k_reactor_fixed(cb2_reactor *R, int n, Mech m, int max_steps,
+                                                                      int scheme, bool conserve) {
+  __shared__ ReactorShared<NS> smem[kReactorWarps];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int id = blockIdx.x * kReactorWarps + wid;
+  if (id >= n) return;  // warp-uniform
+  ReactorShared<NS> &S = smem[wid];
+  double time = R[id].time, T = R[id].T, pr = R[id].p;
+  const double t_end = R[id].t_end, dt = R[id].h;
+  int step = R[id].step, status = R[id].status;
+  if (status || time >= t_end) return;
+  const double rho = R[id].rho, E = R[id].E;
+  if (lane < NS) S.rhoY[lane] = R[id].rhoY[lane];
+  __syncwarp();
+  if (!(dt > 0) || !isfinite(dt)) {
+    if (lane == 0) R[id].status = status | CB2_REACTOR_NONPHYSICAL;
+    return;
+  }
+  const bool gibbs_needed = mech_needs_gibbs(m);
+  for (int a = 0; a < max_steps && time < t_end; ++a) {
+    warp_source<NS>(T, S.rhoY, m, gibbs_needed, S, lane);
+    if (scheme <= CB2_REACTOR_DA) {
+      if (scheme == CB2_REACTOR_EPI) {
+        for (int e = lane; e < NS * NS; e += 32) {
+          const int r = e / NS, c = e % NS;
+          S.lhs[e] = (r == c ? 1.0 : 0.0) - dt * jacobian_entry<NS>(r, c, S, m);
+        }
+        __syncwarp();
+        warp_lu<NS>(S, lane);
+        warp_solve<NS>(S, S.omega, lane);
+      } else if (scheme == CB2_REACTOR_DA) {
+        if (lane < NS) S.omega[lane] /= 1 - dt * jacobian_entry<NS>(lane, lane, S, m);
+        __syncwarp();
+      }
+      if (lane < NS) {
+        const double v = S.rhoY[lane] + S.omega[lane] * dt;
+        S.rhoY[lane] = v < 0 ? 0.0 : v;
+        S.ta[lane] = S.rhoY[lane];
+      }
+      const double sum = warp_sum_ta<NS>(S);
+      if (lane < NS) {
+        S.yk[lane] = S.rhoY[lane] / (conserve ? sum : rho);
+        if (conserve) S.rhoY[lane] = S.yk[lane] * rho;
+      }
+    } else {
+      if (lane < NS) {
+        S.ys[lane] = S.rhoY[lane] + S.omega[lane] * dt;
+        S.yk[lane] = S.ys[lane] / rho;
+        S.ta[lane] = S.yk[lane] / __ldg(m.mw + lane);
+      }
+      double imw = warp_sum_ta<NS>(S);
+      double ts = warp_temperature<NS>(T, imw, E, m, S, lane);
+      warp_source<NS>(ts, S.ys, m, gibbs_needed, S, lane);
+      if (lane < NS) {
+        S.ys[lane] = 0.75 * S.rhoY[lane] + 0.25 * (S.ys[lane] + S.omega[lane] * dt);
+        S.yk[lane] = S.ys[lane] / rho;
+        S.ta[lane] = S.yk[lane] / __ldg(m.mw + lane);
+      }
+      imw = warp_sum_ta<NS>(S);
+      ts = warp_temperature<NS>(ts, imw, E, m, S, lane);
+      warp_source<NS>(ts, S.ys, m, gibbs_needed, S, lane);
+      if (lane < NS) {
+        const double v = (S.rhoY[lane] + 2.0 * (S.ys[lane] + S.omega[lane] * dt)) / 3.0;
+        S.rhoY[lane] = v < 0 ? 0.0 : v;
+        S.yk[lane] = S.rhoY[lane] / rho;
+      }
+    }
+    if (lane < NS) S.ta[lane] = S.yk[lane] / __ldg(m.mw + lane);
+    const double imw = warp_sum_ta<NS>(S);
+    T = warp_temperature<NS>(T, imw, E, m, S, lane);
+    pr = rho * kRu * imw * T;
+    time += dt;
+    ++step;
+    if (!(T > 0) || !isfinite(T)) {
+      status |= CB2_REACTOR_NONPHYSICAL;
+      break;
+    }
+  }
+  __syncwarp();
+  if (lane < NS) R[id].rhoY[lane] = S.rhoY[lane];
+  if (lane == 0) {
+    if (time >= t_end) status |= CB2_REACTOR_DONE;
+    R[id].time = time;
+    R[id].T = T;
+    R[id].p = pr;
+    R[id].step = step;
+    R[id].status = status;
+  }
+}
+
+int launch_reactor_fixed(const Param &p, cb2_reactor *r, int n, int max_steps, int scheme, cudaStream_t s) {
+  const int form = scheme & 0xf;
+  const bool conserve = (scheme & CB2_REACTOR_CONSERVE_MASS) != 0;
+  if (form > CB2_REACTOR_RK3 || (scheme & ~(0xf | CB2_REACTOR_CONSERVE_MASS)) ||
+      (conserve && form == CB2_REACTOR_RK3))
+    return CB2_ERR_INVALID;
+  const unsigned blocks = (unsigned)((n + kReactorWarps - 1) / kReactorWarps);
+  ProfScope prof("reactor_fixed", s);
+  switch (p.n_spec) {
+    case 5: k_reactor_fixed<5><<<blocks, 32 * kReactorWarps, 0, s>>>(r, n, p.mech, max_steps, form, conserve); break;
+    case 9: k_reactor_fixed<9><<<blocks, 32 * kReactorWarps, 0, s>>>(r, n, p.mech, max_steps, form, conserve); break;
+    default: return CB2_ERR_UNSUPPORTED;
+  }
+  return check_launch();
 }
 
 int launch_reactor_setup(const Param &p, cb2_reactor *r, int n, const double *T0, const double *p0,

@@ -48,6 +48,19 @@ int cb2_reactor_setup(cb2_ctx *ctx, cb2_reactor *reactors, int n, const double *
 int cb2_reactor_advance(cb2_ctx *ctx, cb2_reactor *reactors, int n, int max_attempts, double rtol, double atol,
                         void *stream);
 
+/* Fixed-step forms of const_volume_reactor (src/ConstVolumeReactor.cpp:403-441, 708-763). */
+#define CB2_REACTOR_EXPLICIT 0          /* advance_scheme 0, implicit_method 0: rhoY += omega dt  */
+#define CB2_REACTOR_EPI 1               /* implicit_method 1: omega <- (I - dt J)^-1 omega (EPI)   */
+#define CB2_REACTOR_DA 2                /* implicit_method 2: omega_l <- omega_l / (1 - dt J_ll)   */
+#define CB2_REACTOR_RK3 3               /* advance_scheme 3: explicit three-stage Runge-Kutta     */
+#define CB2_REACTOR_CONSERVE_MASS 0x10  /* | with forms 0-2: conserve_mass_corefl = 1             */
+
+/* Advances each unfinished reactor by at most max_steps fixed steps of dt = its h (the h0 of
+ * cb2_reactor_setup, left unchanged) in the form `scheme`, or until it reaches t_end; partial
+ * densities are clipped at 0 after each step as the reference does.  CB2_ERR_INVALID for an
+ * unknown form or CONSERVE_MASS with RK3 (the reference applies it to forms 0-2 only). */
+int cb2_reactor_advance_fixed(cb2_ctx *ctx, cb2_reactor *reactors, int n, int max_steps, int scheme, void *stream);
+
 /* ---- serving: continuous batching of reactors and shock tubes --------------------------- */
 
 #define CB2_REQ_REACTOR 0 /* 0-D constant-volume reactor from (T0, p0, Y) to t_end            */

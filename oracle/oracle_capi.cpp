@@ -218,4 +218,22 @@ void oracle_reactor_run(const cb2_mechanism *m, double T0, double p0, const doub
   out->step = st.step; out->n_reject = st.n_reject; out->status = st.status;
 }
 
+// The same reactor advanced by at most max_steps fixed steps of dt (or to t_end) in the form
+// scheme (CB2_REACTOR_EXPLICIT .. CB2_REACTOR_RK3, optionally | CB2_REACTOR_CONSERVE_MASS).
+void oracle_reactor_run_fixed(const cb2_mechanism *m, double T0, double p0, const double *Y, double t_end,
+                              double dt, int scheme, int max_steps, cb2_reactor *out) {
+  cb2_param_view pv{};
+  pv.mech = m;
+  pv.n_spec = m->n_spec;
+  Param p = make_param(pv);
+  ReactorState st;
+  reactor_setup(p.mech, T0, p0, Y, t_end, dt, st);
+  reactor_advance_fixed(p.mech, st, max_steps, scheme & 0xf, (scheme & CB2_REACTOR_CONSERVE_MASS) != 0);
+  std::memset(out, 0, sizeof(*out));
+  for (int l = 0; l < m->n_spec; ++l) out->rhoY[l] = st.rhoY[l];
+  out->rho = st.rho; out->E = st.E; out->T = st.T; out->p = st.p;
+  out->time = st.time; out->t_end = st.t_end; out->h = st.h; out->err_last = st.err_last;
+  out->step = st.step; out->n_reject = st.n_reject; out->status = st.status;
+}
+
 }  // extern "C"

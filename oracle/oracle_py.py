@@ -230,3 +230,20 @@ def reactor_run(mech, T0, p0, Y, t_end, h0=1e-8, rtol=1e-6, atol=1e-12, max_atte
     f(mech.ptr(), T0, p0, y.ctypes.data_as(C.POINTER(C.c_double)), t_end, h0, rtol, atol,
       min(int(max_attempts), 2**31 - 1), C.byref(out))
     return out
+
+
+def reactor_run_fixed(mech, T0, p0, Y, t_end, dt, scheme, max_steps=10**9):
+    """A 0-D constant-volume reactor from (T0, p0, Y) advanced by the oracle's fixed-step form
+    `scheme` (abi.REACTOR_EXPLICIT .. abi.REACTOR_RK3, optionally | abi.REACTOR_CONSERVE_MASS)
+    with the step dt; returns the state as an abi.Reactor."""
+    import numpy as np
+    lib = load()
+    f = lib.oracle_reactor_run_fixed
+    f.restype = None
+    f.argtypes = [C.POINTER(abi.Mechanism), C.c_double, C.c_double, C.POINTER(C.c_double), C.c_double, C.c_double,
+                  C.c_int, C.c_int, C.POINTER(abi.Reactor)]
+    y = np.ascontiguousarray(Y, dtype=np.float64)
+    out = abi.Reactor()
+    f(mech.ptr(), T0, p0, y.ctypes.data_as(C.POINTER(C.c_double)), t_end, dt, int(scheme),
+      min(int(max_steps), 2**31 - 1), C.byref(out))
+    return out

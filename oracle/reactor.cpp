@@ -9,6 +9,7 @@
 //   temperature  update_t (:1456-1479)
 //   setup        rho = p / (T R_u imw), rhoY = rho Y, E = sum Y h(T) - p / rho (:61-66, :328-336)
 // The ROK4E coefficients are the published table (src/Define.h:33-48 lists the same numbers).
+// reactor_advance_fixed restates the fixed-step forms (explicit, EPI, DA, explicit RK3).
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -209,6 +210,91 @@ void reactor_advance(const Mechanism &m, ReactorState &st, int max_attempts, dou
     } else {
       st.h = h_next;
       ++st.n_reject;
+    }
+  }
+  if (st.time >= st.t_end) st.status |= 1;
+}
+
+// The fixed-step forms of const_volume_reactor with the step st.h: scheme 0 explicit, 1 EPI
+// (omega <- (I - dt J)^-1 omega, src/ConstVolumeReactor.cpp:1779-1793), 2 DA (omega_l <- omega_l /
+// (1 - dt J_ll), :1795-1800) -- advance_scheme = 0 with implicit_method = scheme, the update and
+// the optional conserve_mass_corefl renormalisation of :403-441 -- and 3 the explicit
+// three-stage Runge-Kutta of advance_scheme = 3 (:708-745); then T by update_t, p, time += dt
+// (:747-763).
+void reactor_advance_fixed(const Mechanism &m, ReactorState &st, int max_steps, int scheme, bool conserve) {
+  const int ns = m.n_spec, nr = m.n_reac;
+  if (st.status || st.time >= st.t_end) return;
+  std::vector<double> &rhoY = st.rhoY;
+  std::vector<double> q1(nr), q2(nr), omega(ns), yk(ns), yn(ns), lhs(ns * ns);
+  std::vector<int> piv(ns);
+  const double rho = st.rho, E = st.E, dt = st.h;
+  if (!(dt > 0) || !std::isfinite(dt)) {
+    st.status |= 2;
+    return;
+  }
+  auto jac = [&](int r, int c) {
+    double zz = 0;
+    if (rhoY[c] > 1e-30) {
+      for (int q = 0; q < nr; ++q)
+        zz += (m.stoi_b[q * ns + r] - m.stoi_f[q * ns + r]) *
+              (m.stoi_f[q * ns + c] * q1[q] - m.stoi_b[q * ns + c] * q2[q]);
+      zz /= rhoY[c];
+    }
+    return zz * 1e+3 * m.mw[r];
+  };
+  for (int a = 0; a < max_steps && st.time < st.t_end; ++a) {
+    source(m, st.T, rhoY, q1, q2, omega);
+    double imw = 0;
+    if (scheme <= 2) {
+      if (scheme == 1) {
+        for (int r = 0; r < ns; ++r)
+          for (int c = 0; c < ns; ++c) lhs[r * ns + c] = (r == c ? 1.0 : 0.0) - dt * jac(r, c);
+        lu(lhs, piv, ns);
+        lu_solve(lhs, piv, omega, ns);
+      } else if (scheme == 2) {
+        for (int l = 0; l < ns; ++l) omega[l] /= 1 - dt * jac(l, l);
+      }
+      double sum = 0;
+      for (int l = 0; l < ns; ++l) {
+        rhoY[l] += omega[l] * dt;
+        if (rhoY[l] < 0) rhoY[l] = 0;
+        sum += rhoY[l];
+      }
+      for (int l = 0; l < ns; ++l) {
+        yk[l] = rhoY[l] / (conserve ? sum : rho);
+        if (conserve) rhoY[l] = yk[l] * rho;
+      }
+    } else {
+      for (int l = 0; l < ns; ++l) {
+        yn[l] = rhoY[l] + omega[l] * dt;
+        yk[l] = yn[l] / rho;
+        imw += yk[l] / m.mw[l];
+      }
+      double ts = temperature(m, st.T, imw, yk, E);
+      source(m, ts, yn, q1, q2, omega);
+      imw = 0;
+      for (int l = 0; l < ns; ++l) {
+        yn[l] = 0.75 * rhoY[l] + 0.25 * (yn[l] + omega[l] * dt);
+        yk[l] = yn[l] / rho;
+        imw += yk[l] / m.mw[l];
+      }
+      ts = temperature(m, ts, imw, yk, E);
+      source(m, ts, yn, q1, q2, omega);
+      for (int l = 0; l < ns; ++l) {
+        rhoY[l] = (rhoY[l] + 2.0 * (yn[l] + omega[l] * dt)) / 3.0;
+        if (rhoY[l] < 0) rhoY[l] = 0;
+      }
+      for (int l = 0; l < ns; ++l) yk[l] = rhoY[l] / rho;
+    }
+    imw = 0;
+    for (int l = 0; l < ns; ++l) imw += yk[l] / m.mw[l];
+    st.T = temperature(m, st.T, imw, yk, E);
+    st.p = rho * R_u * imw * st.T;
+    st.time += dt;
+    ++st.step;
+    if (!(st.T > 0) || !std::isfinite(st.T)) {
+      st.status |= 2;
+      break;
     }
   }
   if (st.time >= st.t_end) st.status |= 1;

@@ -7,7 +7,8 @@
 // TEST INFRASTRUCTURE ONLY: built into oracle/_ref/ by oracle/ref_build.py and run by
 // tests/golden/make_mech.py to write tests/golden/h2_reactor_runs.json.
 //
-// Usage (from a directory holding ./input/<files>): dump_reactor <setup-file> <out.json> <n>
+// Usage (from a directory holding ./input/<files>): dump_reactor <setup-file> <out.json> <n> [fixed]
+// With "fixed", every case runs the fixed-step forms instead (advance_fixed below).
 // Case 0 is the reference's example (T0 = 1000 K, p0 = 202650 Pa, X = 0.295775 H2 /
 // 0.147887 O2 / rest N2, 1.2 ms); cases 1..n-1 are seeded (T0, p0, phi) requests to 1 ms.
 #include <algorithm>
@@ -106,8 +107,64 @@ static void advance(const cfd::Species &sp, const cfd::Reaction &re, Run &r, int
   }
 }
 
+// The fixed-step forms of const_volume_reactor (src/ConstVolumeReactor.cpp:403-441, 708-763), with
+// the reference's own cfd::EPI / cfd::DA and Jacobians: scheme 0 explicit, 1 EPI (full Jacobian,
+// LU), 2 DA (diagonal Jacobian) -- advance_scheme = 0 with implicit_method = scheme, optionally
+// with conserve_mass_corefl -- and 3 the explicit three-stage Runge-Kutta (advance_scheme = 3).
+static void advance_fixed(const cfd::Species &sp, const cfd::Reaction &re, Run &r, int max_steps, real dt, int scheme,
+                          bool conserve) {
+  const int ns = sp.n_spec, nr = re.n_reac;
+  std::vector<real> q1(nr), q2(nr), od(ns), om(ns), yk(ns), yn(ns);
+  for (int a = 0; a < max_steps && r.time < r.t_end; ++a) {
+    cfd::compute_src(0, r.T, sp, re, r.rhoY, q1, q2, od, om);
+    real imw = 0;
+    if (scheme <= 2) {
+      if (scheme == 1) cfd::EPI(cfd::compute_chem_src_jacobian(r.rhoY, sp, re, q1, q2), sp, dt, om);
+      else if (scheme == 2) cfd::DA(cfd::compute_chem_src_jacobian_diagonal(r.rhoY, sp, re, q1, q2), sp, dt, om);
+      real sum = 0;
+      for (int l = 0; l < ns; ++l) {
+        r.rhoY[l] += om[l] * dt;
+        if (r.rhoY[l] < 0) r.rhoY[l] = 0;
+        sum += r.rhoY[l];
+      }
+      for (int l = 0; l < ns; ++l) {
+        yk[l] = r.rhoY[l] / (conserve ? sum : r.rho);
+        if (conserve) r.rhoY[l] = yk[l] * r.rho;
+      }
+    } else {
+      for (int l = 0; l < ns; ++l) {
+        yn[l] = r.rhoY[l] + om[l] * dt;
+        yk[l] = yn[l] / r.rho;
+        imw += yk[l] / sp.mw[l];
+      }
+      real ts = cfd::update_t(r.T, imw, sp, yk, r.E);
+      cfd::compute_src(0, ts, sp, re, yn, q1, q2, od, om);
+      imw = 0;
+      for (int l = 0; l < ns; ++l) {
+        yn[l] = 0.75 * r.rhoY[l] + 0.25 * (yn[l] + om[l] * dt);
+        yk[l] = yn[l] / r.rho;
+        imw += yk[l] / sp.mw[l];
+      }
+      ts = cfd::update_t(ts, imw, sp, yk, r.E);
+      cfd::compute_src(0, ts, sp, re, yn, q1, q2, od, om);
+      for (int l = 0; l < ns; ++l) {
+        r.rhoY[l] = (r.rhoY[l] + 2.0 * (yn[l] + om[l] * dt)) / 3.0;
+        if (r.rhoY[l] < 0) r.rhoY[l] = 0;
+      }
+      for (int l = 0; l < ns; ++l) yk[l] = r.rhoY[l] / r.rho;
+    }
+    imw = 0;
+    for (int l = 0; l < ns; ++l) imw += yk[l] / sp.mw[l];
+    r.T = cfd::update_t(r.T, imw, sp, yk, r.E);
+    r.p = r.rho * cfd::R_u * imw * r.T;
+    r.time += dt;
+    ++r.step;
+  }
+}
+
 int main(int argc, char **argv) {
   if (argc < 4) return 2;
+  const bool fixed = argc > 4 && std::string(argv[4]) == "fixed";
   cfd::Parameter parameter{std::string(argv[1])};
   cfd::Species sp(parameter);
   cfd::Reaction re(parameter, sp);
@@ -165,10 +222,31 @@ int main(int argc, char **argv) {
     std::fprintf(out, "%s{\"T0\": %.17g, \"p0\": %.17g, \"t_end\": %.17g, \"Y\": [", c ? ",\n" : "", T0, p0, t_end);
     for (int l = 0; l < ns; ++l) std::fprintf(out, "%s%.17g", l ? ", " : "", y[l]);
     std::fprintf(out, "],\n");
-    advance(sp, re, r, 8, rtol, atol);
-    dump("after_8_attempts", false);
-    advance(sp, re, r, 1000000, rtol, atol);
-    dump("final", true);
+    if (fixed) {
+      // each form from the same initial state: (scheme, conserve_mass, dt, t_end)
+      const Run r0 = r;
+      const struct { int scheme, conserve; real dt, t_end; const char *tag; } forms[] = {
+          {0, 0, 1e-9, 2e-5, "explicit"}, {0, 1, 1e-9, 2e-5, "explicit_conserve"}, {1, 0, 1e-7, 4e-4, "epi"},
+          {1, 1, 1e-7, 4e-4, "epi_conserve"}, {2, 0, 1e-9, 5e-5, "da"}, {3, 0, 1e-9, 2e-5, "rk3"}};
+      const int nf = sizeof(forms) / sizeof(forms[0]);
+      for (int f = 0; f < nf; ++f) {
+        r = r0;
+        r.t_end = forms[f].t_end;
+        r.h = forms[f].dt;
+        std::fprintf(out, "\"%s\": {\"scheme\": %d, \"conserve_mass\": %d, \"dt\": %.17g, \"t_end\": %.17g,\n",
+                     forms[f].tag, forms[f].scheme, forms[f].conserve, forms[f].dt, forms[f].t_end);
+        advance_fixed(sp, re, r, 100, forms[f].dt, forms[f].scheme, forms[f].conserve);
+        dump("after_100_steps", false);
+        advance_fixed(sp, re, r, 100000000, forms[f].dt, forms[f].scheme, forms[f].conserve);
+        dump("final", true);
+        std::fprintf(out, "}%s", f + 1 < nf ? ",\n" : "");
+      }
+    } else {
+      advance(sp, re, r, 8, rtol, atol);
+      dump("after_8_attempts", false);
+      advance(sp, re, r, 1000000, rtol, atol);
+      dump("final", true);
+    }
     std::fprintf(out, "}");
   }
   std::fprintf(out, "\n]\n}\n");

@@ -25,6 +25,11 @@ oracle/ref_build.py) on the reference's example data files and keeps its JSON ou
                    and Newton through the adaptive ROK4E sequence (RTol 1e-6, ATol 1e-12,
                    first step 1e-8): the reference's example case to 1.2 ms and 8 seeded
                    (T0, p0, phi) requests to 1 ms, each after 8 step attempts and at the end
+  h2_reactor_fixed_runs.json : the same reactors (the example case and 2 seeded requests) with
+                   the fixed-step forms of const_volume_reactor, the reference's own EPI and DA:
+                   explicit and EPI (each also with conserve_mass_corefl), DA and the explicit
+                   three-stage Runge-Kutta (dt 1e-9 to 20 us, DA to 50 us, EPI dt 1e-7 to 0.4 ms), after 100
+                   steps and at the end
 Usage: python tests/golden/make_mech.py [/path/to/reference]  (default: oracle/ref_build.py's
 reference_dir())
 """
@@ -71,6 +76,7 @@ def main(ref):
     print(run(ref, "h2_li2004.json", files, 7))
     print(run(ref, "h2_chem_states.json", files, 7, prog="dump_chem", extra=("48",)))
     print(run(ref, "h2_reactor_runs.json", files, 7, prog="dump_reactor", extra=("9",)))
+    print(run(ref, "h2_reactor_fixed_runs.json", files, 7, prog="dump_reactor", extra=("3", "fixed")))
     files_2t = dict(files, two_temperature_file="example/squareCylinder2D_M10_air5_dns/input/chemistry/"
                                                 "two_temperature.dat")
     print(run(ref, "h2_two_temperature.json", files_2t, 7, prog="dump_2t", extra=("40",)))
