@@ -66,6 +66,7 @@ def load():
         "cb2_reactor_setup": (C.c_int, [vp, vp, C.c_int, vp, vp, vp, vp, C.c_double, vp]),
         "cb2_reactor_advance": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_double, C.c_double, vp]),
         "cb2_reactor_advance_fixed": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, vp]),
+        "cb2_reactor_advance_krylov": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_double, C.c_double, vp]),
         "cb2_metrics": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp]),
         "cb2_write_flowfield": (C.c_int, [vp, C.c_char_p, P(vp), P(C.c_char_p), C.c_int, C.c_double, vp]),
         "cb2_read_flowfield": (C.c_int, [vp, C.c_char_p, P(C.c_char_p), P(C.c_double), vp]),
@@ -220,6 +221,11 @@ class Context:
     def reactor_advance(self, reactors, n, max_attempts, rtol=1e-6, atol=1e-12, stream=None):
         check(self.lib.cb2_reactor_advance(self.h, reactors, n, max_attempts, rtol, atol, stream),
               "cb2_reactor_advance")
+
+    def reactor_advance_krylov(self, reactors, n, max_attempts, rtol=1e-6, atol=1e-12, stream=None):
+        """reactor_advance with the Jacobian projected on an Arnoldi basis (build_arnoldi = 1)."""
+        check(self.lib.cb2_reactor_advance_krylov(self.h, reactors, n, max_attempts, rtol, atol, stream),
+              "cb2_reactor_advance_krylov")
 
     def reactor_advance_fixed(self, reactors, n, max_steps, scheme, stream=None):
         """At most max_steps fixed steps (dt = each reactor's h) of the form `scheme`

@@ -1306,6 +1306,17 @@ int cb2_reactor_advance(cb2_ctx *ctx, cb2_reactor *reactors, int n, int max_atte
   return launch_reactor_advance(ctx->p, reactors, n, max_attempts, rtol, atol, (cudaStream_t)stream);
 }
 
+int cb2_reactor_advance_krylov(cb2_ctx *ctx, cb2_reactor *reactors, int n, int max_attempts, double rtol,
+                               double atol, void *stream) {
+  if (!ctx || !reactors || n < 0 || max_attempts < 1 || !(rtol > 0) || !(atol > 0)) return CB2_ERR_INVALID;
+  if (two_temperature(ctx)) return CB2_ERR_UNSUPPORTED;
+  if (ctx->p.n_spec == 0) return CB2_ERR_UNSUPPORTED;
+  if (n == 0) return CB2_OK;
+  ProfGuard pg(ctx);
+  ++ctx->n_launch;
+  return launch_reactor_advance(ctx->p, reactors, n, max_attempts, rtol, atol, (cudaStream_t)stream, true);
+}
+
 int cb2_reactor_advance_fixed(cb2_ctx *ctx, cb2_reactor *reactors, int n, int max_steps, int scheme, void *stream) {
   if (!ctx || !reactors || n < 0 || max_steps < 1) return CB2_ERR_INVALID;
   if (two_temperature(ctx)) return CB2_ERR_UNSUPPORTED;

@@ -131,6 +131,6 @@ int launch_reactor_setup(const Param &p, cb2_reactor *r, int n, const double *T0
                          const double *Y, const double *t_end, double h0, cudaStream_t s);
 int launch_reactor_fixed(const Param &p, cb2_reactor *r, int n, int max_steps, int scheme, cudaStream_t s);
 int launch_reactor_advance(const Param &p, cb2_reactor *r, int n, int max_attempts, double rtol, double atol,
-                           cudaStream_t s);
+                           cudaStream_t s, bool krylov = false);
 
 }  // namespace cb2

@@ -14,8 +14,11 @@
 //                <= 1; next step h * min(5, max(0.2, 0.8 err_last^0.1 err^-0.175)) after the
 //                first accepted step, h * 0.2 on a rejected first step (:664-700)
 // The Rosenbrock coefficients are the published ROK4E table (Tranquilli and Sandu), the same
-// numbers src/Define.h:33-48 lists.  k_reactor_fixed runs the fixed-step forms (explicit, EPI, DA,
+// numbers src/Define.h:33-48 lists.  The Krylov instantiation replaces J by its Arnoldi
+// projection (build_arnoldi = 1, Krylov limit n_spec).  k_reactor_fixed runs the fixed-step forms (explicit, EPI, DA,
 // explicit RK3) of the same function.
+#include <type_traits>
+
 #include "chem.cuh"
 #include "launch.h"
 #include "cb200_serve.h"
@@ -41,8 +44,7 @@ constexpr int kReactorThreads = 64;
 
 // Forward and back substitution with the LU factors of warp_lu (row pivots in piv), as
 // lu_to_solution does (src/ConstVolumeReactor.cpp:1835-1857).
-template <int N>
-__device__ __forceinline__ void lu_solve(const double *a, const int *piv, double *b) {
+__device__ __forceinline__ void lu_solve_n(const double *a, const int *piv, double *b, int N) {
   for (int r = 0; r < N; ++r) {
     const int t = piv[r];
     if (t != r) {
@@ -58,6 +60,11 @@ __device__ __forceinline__ void lu_solve(const double *a, const int *piv, double
     for (int t = r + 1; t < N; ++t) b[r] -= a[r * N + t] * b[t];
     b[r] /= a[r * N + r];
   }
+}
+
+template <int N>
+__device__ __forceinline__ void lu_solve(const double *a, const int *piv, double *b) {
+  lu_solve_n(a, piv, b, N);
 }
 
 template <int NS>
@@ -197,11 +204,12 @@ __device__ __forceinline__ double warp_sum_ta(ReactorShared<NS> &S) {
   return v;
 }
 
-// LU of S.lhs with row pivoting in the Crout ordering of lu_decomp (src/ConstVolumeReactor.cpp:
-// 1802-1833: column n of L, pivot, row n of U, scale), the rows or columns of each step on
-// separate lanes; the pivot search keeps the serial rule (the first largest |.|).
-template <int N, typename SH>
-__device__ __forceinline__ void warp_lu(SH &S, int lane) {
+// LU of the n x n matrix S.lhs with row pivoting in the Crout ordering of lu_decomp
+// (src/ConstVolumeReactor.cpp:1802-1833: column c of L, pivot, row c of U, scale), the rows or
+// columns of each step on separate lanes; the pivot search keeps the serial rule (the first
+// largest |.|).
+template <typename SH>
+__device__ __forceinline__ void warp_lu_n(SH &S, int N, int lane) {
   double *a = S.lhs;
   for (int n = 0; n < N; ++n) {
     if (lane >= n && lane < N) {
@@ -232,11 +240,104 @@ __device__ __forceinline__ void warp_lu(SH &S, int lane) {
   }
 }
 
+template <int N, typename SH>
+__device__ __forceinline__ void warp_lu(SH &S, int lane) {
+  warp_lu_n(S, N, lane);
+}
+
 // Solves LU b = rhs in place on lane 0 (the substitutions are serial), then shares it.
 template <int N, typename SH>
 __device__ __forceinline__ void warp_solve(SH &S, double *b, int lane) {
   __syncwarp();
   if (lane == 0) lu_solve<N>(S.lhs, S.piv, b);
+  __syncwarp();
+}
+
+// ---- the Krylov form (build_arnoldi = 1) ---------------------------------------------------
+template <int NS>
+struct KrylovShared : ReactorShared<NS> {
+  double Q[NS * NS], H[NS * NS], f0[NS], w[NS], g[NS], sol[NS], f[NS];
+};
+
+// sum over s < NS of a[s] * b[s] in index order (gxl::vec_dot), the same value on every lane
+template <int NS>
+__device__ __forceinline__ double warp_dot(ReactorShared<NS> &S, const double *a, const double *b, int lane) {
+  if (lane < NS) S.ta[lane] = a[lane] * b[lane];
+  return warp_sum_ta<NS>(S);
+}
+
+// buildArnoldi (src/ConstVolumeReactor.cpp:1858-1930) with the Krylov limit NS and minimum 4, from
+// f0 = S.f0 at (T, S.rhoY): q0 = f0 / |f0| (e_0 if |f0| < 1e-30); column c: w = (omega(T', rhoY +
+// eps q_c) - f0) / eps, eps = 1e-6 (1 + |rhoY|), T' the Newton temperature of the perturbed state;
+// modified Gram-Schmidt into H(0..c, c); H(c+1, c) = |w|.  Returns the Krylov dimension.
+template <int NS>
+__device__ int warp_arnoldi(double T, double rho, double E, const Mech &m, bool gibbs_needed, KrylovShared<NS> &S,
+                            int lane) {
+  for (int e = lane; e < NS * NS; e += 32) S.Q[e] = S.H[e] = 0.0;
+  __syncwarp();
+  const double eps = 1e-6 * (1 + sqrt(fmax(warp_dot<NS>(S, S.rhoY, S.rhoY, lane), 0.0)));
+  const double nf = sqrt(fmax(warp_dot<NS>(S, S.f0, S.f0, lane), 0.0));
+  if (lane < NS) S.Q[lane] = nf < 1e-30 ? (lane == 0 ? 1.0 : 0.0) : S.f0[lane] / nf;
+  __syncwarp();
+  int kd = 1;
+  for (int col = 0; col < NS; ++col) {
+    if (lane < NS) {
+      S.ys[lane] = S.rhoY[lane] + eps * S.Q[col * NS + lane];
+      S.yk[lane] = S.ys[lane] / rho;
+      S.ta[lane] = S.yk[lane] / __ldg(m.mw + lane);
+    }
+    const double imw = warp_sum_ta<NS>(S);
+    const double ts = warp_temperature<NS>(T, imw, E, m, S, lane);
+    warp_source<NS>(ts, S.ys, m, gibbs_needed, S, lane);
+    if (lane < NS) S.w[lane] = (S.omega[lane] - S.f0[lane]) / eps;
+    __syncwarp();
+    for (int row = 0; row <= col; ++row) {
+      const double hij = warp_dot<NS>(S, S.Q + row * NS, S.w, lane);
+      if (lane == 0) S.H[row * NS + col] = hij;
+      if (lane < NS) S.w[lane] -= hij * S.Q[row * NS + lane];
+      __syncwarp();
+    }
+    double hn = sqrt(fmax(warp_dot<NS>(S, S.w, S.w, lane), 0.0));
+    if (col + 1 < NS && lane == 0) S.H[(col + 1) * NS + col] = hn;
+    if (col + 1 < 4) {
+      if (hn < 1e-30) hn = 1e-30;
+      if (lane < NS) S.Q[(col + 1) * NS + lane] = S.w[lane] / hn;
+      __syncwarp();
+      kd = col + 2;
+      continue;
+    }
+    if (hn > 1e-30 && col + 1 < NS) {
+      if (lane < NS) S.Q[(col + 1) * NS + lane] = S.w[lane] / hn;
+      __syncwarp();
+      kd = col + 2;
+    } else {
+      kd = col + 1;
+      break;
+    }
+  }
+  __syncwarp();
+  return kd;
+}
+
+// One stage on the Krylov basis: g = Q^T f, sol = (I - h gamma H)^-1 g (LU in S.lhs), d = g - sol
+// (stages 1 and 2) or sol - g (stages 3 and 4, as the reference forms it), k = f - Q d.
+template <int NS>
+__device__ __forceinline__ void warp_krylov_stage(KrylovShared<NS> &S, int kd, bool flip, double *k, int lane) {
+  for (int q = 0; q < kd; ++q) {
+    const double d = warp_dot<NS>(S, S.Q + q * NS, S.f, lane);
+    if (lane == 0) S.g[q] = S.sol[q] = d;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    lu_solve_n(S.lhs, S.piv, S.sol, kd);
+    for (int q = 0; q < kd; ++q) S.g[q] = flip ? S.sol[q] - S.g[q] : S.g[q] - S.sol[q];
+  }
+  __syncwarp();
+  if (lane < NS) {
+    double sum = 0;
+    for (int q = 0; q < kd; ++q) sum += S.Q[q * NS + lane] * S.g[q];
+    k[lane] = S.f[lane] - sum;
+  }
   __syncwarp();
 }
 
@@ -256,15 +357,16 @@ __device__ __forceinline__ double jacobian_entry(int r, int c, const ReactorShar
   return zz * 1e+3 * __ldg(m.mw + r);
 }
 
-template <int NS>
+template <int NS, bool KRYLOV>
 __global__ void __launch_bounds__(32 * kReactorWarps) k_reactor_advance(cb2_reactor *R, int n, Mech m,
                                                                         int max_attempts, double rtol, double atol) {
   using namespace rok4e;
-  __shared__ ReactorShared<NS> smem[kReactorWarps];
+  using SH = std::conditional_t<KRYLOV, KrylovShared<NS>, ReactorShared<NS>>;
+  __shared__ SH smem[kReactorWarps];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int id = blockIdx.x * kReactorWarps + wid;
   if (id >= n) return;  // warp-uniform
-  ReactorShared<NS> &S = smem[wid];
+  SH &S = smem[wid];
   double time = R[id].time, t_end = R[id].t_end, hh = R[id].h, err_last = R[id].err_last, T = R[id].T;
   double pr = R[id].p;
   int step = R[id].step, n_reject = R[id].n_reject, status = R[id].status;
@@ -280,48 +382,97 @@ __global__ void __launch_bounds__(32 * kReactorWarps) k_reactor_advance(cb2_reac
       status |= CB2_REACTOR_NONPHYSICAL;
       break;
     }
-    // lhs = I - h gamma J
-    for (int e = lane; e < NS * NS; e += 32) {
-      const int r = e / NS, c = e % NS;
-      const double j = jacobian_entry<NS>(r, c, S, m);
-      S.lhs[e] = r == c ? 1.0 - h * gamma * j : -h * gamma * j;
+    double imw = 0, ts = 0;
+    if constexpr (KRYLOV) {
+      // build_arnoldi = 1 (src/ConstVolumeReactor.cpp:446-594)
+      if (lane < NS) S.f0[lane] = S.omega[lane];
+      __syncwarp();
+      const int kd = warp_arnoldi<NS>(T, rho, E, m, gibbs_needed, S, lane);
+      for (int e = lane; e < kd * kd; e += 32) {
+        const int i = e / kd, j = e % kd;
+        const double hv = S.H[i * NS + j];
+        S.lhs[e] = i == j ? 1.0 - h * gamma * hv : -h * gamma * hv;
+      }
+      __syncwarp();
+      warp_lu_n(S, kd, lane);
+      if (lane < NS) S.f[lane] = S.f0[lane];
+      __syncwarp();
+      warp_krylov_stage<NS>(S, kd, false, S.k1, lane);
+      if (lane < NS) {
+        S.ys[lane] = S.rhoY[lane] + h * a21 * S.k1[lane];
+        S.yk[lane] = S.ys[lane] / rho;
+        S.ta[lane] = S.yk[lane] / __ldg(m.mw + lane);
+      }
+      imw = warp_sum_ta<NS>(S);
+      ts = warp_temperature<NS>(T, imw, E, m, S, lane);
+      warp_source<NS>(ts, S.ys, m, gibbs_needed, S, lane);
+      if (lane < NS) S.f[lane] = S.omega[lane] + g21 * S.k1[lane];
+      __syncwarp();
+      warp_krylov_stage<NS>(S, kd, false, S.k2, lane);
+      if (lane < NS) S.k2[lane] = S.k2[lane] - g21 * S.k1[lane];
+      __syncwarp();
+      if (lane < NS) {
+        S.ys[lane] = S.rhoY[lane] + h * (a31 * S.k1[lane] + a32 * S.k2[lane]);
+        S.yk[lane] = S.ys[lane] / rho;
+        S.ta[lane] = S.yk[lane] / __ldg(m.mw + lane);
+      }
+      imw = warp_sum_ta<NS>(S);
+      ts = warp_temperature<NS>(ts, imw, E, m, S, lane);
+      warp_source<NS>(ts, S.ys, m, gibbs_needed, S, lane);
+      if (lane < NS) S.f[lane] = S.omega[lane] + g31 * S.k1[lane] + g32 * S.k2[lane];
+      __syncwarp();
+      warp_krylov_stage<NS>(S, kd, true, S.k3, lane);
+      if (lane < NS) S.k3[lane] = S.k3[lane] - g31 * S.k1[lane] - g32 * S.k2[lane];
+      __syncwarp();
+      if (lane < NS) S.f[lane] = S.omega[lane] + g41 * S.k1[lane] + g42 * S.k2[lane] + g43 * S.k3[lane];
+      __syncwarp();
+      warp_krylov_stage<NS>(S, kd, true, S.k4, lane);
+      if (lane < NS) S.k4[lane] = S.k4[lane] - g41 * S.k1[lane] - g42 * S.k2[lane] - g43 * S.k3[lane];
+      __syncwarp();
+    } else {
+      // lhs = I - h gamma J
+      for (int e = lane; e < NS * NS; e += 32) {
+        const int r = e / NS, c = e % NS;
+        const double j = jacobian_entry<NS>(r, c, S, m);
+        S.lhs[e] = r == c ? 1.0 - h * gamma * j : -h * gamma * j;
+      }
+      __syncwarp();
+      warp_lu<NS>(S, lane);
+      // stage 1
+      if (lane < NS) S.k1[lane] = S.omega[lane];
+      warp_solve<NS>(S, S.k1, lane);
+      // stage 2
+      if (lane < NS) {
+        S.ys[lane] = S.rhoY[lane] + h * a21 * S.k1[lane];
+        S.yk[lane] = S.ys[lane] / rho;
+        S.ta[lane] = S.yk[lane] / __ldg(m.mw + lane);
+      }
+      imw = warp_sum_ta<NS>(S);
+      ts = warp_temperature<NS>(T, imw, E, m, S, lane);
+      warp_source<NS>(ts, S.ys, m, gibbs_needed, S, lane);
+      if (lane < NS) S.k2[lane] = S.omega[lane] + g21 * S.k1[lane];
+      warp_solve<NS>(S, S.k2, lane);
+      if (lane < NS) S.k2[lane] -= g21 * S.k1[lane];
+      __syncwarp();
+      // stage 3
+      if (lane < NS) {
+        S.ys[lane] = S.rhoY[lane] + h * (a31 * S.k1[lane] + a32 * S.k2[lane]);
+        S.yk[lane] = S.ys[lane] / rho;
+        S.ta[lane] = S.yk[lane] / __ldg(m.mw + lane);
+      }
+      imw = warp_sum_ta<NS>(S);
+      ts = warp_temperature<NS>(ts, imw, E, m, S, lane);
+      warp_source<NS>(ts, S.ys, m, gibbs_needed, S, lane);
+      if (lane < NS) S.k3[lane] = S.omega[lane] + g31 * S.k1[lane] + g32 * S.k2[lane];
+      warp_solve<NS>(S, S.k3, lane);
+      if (lane < NS) S.k3[lane] -= g31 * S.k1[lane] + g32 * S.k2[lane];
+      __syncwarp();
+      // stage 4 (the source of stage 3 again)
+      if (lane < NS) S.k4[lane] = S.omega[lane] + g41 * S.k1[lane] + g42 * S.k2[lane] + g43 * S.k3[lane];
+      warp_solve<NS>(S, S.k4, lane);
+      if (lane < NS) S.k4[lane] -= g41 * S.k1[lane] + g42 * S.k2[lane] + g43 * S.k3[lane];
+      __syncwarp();
     }
-    __syncwarp();
-    warp_lu<NS>(S, lane);
-    // stage 1
-    if (lane < NS) S.k1[lane] = S.omega[lane];
-    warp_solve<NS>(S, S.k1, lane);
-    // stage 2
-    if (lane < NS) {
-      S.ys[lane] = S.rhoY[lane] + h * a21 * S.k1[lane];
-      S.yk[lane] = S.ys[lane] / rho;
-      S.ta[lane] = S.yk[lane] / __ldg(m.mw + lane);
-    }
-    double imw = warp_sum_ta<NS>(S);
-    double ts = warp_temperature<NS>(T, imw, E, m, S, lane);
-    warp_source<NS>(ts, S.ys, m, gibbs_needed, S, lane);
-    if (lane < NS) S.k2[lane] = S.omega[lane] + g21 * S.k1[lane];
-    warp_solve<NS>(S, S.k2, lane);
-    if (lane < NS) S.k2[lane] -= g21 * S.k1[lane];
-    __syncwarp();
-    // stage 3
-    if (lane < NS) {
-      S.ys[lane] = S.rhoY[lane] + h * (a31 * S.k1[lane] + a32 * S.k2[lane]);
-      S.yk[lane] = S.ys[lane] / rho;
-      S.ta[lane] = S.yk[lane] / __ldg(m.mw + lane);
-    }
-    imw = warp_sum_ta<NS>(S);
-    ts = warp_temperature<NS>(ts, imw, E, m, S, lane);
-    warp_source<NS>(ts, S.ys, m, gibbs_needed, S, lane);
-    if (lane < NS) S.k3[lane] = S.omega[lane] + g31 * S.k1[lane] + g32 * S.k2[lane];
-    warp_solve<NS>(S, S.k3, lane);
-    if (lane < NS) S.k3[lane] -= g31 * S.k1[lane] + g32 * S.k2[lane];
-    __syncwarp();
-    // stage 4 (the source of stage 3 again)
-    if (lane < NS) S.k4[lane] = S.omega[lane] + g41 * S.k1[lane] + g42 * S.k2[lane] + g43 * S.k3[lane];
-    warp_solve<NS>(S, S.k4, lane);
-    if (lane < NS) S.k4[lane] -= g41 * S.k1[lane] + g42 * S.k2[lane] + g43 * S.k3[lane];
-    __syncwarp();
     // embedded error estimate and step control
     if (lane < NS) {
       S.ys[lane] = S.rhoY[lane] + h * (b1 * S.k1[lane] + b2 * S.k2[lane] + b4 * S.k4[lane]);
@@ -498,12 +649,15 @@ int launch_reactor_setup(const Param &p, cb2_reactor *r, int n, const double *T0
 }
 
 int launch_reactor_advance(const Param &p, cb2_reactor *r, int n, int max_attempts, double rtol, double atol,
-                           cudaStream_t s) {
+                           cudaStream_t s, bool krylov) {
   const unsigned blocks = (unsigned)((n + kReactorWarps - 1) / kReactorWarps);
-  ProfScope prof("reactor_advance", s);
-  switch (p.n_spec) {
-    case 5: k_reactor_advance<5><<<blocks, 32 * kReactorWarps, 0, s>>>(r, n, p.mech, max_attempts, rtol, atol); break;
-    case 9: k_reactor_advance<9><<<blocks, 32 * kReactorWarps, 0, s>>>(r, n, p.mech, max_attempts, rtol, atol); break;
+  ProfScope prof(krylov ? "reactor_advance_krylov" : "reactor_advance", s);
+  const unsigned th = 32 * kReactorWarps;
+  switch (p.n_spec * 2 + (krylov ? 1 : 0)) {
+    case 10: k_reactor_advance<5, false><<<blocks, th, 0, s>>>(r, n, p.mech, max_attempts, rtol, atol); break;
+    case 11: k_reactor_advance<5, true><<<blocks, th, 0, s>>>(r, n, p.mech, max_attempts, rtol, atol); break;
+    case 18: k_reactor_advance<9, false><<<blocks, th, 0, s>>>(r, n, p.mech, max_attempts, rtol, atol); break;
+    case 19: k_reactor_advance<9, true><<<blocks, th, 0, s>>>(r, n, p.mech, max_attempts, rtol, atol); break;
     default: return CB2_ERR_UNSUPPORTED;
   }
   return check_launch();

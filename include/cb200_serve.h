@@ -48,6 +48,14 @@ int cb2_reactor_setup(cb2_ctx *ctx, cb2_reactor *reactors, int n, const double *
 int cb2_reactor_advance(cb2_ctx *ctx, cb2_reactor *reactors, int n, int max_attempts, double rtol, double atol,
                         void *stream);
 
+/* cb2_reactor_advance with build_arnoldi = 1 (src/ConstVolumeReactor.cpp:446-594, buildArnoldi
+ * :1858-1930): J replaced by its projection on an Arnoldi basis of finite-difference products
+ * (Krylov limit n_spec, minimum 4; n_spec extra source evaluations per attempt).  Stages 3 and 4
+ * take the projected correction with the opposite sign to stages 1 and 2, as the reference does;
+ * its steps shrink until they stall short of t_end on the H2/air reactors. */
+int cb2_reactor_advance_krylov(cb2_ctx *ctx, cb2_reactor *reactors, int n, int max_attempts, double rtol,
+                               double atol, void *stream);
+
 /* Fixed-step forms of const_volume_reactor (src/ConstVolumeReactor.cpp:403-441, 708-763). */
 #define CB2_REACTOR_EXPLICIT 0          /* advance_scheme 0, implicit_method 0: rhoY += omega dt  */
 #define CB2_REACTOR_EPI 1               /* implicit_method 1: omega <- (I - dt J)^-1 omega (EPI)   */

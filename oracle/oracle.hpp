@@ -163,7 +163,8 @@ struct ReactorState {
 };
 void reactor_setup(const Mechanism &m, double T0, double p0, const double *Y, double t_end, double h0,
                    ReactorState &st);
-void reactor_advance(const Mechanism &m, ReactorState &st, int max_attempts, double rtol, double atol);
+void reactor_advance(const Mechanism &m, ReactorState &st, int max_attempts, double rtol, double atol,
+                     bool krylov = false);
 void reactor_advance_fixed(const Mechanism &m, ReactorState &st, int max_steps, int scheme, bool conserve);
 
 }  // namespace oracle

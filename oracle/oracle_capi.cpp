@@ -200,17 +200,18 @@ void oracle_chemistry_source_2t(const cb2_mechanism *m, double rho, double t, do
   chemistry_source_2t(p.mech, rho, t, tve, y, omega, omega_d);
 }
 
-// A 0-D reactor from (T0, p0, Y) advanced by at most max_attempts ROK4E attempts (or to t_end);
+// A 0-D reactor from (T0, p0, Y) advanced by at most max_attempts ROK4E attempts (or to t_end),
+// with the full Jacobian or (krylov != 0) on the Arnoldi basis;
 // the state is returned in the cb2_reactor layout of include/cb200_serve.h.
 void oracle_reactor_run(const cb2_mechanism *m, double T0, double p0, const double *Y, double t_end, double h0,
-                        double rtol, double atol, int max_attempts, cb2_reactor *out) {
+                        double rtol, double atol, int max_attempts, cb2_reactor *out, int krylov) {
   cb2_param_view pv{};
   pv.mech = m;
   pv.n_spec = m->n_spec;
   Param p = make_param(pv);
   ReactorState st;
   reactor_setup(p.mech, T0, p0, Y, t_end, h0, st);
-  reactor_advance(p.mech, st, max_attempts, rtol, atol);
+  reactor_advance(p.mech, st, max_attempts, rtol, atol, krylov != 0);
   std::memset(out, 0, sizeof(*out));
   for (int l = 0; l < m->n_spec; ++l) out->rhoY[l] = st.rhoY[l];
   out->rho = st.rho; out->E = st.E; out->T = st.T; out->p = st.p;

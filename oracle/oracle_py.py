@@ -216,7 +216,7 @@ def nasa7_h_cp(mech, t):
     return h, cp
 
 
-def reactor_run(mech, T0, p0, Y, t_end, h0=1e-8, rtol=1e-6, atol=1e-12, max_attempts=10**9):
+def reactor_run(mech, T0, p0, Y, t_end, h0=1e-8, rtol=1e-6, atol=1e-12, max_attempts=10**9, krylov=False):
     """A 0-D constant-volume reactor from (T0, p0, Y) advanced by the oracle's ROK4E integrator;
     returns the state as an abi.Reactor."""
     import numpy as np
@@ -224,11 +224,11 @@ def reactor_run(mech, T0, p0, Y, t_end, h0=1e-8, rtol=1e-6, atol=1e-12, max_atte
     f = lib.oracle_reactor_run
     f.restype = None
     f.argtypes = [C.POINTER(abi.Mechanism), C.c_double, C.c_double, C.POINTER(C.c_double), C.c_double, C.c_double,
-                  C.c_double, C.c_double, C.c_int, C.POINTER(abi.Reactor)]
+                  C.c_double, C.c_double, C.c_int, C.POINTER(abi.Reactor), C.c_int]
     y = np.ascontiguousarray(Y, dtype=np.float64)
     out = abi.Reactor()
     f(mech.ptr(), T0, p0, y.ctypes.data_as(C.POINTER(C.c_double)), t_end, h0, rtol, atol,
-      min(int(max_attempts), 2**31 - 1), C.byref(out))
+      min(int(max_attempts), 2**31 - 1), C.byref(out), int(bool(krylov)))
     return out
 
 

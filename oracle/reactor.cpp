@@ -95,6 +95,62 @@ void lu_solve(const std::vector<double> &a, const std::vector<int> &piv, std::ve
     b[r] /= a[r * n + r];
   }
 }
+// buildArnoldi (src/ConstVolumeReactor.cpp:1858-1930) with the Krylov limit n_spec and minimum
+// 4: q0 = f0 / |f0| (e_0 when |f0| < 1e-30); column c: w = (omega(T', rhoY + eps q_c) - f0) / eps
+// with eps = 1e-6 (1 + |rhoY|) and T' the Newton temperature of the perturbed state, modified
+// Gram-Schmidt into H(0..c, c), H(c+1, c) = |w|; a new basis vector while c + 1 < 4 (|w| clamped
+// at 1e-30) or |w| > 1e-30 and c + 1 < n_spec.  Q and H are n_spec x n_spec, row-major, H zeroed.
+int arnoldi(const Mechanism &m, const std::vector<double> &rhoY, const std::vector<double> &f0, double T, double rho,
+            double E, std::vector<double> &Q, std::vector<double> &H) {
+  const int ns = m.n_spec, km = ns;
+  auto dot = [&](const double *a, const double *b) {
+    double s = 0;
+    for (int l = 0; l < ns; ++l) s += a[l] * b[l];
+    return s;
+  };
+  auto norm = [&](const double *a) { return std::sqrt(std::max(dot(a, a), 0.0)); };
+  std::fill(Q.begin(), Q.end(), 0.0);
+  std::fill(H.begin(), H.end(), 0.0);
+  const double eps = 1e-6 * (1 + norm(rhoY.data()));
+  const double nf = norm(f0.data());
+  if (nf < 1e-30) Q[0] = 1.0;
+  else
+    for (int l = 0; l < ns; ++l) Q[l] = f0[l] / nf;
+  int kd = 1;
+  std::vector<double> ye(ns), yk(ns), q1(m.n_reac), q2(m.n_reac), fe(ns), w(ns);
+  for (int col = 0; col < km; ++col) {
+    double imw = 0;
+    for (int l = 0; l < ns; ++l) {
+      ye[l] = rhoY[l] + eps * Q[col * ns + l];
+      yk[l] = ye[l] / rho;
+      imw += yk[l] / m.mw[l];
+    }
+    const double ts = temperature(m, T, imw, yk, E);
+    source(m, ts, ye, q1, q2, fe);
+    for (int l = 0; l < ns; ++l) w[l] = (fe[l] - f0[l]) / eps;
+    for (int row = 0; row <= col; ++row) {
+      const double hij = dot(&Q[row * ns], w.data());
+      H[row * km + col] = hij;
+      for (int l = 0; l < ns; ++l) w[l] -= hij * Q[row * ns + l];
+    }
+    double hn = norm(w.data());
+    if (col + 1 < km) H[(col + 1) * km + col] = hn;
+    if (col + 1 < 4) {
+      if (hn < 1e-30) hn = 1e-30;
+      for (int l = 0; l < ns; ++l) Q[(col + 1) * ns + l] = w[l] / hn;
+      kd = col + 2;
+      continue;
+    }
+    if (hn > 1e-30 && col + 1 < km) {
+      for (int l = 0; l < ns; ++l) Q[(col + 1) * ns + l] = w[l] / hn;
+      kd = col + 2;
+    } else {
+      kd = col + 1;
+      break;
+    }
+  }
+  return kd;
+}
 }  // namespace
 
 void reactor_setup(const Mechanism &m, double T0, double p0, const double *Y, double t_end, double h0,
@@ -123,12 +179,13 @@ void reactor_setup(const Mechanism &m, double T0, double p0, const double *Y, do
   st.step = st.n_reject = st.status = 0;
 }
 
-void reactor_advance(const Mechanism &m, ReactorState &st, int max_attempts, double rtol, double atol) {
+void reactor_advance(const Mechanism &m, ReactorState &st, int max_attempts, double rtol, double atol, bool krylov) {
   const int ns = m.n_spec, nr = m.n_reac;
   if (st.status || st.time >= st.t_end) return;
   std::vector<double> &rhoY = st.rhoY;
   std::vector<double> q1(nr), q2(nr), omega(ns), k1(ns), k2(ns), k3(ns), k4(ns), ys(ns), yk(ns), lhs(ns * ns);
   std::vector<int> piv(ns);
+  std::vector<double> Q(ns * ns), H(ns * ns), f(ns);
   const double rho = st.rho, E = st.E;
   for (int a = 0; a < max_attempts && st.time < st.t_end; ++a) {
     source(m, st.T, rhoY, q1, q2, omega);
@@ -137,46 +194,102 @@ void reactor_advance(const Mechanism &m, ReactorState &st, int max_attempts, dou
       st.status |= 2;
       break;
     }
-    for (int r = 0; r < ns; ++r)
-      for (int c = 0; c < ns; ++c) {
-        double zz = 0;
-        if (rhoY[c] > 1e-30) {
-          for (int q = 0; q < nr; ++q)
-            zz += (m.stoi_b[q * ns + r] - m.stoi_f[q * ns + r]) *
-                  (m.stoi_f[q * ns + c] * q1[q] - m.stoi_b[q * ns + c] * q2[q]);
-          zz /= rhoY[c];
+    double imw = 0, ts = 0;
+    if (krylov) {
+      // build_arnoldi = 1 (:446-594): Arnoldi basis Q (Krylov dimension kd <= n_spec) of
+      // finite-difference Jacobian products, LU of I - h gamma H, each stage projected, solved
+      // and projected back; stages 3 and 4 take the correction as solve(g) - g, stages 1 and 2 as
+      // g - solve(g), as the reference does
+      const int kd = arnoldi(m, rhoY, omega, st.T, rho, E, Q, H);
+      std::vector<double> L(kd * kd);
+      std::vector<int> pk(kd);
+      for (int i = 0; i < kd; ++i)
+        for (int j = 0; j < kd; ++j)
+          L[i * kd + j] = i == j ? 1.0 - h * kGamma * H[i * ns + j] : -h * kGamma * H[i * ns + j];
+      lu(L, pk, kd);
+      auto stage = [&](const std::vector<double> &f, bool flip, std::vector<double> &kk) {
+        std::vector<double> g(kd), sol(kd);
+        for (int q = 0; q < kd; ++q) {
+          double d = 0;
+          for (int l = 0; l < ns; ++l) d += Q[q * ns + l] * f[l];
+          g[q] = sol[q] = d;
         }
-        const double j = zz * 1e+3 * m.mw[r];
-        lhs[r * ns + c] = r == c ? 1.0 - h * kGamma * j : -h * kGamma * j;
+        lu_solve(L, pk, sol, kd);
+        for (int q = 0; q < kd; ++q) g[q] = flip ? sol[q] - g[q] : g[q] - sol[q];
+        for (int l = 0; l < ns; ++l) {
+          double sum = 0;
+          for (int q = 0; q < kd; ++q) sum += Q[q * ns + l] * g[q];
+          kk[l] = f[l] - sum;
+        }
+      };
+      stage(omega, false, k1);
+      imw = 0;
+      for (int l = 0; l < ns; ++l) {
+        ys[l] = rhoY[l] + h * kA21 * k1[l];
+        yk[l] = ys[l] / rho;
+        imw += yk[l] / m.mw[l];
       }
-    lu(lhs, piv, ns);
-    k1 = omega;
-    lu_solve(lhs, piv, k1, ns);
-    double imw = 0;
-    for (int l = 0; l < ns; ++l) {
-      ys[l] = rhoY[l] + h * kA21 * k1[l];
-      yk[l] = ys[l] / rho;
-      imw += yk[l] / m.mw[l];
+      ts = temperature(m, st.T, imw, yk, E);
+      source(m, ts, ys, q1, q2, omega);
+      for (int l = 0; l < ns; ++l) f[l] = omega[l] + kG21 * k1[l];
+      stage(f, false, k2);
+      for (int l = 0; l < ns; ++l) k2[l] = k2[l] - kG21 * k1[l];
+      imw = 0;
+      for (int l = 0; l < ns; ++l) {
+        ys[l] = rhoY[l] + h * (kA31 * k1[l] + kA32 * k2[l]);
+        yk[l] = ys[l] / rho;
+        imw += yk[l] / m.mw[l];
+      }
+      ts = temperature(m, ts, imw, yk, E);
+      source(m, ts, ys, q1, q2, omega);
+      for (int l = 0; l < ns; ++l) f[l] = omega[l] + kG31 * k1[l] + kG32 * k2[l];
+      stage(f, true, k3);
+      for (int l = 0; l < ns; ++l) k3[l] = k3[l] - kG31 * k1[l] - kG32 * k2[l];
+      for (int l = 0; l < ns; ++l) f[l] = omega[l] + kG41 * k1[l] + kG42 * k2[l] + kG43 * k3[l];
+      stage(f, true, k4);
+      for (int l = 0; l < ns; ++l) k4[l] = k4[l] - kG41 * k1[l] - kG42 * k2[l] - kG43 * k3[l];
+    } else {
+      for (int r = 0; r < ns; ++r)
+        for (int c = 0; c < ns; ++c) {
+          double zz = 0;
+          if (rhoY[c] > 1e-30) {
+            for (int q = 0; q < nr; ++q)
+              zz += (m.stoi_b[q * ns + r] - m.stoi_f[q * ns + r]) *
+                    (m.stoi_f[q * ns + c] * q1[q] - m.stoi_b[q * ns + c] * q2[q]);
+            zz /= rhoY[c];
+          }
+          const double j = zz * 1e+3 * m.mw[r];
+          lhs[r * ns + c] = r == c ? 1.0 - h * kGamma * j : -h * kGamma * j;
+        }
+      lu(lhs, piv, ns);
+      k1 = omega;
+      lu_solve(lhs, piv, k1, ns);
+      imw = 0;
+      for (int l = 0; l < ns; ++l) {
+        ys[l] = rhoY[l] + h * kA21 * k1[l];
+        yk[l] = ys[l] / rho;
+        imw += yk[l] / m.mw[l];
+      }
+      ts = temperature(m, st.T, imw, yk, E);
+      source(m, ts, ys, q1, q2, omega);
+      for (int l = 0; l < ns; ++l) k2[l] = omega[l] + kG21 * k1[l];
+      lu_solve(lhs, piv, k2, ns);
+      for (int l = 0; l < ns; ++l) k2[l] -= kG21 * k1[l];
+      imw = 0;
+      for (int l = 0; l < ns; ++l) {
+        ys[l] = rhoY[l] + h * (kA31 * k1[l] + kA32 * k2[l]);
+        yk[l] = ys[l] / rho;
+        imw += yk[l] / m.mw[l];
+      }
+      ts = temperature(m, ts, imw, yk, E);
+      source(m, ts, ys, q1, q2, omega);
+      for (int l = 0; l < ns; ++l) k3[l] = omega[l] + kG31 * k1[l] + kG32 * k2[l];
+      lu_solve(lhs, piv, k3, ns);
+      for (int l = 0; l < ns; ++l) k3[l] -= kG31 * k1[l] + kG32 * k2[l];
+      for (int l = 0; l < ns; ++l) k4[l] = omega[l] + kG41 * k1[l] + kG42 * k2[l] + kG43 * k3[l];
+      lu_solve(lhs, piv, k4, ns);
+      for (int l = 0; l < ns; ++l) k4[l] -= kG41 * k1[l] + kG42 * k2[l] + kG43 * k3[l];
     }
-    double ts = temperature(m, st.T, imw, yk, E);
-    source(m, ts, ys, q1, q2, omega);
-    for (int l = 0; l < ns; ++l) k2[l] = omega[l] + kG21 * k1[l];
-    lu_solve(lhs, piv, k2, ns);
-    for (int l = 0; l < ns; ++l) k2[l] -= kG21 * k1[l];
-    imw = 0;
-    for (int l = 0; l < ns; ++l) {
-      ys[l] = rhoY[l] + h * (kA31 * k1[l] + kA32 * k2[l]);
-      yk[l] = ys[l] / rho;
-      imw += yk[l] / m.mw[l];
-    }
-    ts = temperature(m, ts, imw, yk, E);
-    source(m, ts, ys, q1, q2, omega);
-    for (int l = 0; l < ns; ++l) k3[l] = omega[l] + kG31 * k1[l] + kG32 * k2[l];
-    lu_solve(lhs, piv, k3, ns);
-    for (int l = 0; l < ns; ++l) k3[l] -= kG31 * k1[l] + kG32 * k2[l];
-    for (int l = 0; l < ns; ++l) k4[l] = omega[l] + kG41 * k1[l] + kG42 * k2[l] + kG43 * k3[l];
-    lu_solve(lhs, piv, k4, ns);
-    for (int l = 0; l < ns; ++l) k4[l] -= kG41 * k1[l] + kG42 * k2[l] + kG43 * k3[l];
     double err = 0;
     for (int l = 0; l < ns; ++l) {
       ys[l] = rhoY[l] + h * (kB1 * k1[l] + kB2 * k2[l] + kB4 * k4[l]);

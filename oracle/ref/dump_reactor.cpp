@@ -8,7 +8,8 @@
 // tests/golden/make_mech.py to write tests/golden/h2_reactor_runs.json.
 //
 // Usage (from a directory holding ./input/<files>): dump_reactor <setup-file> <out.json> <n> [fixed]
-// With "fixed", every case runs the fixed-step forms instead (advance_fixed below).
+// With "fixed", every case runs the fixed-step forms instead (advance_fixed below); with
+// "krylov", the ROK4E sequence with build_arnoldi = 1.
 // Case 0 is the reference's example (T0 = 1000 K, p0 = 202650 Pa, X = 0.295775 H2 /
 // 0.147887 O2 / rest N2, 1.2 ms); cases 1..n-1 are seeded (T0, p0, phi) requests to 1 ms.
 #include <algorithm>
@@ -30,51 +31,110 @@ struct Run {
 };
 
 static void advance(const cfd::Species &sp, const cfd::Reaction &re, Run &r, int max_attempts, real rtol,
-                    real atol) {
+                    real atol, bool krylov = false) {
   namespace k = cfd::rok4e;
   const int ns = sp.n_spec, nr = re.n_reac;
   std::vector<real> q1(nr), q2(nr), od(ns), om(ns), k1(ns), k2(ns), k3(ns), k4(ns), ys(ns), yk(ns);
   for (int a = 0; a < max_attempts && r.time < r.t_end; ++a) {
     cfd::compute_src(0, r.T, sp, re, r.rhoY, q1, q2, od, om);
     const real h = std::min(r.h, r.t_end - r.time);
-    auto jac = cfd::compute_chem_src_jacobian(r.rhoY, sp, re, q1, q2);
-    std::vector<real> lhs(ns * ns);
-    for (int m = 0; m < ns; ++m)
-      for (int n = 0; n < ns; ++n)
-        lhs[m * ns + n] = m == n ? 1.0 - h * k::gamma * jac[m * ns + n] : -h * k::gamma * jac[m * ns + n];
-    auto piv = cfd::lu_decomp(lhs.data(), ns);
-    auto solve = [&](std::vector<real> &b) {
-      auto l = lhs;
-      cfd::lu_to_solution(l.data(), b.data(), ns, piv);
-    };
-    k1 = om;
-    solve(k1);
-    real imw = 0;
-    for (int l = 0; l < ns; ++l) {
-      ys[l] = r.rhoY[l] + h * k::alpha21 * k1[l];
-      yk[l] = ys[l] / r.rho;
-      imw += yk[l] / sp.mw[l];
+    real imw = 0, ts = 0;
+    if (krylov) {
+      // build_arnoldi = 1 (src/ConstVolumeReactor.cpp:446-594): cfd::buildArnoldi, the LU of
+      // I - h gamma H on the Krylov basis, each stage projected, solved and projected back; stages
+      // 3 and 4 form the correction as solve(g) - g, stages 1 and 2 as g - solve(g), as there
+      constexpr int KM = MAX_SPEC_NUMBER;
+      real Q[KM * KM]{}, H[KM * KM]{}, g[KM]{}, b[KM]{}, L[KM * KM]{}, lu[KM * KM]{};
+      const int kd = cfd::buildArnoldi(sp, r.rhoY, om.data(), Q, H, KM, 0, r.T, re, r.rho, r.E, 4);
+      for (int i = 0; i < kd; ++i)
+        for (int j = 0; j < kd; ++j)
+          L[i * kd + j] = i == j ? 1.0 - h * k::gamma * H[i * KM + j] : -h * k::gamma * H[i * KM + j];
+      auto piv = cfd::lu_decomp(L, kd);
+      auto stage = [&](const std::vector<real> &f, bool flip, std::vector<real> &kk) {
+        for (int q = 0; q < kd; ++q) {
+          real d = 0;
+          for (int l = 0; l < ns; ++l) d += Q[q * ns + l] * f[l];
+          g[q] = d;
+          b[q] = d;
+        }
+        for (int l = 0; l < kd * kd; ++l) lu[l] = L[l];
+        cfd::lu_to_solution(lu, flip ? g : b, kd, piv);
+        for (int q = 0; q < kd; ++q) g[q] -= b[q];
+        for (int l = 0; l < ns; ++l) {
+          real sum = 0;
+          for (int q = 0; q < kd; ++q) sum += Q[q * ns + l] * g[q];
+          kk[l] = f[l] - sum;
+        }
+      };
+      stage(om, false, k1);
+      imw = 0;
+      for (int l = 0; l < ns; ++l) {
+        ys[l] = r.rhoY[l] + h * k::alpha21 * k1[l];
+        yk[l] = ys[l] / r.rho;
+        imw += yk[l] / sp.mw[l];
+      }
+      ts = cfd::update_t(r.T, imw, sp, yk, r.E);
+      cfd::compute_src(0, ts, sp, re, ys, q1, q2, od, om);
+      std::vector<real> f(ns);
+      for (int l = 0; l < ns; ++l) f[l] = om[l] + k::gamma21Gamma * k1[l];
+      stage(f, false, k2);
+      for (int l = 0; l < ns; ++l) k2[l] = k2[l] - k::gamma21Gamma * k1[l];
+      imw = 0;
+      for (int l = 0; l < ns; ++l) {
+        ys[l] = r.rhoY[l] + h * (k::alpha31 * k1[l] + k::alpha32 * k2[l]);
+        yk[l] = ys[l] / r.rho;
+        imw += yk[l] / sp.mw[l];
+      }
+      ts = cfd::update_t(ts, imw, sp, yk, r.E);
+      cfd::compute_src(0, ts, sp, re, ys, q1, q2, od, om);
+      for (int l = 0; l < ns; ++l) f[l] = om[l] + k::gamma31Gamma * k1[l] + k::gamma32Gamma * k2[l];
+      stage(f, true, k3);
+      for (int l = 0; l < ns; ++l) k3[l] = k3[l] - k::gamma31Gamma * k1[l] - k::gamma32Gamma * k2[l];
+      for (int l = 0; l < ns; ++l)
+        f[l] = om[l] + k::gamma41Gamma * k1[l] + k::gamma42Gamma * k2[l] + k::gamma43Gamma * k3[l];
+      stage(f, true, k4);
+      for (int l = 0; l < ns; ++l)
+        k4[l] = k4[l] - k::gamma41Gamma * k1[l] - k::gamma42Gamma * k2[l] - k::gamma43Gamma * k3[l];
+    } else {
+      auto jac = cfd::compute_chem_src_jacobian(r.rhoY, sp, re, q1, q2);
+      std::vector<real> lhs(ns * ns);
+      for (int m = 0; m < ns; ++m)
+        for (int n = 0; n < ns; ++n)
+          lhs[m * ns + n] = m == n ? 1.0 - h * k::gamma * jac[m * ns + n] : -h * k::gamma * jac[m * ns + n];
+      auto piv = cfd::lu_decomp(lhs.data(), ns);
+      auto solve = [&](std::vector<real> &b) {
+        auto l = lhs;
+        cfd::lu_to_solution(l.data(), b.data(), ns, piv);
+      };
+      k1 = om;
+      solve(k1);
+      imw = 0;
+      for (int l = 0; l < ns; ++l) {
+        ys[l] = r.rhoY[l] + h * k::alpha21 * k1[l];
+        yk[l] = ys[l] / r.rho;
+        imw += yk[l] / sp.mw[l];
+      }
+      ts = cfd::update_t(r.T, imw, sp, yk, r.E);
+      cfd::compute_src(0, ts, sp, re, ys, q1, q2, od, om);
+      for (int l = 0; l < ns; ++l) k2[l] = om[l] + k::gamma21Gamma * k1[l];
+      solve(k2);
+      for (int l = 0; l < ns; ++l) k2[l] -= k::gamma21Gamma * k1[l];
+      imw = 0;
+      for (int l = 0; l < ns; ++l) {
+        ys[l] = r.rhoY[l] + h * (k::alpha31 * k1[l] + k::alpha32 * k2[l]);
+        yk[l] = ys[l] / r.rho;
+        imw += yk[l] / sp.mw[l];
+      }
+      ts = cfd::update_t(ts, imw, sp, yk, r.E);
+      cfd::compute_src(0, ts, sp, re, ys, q1, q2, od, om);
+      for (int l = 0; l < ns; ++l) k3[l] = om[l] + k::gamma31Gamma * k1[l] + k::gamma32Gamma * k2[l];
+      solve(k3);
+      for (int l = 0; l < ns; ++l) k3[l] -= k::gamma31Gamma * k1[l] + k::gamma32Gamma * k2[l];
+      for (int l = 0; l < ns; ++l)
+        k4[l] = om[l] + k::gamma41Gamma * k1[l] + k::gamma42Gamma * k2[l] + k::gamma43Gamma * k3[l];
+      solve(k4);
+      for (int l = 0; l < ns; ++l) k4[l] -= k::gamma41Gamma * k1[l] + k::gamma42Gamma * k2[l] + k::gamma43Gamma * k3[l];
     }
-    real ts = cfd::update_t(r.T, imw, sp, yk, r.E);
-    cfd::compute_src(0, ts, sp, re, ys, q1, q2, od, om);
-    for (int l = 0; l < ns; ++l) k2[l] = om[l] + k::gamma21Gamma * k1[l];
-    solve(k2);
-    for (int l = 0; l < ns; ++l) k2[l] -= k::gamma21Gamma * k1[l];
-    imw = 0;
-    for (int l = 0; l < ns; ++l) {
-      ys[l] = r.rhoY[l] + h * (k::alpha31 * k1[l] + k::alpha32 * k2[l]);
-      yk[l] = ys[l] / r.rho;
-      imw += yk[l] / sp.mw[l];
-    }
-    ts = cfd::update_t(ts, imw, sp, yk, r.E);
-    cfd::compute_src(0, ts, sp, re, ys, q1, q2, od, om);
-    for (int l = 0; l < ns; ++l) k3[l] = om[l] + k::gamma31Gamma * k1[l] + k::gamma32Gamma * k2[l];
-    solve(k3);
-    for (int l = 0; l < ns; ++l) k3[l] -= k::gamma31Gamma * k1[l] + k::gamma32Gamma * k2[l];
-    for (int l = 0; l < ns; ++l)
-      k4[l] = om[l] + k::gamma41Gamma * k1[l] + k::gamma42Gamma * k2[l] + k::gamma43Gamma * k3[l];
-    solve(k4);
-    for (int l = 0; l < ns; ++l) k4[l] -= k::gamma41Gamma * k1[l] + k::gamma42Gamma * k2[l] + k::gamma43Gamma * k3[l];
     real err = 0;
     std::vector<real> nw(ns);
     for (int l = 0; l < ns; ++l) {
@@ -165,6 +225,7 @@ static void advance_fixed(const cfd::Species &sp, const cfd::Reaction &re, Run &
 int main(int argc, char **argv) {
   if (argc < 4) return 2;
   const bool fixed = argc > 4 && std::string(argv[4]) == "fixed";
+  const bool krylov = argc > 4 && std::string(argv[4]) == "krylov";
   cfd::Parameter parameter{std::string(argv[1])};
   cfd::Species sp(parameter);
   cfd::Reaction re(parameter, sp);
@@ -242,10 +303,11 @@ int main(int argc, char **argv) {
         std::fprintf(out, "}%s", f + 1 < nf ? ",\n" : "");
       }
     } else {
-      advance(sp, re, r, 8, rtol, atol);
+      advance(sp, re, r, 8, rtol, atol, krylov);
       dump("after_8_attempts", false);
-      advance(sp, re, r, 1000000, rtol, atol);
-      dump("final", true);
+      // the Krylov form shrinks its steps until they stall short of t_end: 2000 attempts in all
+      advance(sp, re, r, krylov ? 1992 : 1000000, rtol, atol, krylov);
+      dump(krylov ? "after_2000_attempts" : "final", true);
     }
     std::fprintf(out, "}");
   }

@@ -30,6 +30,10 @@ oracle/ref_build.py) on the reference's example data files and keeps its JSON ou
                    explicit and EPI (each also with conserve_mass_corefl), DA and the explicit
                    three-stage Runge-Kutta (dt 1e-9 to 20 us, DA to 50 us, EPI dt 1e-7 to 0.4 ms), after 100
                    steps and at the end
+  h2_reactor_krylov_runs.json : the example case and 2 seeded requests through the ROK4E sequence
+                   with build_arnoldi = 1 (cfd::buildArnoldi, Krylov limit MAX_SPEC_NUMBER = 9),
+                   after 8 and after 2000 attempts (its steps shrink until they stall short of
+                   t_end: 1e6 attempts end at 0.82 ms, 0.30 ms and 19 us of 1.2, 1 and 1 ms)
 Usage: python tests/golden/make_mech.py [/path/to/reference]  (default: oracle/ref_build.py's
 reference_dir())
 """
@@ -77,6 +81,7 @@ def main(ref):
     print(run(ref, "h2_chem_states.json", files, 7, prog="dump_chem", extra=("48",)))
     print(run(ref, "h2_reactor_runs.json", files, 7, prog="dump_reactor", extra=("9",)))
     print(run(ref, "h2_reactor_fixed_runs.json", files, 7, prog="dump_reactor", extra=("3", "fixed")))
+    print(run(ref, "h2_reactor_krylov_runs.json", files, 7, prog="dump_reactor", extra=("3", "krylov")))
     files_2t = dict(files, two_temperature_file="example/squareCylinder2D_M10_air5_dns/input/chemistry/"
                                                 "two_temperature.dat")
     print(run(ref, "h2_two_temperature.json", files_2t, 7, prog="dump_2t", extra=("40",)))

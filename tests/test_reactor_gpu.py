@@ -102,3 +102,38 @@ def test_gpu_reactor_result_same_alone_and_in_a_batch(runs, h2):
     assert bytes(alone) == bytes(mixed)
     ctx1.close()
     ctxn.close()
+
+
+def test_krylov_reactors_match_reference_and_oracle(oracle_lib, h2):
+    """cb2_reactor_advance_krylov (build_arnoldi = 1) against the reference's cfd::buildArnoldi
+    sequence (tests/golden/h2_reactor_krylov_runs.json) and the oracle: the same accepted and
+    rejected attempts; the accepted time to 25% only: this form's error norm is dominated by
+    last-bit differences of the finite-difference products (eps = 1e-6), which the step
+    controller turns into step sizes (11% apart after 8 attempts on the device).  The states are
+    taken at those slightly different times: T to 1e-8 after 8 attempts and 1e-4 after 2000, the
+    major partial densities to 10x that of the largest."""
+    import torch
+    with open(os.path.join(HERE, "golden", "h2_reactor_krylov_runs.json")) as f:
+        kr = json.load(f)
+    ctx, st, n, keep = _batch(h2, kr)
+    ctx.reactor_advance_krylov(st.data_ptr(), n, 8, kr["rtol"], kr["atol"])
+    torch.cuda.synchronize()
+    got8 = _read(st, n)
+    ctx.reactor_advance_krylov(st.data_ptr(), n, 1992, kr["rtol"], kr["atol"])
+    torch.cuda.synchronize()
+    got2000 = _read(st, n)
+    for i, r in enumerate(kr["runs"]):
+        for s, key, n_att, tol in ((got8[i], "after_8_attempts", 8, 1e-8),
+                                   (got2000[i], "after_2000_attempts", 2000, 1e-4)):
+            g = r[key]
+            o = oracle_lib.reactor_run(h2, r["T0"], r["p0"], r["Y"], r["t_end"], kr["h0"], kr["rtol"], kr["atol"],
+                                       max_attempts=n_att, krylov=True)
+            for ref in (g, {"T": o.T, "time": o.time, "step": o.step, "n_reject": o.n_reject,
+                            "rhoY": list(o.rhoY)[:h2.ns]}):
+                assert s.step == ref["step"] and s.n_reject == ref["n_reject"], key
+                assert abs(s.T - ref["T"]) <= tol * ref["T"], (key, s.T, ref["T"])
+                rho_y, ref_y = np.array(list(s.rhoY)[:h2.ns]), np.array(ref["rhoY"])
+                major = ref_y > 1e-3 * ref_y.max()
+                assert np.abs(rho_y - ref_y)[major].max() <= 10 * tol * ref_y.max(), key
+                assert abs(s.time - ref["time"]) <= 0.25 * ref["time"], key
+    ctx.close()
